@@ -1,0 +1,335 @@
+#!/usr/bin/env python
+"""Benchmark of the B200-native MLS-MPM solid step.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload NAME]
+
+Workload (default): the 2,097,152-particle J2 linear-hardening drop (64x64x64-cell block, 8 particles
+per cell, 128^3 grid, aluminium E=70 GPa, nu=0.33, yield 250 MPa, hardening 1 GPa), seeded
+synthetic input. One step = one requested step of dt=2e-6 s, sub-stepped on the device to CFL 0.4
+(about 4 substeps); the metric counts actual substeps x particles. Multi-GPU runs are independent
+replicas per GPU (weak scaling; the single-scene path has no exchange step).
+
+--impl reference times the reference's CPU algorithm (the FP64 port under oracle/, all host threads,
+because the reference itself is JavaScript and no JS runtime exists here) on a bounded sub-block
+of the same workload and prints the same JSON line with "impl": "reference".
+"""
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "summer-particle-lab_b200")
+for _p in (ROOT, PKG):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+METRIC = "particle-steps/s, 2M-particle J2 MPM: surrogate+batched vs exact, same stress err"
+UNIT = "particle-steps/s"
+# algorithmic bytes per particle-step (FP32 state read once and written once) and per active node
+BYTES_PER_PARTICLE = {0: 200, 1: 200, 4: 208, 5: 208, 10: 216}
+BYTES_PER_NODE = 56
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="j2_drop")
+    ap.add_argument("--shape", default="64,64,64")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def make_scene(args):
+    from mpm_b200 import scenes
+    if args.workload == "j2_drop":
+        shape = tuple(int(s) for s in args.shape.split(","))
+        return scenes.j2_drop(shape=shape)
+    if args.workload == "j2_drop_plastic":
+        shape = tuple(int(s) for s in args.shape.split(","))
+        return scenes.j2_drop(shape=shape, plastic=True)
+    if args.workload == "elastic_cube":
+        return scenes.elastic_cube()
+    if args.workload == "thermal_j2":
+        return scenes.thermal_j2()
+    if args.workload == "coupled_collision":
+        return scenes.coupled_collision()
+    raise SystemExit(f"unknown workload {args.workload}")
+
+
+def sample_scene(scene, factor=2):
+    """A sub-block of the scene (every axis of the block divided by factor), same grid/material."""
+    from mpm_b200 import scenes
+    x = scene.x
+    d = scene.domain
+    lo = x.min(0)
+    hi = x.max(0)
+    ext = (hi - lo) / factor
+    keep = np.all(x <= lo + ext + 1e-12, axis=1)
+    s = scenes.Scene(name=scene.name + "_sample", domain=d, materials=scene.materials, x=x[keep].copy(),
+                     v=scene.v[keep].copy(), m=scene.m[keep].copy(), V=scene.V[keep].copy(),
+                     mat=scene.mat[keep].copy(), T=None if scene.T is None else scene.T[keep].copy(),
+                     meta=dict(scene.meta))
+    return s
+
+
+def cpu_oracle_rate(scene, dt, steps, threads):
+    """Oracle particle-steps/s on the given scene (steps of dt, OpenMP threads)."""
+    from oracle import oracle as orc
+    st = orc.state_from_scene(scene)
+    st.step(dt, threads=threads)  # warm-up
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        st.step(dt, threads=threads)
+    el = time.perf_counter() - t0
+    return scene.n * steps / el, el
+
+
+class Clocks:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_bench_{os.getpid()}.csv")
+
+    def __enter__(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        rows = []
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = sorted(float(r[1]) for r in rows if r[1].replace(".", "").isdigit())
+        mx = max(float(r[2]) for r in rows if r[2].replace(".", "").isdigit())
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if "Active" in r[5 + k] and "Not" not in r[5 + k]})
+        return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": mx, "reasons": reasons,
+                "samples": len(rows)}
+
+
+def read_traffic_per_particle():
+    """DRAM bytes per particle of one g2p2g launch from the committed ncu summary, if present."""
+    path = os.path.join(ROOT, "profiles", "g2p2g_j2_drop.md")
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        if line.strip().startswith("dram_bytes_per_particle:"):
+            try:
+                return float(line.split(":", 1)[1].split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        d = json.load(open(path))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    scene = make_scene(args)
+    sample = sample_scene(scene, 4)
+    threads = os.cpu_count() or 1
+    dt = 5e-7
+    from oracle import oracle as orc
+    st = orc.state_from_scene(sample)
+    for _ in range(max(1, args.warmup)):
+        st.step(dt, threads=threads)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        st.step(dt, threads=threads)
+    el = time.perf_counter() - t0
+    value = sample.n * args.steps / el
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "impl": "reference",
+            "config": {"workload": scene.meta["workload"], "sample_particles": sample.n,
+                       "dt_substep": dt},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": f"{sample.n}-particle sub-block of {scene.meta['workload']}, "
+                                       f"{args.steps} substeps of {dt} s"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        os.environ["CUDA_VISIBLE_DEVICES"] = str(local)
+    global np
+    import numpy as np
+    import torch
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(0)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        if dist is not None:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
+
+    from mpm_b200 import _lib
+    from mpm_b200.solver import Solver
+    scene = make_scene(args)
+    dt_req = scene.meta.get("dt", 2e-6)
+    model = scene.materials[0].model
+    sol = Solver(scene.domain, scene.n)
+    sol.upload(scene)
+    ext = torch.cuda.ExternalStream(sol.stream())
+    for _ in range(args.warmup):
+        sol.step(dt_req)
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    sol.profile(True)
+    launches0 = sol.launch_count()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    substeps = 0
+    with Clocks(local if world == 1 else 0) as clk:
+        torch.cuda.synchronize()
+        ev0.record(ext)
+        for _ in range(args.steps):
+            s, _adv = sol.step(dt_req)
+            substeps += s
+        ev1.record(ext)
+        torch.cuda.synchronize()
+    launches = sol.launch_count() - launches0
+    prof = sol.profile_read()
+    sol.profile(False)
+    ms = ev0.elapsed_time(ev1)
+    el_t = torch.tensor([ms, scene.n * substeps], dtype=torch.float64, device="cuda")
+    if dist is not None:
+        mx = el_t.clone()
+        dist.all_reduce(mx[0:1], op=dist.ReduceOp.MAX)
+        dist.all_reduce(mx[1:2], op=dist.ReduceOp.SUM)
+        el_t = mx
+    ms_all, psteps = float(el_t[0]), float(el_t[1])
+    value = psteps / (ms_all / 1e3)
+    # roofline of the dominant kernel (g2p2g): algorithmic bytes per launch / average launch time
+    dims, _ = sol.grid_dims()
+    gm, _gp = sol.grid_debug(dt_req / 4)
+    active_nodes = int(np.count_nonzero(gm > 0))
+    g_ms, g_n = prof["g2p2g"]
+    alg_bytes = scene.n * BYTES_PER_PARTICLE[model] + BYTES_PER_NODE * active_nodes
+    hbm, peak_kind = peaks()
+    achieved = alg_bytes / (g_ms / g_n / 1e3) / 1e9 if g_n else None
+    traffic_pp = read_traffic_per_particle()
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                "frac": achieved / hbm if achieved else None,
+                "traffic": (traffic_pp * scene.n if traffic_pp else None),
+                "kernel": "k_g2p2g", "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind,
+                "algorithmic_bytes_per_launch": alg_bytes, "launch_ms": g_ms / g_n if g_n else None,
+                "share_of_step": g_ms / sum(v[0] for v in prof.values()) if g_n else None}
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_all / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": scene.meta["workload"], "particles": scene.n, "grid_nodes": list(dims),
+                       "dt_requested": dt_req, "substeps_per_step": substeps / args.steps,
+                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                       "l2": f"particle state {scene.n * 160 / 1e6:.0f} MB > 126 MB L2 (no flush)",
+                       "active_nodes": active_nodes},
+            "roofline": roofline, "gpu_launches": launches,
+            "kernel_ms": {k: v[0] for k, v in prof.items()}, "clocks": clk.summary()}
+    # end to end through the C ABI with pinned host buffers (x, v in and out every step)
+    if not args.no_e2e:
+        import ctypes
+        n = scene.n
+        bufs = []
+        ptrs = []
+        for k in range(6):
+            p = ctypes.c_void_p()
+            _lib.check(_lib.lib().mpm_host_alloc(n * 4, ctypes.byref(p)))
+            arr = np.ctypeslib.as_array((ctypes.c_float * n).from_address(p.value))
+            arr[:] = (scene.x[:, k] if k < 3 else scene.v[:, k - 3])
+            bufs.append(arr)
+            ptrs.append(p)
+        io = _lib.MpmParticles(dtype=_lib.F32, x=ptrs[0], y=ptrs[1], z=ptrs[2], vx=ptrs[3], vy=ptrs[4], vz=ptrs[5])
+        sub = ctypes.c_int32()
+        for _ in range(max(1, args.warmup)):
+            _lib.check(_lib.lib().mpm_frame_host(sol.h, ctypes.byref(io), dt_req, 48, ctypes.byref(sub)), sol.h)
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        sub_total = 0
+        e0.record(ext)
+        for _ in range(args.steps):
+            _lib.check(_lib.lib().mpm_frame_host(sol.h, ctypes.byref(io), dt_req, 48, ctypes.byref(sub)), sol.h)
+            sub_total += sub.value
+        e1.record(ext)
+        torch.cuda.synchronize()
+        ems = e0.elapsed_time(e1)
+        et = torch.tensor([ems, n * sub_total], dtype=torch.float64, device="cuda")
+        if dist is not None:
+            dist.all_reduce(et[0:1], op=dist.ReduceOp.MAX)
+            dist.all_reduce(et[1:2], op=dist.ReduceOp.SUM)
+        line["e2e"] = {"value": float(et[1]) / (float(et[0]) / 1e3), "unit": UNIT,
+                       "h2d_bytes_per_step": 6 * 4 * n, "d2h_bytes_per_step": 6 * 4 * n,
+                       "api": "mpm_frame_host (f32 pinned host arrays)"}
+        for p in ptrs:
+            _lib.lib().mpm_host_free(p)
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        sample = sample_scene(scene, 4)
+        threads = os.cpu_count() or 1
+        rate, el = cpu_oracle_rate(sample, 5e-7, 3, threads)
+        line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
+                                "sample": f"{sample.n}-particle sub-block of the workload, 3 substeps "
+                                          f"({el:.1f} s), FP64 oracle with OpenMP"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    sol.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,213 @@
+/*
+ * mpm_b200 — C ABI of the B200-native explicit MLS-MPM solid step.
+ *
+ * This is the drop-in boundary for the reference's JavaScript step/state API of the 3D solid
+ * path (src/three/mpm.js:7-136, class MPM3) and the 2D facade named by it
+ * (src/solid-mpm.js:20-116, class SolidMPM). A Node N-API addon, ctypes or any C caller binds
+ * these functions; no PyTorch or C++ types cross the boundary. Plain pointers and sizes only.
+ *
+ * Ownership (reference: the caller owns particle arrays, MPM3 owns F, C and the grid,
+ * src/three/mpm.js:8-18): the library owns every device buffer behind an opaque handle.
+ * Upload and download functions take caller-owned host pointers and counts.
+ *
+ * Errors: every function returns an int status (MPM_OK = 0, negative on failure); no exception
+ * crosses the ABI. mpm_last_error() returns a text for the last failure on a handle.
+ * Threading: one handle per thread; calls on one handle are serialised on its own CUDA stream.
+ */
+#ifndef MPM_B200_H
+#define MPM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MPM_ABI_VERSION 1
+
+/* status codes */
+#define MPM_OK 0
+#define MPM_ERR_INVALID_ARG (-1)   /* reference: thrown Error on invalid domain (src/three/discretization.js:5-10) */
+#define MPM_ERR_OUT_OF_MEMORY (-2)
+#define MPM_ERR_CUDA (-3)
+#define MPM_ERR_NONFINITE (-4)     /* reference: RuntimeError on non-finite state (gpu/solver.py:1033-1034) */
+#define MPM_ERR_INVALID_J (-5)     /* det F <= 0 (src/simulation/particle-health.js:24-27) */
+#define MPM_ERR_OUT_OF_RANGE (-6)  /* a particle left the grid */
+#define MPM_ERR_TIMEOUT (-7)       /* a bounded device wait gave up */
+#define MPM_ERR_STATE (-8)         /* call out of order (e.g. step before upload) */
+#define MPM_ERR_CAPACITY (-9)      /* more particles than the handle's capacity
+                                      (reference: create returns false at capacity, src/three/simulation.js:36) */
+#define MPM_ERR_UNSUPPORTED (-10)  /* material model not built */
+
+/* device status flags (mpm_status) */
+#define MPM_STATUS_NONFINITE 0x1u
+#define MPM_STATUS_INVALID_J 0x2u
+#define MPM_STATUS_OUT_OF_RANGE 0x4u
+#define MPM_STATUS_TIMEOUT 0x8u
+#define MPM_STATUS_SCATTER_OVERFLOW 0x10u /* particle moved more than one cell in a substep (handled) */
+#define MPM_STATUS_SORT_MISMATCH 0x20u    /* tile keys and counts disagreed; the affected writes were skipped */
+
+/* material models (src/three/constitutive.js:6-19 numbering) */
+#define MPM_MODEL_FIXED_COROTATED 0
+#define MPM_MODEL_NEO_HOOKEAN 1
+#define MPM_MODEL_J2 4
+#define MPM_MODEL_J2_HARDENING 5
+#define MPM_MODEL_THERMAL_J2 10
+
+/* element type of the floating-point arrays of mpm_particles */
+#define MPM_F64 0
+#define MPM_F32 1
+
+/* Grid and boundary description (src/three/discretization.js:3-15): origin is
+ * floor(lower/h)*h - 2h, nodes per axis ceil((upper-origin)/h) + 3. Walls: separating slip on all
+ * six faces (src/three/mpm.js:93); optional sticky floor (every velocity component zero within one
+ * cell of lower[1]). CFL rule (src/three/mpm.js:43-55 in SI): dt <= min(dt_max,
+ * cfl*h/max(1, |v| + c*max(1, |F|_row |F|_col, compression)), grad_limit/max(1, sum|C|)),
+ * c = sqrt((lambda + 2 mu) V / m). */
+typedef struct mpm_domain {
+  double lower[3];
+  double upper[3];
+  double cell_size;
+  double gravity[3];       /* applied on the grid: v += dt g (equivalent to the reference's
+                              particle-side v += g dt before P2G, src/three/simulation.js:337-344) */
+  int32_t sticky_floor;
+  int32_t clamp_positions; /* clamp particles into [lower, upper] after advection
+                              (src/three/simulation.js:358-365) */
+  double mass_eps;         /* node mass threshold, 1e-12 in the reference (src/three/mpm.js:89) */
+  double cfl;              /* 0.175 reproduces the reference's 1.4*(h/8) */
+  double dt_max;           /* h/1920 in reference units; <= 0 means unbounded */
+  double grad_limit;       /* 0.08 in the reference */
+  int32_t cubic;           /* 1: every axis uses max(nodes) like src/three/mpm.js:18 */
+  int32_t reserved;
+} mpm_domain;
+
+/* Material (SI). Reference units are mu = lambda = 0.4 E and strengths as stress / E
+ * (src/three/mpm.js:34-37). J2: q = sqrt(6) mu |dev e| / J, yield A + B ep
+ * (src/three/metal-plasticity.js:12-27); thermal J2: (A + B ep)(1 - (1 - hot_ratio) theta),
+ * theta = clamp((T - T_ref)/(T_hot - T_ref), 0, 1) (src/three/thermal-plasticity.js:12-29). */
+typedef struct mpm_material {
+  int32_t model;
+  int32_t reserved;
+  double mu;
+  double lambda;
+  double yield_stress;   /* A */
+  double hardening;      /* B (model 5) or H (model 10) */
+  double T_ref;
+  double T_hot;
+  double hot_ratio;
+  double heat_fraction;  /* beta: share of plastic work converted to heat (gpu/mixed_material.py:150-172) */
+  double specific_heat;  /* cp, J/kg/K */
+} mpm_material;
+
+/* Host particle arrays (structure of arrays, like Simulation3's Float64Arrays,
+ * src/three/simulation.js:27-30; F and C are n x 9 row-major like MPM3.F, src/three/mpm.js:9).
+ * Any pointer may be NULL: on upload NULL means the default (v = 0, F = I, C = 0, ep = 0,
+ * T = 0, material 0, not pinned); on download NULL arrays are skipped. */
+typedef struct mpm_particles {
+  int32_t dtype;         /* MPM_F64 or MPM_F32 for every floating-point array below */
+  int32_t reserved;
+  void* x; void* y; void* z;
+  void* vx; void* vy; void* vz;
+  void* mass;
+  void* volume;
+  void* temperature;
+  void* plastic;         /* accumulated plastic strain (MPM3.plastic) */
+  void* F;               /* n x 9 */
+  void* C;               /* n x 9 */
+  int32_t* material;     /* index into the materials set with mpm_set_material */
+  uint8_t* pinned;       /* pinned particles scatter but are not moved (src/three/mpm.js:84,108) */
+} mpm_particles;
+
+/* FP64 ledger, reduced on the device (src/simulation/mechanical-diagnostics.js:16-37 and
+ * src/simulation/particle-health.js:12-30, SI units). */
+typedef struct mpm_ledger {
+  double mass, kinetic, affine, potential, elastic;
+  double momentum[3];
+  double angular[3];     /* includes the APIC spin m (h^2/4) (C21-C12, C02-C20, C10-C01) */
+  double min_j, max_j, max_plastic, max_von_mises;
+  double plastic_work;   /* heat put into particles by plastic work so far (J) */
+  int64_t count, nonfinite, invalid_j;
+} mpm_ledger;
+
+typedef struct mpm_handle mpm_handle;
+
+/* ---- lifetime (new MPM3(capacity), configure(domain): src/three/mpm.js:8-19) ---- */
+int mpm_abi_version(void);
+const char* mpm_error_string(int status);
+int mpm_create(const mpm_domain* domain, int64_t capacity, mpm_handle** out);
+int mpm_destroy(mpm_handle* h);
+const char* mpm_last_error(const mpm_handle* h);
+int mpm_configure_domain(mpm_handle* h, const mpm_domain* domain);
+int mpm_grid_dims(const mpm_handle* h, int32_t dims[3], double origin[3]);
+int mpm_set_material(mpm_handle* h, int32_t index, const mpm_material* material);
+int mpm_get_stream(mpm_handle* h, void** cuda_stream);
+
+/* ---- state (Simulation3 arrays + MPM3.F/C/plastic) ---- */
+int mpm_upload_particles(mpm_handle* h, int64_t n, const mpm_particles* p);
+int mpm_download_particles(mpm_handle* h, const mpm_particles* p);
+int mpm_count(const mpm_handle* h, int64_t* n);
+/* MPM3.reset() / resetParticle for all: F = I, C = 0, plastic = 0 (src/three/mpm.js:20-21) */
+int mpm_reset_deformation(mpm_handle* h);
+
+/* ---- stepping ---- */
+/* MPM3.stableStep(s) (src/three/mpm.js:40-55) on the current state */
+int mpm_stable_dt(mpm_handle* h, double* dt);
+/* Simulation3.step(dt) sub-stepping (src/three/simulation.js:305-311): advance by dt_requested in
+ * substeps of min(remaining, stable dt), at most max_substeps; the state stays on the device. */
+int mpm_step(mpm_handle* h, double dt_requested, int32_t max_substeps, int32_t* substeps,
+             double* advanced);
+/* nsteps substeps of exactly dt each (no CFL control) */
+int mpm_step_fixed(mpm_handle* h, double dt, int32_t nsteps);
+/* nsteps substeps, each of the scene's own stable dt (ensemble / CFL mode) */
+int mpm_step_cfl(mpm_handle* h, int32_t nsteps, double* time_advanced);
+/* MPM3.step(s, dt) drop-in (src/three/mpm.js:56-134): positions and velocities come from the
+ * caller's host arrays, one step of dt runs, and positions and velocities are written back.
+ * F, C and plastic strain stay on the device (MPM3 owns them). */
+int mpm_step_host(mpm_handle* h, const mpm_particles* io, double dt);
+
+/* Simulation3.step(dt) drop-in for the solid path (src/three/simulation.js:305-311): positions and
+ * velocities come from the caller's host arrays, the step advances dt_requested in CFL substeps on
+ * the device, and positions and velocities are written back. */
+int mpm_frame_host(mpm_handle* h, const mpm_particles* io, double dt_requested, int32_t max_substeps,
+                   int32_t* substeps);
+
+/* ---- diagnostics ---- */
+int mpm_ledger_compute(mpm_handle* h, mpm_ledger* out);
+/* MPM3.minJ(s) (src/three/mpm.js:135) */
+int mpm_min_j(mpm_handle* h, double* out);
+int mpm_status(mpm_handle* h, uint32_t* flags);
+int mpm_clear_status(mpm_handle* h);
+/* Grid after P2G of the current state with a step of dt: node mass and momentum including
+ * dt * (stress force + m g), in node order ((z*ny)+y)*nx+x. Arrays of nx*ny*nz and 3*nx*ny*nz. */
+int mpm_grid_debug(mpm_handle* h, double dt, double* mass, double* momentum);
+
+/* Per-kernel device time, measured with CUDA events on the handle's stream around each launch
+ * while enabled (reference: s.profile stage timers, src/three/mpm.js:60-133).
+ * Kernel ids: 0 begin, 1 grid update, 2 g2p2g, 3 scan, 4 sort scatter, 5 p2g, 6 keys. */
+#define MPM_PROFILE_KERNELS 7
+int mpm_profile_enable(mpm_handle* h, int32_t on);
+int mpm_profile_read(mpm_handle* h, double ms[MPM_PROFILE_KERNELS], int64_t launches[MPM_PROFILE_KERNELS]);
+/* number of kernels this handle has launched (all kinds) */
+int mpm_launch_count(mpm_handle* h, int64_t* count);
+
+/* ---- rollback and checkpoint (gpu/mixed_solver.py:453-480 keeps in-memory rollback copies) ---- */
+int mpm_snapshot(mpm_handle* h);
+int mpm_rollback(mpm_handle* h);
+int mpm_checkpoint_save(mpm_handle* h, const char* path);
+int mpm_checkpoint_load(mpm_handle* h, const char* path);
+
+/* ---- pinned host memory for fast uploads ---- */
+int mpm_host_alloc(size_t bytes, void** out);
+int mpm_host_free(void* p);
+
+/* ---- constitutive batch on the device (projectPlastic + stress, src/three/constitutive.js:52-106)
+ * F_in/F_out n x 9, ep/T/dep n, tau n x 9 (Kirchhoff). Stateless; runs on the default stream. */
+int mpm_return_map_batch(const mpm_material* material, int64_t n, const double* F_in,
+                         const double* ep, const double* T, double dt, double* F_out,
+                         double* dep, double* tau);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MPM_B200_H */

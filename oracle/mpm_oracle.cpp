@@ -1,0 +1,652 @@
+// CPU FP64 restatement of the reference's 3D MLS-MPM solid step.
+//
+// TEST INFRASTRUCTURE ONLY: this file is the checker. Only tests/, the smoke
+// check of __graft_entry__.py and the cpu-baseline leg of bench.py load it.
+// The product library (libmpm_b200.so) never links, calls or falls back to it.
+//
+// Parity pin: the reference is JavaScript and no JS runtime exists on either
+// machine, so this restatement is pinned against the reference's own
+// known-answer tests (tests/metal-plasticity.test.mjs:12-23,
+// tests/thermal-plasticity.test.mjs:12-31, tests/constitutive.test.mjs:10-25,
+// tests/three.test.mjs:8-21, src/simulation/vv-mpm.js:7), restated in
+// tests/test_oracle_kat.py.
+//
+// Units. The reference works in sandbox units with mu = lambda = 0.4 E and
+// strengths given as stress / E (src/three/mpm.js:34-37,
+// src/three/metal-plasticity.js:1-2). Every formula here takes mu, lambda and
+// strengths as parameters, so mu = lambda = 0.4 with strengths / E reproduces
+// the reference numbers exactly, and SI inputs give the SI restatement:
+//   q     = sqrt(6) * mu * |dev e| / J    (reference: sqrt(6)*.4*length/J)
+//   slope = 3 * mu / J                   (reference: 1.2/J)
+//
+// Build: oracle/build_oracle.py (g++ -O3 -fopenmp -shared).
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <vector>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+extern "C" {
+
+// Material parameters. model follows src/three/constitutive.js:6-19:
+// 0 fixed-corotated, 1 Neo-Hookean, 4 ideal J2, 5 linear-hardening J2,
+// 6 Johnson-Cook, 7 simplified Johnson-Cook, 10 thermal J2, 11 Norton creep.
+struct OracleMaterial {
+  int32_t model;
+  int32_t pad;
+  double mu, lambda;
+  // J2 / Johnson-Cook (src/three/metal-plasticity.js:3): A, B, n, C, rate0, Tref, Tm, m
+  double A, B, n, C, rate0, Tref, Tm, m;
+  // thermal (src/three/thermal-plasticity.js:3): Tref, Thot, hotRatio, A, H, rate, Q, n, stress
+  double tTref, tThot, tHotRatio, tA, tH, tRate, tQ, tN, tStress;
+  // plastic heating: heat fraction beta and specific heat cp (gpu/mixed_material.py:150-172)
+  double beta, cp;
+};
+
+struct OracleScene {
+  double origin[3];
+  double H;
+  int32_t dims[3];
+  int32_t sticky_floor;     // 1: nodes within one cell of lower[1] get v = 0
+  double lower[3], upper[3];
+  double gravity[3];
+  int32_t gravity_on_grid;  // 0: v += g dt on particles before P2G (src/three/simulation.js:337-344)
+  int32_t clamp_positions;  // 1: clamp x to [clamp_lo, clamp_hi] after G2P (src/three/simulation.js:358-365)
+  double clamp_lo[3], clamp_hi[3];
+  double mass_eps;          // grid mass threshold (src/three/mpm.js:89 uses 1e-12)
+  // CFL rule (src/three/mpm.js:43-55): dt <= min(dt_max, cfl*H/max(1, |v|+c*max(1,row*col,compr)),
+  // grad_limit/max(1, sum|C|)) with c = sqrt((lambda+2mu)/rho)
+  double cfl, dt_max, grad_limit;
+};
+
+struct OracleLedger {
+  double mass, kinetic, affine, potential, elastic;
+  double momentum[3], angular[3];
+  double min_j, max_j, max_plastic, max_von_mises;
+  int64_t nonfinite, invalid_j, unsupported_elastic;
+};
+
+// ---------------------------------------------------------------------------
+// 3x3 helpers: src/three/math.js:9-32
+static double det3(const double* a) {
+  return a[0] * (a[4] * a[8] - a[5] * a[7]) - a[1] * (a[3] * a[8] - a[5] * a[6]) +
+         a[2] * (a[3] * a[7] - a[4] * a[6]);
+}
+
+// math.js:10-15 inverseTranspose; returns false where |det| < 1e-10
+static bool inverse_transpose(const double* a, double* out) {
+  const double d = det3(a);
+  if (std::fabs(d) < 1e-10) return false;
+  out[0] = (a[4] * a[8] - a[5] * a[7]) / d;
+  out[1] = (a[5] * a[6] - a[3] * a[8]) / d;
+  out[2] = (a[3] * a[7] - a[4] * a[6]) / d;
+  out[3] = (a[2] * a[7] - a[1] * a[8]) / d;
+  out[4] = (a[0] * a[8] - a[2] * a[6]) / d;
+  out[5] = (a[1] * a[6] - a[0] * a[7]) / d;
+  out[6] = (a[1] * a[5] - a[2] * a[4]) / d;
+  out[7] = (a[2] * a[3] - a[0] * a[5]) / d;
+  out[8] = (a[0] * a[4] - a[1] * a[3]) / d;
+  return true;
+}
+
+// math.js:16-24: polar rotation by Newton averaging R <- (R + R^-T)/2, at most 8 iterations
+void oracle_rotation(const double* F, double* R) {
+  double r[9], inv[9];
+  std::memcpy(r, F, sizeof r);
+  for (int it = 0; it < 8; ++it) {
+    if (!inverse_transpose(r, inv)) {
+      for (int k = 0; k < 9; ++k) R[k] = (k % 4 == 0) ? 1.0 : 0.0;
+      return;
+    }
+    double diff = 0;
+    for (int k = 0; k < 9; ++k) {
+      const double v = 0.5 * (r[k] + inv[k]);
+      diff += std::fabs(v - r[k]);
+      r[k] = v;
+    }
+    if (diff < 1e-8) break;
+  }
+  std::memcpy(R, r, sizeof r);
+}
+
+// math.js:25-32: fixed-corotated Kirchhoff stress 2mu(F-R)F^T + lambda(J-1)J I
+void oracle_stress3(const double* F, double mu, double lambda, double* t) {
+  double R[9];
+  oracle_rotation(F, R);
+  const double J = det3(F);
+  for (int a = 0; a < 3; ++a)
+    for (int b = 0; b < 3; ++b) {
+      double s = 0;
+      for (int k = 0; k < 3; ++k) s += 2 * mu * (F[a * 3 + k] - R[a * 3 + k]) * F[b * 3 + k];
+      if (a == b) s += lambda * (J - 1) * J;
+      t[a * 3 + b] = s;
+    }
+}
+
+// constitutive.js:22-42: Jacobi diagonalisation of F^T F (at most 10 sweeps, pairs
+// (0,1),(0,2),(1,2), skip threshold 1e-13*(1+|app|+|aqq|)); sigma = sqrt(max(1e-16, lambda));
+// U = F V / sigma. Singular values are not sorted.
+void oracle_svd3(const double* F, double* u, double* v, double* sigma) {
+  double a[9] = {0};
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j)
+      for (int k = 0; k < 3; ++k) a[i * 3 + j] += F[k * 3 + i] * F[k * 3 + j];
+  for (int k = 0; k < 9; ++k) v[k] = (k % 4 == 0) ? 1.0 : 0.0;
+  static const int pairs[3][2] = {{0, 1}, {0, 2}, {1, 2}};
+  for (int sweep = 0; sweep < 10; ++sweep) {
+    bool changed = false;
+    for (const auto& pq : pairs) {
+      const int p = pq[0], q = pq[1];
+      const double apq = a[p * 3 + q];
+      if (std::fabs(apq) < 1e-13 * (1 + std::fabs(a[p * 3 + p]) + std::fabs(a[q * 3 + q]))) continue;
+      changed = true;
+      const double theta = 0.5 * std::atan2(2 * apq, a[q * 3 + q] - a[p * 3 + p]);
+      const double c = std::cos(theta), s = std::sin(theta);
+      const double app = a[p * 3 + p], aqq = a[q * 3 + q];
+      a[p * 3 + p] = c * c * app - 2 * s * c * apq + s * s * aqq;
+      a[q * 3 + q] = s * s * app + 2 * s * c * apq + c * c * aqq;
+      a[p * 3 + q] = a[q * 3 + p] = 0;
+      for (int k = 0; k < 3; ++k) {
+        if (k != p && k != q) {
+          const double x = a[k * 3 + p], y = a[k * 3 + q];
+          a[k * 3 + p] = a[p * 3 + k] = c * x - s * y;
+          a[k * 3 + q] = a[q * 3 + k] = s * x + c * y;
+        }
+        const double x = v[k * 3 + p], y = v[k * 3 + q];
+        v[k * 3 + p] = c * x - s * y;
+        v[k * 3 + q] = s * x + c * y;
+      }
+    }
+    if (!changed) break;
+  }
+  for (int k = 0; k < 3; ++k) sigma[k] = std::sqrt(std::max(1e-16, a[k * 3 + k]));
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      double s = 0;
+      for (int k = 0; k < 3; ++k) s += F[i * 3 + k] * v[k * 3 + j] / sigma[j];
+      u[i * 3 + j] = s;
+    }
+}
+
+// constitutive.js:43-47: F = U diag(sigma) V^T
+void oracle_compose(const double* u, const double* v, const double* sigma, double* F) {
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      double s = 0;
+      for (int k = 0; k < 3; ++k) s += u[i * 3 + k] * sigma[k] * v[j * 3 + k];
+      F[i * 3 + j] = s;
+    }
+}
+
+// constitutive.js:88-90
+double oracle_von_mises(const double* t, double J) {
+  const double s = 0.5 * ((t[0] - t[4]) * (t[0] - t[4]) + (t[4] - t[8]) * (t[4] - t[8]) +
+                          (t[8] - t[0]) * (t[8] - t[0])) +
+                   3 * (t[1] * t[1] + t[2] * t[2] + t[5] * t[5]);
+  return std::sqrt(std::max(0.0, s)) / std::max(1e-6, J);
+}
+
+// constitutive.js:92-106: models 0 and 2 use stress3 (model 2 scaled by hardening(jp), which is
+// 1 at the default jp = 1, constitutive.js:48), model 1 Neo-Hookean, models >= 3 Hencky
+int oracle_constitutive_stress(const double* F, int model, double mu, double lambda, double* tau) {
+  if (model == 0 || model == 2) {
+    oracle_stress3(F, mu, lambda, tau);
+    return 0;
+  }
+  if (model < 0 || model > 11) return -1;
+  for (int k = 0; k < 9; ++k) tau[k] = 0;
+  if (model == 1) {
+    const double pressure = lambda * std::log(std::max(det3(F), 1e-6));
+    for (int a = 0; a < 3; ++a)
+      for (int b = 0; b < 3; ++b) {
+        double s = 0;
+        for (int k = 0; k < 3; ++k) s += mu * F[a * 3 + k] * F[b * 3 + k];
+        if (a == b) s += pressure - mu;
+        tau[a * 3 + b] = s;
+      }
+    return 0;
+  }
+  double u[9], v[9], sigma[3], e[3];
+  oracle_svd3(F, u, v, sigma);
+  for (int k = 0; k < 3; ++k) e[k] = std::log(std::max(sigma[k], 1e-6));
+  const double trace = e[0] + e[1] + e[2];
+  for (int a = 0; a < 3; ++a)
+    for (int b = 0; b < 3; ++b) {
+      double s = 0;
+      for (int k = 0; k < 3; ++k) s += u[a * 3 + k] * (2 * mu * e[k] + lambda * trace) * u[b * 3 + k];
+      tau[a * 3 + b] = s;
+    }
+  return 0;
+}
+
+// constitutive.js:81-86: Kirchhoff stress from the returned principal stretches, Hencky form
+// (models other than snow): diag = 2 mu e + lambda tr e, tau = U diag U^T
+void oracle_principal_stress(const double* u, const double* sigma, double mu, double lambda,
+                             double* tau) {
+  double e[3];
+  for (int k = 0; k < 3; ++k) e[k] = std::log(sigma[k]);
+  const double trace = e[0] + e[1] + e[2];
+  for (int a = 0; a < 3; ++a)
+    for (int b = 0; b < 3; ++b) {
+      double s = 0;
+      for (int k = 0; k < 3; ++k) s += u[a * 3 + k] * (2 * mu * e[k] + lambda * trace) * u[b * 3 + k];
+      tau[a * 3 + b] = s;
+    }
+}
+
+// metal-plasticity.js:12-19
+double oracle_flow_stress(int model, double ep, double rate, double T, const OracleMaterial* p) {
+  if (model == 4) return p->A;
+  if (model == 5) return p->A + p->B * ep;
+  const double rateFactor = 1 + p->C * std::log(std::max(1.0, rate / p->rate0));
+  const double theta = std::max(0.0, std::min(1.0, (T - p->Tref) / (p->Tm - p->Tref)));
+  return (p->A + p->B * std::pow(ep, p->n)) * rateFactor * (model == 6 ? 1 - std::pow(theta, p->m) : 1);
+}
+
+// metal-plasticity.js:20-38 (models 4-7), mu = 0.4 in reference units
+void oracle_metal_return(const double* sigma, int model, double ep, double dt, double T,
+                         const OracleMaterial* p, double* out, double* increment) {
+  double e[3], dev[3];
+  for (int k = 0; k < 3; ++k) e[k] = std::log(std::max(sigma[k], 1e-6));
+  const double trace = e[0] + e[1] + e[2];
+  for (int k = 0; k < 3; ++k) dev[k] = e[k] - trace / 3;
+  const double length = std::sqrt(dev[0] * dev[0] + dev[1] * dev[1] + dev[2] * dev[2]);
+  const double J = std::max(1e-6, std::exp(trace));
+  const double q = std::sqrt(6.0) * p->mu * length / J;
+  double inc = 0;
+  if (q > oracle_flow_stress(model, ep, 0, T, p)) {
+    const double slope = 3 * p->mu / J;
+    if (model <= 5) {
+      inc = (q - oracle_flow_stress(model, ep, 0, T, p)) / (slope + (model == 5 ? p->B : 0));
+    } else {
+      double lo = 0, hi = q / slope;
+      for (int it = 0; it < 24; ++it) {
+        const double mid = (lo + hi) / 2;
+        if (q - slope * mid > oracle_flow_stress(model, ep + mid, mid / std::max(dt, 1e-12), T, p))
+          lo = mid;
+        else
+          hi = mid;
+      }
+      inc = (lo + hi) / 2;
+    }
+  }
+  const double scale = std::max(0.0, 1 - std::sqrt(1.5) * inc / std::max(length, 1e-20));
+  for (int k = 0; k < 3; ++k) out[k] = std::exp(trace / 3 + scale * dev[k]);
+  *increment = inc;
+}
+
+// thermal-plasticity.js:12-15
+double oracle_thermal_strength(double ep, double T, const OracleMaterial* p) {
+  const double theta = std::max(0.0, std::min(1.0, (T - p->tTref) / (p->tThot - p->tTref)));
+  return (p->tA + p->tH * ep) * (1 - (1 - p->tHotRatio) * theta);
+}
+
+// thermal-plasticity.js:17-21 (temperatures in degrees C, Kelvin offset 273.15)
+double oracle_creep_log_rate(double q, double T, const OracleMaterial* p) {
+  if (p->tRate == 0 || q <= 0) return -INFINITY;
+  const double act = std::max(-60.0, std::min(60.0, p->tQ / 8.314462618 *
+                                                         (1 / (p->tTref + 273.15) -
+                                                          1 / std::max(1.0, T + 273.15))));
+  return std::log(p->tRate) + act + p->tN * std::log(q / p->tStress);
+}
+
+// thermal-plasticity.js:22-40 (models 10, 11)
+void oracle_thermal_return(const double* sigma, int model, double ep, double dt, double T,
+                           const OracleMaterial* p, double* out, double* increment) {
+  double e[3], dev[3];
+  for (int k = 0; k < 3; ++k) e[k] = std::log(std::max(sigma[k], 1e-6));
+  const double tr = e[0] + e[1] + e[2];
+  for (int k = 0; k < 3; ++k) dev[k] = e[k] - tr / 3;
+  const double length = std::sqrt(dev[0] * dev[0] + dev[1] * dev[1] + dev[2] * dev[2]);
+  const double J = std::max(1e-6, std::exp(tr));
+  const double q = std::sqrt(6.0) * p->mu * length / J, slope = 3 * p->mu / J;
+  double inc = 0;
+  if (model == 10) {
+    const double factor = oracle_thermal_strength(0, T, p) / p->tA;
+    inc = std::max(0.0, (q - oracle_thermal_strength(ep, T, p)) / (slope + p->tH * factor));
+  } else if (dt > 0 && p->tRate > 0 && q > 1e-20) {
+    double lo = 0, hi = q / slope;
+    for (int k = 0; k < 32; ++k) {
+      const double mid = (lo + hi) / 2;
+      if (std::log(mid / dt) < oracle_creep_log_rate(std::max(0.0, q - slope * mid), T, p))
+        lo = mid;
+      else
+        hi = mid;
+    }
+    inc = (lo + hi) / 2;
+  }
+  const double scale = std::max(0.0, 1 - std::sqrt(1.5) * inc / std::max(length, 1e-20));
+  for (int k = 0; k < 3; ++k) out[k] = std::exp(tr / 3 + scale * dev[k]);
+  *increment = inc;
+}
+
+// constitutive.js:52-78 (projectPlastic) for the in-scope models 4-7, 10, 11; models 0, 1 return F
+// unchanged. Outputs the projected F, the plastic increment, and the cached Kirchhoff stress of
+// constitutive.js:81-86 (principalStress with mu, lambda). Returns -1 for models out of scope.
+int oracle_project(const double* F, const OracleMaterial* p, double ep, double dt, double T,
+                   double* Fout, double* increment, double* tau_cache) {
+  const int model = p->model;
+  if (model < 2) {
+    std::memcpy(Fout, F, 9 * sizeof(double));
+    *increment = 0;
+    oracle_constitutive_stress(F, model, p->mu, p->lambda, tau_cache);
+    return 0;
+  }
+  double u[9], v[9], s[3], proj[3], inc = 0;
+  oracle_svd3(F, u, v, s);
+  if (model >= 10 && model <= 11)
+    oracle_thermal_return(s, model, ep, dt, T, p, proj, &inc);
+  else if (model >= 4 && model <= 7)
+    oracle_metal_return(s, model, ep, dt, T, p, proj, &inc);
+  else
+    return -1;
+  oracle_compose(u, v, proj, Fout);
+  *increment = inc;
+  oracle_principal_stress(u, proj, p->mu, p->lambda, tau_cache);
+  return 0;
+}
+
+// ---------------------------------------------------------------------------
+// The step. src/three/mpm.js:56-134 (updateStress, P2G, grid update, G2P + F update,
+// return map), with gravity on particles as in src/three/simulation.js:337-344 or on the grid.
+// Arrays: x, v (n x 3), C, F, tau_cache (n x 9), ep, T, m, V (n), mat (n, index into mats),
+// pinned (n, may be null), cache_valid (n, may be null: stress recomputed from F).
+// Optional outputs: grid_mass (nodes), grid_mom (nodes x 3, after P2G incl. gravity),
+// grid_vel (nodes x 3, after the grid update).
+static inline int64_t node_index(const OracleScene* sc, int x, int y, int z) {
+  return ((int64_t)z * sc->dims[1] + y) * sc->dims[0] + x;
+}
+
+struct Stencil {
+  int base[3];
+  double frac[3];
+  double w[3][3];
+};
+
+// mpm.js:25-32
+static inline void stencil(const OracleScene* sc, const double* x, Stencil& st) {
+  for (int a = 0; a < 3; ++a) {
+    const double q = (x[a] - sc->origin[a]) / sc->H;
+    const int b = std::max(0, std::min(sc->dims[a] - 3, (int)std::floor(q - 0.5)));
+    const double t = q - b;
+    st.base[a] = b;
+    st.frac[a] = t;
+    st.w[a][0] = 0.5 * (1.5 - t) * (1.5 - t);
+    st.w[a][1] = 0.75 - (t - 1) * (t - 1);
+    st.w[a][2] = 0.5 * (t - 0.5) * (t - 0.5);
+  }
+}
+
+int oracle_step(const OracleScene* sc, const OracleMaterial* mats, int32_t nmat, int64_t n,
+                double* x, double* v, double* C, double* F, double* ep, double* T,
+                const double* m, const double* V, const int32_t* mat, const uint8_t* pinned,
+                double* tau_cache, uint8_t* cache_valid, double dt, double* grid_mass,
+                double* grid_mom, double* grid_vel, int32_t threads) {
+#ifdef _OPENMP
+  if (threads > 0) omp_set_num_threads(threads);
+#else
+  (void)threads;
+#endif
+  const int64_t nodes = (int64_t)sc->dims[0] * sc->dims[1] * sc->dims[2];
+  const double H = sc->H;
+  std::vector<double> gm(nodes, 0.0), gv(nodes * 3, 0.0);
+  std::vector<uint8_t> fixed(nodes, 0);
+  std::vector<double> tau((size_t)n * 9);
+  for (int64_t p = 0; p < n; ++p)
+    if (mat[p] < 0 || mat[p] >= nmat) return -1;
+
+  // gravity on particle velocities before the MPM step (simulation.js:337-344)
+  if (!sc->gravity_on_grid) {
+#pragma omp parallel for schedule(static)
+    for (int64_t p = 0; p < n; ++p) {
+      if (pinned && pinned[p]) continue;
+      for (int a = 0; a < 3; ++a) v[p * 3 + a] += sc->gravity[a] * dt;
+    }
+  }
+  // updateStress (mpm.js:33-39): cached stress for models >= 2 when valid, else from F
+#pragma omp parallel for schedule(static)
+  for (int64_t p = 0; p < n; ++p) {
+    const OracleMaterial* mp = &mats[mat[p]];
+    if (mp->model >= 2 && cache_valid && cache_valid[p])
+      std::memcpy(&tau[p * 9], &tau_cache[p * 9], 9 * sizeof(double));
+    else
+      oracle_constitutive_stress(&F[p * 9], mp->model, mp->mu, mp->lambda, &tau[p * 9]);
+  }
+  // P2G (mpm.js:66-85). With threads == 1 it is serial, so the summation order is the
+  // particle order; with more threads the scatter uses atomic adds (CPU baseline timing).
+  auto p2g_particle = [&](int64_t p, bool atomic) {
+    Stencil st;
+    stencil(sc, &x[p * 3], st);
+    const double mp = m[p];
+    double A[9];
+    for (int k = 0; k < 9; ++k) A[k] = mp * C[p * 9 + k] - dt * V[p] * 4 / (H * H) * tau[p * 9 + k];
+    for (int k = 0; k < 3; ++k)
+      for (int j = 0; j < 3; ++j)
+        for (int i = 0; i < 3; ++i) {
+          const int64_t nd = node_index(sc, st.base[0] + i, st.base[1] + j, st.base[2] + k);
+          const double w = st.w[0][i] * st.w[1][j] * st.w[2][k];
+          const double dx = (i - st.frac[0]) * H, dy = (j - st.frac[1]) * H, dz = (k - st.frac[2]) * H;
+          const double add[4] = {w * mp, w * (mp * v[p * 3 + 0] + A[0] * dx + A[1] * dy + A[2] * dz),
+                                 w * (mp * v[p * 3 + 1] + A[3] * dx + A[4] * dy + A[5] * dz),
+                                 w * (mp * v[p * 3 + 2] + A[6] * dx + A[7] * dy + A[8] * dz)};
+          if (atomic) {
+#pragma omp atomic
+            gm[nd] += add[0];
+#pragma omp atomic
+            gv[nd * 3 + 0] += add[1];
+#pragma omp atomic
+            gv[nd * 3 + 1] += add[2];
+#pragma omp atomic
+            gv[nd * 3 + 2] += add[3];
+          } else {
+            gm[nd] += add[0];
+            gv[nd * 3 + 0] += add[1];
+            gv[nd * 3 + 1] += add[2];
+            gv[nd * 3 + 2] += add[3];
+          }
+          if (pinned && pinned[p] && w > 1e-8) fixed[nd] = 1;
+        }
+  };
+  if (threads == 1) {
+    for (int64_t p = 0; p < n; ++p) p2g_particle(p, false);
+  } else {
+#pragma omp parallel for schedule(static)
+    for (int64_t p = 0; p < n; ++p) p2g_particle(p, true);
+  }
+  if (sc->gravity_on_grid) {
+    for (int64_t nd = 0; nd < nodes; ++nd)
+      for (int a = 0; a < 3; ++a) gv[nd * 3 + a] += dt * gm[nd] * sc->gravity[a];
+  }
+  if (grid_mass) std::memcpy(grid_mass, gm.data(), nodes * sizeof(double));
+  if (grid_mom) std::memcpy(grid_mom, gv.data(), nodes * 3 * sizeof(double));
+  // grid update (mpm.js:89-102): v = p/m, fixed nodes and separating slip on all six faces;
+  // optional sticky floor (all components zero within one cell of lower[1])
+#pragma omp parallel for schedule(static)
+  for (int64_t nd = 0; nd < nodes; ++nd) {
+    if (!(gm[nd] > sc->mass_eps)) {
+      gv[nd * 3] = gv[nd * 3 + 1] = gv[nd * 3 + 2] = 0;
+      continue;
+    }
+    const int ix = (int)(nd % sc->dims[0]);
+    const int iy = (int)((nd / sc->dims[0]) % sc->dims[1]);
+    const int iz = (int)(nd / ((int64_t)sc->dims[0] * sc->dims[1]));
+    const double q[3] = {sc->origin[0] + ix * H, sc->origin[1] + iy * H, sc->origin[2] + iz * H};
+    const bool sticky = sc->sticky_floor && q[1] < sc->lower[1] + H;
+    for (int a = 0; a < 3; ++a) {
+      double vel = gv[nd * 3 + a] / gm[nd];
+      if (sticky || fixed[nd] || (q[a] < sc->lower[a] + H && vel < 0) ||
+          (q[a] > sc->upper[a] - H && vel > 0))
+        vel = 0;
+      gv[nd * 3 + a] = vel;
+    }
+  }
+  if (grid_vel) std::memcpy(grid_vel, gv.data(), nodes * 3 * sizeof(double));
+  // G2P + F update (mpm.js:107-123), then the return map (mpm.js:126-131)
+  int status = 0;
+#pragma omp parallel for schedule(static) reduction(min : status)
+  for (int64_t p = 0; p < n; ++p) {
+    if (pinned && pinned[p]) continue;
+    Stencil st;
+    stencil(sc, &x[p * 3], st);
+    double vx = 0, vy = 0, vz = 0, c[9] = {0};
+    for (int k = 0; k < 3; ++k)
+      for (int j = 0; j < 3; ++j)
+        for (int i = 0; i < 3; ++i) {
+          const int64_t nd = node_index(sc, st.base[0] + i, st.base[1] + j, st.base[2] + k);
+          const double w = st.w[0][i] * st.w[1][j] * st.w[2][k];
+          const double dx = (i - st.frac[0]) * 4 / H, dy = (j - st.frac[1]) * 4 / H,
+                       dz = (k - st.frac[2]) * 4 / H;
+          const double a = w * gv[nd * 3], b = w * gv[nd * 3 + 1], cc = w * gv[nd * 3 + 2];
+          vx += a; vy += b; vz += cc;
+          c[0] += a * dx; c[1] += a * dy; c[2] += a * dz;
+          c[3] += b * dx; c[4] += b * dy; c[5] += b * dz;
+          c[6] += cc * dx; c[7] += cc * dy; c[8] += cc * dz;
+        }
+    double Fo[9];
+    std::memcpy(Fo, &F[p * 9], sizeof Fo);
+    for (int a = 0; a < 3; ++a)
+      for (int b = 0; b < 3; ++b) {
+        double val = Fo[a * 3 + b];
+        for (int k = 0; k < 3; ++k) val += dt * c[a * 3 + k] * Fo[k * 3 + b];
+        F[p * 9 + a * 3 + b] = val;
+      }
+    std::memcpy(&C[p * 9], c, sizeof c);
+    v[p * 3] = vx; v[p * 3 + 1] = vy; v[p * 3 + 2] = vz;
+    x[p * 3] += dt * vx; x[p * 3 + 1] += dt * vy; x[p * 3 + 2] += dt * vz;
+    if (sc->clamp_positions)
+      for (int a = 0; a < 3; ++a)
+        x[p * 3 + a] = std::max(sc->clamp_lo[a], std::min(sc->clamp_hi[a], x[p * 3 + a]));
+    const OracleMaterial* mp = &mats[mat[p]];
+    if (mp->model >= 2) {
+      double Fn[9], inc = 0, tc[9];
+      if (oracle_project(&F[p * 9], mp, ep[p], dt, T[p], Fn, &inc, tc) != 0) {
+        status = -2;
+        continue;
+      }
+      std::memcpy(&F[p * 9], Fn, sizeof Fn);
+      ep[p] += inc;
+      if (tau_cache) std::memcpy(&tau_cache[p * 9], tc, sizeof tc);
+      if (cache_valid) cache_valid[p] = 1;
+      // plastic-work heating: dT = beta * tau_eq(returned) * dep / (rho0 * cp), tau_eq the
+      // Kirchhoff von Mises stress sqrt(6) mu |dev e_returned| (gpu/mixed_material.py:150-172)
+      if (mp->beta > 0 && inc > 0) {
+        double u[9], vv[9], s[3], e[3];
+        oracle_svd3(&F[p * 9], u, vv, s);
+        for (int k = 0; k < 3; ++k) e[k] = std::log(std::max(s[k], 1e-6));
+        const double tr = (e[0] + e[1] + e[2]) / 3;
+        double dn = 0;
+        for (int k = 0; k < 3; ++k) dn += (e[k] - tr) * (e[k] - tr);
+        const double tau_eq = std::sqrt(6.0) * mp->mu * std::sqrt(dn);
+        T[p] += mp->beta * tau_eq * inc * V[p] / (m[p] * mp->cp);
+      }
+    }
+  }
+  return status;
+}
+
+// src/three/mpm.js:43-55 generalised: c = sqrt((lambda + 2 mu)/rho) per particle
+// (reference units: sqrt(19200 stiffness) since lambda + 2mu = 1.2 E = 1.2*16000*stiffness*rho)
+double oracle_stable_dt(const OracleScene* sc, const OracleMaterial* mats, int64_t n,
+                        const double* v, const double* C, const double* F, const double* m,
+                        const double* V, const int32_t* mat) {
+  double maxw = 1, grad = 1;
+  for (int64_t p = 0; p < n; ++p) {
+    double row = 0, col = 0, g = 0;
+    for (int a = 0; a < 3; ++a) {
+      double r = 0, c = 0;
+      for (int b = 0; b < 3; ++b) {
+        r += std::fabs(F[p * 9 + a * 3 + b]);
+        c += std::fabs(F[p * 9 + b * 3 + a]);
+        g += std::fabs(C[p * 9 + a * 3 + b]);
+      }
+      row = std::max(row, r);
+      col = std::max(col, c);
+    }
+    const OracleMaterial* mp = &mats[mat[p]];
+    const double compression = mp->model == 1 ? 1 / std::max(0.05, det3(&F[p * 9])) : 1;
+    const double c = std::sqrt((mp->lambda + 2 * mp->mu) * V[p] / m[p]);
+    const double speed = std::sqrt(v[p * 3] * v[p * 3] + v[p * 3 + 1] * v[p * 3 + 1] + v[p * 3 + 2] * v[p * 3 + 2]);
+    maxw = std::max(maxw, speed + c * std::max(1.0, std::max(row * col, compression)));
+    grad = std::max(grad, g);
+  }
+  return std::min(sc->dt_max, std::min(sc->cfl * sc->H / maxw, sc->grad_limit / grad));
+}
+
+// src/simulation/mechanical-diagnostics.js:9-37 (SI: no sandbox length factor) and
+// src/simulation/particle-health.js:12-30. Elastic energy density per reference volume:
+// model 0 mu|F-R|^2 + lambda/2 (J-1)^2; model 1 mu/2(|F|^2-3) - mu log J + lambda/2 log^2 J;
+// Hencky models (an extension; the reference reports them unsupported) mu|e|^2 + lambda/2 tr^2 e.
+void oracle_ledger(const OracleScene* sc, const OracleMaterial* mats, int64_t n, const double* x,
+                   const double* v, const double* C, const double* F, const double* ep,
+                   const double* m, const double* V, const int32_t* mat, OracleLedger* out) {
+  OracleLedger L{};
+  L.min_j = INFINITY;
+  L.max_j = -INFINITY;
+  const double D = sc->H * sc->H / 4;
+  for (int64_t p = 0; p < n; ++p) {
+    const double* Fp = &F[p * 9];
+    const double* Cp = &C[p * 9];
+    bool finite = std::isfinite(m[p]);
+    for (int a = 0; a < 3; ++a) finite = finite && std::isfinite(x[p * 3 + a]) && std::isfinite(v[p * 3 + a]);
+    for (int k = 0; k < 9; ++k) finite = finite && std::isfinite(Fp[k]) && std::isfinite(Cp[k]);
+    const double J = det3(Fp);
+    if (std::isfinite(J)) {
+      L.min_j = std::min(L.min_j, J);
+      L.max_j = std::max(L.max_j, J);
+      if (J <= 0) L.invalid_j++;
+    } else {
+      finite = false;
+    }
+    if (!finite) L.nonfinite++;
+    const double mp = m[p];
+    const double* xp = &x[p * 3];
+    const double* vp = &v[p * 3];
+    L.mass += mp;
+    L.kinetic += 0.5 * mp * (vp[0] * vp[0] + vp[1] * vp[1] + vp[2] * vp[2]);
+    L.potential -= mp * (sc->gravity[0] * xp[0] + sc->gravity[1] * xp[1] + sc->gravity[2] * xp[2]);
+    double c2 = 0;
+    for (int k = 0; k < 9; ++k) c2 += Cp[k] * Cp[k];
+    L.affine += 0.5 * mp * D * c2;
+    const double P[3] = {mp * vp[0], mp * vp[1], mp * vp[2]};
+    double Hh[3] = {xp[1] * P[2] - xp[2] * P[1], xp[2] * P[0] - xp[0] * P[2], xp[0] * P[1] - xp[1] * P[0]};
+    const double spin[3] = {Cp[7] - Cp[5], Cp[2] - Cp[6], Cp[3] - Cp[1]};
+    for (int k = 0; k < 3; ++k) {
+      Hh[k] += mp * D * spin[k];
+      L.momentum[k] += P[k];
+      L.angular[k] += Hh[k];
+    }
+    const OracleMaterial* mt = &mats[mat[p]];
+    double W = 0;
+    if (!(J > 0)) {
+      L.unsupported_elastic++;
+    } else if (mt->model == 0) {
+      double R[9];
+      oracle_rotation(Fp, R);
+      double s = 0;
+      for (int k = 0; k < 9; ++k) s += (Fp[k] - R[k]) * (Fp[k] - R[k]);
+      W = mt->mu * s + 0.5 * mt->lambda * (J - 1) * (J - 1);
+    } else if (mt->model == 1) {
+      double s = 0;
+      for (int k = 0; k < 9; ++k) s += Fp[k] * Fp[k];
+      const double lj = std::log(J);
+      W = 0.5 * mt->mu * (s - 3) - mt->mu * lj + 0.5 * mt->lambda * lj * lj;
+    } else {
+      double u[9], vv[9], s[3], e[3];
+      oracle_svd3(Fp, u, vv, s);
+      for (int k = 0; k < 3; ++k) e[k] = std::log(std::max(s[k], 1e-6));
+      const double tr = e[0] + e[1] + e[2];
+      W = mt->mu * (e[0] * e[0] + e[1] * e[1] + e[2] * e[2]) + 0.5 * mt->lambda * tr * tr;
+    }
+    L.elastic += V[p] * W;
+    if (ep) L.max_plastic = std::max(L.max_plastic, ep[p]);
+    double tau[9];
+    oracle_constitutive_stress(Fp, mt->model == 0 || mt->model == 1 ? mt->model : 4, mt->mu, mt->lambda, tau);
+    L.max_von_mises = std::max(L.max_von_mises, oracle_von_mises(tau, J));
+  }
+  *out = L;
+}
+
+}  // extern "C"

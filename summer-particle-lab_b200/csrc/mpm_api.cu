@@ -1,0 +1,1134 @@
+// C ABI of the B200-native MLS-MPM solid step: handle lifetime, buffers, stepping, diagnostics.
+// Declarations and the reference interface each function replaces: include/mpm_b200.h.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/mpm_b200.h"
+#include "mpm_internal.h"
+
+using mpm::Ctx;
+using mpm::MaterialDev;
+using mpm::SceneDev;
+
+namespace {
+
+constexpr int kMaxMats = 256;
+constexpr uint32_t kCheckpointMagic = 0x3242504du;  // "MPB2"
+constexpr uint32_t kCheckpointVersion = 1;
+
+size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+struct Carver {
+  char* base;
+  size_t off = 0;
+  template <typename T>
+  T* take(size_t count) {
+    off = align_up(off, 256);
+    T* p = base ? reinterpret_cast<T*>(base + off) : nullptr;
+    off += count * sizeof(T);
+    return p;
+  }
+};
+
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static bool tried = false;
+  if (!tried) {
+    tried = true;
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  }
+  return fn;
+}
+
+}  // namespace
+
+struct mpm_handle {
+  std::string err;
+  cudaStream_t stream = nullptr;
+  int num_sms = 148;
+  mpm_domain dom{};
+  SceneDev scene{};
+  std::vector<mpm_material> mats_host;
+  std::vector<MaterialDev> mats_dev;
+  std::vector<char> mat_set;
+  int64_t cap = 0;
+  int64_t n = 0;
+  bool uploaded = false;
+  bool grid_valid = false;   // acc[step_index & 1] holds the scatter of the current state
+  bool pending_grid = false; // a scatter sits in acc[step_index & 1] (valid or stale)
+  int use_tma = 1;
+  int last_estimate = 0;
+  // device memory
+  void* pblock = nullptr;  size_t pblock_bytes = 0;   // particle arrays
+  void* gblock = nullptr;  size_t gblock_bytes = 0;   // grid + sort + control
+  void* snap = nullptr;    bool snap_valid = false;  int64_t snap_n = 0;
+  void* staging = nullptr; size_t staging_bytes = 0;
+  void** dptr_table = nullptr;                          // 12 device pointers for conversion
+  double* ledger_partials = nullptr;
+  double* ledger_out = nullptr;
+  mpm::Ctrl* host_ctrl = nullptr;                        // pinned readback
+  double* host_ledger = nullptr;                         // pinned readback
+  Ctx ctx{};
+  int g2p2g_blocks = 0, p2g_blocks = 0, grid_blocks = 0;
+  // profiling: event pairs around launches while enabled
+  bool profiling = false;
+  std::vector<cudaEvent_t> ev_pool;
+  std::vector<std::pair<int, int>> ev_used;  // (kernel id, index of the start event in ev_pool)
+  size_t ev_next = 0;
+  int64_t launches = 0;
+};
+
+// Records a CUDA event pair around one launch when profiling is on.
+struct ProfScope {
+  mpm_handle* h;
+  int id;
+  size_t idx = 0;
+  bool on;
+  ProfScope(mpm_handle* hh, int kid) : h(hh), id(kid), on(hh->profiling) {
+    ++h->launches;
+    if (!on) return;
+    if (h->ev_next + 2 > h->ev_pool.size()) {
+      for (int k = 0; k < 256; ++k) {
+        cudaEvent_t e;
+        cudaEventCreate(&e);
+        h->ev_pool.push_back(e);
+      }
+    }
+    idx = h->ev_next;
+    h->ev_next += 2;
+    cudaEventRecord(h->ev_pool[idx], h->stream);
+  }
+  ~ProfScope() {
+    if (!on) return;
+    cudaEventRecord(h->ev_pool[idx + 1], h->stream);
+    h->ev_used.push_back({id, static_cast<int>(idx)});
+  }
+};
+
+#define MPM_CUDA(h, call)                                                          \
+  do {                                                                             \
+    cudaError_t e_ = (call);                                                       \
+    if (e_ != cudaSuccess) {                                                       \
+      (h)->err = std::string(#call) + ": " + cudaGetErrorString(e_);               \
+      return e_ == cudaErrorMemoryAllocation ? MPM_ERR_OUT_OF_MEMORY : MPM_ERR_CUDA; \
+    }                                                                              \
+  } while (0)
+
+static int fail(mpm_handle* h, int code, const std::string& msg) {
+  if (h) h->err = msg;
+  return code;
+}
+
+// Scene geometry from the domain (src/three/discretization.js:12-14) and the node thresholds the
+// grid update uses, computed in double exactly as the reference compares q < lower + h.
+static int build_scene(mpm_handle* h, const mpm_domain& d, SceneDev& s) {
+  const double H = d.cell_size;
+  if (!(H > 0) || !std::isfinite(H)) return fail(h, MPM_ERR_INVALID_ARG, "cell_size must be positive");
+  int dims[3];
+  double origin[3];
+  for (int a = 0; a < 3; ++a) {
+    if (!std::isfinite(d.lower[a]) || !std::isfinite(d.upper[a]) || !(d.upper[a] - d.lower[a] >= H))
+      return fail(h, MPM_ERR_INVALID_ARG, "domain must span at least one cell on every axis");
+    origin[a] = std::floor(d.lower[a] / H + 1e-9) * H - 2 * H;
+    dims[a] = static_cast<int>(std::ceil((d.upper[a] - origin[a]) / H - 1e-9)) + 3;
+  }
+  if (d.cubic) {
+    const int m = std::max(dims[0], std::max(dims[1], dims[2]));
+    dims[0] = dims[1] = dims[2] = m;
+  }
+  std::memset(&s, 0, sizeof s);
+  s.H = static_cast<float>(H);
+  s.invH = static_cast<float>(1.0 / H);
+  for (int a = 0; a < 3; ++a) {
+    if (dims[a] > 1023 || dims[a] < 4) return fail(h, MPM_ERR_INVALID_ARG, "grid must have 4..1023 nodes per axis");
+    s.dims[a] = dims[a];
+    s.tiles[a] = ((dims[a] - 3) >> 2) + 1;
+    s.gdim[a] = 4 * s.tiles[a] + 4;
+    s.ntiles[a] = s.gdim[a] / 4;
+    s.origin[a] = origin[a];
+    int lo = -1, hi = dims[a];
+    for (int i = 0; i < dims[a]; ++i) {
+      const double q = origin[a] + i * H;
+      if (q < d.lower[a] + H) lo = i;
+      if (q > d.upper[a] - H && hi == dims[a]) hi = i;
+    }
+    s.wall_lo[a] = lo;
+    s.wall_hi[a] = hi;
+    const double clo = d.lower[a] + 1e-6 * H, chi = d.upper[a] - 1e-6 * H;
+    const double qmax = static_cast<double>((static_cast<long long>(dims[a]) - 1) << mpm::kFracBits);
+    s.qlo[a] = static_cast<unsigned>(std::min(qmax, std::max(0.0, std::ceil((clo - origin[a]) / H * 4194304.0))));
+    s.qhi[a] = static_cast<unsigned>(std::min(qmax, std::max(0.0, std::floor((chi - origin[a]) / H * 4194304.0))));
+    s.gravity[a] = static_cast<float>(d.gravity[a]);
+  }
+  s.clamp = d.clamp_positions ? 1 : 0;
+  s.sticky = d.sticky_floor ? 1 : 0;
+  s.mass_eps = static_cast<float>(d.mass_eps > 0 ? d.mass_eps : 1e-12);
+  s.cfl = static_cast<float>(d.cfl > 0 ? d.cfl : 0.4);
+  s.dt_max = static_cast<float>(d.dt_max > 0 ? d.dt_max : 3.0e38);
+  s.grad_limit = static_cast<float>(d.grad_limit > 0 ? d.grad_limit : 0.08);
+  s.node_base = 0;
+  s.tile_base = 0;
+  s.node_tile_base = 0;
+  s.mat_base = 0;
+  return MPM_OK;
+}
+
+static int free_device(mpm_handle* h) {
+  if (h->pblock) cudaFree(h->pblock);
+  if (h->gblock) cudaFree(h->gblock);
+  if (h->snap) cudaFree(h->snap);
+  if (h->staging) cudaFree(h->staging);
+  if (h->dptr_table) cudaFree(h->dptr_table);
+  if (h->ledger_partials) cudaFree(h->ledger_partials);
+  if (h->host_ctrl) cudaFreeHost(h->host_ctrl);
+  if (h->host_ledger) cudaFreeHost(h->host_ledger);
+  h->pblock = h->gblock = h->snap = h->staging = nullptr;
+  h->dptr_table = nullptr;
+  h->ledger_partials = nullptr;
+  h->host_ctrl = nullptr;
+  h->host_ledger = nullptr;
+  return MPM_OK;
+}
+
+// Carve the particle arrays of capacity cap out of one allocation (or measure it with base null).
+static size_t carve_particles(char* base, int64_t cap, mpm::Particles& p) {
+  Carver c{base};
+  p.qx = c.take<unsigned>(cap); p.qy = c.take<unsigned>(cap); p.qz = c.take<unsigned>(cap);
+  p.vx = c.take<float>(cap); p.vy = c.take<float>(cap); p.vz = c.take<float>(cap);
+  p.C = c.take<float>(cap * 9);
+  p.D = c.take<float>(cap * 9);
+  p.m = c.take<float>(cap); p.V = c.take<float>(cap);
+  p.ep = c.take<float>(cap); p.T = c.take<float>(cap);
+  p.mat = c.take<unsigned short>(cap);
+  p.pinned = c.take<unsigned char>(cap);
+  p.key = c.take<unsigned>(cap);
+  p.perm = c.take<unsigned>(cap);
+  p.cap = cap;
+  return align_up(c.off, 256);
+}
+
+static int alloc_grid(mpm_handle* h) {
+  if (h->gblock) {
+    cudaFree(h->gblock);
+    h->gblock = nullptr;
+  }
+  const SceneDev& s = h->scene;
+  const long long nodes = (long long)s.gdim[0] * s.gdim[1] * s.gdim[2];
+  const int tiles = s.tiles[0] * s.tiles[1] * s.tiles[2];
+  const int ntiles = s.ntiles[0] * s.ntiles[1] * s.ntiles[2];
+  const int scan_blocks = (tiles + 1 + 4095) / 4096;
+  auto lay = [&](char* base, Ctx& c, void** tmaps, SceneDev** scenes, MaterialDev** mats) {
+    Carver cv{base};
+    for (int k = 0; k < 2; ++k) {
+      c.g.acc0[k] = cv.take<float4>(nodes);
+      c.g.acc1[k] = cv.take<float4>(nodes);
+    }
+    c.g.vel = cv.take<float4>(nodes);
+    c.g.tile_flag = cv.take<unsigned>(ntiles);
+    c.g.active[0] = cv.take<unsigned>(ntiles);
+    c.g.active[1] = cv.take<unsigned>(ntiles);
+    c.s.count = cv.take<unsigned>(tiles + 1);
+    c.s.start = cv.take<unsigned>(tiles + 1);
+    c.s.block_off = cv.take<unsigned>(scan_blocks + 1);
+    c.s.work[0] = cv.take<uint4>(tiles);
+    c.s.work[1] = cv.take<uint4>(tiles);
+    c.ctrl = cv.take<mpm::Ctrl>(1);
+    c.dt_scene = cv.take<float>(1);
+    c.wave_max = cv.take<unsigned>(1);
+    c.grad_max = cv.take<unsigned>(1);
+    *scenes = cv.take<SceneDev>(1);
+    *mats = cv.take<MaterialDev>(kMaxMats);
+    *tmaps = cv.take<char>(128);
+    return align_up(cv.off, 256);
+  };
+  Ctx probe{};
+  void* t;
+  SceneDev* sp;
+  MaterialDev* mp;
+  const size_t bytes = lay(nullptr, probe, &t, &sp, &mp);
+  MPM_CUDA(h, cudaMalloc(&h->gblock, bytes));
+  h->gblock_bytes = bytes;
+  MPM_CUDA(h, cudaMemsetAsync(h->gblock, 0, bytes, h->stream));
+  Ctx& c = h->ctx;
+  void* tm;
+  SceneDev* scenes;
+  MaterialDev* mats;
+  lay(static_cast<char*>(h->gblock), c, &tm, &scenes, &mats);
+  c.scenes = scenes;
+  c.mats = mats;
+  c.nscenes = 1;
+  c.total_tiles = tiles;
+  c.total_node_tiles = ntiles;
+  MPM_CUDA(h, cudaMemcpyAsync(scenes, &h->scene, sizeof(SceneDev), cudaMemcpyHostToDevice, h->stream));
+  MPM_CUDA(h, cudaMemcpyAsync(mats, h->mats_dev.data(), sizeof(MaterialDev) * kMaxMats, cudaMemcpyHostToDevice,
+                              h->stream));
+  // TMA descriptor of the velocity grid: 4D {channel 4, x, y, z}, box {4, 6, 6, 6}, fp32
+  c.tmaps = nullptr;
+  c.use_tma = 0;
+  auto encode = tensor_map_encoder();
+  if (encode && h->use_tma) {
+    CUtensorMap map;
+    std::memset(&map, 0, sizeof map);
+    cuuint64_t gdims[4] = {4, (cuuint64_t)s.gdim[0], (cuuint64_t)s.gdim[1], (cuuint64_t)s.gdim[2]};
+    cuuint64_t gstrides[3] = {16, 16ull * s.gdim[0], 16ull * s.gdim[0] * s.gdim[1]};
+    cuuint32_t box[4] = {4, mpm::kWinG, mpm::kWinG, mpm::kWinG};
+    cuuint32_t estr[4] = {1, 1, 1, 1};
+    CUresult r = encode(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, c.g.vel, gdims, gstrides, box, estr,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r == CUDA_SUCCESS) {
+      MPM_CUDA(h, cudaMemcpyAsync(tm, &map, sizeof map, cudaMemcpyHostToDevice, h->stream));
+      c.tmaps = tm;
+      c.use_tma = 1;
+    }
+  }
+  h->grid_valid = false;
+  h->pending_grid = false;
+  return MPM_OK;
+}
+
+static void refresh_flags(mpm_handle* h) {
+  bool plastic = false, thermal = false;
+  for (size_t i = 0; i < h->mats_host.size(); ++i) {
+    if (!h->mat_set[i]) continue;
+    const int m = h->mats_host[i].model;
+    if (m >= 4) plastic = true;
+    if (m == 10) thermal = true;
+  }
+  h->ctx.has_plastic = plastic ? 1 : 0;
+  h->ctx.has_thermal = thermal || h->ctx.has_thermal ? 1 : 0;
+}
+
+static int check_status(mpm_handle* h) {
+  MPM_CUDA(h, cudaMemcpyAsync(h->host_ctrl, h->ctx.ctrl, sizeof(mpm::Ctrl), cudaMemcpyDeviceToHost, h->stream));
+  MPM_CUDA(h, cudaStreamSynchronize(h->stream));
+  const unsigned st = h->host_ctrl->status;
+  if (st & MPM_STATUS_TIMEOUT) return fail(h, MPM_ERR_TIMEOUT, "a bounded device wait gave up (TMA copy did not complete)");
+  if (st & MPM_STATUS_NONFINITE) return fail(h, MPM_ERR_NONFINITE, "non-finite particle state");
+  if (st & MPM_STATUS_INVALID_J) return fail(h, MPM_ERR_INVALID_J, "det F <= 0 in a particle");
+  if (st & MPM_STATUS_OUT_OF_RANGE) return fail(h, MPM_ERR_OUT_OF_RANGE, "a particle left the grid");
+  if (st & MPM_STATUS_SORT_MISMATCH) return fail(h, MPM_ERR_STATE, "tile sort keys and counts disagreed");
+  return MPM_OK;
+}
+
+// Counting sort of the current state by tile and the dt-free P2G into acc[step_index & 1].
+static int prepare_grid(mpm_handle* h) {
+  Ctx& c = h->ctx;
+  c.n = h->n;
+  if (h->pending_grid) {
+    ProfScope ps(h, -1);
+    mpm::launch_grid_clear(c, h->stream, h->grid_blocks);
+    MPM_CUDA(h, cudaGetLastError());
+  }
+  { ProfScope ps(h, -1); mpm::launch_control_init(c, h->stream); }
+  MPM_CUDA(h, cudaMemsetAsync(c.s.count, 0, sizeof(unsigned) * (c.total_tiles + 1), h->stream));
+  { ProfScope ps(h, 6); mpm::launch_keys(c, h->stream); }
+  { ProfScope ps(h, 3); mpm::launch_scan(c, h->stream); }
+  { ProfScope ps(h, 4); mpm::launch_sort_scatter(c, h->stream, true); }
+  { ProfScope ps(h, 5); mpm::launch_p2g(c, h->stream, h->p2g_blocks); }
+  MPM_CUDA(h, cudaGetLastError());
+  h->grid_valid = true;
+  h->pending_grid = true;
+  return MPM_OK;
+}
+
+static void launch_substep(mpm_handle* h, bool scatter) {
+  Ctx& c = h->ctx;
+  { ProfScope ps(h, 0); mpm::launch_begin(c, h->stream); }
+  { ProfScope ps(h, 1); mpm::launch_grid_update(c, h->stream, h->grid_blocks); }
+  { ProfScope ps(h, 2); mpm::launch_g2p2g(c, h->stream, h->g2p2g_blocks, scatter); }
+  if (scatter) {
+    { ProfScope ps(h, 3); mpm::launch_scan(c, h->stream); }
+    { ProfScope ps(h, 4); mpm::launch_sort_scatter(c, h->stream, false); }
+  }
+}
+
+static MaterialDev to_device(const mpm_material& m) {
+  MaterialDev d{};
+  d.model = m.model;
+  d.mu = static_cast<float>(m.mu);
+  d.lam = static_cast<float>(m.lambda);
+  d.yield_stress = static_cast<float>(m.yield_stress);
+  d.hardening = static_cast<float>(m.hardening);
+  d.T_ref = static_cast<float>(m.T_ref);
+  d.inv_T_span = m.T_hot > m.T_ref ? static_cast<float>(1.0 / (m.T_hot - m.T_ref)) : 0.f;
+  d.hot_ratio = static_cast<float>(m.hot_ratio);
+  d.heat_per_work = m.specific_heat > 0 ? static_cast<float>(m.heat_fraction / m.specific_heat) : 0.f;
+  d.wave_modulus = static_cast<float>(m.lambda + 2 * m.mu);
+  return d;
+}
+
+static int validate_material(const mpm_material* m, std::string& why) {
+  if (!m) { why = "material is null"; return MPM_ERR_INVALID_ARG; }
+  if (m->model != 0 && m->model != 1 && m->model != 4 && m->model != 5 && m->model != 10) {
+    why = "material model not built (supported: 0, 1, 4, 5, 10)";
+    return MPM_ERR_UNSUPPORTED;
+  }
+  if (!(m->mu > 0) || !(3 * m->lambda + 2 * m->mu > 0) || !std::isfinite(m->mu) || !std::isfinite(m->lambda)) {
+    why = "moduli must satisfy mu > 0 and 3 lambda + 2 mu > 0";
+    return MPM_ERR_INVALID_ARG;
+  }
+  if (m->model >= 4 && (!(m->yield_stress >= 0) || !(m->hardening >= 0))) {
+    why = "yield stress and hardening must be non-negative";
+    return MPM_ERR_INVALID_ARG;
+  }
+  if (m->model == 10 && !(m->T_hot > m->T_ref)) {
+    why = "T_hot must exceed T_ref";
+    return MPM_ERR_INVALID_ARG;
+  }
+  if (m->heat_fraction < 0 || m->heat_fraction > 1) {
+    why = "heat_fraction must lie in [0, 1]";
+    return MPM_ERR_INVALID_ARG;
+  }
+  return MPM_OK;
+}
+
+extern "C" {
+
+int mpm_abi_version(void) { return MPM_ABI_VERSION; }
+
+const char* mpm_error_string(int status) {
+  switch (status) {
+    case MPM_OK: return "ok";
+    case MPM_ERR_INVALID_ARG: return "invalid argument";
+    case MPM_ERR_OUT_OF_MEMORY: return "out of device memory";
+    case MPM_ERR_CUDA: return "CUDA error";
+    case MPM_ERR_NONFINITE: return "non-finite particle state";
+    case MPM_ERR_INVALID_J: return "det F <= 0";
+    case MPM_ERR_OUT_OF_RANGE: return "particle outside the grid";
+    case MPM_ERR_TIMEOUT: return "bounded device wait timed out";
+    case MPM_ERR_STATE: return "call out of order";
+    case MPM_ERR_CAPACITY: return "capacity exceeded";
+    case MPM_ERR_UNSUPPORTED: return "unsupported material model";
+    default: return "unknown status";
+  }
+}
+
+int mpm_create(const mpm_domain* domain, int64_t capacity, mpm_handle** out) {
+  if (!out || !domain || capacity <= 0 || capacity > (int64_t)1 << 31) return MPM_ERR_INVALID_ARG;
+  *out = nullptr;
+  mpm_handle* h = new mpm_handle();
+  SceneDev s;
+  int rc = build_scene(h, *domain, s);
+  if (rc != MPM_OK) {
+    delete h;
+    return rc;
+  }
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) {
+    delete h;
+    return MPM_ERR_CUDA;
+  }
+  cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, dev);
+  if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    delete h;
+    return MPM_ERR_CUDA;
+  }
+  h->dom = *domain;
+  h->scene = s;
+  h->cap = capacity;
+  h->use_tma = std::getenv("MPM_B200_NO_TMA") ? 0 : 1;  // plain-load gather window when set
+  h->mats_host.assign(kMaxMats, mpm_material{});
+  h->mats_dev.assign(kMaxMats, MaterialDev{});
+  h->mat_set.assign(kMaxMats, 0);
+  mpm::Particles p{};
+  const size_t pbytes = carve_particles(nullptr, capacity, p);
+  auto bail = [&](int code) {
+    free_device(h);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+    return code;
+  };
+  if (cudaMalloc(&h->pblock, pbytes) != cudaSuccess) return bail(MPM_ERR_OUT_OF_MEMORY);
+  h->pblock_bytes = pbytes;
+  carve_particles(static_cast<char*>(h->pblock), capacity, h->ctx.p);
+  if (cudaMemsetAsync(h->pblock, 0, pbytes, h->stream) != cudaSuccess) return bail(MPM_ERR_CUDA);
+  if (cudaMalloc(reinterpret_cast<void**>(&h->dptr_table), 16 * sizeof(void*)) != cudaSuccess) return bail(MPM_ERR_OUT_OF_MEMORY);
+  if (cudaMallocHost(reinterpret_cast<void**>(&h->host_ctrl), sizeof(mpm::Ctrl)) != cudaSuccess) return bail(MPM_ERR_OUT_OF_MEMORY);
+  if (cudaMallocHost(reinterpret_cast<void**>(&h->host_ledger), 32 * sizeof(double)) != cudaSuccess) return bail(MPM_ERR_OUT_OF_MEMORY);
+  const int ledger_blocks = h->num_sms * 4;
+  if (cudaMalloc(reinterpret_cast<void**>(&h->ledger_partials), (ledger_blocks * 19 + 32) * sizeof(double)) != cudaSuccess)
+    return bail(MPM_ERR_OUT_OF_MEMORY);
+  h->ledger_out = h->ledger_partials + ledger_blocks * 19;
+  // default material 0: fixed-corotated, unit moduli (the caller sets real materials)
+  mpm_material def{};
+  def.model = 0;
+  def.mu = 1;
+  def.lambda = 1;
+  h->mats_host[0] = def;
+  h->mats_dev[0] = to_device(def);
+  if (alloc_grid(h) != MPM_OK) return bail(MPM_ERR_OUT_OF_MEMORY);
+  h->g2p2g_blocks = h->num_sms * mpm::g2p2g_blocks_per_sm(true);
+  h->p2g_blocks = h->num_sms * mpm::p2g_blocks_per_sm();
+  h->grid_blocks = h->num_sms * 8;
+  if (cudaStreamSynchronize(h->stream) != cudaSuccess) return bail(MPM_ERR_CUDA);
+  *out = h;
+  return MPM_OK;
+}
+
+int mpm_destroy(mpm_handle* h) {
+  if (!h) return MPM_ERR_INVALID_ARG;
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  for (cudaEvent_t e : h->ev_pool) cudaEventDestroy(e);
+  free_device(h);
+  if (h->stream) cudaStreamDestroy(h->stream);
+  delete h;
+  return MPM_OK;
+}
+
+const char* mpm_last_error(const mpm_handle* h) { return h ? h->err.c_str() : "null handle"; }
+
+int mpm_configure_domain(mpm_handle* h, const mpm_domain* domain) {
+  if (!h || !domain) return MPM_ERR_INVALID_ARG;
+  SceneDev s;
+  int rc = build_scene(h, *domain, s);
+  if (rc != MPM_OK) return rc;
+  MPM_CUDA(h, cudaStreamSynchronize(h->stream));
+  h->dom = *domain;
+  h->scene = s;
+  rc = alloc_grid(h);
+  if (rc != MPM_OK) return rc;
+  h->uploaded = false;  // positions are relative to the grid origin: upload again
+  h->n = 0;
+  return MPM_OK;
+}
+
+int mpm_grid_dims(const mpm_handle* h, int32_t dims[3], double origin[3]) {
+  if (!h) return MPM_ERR_INVALID_ARG;
+  for (int a = 0; a < 3; ++a) {
+    if (dims) dims[a] = h->scene.dims[a];
+    if (origin) origin[a] = h->scene.origin[a];
+  }
+  return MPM_OK;
+}
+
+int mpm_set_material(mpm_handle* h, int32_t index, const mpm_material* material) {
+  if (!h) return MPM_ERR_INVALID_ARG;
+  if (index < 0 || index >= kMaxMats) return fail(h, MPM_ERR_INVALID_ARG, "material index out of range [0, 256)");
+  std::string why;
+  const int rc = validate_material(material, why);
+  if (rc != MPM_OK) return fail(h, rc, why);
+  h->mats_host[index] = *material;
+  h->mats_dev[index] = to_device(*material);
+  h->mat_set[index] = 1;
+  MPM_CUDA(h, cudaMemcpyAsync(const_cast<MaterialDev*>(h->ctx.mats) + index, &h->mats_dev[index], sizeof(MaterialDev),
+                              cudaMemcpyHostToDevice, h->stream));
+  refresh_flags(h);
+  h->grid_valid = false;  // stresses change
+  return MPM_OK;
+}
+
+int mpm_get_stream(mpm_handle* h, void** cuda_stream) {
+  if (!h || !cuda_stream) return MPM_ERR_INVALID_ARG;
+  *cuda_stream = h->stream;
+  return MPM_OK;
+}
+
+static int ensure_staging(mpm_handle* h, size_t bytes) {
+  if (h->staging_bytes >= bytes) return MPM_OK;
+  if (h->staging) cudaFree(h->staging);
+  h->staging = nullptr;
+  h->staging_bytes = 0;
+  MPM_CUDA(h, cudaMalloc(&h->staging, bytes));
+  h->staging_bytes = bytes;
+  return MPM_OK;
+}
+
+// Copies the caller's host arrays into device staging; fills ptrs with device addresses (or null).
+static int stage_in(mpm_handle* h, int64_t n, const mpm_particles* p, void* ptrs[12], const int** mat_dev,
+                    const unsigned char** pin_dev, unsigned fields) {
+  const size_t es = p->dtype == MPM_F32 ? 4 : 8;
+  const void* src[12] = {p->x, p->y, p->z, p->vx, p->vy, p->vz, p->mass, p->volume, p->temperature, p->plastic, p->F, p->C};
+  const unsigned need[12] = {mpm::kFieldPos, mpm::kFieldPos, mpm::kFieldPos, mpm::kFieldVel, mpm::kFieldVel,
+                             mpm::kFieldVel, mpm::kFieldMass, mpm::kFieldVolume, mpm::kFieldTemp, mpm::kFieldPlastic,
+                             mpm::kFieldF, mpm::kFieldC};
+  size_t total = 0;
+  for (int k = 0; k < 12; ++k)
+    if (src[k] && (fields & need[k])) total += align_up((k >= 10 ? 9 : 1) * n * es, 256);
+  if ((fields & mpm::kFieldMass) && p->material) total += align_up(n * 4, 256);
+  if ((fields & mpm::kFieldMass) && p->pinned) total += align_up(n, 256);
+  int rc = ensure_staging(h, std::max<size_t>(total, 256));
+  if (rc != MPM_OK) return rc;
+  char* base = static_cast<char*>(h->staging);
+  size_t off = 0;
+  for (int k = 0; k < 12; ++k) {
+    ptrs[k] = nullptr;
+    if (!src[k] || !(fields & need[k])) continue;
+    const size_t bytes = (k >= 10 ? 9 : 1) * n * es;
+    ptrs[k] = base + off;
+    MPM_CUDA(h, cudaMemcpyAsync(ptrs[k], src[k], bytes, cudaMemcpyHostToDevice, h->stream));
+    off += align_up(bytes, 256);
+  }
+  *mat_dev = nullptr;
+  *pin_dev = nullptr;
+  if ((fields & mpm::kFieldMass) && p->material) {
+    *mat_dev = reinterpret_cast<const int*>(base + off);
+    MPM_CUDA(h, cudaMemcpyAsync(base + off, p->material, n * 4, cudaMemcpyHostToDevice, h->stream));
+    off += align_up(n * 4, 256);
+  }
+  if ((fields & mpm::kFieldMass) && p->pinned) {
+    *pin_dev = reinterpret_cast<const unsigned char*>(base + off);
+    MPM_CUDA(h, cudaMemcpyAsync(base + off, p->pinned, n, cudaMemcpyHostToDevice, h->stream));
+    off += align_up(n, 256);
+  }
+  MPM_CUDA(h, cudaMemcpyAsync(h->dptr_table, ptrs, 12 * sizeof(void*), cudaMemcpyHostToDevice, h->stream));
+  return MPM_OK;
+}
+
+int mpm_upload_particles(mpm_handle* h, int64_t n, const mpm_particles* p) {
+  if (!h || !p || n < 0) return MPM_ERR_INVALID_ARG;
+  if (n > h->cap) return fail(h, MPM_ERR_CAPACITY, "particle count exceeds the handle's capacity");
+  if (p->dtype != MPM_F64 && p->dtype != MPM_F32) return fail(h, MPM_ERR_INVALID_ARG, "dtype must be MPM_F64 or MPM_F32");
+  if (n > 0 && (!p->x || !p->y || !p->z || !p->mass || !p->volume))
+    return fail(h, MPM_ERR_INVALID_ARG, "positions, mass and volume are required");
+  bool single = true, pinned_any = false;
+  if (p->material) {
+    for (int64_t i = 0; i < n; ++i) {
+      const int m = p->material[i];
+      if (m < 0 || m >= kMaxMats || !h->mat_set[m]) return fail(h, MPM_ERR_INVALID_ARG, "particle material not set");
+      if (m != p->material[0]) single = false;
+    }
+  } else if (!h->mat_set[0] && n > 0) {
+    return fail(h, MPM_ERR_INVALID_ARG, "material 0 is not set");
+  }
+  if (p->pinned)
+    for (int64_t i = 0; i < n && !pinned_any; ++i) pinned_any = p->pinned[i] != 0;
+  const size_t es = p->dtype == MPM_F32 ? 4 : 8;
+  if (n > 0 && p->dtype == MPM_F64) {
+    const double* m = static_cast<const double*>(p->mass);
+    const double* v = static_cast<const double*>(p->volume);
+    for (int64_t i = 0; i < n; ++i)
+      if (!(m[i] > 0) || !(v[i] > 0)) return fail(h, MPM_ERR_INVALID_ARG, "mass and volume must be positive");
+  } else if (n > 0) {
+    const float* m = static_cast<const float*>(p->mass);
+    const float* v = static_cast<const float*>(p->volume);
+    for (int64_t i = 0; i < n; ++i)
+      if (!(m[i] > 0) || !(v[i] > 0)) return fail(h, MPM_ERR_INVALID_ARG, "mass and volume must be positive");
+  }
+  (void)es;
+  MPM_CUDA(h, cudaStreamSynchronize(h->stream));
+  void* ptrs[12];
+  const int* mat_dev;
+  const unsigned char* pin_dev;
+  const unsigned all = 0xffu;
+  int rc = stage_in(h, n, p, ptrs, &mat_dev, &pin_dev, all);
+  if (rc != MPM_OK) return rc;
+  h->ctx.n = n;
+  h->ctx.has_pinned = pinned_any ? 1 : 0;
+  h->ctx.single_material = single ? 1 : 0;
+  h->scene.mat_base = (single && p->material && n > 0) ? p->material[0] : 0;
+  h->scene.p_begin = 0;
+  h->scene.p_end = n;
+  if (p->temperature) h->ctx.has_thermal = 1;
+  refresh_flags(h);
+  MPM_CUDA(h, cudaMemcpyAsync(const_cast<SceneDev*>(h->ctx.scenes), &h->scene, sizeof(SceneDev), cudaMemcpyHostToDevice,
+                              h->stream));
+  // the conversion kernel writes the material index relative to mat_base = 0
+  SceneDev tmp = h->scene;
+  tmp.mat_base = 0;
+  MPM_CUDA(h, cudaMemcpyAsync(const_cast<SceneDev*>(h->ctx.scenes), &tmp, sizeof(SceneDev), cudaMemcpyHostToDevice, h->stream));
+  { ProfScope ps(h, -1);
+    mpm::launch_upload_convert(h->ctx, h->stream, n, p->dtype, reinterpret_cast<const void* const*>(h->dptr_table), mat_dev,
+                               pin_dev, all); }
+  MPM_CUDA(h, cudaGetLastError());
+  MPM_CUDA(h, cudaMemcpyAsync(const_cast<SceneDev*>(h->ctx.scenes), &h->scene, sizeof(SceneDev), cudaMemcpyHostToDevice,
+                              h->stream));
+  h->n = n;
+  h->uploaded = true;
+  h->grid_valid = false;
+  MPM_CUDA(h, cudaStreamSynchronize(h->stream));
+  return MPM_OK;
+}
+
+static unsigned download_fields(const mpm_particles* p) {
+  unsigned f = 0;
+  if (p->x && p->y && p->z) f |= mpm::kFieldPos;
+  if (p->vx && p->vy && p->vz) f |= mpm::kFieldVel;
+  if (p->mass) f |= mpm::kFieldMass;
+  if (p->volume) f |= mpm::kFieldVolume;
+  if (p->temperature) f |= mpm::kFieldTemp;
+  if (p->plastic) f |= mpm::kFieldPlastic;
+  if (p->F) f |= mpm::kFieldF;
+  if (p->C) f |= mpm::kFieldC;
+  return f;
+}
+
+int mpm_download_particles(mpm_handle* h, const mpm_particles* p) {
+  if (!h || !p) return MPM_ERR_INVALID_ARG;
+  if (!h->uploaded) return fail(h, MPM_ERR_STATE, "no particles uploaded");
+  const int64_t n = h->n;
+  if (n == 0) return MPM_OK;
+  const size_t es = p->dtype == MPM_F32 ? 4 : 8;
+  const unsigned fields = download_fields(p);
+  void* dst[12] = {p->x, p->y, p->z, p->vx, p->vy, p->vz, p->mass, p->volume, p->temperature, p->plastic, p->F, p->C};
+  size_t total = 0;
+  for (int k = 0; k < 12; ++k)
+    if (dst[k]) total += align_up((k >= 10 ? 9 : 1) * n * es, 256);
+  int rc = ensure_staging(h, std::max<size_t>(total, 256));
+  if (rc != MPM_OK) return rc;
+  void* dev[12];
+  char* base = static_cast<char*>(h->staging);
+  size_t off = 0;
+  for (int k = 0; k < 12; ++k) {
+    dev[k] = nullptr;
+    if (!dst[k]) continue;
+    dev[k] = base + off;
+    off += align_up((k >= 10 ? 9 : 1) * n * es, 256);
+  }
+  MPM_CUDA(h, cudaMemcpyAsync(h->dptr_table, dev, 12 * sizeof(void*), cudaMemcpyHostToDevice, h->stream));
+  { ProfScope ps(h, -1); mpm::launch_download_convert(h->ctx, h->stream, n, p->dtype, reinterpret_cast<void* const*>(h->dptr_table), fields); }
+  MPM_CUDA(h, cudaGetLastError());
+  for (int k = 0; k < 12; ++k)
+    if (dst[k]) MPM_CUDA(h, cudaMemcpyAsync(dst[k], dev[k], (k >= 10 ? 9 : 1) * n * es, cudaMemcpyDeviceToHost, h->stream));
+  MPM_CUDA(h, cudaStreamSynchronize(h->stream));
+  return MPM_OK;
+}
+
+int mpm_count(const mpm_handle* h, int64_t* n) {
+  if (!h || !n) return MPM_ERR_INVALID_ARG;
+  *n = h->n;
+  return MPM_OK;
+}
+
+int mpm_reset_deformation(mpm_handle* h) {
+  if (!h) return MPM_ERR_INVALID_ARG;
+  const mpm::Particles& p = h->ctx.p;
+  MPM_CUDA(h, cudaMemsetAsync(p.C, 0, sizeof(float) * 9 * p.cap, h->stream));
+  MPM_CUDA(h, cudaMemsetAsync(p.D, 0, sizeof(float) * 9 * p.cap, h->stream));
+  MPM_CUDA(h, cudaMemsetAsync(p.ep, 0, sizeof(float) * p.cap, h->stream));
+  h->grid_valid = false;
+  MPM_CUDA(h, cudaStreamSynchronize(h->stream));
+  return MPM_OK;
+}
+
+int mpm_stable_dt(mpm_handle* h, double* dt) {
+  if (!h || !dt) return MPM_ERR_INVALID_ARG;
+  if (!h->uploaded) return fail(h, MPM_ERR_STATE, "no particles uploaded");
+  if (h->n == 0) {
+    *dt = h->scene.dt_max;
+    return MPM_OK;
+  }
+  if (!h->grid_valid) {
+    int rc = prepare_grid(h);
+    if (rc != MPM_OK) return rc;
+  }
+  unsigned wg[2];
+  MPM_CUDA(h, cudaMemcpyAsync(&wg[0], h->ctx.wave_max, 4, cudaMemcpyDeviceToHost, h->stream));
+  MPM_CUDA(h, cudaMemcpyAsync(&wg[1], h->ctx.grad_max, 4, cudaMemcpyDeviceToHost, h->stream));
+  MPM_CUDA(h, cudaStreamSynchronize(h->stream));
+  float wave, grad;
+  std::memcpy(&wave, &wg[0], 4);
+  std::memcpy(&grad, &wg[1], 4);
+  const SceneDev& s = h->scene;
+  *dt = std::min<double>(s.dt_max, std::min<double>(s.cfl * s.H / std::max(1.f, wave), s.grad_limit / std::max(1.f, grad)));
+  return MPM_OK;
+}
+
+static int run_substeps(mpm_handle* h, int mode, double dt_req, int max_substeps, float dt_fixed, int* substeps,
+                        double* advanced) {
+  if (!h->uploaded) return fail(h, MPM_ERR_STATE, "no particles uploaded");
+  if (h->n == 0) {
+    if (substeps) *substeps = 0;
+    if (advanced) *advanced = 0;
+    return MPM_OK;
+  }
+  if (!h->grid_valid) {
+    int rc = prepare_grid(h);
+    if (rc != MPM_OK) return rc;
+  }
+  h->ctx.n = h->n;
+  { ProfScope ps(h, -1); mpm::launch_control_step(h->ctx, h->stream, mode, dt_req, max_substeps, dt_fixed); }
+  int launched = 0;
+  int est;
+  if (mode == mpm::kModeRequested) {
+    double dt = 0;
+    int rc = mpm_stable_dt(h, &dt);
+    if (rc != MPM_OK) return rc;
+    est = static_cast<int>(std::ceil(dt_req / std::max(dt, 1e-30) - 1e-9));
+    est = std::max(1, std::min(est, max_substeps));
+  } else {
+    est = max_substeps;
+  }
+  while (true) {
+    for (int i = 0; i < est; ++i) launch_substep(h, true);
+    launched += est;
+    MPM_CUDA(h, cudaGetLastError());
+    MPM_CUDA(h, cudaMemcpyAsync(h->host_ctrl, h->ctx.ctrl, sizeof(mpm::Ctrl), cudaMemcpyDeviceToHost, h->stream));
+    MPM_CUDA(h, cudaStreamSynchronize(h->stream));
+    const mpm::Ctrl& ct = *h->host_ctrl;
+    const bool finished = ct.done || ct.substeps >= max_substeps ||
+                          (mode == mpm::kModeRequested && !(ct.remaining > 1e-6 * dt_req)) || launched >= max_substeps;
+    if (finished || (ct.status & (MPM_STATUS_NONFINITE | MPM_STATUS_TIMEOUT))) break;
+    est = 1;
+  }
+  h->pending_grid = true;
+  const mpm::Ctrl& ct = *h->host_ctrl;
+  if (substeps) *substeps = ct.substeps;
+  if (advanced) *advanced = ct.advanced;
+  h->last_estimate = ct.substeps;
+  return check_status(h);
+}
+
+int mpm_step(mpm_handle* h, double dt_requested, int32_t max_substeps, int32_t* substeps, double* advanced) {
+  if (!h) return MPM_ERR_INVALID_ARG;
+  if (!(dt_requested > 0) || !std::isfinite(dt_requested)) return fail(h, MPM_ERR_INVALID_ARG, "dt must be positive");
+  if (max_substeps <= 0) max_substeps = 48;  // the reference's cap (src/three/simulation.js:308)
+  int sub = 0;
+  const int rc = run_substeps(h, mpm::kModeRequested, dt_requested, max_substeps, 0.f, &sub, advanced);
+  if (substeps) *substeps = sub;
+  return rc;
+}
+
+int mpm_step_fixed(mpm_handle* h, double dt, int32_t nsteps) {
+  if (!h) return MPM_ERR_INVALID_ARG;
+  if (!(dt > 0) || nsteps <= 0) return fail(h, MPM_ERR_INVALID_ARG, "dt and nsteps must be positive");
+  return run_substeps(h, mpm::kModeFixed, 0.0, nsteps, static_cast<float>(dt), nullptr, nullptr);
+}
+
+int mpm_step_cfl(mpm_handle* h, int32_t nsteps, double* time_advanced) {
+  if (!h) return MPM_ERR_INVALID_ARG;
+  if (nsteps <= 0) return fail(h, MPM_ERR_INVALID_ARG, "nsteps must be positive");
+  return run_substeps(h, mpm::kModeCfl, 0.0, nsteps, 0.f, nullptr, time_advanced);
+}
+
+int mpm_step_host(mpm_handle* h, const mpm_particles* io, double dt) {
+  if (!h || !io) return MPM_ERR_INVALID_ARG;
+  if (!h->uploaded) return fail(h, MPM_ERR_STATE, "no particles uploaded");
+  if (!(dt > 0)) return fail(h, MPM_ERR_INVALID_ARG, "dt must be positive");
+  if (!io->x || !io->y || !io->z || !io->vx || !io->vy || !io->vz)
+    return fail(h, MPM_ERR_INVALID_ARG, "positions and velocities are required");
+  const int64_t n = h->n;
+  if (n == 0) return MPM_OK;
+  void* ptrs[12];
+  const int* mat_dev;
+  const unsigned char* pin_dev;
+  const unsigned fields = mpm::kFieldPos | mpm::kFieldVel;
+  int rc = stage_in(h, n, io, ptrs, &mat_dev, &pin_dev, fields);
+  if (rc != MPM_OK) return rc;
+  { ProfScope ps(h, -1);
+    mpm::launch_upload_convert(h->ctx, h->stream, n, io->dtype, reinterpret_cast<const void* const*>(h->dptr_table), nullptr,
+                               nullptr, fields); }
+  MPM_CUDA(h, cudaGetLastError());
+  rc = prepare_grid(h);
+  if (rc != MPM_OK) return rc;
+  { ProfScope ps(h, -1); mpm::launch_control_step(h->ctx, h->stream, mpm::kModeFixed, 0.0, 1, static_cast<float>(dt)); }
+  launch_substep(h, false);
+  MPM_CUDA(h, cudaGetLastError());
+  h->grid_valid = false;
+  h->pending_grid = false;
+  // positions and velocities back to the caller's arrays
+  mpm_particles out{};
+  out.dtype = io->dtype;
+  out.x = io->x; out.y = io->y; out.z = io->z;
+  out.vx = io->vx; out.vy = io->vy; out.vz = io->vz;
+  rc = mpm_download_particles(h, &out);
+  if (rc != MPM_OK) return rc;
+  return check_status(h);
+}
+
+int mpm_frame_host(mpm_handle* h, const mpm_particles* io, double dt_requested, int32_t max_substeps,
+                   int32_t* substeps) {
+  if (!h || !io) return MPM_ERR_INVALID_ARG;
+  if (!h->uploaded) return fail(h, MPM_ERR_STATE, "no particles uploaded");
+  if (!io->x || !io->y || !io->z || !io->vx || !io->vy || !io->vz)
+    return fail(h, MPM_ERR_INVALID_ARG, "positions and velocities are required");
+  const int64_t n = h->n;
+  if (n == 0) return MPM_OK;
+  void* ptrs[12];
+  const int* mat_dev;
+  const unsigned char* pin_dev;
+  const unsigned fields = mpm::kFieldPos | mpm::kFieldVel;
+  int rc = stage_in(h, n, io, ptrs, &mat_dev, &pin_dev, fields);
+  if (rc != MPM_OK) return rc;
+  { ProfScope ps(h, -1);
+    mpm::launch_upload_convert(h->ctx, h->stream, n, io->dtype, reinterpret_cast<const void* const*>(h->dptr_table), nullptr,
+                               nullptr, fields); }
+  MPM_CUDA(h, cudaGetLastError());
+  h->grid_valid = false;
+  rc = mpm_step(h, dt_requested, max_substeps, substeps, nullptr);
+  if (rc != MPM_OK) return rc;
+  mpm_particles out{};
+  out.dtype = io->dtype;
+  out.x = io->x; out.y = io->y; out.z = io->z;
+  out.vx = io->vx; out.vy = io->vy; out.vz = io->vz;
+  return mpm_download_particles(h, &out);
+}
+
+int mpm_profile_enable(mpm_handle* h, int32_t on) {
+  if (!h) return MPM_ERR_INVALID_ARG;
+  MPM_CUDA(h, cudaStreamSynchronize(h->stream));
+  h->profiling = on != 0;
+  h->ev_used.clear();
+  h->ev_next = 0;
+  return MPM_OK;
+}
+
+int mpm_profile_read(mpm_handle* h, double ms[MPM_PROFILE_KERNELS], int64_t launches[MPM_PROFILE_KERNELS]) {
+  if (!h || !ms || !launches) return MPM_ERR_INVALID_ARG;
+  MPM_CUDA(h, cudaStreamSynchronize(h->stream));
+  for (int k = 0; k < MPM_PROFILE_KERNELS; ++k) {
+    ms[k] = 0;
+    launches[k] = 0;
+  }
+  for (const auto& u : h->ev_used) {
+    if (u.first < 0 || u.first >= MPM_PROFILE_KERNELS) continue;
+    float t = 0;
+    MPM_CUDA(h, cudaEventElapsedTime(&t, h->ev_pool[u.second], h->ev_pool[u.second + 1]));
+    ms[u.first] += t;
+    launches[u.first] += 1;
+  }
+  return MPM_OK;
+}
+
+int mpm_launch_count(mpm_handle* h, int64_t* count) {
+  if (!h || !count) return MPM_ERR_INVALID_ARG;
+  *count = h->launches;
+  return MPM_OK;
+}
+
+int mpm_ledger_compute(mpm_handle* h, mpm_ledger* out) {
+  if (!h || !out) return MPM_ERR_INVALID_ARG;
+  if (!h->uploaded) return fail(h, MPM_ERR_STATE, "no particles uploaded");
+  std::memset(out, 0, sizeof *out);
+  h->ctx.n = h->n;
+  const int blocks = h->num_sms * 4;
+  { ProfScope ps(h, -1); ProfScope ps2(h, -1); mpm::launch_ledger(h->ctx, h->stream, h->ledger_partials, blocks, h->ledger_out); }
+  MPM_CUDA(h, cudaGetLastError());
+  MPM_CUDA(h, cudaMemcpyAsync(h->host_ledger, h->ledger_out, 19 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  MPM_CUDA(h, cudaMemcpyAsync(h->host_ctrl, h->ctx.ctrl, sizeof(mpm::Ctrl), cudaMemcpyDeviceToHost, h->stream));
+  MPM_CUDA(h, cudaStreamSynchronize(h->stream));
+  const double* r = h->host_ledger;
+  out->mass = r[0];
+  out->kinetic = r[1];
+  out->affine = r[2];
+  out->potential = r[3];
+  out->elastic = r[4];
+  for (int a = 0; a < 3; ++a) {
+    out->momentum[a] = r[5 + a];
+    out->angular[a] = r[8 + a];
+  }
+  out->min_j = h->n ? r[13] : 1.0;
+  out->max_j = h->n ? r[14] : 1.0;
+  out->max_plastic = r[15];
+  out->max_von_mises = r[16];
+  out->nonfinite = static_cast<int64_t>(r[17]);
+  out->invalid_j = static_cast<int64_t>(r[18]);
+  out->count = h->n;
+  out->plastic_work = h->host_ctrl->plastic_work;
+  return MPM_OK;
+}
+
+int mpm_min_j(mpm_handle* h, double* out) {
+  if (!out) return MPM_ERR_INVALID_ARG;
+  mpm_ledger L;
+  const int rc = mpm_ledger_compute(h, &L);
+  if (rc == MPM_OK) *out = L.min_j;
+  return rc;
+}
+
+int mpm_status(mpm_handle* h, uint32_t* flags) {
+  if (!h || !flags) return MPM_ERR_INVALID_ARG;
+  MPM_CUDA(h, cudaMemcpyAsync(h->host_ctrl, h->ctx.ctrl, sizeof(mpm::Ctrl), cudaMemcpyDeviceToHost, h->stream));
+  MPM_CUDA(h, cudaStreamSynchronize(h->stream));
+  *flags = h->host_ctrl->status;
+  return MPM_OK;
+}
+
+int mpm_clear_status(mpm_handle* h) {
+  if (!h) return MPM_ERR_INVALID_ARG;
+  MPM_CUDA(h, cudaMemsetAsync(&h->ctx.ctrl->status, 0, sizeof(unsigned), h->stream));
+  MPM_CUDA(h, cudaStreamSynchronize(h->stream));
+  return MPM_OK;
+}
+
+int mpm_grid_debug(mpm_handle* h, double dt, double* mass, double* momentum) {
+  if (!h || !mass || !momentum) return MPM_ERR_INVALID_ARG;
+  if (!h->uploaded) return fail(h, MPM_ERR_STATE, "no particles uploaded");
+  if (!h->grid_valid) {
+    const int rc = prepare_grid(h);
+    if (rc != MPM_OK) return rc;
+  }
+  const SceneDev& s = h->scene;
+  const size_t nodes = (size_t)s.dims[0] * s.dims[1] * s.dims[2];
+  double* dev = nullptr;
+  MPM_CUDA(h, cudaMalloc(&dev, nodes * 4 * sizeof(double)));
+  mpm::launch_grid_debug(h->ctx, h->stream, 0, static_cast<float>(dt), dev, dev + nodes);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpyAsync(mass, dev, nodes * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(momentum, dev + nodes, nodes * 3 * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  cudaFree(dev);
+  if (e != cudaSuccess) return fail(h, MPM_ERR_CUDA, cudaGetErrorString(e));
+  return MPM_OK;
+}
+
+int mpm_snapshot(mpm_handle* h) {
+  if (!h) return MPM_ERR_INVALID_ARG;
+  if (!h->snap) MPM_CUDA(h, cudaMalloc(&h->snap, h->pblock_bytes));
+  MPM_CUDA(h, cudaMemcpyAsync(h->snap, h->pblock, h->pblock_bytes, cudaMemcpyDeviceToDevice, h->stream));
+  MPM_CUDA(h, cudaStreamSynchronize(h->stream));
+  h->snap_valid = true;
+  h->snap_n = h->n;
+  return MPM_OK;
+}
+
+int mpm_rollback(mpm_handle* h) {
+  if (!h) return MPM_ERR_INVALID_ARG;
+  if (!h->snap_valid) return fail(h, MPM_ERR_STATE, "no snapshot taken");
+  MPM_CUDA(h, cudaMemcpyAsync(h->pblock, h->snap, h->pblock_bytes, cudaMemcpyDeviceToDevice, h->stream));
+  MPM_CUDA(h, cudaMemsetAsync(&h->ctx.ctrl->status, 0, sizeof(unsigned), h->stream));
+  MPM_CUDA(h, cudaStreamSynchronize(h->stream));
+  h->n = h->snap_n;
+  h->grid_valid = false;
+  return MPM_OK;
+}
+
+struct CheckpointHeader {
+  uint32_t magic, version;
+  int64_t n;
+  mpm_domain dom;
+  int32_t has_pinned, single_material, has_thermal, has_plastic, mat_base, reserved;
+};
+
+// Raw device state of the n live particles, array by array, after a header with the domain and
+// the materials (so a load reproduces the state bit for bit).
+int mpm_checkpoint_save(mpm_handle* h, const char* path) {
+  if (!h || !path) return MPM_ERR_INVALID_ARG;
+  if (!h->uploaded) return fail(h, MPM_ERR_STATE, "no particles uploaded");
+  FILE* f = std::fopen(path, "wb");
+  if (!f) return fail(h, MPM_ERR_INVALID_ARG, std::string("cannot open ") + path);
+  CheckpointHeader hd{kCheckpointMagic, kCheckpointVersion, h->n, h->dom, h->ctx.has_pinned, h->ctx.single_material,
+                      h->ctx.has_thermal, h->ctx.has_plastic, h->scene.mat_base, 0};
+  bool ok = std::fwrite(&hd, sizeof hd, 1, f) == 1;
+  ok = ok && std::fwrite(h->mat_set.data(), 1, kMaxMats, f) == (size_t)kMaxMats;
+  ok = ok && std::fwrite(h->mats_host.data(), sizeof(mpm_material), kMaxMats, f) == (size_t)kMaxMats;
+  const mpm::Particles& p = h->ctx.p;
+  struct Arr { const void* d; size_t es; int comps; } arrs[] = {
+      {p.qx, 4, 1}, {p.qy, 4, 1}, {p.qz, 4, 1}, {p.vx, 4, 1}, {p.vy, 4, 1}, {p.vz, 4, 1}, {p.C, 4, 9}, {p.D, 4, 9},
+      {p.m, 4, 1}, {p.V, 4, 1}, {p.ep, 4, 1}, {p.T, 4, 1}, {p.mat, 2, 1}, {p.pinned, 1, 1}};
+  std::vector<char> buf;
+  cudaStreamSynchronize(h->stream);
+  for (const Arr& a : arrs) {
+    for (int comp = 0; comp < a.comps && ok; ++comp) {
+      const size_t bytes = a.es * h->n;
+      buf.resize(bytes + 1);
+      const char* src = static_cast<const char*>(a.d) + comp * a.es * p.cap;
+      if (bytes && cudaMemcpy(buf.data(), src, bytes, cudaMemcpyDeviceToHost) != cudaSuccess) ok = false;
+      ok = ok && (bytes == 0 || std::fwrite(buf.data(), 1, bytes, f) == bytes);
+    }
+  }
+  std::fclose(f);
+  return ok ? MPM_OK : fail(h, MPM_ERR_CUDA, "checkpoint write failed");
+}
+
+int mpm_checkpoint_load(mpm_handle* h, const char* path) {
+  if (!h || !path) return MPM_ERR_INVALID_ARG;
+  FILE* f = std::fopen(path, "rb");
+  if (!f) return fail(h, MPM_ERR_INVALID_ARG, std::string("cannot open ") + path);
+  CheckpointHeader hd;
+  bool ok = std::fread(&hd, sizeof hd, 1, f) == 1 && hd.magic == kCheckpointMagic && hd.version == kCheckpointVersion;
+  if (!ok) {
+    std::fclose(f);
+    return fail(h, MPM_ERR_INVALID_ARG, "not a checkpoint of this format");
+  }
+  if (hd.n > h->cap) {
+    std::fclose(f);
+    return fail(h, MPM_ERR_CAPACITY, "checkpoint holds more particles than the handle's capacity");
+  }
+  std::vector<char> set(kMaxMats);
+  std::vector<mpm_material> mats(kMaxMats);
+  ok = std::fread(set.data(), 1, kMaxMats, f) == (size_t)kMaxMats &&
+       std::fread(mats.data(), sizeof(mpm_material), kMaxMats, f) == (size_t)kMaxMats;
+  if (!ok) {
+    std::fclose(f);
+    return fail(h, MPM_ERR_INVALID_ARG, "truncated checkpoint");
+  }
+  int rc = mpm_configure_domain(h, &hd.dom);
+  if (rc != MPM_OK) {
+    std::fclose(f);
+    return rc;
+  }
+  for (int i = 0; i < kMaxMats; ++i)
+    if (set[i]) mpm_set_material(h, i, &mats[i]);
+  const mpm::Particles& p = h->ctx.p;
+  struct Arr { void* d; size_t es; int comps; } arrs[] = {
+      {p.qx, 4, 1}, {p.qy, 4, 1}, {p.qz, 4, 1}, {p.vx, 4, 1}, {p.vy, 4, 1}, {p.vz, 4, 1}, {p.C, 4, 9}, {p.D, 4, 9},
+      {p.m, 4, 1}, {p.V, 4, 1}, {p.ep, 4, 1}, {p.T, 4, 1}, {p.mat, 2, 1}, {p.pinned, 1, 1}};
+  std::vector<char> buf;
+  cudaStreamSynchronize(h->stream);
+  for (const Arr& a : arrs) {
+    for (int comp = 0; comp < a.comps && ok; ++comp) {
+      const size_t bytes = a.es * hd.n;
+      buf.resize(bytes + 1);
+      ok = bytes == 0 || std::fread(buf.data(), 1, bytes, f) == bytes;
+      char* dst = static_cast<char*>(a.d) + comp * a.es * p.cap;
+      if (ok && bytes && cudaMemcpy(dst, buf.data(), bytes, cudaMemcpyHostToDevice) != cudaSuccess) ok = false;
+    }
+  }
+  std::fclose(f);
+  if (!ok) return fail(h, MPM_ERR_INVALID_ARG, "truncated checkpoint");
+  h->n = hd.n;
+  h->ctx.n = hd.n;
+  h->ctx.has_pinned = hd.has_pinned;
+  h->ctx.single_material = hd.single_material;
+  h->ctx.has_thermal = hd.has_thermal;
+  h->ctx.has_plastic = hd.has_plastic;
+  h->scene.mat_base = hd.mat_base;
+  h->scene.p_begin = 0;
+  h->scene.p_end = hd.n;
+  MPM_CUDA(h, cudaMemcpyAsync(const_cast<SceneDev*>(h->ctx.scenes), &h->scene, sizeof(SceneDev), cudaMemcpyHostToDevice,
+                              h->stream));
+  MPM_CUDA(h, cudaStreamSynchronize(h->stream));
+  h->uploaded = true;
+  h->grid_valid = false;
+  return MPM_OK;
+}
+
+int mpm_host_alloc(size_t bytes, void** out) {
+  if (!out || bytes == 0) return MPM_ERR_INVALID_ARG;
+  return cudaMallocHost(out, bytes) == cudaSuccess ? MPM_OK : MPM_ERR_OUT_OF_MEMORY;
+}
+
+int mpm_host_free(void* p) { return cudaFreeHost(p) == cudaSuccess ? MPM_OK : MPM_ERR_CUDA; }
+
+int mpm_return_map_batch(const mpm_material* material, int64_t n, const double* F_in, const double* ep, const double* T,
+                         double dt, double* F_out, double* dep, double* tau) {
+  std::string why;
+  int rc = validate_material(material, why);
+  if (rc != MPM_OK) return rc;
+  if (n < 0 || (n > 0 && (!F_in || !F_out || !dep || !tau))) return MPM_ERR_INVALID_ARG;
+  if (n == 0) return MPM_OK;
+  const MaterialDev md = to_device(*material);
+  double* d = nullptr;
+  const size_t bytes = (size_t)n * (9 + 1 + 1 + 9 + 1 + 9) * sizeof(double);
+  if (cudaMalloc(&d, bytes) != cudaSuccess) return MPM_ERR_OUT_OF_MEMORY;
+  double *dF = d, *dep_in = dF + 9 * n, *dT = dep_in + n, *dFo = dT + n, *ddep = dFo + 9 * n, *dtau = ddep + n;
+  cudaError_t e = cudaMemcpy(dF, F_in, 9 * n * sizeof(double), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess && ep) e = cudaMemcpy(dep_in, ep, n * sizeof(double), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess && T) e = cudaMemcpy(dT, T, n * sizeof(double), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) {
+    mpm::launch_return_map_batch(md, n, dF, ep ? dep_in : nullptr, T ? dT : nullptr, static_cast<float>(dt), dFo, ddep, dtau,
+                                 nullptr);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpy(F_out, dFo, 9 * n * sizeof(double), cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess) e = cudaMemcpy(dep, ddep, n * sizeof(double), cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess) e = cudaMemcpy(tau, dtau, 9 * n * sizeof(double), cudaMemcpyDeviceToHost);
+  cudaFree(d);
+  return e == cudaSuccess ? MPM_OK : MPM_ERR_CUDA;
+}
+
+}  // extern "C"

@@ -1,0 +1,160 @@
+// Internal device data layout of the MLS-MPM step (not part of the C ABI).
+//
+// HBM layout (structure of arrays, one array per component, all 4-byte aligned and coalesced):
+//   particles  qx,qy,qz  u32 fixed-point position in cell units from the scene's grid origin
+//                        (22 fractional bits: 2^-22 cell resolution, grids up to 1023 nodes/axis)
+//              vx,vy,vz  f32 velocity (m/s)
+//              C[9]      f32 APIC affine matrix (1/s)
+//              D[9]      f32 F - I (centred deformation gradient)
+//              m, V      f32 mass, reference volume (read-only in the step)
+//              ep, T     f32 plastic strain, temperature
+//              mat       u16 material index, pinned u8 (read only when the scene needs them)
+//              key       u32 particle-tile key for the next counting sort, perm u32 sorted->home
+//   grid       acc0[2]   float4 (m, px, py, pz)  scatter accumulators, ping-pong by substep
+//              acc1[2]   float4 (fx, fy, fz, pinned mass)  stress force (dt-free) channel
+//              vel       float4 (vx, vy, vz, m) updated grid velocity, TMA source of the gather
+//              node order per scene ((z*gy)+y)*gx+x, gx,gy,gz multiples of 4 (storage dims)
+//   tiles      particle tile = 4x4x4 stencil bases; node tile = 4x4x4 nodes
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "mpm_math.h"
+
+namespace mpm {
+
+constexpr int kFracBits = 22;
+constexpr float kFixedOne = 4194304.0f;        // 2^22
+constexpr float kInvFixedOne = 2.384185791015625e-07f;
+constexpr int kTile = 4;                         // tile edge (cells / nodes)
+constexpr int kWinG = 6;                         // gather window edge (nodes)
+constexpr int kWinS = 8;                         // scatter window edge (nodes)
+constexpr int kWinSNodes = kWinS * kWinS * kWinS;
+constexpr int kChannels = 8;                     // m, px, py, pz, fx, fy, fz, pinned mass
+constexpr int kBlock = 256;                      // threads per CTA in the particle kernels
+constexpr int kMaxScenes = 4096;
+constexpr int kMaxMaterials = 4096;
+
+enum StepMode : int { kModeFixed = 0, kModeRequested = 1, kModeCfl = 2 };
+
+struct SceneDev {
+  float H, invH;
+  int dims[3];          // reference node counts per axis
+  int gdim[3];          // storage dims (4 * tiles + 4)
+  int tiles[3];         // particle tiles per axis
+  int ntiles[3];        // node tiles per axis (gdim / 4)
+  long long node_base;  // first node of this scene in the grid arrays
+  int tile_base;        // first particle tile (global id)
+  int node_tile_base;   // first node tile (global id)
+  int wall_lo[3];       // node index <= wall_lo: within one cell of lower (reference q < lower + h)
+  int wall_hi[3];       // node index >= wall_hi: within one cell of upper (q > upper - h)
+  unsigned qlo[3], qhi[3];  // fixed-point clamp range of positions
+  int clamp, sticky;
+  float gravity[3];
+  float mass_eps;
+  float cfl, dt_max, grad_limit;
+  int mat_base, nmat;
+  long long p_begin, p_end;  // home particle range
+  double origin[3];
+};
+
+struct Ctrl {
+  double remaining;     // requested-mode time left in this call
+  double dt_requested;
+  double advanced;
+  double plastic_work;  // accumulated heat from plastic work (J), FP64
+  int substeps;         // substeps done in this call
+  int max_substeps;
+  int done;
+  int mode;
+  float dt_fixed;
+  unsigned step_index;  // parity source: grid state lives in acc[(step_index) & 1] before a substep
+  unsigned status;      // MPM_STATUS_* flags
+  unsigned work_count[2];
+  unsigned work_next;
+  unsigned active_count[2];
+  unsigned grid_next;
+  unsigned scan_ticket;
+  unsigned pad[2];
+};
+
+struct Particles {
+  unsigned *qx, *qy, *qz;
+  float *vx, *vy, *vz;
+  float* C;   // 9 component arrays, stride cap
+  float* D;   // 9 component arrays, stride cap
+  float *m, *V, *ep, *T;
+  unsigned short* mat;
+  unsigned char* pinned;
+  unsigned* key;
+  unsigned* perm;
+  long long cap;
+};
+
+struct Grid {
+  float4* acc0[2];
+  float4* acc1[2];
+  float4* vel;
+  unsigned* tile_flag;   // per node tile
+  unsigned* active[2];   // active node-tile lists
+};
+
+struct SortBufs {
+  unsigned* count;      // per particle tile, total_tiles + 1
+  unsigned* start;      // block-local exclusive scan, total_tiles + 1
+  unsigned* block_off;  // exclusive scan of block sums
+  uint4* work[2];       // (tile, start, count, scene)
+};
+
+struct Ctx {
+  Particles p;
+  Grid g;
+  SortBufs s;
+  const SceneDev* scenes;
+  const MaterialDev* mats;
+  Ctrl* ctrl;
+  float* dt_scene;      // per scene
+  unsigned* wave_max;   // per scene, float bits of max(|v| + c * stretch)
+  unsigned* grad_max;   // per scene, float bits of max sum|C|
+  const void* tmaps;    // per scene CUtensorMap (64-byte aligned), or null
+  long long n;
+  int nscenes;
+  int total_tiles;
+  int total_node_tiles;
+  int has_pinned;
+  int single_material;
+  int has_thermal;      // temperature array is read and written
+  int has_plastic;      // plastic strain array is read and written
+  int use_tma;
+};
+
+// Launch wrappers (mpm_kernels.cu)
+void launch_control_init(const Ctx& c, cudaStream_t st);
+void launch_keys(const Ctx& c, cudaStream_t st);
+void launch_scan(const Ctx& c, cudaStream_t st);
+void launch_sort_scatter(const Ctx& c, cudaStream_t st, bool initial);
+void launch_p2g(const Ctx& c, cudaStream_t st, int grid_blocks);
+void launch_control_step(const Ctx& c, cudaStream_t st, int mode, double dt_req, int max_substeps, float dt_fixed);
+void launch_begin(const Ctx& c, cudaStream_t st);
+void launch_grid_clear(const Ctx& c, cudaStream_t st, int grid_blocks);
+void launch_grid_update(const Ctx& c, cudaStream_t st, int grid_blocks);
+void launch_g2p2g(const Ctx& c, cudaStream_t st, int grid_blocks, bool scatter);
+void launch_ledger(const Ctx& c, cudaStream_t st, double* partials, int blocks, double* out);
+void launch_grid_debug(const Ctx& c, cudaStream_t st, int scene, float dt, double* mass, double* mom);
+void launch_upload_convert(const Ctx& c, cudaStream_t st, long long n, int dtype, const void* const* src,
+                           const int* material, const unsigned char* pinned, unsigned fields);
+void launch_download_convert(const Ctx& c, cudaStream_t st, long long n, int dtype, void* const* dst,
+                             unsigned fields);
+void launch_return_map_batch(const MaterialDev& m, long long n, const double* F_in, const double* ep,
+                             const double* T, float dt, double* F_out, double* dep, double* tau,
+                             cudaStream_t st);
+int g2p2g_blocks_per_sm(bool scatter);
+int p2g_blocks_per_sm();
+
+// field bits of the conversion kernels
+enum Field : unsigned {
+  kFieldPos = 1u << 0, kFieldVel = 1u << 1, kFieldMass = 1u << 2, kFieldVolume = 1u << 3,
+  kFieldTemp = 1u << 4, kFieldPlastic = 1u << 5, kFieldF = 1u << 6, kFieldC = 1u << 7
+};
+
+}  // namespace mpm

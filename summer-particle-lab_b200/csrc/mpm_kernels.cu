@@ -1,0 +1,1237 @@
+// CUDA kernels of the B200-native MLS-MPM solid step (sm_100a).
+//
+// One substep is five launches on one stream (all persistent or grid-stride, no host sync):
+//   k_begin        1 CTA: dt from the device-side CFL maxima, step bookkeeping, list resets
+//   k_grid_update  active node tiles only: v = (p + dt (f + m g)) / m, walls, sticky floor
+//   k_g2p2g        per particle tile: TMA-staged 6^3 velocity window -> gather v, C -> F update
+//                  -> advect -> constitutive update / J2 return -> scatter m, p, f of the new
+//                  state into an 8^3 shared-memory window -> one float4 atomic per node per tile;
+//                  emits the next sort key and the next CFL maxima
+//   k_scan         exclusive scan of per-tile counts (last-block-done, one launch)
+//   k_sort_scatter counting sort: perm[start + rank] = particle, first claimer appends the tile
+//                  to the work list
+// The scatter is dt-free (m, p = sum w (m v + m C dpos), f = -sum w (4V/h) tau dpos), so the next
+// substep's dt can be chosen on the device after the whole state is known, as the reference does
+// (src/three/simulation.js:308-310); the grid update applies dt.
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "mpm_internal.h"
+
+namespace mpm {
+
+// ---------------------------------------------------------------------------------------------
+// small device helpers
+
+__device__ __forceinline__ unsigned smem_addr(const void* p) {
+  return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void fence_barrier_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void fence_proxy_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(unsigned long long* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+               : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_addr(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// Bounded wait: gives up after about 2^31 SM cycles (~1 s) and reports false.
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsigned parity) {
+  const long long t0 = clock64();
+  while (!mbar_try_wait(bar, parity)) {
+    if (clock64() - t0 > (1ll << 31)) return false;
+  }
+  return true;
+}
+
+// 4D tiled TMA load (no multicast): box {4 channels, 6, 6, 6} of the grid velocity array.
+// The innermost coordinate is the channel index 0, so the 16-byte alignment rule holds.
+__device__ __forceinline__ void tma_load_4d(void* dst, const void* tmap, int c0, int c1, int c2, int c3,
+                                            unsigned long long* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, "
+      "%4, %5}], [%6];" ::"r"(smem_addr(dst)),
+      "l"(tmap), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(smem_addr(bar))
+      : "memory");
+}
+
+__device__ __forceinline__ int find_scene_by_particle(const SceneDev* sc, int ns, long long i) {
+  int lo = 0, hi = ns - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (sc[mid].p_begin <= i) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+__device__ __forceinline__ int find_scene_by_tile(const SceneDev* sc, int ns, int t) {
+  int lo = 0, hi = ns - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (sc[mid].tile_base <= t) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+__device__ __forceinline__ int find_scene_by_node_tile(const SceneDev* sc, int ns, int t) {
+  int lo = 0, hi = ns - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (sc[mid].node_tile_base <= t) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+// Stencil along one axis from a fixed-point position (src/three/mpm.js:25-32):
+// base = clamp(floor(q - 0.5), 0, N - 3), t = q - base (exact: integer below 2^24 times 2^-22).
+__device__ __forceinline__ void stencil_axis(unsigned q, int dim, int& base, float& t) {
+  int b = (q < (1u << (kFracBits - 1))) ? -1 : static_cast<int>((q - (1u << (kFracBits - 1))) >> kFracBits);
+  b = min(max(b, 0), dim - 3);
+  base = b;
+  t = static_cast<float>(static_cast<long long>(q) - (static_cast<long long>(b) << kFracBits)) * kInvFixedOne;
+}
+
+__device__ __forceinline__ unsigned tile_key(const SceneDev& sc, const int b[3]) {
+  return static_cast<unsigned>(sc.tile_base) +
+         static_cast<unsigned>(((b[2] >> 2) * sc.tiles[1] + (b[1] >> 2)) * sc.tiles[0] + (b[0] >> 2));
+}
+
+__device__ __forceinline__ void mark_node_tile(const Ctx& c, unsigned tile, int list) {
+  if (atomicExch(&c.g.tile_flag[tile], 1u) == 0u) {
+    const unsigned idx = atomicAdd(&c.ctrl->active_count[list], 1u);
+    c.g.active[list][idx] = tile;
+  }
+}
+
+__device__ __forceinline__ void mark_node_tiles_of(const Ctx& c, const SceneDev& sc, int n0, int n1, int n2,
+                                                   int list) {
+  // node tiles covering nodes [n, n+2] on each axis
+  for (int tz = n2 >> 2; tz <= (n2 + 2) >> 2; ++tz)
+    for (int ty = n1 >> 2; ty <= (n1 + 2) >> 2; ++ty)
+      for (int tx = n0 >> 2; tx <= (n0 + 2) >> 2; ++tx)
+        mark_node_tile(c, sc.node_tile_base + (tz * sc.ntiles[1] + ty) * sc.ntiles[0] + tx, list);
+}
+
+// Warp-aggregated increment of the per-tile particle count.
+__device__ __forceinline__ void count_key(const Ctx& c, unsigned key) {
+  const unsigned mask = __match_any_sync(0xffffffffu, key);
+  const int lane = threadIdx.x & 31;
+  if (key != 0xffffffffu && lane == __ffs(mask) - 1) atomicAdd(&c.s.count[key], __popc(mask));
+}
+
+__device__ __forceinline__ double warp_sum_d(double x) {
+  for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+  return x;
+}
+
+__device__ __forceinline__ unsigned fbits(float x) { return __float_as_uint(fmaxf(x, 0.f)); }
+
+struct StepOut {
+  float wave, grad;
+  unsigned key;
+  unsigned flags;
+};
+
+// CFL terms of src/three/mpm.js:43-54 for one particle (F = I + D)
+__device__ __forceinline__ void cfl_terms(const MaterialDev& mt, const float D[9], const float v[3],
+                                          const float C[9], float m, float V, float Jm1, float& wave,
+                                          float& grad) {
+  float row = 0.f, col = 0.f, g = 0.f;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    float r = 0.f, cc = 0.f;
+#pragma unroll
+    for (int b = 0; b < 3; ++b) {
+      r += fabsf(D[a * 3 + b] + (a == b ? 1.f : 0.f));
+      cc += fabsf(D[b * 3 + a] + (a == b ? 1.f : 0.f));
+      g += fabsf(C[a * 3 + b]);
+    }
+    row = fmaxf(row, r);
+    col = fmaxf(col, cc);
+  }
+  const float compression = mt.model == 1 ? 1.f / fmaxf(0.05f, 1.f + Jm1) : 1.f;
+  const float c = sqrtf(mt.wave_modulus * V / m);
+  const float speed = sqrtf(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+  wave = speed + c * fmaxf(1.f, fmaxf(row * col, compression));
+  grad = g;
+}
+
+// ---------------------------------------------------------------------------------------------
+// control
+
+struct ControlOp {
+  int op;           // 0: reset lists for an initial sort + P2G, 1: start a step call
+  int mode;
+  double dt_requested;
+  int max_substeps;
+  float dt_fixed;
+};
+
+__global__ void k_control(Ctx c, ControlOp op) {
+  Ctrl* ct = c.ctrl;
+  if (threadIdx.x == 0) {
+    const unsigned k = ct->step_index;
+    if (op.op == 0) {
+      ct->work_count[k & 1] = 0;
+      ct->active_count[k & 1] = 0;
+      ct->work_next = 0;
+      ct->done = 0;
+    } else {
+      ct->remaining = op.dt_requested;
+      ct->dt_requested = op.dt_requested;
+      ct->advanced = 0.0;
+      ct->substeps = 0;
+      ct->max_substeps = op.max_substeps;
+      ct->done = 0;
+      ct->mode = op.mode;
+      ct->dt_fixed = op.dt_fixed;
+    }
+  }
+  if (op.op == 0) {
+    for (int s = threadIdx.x; s < c.nscenes; s += blockDim.x) {
+      c.wave_max[s] = 0u;
+      c.grad_max[s] = 0u;
+    }
+  }
+}
+
+void launch_control_init(const Ctx& c, cudaStream_t st) {
+  ControlOp op{0, 0, 0.0, 0, 0.f};
+  k_control<<<1, 256, 0, st>>>(c, op);
+}
+
+void launch_control_step(const Ctx& c, cudaStream_t st, int mode, double dt_req, int max_substeps, float dt_fixed) {
+  ControlOp op{1, mode, dt_req, max_substeps, dt_fixed};
+  k_control<<<1, 32, 0, st>>>(c, op);
+}
+
+// Substep prologue: picks dt per scene, or marks the call done.
+__global__ void __launch_bounds__(256) k_begin(Ctx c) {
+  Ctrl* ct = c.ctrl;
+  __shared__ float smin[8];
+  __shared__ int sdone;
+  __shared__ float sdt;
+  if (ct->done) return;
+  if (ct->status & 0x8u) {  // a bounded wait gave up: stop this call
+    if (threadIdx.x == 0) ct->done = 1;
+    return;
+  }
+  float local = 3.0e38f;
+  for (int s = threadIdx.x; s < c.nscenes; s += blockDim.x) {
+    const SceneDev& sc = c.scenes[s];
+    const float wave = fmaxf(1.f, __uint_as_float(c.wave_max[s]));
+    const float grad = fmaxf(1.f, __uint_as_float(c.grad_max[s]));
+    const float dt = fminf(sc.dt_max, fminf(sc.cfl * sc.H / wave, sc.grad_limit / grad));
+    c.dt_scene[s] = dt;  // provisional: the scene's own stable dt
+    local = fminf(local, dt);
+  }
+  for (int o = 16; o > 0; o >>= 1) local = fminf(local, __shfl_xor_sync(0xffffffffu, local, o));
+  if ((threadIdx.x & 31) == 0) smin[threadIdx.x >> 5] = local;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    float m = smin[0];
+    for (int w = 1; w < (int)(blockDim.x >> 5); ++w) m = fminf(m, smin[w]);
+    int done = 0;
+    float dt = m;
+    if (ct->substeps >= ct->max_substeps) done = 1;
+    if (ct->mode == kModeRequested) {
+      if (!(ct->remaining > 1e-6 * ct->dt_requested)) done = 1;
+      dt = static_cast<float>(fmin(ct->remaining, static_cast<double>(m)));
+      if (!done) {
+        // the last substep takes exactly what is left (src/three/simulation.js:309)
+        if (ct->remaining - dt <= 1e-6 * ct->dt_requested) dt = static_cast<float>(ct->remaining);
+        ct->remaining -= dt;
+      }
+    } else if (ct->mode == kModeFixed) {
+      dt = ct->dt_fixed;
+    }
+    if (done) {
+      ct->done = 1;
+    } else {
+      ct->substeps += 1;
+      ct->advanced += dt;
+      const unsigned k = ct->step_index + 1;
+      ct->step_index = k;
+      ct->work_count[k & 1] = 0;
+      ct->active_count[k & 1] = 0;
+      ct->work_next = 0;
+      ct->grid_next = 0;
+    }
+    sdone = done;
+    sdt = dt;
+  }
+  __syncthreads();
+  if (sdone) return;
+  for (int s = threadIdx.x; s < c.nscenes; s += blockDim.x) {
+    if (ct->mode != kModeCfl) c.dt_scene[s] = sdt;
+    c.wave_max[s] = 0u;
+    c.grad_max[s] = 0u;
+  }
+}
+
+void launch_begin(const Ctx& c, cudaStream_t st) { k_begin<<<1, 256, 0, st>>>(c); }
+
+// ---------------------------------------------------------------------------------------------
+// counting sort by particle tile
+
+__global__ void __launch_bounds__(256) k_keys(Ctx c) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  unsigned key = 0xffffffffu;
+  if (i < c.n) {
+    const int s = c.nscenes == 1 ? 0 : find_scene_by_particle(c.scenes, c.nscenes, i);
+    const SceneDev& sc = c.scenes[s];
+    int b[3];
+    float t;
+    stencil_axis(c.p.qx[i], sc.dims[0], b[0], t);
+    stencil_axis(c.p.qy[i], sc.dims[1], b[1], t);
+    stencil_axis(c.p.qz[i], sc.dims[2], b[2], t);
+    key = tile_key(sc, b);
+    c.p.key[i] = key;
+  }
+  count_key(c, key);
+}
+
+void launch_keys(const Ctx& c, cudaStream_t st) {
+  const long long blocks = (c.n + 255) / 256;
+  if (blocks > 0) k_keys<<<static_cast<unsigned>(blocks), 256, 0, st>>>(c);
+}
+
+constexpr int kScanThreads = 1024;
+constexpr int kScanPer = 4;
+constexpr int kScanChunk = kScanThreads * kScanPer;  // 4096 tiles per block
+
+// Exclusive scan of count[0..T] into start (block-local) + block_off (per 4096 tiles).
+// The last block to finish scans the block sums (threadfence + ticket).
+__global__ void __launch_bounds__(kScanThreads) k_scan(Ctx c) {
+  if (c.ctrl->done) return;
+  if (c.ctrl->status & 0x8u) return;
+  __shared__ unsigned warp_sums[32];
+  __shared__ bool last;
+  const int T = c.total_tiles + 1;
+  const int base = blockIdx.x * kScanChunk + threadIdx.x * kScanPer;
+  unsigned v[kScanPer];
+  unsigned sum = 0;
+#pragma unroll
+  for (int k = 0; k < kScanPer; ++k) {
+    v[k] = (base + k < c.total_tiles) ? c.s.count[base + k] : 0u;
+    sum += v[k];
+  }
+  // block exclusive scan of per-thread sums
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  unsigned incl = sum;
+  for (int o = 1; o < 32; o <<= 1) {
+    const unsigned y = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += y;
+  }
+  if (lane == 31) warp_sums[wid] = incl;
+  __syncthreads();
+  if (wid == 0) {
+    unsigned ws = warp_sums[lane];
+    unsigned wi = ws;
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned y = __shfl_up_sync(0xffffffffu, wi, o);
+      if (lane >= o) wi += y;
+    }
+    warp_sums[lane] = wi - ws;
+  }
+  __syncthreads();
+  unsigned run = warp_sums[wid] + incl - sum;
+#pragma unroll
+  for (int k = 0; k < kScanPer; ++k) {
+    if (base + k < T) c.s.start[base + k] = run;
+    run += v[k];
+  }
+  if (threadIdx.x == kScanThreads - 1) c.s.block_off[blockIdx.x] = run;  // block total
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = (atomicAdd(&c.ctrl->scan_ticket, 1u) == gridDim.x - 1);
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  // last block: exclusive scan of the block totals (gridDim.x <= 1024 * 64 blocks)
+  __shared__ unsigned carry;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  for (int b0 = 0; b0 < (int)gridDim.x; b0 += kScanThreads) {
+    const int b = b0 + threadIdx.x;
+    const unsigned x = (b < (int)gridDim.x) ? *((volatile unsigned*)&c.s.block_off[b]) : 0u;
+    unsigned inc = x;
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned y = __shfl_up_sync(0xffffffffu, inc, o);
+      if (lane >= o) inc += y;
+    }
+    if (lane == 31) warp_sums[wid] = inc;
+    __syncthreads();
+    if (wid == 0) {
+      unsigned ws = warp_sums[lane];
+      unsigned wi = ws;
+      for (int o = 1; o < 32; o <<= 1) {
+        const unsigned y = __shfl_up_sync(0xffffffffu, wi, o);
+        if (lane >= o) wi += y;
+      }
+      warp_sums[lane] = wi - ws;
+    }
+    __syncthreads();
+    const unsigned excl = carry + warp_sums[wid] + inc - x;
+    if (b < (int)gridDim.x) c.s.block_off[b] = excl;
+    __syncthreads();
+    if (threadIdx.x == kScanThreads - 1) carry = excl + x;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) c.ctrl->scan_ticket = 0;
+}
+
+void launch_scan(const Ctx& c, cudaStream_t st) {
+  const int blocks = (c.total_tiles + 1 + kScanChunk - 1) / kScanChunk;
+  k_scan<<<blocks, kScanThreads, 0, st>>>(c);
+}
+
+__device__ __forceinline__ unsigned tile_start(const Ctx& c, unsigned k) {
+  return c.s.start[k] + c.s.block_off[k / kScanChunk];
+}
+
+// perm[start(k) + rank] = home slot; the group that claims a tile first appends the work item.
+__global__ void __launch_bounds__(256) k_sort_scatter(Ctx c, int initial) {
+  if (!initial && c.ctrl->done) return;
+  if (c.ctrl->status & 0x8u) return;  // a bounded wait gave up this substep
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const unsigned key = i < c.n ? c.p.key[i] : 0xffffffffu;
+  const unsigned mask = __match_any_sync(0xffffffffu, key);
+  if (key == 0xffffffffu) return;
+  const int lane = threadIdx.x & 31;
+  const int leader = __ffs(mask) - 1;
+  const unsigned below = __popc(mask & ((1u << lane) - 1u));
+  const unsigned group = __popc(mask);
+  unsigned old = 0;
+  if (lane == leader) old = atomicSub(&c.s.count[key], group);
+  old = __shfl_sync(mask, old, leader);
+  const unsigned s0 = tile_start(c, key);
+  const unsigned cnt = tile_start(c, key + 1) - s0;
+  // counts and keys always agree; a mismatch is reported and the write skipped
+  if (old < below + 1 || old > cnt || static_cast<long long>(s0) + old - 1 - below >= c.n) {
+    atomicOr(&c.ctrl->status, 0x20u);
+    return;
+  }
+  c.p.perm[s0 + old - 1 - below] = static_cast<unsigned>(i);
+  if (lane == leader && old == cnt) {
+    const unsigned list = c.ctrl->step_index & 1u;
+    const unsigned idx = atomicAdd(&c.ctrl->work_count[list], 1u);
+    const int s = c.nscenes == 1 ? 0 : find_scene_by_tile(c.scenes, c.nscenes, static_cast<int>(key));
+    if (idx < static_cast<unsigned>(c.total_tiles)) c.s.work[list][idx] = make_uint4(key, s0, cnt, static_cast<unsigned>(s));
+  }
+}
+
+void launch_sort_scatter(const Ctx& c, cudaStream_t st, bool initial) {
+  const long long blocks = (c.n + 255) / 256;
+  if (blocks > 0) k_sort_scatter<<<static_cast<unsigned>(blocks), 256, 0, st>>>(c, initial ? 1 : 0);
+}
+
+// ---------------------------------------------------------------------------------------------
+// particle kernels
+
+struct __align__(128) TileSmem {
+  float4 vwin[kWinG * kWinG * kWinG];   // 3456 bytes, TMA destination
+  float acc[kChannels * kWinSNodes];    // 16 KiB scatter window
+  unsigned long long mbar;
+  uint4 item;
+  int abort_flag;
+  unsigned red[3 * (kBlock / 32)];
+  double work[kBlock / 32];
+};
+
+// Scatter one particle's m, p, f (and pinned mass) into the shared window, or to global memory
+// when its stencil leaves the window (moved more than one cell in one substep).
+__device__ __forceinline__ void scatter_particle(const Ctx& c, const SceneDev& sc, TileSmem& sm, int nxt,
+                                                 const int tile[3], const unsigned q[3], float m, float V,
+                                                 const float v[3], const float C[9], const Sym3& tau,
+                                                 bool pinned, unsigned& key) {
+  int b[3];
+  float t[3], w[3][3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    stencil_axis(q[a], sc.dims[a], b[a], t[a]);
+    bspline_weights(t[a], w[a]);
+  }
+  key = tile_key(sc, b);
+  const float H = sc.H;
+  const float mH = m * H;
+  // p = w (m v + m C dpos), dpos = (i - t) H ; f = -w (4 V / H) tau (i - t)
+  const float mv0 = m * v[0], mv1 = m * v[1], mv2 = m * v[2];
+  const float a00 = mH * C[0], a01 = mH * C[1], a02 = mH * C[2];
+  const float a10 = mH * C[3], a11 = mH * C[4], a12 = mH * C[5];
+  const float a20 = mH * C[6], a21 = mH * C[7], a22 = mH * C[8];
+  const float s = -4.f * V * sc.invH;
+  const float s00 = s * tau.xx, s01 = s * tau.xy, s02 = s * tau.xz;
+  const float s11 = s * tau.yy, s12 = s * tau.yz, s22 = s * tau.zz;
+  const int l0 = b[0] - (tile[0] * kTile - 1), l1 = b[1] - (tile[1] * kTile - 1), l2 = b[2] - (tile[2] * kTile - 1);
+  const bool in_window = l0 >= 0 && l0 <= kWinS - 3 && l1 >= 0 && l1 <= kWinS - 3 && l2 >= 0 && l2 <= kWinS - 3;
+  if (!in_window) atomicOr(&c.ctrl->status, 0x10u);
+#pragma unroll
+  for (int kz = 0; kz < 3; ++kz) {
+    const float dz = static_cast<float>(kz) - t[2];
+#pragma unroll
+    for (int ky = 0; ky < 3; ++ky) {
+      const float dy = static_cast<float>(ky) - t[1];
+      const float wyz = w[1][ky] * w[2][kz];
+      const float p0 = mv0 + a01 * dy + a02 * dz, p1 = mv1 + a11 * dy + a12 * dz, p2 = mv2 + a21 * dy + a22 * dz;
+      const float f0 = s01 * dy + s02 * dz, f1 = s11 * dy + s12 * dz, f2 = s12 * dy + s22 * dz;
+#pragma unroll
+      for (int kx = 0; kx < 3; ++kx) {
+        const float dx = static_cast<float>(kx) - t[0];
+        const float wt = w[0][kx] * wyz;
+        const float vals[7] = {wt * m,
+                               wt * (p0 + a00 * dx),
+                               wt * (p1 + a10 * dx),
+                               wt * (p2 + a20 * dx),
+                               wt * (f0 + s00 * dx),
+                               wt * (f1 + s01 * dx),
+                               wt * (f2 + s02 * dx)};
+        if (in_window) {
+          const int node = ((l2 + kz) * kWinS + (l1 + ky)) * kWinS + (l0 + kx);
+#pragma unroll
+          for (int ch = 0; ch < 7; ++ch) atomicAdd(&sm.acc[ch * kWinSNodes + node], vals[ch]);
+          if (pinned && wt > 1e-8f) atomicAdd(&sm.acc[7 * kWinSNodes + node], wt * m);
+        } else {
+          const long long node = sc.node_base +
+                                 ((long long)(b[2] + kz) * sc.gdim[1] + (b[1] + ky)) * sc.gdim[0] + (b[0] + kx);
+          float* a0 = reinterpret_cast<float*>(&c.g.acc0[nxt][node]);
+          float* a1 = reinterpret_cast<float*>(&c.g.acc1[nxt][node]);
+          atomicAdd(a0 + 0, vals[0]);
+          atomicAdd(a0 + 1, vals[1]);
+          atomicAdd(a0 + 2, vals[2]);
+          atomicAdd(a0 + 3, vals[3]);
+          atomicAdd(a1 + 0, vals[4]);
+          atomicAdd(a1 + 1, vals[5]);
+          atomicAdd(a1 + 2, vals[6]);
+          if (pinned && wt > 1e-8f) atomicAdd(a1 + 3, wt * m);
+        }
+      }
+    }
+  }
+  if (!in_window) mark_node_tiles_of(c, sc, b[0], b[1], b[2], nxt);
+}
+
+// Flush the shared scatter window of one tile to the global accumulators (one float4 atomic per
+// touched node and channel group) and clear it; mark the 27 node tiles it covers as active.
+__device__ __forceinline__ void flush_window(const Ctx& c, const SceneDev& sc, TileSmem& sm, int nxt,
+                                             const int tile[3]) {
+  const int o0 = tile[0] * kTile - 1, o1 = tile[1] * kTile - 1, o2 = tile[2] * kTile - 1;
+  for (int i = threadIdx.x; i < kWinSNodes; i += kBlock) {
+    const float mass = sm.acc[i];
+    if (mass != 0.f) {
+      const int x = o0 + (i & 7), y = o1 + ((i >> 3) & 7), z = o2 + (i >> 6);
+      if (x >= 0 && y >= 0 && z >= 0) {
+        const long long node = sc.node_base + ((long long)z * sc.gdim[1] + y) * sc.gdim[0] + x;
+        atomicAdd(&c.g.acc0[nxt][node], make_float4(mass, sm.acc[1 * kWinSNodes + i], sm.acc[2 * kWinSNodes + i],
+                                                    sm.acc[3 * kWinSNodes + i]));
+        atomicAdd(&c.g.acc1[nxt][node], make_float4(sm.acc[4 * kWinSNodes + i], sm.acc[5 * kWinSNodes + i],
+                                                    sm.acc[6 * kWinSNodes + i], sm.acc[7 * kWinSNodes + i]));
+      }
+    }
+#pragma unroll
+    for (int ch = 0; ch < kChannels; ++ch) sm.acc[ch * kWinSNodes + i] = 0.f;
+  }
+  if (threadIdx.x < 27) {
+    const int dx = threadIdx.x % 3 - 1, dy = (threadIdx.x / 3) % 3 - 1, dz = threadIdx.x / 9 - 1;
+    const int tx = tile[0] + dx, ty = tile[1] + dy, tz = tile[2] + dz;
+    if (tx >= 0 && ty >= 0 && tz >= 0 && tx < sc.ntiles[0] && ty < sc.ntiles[1] && tz < sc.ntiles[2])
+      mark_node_tile(c, sc.node_tile_base + (tz * sc.ntiles[1] + ty) * sc.ntiles[0] + tx, nxt);
+  }
+}
+
+// Block reduction of the per-thread CFL maxima and status flags of one tile, then one atomic per
+// tile and scene. Every thread of the CTA calls it; red holds 3 values per warp.
+__device__ __forceinline__ void block_reduce_item(const Ctx& c, int scene, float wave, float grad, unsigned flags,
+                                                  unsigned* red) {
+  const unsigned wb = __reduce_max_sync(0xffffffffu, fbits(wave));
+  const unsigned gb = __reduce_max_sync(0xffffffffu, fbits(grad));
+  const unsigned fl = __reduce_or_sync(0xffffffffu, flags);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0) {
+    red[wid * 3 + 0] = wb;
+    red[wid * 3 + 1] = gb;
+    red[wid * 3 + 2] = fl;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned w = 0, g = 0, f = 0;
+    for (int k = 0; k < kBlock / 32; ++k) {
+      w = max(w, red[k * 3 + 0]);
+      g = max(g, red[k * 3 + 1]);
+      f |= red[k * 3 + 2];
+    }
+    atomicMax(&c.wave_max[scene], w);
+    atomicMax(&c.grad_max[scene], g);
+    if (f) atomicOr(&c.ctrl->status, f);
+  }
+}
+
+__device__ __forceinline__ unsigned state_flags(const float v[3], const float D[9], const Sym3& tau, float Jm1) {
+  float s = v[0] + v[1] + v[2] + tau.xx + tau.yy + tau.zz + tau.xy + tau.xz + tau.yz;
+#pragma unroll
+  for (int k = 0; k < 9; ++k) s += D[k];
+  unsigned f = 0;
+  if (!isfinite(s)) f |= 0x1u;
+  if (!(Jm1 > -1.f)) f |= 0x2u;
+  return f;
+}
+
+// Initial P2G of the uploaded state (stress from F without a return, as updateStress does when no
+// cached stress exists, src/three/mpm.js:33-37), plus the CFL maxima of that state.
+__global__ void __launch_bounds__(kBlock, 2) k_p2g(const __grid_constant__ Ctx c) {
+  __shared__ TileSmem sm;
+  const unsigned k = c.ctrl->step_index;
+  const int lst = k & 1, nxt = k & 1;
+  for (int i = threadIdx.x; i < kChannels * kWinSNodes; i += kBlock) sm.acc[i] = 0.f;
+  __syncthreads();
+  const long long cap = c.p.cap;
+  while (true) {
+    if (threadIdx.x == 0) {
+      const unsigned idx = atomicAdd(&c.ctrl->work_next, 1u);
+      sm.item = idx < c.ctrl->work_count[lst] ? c.s.work[lst][idx] : make_uint4(0xffffffffu, 0, 0, 0);
+    }
+    __syncthreads();
+    const uint4 it = sm.item;
+    if (it.x == 0xffffffffu) break;
+    const int scene = static_cast<int>(it.w);
+    const SceneDev& sc = c.scenes[scene];
+    int tile[3];
+    {
+      const int lt = static_cast<int>(it.x) - sc.tile_base;
+      tile[0] = lt % sc.tiles[0];
+      tile[1] = (lt / sc.tiles[0]) % sc.tiles[1];
+      tile[2] = lt / (sc.tiles[0] * sc.tiles[1]);
+    }
+    float wave_acc = 0.f, grad_acc = 0.f;
+    unsigned flags_acc = 0;
+    for (unsigned j0 = 0; j0 < it.z; j0 += kBlock) {
+      const unsigned j = j0 + threadIdx.x;
+      if (j < it.z) {
+        float wave = 0.f, grad = 0.f;
+        const unsigned home = c.p.perm[it.y + j];
+        const unsigned q[3] = {c.p.qx[home], c.p.qy[home], c.p.qz[home]};
+        float D[9], C[9];
+#pragma unroll
+        for (int e = 0; e < 9; ++e) {
+          D[e] = c.p.D[e * cap + home];
+          C[e] = c.p.C[e * cap + home];
+        }
+        const float v[3] = {c.p.vx[home], c.p.vy[home], c.p.vz[home]};
+        const float m = c.p.m[home], V = c.p.V[home];
+        const int mi = c.single_material ? sc.mat_base : c.p.mat[home];
+        const MaterialDev mt = c.mats[mi];
+        const bool pinned = c.has_pinned && c.p.pinned[home];
+        const float ep = c.has_plastic ? c.p.ep[home] : 0.f;
+        const float T = c.has_thermal ? c.p.T[home] : 0.f;
+        float Dc[9];
+#pragma unroll
+        for (int e = 0; e < 9; ++e) Dc[e] = D[e];
+        const ConstitutiveOut co = constitutive_update(mt, Dc, ep, T, V / m, false);
+        unsigned key;
+        scatter_particle(c, sc, sm, nxt, tile, q, m, V, v, C, co.tau, pinned, key);
+        cfl_terms(mt, D, v, C, m, V, co.Jm1, wave, grad);
+        flags_acc |= state_flags(v, D, co.tau, co.Jm1);
+        wave_acc = fmaxf(wave_acc, wave);
+        grad_acc = fmaxf(grad_acc, grad);
+      }
+    }
+    block_reduce_item(c, scene, wave_acc, grad_acc, flags_acc, sm.red);
+    __syncthreads();
+    flush_window(c, sc, sm, nxt, tile);
+    __syncthreads();
+  }
+}
+
+// Grid update over the active node tiles (src/three/mpm.js:89-102 with gravity on the grid).
+__global__ void __launch_bounds__(256) k_grid_update(Ctx c) {
+  Ctrl* ct = c.ctrl;
+  if (ct->done) return;
+  const unsigned k = ct->step_index;
+  const int cur = (k - 1) & 1;
+  const unsigned count = ct->active_count[cur];
+  const int sub = threadIdx.x >> 6, lid = threadIdx.x & 63;
+  for (unsigned ti = blockIdx.x * 4 + sub; ti < count; ti += gridDim.x * 4) {
+    const unsigned tile = c.g.active[cur][ti];
+    const int s = c.nscenes == 1 ? 0 : find_scene_by_node_tile(c.scenes, c.nscenes, static_cast<int>(tile));
+    const SceneDev& sc = c.scenes[s];
+    const int lt = static_cast<int>(tile) - sc.node_tile_base;
+    const int ntx = lt % sc.ntiles[0], nty = (lt / sc.ntiles[0]) % sc.ntiles[1], ntz = lt / (sc.ntiles[0] * sc.ntiles[1]);
+    const int x = ntx * 4 + (lid & 3), y = nty * 4 + ((lid >> 2) & 3), z = ntz * 4 + (lid >> 4);
+    const long long node = sc.node_base + ((long long)z * sc.gdim[1] + y) * sc.gdim[0] + x;
+    const float4 a0 = c.g.acc0[cur][node];
+    const float4 a1 = c.g.acc1[cur][node];
+    float4 out = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (a0.x > sc.mass_eps) {
+      const float dt = c.dt_scene[s];
+      const float inv = 1.f / a0.x;
+      float v[3] = {(a0.y + dt * (a1.x + a0.x * sc.gravity[0])) * inv,
+                    (a0.z + dt * (a1.y + a0.x * sc.gravity[1])) * inv,
+                    (a0.w + dt * (a1.z + a0.x * sc.gravity[2])) * inv};
+      const int idx[3] = {x, y, z};
+      const bool all_zero = (a1.w > 0.f) || (sc.sticky && y <= sc.wall_lo[1]);
+#pragma unroll
+      for (int a = 0; a < 3; ++a)
+        if (all_zero || (idx[a] <= sc.wall_lo[a] && v[a] < 0.f) || (idx[a] >= sc.wall_hi[a] && v[a] > 0.f)) v[a] = 0.f;
+      out = make_float4(v[0], v[1], v[2], a0.x);
+    }
+    c.g.vel[node] = out;
+    c.g.acc0[cur][node] = make_float4(0.f, 0.f, 0.f, 0.f);
+    c.g.acc1[cur][node] = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (lid == 0) c.g.tile_flag[tile] = 0u;
+  }
+}
+
+// Clears a pending scattered grid (acc[step_index & 1] over its active list) without using it.
+__global__ void __launch_bounds__(256) k_grid_clear(Ctx c) {
+  Ctrl* ct = c.ctrl;
+  const int par = ct->step_index & 1;
+  const unsigned count = ct->active_count[par];
+  const int sub = threadIdx.x >> 6, lid = threadIdx.x & 63;
+  for (unsigned ti = blockIdx.x * 4 + sub; ti < count; ti += gridDim.x * 4) {
+    const unsigned tile = c.g.active[par][ti];
+    const int s = c.nscenes == 1 ? 0 : find_scene_by_node_tile(c.scenes, c.nscenes, static_cast<int>(tile));
+    const SceneDev& sc = c.scenes[s];
+    const int lt = static_cast<int>(tile) - sc.node_tile_base;
+    const int ntx = lt % sc.ntiles[0], nty = (lt / sc.ntiles[0]) % sc.ntiles[1], ntz = lt / (sc.ntiles[0] * sc.ntiles[1]);
+    const int x = ntx * 4 + (lid & 3), y = nty * 4 + ((lid >> 2) & 3), z = ntz * 4 + (lid >> 4);
+    const long long node = sc.node_base + ((long long)z * sc.gdim[1] + y) * sc.gdim[0] + x;
+    c.g.acc0[par][node] = make_float4(0.f, 0.f, 0.f, 0.f);
+    c.g.acc1[par][node] = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (lid == 0) c.g.tile_flag[tile] = 0u;
+  }
+}
+
+void launch_grid_clear(const Ctx& c, cudaStream_t st, int grid_blocks) {
+  k_grid_clear<<<grid_blocks, 256, 0, st>>>(c);
+}
+
+void launch_grid_update(const Ctx& c, cudaStream_t st, int grid_blocks) {
+  k_grid_update<<<grid_blocks, 256, 0, st>>>(c);
+}
+
+// Fused G2P + F update + return map + P2G of the new state (one particle pass per substep).
+template <bool SCATTER>
+__global__ void __launch_bounds__(kBlock, 2) k_g2p2g(const __grid_constant__ Ctx c) {
+  __shared__ TileSmem sm;
+  Ctrl* ct = c.ctrl;
+  if (ct->done) return;
+  const unsigned k = ct->step_index;
+  const int cur = (k - 1) & 1, nxt = k & 1;
+  if (SCATTER)
+    for (int i = threadIdx.x; i < kChannels * kWinSNodes; i += kBlock) sm.acc[i] = 0.f;
+  if (threadIdx.x == 0) {
+    mbar_init(&sm.mbar, 1);
+    fence_barrier_init();
+    sm.abort_flag = 0;
+  }
+  __syncthreads();
+  unsigned phase = 0;
+  double work_acc = 0.0;
+  const long long cap = c.p.cap;
+  while (true) {
+    if (threadIdx.x == 0) {
+      const unsigned idx = atomicAdd(&ct->work_next, 1u);
+      sm.item = idx < ct->work_count[cur] ? c.s.work[cur][idx] : make_uint4(0xffffffffu, 0, 0, 0);
+    }
+    __syncthreads();
+    const uint4 it = sm.item;
+    if (it.x == 0xffffffffu) break;
+    const int scene = static_cast<int>(it.w);
+    const SceneDev& sc = c.scenes[scene];
+    int tile[3];
+    {
+      const int lt = static_cast<int>(it.x) - sc.tile_base;
+      tile[0] = lt % sc.tiles[0];
+      tile[1] = (lt / sc.tiles[0]) % sc.tiles[1];
+      tile[2] = lt / (sc.tiles[0] * sc.tiles[1]);
+    }
+    // stage the 6^3 velocity window at nodes [4 t, 4 t + 5]
+    if (c.use_tma) {
+      if (threadIdx.x == 0) {
+        fence_proxy_async_smem();
+        mbar_arrive_expect_tx(&sm.mbar, sizeof(sm.vwin));
+        const char* maps = static_cast<const char*>(c.tmaps);
+        tma_load_4d(sm.vwin, maps + 128 * scene, 0, tile[0] * kTile, tile[1] * kTile, tile[2] * kTile, &sm.mbar);
+        if (!mbar_wait_bounded(&sm.mbar, phase)) {
+          atomicOr(&ct->status, 0x8u);
+          mbar_wait_bounded(&sm.mbar, phase);  // give an in-flight copy a second bounded chance
+          sm.abort_flag = 1;
+        }
+      }
+      phase ^= 1u;
+    } else {
+      for (int i = threadIdx.x; i < kWinG * kWinG * kWinG; i += kBlock) {
+        const int x = tile[0] * kTile + i % kWinG, y = tile[1] * kTile + (i / kWinG) % kWinG,
+                  z = tile[2] * kTile + i / (kWinG * kWinG);
+        sm.vwin[i] = c.g.vel[sc.node_base + ((long long)z * sc.gdim[1] + y) * sc.gdim[0] + x];
+      }
+    }
+    __syncthreads();
+    if (sm.abort_flag) return;
+    const float dt = c.dt_scene[scene];
+    const float invH = sc.invH;
+    float wave_acc = 0.f, grad_acc = 0.f;
+    unsigned flags_acc = 0;
+    for (unsigned j0 = 0; j0 < it.z; j0 += kBlock) {
+      const unsigned j = j0 + threadIdx.x;
+      unsigned key = 0xffffffffu;
+      if (j < it.z) {
+        float wave = 0.f, grad = 0.f;
+        unsigned flags = 0;
+        const unsigned home = c.p.perm[it.y + j];
+        unsigned q[3] = {c.p.qx[home], c.p.qy[home], c.p.qz[home]};
+        float D[9];
+#pragma unroll
+        for (int e = 0; e < 9; ++e) D[e] = c.p.D[e * cap + home];
+        const float m = c.p.m[home], V = c.p.V[home];
+        const int mi = c.single_material ? sc.mat_base : c.p.mat[home];
+        const MaterialDev mt = c.mats[mi];
+        const bool pinned = c.has_pinned && c.p.pinned[home];
+        float ep = c.has_plastic ? c.p.ep[home] : 0.f;
+        float T = c.has_thermal ? c.p.T[home] : 0.f;
+        float v[3], C[9];
+        ConstitutiveOut co;
+        if (!pinned) {
+          int b[3];
+          float t[3], w[3][3];
+#pragma unroll
+          for (int a = 0; a < 3; ++a) {
+            stencil_axis(q[a], sc.dims[a], b[a], t[a]);
+            bspline_weights(t[a], w[a]);
+          }
+          const int l0 = b[0] - tile[0] * kTile, l1 = b[1] - tile[1] * kTile, l2 = b[2] - tile[2] * kTile;
+          // the sort key always places the stencil inside the staged window; if it ever does not,
+          // the particle reads the grid from global memory instead (and the step reports it)
+          const bool in_g = l0 >= 0 && l0 <= kWinG - 3 && l1 >= 0 && l1 <= kWinG - 3 && l2 >= 0 && l2 <= kWinG - 3;
+          if (!in_g) flags |= 0x20u;
+          // G2P (src/three/mpm.js:107-118): v = sum w v_i, C = sum w v_i (i - t)^T 4/h
+          float v0 = 0.f, v1 = 0.f, v2 = 0.f;
+          float c0 = 0.f, c1 = 0.f, c2 = 0.f, c3 = 0.f, c4 = 0.f, c5 = 0.f, c6 = 0.f, c7 = 0.f, c8 = 0.f;
+#pragma unroll
+          for (int kz = 0; kz < 3; ++kz) {
+            const float dz = static_cast<float>(kz) - t[2];
+#pragma unroll
+            for (int ky = 0; ky < 3; ++ky) {
+              const float dy = static_cast<float>(ky) - t[1];
+              const float wyz = w[1][ky] * w[2][kz];
+#pragma unroll
+              for (int kx = 0; kx < 3; ++kx) {
+                const float dx = static_cast<float>(kx) - t[0];
+                const float wt = w[0][kx] * wyz;
+                const float4 g =
+                    in_g ? sm.vwin[((l2 + kz) * kWinG + (l1 + ky)) * kWinG + (l0 + kx)]
+                         : c.g.vel[sc.node_base + ((long long)(b[2] + kz) * sc.gdim[1] + (b[1] + ky)) * sc.gdim[0] +
+                                   (b[0] + kx)];
+                const float a = wt * g.x, bb = wt * g.y, cc = wt * g.z;
+                v0 += a; v1 += bb; v2 += cc;
+                c0 += a * dx; c1 += a * dy; c2 += a * dz;
+                c3 += bb * dx; c4 += bb * dy; c5 += bb * dz;
+                c6 += cc * dx; c7 += cc * dy; c8 += cc * dz;
+              }
+            }
+          }
+          const float s4 = 4.f * invH;
+          v[0] = v0; v[1] = v1; v[2] = v2;
+          C[0] = c0 * s4; C[1] = c1 * s4; C[2] = c2 * s4;
+          C[3] = c3 * s4; C[4] = c4 * s4; C[5] = c5 * s4;
+          C[6] = c6 * s4; C[7] = c7 * s4; C[8] = c8 * s4;
+          // F <- (I + dt C) F in centred form: D <- D + dt C (I + D) (src/three/mpm.js:119-121)
+          float Dn[9];
+#pragma unroll
+          for (int a = 0; a < 3; ++a)
+#pragma unroll
+            for (int bcol = 0; bcol < 3; ++bcol)
+              Dn[a * 3 + bcol] = D[a * 3 + bcol] +
+                                 dt * (C[a * 3 + bcol] + C[a * 3 + 0] * D[0 * 3 + bcol] +
+                                       C[a * 3 + 1] * D[1 * 3 + bcol] + C[a * 3 + 2] * D[2 * 3 + bcol]);
+#pragma unroll
+          for (int e = 0; e < 9; ++e) D[e] = Dn[e];
+          // x += dt v (src/three/mpm.js:122), in fixed point, clamped into the box
+          const float s = dt * invH * kFixedOne;
+#pragma unroll
+          for (int a = 0; a < 3; ++a) {
+            long long qn = static_cast<long long>(q[a]) + __float2ll_rn(s * v[a]);
+            if (sc.clamp) {
+              qn = qn < (long long)sc.qlo[a] ? (long long)sc.qlo[a] : qn;
+              qn = qn > (long long)sc.qhi[a] ? (long long)sc.qhi[a] : qn;
+            } else {
+              const long long hi = (static_cast<long long>(sc.dims[a]) - 1) << kFracBits;
+              if (qn < 0 || qn > hi) flags |= 0x4u;
+              qn = qn < 0 ? 0 : (qn > hi ? hi : qn);
+            }
+            q[a] = static_cast<unsigned>(qn);
+          }
+          // return map / stress for the next P2G (src/three/mpm.js:126-131)
+          co = constitutive_update(mt, D, ep, T, V / m, true);
+          ep += co.dep;
+          T += co.dT;
+          c.p.qx[home] = q[0]; c.p.qy[home] = q[1]; c.p.qz[home] = q[2];
+          c.p.vx[home] = v[0]; c.p.vy[home] = v[1]; c.p.vz[home] = v[2];
+#pragma unroll
+          for (int e = 0; e < 9; ++e) {
+            c.p.C[e * cap + home] = C[e];
+            c.p.D[e * cap + home] = D[e];
+          }
+          if (c.has_plastic) c.p.ep[home] = ep;
+          if (c.has_thermal) c.p.T[home] = T;
+          if (co.dep > 0.f && mt.heat_per_work > 0.f) work_acc += static_cast<double>(co.dT) * m / mt.heat_per_work;
+        } else {
+          // pinned particles keep their state (src/three/mpm.js:108) but still scatter
+          v[0] = c.p.vx[home]; v[1] = c.p.vy[home]; v[2] = c.p.vz[home];
+#pragma unroll
+          for (int e = 0; e < 9; ++e) C[e] = c.p.C[e * cap + home];
+          float Dc[9];
+#pragma unroll
+          for (int e = 0; e < 9; ++e) Dc[e] = D[e];
+          co = constitutive_update(mt, Dc, ep, T, V / m, false);
+        }
+        if (SCATTER) scatter_particle(c, sc, sm, nxt, tile, q, m, V, v, C, co.tau, pinned, key);
+        if (SCATTER) c.p.key[home] = key;
+        cfl_terms(mt, D, v, C, m, V, co.Jm1, wave, grad);
+        flags |= state_flags(v, D, co.tau, co.Jm1);
+        flags_acc |= flags;
+        wave_acc = fmaxf(wave_acc, wave);
+        grad_acc = fmaxf(grad_acc, grad);
+      }
+      if (SCATTER) count_key(c, key);
+    }
+    block_reduce_item(c, scene, wave_acc, grad_acc, flags_acc, sm.red);
+    __syncthreads();
+    if (SCATTER) flush_window(c, sc, sm, nxt, tile);
+    __syncthreads();
+  }
+  // heat from plastic work: one FP64 atomic per CTA
+  double wsum = warp_sum_d(work_acc);
+  if ((threadIdx.x & 31) == 0) sm.work[threadIdx.x >> 5] = wsum;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < kBlock / 32; ++w) t += sm.work[w];
+    if (t != 0.0) atomicAdd(&ct->plastic_work, t);
+  }
+}
+
+void launch_p2g(const Ctx& c, cudaStream_t st, int grid_blocks) { k_p2g<<<grid_blocks, kBlock, 0, st>>>(c); }
+
+void launch_g2p2g(const Ctx& c, cudaStream_t st, int grid_blocks, bool scatter) {
+  if (scatter)
+    k_g2p2g<true><<<grid_blocks, kBlock, 0, st>>>(c);
+  else
+    k_g2p2g<false><<<grid_blocks, kBlock, 0, st>>>(c);
+}
+
+int g2p2g_blocks_per_sm(bool scatter) {
+  int n = 0;
+  if (scatter)
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_g2p2g<true>, kBlock, 0);
+  else
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_g2p2g<false>, kBlock, 0);
+  return n > 0 ? n : 1;
+}
+
+int p2g_blocks_per_sm() {
+  int n = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_p2g, kBlock, 0);
+  return n > 0 ? n : 1;
+}
+
+// ---------------------------------------------------------------------------------------------
+// FP64 ledger (src/simulation/mechanical-diagnostics.js:16-37, src/simulation/particle-health.js)
+
+constexpr int kLedgerSums = 13;   // mass kin aff pot ela mom3 ang3
+constexpr int kLedgerFields = 19; // + minJ maxJ maxEp maxVm nonfinite invalidJ
+
+__device__ __forceinline__ double warp_sum(double x) {
+  for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+  return x;
+}
+
+__global__ void __launch_bounds__(256) k_ledger(Ctx c, double* partials) {
+  __shared__ double sh[8][kLedgerFields];
+  double acc[kLedgerFields];
+#pragma unroll
+  for (int k = 0; k < kLedgerSums; ++k) acc[k] = 0.0;
+  acc[13] = 1e300; acc[14] = -1e300; acc[15] = 0.0; acc[16] = 0.0; acc[17] = 0.0; acc[18] = 0.0;
+  const long long cap = c.p.cap;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < c.n; i += (long long)gridDim.x * blockDim.x) {
+    const int s = c.nscenes == 1 ? 0 : find_scene_by_particle(c.scenes, c.nscenes, i);
+    const SceneDev& sc = c.scenes[s];
+    const double Hs = sc.H;
+    const double x[3] = {sc.origin[0] + c.p.qx[i] * (Hs / 4194304.0), sc.origin[1] + c.p.qy[i] * (Hs / 4194304.0),
+                         sc.origin[2] + c.p.qz[i] * (Hs / 4194304.0)};
+    const double v[3] = {c.p.vx[i], c.p.vy[i], c.p.vz[i]};
+    float D[9], C[9];
+#pragma unroll
+    for (int e = 0; e < 9; ++e) {
+      D[e] = c.p.D[e * cap + i];
+      C[e] = c.p.C[e * cap + i];
+    }
+    const double m = c.p.m[i], V = c.p.V[i];
+    const int mi = c.single_material ? sc.mat_base : c.p.mat[i];
+    const MaterialDev mt = c.mats[mi];
+    const double Dap = Hs * Hs / 4.0;
+    acc[0] += m;
+    acc[1] += 0.5 * m * (v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+    double c2 = 0.0;
+#pragma unroll
+    for (int e = 0; e < 9; ++e) c2 += (double)C[e] * C[e];
+    acc[2] += 0.5 * m * Dap * c2;
+    acc[3] -= m * (sc.gravity[0] * x[0] + sc.gravity[1] * x[1] + sc.gravity[2] * x[2]);
+    const double P[3] = {m * v[0], m * v[1], m * v[2]};
+    const double spin[3] = {(double)C[7] - C[5], (double)C[2] - C[6], (double)C[3] - C[1]};
+    acc[5] += P[0]; acc[6] += P[1]; acc[7] += P[2];
+    acc[8] += x[1] * P[2] - x[2] * P[1] + m * Dap * spin[0];
+    acc[9] += x[2] * P[0] - x[0] * P[2] + m * Dap * spin[1];
+    acc[10] += x[0] * P[1] - x[1] * P[0] + m * Dap * spin[2];
+    // elastic energy density per reference volume by model
+    const float Jm1 = det_minus_one(D);
+    const double J = 1.0 + (double)Jm1;
+    float Dc[9];
+#pragma unroll
+    for (int e = 0; e < 9; ++e) Dc[e] = D[e];
+    const ConstitutiveOut co = constitutive_update(mt, Dc, 0.f, c.has_thermal ? c.p.T[i] : 0.f, (float)(V / m), false);
+    double W = 0.0;
+    if (J > 0.0) {
+      const Sym3 B = cauchy_green_minus_identity(D);
+      if (mt.model == 1) {
+        const double lj = log1p((double)Jm1);
+        W = 0.5 * mt.mu * ((double)B.xx + B.yy + B.zz) - mt.mu * lj + 0.5 * mt.lam * lj * lj;
+      } else {
+        float beta[3], U[9];
+        sym_eig3(B, beta, U);
+        if (mt.model == 0) {
+          double s2 = 0.0;
+          for (int kk = 0; kk < 3; ++kk) {
+            const double sm1 = beta[kk] / (1.0 + sqrt(fmax(1.0 + beta[kk], 0.0)));
+            s2 += sm1 * sm1;
+          }
+          W = mt.mu * s2 + 0.5 * mt.lam * (double)Jm1 * Jm1;
+        } else {
+          double e2 = 0.0, tr = 0.0;
+          for (int kk = 0; kk < 3; ++kk) {
+            const double e = fmax(0.5 * log1p((double)beta[kk]), -13.815510558);
+            e2 += e * e;
+            tr += e;
+          }
+          W = mt.mu * e2 + 0.5 * mt.lam * tr * tr;
+        }
+      }
+    }
+    acc[4] += V * W;
+    const double tvm = 0.5 * ((double)(co.tau.xx - co.tau.yy) * (co.tau.xx - co.tau.yy) +
+                              (double)(co.tau.yy - co.tau.zz) * (co.tau.yy - co.tau.zz) +
+                              (double)(co.tau.zz - co.tau.xx) * (co.tau.zz - co.tau.xx)) +
+                       3.0 * ((double)co.tau.xy * co.tau.xy + (double)co.tau.xz * co.tau.xz + (double)co.tau.yz * co.tau.yz);
+    const double vm = sqrt(fmax(0.0, tvm)) / fmax(1e-6, J);
+    bool finite = isfinite(m) && isfinite(v[0] + v[1] + v[2]) && isfinite(J) && isfinite(c2);
+#pragma unroll
+    for (int e = 0; e < 9; ++e) finite = finite && isfinite(D[e]);
+    if (isfinite(J)) {
+      acc[13] = fmin(acc[13], J);
+      acc[14] = fmax(acc[14], J);
+      if (J <= 0.0) acc[18] += 1.0;
+    }
+    if (c.has_plastic) acc[15] = fmax(acc[15], (double)c.p.ep[i]);
+    if (isfinite(vm)) acc[16] = fmax(acc[16], vm);
+    if (!finite) acc[17] += 1.0;
+  }
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+  for (int k = 0; k < kLedgerSums; ++k) acc[k] = warp_sum(acc[k]);
+  for (int o = 16; o > 0; o >>= 1) {
+    acc[13] = fmin(acc[13], __shfl_xor_sync(0xffffffffu, acc[13], o));
+    acc[14] = fmax(acc[14], __shfl_xor_sync(0xffffffffu, acc[14], o));
+    acc[15] = fmax(acc[15], __shfl_xor_sync(0xffffffffu, acc[15], o));
+    acc[16] = fmax(acc[16], __shfl_xor_sync(0xffffffffu, acc[16], o));
+  }
+  acc[17] = warp_sum(acc[17]);
+  acc[18] = warp_sum(acc[18]);
+  if (lane == 0)
+    for (int k = 0; k < kLedgerFields; ++k) sh[wid][k] = acc[k];
+  __syncthreads();
+  if (threadIdx.x < kLedgerFields) {
+    const int k = threadIdx.x;
+    double r = sh[0][k];
+    for (int w = 1; w < 8; ++w) {
+      const double y = sh[w][k];
+      if (k == 13) r = fmin(r, y);
+      else if (k >= 14 && k <= 16) r = fmax(r, y);
+      else r += y;
+    }
+    partials[blockIdx.x * kLedgerFields + k] = r;
+  }
+}
+
+// Deterministic final reduction of the per-block partials (fixed order).
+__global__ void k_ledger_final(const double* partials, int blocks, double* out) {
+  const int k = threadIdx.x;
+  if (k >= kLedgerFields) return;
+  double r = (k == 13) ? 1e300 : (k >= 14 && k <= 16) ? -1e300 : 0.0;
+  if (k == 15 || k == 16) r = 0.0;
+  for (int b = 0; b < blocks; ++b) {
+    const double y = partials[b * kLedgerFields + k];
+    if (k == 13) r = fmin(r, y);
+    else if (k >= 14 && k <= 16) r = fmax(r, y);
+    else r += y;
+  }
+  out[k] = r;
+}
+
+void launch_ledger(const Ctx& c, cudaStream_t st, double* partials, int blocks, double* out) {
+  k_ledger<<<blocks, 256, 0, st>>>(c, partials);
+  k_ledger_final<<<1, 32, 0, st>>>(partials, blocks, out);
+}
+
+// Grid after P2G of one scene in the reference's node order: mass and p + dt (f + m g).
+__global__ void k_grid_debug(Ctx c, int scene, float dt, double* mass, double* mom) {
+  const SceneDev& sc = c.scenes[scene];
+  const int nx = sc.dims[0], ny = sc.dims[1], nz = sc.dims[2];
+  const long long total = (long long)nx * ny * nz;
+  const int par = c.ctrl->step_index & 1;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x) {
+    const int x = static_cast<int>(i % nx), y = static_cast<int>((i / nx) % ny), z = static_cast<int>(i / ((long long)nx * ny));
+    const long long node = sc.node_base + ((long long)z * sc.gdim[1] + y) * sc.gdim[0] + x;
+    const float4 a0 = c.g.acc0[par][node], a1 = c.g.acc1[par][node];
+    mass[i] = a0.x;
+    mom[i * 3 + 0] = (double)a0.y + (double)dt * ((double)a1.x + (double)a0.x * sc.gravity[0]);
+    mom[i * 3 + 1] = (double)a0.z + (double)dt * ((double)a1.y + (double)a0.x * sc.gravity[1]);
+    mom[i * 3 + 2] = (double)a0.w + (double)dt * ((double)a1.z + (double)a0.x * sc.gravity[2]);
+  }
+}
+
+void launch_grid_debug(const Ctx& c, cudaStream_t st, int scene, float dt, double* mass, double* mom) {
+  k_grid_debug<<<1024, 256, 0, st>>>(c, scene, dt, mass, mom);
+}
+
+// ---------------------------------------------------------------------------------------------
+// host <-> device conversion (staging buffers hold the caller's f64 or f32 arrays)
+
+template <typename Tsrc>
+__global__ void k_upload(Ctx c, long long n, const Tsrc* const* src, const int* material,
+                         const unsigned char* pinned, unsigned fields) {
+  const long long cap = c.p.cap;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const int s = c.nscenes == 1 ? 0 : find_scene_by_particle(c.scenes, c.nscenes, i);
+    const SceneDev& sc = c.scenes[s];
+    if (fields & kFieldPos) {
+      unsigned* qs[3] = {c.p.qx, c.p.qy, c.p.qz};
+      for (int a = 0; a < 3; ++a) {
+        const double q = rint(((double)src[a][i] - sc.origin[a]) / (double)sc.H * 4194304.0);
+        const double hi = (double)(((long long)sc.dims[a] - 1) << kFracBits);
+        qs[a][i] = static_cast<unsigned>(fmin(fmax(q, 0.0), hi));
+      }
+    }
+    if (fields & kFieldVel) {
+      c.p.vx[i] = src[3] ? (float)src[3][i] : 0.f;
+      c.p.vy[i] = src[4] ? (float)src[4][i] : 0.f;
+      c.p.vz[i] = src[5] ? (float)src[5][i] : 0.f;
+    }
+    if (fields & kFieldMass) c.p.m[i] = (float)src[6][i];
+    if (fields & kFieldVolume) c.p.V[i] = (float)src[7][i];
+    if (fields & kFieldTemp) c.p.T[i] = src[8] ? (float)src[8][i] : 0.f;
+    if (fields & kFieldPlastic) c.p.ep[i] = src[9] ? (float)src[9][i] : 0.f;
+    if (fields & kFieldF)
+      for (int e = 0; e < 9; ++e)
+        c.p.D[e * cap + i] = src[10] ? (float)((double)src[10][i * 9 + e] - ((e % 4 == 0) ? 1.0 : 0.0)) : 0.f;
+    if (fields & kFieldC)
+      for (int e = 0; e < 9; ++e) c.p.C[e * cap + i] = src[11] ? (float)src[11][i * 9 + e] : 0.f;
+    if (fields & kFieldMass) {
+      c.p.mat[i] = material ? static_cast<unsigned short>(sc.mat_base + material[i])
+                            : static_cast<unsigned short>(sc.mat_base);
+      if (c.p.pinned) c.p.pinned[i] = pinned ? pinned[i] : 0;
+    }
+  }
+}
+
+void launch_upload_convert(const Ctx& c, cudaStream_t st, long long n, int dtype, const void* const* src,
+                           const int* material, const unsigned char* pinned, unsigned fields) {
+  if (n <= 0) return;
+  const int blocks = static_cast<int>((n + 255) / 256 < 65536 ? (n + 255) / 256 : 65536);
+  if (dtype == 0)
+    k_upload<double><<<blocks, 256, 0, st>>>(c, n, reinterpret_cast<const double* const*>(src), material, pinned, fields);
+  else
+    k_upload<float><<<blocks, 256, 0, st>>>(c, n, reinterpret_cast<const float* const*>(src), material, pinned, fields);
+}
+
+template <typename Tdst>
+__global__ void k_download(Ctx c, long long n, Tdst* const* dst, unsigned fields) {
+  const long long cap = c.p.cap;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const int s = c.nscenes == 1 ? 0 : find_scene_by_particle(c.scenes, c.nscenes, i);
+    const SceneDev& sc = c.scenes[s];
+    if (fields & kFieldPos) {
+      const unsigned q[3] = {c.p.qx[i], c.p.qy[i], c.p.qz[i]};
+      for (int a = 0; a < 3; ++a) dst[a][i] = (Tdst)(sc.origin[a] + (double)q[a] * ((double)sc.H / 4194304.0));
+    }
+    if (fields & kFieldVel) {
+      dst[3][i] = (Tdst)c.p.vx[i];
+      dst[4][i] = (Tdst)c.p.vy[i];
+      dst[5][i] = (Tdst)c.p.vz[i];
+    }
+    if (fields & kFieldMass) dst[6][i] = (Tdst)c.p.m[i];
+    if (fields & kFieldVolume) dst[7][i] = (Tdst)c.p.V[i];
+    if (fields & kFieldTemp) dst[8][i] = (Tdst)c.p.T[i];
+    if (fields & kFieldPlastic) dst[9][i] = (Tdst)c.p.ep[i];
+    for (int e = 0; e < 9; ++e) {
+      const double ident = (e % 4 == 0) ? 1.0 : 0.0;
+      if (fields & kFieldF) dst[10][i * 9 + e] = (Tdst)((double)c.p.D[e * cap + i] + ident);
+      if (fields & kFieldC) dst[11][i * 9 + e] = (Tdst)c.p.C[e * cap + i];
+    }
+  }
+}
+
+void launch_download_convert(const Ctx& c, cudaStream_t st, long long n, int dtype, void* const* dst, unsigned fields) {
+  if (n <= 0) return;
+  const int blocks = static_cast<int>((n + 255) / 256 < 65536 ? (n + 255) / 256 : 65536);
+  if (dtype == 0)
+    k_download<double><<<blocks, 256, 0, st>>>(c, n, reinterpret_cast<double* const*>(dst), fields);
+  else
+    k_download<float><<<blocks, 256, 0, st>>>(c, n, reinterpret_cast<float* const*>(dst), fields);
+}
+
+// ---------------------------------------------------------------------------------------------
+// stateless constitutive batch: projectPlastic + stress (src/three/constitutive.js:52-86)
+
+__global__ void k_return_map(MaterialDev mt, long long n, const double* F_in, const double* ep, const double* T,
+                             double* F_out, double* dep, double* tau) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    float D[9];
+    for (int e = 0; e < 9; ++e) D[e] = (float)(F_in[i * 9 + e] - ((e % 4 == 0) ? 1.0 : 0.0));
+    const float epi = ep ? (float)ep[i] : 0.f, Ti = T ? (float)T[i] : 0.f;
+    const ConstitutiveOut co = constitutive_update(mt, D, epi, Ti, 1.f, true);
+    for (int e = 0; e < 9; ++e) F_out[i * 9 + e] = (double)D[e] + ((e % 4 == 0) ? 1.0 : 0.0);
+    dep[i] = co.dep;
+    const float t9[9] = {co.tau.xx, co.tau.xy, co.tau.xz, co.tau.xy, co.tau.yy, co.tau.yz, co.tau.xz, co.tau.yz, co.tau.zz};
+    for (int e = 0; e < 9; ++e) tau[i * 9 + e] = t9[e];
+  }
+}
+
+void launch_return_map_batch(const MaterialDev& m, long long n, const double* F_in, const double* ep, const double* T,
+                             float dt, double* F_out, double* dep, double* tau, cudaStream_t st) {
+  (void)dt;
+  const int blocks = static_cast<int>((n + 255) / 256 < 4096 ? (n + 255) / 256 : 4096);
+  if (blocks > 0) k_return_map<<<blocks, 256, 0, st>>>(m, n, F_in, ep, T, F_out, dep, tau);
+}
+
+}  // namespace mpm

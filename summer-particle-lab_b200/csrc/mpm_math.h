@@ -1,0 +1,239 @@
+// Constitutive and transfer math of the MLS-MPM solid step, FP32, for device and host.
+//
+// Centred form. Deformation gradients are held as D = F - I, so small elastic strains keep full
+// FP32 precision (F ~ 1 + 1e-3 would keep only 4 significant digits of the strain). The left
+// Cauchy-Green tensor is formed as B - I = D + D^T + D D^T, its eigenvalues beta_k = sigma_k^2 - 1
+// are found by cyclic Jacobi rotations, and strains use log1p/expm1.
+//
+// The eigen-decomposition of F F^T replaces the reference's SVD of F (src/three/constitutive.js:
+// 22-42) and Newton polar iteration (src/three/math.js:16-24): with F = U S V^T the left singular
+// vectors U are the eigenvectors of F F^T and
+//   fixed-corotated  (F - R) F^T = (V_l - I) V_l = U diag((s-1) s) U^T      (math.js:25-32)
+//   Hencky           tau = U diag(2 mu e + lambda tr e) U^T, e = log s      (constitutive.js:101-104)
+//   return map       F' = U diag(s'/s) U^T F                                 (constitutive.js:77)
+// so V is never needed.
+#pragma once
+#include <math.h>
+
+#if defined(__CUDACC__)
+#define MPM_HD __host__ __device__ __forceinline__
+#else
+#define MPM_HD inline
+#endif
+
+namespace mpm {
+
+struct Sym3 {
+  float xx, yy, zz, xy, xz, yz;
+};
+
+MPM_HD float rsqrt_hd(float x) {
+#if defined(__CUDA_ARCH__)
+  return rsqrtf(x);
+#else
+  return 1.0f / sqrtf(x);
+#endif
+}
+
+// Quadratic B-spline weights for fraction t in [0.5, 1.5) (src/three/mpm.js:28-30)
+MPM_HD void bspline_weights(float t, float w[3]) {
+  const float a = 1.5f - t, b = t - 1.0f, c = t - 0.5f;
+  w[0] = 0.5f * a * a;
+  w[1] = 0.75f - b * b;
+  w[2] = 0.5f * c * c;
+}
+
+// B - I = D + D^T + D D^T
+MPM_HD Sym3 cauchy_green_minus_identity(const float D[9]) {
+  Sym3 b;
+  b.xx = 2.f * D[0] + (D[0] * D[0] + D[1] * D[1] + D[2] * D[2]);
+  b.yy = 2.f * D[4] + (D[3] * D[3] + D[4] * D[4] + D[5] * D[5]);
+  b.zz = 2.f * D[8] + (D[6] * D[6] + D[7] * D[7] + D[8] * D[8]);
+  b.xy = D[1] + D[3] + (D[0] * D[3] + D[1] * D[4] + D[2] * D[5]);
+  b.xz = D[2] + D[6] + (D[0] * D[6] + D[1] * D[7] + D[2] * D[8]);
+  b.yz = D[5] + D[7] + (D[3] * D[6] + D[4] * D[7] + D[5] * D[8]);
+  return b;
+}
+
+// det(I + D) - 1 = tr D + (sum of principal 2x2 minors of D) + det D
+MPM_HD float det_minus_one(const float D[9]) {
+  const float tr = D[0] + D[4] + D[8];
+  const float m2 = (D[0] * D[4] - D[1] * D[3]) + (D[0] * D[8] - D[2] * D[6]) + (D[4] * D[8] - D[5] * D[7]);
+  const float d3 = D[0] * (D[4] * D[8] - D[5] * D[7]) - D[1] * (D[3] * D[8] - D[5] * D[6]) +
+                   D[2] * (D[3] * D[7] - D[4] * D[6]);
+  return tr + m2 + d3;
+}
+
+// One Jacobi rotation annihilating a_pq (Golub & Van Loan, symmetric Schur 2x2):
+// theta = (a_qq - a_pp) / (2 a_pq), t = sgn(theta)/(|theta| + sqrt(theta^2 + 1)),
+// c = 1/sqrt(1 + t^2), s = t c. r is the third index. U columns p, q rotate with it.
+MPM_HD void jacobi_rotate(float& app, float& aqq, float& apq, float& arp, float& arq, float& u0p,
+                          float& u0q, float& u1p, float& u1q, float& u2p, float& u2q) {
+  if (apq == 0.f) return;
+  const float theta = (aqq - app) / (2.f * apq);
+  const float t = copysignf(1.f, theta) / (fabsf(theta) + sqrtf(fmaf(theta, theta, 1.f)));
+  const float c = rsqrt_hd(fmaf(t, t, 1.f));
+  const float s = t * c;
+  app = fmaf(-t, apq, app);
+  aqq = fmaf(t, apq, aqq);
+  apq = 0.f;
+  const float rp = arp, rq = arq;
+  arp = c * rp - s * rq;
+  arq = s * rp + c * rq;
+  float x, y;
+  x = u0p; y = u0q; u0p = c * x - s * y; u0q = s * x + c * y;
+  x = u1p; y = u1q; u1p = c * x - s * y; u1q = s * x + c * y;
+  x = u2p; y = u2q; u2p = c * x - s * y; u2q = s * x + c * y;
+}
+
+// Cyclic Jacobi eigen-decomposition of a symmetric 3x3 matrix: a = U diag(lam) U^T, U row-major
+// with eigenvectors in columns. Stops when the off-diagonal mass is below 2^-24 of the diagonal.
+MPM_HD void sym_eig3(Sym3 a, float lam[3], float U[9]) {
+  float u00 = 1.f, u01 = 0.f, u02 = 0.f, u10 = 0.f, u11 = 1.f, u12 = 0.f, u20 = 0.f, u21 = 0.f,
+        u22 = 1.f;
+  for (int sweep = 0; sweep < 6; ++sweep) {
+    const float off = fabsf(a.xy) + fabsf(a.xz) + fabsf(a.yz);
+    const float dia = fabsf(a.xx) + fabsf(a.yy) + fabsf(a.zz);
+    if (!(off > 5.9604645e-8f * dia) && sweep > 0) break;
+    if (off == 0.f) break;
+    jacobi_rotate(a.xx, a.yy, a.xy, a.xz, a.yz, u00, u01, u10, u11, u20, u21);  // (0,1), r=2
+    jacobi_rotate(a.xx, a.zz, a.xz, a.xy, a.yz, u00, u02, u10, u12, u20, u22);  // (0,2), r=1
+    jacobi_rotate(a.yy, a.zz, a.yz, a.xy, a.xz, u01, u02, u11, u12, u21, u22);  // (1,2), r=0
+  }
+  lam[0] = a.xx; lam[1] = a.yy; lam[2] = a.zz;
+  U[0] = u00; U[1] = u01; U[2] = u02;
+  U[3] = u10; U[4] = u11; U[5] = u12;
+  U[6] = u20; U[7] = u21; U[8] = u22;
+}
+
+// S = U diag(d) U^T (symmetric)
+MPM_HD Sym3 rotate_diag(const float U[9], const float d[3]) {
+  Sym3 s;
+  s.xx = U[0] * U[0] * d[0] + U[1] * U[1] * d[1] + U[2] * U[2] * d[2];
+  s.yy = U[3] * U[3] * d[0] + U[4] * U[4] * d[1] + U[5] * U[5] * d[2];
+  s.zz = U[6] * U[6] * d[0] + U[7] * U[7] * d[1] + U[8] * U[8] * d[2];
+  s.xy = U[0] * U[3] * d[0] + U[1] * U[4] * d[1] + U[2] * U[5] * d[2];
+  s.xz = U[0] * U[6] * d[0] + U[1] * U[7] * d[1] + U[2] * U[8] * d[2];
+  s.yz = U[3] * U[6] * d[0] + U[4] * U[7] * d[1] + U[5] * U[8] * d[2];
+  return s;
+}
+
+// Per-material constants on the device (SI). See mpm_material in include/mpm_b200.h.
+struct MaterialDev {
+  int model;
+  float mu, lam;
+  float yield_stress, hardening;
+  float T_ref, inv_T_span, hot_ratio;
+  float heat_per_work;   // heat_fraction / specific_heat (K per J/kg)
+  float wave_modulus;    // lambda + 2 mu (CFL wave speed c = sqrt(wave_modulus V / m))
+};
+
+struct ConstitutiveOut {
+  Sym3 tau;       // Kirchhoff stress for the next P2G
+  float dep;      // plastic strain increment
+  float dT;       // temperature increment from plastic work
+  float Jm1;      // det F - 1 after the return
+};
+
+// Hencky strains e_k = log(max(s_k, 1e-6)) from beta_k = s_k^2 - 1 (constitutive.js:58,
+// metal-plasticity.js:21)
+MPM_HD float hencky_strain(float beta) {
+  return fmaxf(0.5f * log1pf(beta), -13.815510558f);
+}
+
+// Constitutive update of one particle after the F update, in place on D (= F - I):
+// models 4/5/10 run the J2 radial return (src/three/metal-plasticity.js:20-27,
+// src/three/thermal-plasticity.js:22-29) and give the Hencky stress of the returned state
+// (src/three/constitutive.js:81-86); models 0 and 1 give the elastic stress of F
+// (src/three/math.js:25-32, src/three/constitutive.js:94-100).
+// ep is the accumulated plastic strain, T the temperature; rho0 = m / V for the heat term.
+// With do_return false the J2 models give the stress of F without a return (the reference's
+// updateStress when no cached stress exists, src/three/mpm.js:36).
+MPM_HD ConstitutiveOut constitutive_update(const MaterialDev& mt, float D[9], float ep, float T,
+                                           float inv_rho0, bool do_return) {
+  ConstitutiveOut out;
+  out.dep = 0.f;
+  out.dT = 0.f;
+  const Sym3 B = cauchy_green_minus_identity(D);
+  if (mt.model == 1) {  // Neo-Hookean: mu (F F^T - I) + lambda log J I
+    const float Jm1 = det_minus_one(D);
+    const float J = 1.f + Jm1;
+    const float lj = J > 1e-6f ? log1pf(Jm1) : -13.815510558f;
+    out.tau.xx = mt.mu * B.xx + mt.lam * lj;
+    out.tau.yy = mt.mu * B.yy + mt.lam * lj;
+    out.tau.zz = mt.mu * B.zz + mt.lam * lj;
+    out.tau.xy = mt.mu * B.xy;
+    out.tau.xz = mt.mu * B.xz;
+    out.tau.yz = mt.mu * B.yz;
+    out.Jm1 = Jm1;
+    return out;
+  }
+  float beta[3], U[9];
+  sym_eig3(B, beta, U);
+  if (mt.model == 0) {  // fixed-corotated: U diag(2 mu (s-1) s) U^T + lambda (J-1) J I
+    float d[3];
+    for (int k = 0; k < 3; ++k) {
+      const float sm1 = beta[k] / (1.f + sqrtf(fmaxf(1.f + beta[k], 0.f)));  // s - 1
+      d[k] = 2.f * mt.mu * (beta[k] - sm1);                                  // (s - 1) s = beta - (s - 1)
+    }
+    const float Jm1 = det_minus_one(D);
+    const float vol = mt.lam * Jm1 * (1.f + Jm1);
+    out.tau = rotate_diag(U, d);
+    out.tau.xx += vol;
+    out.tau.yy += vol;
+    out.tau.zz += vol;
+    out.Jm1 = Jm1;
+    return out;
+  }
+  // J2 family on Hencky strains
+  float e[3];
+  for (int k = 0; k < 3; ++k) e[k] = hencky_strain(beta[k]);
+  const float tr = e[0] + e[1] + e[2];
+  const float tr3 = tr * (1.f / 3.f);
+  float dev[3];
+  for (int k = 0; k < 3; ++k) dev[k] = e[k] - tr3;
+  const float len = sqrtf(dev[0] * dev[0] + dev[1] * dev[1] + dev[2] * dev[2]);
+  const float J = fmaxf(1e-6f, expf(tr));
+  const float q = 2.449489742783178f * mt.mu * len / J;
+  float soft = 1.f;
+  if (mt.model == 10) {
+    const float theta = fminf(1.f, fmaxf(0.f, (T - mt.T_ref) * mt.inv_T_span));
+    soft = 1.f - (1.f - mt.hot_ratio) * theta;
+  }
+  const float yield = (mt.yield_stress + (mt.model == 4 ? 0.f : mt.hardening * ep)) * soft;
+  float dep = 0.f;
+  if (do_return && q > yield) {
+    const float hard = mt.model == 4 ? 0.f : mt.hardening * soft;
+    dep = (q - yield) / (3.f * mt.mu / J + hard);
+  }
+  float scale = 1.f;
+  if (dep > 0.f) {
+    scale = fmaxf(0.f, 1.f - 1.224744871391589f * dep / fmaxf(len, 1e-20f));
+    // D' = M + M D + D with M = U diag(expm1((scale - 1) dev_k)) U^T
+    float r[3];
+    for (int k = 0; k < 3; ++k) r[k] = expm1f((scale - 1.f) * dev[k]);
+    const Sym3 M = rotate_diag(U, r);
+    float Dn[9];
+    const float m00 = M.xx, m01 = M.xy, m02 = M.xz, m11 = M.yy, m12 = M.yz, m22 = M.zz;
+    for (int b = 0; b < 3; ++b) {
+      Dn[0 * 3 + b] = m00 * D[0 * 3 + b] + m01 * D[1 * 3 + b] + m02 * D[2 * 3 + b];
+      Dn[1 * 3 + b] = m01 * D[0 * 3 + b] + m11 * D[1 * 3 + b] + m12 * D[2 * 3 + b];
+      Dn[2 * 3 + b] = m02 * D[0 * 3 + b] + m12 * D[1 * 3 + b] + m22 * D[2 * 3 + b];
+    }
+    Dn[0] += m00; Dn[1] += m01; Dn[2] += m02;
+    Dn[3] += m01; Dn[4] += m11; Dn[5] += m12;
+    Dn[6] += m02; Dn[7] += m12; Dn[8] += m22;
+    for (int k = 0; k < 9; ++k) D[k] += Dn[k];
+    // plastic work heating (gpu/mixed_material.py:150-172): dT = beta * tau_eq * dep / (rho0 cp)
+    // with tau_eq = sqrt(6) mu |dev e_returned| the returned Kirchhoff von Mises stress
+    out.dT = mt.heat_per_work * 2.449489742783178f * mt.mu * scale * len * dep * inv_rho0;
+  }
+  float d[3];
+  for (int k = 0; k < 3; ++k) d[k] = 2.f * mt.mu * (tr3 + scale * dev[k]) + mt.lam * tr;
+  out.tau = rotate_diag(U, d);
+  out.dep = dep;
+  out.Jm1 = expm1f(tr);
+  return out;
+}
+
+}  // namespace mpm

@@ -1,0 +1,119 @@
+"""ctypes binding of libmpm_b200.so (the C ABI declared in include/mpm_b200.h).
+
+The library is built in-tree by summer-particle-lab_b200/build_lib.py. There is no CPU fallback:
+if the shared object is missing or cannot be loaded, every entry point raises.
+"""
+import ctypes
+import os
+
+PKG = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB_PATH = os.path.join(PKG, "lib", "libmpm_b200.so")
+
+_D = ctypes.c_double
+_I32 = ctypes.c_int32
+_I64 = ctypes.c_int64
+_P = ctypes.c_void_p
+
+OK = 0
+ERRORS = {
+    -1: "MPM_ERR_INVALID_ARG", -2: "MPM_ERR_OUT_OF_MEMORY", -3: "MPM_ERR_CUDA", -4: "MPM_ERR_NONFINITE",
+    -5: "MPM_ERR_INVALID_J", -6: "MPM_ERR_OUT_OF_RANGE", -7: "MPM_ERR_TIMEOUT", -8: "MPM_ERR_STATE",
+    -9: "MPM_ERR_CAPACITY", -10: "MPM_ERR_UNSUPPORTED",
+}
+STATUS_NONFINITE, STATUS_INVALID_J, STATUS_OUT_OF_RANGE, STATUS_TIMEOUT, STATUS_SCATTER_OVERFLOW = 1, 2, 4, 8, 16
+F64, F32 = 0, 1
+PROFILE_KERNELS = ("begin", "grid_update", "g2p2g", "scan", "sort_scatter", "p2g", "keys")
+
+
+class MpmDomain(ctypes.Structure):
+    _fields_ = [("lower", _D * 3), ("upper", _D * 3), ("cell_size", _D), ("gravity", _D * 3),
+                ("sticky_floor", _I32), ("clamp_positions", _I32), ("mass_eps", _D), ("cfl", _D),
+                ("dt_max", _D), ("grad_limit", _D), ("cubic", _I32), ("reserved", _I32)]
+
+
+class MpmMaterial(ctypes.Structure):
+    _fields_ = [("model", _I32), ("reserved", _I32), ("mu", _D), ("lam", _D), ("yield_stress", _D),
+                ("hardening", _D), ("T_ref", _D), ("T_hot", _D), ("hot_ratio", _D),
+                ("heat_fraction", _D), ("specific_heat", _D)]
+
+
+class MpmParticles(ctypes.Structure):
+    _fields_ = [("dtype", _I32), ("reserved", _I32), ("x", _P), ("y", _P), ("z", _P), ("vx", _P),
+                ("vy", _P), ("vz", _P), ("mass", _P), ("volume", _P), ("temperature", _P),
+                ("plastic", _P), ("F", _P), ("C", _P), ("material", _P), ("pinned", _P)]
+
+
+class MpmLedger(ctypes.Structure):
+    _fields_ = [("mass", _D), ("kinetic", _D), ("affine", _D), ("potential", _D), ("elastic", _D),
+                ("momentum", _D * 3), ("angular", _D * 3), ("min_j", _D), ("max_j", _D),
+                ("max_plastic", _D), ("max_von_mises", _D), ("plastic_work", _D), ("count", _I64),
+                ("nonfinite", _I64), ("invalid_j", _I64)]
+
+
+# name -> (restype, argtypes)
+SIGNATURES = {
+    "mpm_abi_version": (ctypes.c_int, []),
+    "mpm_error_string": (ctypes.c_char_p, [ctypes.c_int]),
+    "mpm_create": (ctypes.c_int, [ctypes.POINTER(MpmDomain), _I64, ctypes.POINTER(_P)]),
+    "mpm_destroy": (ctypes.c_int, [_P]),
+    "mpm_last_error": (ctypes.c_char_p, [_P]),
+    "mpm_configure_domain": (ctypes.c_int, [_P, ctypes.POINTER(MpmDomain)]),
+    "mpm_grid_dims": (ctypes.c_int, [_P, ctypes.POINTER(_I32), ctypes.POINTER(_D)]),
+    "mpm_set_material": (ctypes.c_int, [_P, _I32, ctypes.POINTER(MpmMaterial)]),
+    "mpm_get_stream": (ctypes.c_int, [_P, ctypes.POINTER(_P)]),
+    "mpm_upload_particles": (ctypes.c_int, [_P, _I64, ctypes.POINTER(MpmParticles)]),
+    "mpm_download_particles": (ctypes.c_int, [_P, ctypes.POINTER(MpmParticles)]),
+    "mpm_count": (ctypes.c_int, [_P, ctypes.POINTER(_I64)]),
+    "mpm_reset_deformation": (ctypes.c_int, [_P]),
+    "mpm_stable_dt": (ctypes.c_int, [_P, ctypes.POINTER(_D)]),
+    "mpm_step": (ctypes.c_int, [_P, _D, _I32, ctypes.POINTER(_I32), ctypes.POINTER(_D)]),
+    "mpm_step_fixed": (ctypes.c_int, [_P, _D, _I32]),
+    "mpm_step_cfl": (ctypes.c_int, [_P, _I32, ctypes.POINTER(_D)]),
+    "mpm_step_host": (ctypes.c_int, [_P, ctypes.POINTER(MpmParticles), _D]),
+    "mpm_frame_host": (ctypes.c_int, [_P, ctypes.POINTER(MpmParticles), _D, _I32, ctypes.POINTER(_I32)]),
+    "mpm_profile_enable": (ctypes.c_int, [_P, _I32]),
+    "mpm_profile_read": (ctypes.c_int, [_P, ctypes.POINTER(_D), ctypes.POINTER(_I64)]),
+    "mpm_launch_count": (ctypes.c_int, [_P, ctypes.POINTER(_I64)]),
+    "mpm_ledger_compute": (ctypes.c_int, [_P, ctypes.POINTER(MpmLedger)]),
+    "mpm_min_j": (ctypes.c_int, [_P, ctypes.POINTER(_D)]),
+    "mpm_status": (ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_uint32)]),
+    "mpm_clear_status": (ctypes.c_int, [_P]),
+    "mpm_grid_debug": (ctypes.c_int, [_P, _D, _P, _P]),
+    "mpm_snapshot": (ctypes.c_int, [_P]),
+    "mpm_rollback": (ctypes.c_int, [_P]),
+    "mpm_checkpoint_save": (ctypes.c_int, [_P, ctypes.c_char_p]),
+    "mpm_checkpoint_load": (ctypes.c_int, [_P, ctypes.c_char_p]),
+    "mpm_host_alloc": (ctypes.c_int, [ctypes.c_size_t, ctypes.POINTER(_P)]),
+    "mpm_host_free": (ctypes.c_int, [_P]),
+    "mpm_return_map_batch": (ctypes.c_int, [ctypes.POINTER(MpmMaterial), _I64, _P, _P, _P, _D, _P, _P, _P]),
+}
+
+_lib = None
+
+
+class MpmError(RuntimeError):
+    def __init__(self, code, message):
+        super().__init__(f"{ERRORS.get(code, code)}: {message}")
+        self.code = code
+
+
+def lib():
+    """The loaded library. Raises when the in-tree build is missing (no CPU fallback exists)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with `python __graft_entry__.py build`")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(rc, handle=None):
+    if rc != OK:
+        msg = lib().mpm_last_error(handle).decode() if handle else lib().mpm_error_string(rc).decode()
+        raise MpmError(rc, msg)
+    return rc

@@ -1,0 +1,216 @@
+"""Host-side handle of the device MLS-MPM step (one scene), over the C ABI.
+
+``Solver`` owns one library handle: it uploads a ``scenes.Scene``, advances it on the device and
+downloads the state. It is the Python face of the same entry points a Node N-API addon binds.
+"""
+import ctypes
+import math
+
+import numpy as np
+
+from . import _lib
+from ._lib import MpmDomain, MpmMaterial, MpmParticles, MpmLedger, check
+
+_P = ctypes.c_void_p
+
+
+def domain_struct(d):
+    s = MpmDomain()
+    for a in range(3):
+        s.lower[a] = d.lower[a]
+        s.upper[a] = d.upper[a]
+        s.gravity[a] = d.gravity[a]
+    s.cell_size = d.H
+    s.sticky_floor = int(d.sticky_floor)
+    s.clamp_positions = int(d.clamp_positions)
+    s.mass_eps = d.mass_eps
+    s.cfl = d.cfl
+    s.dt_max = d.dt_max if math.isfinite(d.dt_max) else 0.0
+    s.grad_limit = d.grad_limit
+    s.cubic = int(d.cubic)
+    return s
+
+
+def material_struct(m):
+    return MpmMaterial(model=m.model, mu=m.mu, lam=m.lam, yield_stress=m.yield_stress,
+                       hardening=m.hardening, T_ref=m.T_ref, T_hot=m.T_hot, hot_ratio=m.hot_ratio,
+                       heat_fraction=m.heat_fraction, specific_heat=m.specific_heat)
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(_P)
+
+
+class Solver:
+    def __init__(self, domain, capacity):
+        self._keep = []
+        self.domain = domain
+        h = _P()
+        check(_lib.lib().mpm_create(ctypes.byref(domain_struct(domain)), int(capacity), ctypes.byref(h)))
+        self.h = h
+        self.capacity = int(capacity)
+        self.n = 0
+
+    def close(self):
+        if self.h:
+            _lib.lib().mpm_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc):
+        return check(rc, self.h)
+
+    def set_material(self, index, m):
+        self._check(_lib.lib().mpm_set_material(self.h, index, ctypes.byref(material_struct(m))))
+
+    def upload(self, scene, dtype=np.float64):
+        for i, m in enumerate(scene.materials):
+            self.set_material(i, m)
+        n = scene.n
+        f = np.dtype(dtype)
+        arr = lambda a: None if a is None else np.ascontiguousarray(a, dtype=f)
+        x = np.ascontiguousarray(scene.x, dtype=f)
+        v = np.ascontiguousarray(scene.v, dtype=f)
+        cols = [np.ascontiguousarray(x[:, a]) for a in range(3)] + [np.ascontiguousarray(v[:, a]) for a in range(3)]
+        m, V = arr(scene.m), arr(scene.V)
+        T, ep = arr(scene.T), arr(scene.ep)
+        F = None if scene.F is None else np.ascontiguousarray(np.asarray(scene.F).reshape(n, 9), dtype=f)
+        C = None if scene.C is None else np.ascontiguousarray(np.asarray(scene.C).reshape(n, 9), dtype=f)
+        mat = np.ascontiguousarray(scene.mat, dtype=np.int32)
+        pin = None if scene.pinned is None else np.ascontiguousarray(scene.pinned, dtype=np.uint8)
+        p = MpmParticles(dtype=_lib.F64 if f == np.float64 else _lib.F32,
+                         x=_ptr(cols[0]), y=_ptr(cols[1]), z=_ptr(cols[2]), vx=_ptr(cols[3]), vy=_ptr(cols[4]),
+                         vz=_ptr(cols[5]), mass=_ptr(m), volume=_ptr(V), temperature=_ptr(T), plastic=_ptr(ep),
+                         F=_ptr(F), C=_ptr(C), material=_ptr(mat), pinned=_ptr(pin))
+        self._check(_lib.lib().mpm_upload_particles(self.h, n, ctypes.byref(p)))
+        self.n = n
+
+    def download(self, fields=("x", "v", "F", "C", "ep", "T"), dtype=np.float64):
+        n = self.n
+        f = np.dtype(dtype)
+        out = {}
+        p = MpmParticles(dtype=_lib.F64 if f == np.float64 else _lib.F32)
+        cols = {}
+        if "x" in fields:
+            for k, a in zip(("x", "y", "z"), range(3)):
+                cols[k] = np.empty(n, dtype=f)
+                setattr(p, k, _ptr(cols[k]))
+        if "v" in fields:
+            for k in ("vx", "vy", "vz"):
+                cols[k] = np.empty(n, dtype=f)
+                setattr(p, k, _ptr(cols[k]))
+        one = {"m": "mass", "V": "volume", "T": "temperature", "ep": "plastic"}
+        for k, name in one.items():
+            if k in fields:
+                out[k] = np.empty(n, dtype=f)
+                setattr(p, name, _ptr(out[k]))
+        for k in ("F", "C"):
+            if k in fields:
+                out[k] = np.empty((n, 9), dtype=f)
+                setattr(p, k, _ptr(out[k]))
+        self._check(_lib.lib().mpm_download_particles(self.h, ctypes.byref(p)))
+        if "x" in fields:
+            out["x"] = np.stack([cols["x"], cols["y"], cols["z"]], axis=1)
+        if "v" in fields:
+            out["v"] = np.stack([cols["vx"], cols["vy"], cols["vz"]], axis=1)
+        return out
+
+    def step(self, dt_requested, max_substeps=48):
+        sub = ctypes.c_int32()
+        adv = ctypes.c_double()
+        self._check(_lib.lib().mpm_step(self.h, dt_requested, max_substeps, ctypes.byref(sub), ctypes.byref(adv)))
+        return sub.value, adv.value
+
+    def step_fixed(self, dt, nsteps=1):
+        self._check(_lib.lib().mpm_step_fixed(self.h, dt, nsteps))
+
+    def step_cfl(self, nsteps=1):
+        t = ctypes.c_double()
+        self._check(_lib.lib().mpm_step_cfl(self.h, nsteps, ctypes.byref(t)))
+        return t.value
+
+    def stable_dt(self):
+        d = ctypes.c_double()
+        self._check(_lib.lib().mpm_stable_dt(self.h, ctypes.byref(d)))
+        return d.value
+
+    def ledger(self):
+        L = MpmLedger()
+        self._check(_lib.lib().mpm_ledger_compute(self.h, ctypes.byref(L)))
+        return L
+
+    def status(self):
+        s = ctypes.c_uint32()
+        self._check(_lib.lib().mpm_status(self.h, ctypes.byref(s)))
+        return s.value
+
+    def clear_status(self):
+        self._check(_lib.lib().mpm_clear_status(self.h))
+
+    def grid_dims(self):
+        dims = (ctypes.c_int32 * 3)()
+        org = (ctypes.c_double * 3)()
+        self._check(_lib.lib().mpm_grid_dims(self.h, dims, org))
+        return tuple(dims), tuple(org)
+
+    def grid_debug(self, dt):
+        dims, _ = self.grid_dims()
+        nodes = int(np.prod(dims))
+        m = np.empty(nodes)
+        p = np.empty((nodes, 3))
+        self._check(_lib.lib().mpm_grid_debug(self.h, dt, _ptr(m), _ptr(p)))
+        return m, p
+
+    def snapshot(self):
+        self._check(_lib.lib().mpm_snapshot(self.h))
+
+    def rollback(self):
+        self._check(_lib.lib().mpm_rollback(self.h))
+
+    def save(self, path):
+        self._check(_lib.lib().mpm_checkpoint_save(self.h, str(path).encode()))
+
+    def load(self, path):
+        self._check(_lib.lib().mpm_checkpoint_load(self.h, str(path).encode()))
+        cnt = ctypes.c_int64()
+        self._check(_lib.lib().mpm_count(self.h, ctypes.byref(cnt)))
+        self.n = cnt.value
+
+    def profile(self, on=True):
+        self._check(_lib.lib().mpm_profile_enable(self.h, 1 if on else 0))
+
+    def profile_read(self):
+        n = len(_lib.PROFILE_KERNELS)
+        ms = (ctypes.c_double * n)()
+        cnt = (ctypes.c_int64 * n)()
+        self._check(_lib.lib().mpm_profile_read(self.h, ms, cnt))
+        return {k: (ms[i], cnt[i]) for i, k in enumerate(_lib.PROFILE_KERNELS)}
+
+    def launch_count(self):
+        c = ctypes.c_int64()
+        self._check(_lib.lib().mpm_launch_count(self.h, ctypes.byref(c)))
+        return c.value
+
+    def stream(self):
+        s = _P()
+        self._check(_lib.lib().mpm_get_stream(self.h, ctypes.byref(s)))
+        return s.value
+
+
+def return_map_batch(material, F, ep=None, T=None, dt=0.01):
+    """Device projectPlastic + stress for a batch (n x 9 F): returns (F_out, dep, tau)."""
+    F = np.ascontiguousarray(np.asarray(F, dtype=np.float64).reshape(-1, 9))
+    n = F.shape[0]
+    ep = None if ep is None else np.ascontiguousarray(np.broadcast_to(np.asarray(ep, dtype=np.float64), (n,)))
+    T = None if T is None else np.ascontiguousarray(np.broadcast_to(np.asarray(T, dtype=np.float64), (n,)))
+    Fo = np.empty((n, 9))
+    dep = np.empty(n)
+    tau = np.empty((n, 9))
+    check(_lib.lib().mpm_return_map_batch(ctypes.byref(material_struct(material)), n, _ptr(F), _ptr(ep),
+                                          _ptr(T), dt, _ptr(Fo), _ptr(dep), _ptr(tau)))
+    return Fo, dep, tau

@@ -1,0 +1,37 @@
+// Host build of the device constitutive math (summer-particle-lab_b200/csrc/mpm_math.h) for CPU
+// tests against the FP64 oracle. Test infrastructure: compiled by tests/test_host_math.py.
+#include "mpm_math.h"
+
+extern "C" void harness_constitutive(int model, double mu, double lam, double A, double B, double Tref,
+                                     double Thot, double hot, int n, const double* F, const double* ep,
+                                     const double* T, int do_return, double* Fout, double* dep, double* tau) {
+  mpm::MaterialDev m{};
+  m.model = model;
+  m.mu = (float)mu;
+  m.lam = (float)lam;
+  m.yield_stress = (float)A;
+  m.hardening = (float)B;
+  m.T_ref = (float)Tref;
+  m.inv_T_span = Thot > Tref ? (float)(1.0 / (Thot - Tref)) : 0.f;
+  m.hot_ratio = (float)hot;
+  for (int i = 0; i < n; ++i) {
+    float D[9];
+    for (int e = 0; e < 9; ++e) D[e] = (float)(F[i * 9 + e] - (e % 4 == 0 ? 1.0 : 0.0));
+    mpm::ConstitutiveOut o = mpm::constitutive_update(m, D, (float)ep[i], (float)T[i], 1.f, do_return != 0);
+    for (int e = 0; e < 9; ++e) Fout[i * 9 + e] = (double)D[e] + (e % 4 == 0 ? 1.0 : 0.0);
+    dep[i] = o.dep;
+    const float t9[9] = {o.tau.xx, o.tau.xy, o.tau.xz, o.tau.xy, o.tau.yy, o.tau.yz, o.tau.xz, o.tau.yz, o.tau.zz};
+    for (int e = 0; e < 9; ++e) tau[i * 9 + e] = t9[e];
+  }
+}
+
+extern "C" void harness_eig(int n, const double* S6, double* lam, double* U) {
+  for (int i = 0; i < n; ++i) {
+    mpm::Sym3 a{(float)S6[i * 6 + 0], (float)S6[i * 6 + 1], (float)S6[i * 6 + 2],
+                (float)S6[i * 6 + 3], (float)S6[i * 6 + 4], (float)S6[i * 6 + 5]};
+    float l[3], u[9];
+    mpm::sym_eig3(a, l, u);
+    for (int k = 0; k < 3; ++k) lam[i * 3 + k] = l[k];
+    for (int k = 0; k < 9; ++k) U[i * 9 + k] = u[k];
+  }
+}

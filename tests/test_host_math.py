@@ -1,0 +1,107 @@
+"""The device constitutive math (mpm_math.h, FP32, centred form) compiled for the host and checked
+against the FP64 oracle on CPU: Jacobi eigensolver, fixed-corotated, Neo-Hookean, Hencky stress and
+the J2 / thermal J2 return maps, with the tolerances of the reference's own CPU/GPU return-map test
+(gpu/test_metal_plasticity.py:31-33: F atol 4e-6 rtol 4e-5)."""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from oracle import oracle as orc
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+CSRC = os.path.join(ROOT, "summer-particle-lab_b200", "csrc")
+P = ctypes.c_void_p
+
+
+@pytest.fixture(scope="module")
+def harness(tmp_path_factory):
+    out = tmp_path_factory.mktemp("h") / "libharness.so"
+    subprocess.check_call(["g++", "-O2", "-std=c++17", "-fPIC", "-shared", "-I", CSRC, "-o", str(out),
+                           os.path.join(ROOT, "tests", "native", "math_harness.cpp")])
+    L = ctypes.CDLL(str(out))
+    d = ctypes.c_double
+    L.harness_constitutive.argtypes = [ctypes.c_int, d, d, d, d, d, d, d, ctypes.c_int, P, P, P, ctypes.c_int, P, P, P]
+    L.harness_eig.argtypes = [ctypes.c_int, P, P, P]
+    return L
+
+
+def run(L, model, F, ep, T, mu=.4, lam=.4, A=.025, B=.08, Tref=20, Thot=180, hot=.08, do_return=True):
+    F = np.ascontiguousarray(np.asarray(F, dtype=np.float64).reshape(-1, 9))
+    n = F.shape[0]
+    ep = np.ascontiguousarray(np.broadcast_to(np.asarray(ep, dtype=np.float64), (n,)))
+    T = np.ascontiguousarray(np.broadcast_to(np.asarray(T, dtype=np.float64), (n,)))
+    Fo, dep, tau = np.empty((n, 9)), np.empty(n), np.empty((n, 9))
+    c = lambda a: a.ctypes.data_as(P)
+    L.harness_constitutive(model, mu, lam, A, B, Tref, Thot, hot, n, c(F), c(ep), c(T), int(do_return), c(Fo), c(dep), c(tau))
+    return Fo, dep, tau
+
+
+def random_F(n, scale, seed):
+    rng = np.random.default_rng(seed)
+    return np.tile(np.eye(3).ravel(), (n, 1)) + scale * rng.standard_normal((n, 9))
+
+
+def test_jacobi_eigensolver_reconstructs(harness):
+    rng = np.random.default_rng(1)
+    for scale in (1e-4, 1e-2, 1.0):
+        M = scale * rng.standard_normal((500, 3, 3))
+        S = M + M.transpose(0, 2, 1)
+        S6 = np.stack([S[:, 0, 0], S[:, 1, 1], S[:, 2, 2], S[:, 0, 1], S[:, 0, 2], S[:, 1, 2]], 1).copy()
+        lam, U = np.empty((500, 3)), np.empty((500, 9))
+        harness.harness_eig(500, S6.ctypes.data_as(P), lam.ctypes.data_as(P), U.ctypes.data_as(P))
+        U = U.reshape(-1, 3, 3)
+        rec = U @ (lam[:, :, None] * U.transpose(0, 2, 1))
+        err = np.max(np.abs(rec - S), axis=(1, 2)) / np.max(np.abs(S), axis=(1, 2))
+        assert np.max(err) < 2e-6, (scale, np.max(err))
+        orth = np.max(np.abs(U @ U.transpose(0, 2, 1) - np.eye(3)))
+        assert orth < 2e-6
+
+
+@pytest.mark.parametrize("model", [0, 1])
+def test_elastic_stress_matches_oracle(harness, model):
+    for scale in (1e-3, 5e-2):
+        F = random_F(300, scale, 2 + model)
+        _, _, tau = run(harness, model, F, 0, 0, mu=400, lam=300)
+        for i in range(F.shape[0]):
+            ref = orc.constitutive_stress(F[i], model, 400, 300)
+            np.testing.assert_allclose(tau[i], ref, atol=2e-5 * np.max(np.abs(ref)) + 1e-9, rtol=0)
+
+
+@pytest.mark.parametrize("model", [4, 5])
+def test_j2_return_matches_oracle(harness, model):
+    F = random_F(400, 0.05, 7 + model)
+    Fo, dep, tau = run(harness, model, F, .05, 20)
+    mat = orc.material(model)
+    n_yield = 0
+    for i in range(F.shape[0]):
+        Fr, inc, tr = orc.project(F[i], mat, ep=.05, dt=.01, T=20)
+        np.testing.assert_allclose(Fo[i], Fr, atol=4e-6, rtol=4e-5)
+        assert abs(dep[i] - inc) < 1e-5
+        np.testing.assert_allclose(tau[i], tr, atol=3e-6, rtol=5e-4)
+        n_yield += inc > 0
+    assert n_yield > 50
+
+
+def test_thermal_j2_return_matches_oracle(harness):
+    F = random_F(300, 0.05, 19)
+    T = np.linspace(-100, 800, 300)
+    Fo, dep, tau = run(harness, 10, F, .05, T, A=.04, B=.04)
+    mat = orc.material(10)
+    for i in range(F.shape[0]):
+        Fr, inc, tr = orc.project(F[i], mat, ep=.05, dt=.01, T=T[i])
+        np.testing.assert_allclose(Fo[i], Fr, atol=4e-6, rtol=5e-5)
+        assert abs(dep[i] - inc) < 1e-5
+
+
+def test_small_strain_precision_of_centred_form(harness):
+    """Elastic metal strains (~1e-4): the centred form keeps ~1e-6 relative stress accuracy."""
+    E = 70e9
+    mu, lam = E / 2.66, E * .33 / (1.33 * .34)
+    F = random_F(200, 1e-4, 23)
+    _, _, tau = run(harness, 5, F, 0, 0, mu=mu, lam=lam, A=250e6, B=1e9)
+    for i in range(F.shape[0]):
+        ref = orc.constitutive_stress(F[i], 5, mu, lam)
+        np.testing.assert_allclose(tau[i], ref, atol=2e-5 * np.max(np.abs(ref)), rtol=0)
