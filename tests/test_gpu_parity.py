@@ -19,11 +19,18 @@ from mpm_b200.solver import Solver, return_map_batch
 pytestmark = pytest.mark.gpu
 
 
-def rel(a, b):
+def rel(a, b, floor=0.0):
+    """max |a - b| / max(max |b|, floor): normwise relative error with an absolute scale floor for
+    fields that are pure rounding noise in the FP64 oracle (e.g. C of a uniform velocity field)."""
     a = np.asarray(a, dtype=np.float64)
     b = np.asarray(b, dtype=np.float64)
-    scale = np.max(np.abs(b))
+    scale = max(float(np.max(np.abs(b))), floor)
     return float(np.max(np.abs(a - b)) / (scale if scale > 0 else 1.0))
+
+
+def c_scale(v, H):
+    """Natural scale of the APIC matrix: a velocity difference of max |v| across a cell (4/h)."""
+    return float(np.max(np.abs(v))) * 4.0 / H
 
 
 def run_pair(scene, dt, steps, capacity=None):
@@ -123,7 +130,7 @@ def test_elastic_cube_one_step_grid_and_particles():
     out = sol.download()
     assert np.max(np.abs(out["x"] - st.x)) <= 1e-6
     assert rel(out["v"], st.v) <= 1e-6
-    assert rel(out["C"], st.C) <= 1e-6
+    assert rel(out["C"], st.C, c_scale(st.v, sc.domain.H)) <= 1e-6
     assert np.max(np.abs(out["F"] - st.F)) <= 1e-6
 
 
@@ -215,8 +222,9 @@ def test_tma_and_plain_gather_agree(monkeypatch):
     b.upload(sc)
     b.step_fixed(2e-7, 4)
     oa, ob = a.download(), b.download()
-    for k in ("x", "v", "F", "C"):
+    for k in ("x", "v", "F"):
         assert rel(oa[k], ob[k]) <= 1e-6
+    assert rel(oa["C"], ob["C"], c_scale(ob["v"], sc.domain.H)) <= 1e-6
 
 
 def test_step_host_drop_in_matches_resident_step():
