@@ -102,13 +102,21 @@ class Clocks:
         self.proc = None
         self.path = os.path.join(ROOT, "gpurun_out", f"clocks_bench_{os.getpid()}.csv")
 
+    def wait_first_sample(self, timeout=5.0):
+        t0 = time.time()
+        while self.proc is not None and time.time() - t0 < timeout:
+            if os.path.exists(self.path) and os.path.getsize(self.path) > 0:
+                return
+            time.sleep(0.05)
+
     def __enter__(self):
         try:
             os.makedirs(os.path.dirname(self.path), exist_ok=True)
             self.f = open(self.path, "w")
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
                                          stdout=self.f, stderr=subprocess.DEVNULL)
+            self.t0 = time.time()
         except Exception:
             self.proc = None
         return self
@@ -122,14 +130,22 @@ class Clocks:
                 self.proc.kill()
             self.f.close()
 
-    def summary(self):
+    def summary(self, t_start=None, t_end=None):
+        """Samples taken during [t_start, t_end] (the timed region), widened by one sampling period
+        on each side when the region is shorter than the sampling interval."""
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        rows = []
+        rows_all = []
         for line in open(self.path):
             parts = [p.strip() for p in line.split(",")]
             if len(parts) >= 9:
-                rows.append(parts)
+                rows_all.append(parts)
+        # nvidia-smi -lms prints one row per period from t0; map row i to t0 + (i + 1) * period
+        rows = rows_all
+        if t_start is not None and rows_all:
+            per = 0.1
+            sel = [r for i, r in enumerate(rows_all) if t_start - per <= self.t0 + (i + 1) * per <= t_end + per]
+            rows = sel if sel else rows_all[-2:]
         if not rows:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
         sm = sorted(float(r[1]) for r in rows if r[1].replace(".", "").isdigit())
@@ -222,9 +238,12 @@ def main():
     sol = Solver(scene.domain, scene.n)
     sol.upload(scene)
     ext = torch.cuda.ExternalStream(sol.stream())
+    clk = Clocks(local if world == 1 else 0)
+    clk.__enter__()  # sampling starts before warm-up so the timed region is covered
     for _ in range(args.warmup):
         sol.step(dt_req)
     torch.cuda.synchronize()
+    clk.wait_first_sample()
     if dist is not None:
         dist.barrier()
     sol.profile(True)
@@ -232,14 +251,17 @@ def main():
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
     substeps = 0
-    with Clocks(local if world == 1 else 0) as clk:
-        torch.cuda.synchronize()
-        ev0.record(ext)
-        for _ in range(args.steps):
-            s, _adv = sol.step(dt_req)
-            substeps += s
-        ev1.record(ext)
-        torch.cuda.synchronize()
+    torch.cuda.synchronize()
+    t_start = time.time()
+    ev0.record(ext)
+    for _ in range(args.steps):
+        s, _adv = sol.step(dt_req)
+        substeps += s
+    ev1.record(ext)
+    torch.cuda.synchronize()
+    t_end = time.time()
+    time.sleep(0.25)
+    clk.__exit__()
     launches = sol.launch_count() - launches0
     prof = sol.profile_read()
     sol.profile(False)
@@ -276,7 +298,7 @@ def main():
                        "l2": f"particle state {scene.n * 160 / 1e6:.0f} MB > 126 MB L2 (no flush)",
                        "active_nodes": active_nodes},
             "roofline": roofline, "gpu_launches": launches,
-            "kernel_ms": {k: v[0] for k, v in prof.items()}, "clocks": clk.summary()}
+            "kernel_ms": {k: v[0] for k, v in prof.items()}, "clocks": clk.summary(t_start, t_end)}
     # end to end through the C ABI with pinned host buffers (x, v in and out every step)
     if not args.no_e2e:
         import ctypes

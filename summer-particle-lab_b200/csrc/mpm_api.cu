@@ -12,7 +12,7 @@
 #include <string>
 #include <vector>
 
-#include "../../include/mpm_b200.h"
+#include "mpm_b200.h"
 #include "mpm_internal.h"
 
 using mpm::Ctx;
@@ -210,6 +210,10 @@ static size_t carve_particles(char* base, int64_t cap, mpm::Particles& p) {
   p.vx = c.take<float>(cap); p.vy = c.take<float>(cap); p.vz = c.take<float>(cap);
   p.C = c.take<float>(cap * 9);
   p.D = c.take<float>(cap * 9);
+  for (int e = 0; e < 9; ++e) {
+    p.Cc[e] = p.C ? p.C + e * cap : nullptr;
+    p.Dc[e] = p.D ? p.D + e * cap : nullptr;
+  }
   p.m = c.take<float>(cap); p.V = c.take<float>(cap);
   p.ep = c.take<float>(cap); p.T = c.take<float>(cap);
   p.mat = c.take<unsigned short>(cap);
@@ -471,6 +475,7 @@ int mpm_create(const mpm_domain* domain, int64_t capacity, mpm_handle** out) {
   h->mats_host[0] = def;
   h->mats_dev[0] = to_device(def);
   if (alloc_grid(h) != MPM_OK) return bail(MPM_ERR_OUT_OF_MEMORY);
+  mpm::g2p2g_blocks_per_sm(false);  // sets the dynamic shared memory limit of the no-scatter pass
   h->g2p2g_blocks = h->num_sms * mpm::g2p2g_blocks_per_sm(true);
   h->p2g_blocks = h->num_sms * mpm::p2g_blocks_per_sm();
   h->grid_blocks = h->num_sms * 8;

@@ -83,6 +83,8 @@ struct Particles {
   float *vx, *vy, *vz;
   float* C;   // 9 component arrays, stride cap
   float* D;   // 9 component arrays, stride cap
+  float* Cc[9];  // the same component arrays as separate pointers (32-bit indexing in kernels)
+  float* Dc[9];
   float *m, *V, *ep, *T;
   unsigned short* mat;
   unsigned char* pinned;

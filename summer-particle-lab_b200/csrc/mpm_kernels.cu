@@ -449,92 +449,88 @@ void launch_sort_scatter(const Ctx& c, cudaStream_t st, bool initial) {
 
 // ---------------------------------------------------------------------------------------------
 // particle kernels
+//
+// One persistent kernel template serves the three particle passes:
+//   kPassP2G    scatter of the current state (stress from F without a return)
+//   kPassG2P2G  gather -> F update -> advect -> return map -> scatter of the new state
+//   kPassG2P    gather -> F update -> advect -> return map (no scatter; host round-trip steps)
+// Scatter in two phases per tile (up to kCap particles per round):
+//   A  thread per particle: compute the new state and a 22-float payload (fraction t, m, m v,
+//      m C h, -4V/h tau); bucket it by its stencil base inside the 8^3 scatter window
+//      (shared-memory counting sort, native integer atomics)
+//   B  thread per (non-empty base bucket, z layer): all particles of a bucket hit the same 27
+//      nodes, so the 9 nodes x 7 channels of one layer are summed in registers and written with
+//      63 shared atomics per bucket and layer (about 24 per particle instead of 189)
+// then one float4 atomic per touched node and channel group flushes the window to HBM.
 
-struct __align__(128) TileSmem {
-  float4 vwin[kWinG * kWinG * kWinG];   // 3456 bytes, TMA destination
-  float acc[kChannels * kWinSNodes];    // 16 KiB scatter window
-  unsigned long long mbar;
-  uint4 item;
+constexpr int kCap = 512;      // particles per scatter round
+constexpr int kPay = 22;       // payload floats per particle
+constexpr int kBuckets = 216;  // 6^3 possible stencil bases in the scatter window
+constexpr unsigned kMetaInvalid = 0x80000000u;
+
+enum Pass : int { kPassP2G = 0, kPassG2P2G = 1, kPassG2P = 2 };
+
+struct __align__(128) PartSmem {
+  float4 vwin[2][kWinG * kWinG * kWinG];  // double-buffered TMA destinations (3456 B each)
+  float acc[kChannels * kWinSNodes];      // 16 KiB scatter window
+  float pay[kPay * kCap];                 // 44 KiB payloads, structure of arrays
+  unsigned meta[kCap];                    // bucket | rank << 8 (or kMetaInvalid)
+  unsigned short sidx[kCap];              // slots sorted by bucket
+  int hist[kBuckets];
+  int bstart[kBuckets + 1];
+  unsigned short blist[kBuckets];
+  int nbuckets;
+  unsigned long long mbar[2];
+  uint4 item[2];
   int abort_flag;
   unsigned red[3 * (kBlock / 32)];
   double work[kBlock / 32];
 };
 
-// Scatter one particle's m, p, f (and pinned mass) into the shared window, or to global memory
-// when its stencil leaves the window (moved more than one cell in one substep).
-__device__ __forceinline__ void scatter_particle(const Ctx& c, const SceneDev& sc, TileSmem& sm, int nxt,
-                                                 const int tile[3], const unsigned q[3], float m, float V,
-                                                 const float v[3], const float C[9], const Sym3& tau,
-                                                 bool pinned, unsigned& key) {
-  int b[3];
-  float t[3], w[3][3];
+size_t particle_smem_bytes() { return sizeof(PartSmem); }
+
+// Per-tile constants copied out of the scene table into registers.
+struct TileCtx {
+  int tile[3];
+  int dims[3];
+  int gdim[3];
+  unsigned qlo[3], qhi[3];
+  long long node_base;
+  float H, invH;
+  int clamp;
+};
+
+// Direct global scatter (rare: particles that left the window, pinned particles): 27 nodes x
+// channel atomics straight to the accumulators, and the node tiles they touch become active.
+__device__ __noinline__ void scatter_global(const Ctx& c, const SceneDev& sc, const TileCtx& tc, int nxt,
+                                               const int b[3], const float t[3], float m, const float mv[3],
+                                               const float mC[9], const float s6[6], bool pinned) {
+  float w[3][3];
 #pragma unroll
-  for (int a = 0; a < 3; ++a) {
-    stencil_axis(q[a], sc.dims[a], b[a], t[a]);
-    bspline_weights(t[a], w[a]);
-  }
-  key = tile_key(sc, b);
-  const float H = sc.H;
-  const float mH = m * H;
-  // p = w (m v + m C dpos), dpos = (i - t) H ; f = -w (4 V / H) tau (i - t)
-  const float mv0 = m * v[0], mv1 = m * v[1], mv2 = m * v[2];
-  const float a00 = mH * C[0], a01 = mH * C[1], a02 = mH * C[2];
-  const float a10 = mH * C[3], a11 = mH * C[4], a12 = mH * C[5];
-  const float a20 = mH * C[6], a21 = mH * C[7], a22 = mH * C[8];
-  const float s = -4.f * V * sc.invH;
-  const float s00 = s * tau.xx, s01 = s * tau.xy, s02 = s * tau.xz;
-  const float s11 = s * tau.yy, s12 = s * tau.yz, s22 = s * tau.zz;
-  const int l0 = b[0] - (tile[0] * kTile - 1), l1 = b[1] - (tile[1] * kTile - 1), l2 = b[2] - (tile[2] * kTile - 1);
-  const bool in_window = l0 >= 0 && l0 <= kWinS - 3 && l1 >= 0 && l1 <= kWinS - 3 && l2 >= 0 && l2 <= kWinS - 3;
-  if (!in_window) atomicOr(&c.ctrl->status, 0x10u);
-#pragma unroll
-  for (int kz = 0; kz < 3; ++kz) {
-    const float dz = static_cast<float>(kz) - t[2];
-#pragma unroll
-    for (int ky = 0; ky < 3; ++ky) {
-      const float dy = static_cast<float>(ky) - t[1];
-      const float wyz = w[1][ky] * w[2][kz];
-      const float p0 = mv0 + a01 * dy + a02 * dz, p1 = mv1 + a11 * dy + a12 * dz, p2 = mv2 + a21 * dy + a22 * dz;
-      const float f0 = s01 * dy + s02 * dz, f1 = s11 * dy + s12 * dz, f2 = s12 * dy + s22 * dz;
-#pragma unroll
+  for (int a = 0; a < 3; ++a) bspline_weights(t[a], w[a]);
+  for (int kz = 0; kz < 3; ++kz)
+    for (int ky = 0; ky < 3; ++ky)
       for (int kx = 0; kx < 3; ++kx) {
-        const float dx = static_cast<float>(kx) - t[0];
-        const float wt = w[0][kx] * wyz;
-        const float vals[7] = {wt * m,
-                               wt * (p0 + a00 * dx),
-                               wt * (p1 + a10 * dx),
-                               wt * (p2 + a20 * dx),
-                               wt * (f0 + s00 * dx),
-                               wt * (f1 + s01 * dx),
-                               wt * (f2 + s02 * dx)};
-        if (in_window) {
-          const int node = ((l2 + kz) * kWinS + (l1 + ky)) * kWinS + (l0 + kx);
-#pragma unroll
-          for (int ch = 0; ch < 7; ++ch) atomicAdd(&sm.acc[ch * kWinSNodes + node], vals[ch]);
-          if (pinned && wt > 1e-8f) atomicAdd(&sm.acc[7 * kWinSNodes + node], wt * m);
-        } else {
-          const long long node = sc.node_base +
-                                 ((long long)(b[2] + kz) * sc.gdim[1] + (b[1] + ky)) * sc.gdim[0] + (b[0] + kx);
-          float* a0 = reinterpret_cast<float*>(&c.g.acc0[nxt][node]);
-          float* a1 = reinterpret_cast<float*>(&c.g.acc1[nxt][node]);
-          atomicAdd(a0 + 0, vals[0]);
-          atomicAdd(a0 + 1, vals[1]);
-          atomicAdd(a0 + 2, vals[2]);
-          atomicAdd(a0 + 3, vals[3]);
-          atomicAdd(a1 + 0, vals[4]);
-          atomicAdd(a1 + 1, vals[5]);
-          atomicAdd(a1 + 2, vals[6]);
-          if (pinned && wt > 1e-8f) atomicAdd(a1 + 3, wt * m);
-        }
+        const float dx = kx - t[0], dy = ky - t[1], dz = kz - t[2];
+        const float wt = w[0][kx] * w[1][ky] * w[2][kz];
+        const long long node = tc.node_base + ((long long)(b[2] + kz) * tc.gdim[1] + (b[1] + ky)) * tc.gdim[0] + (b[0] + kx);
+        float* a0 = reinterpret_cast<float*>(&c.g.acc0[nxt][node]);
+        float* a1 = reinterpret_cast<float*>(&c.g.acc1[nxt][node]);
+        atomicAdd(a0 + 0, wt * m);
+        atomicAdd(a0 + 1, wt * (mv[0] + mC[0] * dx + mC[1] * dy + mC[2] * dz));
+        atomicAdd(a0 + 2, wt * (mv[1] + mC[3] * dx + mC[4] * dy + mC[5] * dz));
+        atomicAdd(a0 + 3, wt * (mv[2] + mC[6] * dx + mC[7] * dy + mC[8] * dz));
+        atomicAdd(a1 + 0, wt * (s6[0] * dx + s6[3] * dy + s6[4] * dz));
+        atomicAdd(a1 + 1, wt * (s6[3] * dx + s6[1] * dy + s6[5] * dz));
+        atomicAdd(a1 + 2, wt * (s6[4] * dx + s6[5] * dy + s6[2] * dz));
+        if (pinned && wt > 1e-8f) atomicAdd(a1 + 3, wt * m);
       }
-    }
-  }
-  if (!in_window) mark_node_tiles_of(c, sc, b[0], b[1], b[2], nxt);
+  mark_node_tiles_of(c, sc, b[0], b[1], b[2], nxt);
 }
 
 // Flush the shared scatter window of one tile to the global accumulators (one float4 atomic per
 // touched node and channel group) and clear it; mark the 27 node tiles it covers as active.
-__device__ __forceinline__ void flush_window(const Ctx& c, const SceneDev& sc, TileSmem& sm, int nxt,
+__device__ __forceinline__ void flush_window(const Ctx& c, const SceneDev& sc, PartSmem& sm, int nxt,
                                              const int tile[3]) {
   const int o0 = tile[0] * kTile - 1, o1 = tile[1] * kTile - 1, o2 = tile[2] * kTile - 1;
   for (int i = threadIdx.x; i < kWinSNodes; i += kBlock) {
@@ -561,7 +557,7 @@ __device__ __forceinline__ void flush_window(const Ctx& c, const SceneDev& sc, T
 }
 
 // Block reduction of the per-thread CFL maxima and status flags of one tile, then one atomic per
-// tile and scene. Every thread of the CTA calls it; red holds 3 values per warp.
+// tile and scene. Every thread of the CTA calls it.
 __device__ __forceinline__ void block_reduce_item(const Ctx& c, int scene, float wave, float grad, unsigned flags,
                                                   unsigned* red) {
   const unsigned wb = __reduce_max_sync(0xffffffffu, fbits(wave));
@@ -597,71 +593,458 @@ __device__ __forceinline__ unsigned state_flags(const float v[3], const float D[
   return f;
 }
 
-// Initial P2G of the uploaded state (stress from F without a return, as updateStress does when no
-// cached stress exists, src/three/mpm.js:33-37), plus the CFL maxima of that state.
-__global__ void __launch_bounds__(kBlock, 2) k_p2g(const __grid_constant__ Ctx c) {
-  __shared__ TileSmem sm;
-  const unsigned k = c.ctrl->step_index;
-  const int lst = k & 1, nxt = k & 1;
-  for (int i = threadIdx.x; i < kChannels * kWinSNodes; i += kBlock) sm.acc[i] = 0.f;
-  __syncthreads();
-  const long long cap = c.p.cap;
-  while (true) {
-    if (threadIdx.x == 0) {
-      const unsigned idx = atomicAdd(&c.ctrl->work_next, 1u);
-      sm.item = idx < c.ctrl->work_count[lst] ? c.s.work[lst][idx] : make_uint4(0xffffffffu, 0, 0, 0);
+// Phase B task: one non-empty base bucket, one z layer of its stencil. Sums the 3x3 nodes x 7
+// channels over the bucket's particles in registers, then adds them to the shared window.
+__device__ __forceinline__ void bucket_layer(PartSmem& sm, int b, int kz) {
+  const int lx = b % 6, ly = (b / 6) % 6, lz = b / 36;
+  float a[3][3][7];
+#pragma unroll
+  for (int y = 0; y < 3; ++y)
+#pragma unroll
+    for (int x = 0; x < 3; ++x)
+#pragma unroll
+      for (int ch = 0; ch < 7; ++ch) a[y][x][ch] = 0.f;
+  const int i1 = sm.bstart[b + 1];
+  for (int i = sm.bstart[b]; i < i1; ++i) {
+    const int j = sm.sidx[i];
+    const float* P = sm.pay + j;
+    const float tx = P[0 * kCap], ty = P[1 * kCap], tz = P[2 * kCap], m = P[3 * kCap];
+    const float mv0 = P[4 * kCap], mv1 = P[5 * kCap], mv2 = P[6 * kCap];
+    const float c00 = P[7 * kCap], c01 = P[8 * kCap], c02 = P[9 * kCap];
+    const float c10 = P[10 * kCap], c11 = P[11 * kCap], c12 = P[12 * kCap];
+    const float c20 = P[13 * kCap], c21 = P[14 * kCap], c22 = P[15 * kCap];
+    const float s00 = P[16 * kCap], s11 = P[17 * kCap], s22 = P[18 * kCap];
+    const float s01 = P[19 * kCap], s02 = P[20 * kCap], s12 = P[21 * kCap];
+    float wx[3], wy[3], wzv[3];
+    bspline_weights(tx, wx);
+    bspline_weights(ty, wy);
+    bspline_weights(tz, wzv);
+    const float wz = kz == 0 ? wzv[0] : (kz == 1 ? wzv[1] : wzv[2]);
+    const float dz = static_cast<float>(kz) - tz;
+    const float q0 = mv0 + c02 * dz, q1 = mv1 + c12 * dz, q2 = mv2 + c22 * dz;
+    const float g0 = s02 * dz, g1 = s12 * dz, g2 = s22 * dz;
+    const float mwz = m * wz;
+#pragma unroll
+    for (int y = 0; y < 3; ++y) {
+      const float dy = static_cast<float>(y) - ty;
+      const float wyz = wy[y] * wz;
+      const float p0 = q0 + c01 * dy, p1 = q1 + c11 * dy, p2 = q2 + c21 * dy;
+      const float f0 = g0 + s01 * dy, f1 = g1 + s11 * dy, f2 = g2 + s12 * dy;
+      const float mwyz = mwz * wy[y];
+#pragma unroll
+      for (int x = 0; x < 3; ++x) {
+        const float dx = static_cast<float>(x) - tx;
+        const float wt = wx[x] * wyz;
+        a[y][x][0] += wx[x] * mwyz;
+        a[y][x][1] += wt * (p0 + c00 * dx);
+        a[y][x][2] += wt * (p1 + c10 * dx);
+        a[y][x][3] += wt * (p2 + c20 * dx);
+        a[y][x][4] += wt * (f0 + s00 * dx);
+        a[y][x][5] += wt * (f1 + s01 * dx);
+        a[y][x][6] += wt * (f2 + s02 * dx);
+      }
     }
+  }
+#pragma unroll
+  for (int y = 0; y < 3; ++y)
+#pragma unroll
+    for (int x = 0; x < 3; ++x) {
+      const int node = ((lz + kz) * kWinS + (ly + y)) * kWinS + (lx + x);
+#pragma unroll
+      for (int ch = 0; ch < 7; ++ch) atomicAdd(&sm.acc[ch * kWinSNodes + node], a[y][x][ch]);
+    }
+}
+
+// Exclusive scan of the bucket histogram by warp 0, with the compact list of non-empty buckets.
+__device__ __forceinline__ void scan_buckets(PartSmem& sm) {
+  if (threadIdx.x >= 32) return;
+  const int lane = threadIdx.x;
+  int carry = 0, ncarry = 0;
+  for (int b0 = 0; b0 < kBuckets; b0 += 32) {
+    const int b = b0 + lane;
+    const int h = b < kBuckets ? sm.hist[b] : 0;
+    int inc = h;
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, inc, o);
+      if (lane >= o) inc += y;
+    }
+    if (b < kBuckets) sm.bstart[b] = carry + inc - h;
+    const unsigned nz = __ballot_sync(0xffffffffu, h > 0);
+    if (h > 0) sm.blist[ncarry + __popc(nz & ((1u << lane) - 1u))] = static_cast<unsigned short>(b);
+    carry += __shfl_sync(0xffffffffu, inc, 31);
+    ncarry += __popc(nz);
+  }
+  if (lane == 0) {
+    sm.bstart[kBuckets] = carry;
+    sm.nbuckets = ncarry;
+  }
+}
+
+
+// Weighted gather of the 27 stencil nodes: out = (v, C / (4/h)) with v = sum w v_i and
+// C_ab = sum w v_i,a (i - t)_b (src/three/mpm.js:110-117). ld(kz, ky, kx) returns the node velocity.
+template <typename Ld>
+__device__ __forceinline__ void gather27(Ld ld, const float t[3], const float w[3][3], float out[12]) {
+  float v0 = 0.f, v1 = 0.f, v2 = 0.f;
+  float c0 = 0.f, c1 = 0.f, c2 = 0.f, c3 = 0.f, c4 = 0.f, c5 = 0.f, c6 = 0.f, c7 = 0.f, c8 = 0.f;
+#pragma unroll
+  for (int kz = 0; kz < 3; ++kz) {
+    const float dz = static_cast<float>(kz) - t[2];
+#pragma unroll
+    for (int ky = 0; ky < 3; ++ky) {
+      const float dy = static_cast<float>(ky) - t[1];
+      const float wyz = w[1][ky] * w[2][kz];
+#pragma unroll
+      for (int kx = 0; kx < 3; ++kx) {
+        const float dx = static_cast<float>(kx) - t[0];
+        const float wt = w[0][kx] * wyz;
+        const float4 g = ld(kz, ky, kx);
+        const float ga = wt * g.x, gb = wt * g.y, gc = wt * g.z;
+        v0 += ga; v1 += gb; v2 += gc;
+        c0 += ga * dx; c1 += ga * dy; c2 += ga * dz;
+        c3 += gb * dx; c4 += gb * dy; c5 += gb * dz;
+        c6 += gc * dx; c7 += gc * dy; c8 += gc * dz;
+      }
+    }
+  }
+  out[0] = v0; out[1] = v1; out[2] = v2;
+  out[3] = c0; out[4] = c1; out[5] = c2; out[6] = c3; out[7] = c4; out[8] = c5; out[9] = c6; out[10] = c7; out[11] = c8;
+}
+
+// Gather straight from global memory (a particle whose stencil is outside the staged window).
+__device__ __noinline__ void gather_global(const float4* base, int sy, long long sz, const float t[3], const float w[3][3],
+                                           float out[12]) {
+  gather27([&](int kz, int ky, int kx) { return base[kz * sz + ky * sy + kx]; }, t, w, out);
+}
+
+template <int PASS>
+__global__ void __launch_bounds__(kBlock, 2) k_particles(const __grid_constant__ Ctx c) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  PartSmem& sm = *reinterpret_cast<PartSmem*>(smem_raw);
+  constexpr bool SCATTER = PASS != kPassG2P;
+  constexpr bool GATHER = PASS != kPassP2G;
+  Ctrl* ct = c.ctrl;
+  if (PASS != kPassP2G && ct->done) return;
+  const unsigned k = ct->step_index;
+  // lists: the P2G pass reads the list its sort just wrote (k & 1) and scatters into acc[k & 1];
+  // a substep (after k_begin advanced k) reads list (k - 1) & 1 and scatters into acc[k & 1]
+  const int lst = PASS == kPassP2G ? (k & 1) : ((k - 1) & 1);
+  const int nxt = k & 1;
+  const bool use_tma = GATHER && c.use_tma;
+  if (SCATTER)
+    for (int i = threadIdx.x; i < kChannels * kWinSNodes; i += kBlock) sm.acc[i] = 0.f;
+  if (threadIdx.x == 0) {
+    mbar_init(&sm.mbar[0], 1);
+    mbar_init(&sm.mbar[1], 1);
+    fence_barrier_init();
+    sm.abort_flag = 0;
+    const unsigned idx = atomicAdd(&ct->work_next, 1u);
+    sm.item[0] = idx < ct->work_count[lst] ? c.s.work[lst][idx] : make_uint4(0xffffffffu, 0, 0, 0);
+    if (use_tma && sm.item[0].x != 0xffffffffu) {
+      const uint4 it = sm.item[0];
+      const SceneDev& sc = c.scenes[it.w];
+      const int lt = static_cast<int>(it.x) - sc.tile_base;
+      mbar_arrive_expect_tx(&sm.mbar[0], sizeof(sm.vwin[0]));
+      tma_load_4d(sm.vwin[0], static_cast<const char*>(c.tmaps) + 128 * it.w, 0, (lt % sc.tiles[0]) * kTile,
+                  ((lt / sc.tiles[0]) % sc.tiles[1]) * kTile, (lt / (sc.tiles[0] * sc.tiles[1])) * kTile, &sm.mbar[0]);
+    }
+  }
+  unsigned phase0 = 0, phase1 = 0;
+  double work_acc = 0.0;
+  int cb = 0;
+  // perm entries of the next tile's first round (j = tid, tid + kBlock), loaded one tile ahead
+  unsigned pf[kCap / kBlock] = {0u, 0u};
+  bool pf_ok = false;
+  while (true) {
     __syncthreads();
-    const uint4 it = sm.item;
+    const uint4 it = sm.item[cb];
     if (it.x == 0xffffffffu) break;
+    if (threadIdx.x == 0) {
+      if (use_tma) {
+        const unsigned ph = cb ? phase1 : phase0;
+        if (!mbar_wait_bounded(&sm.mbar[cb], ph)) {
+          atomicOr(&ct->status, 0x8u);
+          mbar_wait_bounded(&sm.mbar[cb], ph);  // a second bounded chance for the copy in flight
+          sm.abort_flag = 1;
+        }
+        if (cb) phase1 ^= 1u; else phase0 ^= 1u;
+      }
+    }
+    // The next work item is claimed, and its velocity window requested, by thread 0 after phase A
+    // of this tile's first round, so the two dependent global round trips overlap other warps' work.
+    auto prefetch_next = [&]() {
+      if (threadIdx.x != 0) return;
+      const unsigned idx = atomicAdd(&ct->work_next, 1u);
+      const uint4 nx = idx < ct->work_count[lst] ? c.s.work[lst][idx] : make_uint4(0xffffffffu, 0, 0, 0);
+      sm.item[cb ^ 1] = nx;
+      if (use_tma && nx.x != 0xffffffffu && !sm.abort_flag) {
+        const SceneDev& sn = c.scenes[nx.w];
+        const int lt = static_cast<int>(nx.x) - sn.tile_base;
+        fence_proxy_async_smem();
+        mbar_arrive_expect_tx(&sm.mbar[cb ^ 1], sizeof(sm.vwin[0]));
+        tma_load_4d(sm.vwin[cb ^ 1], static_cast<const char*>(c.tmaps) + 128 * nx.w, 0, (lt % sn.tiles[0]) * kTile,
+                    ((lt / sn.tiles[0]) % sn.tiles[1]) * kTile, (lt / (sn.tiles[0] * sn.tiles[1])) * kTile,
+                    &sm.mbar[cb ^ 1]);
+      }
+    };
     const int scene = static_cast<int>(it.w);
     const SceneDev& sc = c.scenes[scene];
-    int tile[3];
+    TileCtx tc;
     {
       const int lt = static_cast<int>(it.x) - sc.tile_base;
-      tile[0] = lt % sc.tiles[0];
-      tile[1] = (lt / sc.tiles[0]) % sc.tiles[1];
-      tile[2] = lt / (sc.tiles[0] * sc.tiles[1]);
+      tc.tile[0] = lt % sc.tiles[0];
+      tc.tile[1] = (lt / sc.tiles[0]) % sc.tiles[1];
+      tc.tile[2] = lt / (sc.tiles[0] * sc.tiles[1]);
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        tc.dims[a] = sc.dims[a];
+        tc.gdim[a] = sc.gdim[a];
+        tc.qlo[a] = sc.qlo[a];
+        tc.qhi[a] = sc.qhi[a];
+      }
+      tc.node_base = sc.node_base;
+      tc.H = sc.H;
+      tc.invH = sc.invH;
+      tc.clamp = sc.clamp;
     }
+    if (GATHER && !use_tma) {
+      for (int i = threadIdx.x; i < kWinG * kWinG * kWinG; i += kBlock) {
+        const int x = tc.tile[0] * kTile + i % kWinG, y = tc.tile[1] * kTile + (i / kWinG) % kWinG,
+                  z = tc.tile[2] * kTile + i / (kWinG * kWinG);
+        sm.vwin[cb][i] = c.g.vel[tc.node_base + ((long long)z * tc.gdim[1] + y) * tc.gdim[0] + x];
+      }
+    }
+    __syncthreads();
+    if (sm.abort_flag) return;
+    const float dt = GATHER ? c.dt_scene[scene] : 0.f;
+    const bool single = c.single_material != 0;
+    MaterialDev mt_tile;
+    if (single) mt_tile = c.mats[sc.mat_base];
     float wave_acc = 0.f, grad_acc = 0.f;
     unsigned flags_acc = 0;
-    for (unsigned j0 = 0; j0 < it.z; j0 += kBlock) {
-      const unsigned j = j0 + threadIdx.x;
-      if (j < it.z) {
-        float wave = 0.f, grad = 0.f;
-        const unsigned home = c.p.perm[it.y + j];
-        const unsigned q[3] = {c.p.qx[home], c.p.qy[home], c.p.qz[home]};
-        float D[9], C[9];
+    for (unsigned r0 = 0; r0 < it.z; r0 += kCap) {
+      const unsigned nround = min(static_cast<unsigned>(kCap), it.z - r0);
+      if (SCATTER) {
+        for (int i = threadIdx.x; i < kBuckets; i += kBlock) sm.hist[i] = 0;
+        __syncthreads();
+      }
+      // ---- phase A: one thread per particle ----
+      for (unsigned jj = 0; jj < nround; jj += kBlock) {
+        const unsigned j = jj + threadIdx.x;
+        unsigned key = 0xffffffffu;
+        if (j < nround) {
+          const unsigned home = (r0 == 0 && pf_ok) ? (jj == 0 ? pf[0] : pf[1]) : c.p.perm[it.y + r0 + j];
+          unsigned q[3] = {c.p.qx[home], c.p.qy[home], c.p.qz[home]};
+          float D[9];
 #pragma unroll
-        for (int e = 0; e < 9; ++e) {
-          D[e] = c.p.D[e * cap + home];
-          C[e] = c.p.C[e * cap + home];
+          for (int e = 0; e < 9; ++e) D[e] = c.p.Dc[e][home];
+          const float m = c.p.m[home], V = c.p.V[home];
+          const MaterialDev mt = single ? mt_tile : c.mats[c.p.mat[home]];
+          const bool pinned = c.has_pinned && c.p.pinned[home];
+          float ep = c.has_plastic ? c.p.ep[home] : 0.f;
+          float T = c.has_thermal ? c.p.T[home] : 0.f;
+          float v[3], C[9];
+          ConstitutiveOut co;
+          unsigned flags = 0;
+          if (GATHER && !pinned) {
+            int b[3];
+            float t[3], w[3][3];
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+              stencil_axis(q[a], tc.dims[a], b[a], t[a]);
+              bspline_weights(t[a], w[a]);
+            }
+            const int l0 = b[0] - tc.tile[0] * kTile, l1 = b[1] - tc.tile[1] * kTile, l2 = b[2] - tc.tile[2] * kTile;
+            // the sort key places the stencil inside the staged window; if it ever does not, the
+            // particle reads the grid from global memory instead (and the step reports it)
+            const bool in_g = l0 >= 0 && l0 <= kWinG - 3 && l1 >= 0 && l1 <= kWinG - 3 && l2 >= 0 && l2 <= kWinG - 3;
+            if (!in_g) flags |= 0x20u;
+            // G2P (src/three/mpm.js:107-118): v = sum w v_i, C = sum w v_i (i - t)^T 4/h
+            float acc12[12];
+            if (in_g) {
+              const float4* win = &sm.vwin[cb][(l2 * kWinG + l1) * kWinG + l0];
+              gather27([&](int kz, int ky, int kx) { return win[(kz * kWinG + ky) * kWinG + kx]; }, t, w, acc12);
+            } else {
+              gather_global(c.g.vel + tc.node_base + ((long long)b[2] * tc.gdim[1] + b[1]) * tc.gdim[0] + b[0], tc.gdim[0],
+                            (long long)tc.gdim[0] * tc.gdim[1], t, w, acc12);
+            }
+            const float v0 = acc12[0], v1 = acc12[1], v2 = acc12[2];
+            const float c0 = acc12[3], c1 = acc12[4], c2 = acc12[5], c3 = acc12[6], c4 = acc12[7], c5 = acc12[8],
+                        c6 = acc12[9], c7 = acc12[10], c8 = acc12[11];
+            const float s4 = 4.f * tc.invH;
+            v[0] = v0; v[1] = v1; v[2] = v2;
+            C[0] = c0 * s4; C[1] = c1 * s4; C[2] = c2 * s4;
+            C[3] = c3 * s4; C[4] = c4 * s4; C[5] = c5 * s4;
+            C[6] = c6 * s4; C[7] = c7 * s4; C[8] = c8 * s4;
+            // F <- (I + dt C) F in centred form: D <- D + dt C (I + D) (src/three/mpm.js:119-121)
+            float Dn[9];
+#pragma unroll
+            for (int a = 0; a < 3; ++a)
+#pragma unroll
+              for (int bc = 0; bc < 3; ++bc)
+                Dn[a * 3 + bc] = D[a * 3 + bc] + dt * (C[a * 3 + bc] + C[a * 3 + 0] * D[0 * 3 + bc] +
+                                                       C[a * 3 + 1] * D[1 * 3 + bc] + C[a * 3 + 2] * D[2 * 3 + bc]);
+#pragma unroll
+            for (int e = 0; e < 9; ++e) D[e] = Dn[e];
+            // x += dt v (src/three/mpm.js:122) in fixed point, clamped into the box
+            const float s = dt * tc.invH * kFixedOne;
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+              // |dq| stays below 2^30 (a particle moves far less than 256 cells in a substep)
+              long long qn = static_cast<long long>(q[a]) + __float2int_rn(fminf(fmaxf(s * v[a], -1.0e9f), 1.0e9f));
+              if (tc.clamp) {
+                qn = qn < (long long)tc.qlo[a] ? (long long)tc.qlo[a] : qn;
+                qn = qn > (long long)tc.qhi[a] ? (long long)tc.qhi[a] : qn;
+              } else {
+                const long long hi = (static_cast<long long>(tc.dims[a]) - 1) << kFracBits;
+                if (qn < 0 || qn > hi) flags |= 0x4u;
+                qn = qn < 0 ? 0 : (qn > hi ? hi : qn);
+              }
+              q[a] = static_cast<unsigned>(qn);
+            }
+            // return map / stress for the next P2G (src/three/mpm.js:126-131)
+            co = constitutive_update(mt, D, ep, T, V / m, true);
+            ep += co.dep;
+            T += co.dT;
+            c.p.qx[home] = q[0]; c.p.qy[home] = q[1]; c.p.qz[home] = q[2];
+            c.p.vx[home] = v[0]; c.p.vy[home] = v[1]; c.p.vz[home] = v[2];
+#pragma unroll
+            for (int e = 0; e < 9; ++e) {
+              c.p.Cc[e][home] = C[e];
+              c.p.Dc[e][home] = D[e];
+            }
+            if (c.has_plastic) c.p.ep[home] = ep;
+            if (c.has_thermal) c.p.T[home] = T;
+            if (co.dep > 0.f && mt.heat_per_work > 0.f) work_acc += static_cast<double>(co.dT) * m / mt.heat_per_work;
+          } else {
+            // P2G of the stored state, and pinned particles (not moved, src/three/mpm.js:108)
+            v[0] = c.p.vx[home]; v[1] = c.p.vy[home]; v[2] = c.p.vz[home];
+#pragma unroll
+            for (int e = 0; e < 9; ++e) C[e] = c.p.Cc[e][home];
+            float Dc[9];
+#pragma unroll
+            for (int e = 0; e < 9; ++e) Dc[e] = D[e];
+            co = constitutive_update(mt, Dc, ep, T, V / m, false);
+          }
+          if (SCATTER) {
+            // payload of the scatter: fraction t, m, m v, m C h, -4 V / h tau
+            int nb[3];
+            float t[3];
+#pragma unroll
+            for (int a = 0; a < 3; ++a) stencil_axis(q[a], tc.dims[a], nb[a], t[a]);
+            key = tile_key(sc, nb);
+            if (PASS == kPassG2P2G) c.p.key[home] = key;
+            const float mv[3] = {m * v[0], m * v[1], m * v[2]};
+            const float mH = m * tc.H;
+            float mC[9];
+#pragma unroll
+            for (int e = 0; e < 9; ++e) mC[e] = mH * C[e];
+            const float sv = -4.f * V * tc.invH;
+            const float s6[6] = {sv * co.tau.xx, sv * co.tau.yy, sv * co.tau.zz, sv * co.tau.xy, sv * co.tau.xz, sv * co.tau.yz};
+            const int l0 = nb[0] - (tc.tile[0] * kTile - 1), l1 = nb[1] - (tc.tile[1] * kTile - 1),
+                      l2 = nb[2] - (tc.tile[2] * kTile - 1);
+            const bool in_w = l0 >= 0 && l0 <= kWinS - 3 && l1 >= 0 && l1 <= kWinS - 3 && l2 >= 0 && l2 <= kWinS - 3;
+            if (in_w && !pinned) {
+              const int bucket = (l2 * 6 + l1) * 6 + l0;
+              const int rank = atomicAdd(&sm.hist[bucket], 1);
+              sm.meta[j] = static_cast<unsigned>(bucket) | (static_cast<unsigned>(rank) << 8);
+              float* P = sm.pay + j;
+              P[0 * kCap] = t[0]; P[1 * kCap] = t[1]; P[2 * kCap] = t[2]; P[3 * kCap] = m;
+              P[4 * kCap] = mv[0]; P[5 * kCap] = mv[1]; P[6 * kCap] = mv[2];
+#pragma unroll
+              for (int e = 0; e < 9; ++e) P[(7 + e) * kCap] = mC[e];
+#pragma unroll
+              for (int e = 0; e < 6; ++e) P[(16 + e) * kCap] = s6[e];
+            } else {
+              sm.meta[j] = kMetaInvalid;
+              if (!in_w) flags |= 0x10u;
+              scatter_global(c, sc, tc, nxt, nb, t, m, mv, mC, s6, pinned);
+            }
+          }
+          float wave, grad;
+          cfl_terms(mt, D, v, C, m, V, co.Jm1, wave, grad);
+          flags |= state_flags(v, D, co.tau, co.Jm1);
+          flags_acc |= flags;
+          wave_acc = fmaxf(wave_acc, wave);
+          grad_acc = fmaxf(grad_acc, grad);
         }
-        const float v[3] = {c.p.vx[home], c.p.vy[home], c.p.vz[home]};
-        const float m = c.p.m[home], V = c.p.V[home];
-        const int mi = c.single_material ? sc.mat_base : c.p.mat[home];
-        const MaterialDev mt = c.mats[mi];
-        const bool pinned = c.has_pinned && c.p.pinned[home];
-        const float ep = c.has_plastic ? c.p.ep[home] : 0.f;
-        const float T = c.has_thermal ? c.p.T[home] : 0.f;
-        float Dc[9];
+        if (PASS == kPassG2P2G) count_key(c, key);
+      }
+      if (r0 == 0) prefetch_next();
+      if (SCATTER) {
+        __syncthreads();
+        scan_buckets(sm);
+        if (r0 == 0) {
+          const uint4 nx = sm.item[cb ^ 1];
+          pf_ok = nx.x != 0xffffffffu;
+          if (pf_ok) {
 #pragma unroll
-        for (int e = 0; e < 9; ++e) Dc[e] = D[e];
-        const ConstitutiveOut co = constitutive_update(mt, Dc, ep, T, V / m, false);
-        unsigned key;
-        scatter_particle(c, sc, sm, nxt, tile, q, m, V, v, C, co.tau, pinned, key);
-        cfl_terms(mt, D, v, C, m, V, co.Jm1, wave, grad);
-        flags_acc |= state_flags(v, D, co.tau, co.Jm1);
-        wave_acc = fmaxf(wave_acc, wave);
-        grad_acc = fmaxf(grad_acc, grad);
+            for (int k = 0; k < kCap / kBlock; ++k) {
+              const unsigned j = k * kBlock + threadIdx.x;
+              pf[k] = j < nx.z ? c.p.perm[nx.y + j] : 0u;
+            }
+          }
+        }
+        __syncthreads();
+        for (unsigned j = threadIdx.x; j < nround; j += kBlock) {
+          const unsigned mm = sm.meta[j];
+          if (!(mm & kMetaInvalid)) sm.sidx[sm.bstart[mm & 0xffu] + (mm >> 8)] = static_cast<unsigned short>(j);
+        }
+        __syncthreads();
+        // ---- phase B: one thread per (non-empty bucket, z layer) ----
+        const int nbk = sm.nbuckets;
+        for (int task = threadIdx.x; task < 3 * nbk; task += kBlock) {
+          const int kz = task / nbk;
+          bucket_layer(sm, sm.blist[task - kz * nbk], kz);
+        }
+        __syncthreads();
       }
     }
     block_reduce_item(c, scene, wave_acc, grad_acc, flags_acc, sm.red);
     __syncthreads();
-    flush_window(c, sc, sm, nxt, tile);
+    if (SCATTER) flush_window(c, sc, sm, nxt, tc.tile);
+    cb ^= 1;
+  }
+  // heat from plastic work: one FP64 atomic per CTA
+  if (GATHER) {
+    double wsum = warp_sum_d(work_acc);
     __syncthreads();
+    if ((threadIdx.x & 31) == 0) sm.work[threadIdx.x >> 5] = wsum;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double tsum = 0.0;
+      for (int w = 0; w < kBlock / 32; ++w) tsum += sm.work[w];
+      if (tsum != 0.0) atomicAdd(&ct->plastic_work, tsum);
+    }
   }
 }
+
+template <int PASS>
+static void launch_pass(const Ctx& c, cudaStream_t st, int grid_blocks) {
+  k_particles<PASS><<<grid_blocks, kBlock, sizeof(PartSmem), st>>>(c);
+}
+
+void launch_p2g(const Ctx& c, cudaStream_t st, int grid_blocks) { launch_pass<kPassP2G>(c, st, grid_blocks); }
+
+void launch_g2p2g(const Ctx& c, cudaStream_t st, int grid_blocks, bool scatter) {
+  if (scatter)
+    launch_pass<kPassG2P2G>(c, st, grid_blocks);
+  else
+    launch_pass<kPassG2P>(c, st, grid_blocks);
+}
+
+template <int PASS>
+static int blocks_per_sm() {
+  cudaFuncSetAttribute(k_particles<PASS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(PartSmem));
+  int n = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_particles<PASS>, kBlock, sizeof(PartSmem));
+  return n > 0 ? n : 1;
+}
+
+int g2p2g_blocks_per_sm(bool scatter) { return scatter ? blocks_per_sm<kPassG2P2G>() : blocks_per_sm<kPassG2P>(); }
+
+int p2g_blocks_per_sm() { return blocks_per_sm<kPassP2G>(); }
+
 
 // Grid update over the active node tiles (src/three/mpm.js:89-102 with gravity on the grid).
 __global__ void __launch_bounds__(256) k_grid_update(Ctx c) {
@@ -730,231 +1113,6 @@ void launch_grid_update(const Ctx& c, cudaStream_t st, int grid_blocks) {
   k_grid_update<<<grid_blocks, 256, 0, st>>>(c);
 }
 
-// Fused G2P + F update + return map + P2G of the new state (one particle pass per substep).
-template <bool SCATTER>
-__global__ void __launch_bounds__(kBlock, 2) k_g2p2g(const __grid_constant__ Ctx c) {
-  __shared__ TileSmem sm;
-  Ctrl* ct = c.ctrl;
-  if (ct->done) return;
-  const unsigned k = ct->step_index;
-  const int cur = (k - 1) & 1, nxt = k & 1;
-  if (SCATTER)
-    for (int i = threadIdx.x; i < kChannels * kWinSNodes; i += kBlock) sm.acc[i] = 0.f;
-  if (threadIdx.x == 0) {
-    mbar_init(&sm.mbar, 1);
-    fence_barrier_init();
-    sm.abort_flag = 0;
-  }
-  __syncthreads();
-  unsigned phase = 0;
-  double work_acc = 0.0;
-  const long long cap = c.p.cap;
-  while (true) {
-    if (threadIdx.x == 0) {
-      const unsigned idx = atomicAdd(&ct->work_next, 1u);
-      sm.item = idx < ct->work_count[cur] ? c.s.work[cur][idx] : make_uint4(0xffffffffu, 0, 0, 0);
-    }
-    __syncthreads();
-    const uint4 it = sm.item;
-    if (it.x == 0xffffffffu) break;
-    const int scene = static_cast<int>(it.w);
-    const SceneDev& sc = c.scenes[scene];
-    int tile[3];
-    {
-      const int lt = static_cast<int>(it.x) - sc.tile_base;
-      tile[0] = lt % sc.tiles[0];
-      tile[1] = (lt / sc.tiles[0]) % sc.tiles[1];
-      tile[2] = lt / (sc.tiles[0] * sc.tiles[1]);
-    }
-    // stage the 6^3 velocity window at nodes [4 t, 4 t + 5]
-    if (c.use_tma) {
-      if (threadIdx.x == 0) {
-        fence_proxy_async_smem();
-        mbar_arrive_expect_tx(&sm.mbar, sizeof(sm.vwin));
-        const char* maps = static_cast<const char*>(c.tmaps);
-        tma_load_4d(sm.vwin, maps + 128 * scene, 0, tile[0] * kTile, tile[1] * kTile, tile[2] * kTile, &sm.mbar);
-        if (!mbar_wait_bounded(&sm.mbar, phase)) {
-          atomicOr(&ct->status, 0x8u);
-          mbar_wait_bounded(&sm.mbar, phase);  // give an in-flight copy a second bounded chance
-          sm.abort_flag = 1;
-        }
-      }
-      phase ^= 1u;
-    } else {
-      for (int i = threadIdx.x; i < kWinG * kWinG * kWinG; i += kBlock) {
-        const int x = tile[0] * kTile + i % kWinG, y = tile[1] * kTile + (i / kWinG) % kWinG,
-                  z = tile[2] * kTile + i / (kWinG * kWinG);
-        sm.vwin[i] = c.g.vel[sc.node_base + ((long long)z * sc.gdim[1] + y) * sc.gdim[0] + x];
-      }
-    }
-    __syncthreads();
-    if (sm.abort_flag) return;
-    const float dt = c.dt_scene[scene];
-    const float invH = sc.invH;
-    float wave_acc = 0.f, grad_acc = 0.f;
-    unsigned flags_acc = 0;
-    for (unsigned j0 = 0; j0 < it.z; j0 += kBlock) {
-      const unsigned j = j0 + threadIdx.x;
-      unsigned key = 0xffffffffu;
-      if (j < it.z) {
-        float wave = 0.f, grad = 0.f;
-        unsigned flags = 0;
-        const unsigned home = c.p.perm[it.y + j];
-        unsigned q[3] = {c.p.qx[home], c.p.qy[home], c.p.qz[home]};
-        float D[9];
-#pragma unroll
-        for (int e = 0; e < 9; ++e) D[e] = c.p.D[e * cap + home];
-        const float m = c.p.m[home], V = c.p.V[home];
-        const int mi = c.single_material ? sc.mat_base : c.p.mat[home];
-        const MaterialDev mt = c.mats[mi];
-        const bool pinned = c.has_pinned && c.p.pinned[home];
-        float ep = c.has_plastic ? c.p.ep[home] : 0.f;
-        float T = c.has_thermal ? c.p.T[home] : 0.f;
-        float v[3], C[9];
-        ConstitutiveOut co;
-        if (!pinned) {
-          int b[3];
-          float t[3], w[3][3];
-#pragma unroll
-          for (int a = 0; a < 3; ++a) {
-            stencil_axis(q[a], sc.dims[a], b[a], t[a]);
-            bspline_weights(t[a], w[a]);
-          }
-          const int l0 = b[0] - tile[0] * kTile, l1 = b[1] - tile[1] * kTile, l2 = b[2] - tile[2] * kTile;
-          // the sort key always places the stencil inside the staged window; if it ever does not,
-          // the particle reads the grid from global memory instead (and the step reports it)
-          const bool in_g = l0 >= 0 && l0 <= kWinG - 3 && l1 >= 0 && l1 <= kWinG - 3 && l2 >= 0 && l2 <= kWinG - 3;
-          if (!in_g) flags |= 0x20u;
-          // G2P (src/three/mpm.js:107-118): v = sum w v_i, C = sum w v_i (i - t)^T 4/h
-          float v0 = 0.f, v1 = 0.f, v2 = 0.f;
-          float c0 = 0.f, c1 = 0.f, c2 = 0.f, c3 = 0.f, c4 = 0.f, c5 = 0.f, c6 = 0.f, c7 = 0.f, c8 = 0.f;
-#pragma unroll
-          for (int kz = 0; kz < 3; ++kz) {
-            const float dz = static_cast<float>(kz) - t[2];
-#pragma unroll
-            for (int ky = 0; ky < 3; ++ky) {
-              const float dy = static_cast<float>(ky) - t[1];
-              const float wyz = w[1][ky] * w[2][kz];
-#pragma unroll
-              for (int kx = 0; kx < 3; ++kx) {
-                const float dx = static_cast<float>(kx) - t[0];
-                const float wt = w[0][kx] * wyz;
-                const float4 g =
-                    in_g ? sm.vwin[((l2 + kz) * kWinG + (l1 + ky)) * kWinG + (l0 + kx)]
-                         : c.g.vel[sc.node_base + ((long long)(b[2] + kz) * sc.gdim[1] + (b[1] + ky)) * sc.gdim[0] +
-                                   (b[0] + kx)];
-                const float a = wt * g.x, bb = wt * g.y, cc = wt * g.z;
-                v0 += a; v1 += bb; v2 += cc;
-                c0 += a * dx; c1 += a * dy; c2 += a * dz;
-                c3 += bb * dx; c4 += bb * dy; c5 += bb * dz;
-                c6 += cc * dx; c7 += cc * dy; c8 += cc * dz;
-              }
-            }
-          }
-          const float s4 = 4.f * invH;
-          v[0] = v0; v[1] = v1; v[2] = v2;
-          C[0] = c0 * s4; C[1] = c1 * s4; C[2] = c2 * s4;
-          C[3] = c3 * s4; C[4] = c4 * s4; C[5] = c5 * s4;
-          C[6] = c6 * s4; C[7] = c7 * s4; C[8] = c8 * s4;
-          // F <- (I + dt C) F in centred form: D <- D + dt C (I + D) (src/three/mpm.js:119-121)
-          float Dn[9];
-#pragma unroll
-          for (int a = 0; a < 3; ++a)
-#pragma unroll
-            for (int bcol = 0; bcol < 3; ++bcol)
-              Dn[a * 3 + bcol] = D[a * 3 + bcol] +
-                                 dt * (C[a * 3 + bcol] + C[a * 3 + 0] * D[0 * 3 + bcol] +
-                                       C[a * 3 + 1] * D[1 * 3 + bcol] + C[a * 3 + 2] * D[2 * 3 + bcol]);
-#pragma unroll
-          for (int e = 0; e < 9; ++e) D[e] = Dn[e];
-          // x += dt v (src/three/mpm.js:122), in fixed point, clamped into the box
-          const float s = dt * invH * kFixedOne;
-#pragma unroll
-          for (int a = 0; a < 3; ++a) {
-            long long qn = static_cast<long long>(q[a]) + __float2ll_rn(s * v[a]);
-            if (sc.clamp) {
-              qn = qn < (long long)sc.qlo[a] ? (long long)sc.qlo[a] : qn;
-              qn = qn > (long long)sc.qhi[a] ? (long long)sc.qhi[a] : qn;
-            } else {
-              const long long hi = (static_cast<long long>(sc.dims[a]) - 1) << kFracBits;
-              if (qn < 0 || qn > hi) flags |= 0x4u;
-              qn = qn < 0 ? 0 : (qn > hi ? hi : qn);
-            }
-            q[a] = static_cast<unsigned>(qn);
-          }
-          // return map / stress for the next P2G (src/three/mpm.js:126-131)
-          co = constitutive_update(mt, D, ep, T, V / m, true);
-          ep += co.dep;
-          T += co.dT;
-          c.p.qx[home] = q[0]; c.p.qy[home] = q[1]; c.p.qz[home] = q[2];
-          c.p.vx[home] = v[0]; c.p.vy[home] = v[1]; c.p.vz[home] = v[2];
-#pragma unroll
-          for (int e = 0; e < 9; ++e) {
-            c.p.C[e * cap + home] = C[e];
-            c.p.D[e * cap + home] = D[e];
-          }
-          if (c.has_plastic) c.p.ep[home] = ep;
-          if (c.has_thermal) c.p.T[home] = T;
-          if (co.dep > 0.f && mt.heat_per_work > 0.f) work_acc += static_cast<double>(co.dT) * m / mt.heat_per_work;
-        } else {
-          // pinned particles keep their state (src/three/mpm.js:108) but still scatter
-          v[0] = c.p.vx[home]; v[1] = c.p.vy[home]; v[2] = c.p.vz[home];
-#pragma unroll
-          for (int e = 0; e < 9; ++e) C[e] = c.p.C[e * cap + home];
-          float Dc[9];
-#pragma unroll
-          for (int e = 0; e < 9; ++e) Dc[e] = D[e];
-          co = constitutive_update(mt, Dc, ep, T, V / m, false);
-        }
-        if (SCATTER) scatter_particle(c, sc, sm, nxt, tile, q, m, V, v, C, co.tau, pinned, key);
-        if (SCATTER) c.p.key[home] = key;
-        cfl_terms(mt, D, v, C, m, V, co.Jm1, wave, grad);
-        flags |= state_flags(v, D, co.tau, co.Jm1);
-        flags_acc |= flags;
-        wave_acc = fmaxf(wave_acc, wave);
-        grad_acc = fmaxf(grad_acc, grad);
-      }
-      if (SCATTER) count_key(c, key);
-    }
-    block_reduce_item(c, scene, wave_acc, grad_acc, flags_acc, sm.red);
-    __syncthreads();
-    if (SCATTER) flush_window(c, sc, sm, nxt, tile);
-    __syncthreads();
-  }
-  // heat from plastic work: one FP64 atomic per CTA
-  double wsum = warp_sum_d(work_acc);
-  if ((threadIdx.x & 31) == 0) sm.work[threadIdx.x >> 5] = wsum;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double t = 0.0;
-    for (int w = 0; w < kBlock / 32; ++w) t += sm.work[w];
-    if (t != 0.0) atomicAdd(&ct->plastic_work, t);
-  }
-}
-
-void launch_p2g(const Ctx& c, cudaStream_t st, int grid_blocks) { k_p2g<<<grid_blocks, kBlock, 0, st>>>(c); }
-
-void launch_g2p2g(const Ctx& c, cudaStream_t st, int grid_blocks, bool scatter) {
-  if (scatter)
-    k_g2p2g<true><<<grid_blocks, kBlock, 0, st>>>(c);
-  else
-    k_g2p2g<false><<<grid_blocks, kBlock, 0, st>>>(c);
-}
-
-int g2p2g_blocks_per_sm(bool scatter) {
-  int n = 0;
-  if (scatter)
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_g2p2g<true>, kBlock, 0);
-  else
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_g2p2g<false>, kBlock, 0);
-  return n > 0 ? n : 1;
-}
-
-int p2g_blocks_per_sm() {
-  int n = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_p2g, kBlock, 0);
-  return n > 0 ? n : 1;
-}
 
 // ---------------------------------------------------------------------------------------------
 // FP64 ledger (src/simulation/mechanical-diagnostics.js:16-37, src/simulation/particle-health.js)

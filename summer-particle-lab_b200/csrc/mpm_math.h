@@ -17,8 +17,10 @@
 
 #if defined(__CUDACC__)
 #define MPM_HD __host__ __device__ __forceinline__
+#define MPM_NOINLINE static __host__ __device__ __noinline__
 #else
 #define MPM_HD inline
+#define MPM_NOINLINE static __attribute__((noinline))
 #endif
 
 namespace mpm {
@@ -118,6 +120,74 @@ MPM_HD Sym3 rotate_diag(const float U[9], const float d[3]) {
   return s;
 }
 
+// Product of two commuting symmetric matrices (polynomials in the same B): symmetric, 6 entries.
+MPM_HD Sym3 sym_mul(const Sym3& a, const Sym3& b) {
+  Sym3 r;
+  r.xx = a.xx * b.xx + a.xy * b.xy + a.xz * b.xz;
+  r.yy = a.xy * b.xy + a.yy * b.yy + a.yz * b.yz;
+  r.zz = a.xz * b.xz + a.yz * b.yz + a.zz * b.zz;
+  r.xy = a.xx * b.xy + a.xy * b.yy + a.xz * b.yz;
+  r.xz = a.xx * b.xz + a.xy * b.yz + a.xz * b.zz;
+  r.yz = a.xy * b.xz + a.yy * b.yz + a.yz * b.zz;
+  return r;
+}
+
+MPM_HD float sym_norm(const Sym3& a) {
+  return sqrtf(a.xx * a.xx + a.yy * a.yy + a.zz * a.zz + 2.f * (a.xy * a.xy + a.xz * a.xz + a.yz * a.yz));
+}
+
+// Number of power-series terms for a symmetric argument of Frobenius norm r (a bound on its
+// spectral radius) so that the truncation r^(n+1)/(n+1) stays below ~1e-8 r; 0 means "too large:
+// use the eigen-decomposition".
+constexpr float kSeriesMaxNorm = 0.15f;
+MPM_HD int series_terms(float r) {
+  return r <= 1e-3f ? 3 : r <= 1e-2f ? 4 : r <= 3e-2f ? 5 : r <= 6e-2f ? 6 : r <= 0.1f ? 8 : r <= kSeriesMaxNorm ? 10 : 0;
+}
+
+// Coefficient c_k of x^(k+1) in the series (Taylor coefficients, exact rationals):
+//   kind 0  log(1 + x)      = x - x^2/2 + x^3/3 - ...          c_k = (-1)^k / (k + 1)
+//   kind 1  sqrt(1 + x) - 1 = x/2 - x^2/8 + x^3/16 - ...       c_k = binom(1/2, k + 1)
+//   kind 2  exp(x) - 1      = x + x^2/2 + x^3/6 + ...          c_k = 1 / (k + 1)!
+MPM_HD constexpr double series_coeff(int kind, int k) {
+  if (kind == 0) return ((k & 1) ? -1.0 : 1.0) / (k + 1);
+  double c = 1.0;
+  if (kind == 1) {
+    for (int j = 0; j <= k; ++j) c *= (0.5 - j) / (j + 1);
+    return c;
+  }
+  for (int j = 1; j <= k + 1; ++j) c /= j;
+  return c;
+}
+
+// sum_{k=0..N-1} c_k B^(k+1) by Horner's scheme: B (c_0 I + B (c_1 I + ... + B c_(N-1) I)),
+// fully unrolled with compile-time coefficients
+template <int KIND, int N>
+MPM_HD Sym3 series_n(const Sym3& B) {
+  constexpr float last = static_cast<float>(series_coeff(KIND, N - 1));
+  Sym3 Q{last, last, last, 0.f, 0.f, 0.f};
+#pragma unroll
+  for (int k = N - 2; k >= 0; --k) {
+    Q = sym_mul(B, Q);
+    const float ck = static_cast<float>(series_coeff(KIND, k));
+    Q.xx += ck;
+    Q.yy += ck;
+    Q.zz += ck;
+  }
+  return sym_mul(B, Q);
+}
+
+template <int KIND>
+MPM_HD Sym3 matrix_series(const Sym3& B, int n) {
+  switch (n) {
+    case 3: return series_n<KIND, 3>(B);
+    case 4: return series_n<KIND, 4>(B);
+    case 5: return series_n<KIND, 5>(B);
+    case 6: return series_n<KIND, 6>(B);
+    case 8: return series_n<KIND, 8>(B);
+    default: return series_n<KIND, 10>(B);
+  }
+}
+
 // Per-material constants on the device (SI). See mpm_material in include/mpm_b200.h.
 struct MaterialDev {
   int model;
@@ -141,33 +211,13 @@ MPM_HD float hencky_strain(float beta) {
   return fmaxf(0.5f * log1pf(beta), -13.815510558f);
 }
 
-// Constitutive update of one particle after the F update, in place on D (= F - I):
-// models 4/5/10 run the J2 radial return (src/three/metal-plasticity.js:20-27,
-// src/three/thermal-plasticity.js:22-29) and give the Hencky stress of the returned state
-// (src/three/constitutive.js:81-86); models 0 and 1 give the elastic stress of F
-// (src/three/math.js:25-32, src/three/constitutive.js:94-100).
-// ep is the accumulated plastic strain, T the temperature; rho0 = m / V for the heat term.
-// With do_return false the J2 models give the stress of F without a return (the reference's
-// updateStress when no cached stress exists, src/three/mpm.js:36).
-MPM_HD ConstitutiveOut constitutive_update(const MaterialDev& mt, float D[9], float ep, float T,
-                                           float inv_rho0, bool do_return) {
+// Large-strain path (|B| > 0.15): Jacobi eigen-decomposition of B. Out of line so its registers do
+// not count against the series path that almost every particle takes.
+MPM_NOINLINE ConstitutiveOut constitutive_eigen(const MaterialDev& mt, const Sym3& B, float D[9], float ep,
+                                                float T, float inv_rho0, bool do_return) {
   ConstitutiveOut out;
   out.dep = 0.f;
   out.dT = 0.f;
-  const Sym3 B = cauchy_green_minus_identity(D);
-  if (mt.model == 1) {  // Neo-Hookean: mu (F F^T - I) + lambda log J I
-    const float Jm1 = det_minus_one(D);
-    const float J = 1.f + Jm1;
-    const float lj = J > 1e-6f ? log1pf(Jm1) : -13.815510558f;
-    out.tau.xx = mt.mu * B.xx + mt.lam * lj;
-    out.tau.yy = mt.mu * B.yy + mt.lam * lj;
-    out.tau.zz = mt.mu * B.zz + mt.lam * lj;
-    out.tau.xy = mt.mu * B.xy;
-    out.tau.xz = mt.mu * B.xz;
-    out.tau.yz = mt.mu * B.yz;
-    out.Jm1 = Jm1;
-    return out;
-  }
   float beta[3], U[9];
   sym_eig3(B, beta, U);
   if (mt.model == 0) {  // fixed-corotated: U diag(2 mu (s-1) s) U^T + lambda (J-1) J I
@@ -234,6 +284,105 @@ MPM_HD ConstitutiveOut constitutive_update(const MaterialDev& mt, float D[9], fl
   out.dep = dep;
   out.Jm1 = expm1f(tr);
   return out;
+}
+
+// Constitutive update of one particle after the F update, in place on D (= F - I):
+// models 4/5/10 run the J2 radial return (src/three/metal-plasticity.js:20-27,
+// src/three/thermal-plasticity.js:22-29) and give the Hencky stress of the returned state
+// (src/three/constitutive.js:81-86); models 0 and 1 give the elastic stress of F
+// (src/three/math.js:25-32, src/three/constitutive.js:94-100).
+// ep is the accumulated plastic strain, T the temperature; rho0 = m / V for the heat term.
+// With do_return false the J2 models give the stress of F without a return (the reference's
+// updateStress when no cached stress exists, src/three/mpm.js:36).
+MPM_HD ConstitutiveOut constitutive_update(const MaterialDev& mt, float D[9], float ep, float T,
+                                           float inv_rho0, bool do_return) {
+  ConstitutiveOut out;
+  out.dep = 0.f;
+  out.dT = 0.f;
+  const Sym3 B = cauchy_green_minus_identity(D);
+  if (mt.model == 1) {  // Neo-Hookean: mu (F F^T - I) + lambda log J I
+    const float Jm1 = det_minus_one(D);
+    const float J = 1.f + Jm1;
+    const float lj = J > 1e-6f ? log1pf(Jm1) : -13.815510558f;
+    out.tau.xx = mt.mu * B.xx + mt.lam * lj;
+    out.tau.yy = mt.mu * B.yy + mt.lam * lj;
+    out.tau.zz = mt.mu * B.zz + mt.lam * lj;
+    out.tau.xy = mt.mu * B.xy;
+    out.tau.xz = mt.mu * B.xz;
+    out.tau.yz = mt.mu * B.yz;
+    out.Jm1 = Jm1;
+    return out;
+  }
+  // Small strain (|B| <= 0.15): isotropic matrix functions of B by power series, no eigenvectors.
+  // fixed-corotated: V_l = sqrt(I + B), (F - R) F^T = (V_l - I) V_l;  Hencky: L = log(V_l) =
+  // log(I + B)/2, |dev e| = |dev L|_F, returned L' = tr L/3 I + scale dev L, and the return
+  // F' = U diag(s'/s) U^T F = exp((scale - 1) dev L) F.
+  const int nt = series_terms(sym_norm(B));
+  if (nt > 0) {
+    if (mt.model == 0) {
+      const Sym3 S1 = matrix_series<1>(B, nt);  // sqrt(I + B) - I
+      const Sym3 S2 = sym_mul(S1, S1);
+      const float Jm1 = det_minus_one(D);
+      const float vol = mt.lam * Jm1 * (1.f + Jm1);
+      const float m2 = 2.f * mt.mu;
+      out.tau.xx = m2 * (S1.xx + S2.xx) + vol;
+      out.tau.yy = m2 * (S1.yy + S2.yy) + vol;
+      out.tau.zz = m2 * (S1.zz + S2.zz) + vol;
+      out.tau.xy = m2 * (S1.xy + S2.xy);
+      out.tau.xz = m2 * (S1.xz + S2.xz);
+      out.tau.yz = m2 * (S1.yz + S2.yz);
+      out.Jm1 = Jm1;
+      return out;
+    }
+    Sym3 L = matrix_series<0>(B, nt);  // log(I + B) = 2 log V_l
+    L.xx *= 0.5f; L.yy *= 0.5f; L.zz *= 0.5f; L.xy *= 0.5f; L.xz *= 0.5f; L.yz *= 0.5f;
+    const float trL = L.xx + L.yy + L.zz;
+    const float tr3 = trL * (1.f / 3.f);
+    Sym3 dv = L;
+    dv.xx -= tr3; dv.yy -= tr3; dv.zz -= tr3;
+    const float len = sym_norm(dv);
+    const float J = fmaxf(1e-6f, expf(trL));
+    const float q = 2.449489742783178f * mt.mu * len / J;
+    float soft = 1.f;
+    if (mt.model == 10) {
+      const float theta = fminf(1.f, fmaxf(0.f, (T - mt.T_ref) * mt.inv_T_span));
+      soft = 1.f - (1.f - mt.hot_ratio) * theta;
+    }
+    const float yield = (mt.yield_stress + (mt.model == 4 ? 0.f : mt.hardening * ep)) * soft;
+    float dep = 0.f, scale = 1.f;
+    if (do_return && q > yield) {
+      const float hard = mt.model == 4 ? 0.f : mt.hardening * soft;
+      dep = (q - yield) / (3.f * mt.mu / J + hard);
+      scale = fmaxf(0.f, 1.f - 1.224744871391589f * dep / fmaxf(len, 1e-20f));
+      const float g = scale - 1.f;
+      const Sym3 M{g * dv.xx, g * dv.yy, g * dv.zz, g * dv.xy, g * dv.xz, g * dv.yz};
+      const int nm = series_terms(sym_norm(M));
+      const Sym3 E = matrix_series<2>(M, nm > 0 ? nm : 10);  // exp(M) - I
+      float Dn[9];
+#pragma unroll
+      for (int b = 0; b < 3; ++b) {
+        Dn[0 * 3 + b] = E.xx * D[0 * 3 + b] + E.xy * D[1 * 3 + b] + E.xz * D[2 * 3 + b];
+        Dn[1 * 3 + b] = E.xy * D[0 * 3 + b] + E.yy * D[1 * 3 + b] + E.yz * D[2 * 3 + b];
+        Dn[2 * 3 + b] = E.xz * D[0 * 3 + b] + E.yz * D[1 * 3 + b] + E.zz * D[2 * 3 + b];
+      }
+      D[0] += Dn[0] + E.xx; D[1] += Dn[1] + E.xy; D[2] += Dn[2] + E.xz;
+      D[3] += Dn[3] + E.xy; D[4] += Dn[4] + E.yy; D[5] += Dn[5] + E.yz;
+      D[6] += Dn[6] + E.xz; D[7] += Dn[7] + E.yz; D[8] += Dn[8] + E.zz;
+      out.dT = mt.heat_per_work * 2.449489742783178f * mt.mu * scale * len * dep * inv_rho0;
+    }
+    const float m2s = 2.f * mt.mu * scale;
+    const float iso = 2.f * mt.mu * tr3 + mt.lam * trL;
+    out.tau.xx = m2s * dv.xx + iso;
+    out.tau.yy = m2s * dv.yy + iso;
+    out.tau.zz = m2s * dv.zz + iso;
+    out.tau.xy = m2s * dv.xy;
+    out.tau.xz = m2s * dv.xz;
+    out.tau.yz = m2s * dv.yz;
+    out.dep = dep;
+    out.Jm1 = expm1f(trL);
+    return out;
+  }
+  return constitutive_eigen(mt, B, D, ep, T, inv_rho0, do_return);
 }
 
 }  // namespace mpm

@@ -43,7 +43,7 @@ def run_pair(scene, dt, steps, capacity=None):
     return sol, st
 
 
-def small_j2_scene(v0=-20.0, model=5, grid=32, block=(12, 6, 12), seed=7):
+def small_j2_scene(v0=-60.0, model=5, grid=32, block=(12, 6, 12), seed=7):
     d = scenes.Domain(lower=(0, 0, 0), upper=(1, 1, 1), H=1 / grid, gravity=(0, -9.8, 0), sticky_floor=True)
     mat = scenes.aluminium_j2(model)
     x = scenes.block_particles(d, (10, 1, 10), (10 + block[0], 1 + block[1], 10 + block[2]), seed)
@@ -145,7 +145,7 @@ def test_elastic_cube_fifty_steps_positions():
 
 def test_j2_plastic_one_step_and_ten_steps():
     sc = small_j2_scene()
-    dt = 2e-7
+    dt = 1e-6
     sol = Solver(sc.domain, sc.n)
     sol.upload(sc)
     st = orc.state_from_scene(sc)
@@ -165,9 +165,9 @@ def test_j2_plastic_one_step_and_ten_steps():
 
 
 def test_thermal_j2_with_plastic_heating():
-    sc = scenes.thermal_j2(grid=32, block=10)
-    dt = 2e-7
-    sol, st = run_pair(sc, dt, 5)
+    sc = scenes.thermal_j2(grid=32, block=10, v0=-60.0)
+    dt = 1e-6
+    sol, st = run_pair(sc, dt, 10)
     out = sol.download()
     assert np.max(st.ep) > 0
     assert np.max(np.abs(out["x"] - st.x)) <= 1e-6

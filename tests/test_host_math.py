@@ -105,3 +105,53 @@ def test_small_strain_precision_of_centred_form(harness):
     for i in range(F.shape[0]):
         ref = orc.constitutive_stress(F[i], 5, mu, lam)
         np.testing.assert_allclose(tau[i], ref, atol=2e-5 * np.max(np.abs(ref)), rtol=0)
+
+
+def b_norm(F):
+    Fm = F.reshape(-1, 3, 3)
+    B = Fm @ Fm.transpose(0, 2, 1) - np.eye(3)
+    return np.sqrt(np.sum(B * B, axis=(1, 2)))
+
+
+@pytest.mark.parametrize("scale", [3e-4, 3e-3, 1e-2, 2.5e-2, 0.2])
+def test_series_and_eigen_paths_match_oracle_j2(harness, scale):
+    """|B| <= 0.15 runs the matrix-series path, larger strains the Jacobi path; both match the
+    oracle's SVD-based return map (reference units, yield strain lowered so small strains yield)."""
+    F = random_F(400, scale, 31)
+    A = 0.002
+    Fo, dep, tau = run(harness, 5, F, .01, 20, A=A, B=.08)
+    mat = orc.material(5, plasticity=dict(A=A, B=.08))
+    series = b_norm(F) <= 0.15
+    assert series.all() if scale <= 1e-2 else True
+    n_yield = 0
+    for i in range(F.shape[0]):
+        Fr, inc, tr = orc.project(F[i], mat, ep=.01, dt=.01, T=20)
+        np.testing.assert_allclose(Fo[i], Fr, atol=4e-6, rtol=4e-5)
+        assert abs(dep[i] - inc) < 1e-5 * max(1.0, inc)
+        np.testing.assert_allclose(tau[i], tr, atol=3e-6 * max(1.0, np.max(np.abs(tr))), rtol=5e-4)
+        n_yield += inc > 0
+    if scale >= 3e-3:
+        assert n_yield > 20
+
+
+@pytest.mark.parametrize("scale", [3e-4, 1e-2, 4e-2, 0.2])
+def test_series_and_eigen_paths_fixed_corotated(harness, scale):
+    F = random_F(300, scale, 37)
+    _, _, tau = run(harness, 0, F, 0, 0, mu=400, lam=300)
+    for i in range(F.shape[0]):
+        ref = orc.constitutive_stress(F[i], 0, 400, 300)
+        np.testing.assert_allclose(tau[i], ref, atol=2e-5 * np.max(np.abs(ref)) + 1e-9, rtol=0)
+
+
+def test_thermal_series_path_with_softening(harness):
+    F = random_F(300, 8e-3, 41)
+    T = np.linspace(0, 400, 300)
+    Fo, dep, tau = run(harness, 10, F, .02, T, A=.004, B=.04)
+    mat = orc.material(10, thermal=dict(A=.004, H=.04))
+    n_yield = 0
+    for i in range(F.shape[0]):
+        Fr, inc, tr = orc.project(F[i], mat, ep=.02, dt=.01, T=T[i])
+        np.testing.assert_allclose(Fo[i], Fr, atol=4e-6, rtol=5e-5)
+        assert abs(dep[i] - inc) < 1e-5
+        n_yield += inc > 0
+    assert n_yield > 20
