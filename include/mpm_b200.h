@@ -207,6 +207,25 @@ int mpm_return_map_batch(const mpm_material* material, int64_t n, const double* 
                          const double* ep, const double* T, double dt, double* F_out,
                          double* dep, double* tau);
 
+/* ---- allocation-free particle-to-grid transfer ----
+ * No counterpart in the reference. For callers that cannot allocate device memory themselves: a
+ * host that owns every device byte through its own pool and passes this library only buffers it
+ * already holds, or code running where cudaMalloc is not allowed. Scatters caller-owned device
+ * particle arrays onto the domain's grid (stress from F without a return, like the first P2G of an
+ * uploaded state) and writes, for every node in ((z*ny)+y)*nx+x order, the mass (nx*ny*nz doubles)
+ * and the momentum including dt * (stress force + m g) (3*nx*ny*nz doubles): the values
+ * mpm_grid_debug returns for the same state. Device pointers: x (n x 3) and F (n x 9 row-major)
+ * double; v (n x 3), C (n x 9), m and V float.
+ * The intermediate grid lives in one fixed device array of 262,144 nodes (8 MiB) that every GPU
+ * which loads the library holds until the process exits; larger grids return MPM_ERR_CAPACITY.
+ * The call allocates and frees no device memory. Its first call on a device looks up that array's
+ * device address once (make this first call before any stream capture). Every call reuses the same
+ * array and clears the nodes it needs first; calls that overlap on the GPU race on it.
+ * Launches on `stream` (NULL: the default stream) and returns without waiting. */
+int mpm_p2g_noalloc(const mpm_domain* domain, const mpm_material* material, int64_t n, const double* x,
+                    const float* v, const double* F, const float* C, const float* m, const float* V,
+                    double dt, double* mass, double* momentum, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -86,6 +86,8 @@ SIGNATURES = {
     "mpm_host_alloc": (ctypes.c_int, [ctypes.c_size_t, ctypes.POINTER(_P)]),
     "mpm_host_free": (ctypes.c_int, [_P]),
     "mpm_return_map_batch": (ctypes.c_int, [ctypes.POINTER(MpmMaterial), _I64, _P, _P, _P, _D, _P, _P, _P]),
+    "mpm_p2g_noalloc": (ctypes.c_int, [ctypes.POINTER(MpmDomain), ctypes.POINTER(MpmMaterial), _I64, _P, _P, _P, _P, _P,
+                                        _P, _D, _P, _P, _P]),
 }
 
 _lib = None
