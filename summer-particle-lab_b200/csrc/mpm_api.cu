@@ -23,7 +23,7 @@ namespace {
 
 constexpr int kMaxMats = 256;
 constexpr uint32_t kCheckpointMagic = 0x3242504du;  // "MPB2"
-constexpr uint32_t kCheckpointVersion = 1;
+constexpr uint32_t kCheckpointVersion = 2;  // 2: home-slot id array saved
 
 size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
@@ -72,7 +72,13 @@ struct mpm_handle {
   int use_tma = 1;
   int last_estimate = 0;
   // device memory
-  void* pblock = nullptr;  size_t pblock_bytes = 0;   // particle arrays
+  void* pblock = nullptr;  size_t pblock_bytes = 0;   // particle arrays (current home order)
+  void* pblock_alt = nullptr;                           // the other buffer of the permutation pass
+  void* sblock = nullptr;                               // key and perm (shared by both buffers)
+  mpm::Particles palt{};
+  bool reorder_pending = false;   // permute into tile order at the next grid preparation
+  int reorder_interval = 32;      // substeps between permutation passes (0: only at upload)
+  int64_t substeps_since_reorder = 0;
   void* gblock = nullptr;  size_t gblock_bytes = 0;   // grid + sort + control
   void* snap = nullptr;    bool snap_valid = false;  int64_t snap_n = 0;
   void* staging = nullptr; size_t staging_bytes = 0;
@@ -188,6 +194,9 @@ static int build_scene(mpm_handle* h, const mpm_domain& d, SceneDev& s) {
 
 static int free_device(mpm_handle* h) {
   if (h->pblock) cudaFree(h->pblock);
+  if (h->pblock_alt) cudaFree(h->pblock_alt);
+  if (h->sblock) cudaFree(h->sblock);
+  h->pblock_alt = h->sblock = nullptr;
   if (h->gblock) cudaFree(h->gblock);
   if (h->snap) cudaFree(h->snap);
   if (h->staging) cudaFree(h->staging);
@@ -218,10 +227,22 @@ static size_t carve_particles(char* base, int64_t cap, mpm::Particles& p) {
   p.ep = c.take<float>(cap); p.T = c.take<float>(cap);
   p.mat = c.take<unsigned short>(cap);
   p.pinned = c.take<unsigned char>(cap);
-  p.key = c.take<unsigned>(cap);
-  p.perm = c.take<unsigned>(cap);
+  p.id = c.take<unsigned>(cap);
   p.cap = cap;
   return align_up(c.off, 256);
+}
+
+// Permutation pass: rewrite the state in sort order into the other buffer and make it current.
+static int permute_state(mpm_handle* h) {
+  h->ctx.n = h->n;
+  mpm::launch_permute(h->ctx, h->palt, h->stream);
+  MPM_CUDA(h, cudaGetLastError());
+  std::swap(h->pblock, h->pblock_alt);
+  mpm::Particles cur = h->palt;
+  h->palt = h->ctx.p;
+  h->ctx.p = cur;
+  h->substeps_since_reorder = 0;
+  return MPM_OK;
 }
 
 static int alloc_grid(mpm_handle* h) {
@@ -342,7 +363,13 @@ static int prepare_grid(mpm_handle* h) {
   { ProfScope ps(h, 6); mpm::launch_keys(c, h->stream); }
   { ProfScope ps(h, 3); mpm::launch_scan(c, h->stream); }
   { ProfScope ps(h, 4); mpm::launch_sort_scatter(c, h->stream, true); }
-  { ProfScope ps(h, 5); mpm::launch_p2g(c, h->stream, h->p2g_blocks); }
+  if (h->reorder_pending) {
+    ProfScope ps(h, -1);
+    const int rc = permute_state(h);
+    if (rc != MPM_OK) return rc;
+    h->reorder_pending = false;
+  }
+  { ProfScope ps(h, 5); mpm::launch_p2g(h->ctx, h->stream, h->p2g_blocks); }
   MPM_CUDA(h, cudaGetLastError());
   h->grid_valid = true;
   h->pending_grid = true;
@@ -457,9 +484,15 @@ int mpm_create(const mpm_domain* domain, int64_t capacity, mpm_handle** out) {
     return code;
   };
   if (cudaMalloc(&h->pblock, pbytes) != cudaSuccess) return bail(MPM_ERR_OUT_OF_MEMORY);
+  if (cudaMalloc(&h->pblock_alt, pbytes) != cudaSuccess) return bail(MPM_ERR_OUT_OF_MEMORY);
+  if (cudaMalloc(&h->sblock, 2 * capacity * sizeof(unsigned) + 512) != cudaSuccess) return bail(MPM_ERR_OUT_OF_MEMORY);
   h->pblock_bytes = pbytes;
   carve_particles(static_cast<char*>(h->pblock), capacity, h->ctx.p);
+  carve_particles(static_cast<char*>(h->pblock_alt), capacity, h->palt);
+  h->ctx.p.key = h->palt.key = static_cast<unsigned*>(h->sblock);
+  h->ctx.p.perm = h->palt.perm = static_cast<unsigned*>(h->sblock) + align_up(capacity, 64);
   if (cudaMemsetAsync(h->pblock, 0, pbytes, h->stream) != cudaSuccess) return bail(MPM_ERR_CUDA);
+  if (cudaMemsetAsync(h->pblock_alt, 0, pbytes, h->stream) != cudaSuccess) return bail(MPM_ERR_CUDA);
   if (cudaMalloc(reinterpret_cast<void**>(&h->dptr_table), 16 * sizeof(void*)) != cudaSuccess) return bail(MPM_ERR_OUT_OF_MEMORY);
   if (cudaMallocHost(reinterpret_cast<void**>(&h->host_ctrl), sizeof(mpm::Ctrl)) != cudaSuccess) return bail(MPM_ERR_OUT_OF_MEMORY);
   if (cudaMallocHost(reinterpret_cast<void**>(&h->host_ledger), 32 * sizeof(double)) != cudaSuccess) return bail(MPM_ERR_OUT_OF_MEMORY);
@@ -647,13 +680,14 @@ int mpm_upload_particles(mpm_handle* h, int64_t n, const mpm_particles* p) {
   MPM_CUDA(h, cudaMemcpyAsync(const_cast<SceneDev*>(h->ctx.scenes), &tmp, sizeof(SceneDev), cudaMemcpyHostToDevice, h->stream));
   { ProfScope ps(h, -1);
     mpm::launch_upload_convert(h->ctx, h->stream, n, p->dtype, reinterpret_cast<const void* const*>(h->dptr_table), mat_dev,
-                               pin_dev, all); }
+                               pin_dev, all, false); }
   MPM_CUDA(h, cudaGetLastError());
   MPM_CUDA(h, cudaMemcpyAsync(const_cast<SceneDev*>(h->ctx.scenes), &h->scene, sizeof(SceneDev), cudaMemcpyHostToDevice,
                               h->stream));
   h->n = n;
   h->uploaded = true;
   h->grid_valid = false;
+  h->reorder_pending = true;
   MPM_CUDA(h, cudaStreamSynchronize(h->stream));
   return MPM_OK;
 }
@@ -768,7 +802,15 @@ static int run_substeps(mpm_handle* h, int mode, double dt_req, int max_substeps
     est = max_substeps;
   }
   while (true) {
-    for (int i = 0; i < est; ++i) launch_substep(h, true);
+    for (int i = 0; i < est; ++i) {
+      launch_substep(h, true);
+      // keep tiles contiguous in memory: a permutation pass after every reorder_interval substeps
+      if (h->reorder_interval > 0 && ++h->substeps_since_reorder >= h->reorder_interval) {
+        ProfScope ps(h, -1);
+        const int rc = permute_state(h);
+        if (rc != MPM_OK) return rc;
+      }
+    }
     launched += est;
     MPM_CUDA(h, cudaGetLastError());
     MPM_CUDA(h, cudaMemcpyAsync(h->host_ctrl, h->ctx.ctrl, sizeof(mpm::Ctrl), cudaMemcpyDeviceToHost, h->stream));
@@ -825,7 +867,7 @@ int mpm_step_host(mpm_handle* h, const mpm_particles* io, double dt) {
   if (rc != MPM_OK) return rc;
   { ProfScope ps(h, -1);
     mpm::launch_upload_convert(h->ctx, h->stream, n, io->dtype, reinterpret_cast<const void* const*>(h->dptr_table), nullptr,
-                               nullptr, fields); }
+                               nullptr, fields, true); }
   MPM_CUDA(h, cudaGetLastError());
   rc = prepare_grid(h);
   if (rc != MPM_OK) return rc;
@@ -860,7 +902,7 @@ int mpm_frame_host(mpm_handle* h, const mpm_particles* io, double dt_requested, 
   if (rc != MPM_OK) return rc;
   { ProfScope ps(h, -1);
     mpm::launch_upload_convert(h->ctx, h->stream, n, io->dtype, reinterpret_cast<const void* const*>(h->dptr_table), nullptr,
-                               nullptr, fields); }
+                               nullptr, fields, true); }
   MPM_CUDA(h, cudaGetLastError());
   h->grid_valid = false;
   rc = mpm_step(h, dt_requested, max_substeps, substeps, nullptr);
@@ -1023,7 +1065,7 @@ int mpm_checkpoint_save(mpm_handle* h, const char* path) {
   const mpm::Particles& p = h->ctx.p;
   struct Arr { const void* d; size_t es; int comps; } arrs[] = {
       {p.qx, 4, 1}, {p.qy, 4, 1}, {p.qz, 4, 1}, {p.vx, 4, 1}, {p.vy, 4, 1}, {p.vz, 4, 1}, {p.C, 4, 9}, {p.D, 4, 9},
-      {p.m, 4, 1}, {p.V, 4, 1}, {p.ep, 4, 1}, {p.T, 4, 1}, {p.mat, 2, 1}, {p.pinned, 1, 1}};
+      {p.m, 4, 1}, {p.V, 4, 1}, {p.ep, 4, 1}, {p.T, 4, 1}, {p.mat, 2, 1}, {p.pinned, 1, 1}, {p.id, 4, 1}};
   std::vector<char> buf;
   cudaStreamSynchronize(h->stream);
   for (const Arr& a : arrs) {
@@ -1071,7 +1113,7 @@ int mpm_checkpoint_load(mpm_handle* h, const char* path) {
   const mpm::Particles& p = h->ctx.p;
   struct Arr { void* d; size_t es; int comps; } arrs[] = {
       {p.qx, 4, 1}, {p.qy, 4, 1}, {p.qz, 4, 1}, {p.vx, 4, 1}, {p.vy, 4, 1}, {p.vz, 4, 1}, {p.C, 4, 9}, {p.D, 4, 9},
-      {p.m, 4, 1}, {p.V, 4, 1}, {p.ep, 4, 1}, {p.T, 4, 1}, {p.mat, 2, 1}, {p.pinned, 1, 1}};
+      {p.m, 4, 1}, {p.V, 4, 1}, {p.ep, 4, 1}, {p.T, 4, 1}, {p.mat, 2, 1}, {p.pinned, 1, 1}, {p.id, 4, 1}};
   std::vector<char> buf;
   cudaStreamSynchronize(h->stream);
   for (const Arr& a : arrs) {

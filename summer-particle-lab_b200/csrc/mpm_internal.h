@@ -9,7 +9,10 @@
 //              m, V      f32 mass, reference volume (read-only in the step)
 //              ep, T     f32 plastic strain, temperature
 //              mat       u16 material index, pinned u8 (read only when the scene needs them)
+//              id        u32 caller's index of the particle held in this slot
 //              key       u32 particle-tile key for the next counting sort, perm u32 sorted->home
+//   The particle arrays are double-buffered: a permutation pass rewrites the state in tile order
+//   (home order = sort order) at upload and periodically, so tiles read contiguous memory.
 //   grid       acc0[2]   float4 (m, px, py, pz)  scatter accumulators, ping-pong by substep
 //              acc1[2]   float4 (fx, fy, fz, pinned mass)  stress force (dt-free) channel
 //              vel       float4 (vx, vy, vz, m) updated grid velocity, TMA source of the gather
@@ -88,8 +91,9 @@ struct Particles {
   float *m, *V, *ep, *T;
   unsigned short* mat;
   unsigned char* pinned;
-  unsigned* key;
-  unsigned* perm;
+  unsigned* id;     // caller's index of the particle in this home slot
+  unsigned* key;    // shared by both particle buffers
+  unsigned* perm;   // shared by both particle buffers
   long long cap;
 };
 
@@ -144,9 +148,10 @@ void launch_g2p2g(const Ctx& c, cudaStream_t st, int grid_blocks, bool scatter);
 void launch_ledger(const Ctx& c, cudaStream_t st, double* partials, int blocks, double* out);
 void launch_grid_debug(const Ctx& c, cudaStream_t st, int scene, float dt, double* mass, double* mom);
 void launch_upload_convert(const Ctx& c, cudaStream_t st, long long n, int dtype, const void* const* src,
-                           const int* material, const unsigned char* pinned, unsigned fields);
+                           const int* material, const unsigned char* pinned, unsigned fields, bool by_id);
 void launch_download_convert(const Ctx& c, cudaStream_t st, long long n, int dtype, void* const* dst,
                              unsigned fields);
+void launch_permute(const Ctx& c, const Particles& dst, cudaStream_t st);
 void launch_return_map_batch(const MaterialDev& m, long long n, const double* F_in, const double* ep,
                              const double* T, float dt, double* F_out, double* dep, double* tau,
                              cudaStream_t st);

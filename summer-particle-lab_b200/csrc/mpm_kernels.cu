@@ -470,6 +470,17 @@ constexpr unsigned kMetaInvalid = 0x80000000u;
 
 enum Pass : int { kPassP2G = 0, kPassG2P2G = 1, kPassG2P = 2 };
 
+// Per-tile constants copied out of the scene table (kept in shared memory for the whole tile).
+struct TileCtx {
+  int tile[3];
+  int dims[3];
+  int gdim[3];
+  unsigned qlo[3], qhi[3];
+  long long node_base;
+  float H, invH;
+  int clamp;
+};
+
 struct __align__(128) PartSmem {
   float4 vwin[2][kWinG * kWinG * kWinG];  // double-buffered TMA destinations (3456 B each)
   float acc[kChannels * kWinSNodes];      // 16 KiB scatter window
@@ -485,20 +496,11 @@ struct __align__(128) PartSmem {
   int abort_flag;
   unsigned red[3 * (kBlock / 32)];
   double work[kBlock / 32];
+  TileCtx tc;
+  MaterialDev mt;
 };
 
 size_t particle_smem_bytes() { return sizeof(PartSmem); }
-
-// Per-tile constants copied out of the scene table into registers.
-struct TileCtx {
-  int tile[3];
-  int dims[3];
-  int gdim[3];
-  unsigned qlo[3], qhi[3];
-  long long node_base;
-  float H, invH;
-  int clamp;
-};
 
 // Direct global scatter (rare: particles that left the window, pinned particles): 27 nodes x
 // channel atomics straight to the accumulators, and the node tiles they touch become active.
@@ -682,33 +684,47 @@ __device__ __forceinline__ void scan_buckets(PartSmem& sm) {
 
 
 // Weighted gather of the 27 stencil nodes: out = (v, C / (4/h)) with v = sum w v_i and
-// C_ab = sum w v_i,a (i - t)_b (src/three/mpm.js:110-117). ld(kz, ky, kx) returns the node velocity.
+// C_ab = sum w v_i,a (i - t)_b (src/three/mpm.js:110-117). The tensor-product weights are contracted
+// one axis at a time (x, then y, then z), which needs about 280 FMAs instead of 430.
+// ld(kz, ky, kx) returns the node velocity.
 template <typename Ld>
 __device__ __forceinline__ void gather27(Ld ld, const float t[3], const float w[3][3], float out[12]) {
+  const float dx[3] = {-t[0], 1.f - t[0], 2.f - t[0]};
+  const float dy[3] = {-t[1], 1.f - t[1], 2.f - t[1]};
+  const float dz[3] = {-t[2], 1.f - t[2], 2.f - t[2]};
+  const float wxd[3] = {w[0][0] * dx[0], w[0][1] * dx[1], w[0][2] * dx[2]};
   float v0 = 0.f, v1 = 0.f, v2 = 0.f;
-  float c0 = 0.f, c1 = 0.f, c2 = 0.f, c3 = 0.f, c4 = 0.f, c5 = 0.f, c6 = 0.f, c7 = 0.f, c8 = 0.f;
+  float cx0 = 0.f, cx1 = 0.f, cx2 = 0.f, cy0 = 0.f, cy1 = 0.f, cy2 = 0.f, cz0 = 0.f, cz1 = 0.f, cz2 = 0.f;
 #pragma unroll
   for (int kz = 0; kz < 3; ++kz) {
-    const float dz = static_cast<float>(kz) - t[2];
+    float s00 = 0.f, s01 = 0.f, s02 = 0.f;  // sum_y wy r0
+    float s10 = 0.f, s11 = 0.f, s12 = 0.f;  // sum_y wy r1
+    float s20 = 0.f, s21 = 0.f, s22 = 0.f;  // sum_y wy dy r0
 #pragma unroll
     for (int ky = 0; ky < 3; ++ky) {
-      const float dy = static_cast<float>(ky) - t[1];
-      const float wyz = w[1][ky] * w[2][kz];
+      float r00 = 0.f, r01 = 0.f, r02 = 0.f, r10 = 0.f, r11 = 0.f, r12 = 0.f;
 #pragma unroll
       for (int kx = 0; kx < 3; ++kx) {
-        const float dx = static_cast<float>(kx) - t[0];
-        const float wt = w[0][kx] * wyz;
         const float4 g = ld(kz, ky, kx);
-        const float ga = wt * g.x, gb = wt * g.y, gc = wt * g.z;
-        v0 += ga; v1 += gb; v2 += gc;
-        c0 += ga * dx; c1 += ga * dy; c2 += ga * dz;
-        c3 += gb * dx; c4 += gb * dy; c5 += gb * dz;
-        c6 += gc * dx; c7 += gc * dy; c8 += gc * dz;
+        r00 = fmaf(w[0][kx], g.x, r00); r01 = fmaf(w[0][kx], g.y, r01); r02 = fmaf(w[0][kx], g.z, r02);
+        r10 = fmaf(wxd[kx], g.x, r10); r11 = fmaf(wxd[kx], g.y, r11); r12 = fmaf(wxd[kx], g.z, r12);
       }
+      const float wy = w[1][ky], wyd = wy * dy[ky];
+      s00 = fmaf(wy, r00, s00); s01 = fmaf(wy, r01, s01); s02 = fmaf(wy, r02, s02);
+      s10 = fmaf(wy, r10, s10); s11 = fmaf(wy, r11, s11); s12 = fmaf(wy, r12, s12);
+      s20 = fmaf(wyd, r00, s20); s21 = fmaf(wyd, r01, s21); s22 = fmaf(wyd, r02, s22);
     }
+    const float wz = w[2][kz], wzd = wz * dz[kz];
+    v0 = fmaf(wz, s00, v0); v1 = fmaf(wz, s01, v1); v2 = fmaf(wz, s02, v2);
+    cx0 = fmaf(wz, s10, cx0); cx1 = fmaf(wz, s11, cx1); cx2 = fmaf(wz, s12, cx2);
+    cy0 = fmaf(wz, s20, cy0); cy1 = fmaf(wz, s21, cy1); cy2 = fmaf(wz, s22, cy2);
+    cz0 = fmaf(wzd, s00, cz0); cz1 = fmaf(wzd, s01, cz1); cz2 = fmaf(wzd, s02, cz2);
   }
+  // out[3 + 3a + b] = C_ab (velocity component a, offset axis b)
   out[0] = v0; out[1] = v1; out[2] = v2;
-  out[3] = c0; out[4] = c1; out[5] = c2; out[6] = c3; out[7] = c4; out[8] = c5; out[9] = c6; out[10] = c7; out[11] = c8;
+  out[3] = cx0; out[4] = cy0; out[5] = cz0;
+  out[6] = cx1; out[7] = cy1; out[8] = cz1;
+  out[9] = cx2; out[10] = cy2; out[11] = cz2;
 }
 
 // Gather straight from global memory (a particle whose stencil is outside the staged window).
@@ -773,7 +789,6 @@ __global__ void __launch_bounds__(kBlock, 2) k_particles(const __grid_constant__
     // The next work item is claimed, and its velocity window requested, by thread 0 after phase A
     // of this tile's first round, so the two dependent global round trips overlap other warps' work.
     auto prefetch_next = [&]() {
-      if (threadIdx.x != 0) return;
       const unsigned idx = atomicAdd(&ct->work_next, 1u);
       const uint4 nx = idx < ct->work_count[lst] ? c.s.work[lst][idx] : make_uint4(0xffffffffu, 0, 0, 0);
       sm.item[cb ^ 1] = nx;
@@ -789,37 +804,40 @@ __global__ void __launch_bounds__(kBlock, 2) k_particles(const __grid_constant__
     };
     const int scene = static_cast<int>(it.w);
     const SceneDev& sc = c.scenes[scene];
-    TileCtx tc;
-    {
+    if (threadIdx.x == 0) {  // per-tile constants, computed once and read from shared memory
+      TileCtx tl;
       const int lt = static_cast<int>(it.x) - sc.tile_base;
-      tc.tile[0] = lt % sc.tiles[0];
-      tc.tile[1] = (lt / sc.tiles[0]) % sc.tiles[1];
-      tc.tile[2] = lt / (sc.tiles[0] * sc.tiles[1]);
+      tl.tile[0] = lt % sc.tiles[0];
+      tl.tile[1] = (lt / sc.tiles[0]) % sc.tiles[1];
+      tl.tile[2] = lt / (sc.tiles[0] * sc.tiles[1]);
 #pragma unroll
       for (int a = 0; a < 3; ++a) {
-        tc.dims[a] = sc.dims[a];
-        tc.gdim[a] = sc.gdim[a];
-        tc.qlo[a] = sc.qlo[a];
-        tc.qhi[a] = sc.qhi[a];
+        tl.dims[a] = sc.dims[a];
+        tl.gdim[a] = sc.gdim[a];
+        tl.qlo[a] = sc.qlo[a];
+        tl.qhi[a] = sc.qhi[a];
       }
-      tc.node_base = sc.node_base;
-      tc.H = sc.H;
-      tc.invH = sc.invH;
-      tc.clamp = sc.clamp;
-    }
-    if (GATHER && !use_tma) {
-      for (int i = threadIdx.x; i < kWinG * kWinG * kWinG; i += kBlock) {
-        const int x = tc.tile[0] * kTile + i % kWinG, y = tc.tile[1] * kTile + (i / kWinG) % kWinG,
-                  z = tc.tile[2] * kTile + i / (kWinG * kWinG);
-        sm.vwin[cb][i] = c.g.vel[tc.node_base + ((long long)z * tc.gdim[1] + y) * tc.gdim[0] + x];
-      }
+      tl.node_base = sc.node_base;
+      tl.H = sc.H;
+      tl.invH = sc.invH;
+      tl.clamp = sc.clamp;
+      sm.tc = tl;
+      if (c.single_material) sm.mt = c.mats[sc.mat_base];
     }
     __syncthreads();
     if (sm.abort_flag) return;
+    if (GATHER && !use_tma) {
+      const TileCtx& tl = sm.tc;
+      for (int i = threadIdx.x; i < kWinG * kWinG * kWinG; i += kBlock) {
+        const int x = tl.tile[0] * kTile + i % kWinG, y = tl.tile[1] * kTile + (i / kWinG) % kWinG,
+                  z = tl.tile[2] * kTile + i / (kWinG * kWinG);
+        sm.vwin[cb][i] = c.g.vel[tl.node_base + ((long long)z * tl.gdim[1] + y) * tl.gdim[0] + x];
+      }
+      __syncthreads();
+    }
+    const TileCtx& tc = sm.tc;
     const float dt = GATHER ? c.dt_scene[scene] : 0.f;
     const bool single = c.single_material != 0;
-    MaterialDev mt_tile;
-    if (single) mt_tile = c.mats[sc.mat_base];
     float wave_acc = 0.f, grad_acc = 0.f;
     unsigned flags_acc = 0;
     for (unsigned r0 = 0; r0 < it.z; r0 += kCap) {
@@ -839,7 +857,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_particles(const __grid_constant__
 #pragma unroll
           for (int e = 0; e < 9; ++e) D[e] = c.p.Dc[e][home];
           const float m = c.p.m[home], V = c.p.V[home];
-          const MaterialDev mt = single ? mt_tile : c.mats[c.p.mat[home]];
+          const MaterialDev mt = single ? sm.mt : c.mats[c.p.mat[home]];
           const bool pinned = c.has_pinned && c.p.pinned[home];
           float ep = c.has_plastic ? c.p.ep[home] : 0.f;
           float T = c.has_thermal ? c.p.T[home] : 0.f;
@@ -970,11 +988,26 @@ __global__ void __launch_bounds__(kBlock, 2) k_particles(const __grid_constant__
         }
         if (PASS == kPassG2P2G) count_key(c, key);
       }
-      if (r0 == 0) prefetch_next();
+      if (!SCATTER && r0 == 0 && threadIdx.x == 0) prefetch_next();
       if (SCATTER) {
         __syncthreads();
         scan_buckets(sm);
-        if (r0 == 0) {
+        __syncthreads();
+        for (unsigned j = threadIdx.x; j < nround; j += kBlock) {
+          const unsigned mm = sm.meta[j];
+          if (!(mm & kMetaInvalid)) sm.sidx[sm.bstart[mm & 0xffu] + (mm >> 8)] = static_cast<unsigned short>(j);
+        }
+        __syncthreads();
+        // ---- phase B: one thread per (non-empty bucket, z layer); the last thread claims the next
+        // tile meanwhile (a full tile has about 3 x 64 tasks, so it rarely has one)
+        if (r0 == 0 && threadIdx.x == kBlock - 1) prefetch_next();
+        const int nbk = sm.nbuckets;
+        for (int task = threadIdx.x; task < 3 * nbk; task += kBlock) {
+          const int kz = task / nbk;
+          bucket_layer(sm, sm.blist[task - kz * nbk], kz);
+        }
+        __syncthreads();
+        if (r0 == 0) {  // perm of the next tile's first round, consumed there
           const uint4 nx = sm.item[cb ^ 1];
           pf_ok = nx.x != 0xffffffffu;
           if (pf_ok) {
@@ -985,19 +1018,6 @@ __global__ void __launch_bounds__(kBlock, 2) k_particles(const __grid_constant__
             }
           }
         }
-        __syncthreads();
-        for (unsigned j = threadIdx.x; j < nround; j += kBlock) {
-          const unsigned mm = sm.meta[j];
-          if (!(mm & kMetaInvalid)) sm.sidx[sm.bstart[mm & 0xffu] + (mm >> 8)] = static_cast<unsigned short>(j);
-        }
-        __syncthreads();
-        // ---- phase B: one thread per (non-empty bucket, z layer) ----
-        const int nbk = sm.nbuckets;
-        for (int task = threadIdx.x; task < 3 * nbk; task += kBlock) {
-          const int kz = task / nbk;
-          bucket_layer(sm, sm.blist[task - kz * nbk], kz);
-        }
-        __syncthreads();
       }
     }
     block_reduce_item(c, scene, wave_acc, grad_acc, flags_acc, sm.red);
@@ -1285,76 +1305,108 @@ void launch_grid_debug(const Ctx& c, cudaStream_t st, int scene, float dt, doubl
 // ---------------------------------------------------------------------------------------------
 // host <-> device conversion (staging buffers hold the caller's f64 or f32 arrays)
 
+// Host arrays (staged on the device) into the SoA state. A full upload sets the home order to the
+// caller's order (id = i); with by_id the caller's particle id[i] is read into home slot i.
 template <typename Tsrc>
 __global__ void k_upload(Ctx c, long long n, const Tsrc* const* src, const int* material,
-                         const unsigned char* pinned, unsigned fields) {
+                         const unsigned char* pinned, unsigned fields, int by_id) {
   const long long cap = c.p.cap;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-    const int s = c.nscenes == 1 ? 0 : find_scene_by_particle(c.scenes, c.nscenes, i);
+  for (long long h = blockIdx.x * (long long)blockDim.x + threadIdx.x; h < n; h += (long long)gridDim.x * blockDim.x) {
+    const long long i = by_id ? (long long)c.p.id[h] : h;
+    if (!by_id) c.p.id[h] = static_cast<unsigned>(h);
+    const int s = c.nscenes == 1 ? 0 : find_scene_by_particle(c.scenes, c.nscenes, h);
     const SceneDev& sc = c.scenes[s];
     if (fields & kFieldPos) {
       unsigned* qs[3] = {c.p.qx, c.p.qy, c.p.qz};
       for (int a = 0; a < 3; ++a) {
         const double q = rint(((double)src[a][i] - sc.origin[a]) / (double)sc.H * 4194304.0);
         const double hi = (double)(((long long)sc.dims[a] - 1) << kFracBits);
-        qs[a][i] = static_cast<unsigned>(fmin(fmax(q, 0.0), hi));
+        qs[a][h] = static_cast<unsigned>(fmin(fmax(q, 0.0), hi));
       }
     }
     if (fields & kFieldVel) {
-      c.p.vx[i] = src[3] ? (float)src[3][i] : 0.f;
-      c.p.vy[i] = src[4] ? (float)src[4][i] : 0.f;
-      c.p.vz[i] = src[5] ? (float)src[5][i] : 0.f;
+      c.p.vx[h] = src[3] ? (float)src[3][i] : 0.f;
+      c.p.vy[h] = src[4] ? (float)src[4][i] : 0.f;
+      c.p.vz[h] = src[5] ? (float)src[5][i] : 0.f;
     }
-    if (fields & kFieldMass) c.p.m[i] = (float)src[6][i];
-    if (fields & kFieldVolume) c.p.V[i] = (float)src[7][i];
-    if (fields & kFieldTemp) c.p.T[i] = src[8] ? (float)src[8][i] : 0.f;
-    if (fields & kFieldPlastic) c.p.ep[i] = src[9] ? (float)src[9][i] : 0.f;
+    if (fields & kFieldMass) c.p.m[h] = (float)src[6][i];
+    if (fields & kFieldVolume) c.p.V[h] = (float)src[7][i];
+    if (fields & kFieldTemp) c.p.T[h] = src[8] ? (float)src[8][i] : 0.f;
+    if (fields & kFieldPlastic) c.p.ep[h] = src[9] ? (float)src[9][i] : 0.f;
     if (fields & kFieldF)
       for (int e = 0; e < 9; ++e)
-        c.p.D[e * cap + i] = src[10] ? (float)((double)src[10][i * 9 + e] - ((e % 4 == 0) ? 1.0 : 0.0)) : 0.f;
+        c.p.D[e * cap + h] = src[10] ? (float)((double)src[10][i * 9 + e] - ((e % 4 == 0) ? 1.0 : 0.0)) : 0.f;
     if (fields & kFieldC)
-      for (int e = 0; e < 9; ++e) c.p.C[e * cap + i] = src[11] ? (float)src[11][i * 9 + e] : 0.f;
+      for (int e = 0; e < 9; ++e) c.p.C[e * cap + h] = src[11] ? (float)src[11][i * 9 + e] : 0.f;
     if (fields & kFieldMass) {
-      c.p.mat[i] = material ? static_cast<unsigned short>(sc.mat_base + material[i])
+      c.p.mat[h] = material ? static_cast<unsigned short>(sc.mat_base + material[i])
                             : static_cast<unsigned short>(sc.mat_base);
-      if (c.p.pinned) c.p.pinned[i] = pinned ? pinned[i] : 0;
+      if (c.p.pinned) c.p.pinned[h] = pinned ? pinned[i] : 0;
     }
   }
 }
 
 void launch_upload_convert(const Ctx& c, cudaStream_t st, long long n, int dtype, const void* const* src,
-                           const int* material, const unsigned char* pinned, unsigned fields) {
+                           const int* material, const unsigned char* pinned, unsigned fields, bool by_id) {
   if (n <= 0) return;
   const int blocks = static_cast<int>((n + 255) / 256 < 65536 ? (n + 255) / 256 : 65536);
   if (dtype == 0)
-    k_upload<double><<<blocks, 256, 0, st>>>(c, n, reinterpret_cast<const double* const*>(src), material, pinned, fields);
+    k_upload<double><<<blocks, 256, 0, st>>>(c, n, reinterpret_cast<const double* const*>(src), material, pinned, fields,
+                                             by_id ? 1 : 0);
   else
-    k_upload<float><<<blocks, 256, 0, st>>>(c, n, reinterpret_cast<const float* const*>(src), material, pinned, fields);
+    k_upload<float><<<blocks, 256, 0, st>>>(c, n, reinterpret_cast<const float* const*>(src), material, pinned, fields,
+                                            by_id ? 1 : 0);
+}
+
+// Rewrites the state in sort order: dst[i] = current[perm[i]] for every field, then perm = identity,
+// so each tile's particles are contiguous in every array.
+__global__ void k_permute(Ctx c, Particles d) {
+  const Particles& s = c.p;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < c.n; i += (long long)gridDim.x * blockDim.x) {
+    const unsigned h = s.perm[i];
+    d.qx[i] = s.qx[h]; d.qy[i] = s.qy[h]; d.qz[i] = s.qz[h];
+    d.vx[i] = s.vx[h]; d.vy[i] = s.vy[h]; d.vz[i] = s.vz[h];
+#pragma unroll
+    for (int e = 0; e < 9; ++e) {
+      d.Cc[e][i] = s.Cc[e][h];
+      d.Dc[e][i] = s.Dc[e][h];
+    }
+    d.m[i] = s.m[h]; d.V[i] = s.V[h]; d.ep[i] = s.ep[h]; d.T[i] = s.T[h];
+    d.mat[i] = s.mat[h]; d.pinned[i] = s.pinned[h]; d.id[i] = s.id[h];
+    s.perm[i] = static_cast<unsigned>(i);
+  }
+}
+
+void launch_permute(const Ctx& c, const Particles& dst, cudaStream_t st) {
+  if (c.n <= 0) return;
+  const long long blocks = (c.n + 255) / 256 < 65536 ? (c.n + 255) / 256 : 65536;
+  k_permute<<<static_cast<unsigned>(blocks), 256, 0, st>>>(c, dst);
 }
 
 template <typename Tdst>
 __global__ void k_download(Ctx c, long long n, Tdst* const* dst, unsigned fields) {
   const long long cap = c.p.cap;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-    const int s = c.nscenes == 1 ? 0 : find_scene_by_particle(c.scenes, c.nscenes, i);
+  for (long long h = blockIdx.x * (long long)blockDim.x + threadIdx.x; h < n; h += (long long)gridDim.x * blockDim.x) {
+    const long long i = c.p.id[h];  // caller's index of home slot h
+    const int s = c.nscenes == 1 ? 0 : find_scene_by_particle(c.scenes, c.nscenes, h);
     const SceneDev& sc = c.scenes[s];
     if (fields & kFieldPos) {
-      const unsigned q[3] = {c.p.qx[i], c.p.qy[i], c.p.qz[i]};
+      const unsigned q[3] = {c.p.qx[h], c.p.qy[h], c.p.qz[h]};
       for (int a = 0; a < 3; ++a) dst[a][i] = (Tdst)(sc.origin[a] + (double)q[a] * ((double)sc.H / 4194304.0));
     }
     if (fields & kFieldVel) {
-      dst[3][i] = (Tdst)c.p.vx[i];
-      dst[4][i] = (Tdst)c.p.vy[i];
-      dst[5][i] = (Tdst)c.p.vz[i];
+      dst[3][i] = (Tdst)c.p.vx[h];
+      dst[4][i] = (Tdst)c.p.vy[h];
+      dst[5][i] = (Tdst)c.p.vz[h];
     }
-    if (fields & kFieldMass) dst[6][i] = (Tdst)c.p.m[i];
-    if (fields & kFieldVolume) dst[7][i] = (Tdst)c.p.V[i];
-    if (fields & kFieldTemp) dst[8][i] = (Tdst)c.p.T[i];
-    if (fields & kFieldPlastic) dst[9][i] = (Tdst)c.p.ep[i];
+    if (fields & kFieldMass) dst[6][i] = (Tdst)c.p.m[h];
+    if (fields & kFieldVolume) dst[7][i] = (Tdst)c.p.V[h];
+    if (fields & kFieldTemp) dst[8][i] = (Tdst)c.p.T[h];
+    if (fields & kFieldPlastic) dst[9][i] = (Tdst)c.p.ep[h];
     for (int e = 0; e < 9; ++e) {
       const double ident = (e % 4 == 0) ? 1.0 : 0.0;
-      if (fields & kFieldF) dst[10][i * 9 + e] = (Tdst)((double)c.p.D[e * cap + i] + ident);
-      if (fields & kFieldC) dst[11][i * 9 + e] = (Tdst)c.p.C[e * cap + i];
+      if (fields & kFieldF) dst[10][i * 9 + e] = (Tdst)((double)c.p.D[e * cap + h] + ident);
+      if (fields & kFieldC) dst[11][i * 9 + e] = (Tdst)c.p.C[e * cap + h];
     }
   }
 }
