@@ -226,6 +226,67 @@ int mpm_p2g_noalloc(const mpm_domain* domain, const mpm_material* material, int6
                     const float* v, const double* F, const float* C, const float* m, const float* V,
                     double dt, double* mass, double* momentum, void* stream);
 
+/* ======================================================================================
+ * 2D elastic solid: drop-in for the reference's SolidMPM (src/solid-mpm.js:20-116).
+ * Fixed 149 x 149 node grid, DX = 8, origin -592 (src/solid-mpm.js:4); fixed-corotated
+ * elasticity with E = rho * 16000 * solidStiffness and mu = lambda = 0.4 E. The handle owns
+ * F and C on the device (the reference's f00..c11 fields); the caller owns the particle
+ * arrays and passes them with every call, like `s` in the reference (host pointers, copied
+ * in and, for x/y/vx/vy, back out).
+ * ====================================================================================== */
+#define SMPM_SCENE_OTHER 0
+#define SMPM_SCENE_SOFTBODY 1 /* s.scene === 'softbody' (src/solid-mpm.js:65) */
+#define SMPM_SCENE_BASIN 2    /* s.scene === 'basin' */
+#define SMPM_GRAVITY_NONE 0
+#define SMPM_GRAVITY_CENTER 1 /* settings.gravity 'center' (src/simulation.js:276-278) */
+#define SMPM_GRAVITY_UNIFORM 2
+
+/* The caller's particle arrays and the settings the step reads (src/simulation.js:18-31). */
+typedef struct smpm_sim {
+  int32_t count;
+  int32_t scene;             /* SMPM_SCENE_* */
+  int32_t boundary;          /* settings.boundary */
+  int32_t gravity;           /* SMPM_GRAVITY_*; read by smpm_frame only */
+  double solid_stiffness;    /* settings.solidStiffness */
+  double strength;           /* settings.strength; read by smpm_frame only */
+  float *x, *y, *vx, *vy;    /* in/out */
+  const float *mass, *volume;
+  const uint8_t *material, *pinned;
+} smpm_sim;
+
+typedef struct smpm_stats { /* SolidMPM.stats (src/solid-mpm.js:108-116) */
+  int32_t count;
+  int32_t nodes;
+  int32_t substeps;
+  int32_t pad;
+  double min_j, max_j, strain;
+} smpm_stats;
+
+typedef struct smpm_handle smpm_handle;
+
+/* new SolidMPM(capacity) (src/solid-mpm.js:21-25): F = I, C = 0 for every slot. */
+int smpm_create(int64_t capacity, smpm_handle** out);
+int smpm_destroy(smpm_handle* h);
+const char* smpm_last_error(const smpm_handle* h);
+/* Material ids treated as MPM solids (MATERIALS[m].mpm, src/solid-mpm.js:7); default {11}. */
+int smpm_set_mpm_materials(smpm_handle* h, const uint8_t* ids, int32_t n);
+int smpm_reset(smpm_handle* h);                                   /* SolidMPM.reset */
+int smpm_reset_particle(smpm_handle* h, int64_t i);               /* SolidMPM.resetParticle */
+int smpm_remove_particle(smpm_handle* h, int64_t i, int64_t last); /* SolidMPM.removeParticle */
+int smpm_has_particles(smpm_handle* h, const smpm_sim* s, int32_t* out); /* SolidMPM.hasParticles */
+int smpm_stable_step(smpm_handle* h, const smpm_sim* s, double* dt);     /* SolidMPM.stableStep */
+int smpm_step(smpm_handle* h, const smpm_sim* s, double dt);             /* SolidMPM.step */
+int smpm_stats_get(smpm_handle* h, const smpm_sim* s, smpm_stats* out);  /* SolidMPM.stats */
+/* The MPM branch of Simulation.step (src/simulation.js:246-254) for a simulation whose moving
+ * particles are all MPM solids, on the device: up to 96 substeps of h = min(remaining,
+ * stableStep), each applying the body force of Simulation.substep (src/simulation.js:270-288)
+ * before the step. dt is clamped to [0, 0.05]. One host round trip per call. */
+int smpm_frame(smpm_handle* h, const smpm_sim* s, double dt, int32_t* substeps, double* advanced);
+/* Read / write the eight deformation fields (f00 f01 f10 f11 c00 c01 c10 c11) of slots
+ * [0, n) as fields[8][n] doubles. */
+int smpm_get_fields(smpm_handle* h, int64_t n, double* fields);
+int smpm_set_fields(smpm_handle* h, int64_t n, const double* fields);
+
 #ifdef __cplusplus
 }
 #endif

@@ -50,6 +50,20 @@ class MpmLedger(ctypes.Structure):
                 ("nonfinite", _I64), ("invalid_j", _I64)]
 
 
+class SmpmSim(ctypes.Structure):
+    _fields_ = [("count", _I32), ("scene", _I32), ("boundary", _I32), ("gravity", _I32),
+                ("solid_stiffness", _D), ("strength", _D), ("x", _P), ("y", _P), ("vx", _P), ("vy", _P),
+                ("mass", _P), ("volume", _P), ("material", _P), ("pinned", _P)]
+
+
+class SmpmStats(ctypes.Structure):
+    _fields_ = [("count", _I32), ("nodes", _I32), ("substeps", _I32), ("pad", _I32), ("min_j", _D),
+                ("max_j", _D), ("strain", _D)]
+
+
+SMPM_SCENES = {"softbody": 1, "basin": 2}
+SMPM_GRAVITY = {"none": 0, "center": 1, "uniform": 2}
+
 # name -> (restype, argtypes)
 SIGNATURES = {
     "mpm_abi_version": (ctypes.c_int, []),
@@ -88,6 +102,20 @@ SIGNATURES = {
     "mpm_return_map_batch": (ctypes.c_int, [ctypes.POINTER(MpmMaterial), _I64, _P, _P, _P, _D, _P, _P, _P]),
     "mpm_p2g_noalloc": (ctypes.c_int, [ctypes.POINTER(MpmDomain), ctypes.POINTER(MpmMaterial), _I64, _P, _P, _P, _P, _P,
                                         _P, _D, _P, _P, _P]),
+    "smpm_create": (ctypes.c_int, [_I64, ctypes.POINTER(_P)]),
+    "smpm_destroy": (ctypes.c_int, [_P]),
+    "smpm_last_error": (ctypes.c_char_p, [_P]),
+    "smpm_set_mpm_materials": (ctypes.c_int, [_P, _P, _I32]),
+    "smpm_reset": (ctypes.c_int, [_P]),
+    "smpm_reset_particle": (ctypes.c_int, [_P, _I64]),
+    "smpm_remove_particle": (ctypes.c_int, [_P, _I64, _I64]),
+    "smpm_has_particles": (ctypes.c_int, [_P, ctypes.POINTER(SmpmSim), ctypes.POINTER(_I32)]),
+    "smpm_stable_step": (ctypes.c_int, [_P, ctypes.POINTER(SmpmSim), ctypes.POINTER(_D)]),
+    "smpm_step": (ctypes.c_int, [_P, ctypes.POINTER(SmpmSim), _D]),
+    "smpm_stats_get": (ctypes.c_int, [_P, ctypes.POINTER(SmpmSim), ctypes.POINTER(SmpmStats)]),
+    "smpm_frame": (ctypes.c_int, [_P, ctypes.POINTER(SmpmSim), _D, ctypes.POINTER(_I32), ctypes.POINTER(_D)]),
+    "smpm_get_fields": (ctypes.c_int, [_P, _I64, _P]),
+    "smpm_set_fields": (ctypes.c_int, [_P, _I64, _P]),
 }
 
 _lib = None
@@ -117,5 +145,13 @@ def lib():
 def check(rc, handle=None):
     if rc != OK:
         msg = lib().mpm_last_error(handle).decode() if handle else lib().mpm_error_string(rc).decode()
+        raise MpmError(rc, msg)
+    return rc
+
+
+def check2(rc, handle=None):
+    """check() for the 2D (smpm_*) handles."""
+    if rc != OK:
+        msg = lib().smpm_last_error(handle).decode() if handle else lib().mpm_error_string(rc).decode()
         raise MpmError(rc, msg)
     return rc

@@ -13,7 +13,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 def declared_functions():
     text = open(os.path.join(ROOT, "include", "mpm_b200.h")).read()
     text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
-    return sorted(set(re.findall(r"^\s*(?:const\s+)?\w+\**\s+\**(mpm_\w+)\s*\(", text, flags=re.M)))
+    return sorted(set(re.findall(r"^\s*(?:const\s+)?\w+\**\s+\**(s?mpm_\w+)\s*\(", text, flags=re.M)))
 
 
 def test_library_exports_every_declared_symbol():
@@ -38,6 +38,8 @@ def test_struct_layouts_match_header_sizes():
     assert ctypes.sizeof(_lib.MpmMaterial) == 8 + 9 * 8
     assert ctypes.sizeof(_lib.MpmParticles) == 8 + 14 * 8
     assert ctypes.sizeof(_lib.MpmLedger) == 5 * 8 + 6 * 8 + 5 * 8 + 3 * 8
+    assert ctypes.sizeof(_lib.SmpmSim) == 4 * 4 + 2 * 8 + 8 * 8
+    assert ctypes.sizeof(_lib.SmpmStats) == 4 * 4 + 3 * 8
 
 
 def test_invalid_arguments_are_rejected_without_touching_a_device():
@@ -45,5 +47,7 @@ def test_invalid_arguments_are_rejected_without_touching_a_device():
     h = ctypes.c_void_p()
     assert L.mpm_create(None, 10, ctypes.byref(h)) == -1
     assert L.mpm_destroy(None) == -1
+    assert L.smpm_create(0, ctypes.byref(h)) == -1
+    assert L.smpm_destroy(None) == -1
     m = _lib.MpmMaterial(model=7, mu=1, lam=1)
     assert L.mpm_return_map_batch(ctypes.byref(m), 0, None, None, None, 0.0, None, None, None) == -10
