@@ -149,6 +149,13 @@ int mpm_download_particles(mpm_handle* h, const mpm_particles* p);
 int mpm_count(const mpm_handle* h, int64_t* n);
 /* MPM3.reset() / resetParticle for all: F = I, C = 0, plastic = 0 (src/three/mpm.js:20-21) */
 int mpm_reset_deformation(mpm_handle* h);
+/* MPM3.resetParticle(p) (src/three/mpm.js:21): F = I, C = 0, plastic = 0 for the caller's
+ * particle index p (the index used at upload). */
+int mpm_reset_particle(mpm_handle* h, int64_t index);
+/* MPM3.remove(p, last) with the caller's Simulation3.remove(i) (src/three/mpm.js:22-25,
+ * src/three/simulation.js:114): particle `last` takes index p with all of its state and the
+ * count drops by one; `last` must be the current count - 1. Single-scene handles only. */
+int mpm_remove_particle(mpm_handle* h, int64_t index, int64_t last);
 
 /* ---- stepping ---- */
 /* MPM3.stableStep(s) (src/three/mpm.js:40-55) on the current state */
@@ -225,6 +232,50 @@ int mpm_return_map_batch(const mpm_material* material, int64_t n, const double* 
 int mpm_p2g_noalloc(const mpm_domain* domain, const mpm_material* material, int64_t n, const double* x,
                     const float* v, const double* F, const float* C, const float* m, const float* V,
                     double dt, double* mass, double* momentum, void* stream);
+
+/* ======================================================================================
+ * Batched ensembles: many independent scenes stepped by one handle.
+ * The reference runs its V&V cases one at a time (src/simulation/vv-mpm.js:30-60 builds and
+ * steps one engine per grid phase; src/simulation/vv-benchmarks.js:107-115 solves one sample of
+ * an ensemble at a time); these calls replace such loops. Every scene keeps its own domain,
+ * grid, material and CFL time step; each substep of the handle advances every scene by its own
+ * dt in one launch sequence over all scenes (one persistent G2P2G launch whose work list holds
+ * the tiles of every scene). Particles are uploaded and downloaded with mpm_upload_particles /
+ * mpm_download_particles as one array in scene order.
+ * ====================================================================================== */
+typedef struct mpm_scene_desc {
+  mpm_domain domain;
+  int32_t material;  /* index into the handle's material table (mpm_set_material) */
+  int32_t reserved;
+  int64_t count;     /* particles of this scene */
+} mpm_scene_desc;
+
+typedef struct mpm_tuning {
+  int32_t blocks_per_sm;     /* resident G2P2G CTAs per SM chosen */
+  int32_t reorder_interval;  /* substeps between physical re-sorts of the particle state */
+  int32_t use_tma;           /* TMA (1) or plain loads (0) for the gather window */
+  int32_t trials;            /* configurations timed */
+  double ms_per_substep;     /* best configuration */
+  double ms_per_substep_default;
+} mpm_tuning;
+
+#define MPM_MAX_SCENES 4096
+int mpm_batch_create(const mpm_scene_desc* scenes, int32_t nscenes, mpm_handle** out);
+int mpm_batch_count(const mpm_handle* h, int32_t* nscenes);
+/* nsteps CFL substeps of every scene (each with its own dt). use_graph != 0 replays the
+ * substep sequence from a captured CUDA graph (captured on first use, reused while the
+ * handle's buffer parity and re-sort phase match). */
+int mpm_batch_run(mpm_handle* h, int32_t nsteps, int32_t use_graph);
+/* Per-scene simulated time since upload and the dt of the last substep (nscenes each). */
+int mpm_batch_times(mpm_handle* h, double* time, double* last_dt);
+/* FP64 ledger of one scene (the quantities of mpm_ledger_compute over its particles). */
+int mpm_batch_ledger(mpm_handle* h, int32_t scene, mpm_ledger* out);
+/* Grid mass and momentum of one scene after P2G (like mpm_grid_debug). */
+int mpm_batch_grid_debug(mpm_handle* h, int32_t scene, double dt, double* mass, double* momentum);
+/* Autotuner: times trial_substeps substeps for each G2P2G schedule (CTAs per SM, re-sort
+ * interval, TMA or plain gather) from the same snapshot of the state, keeps the fastest and
+ * restores the state and the scenes' clocks. Works on any handle. */
+int mpm_batch_autotune(mpm_handle* h, int32_t trial_substeps, mpm_tuning* out);
 
 /* ======================================================================================
  * 2D elastic solid: drop-in for the reference's SolidMPM (src/solid-mpm.js:20-116).

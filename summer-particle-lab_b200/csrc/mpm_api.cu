@@ -60,7 +60,14 @@ struct mpm_handle {
   cudaStream_t stream = nullptr;
   int num_sms = 148;
   mpm_domain dom{};
-  SceneDev scene{};
+  SceneDev scene{};                  // scene 0 (the only scene of a single-scene handle)
+  std::vector<SceneDev> scenes;      // every scene, in particle and grid order
+  std::vector<int32_t> scene_material;  // batch handles: the material of each scene
+  bool batch = false;                // created by mpm_batch_create
+  cudaGraphExec_t graph = nullptr;   // captured substeps of mpm_batch_run
+  int graph_substeps = 0;
+  const unsigned* graph_parity = nullptr;  // particle buffer current when the graph was captured
+  int64_t launches_per_graph = 0;
   std::vector<mpm_material> mats_host;
   std::vector<MaterialDev> mats_dev;
   std::vector<char> mat_set;
@@ -132,6 +139,12 @@ struct ProfScope {
       return e_ == cudaErrorMemoryAllocation ? MPM_ERR_OUT_OF_MEMORY : MPM_ERR_CUDA; \
     }                                                                              \
   } while (0)
+
+static void drop_graph(mpm_handle* h) {
+  if (h->graph) cudaGraphExecDestroy(h->graph);
+  h->graph = nullptr;
+  h->graph_substeps = 0;
+}
 
 static int fail(mpm_handle* h, int code, const std::string& msg) {
   if (h) h->err = msg;
@@ -245,15 +258,27 @@ static int permute_state(mpm_handle* h) {
   return MPM_OK;
 }
 
+// Grid, sort buffers and control block of every scene in one allocation. Scene s owns nodes
+// [node_base, node_base + gdim^3), particle tiles [tile_base, ...) and node tiles
+// [node_tile_base, ...); bases increase with s, so a tile-sorted particle order keeps each
+// scene's particles contiguous and in scene order.
 static int alloc_grid(mpm_handle* h) {
   if (h->gblock) {
     cudaFree(h->gblock);
     h->gblock = nullptr;
   }
-  const SceneDev& s = h->scene;
-  const long long nodes = (long long)s.gdim[0] * s.gdim[1] * s.gdim[2];
-  const int tiles = s.tiles[0] * s.tiles[1] * s.tiles[2];
-  const int ntiles = s.ntiles[0] * s.ntiles[1] * s.ntiles[2];
+  const int ns = static_cast<int>(h->scenes.size());
+  long long nodes = 0;
+  int tiles = 0, ntiles = 0;
+  for (SceneDev& s : h->scenes) {
+    s.node_base = nodes;
+    s.tile_base = tiles;
+    s.node_tile_base = ntiles;
+    nodes += (long long)s.gdim[0] * s.gdim[1] * s.gdim[2];
+    tiles += s.tiles[0] * s.tiles[1] * s.tiles[2];
+    ntiles += s.ntiles[0] * s.ntiles[1] * s.ntiles[2];
+  }
+  h->scene = h->scenes[0];
   const int scan_blocks = (tiles + 1 + 4095) / 4096;
   auto lay = [&](char* base, Ctx& c, void** tmaps, SceneDev** scenes, MaterialDev** mats) {
     Carver cv{base};
@@ -271,12 +296,13 @@ static int alloc_grid(mpm_handle* h) {
     c.s.work[0] = cv.take<uint4>(tiles);
     c.s.work[1] = cv.take<uint4>(tiles);
     c.ctrl = cv.take<mpm::Ctrl>(1);
-    c.dt_scene = cv.take<float>(1);
-    c.wave_max = cv.take<unsigned>(1);
-    c.grad_max = cv.take<unsigned>(1);
-    *scenes = cv.take<SceneDev>(1);
+    c.dt_scene = cv.take<float>(ns);
+    c.wave_max = cv.take<unsigned>(ns);
+    c.grad_max = cv.take<unsigned>(ns);
+    c.time_scene = cv.take<double>(ns);
+    *scenes = cv.take<SceneDev>(ns);
     *mats = cv.take<MaterialDev>(kMaxMats);
-    *tmaps = cv.take<char>(128);
+    *tmaps = cv.take<char>(128 * (size_t)ns);
     return align_up(cv.off, 256);
   };
   Ctx probe{};
@@ -294,28 +320,36 @@ static int alloc_grid(mpm_handle* h) {
   lay(static_cast<char*>(h->gblock), c, &tm, &scenes, &mats);
   c.scenes = scenes;
   c.mats = mats;
-  c.nscenes = 1;
+  c.nscenes = ns;
   c.total_tiles = tiles;
   c.total_node_tiles = ntiles;
-  MPM_CUDA(h, cudaMemcpyAsync(scenes, &h->scene, sizeof(SceneDev), cudaMemcpyHostToDevice, h->stream));
+  MPM_CUDA(h, cudaMemcpyAsync(scenes, h->scenes.data(), sizeof(SceneDev) * ns, cudaMemcpyHostToDevice, h->stream));
   MPM_CUDA(h, cudaMemcpyAsync(mats, h->mats_dev.data(), sizeof(MaterialDev) * kMaxMats, cudaMemcpyHostToDevice,
                               h->stream));
-  // TMA descriptor of the velocity grid: 4D {channel 4, x, y, z}, box {4, 6, 6, 6}, fp32
+  // TMA descriptor of each scene's velocity grid: 4D {channel 4, x, y, z}, box {4, 6, 6, 6}, fp32.
+  // A scene's grid starts at a float4 node (16-byte aligned) and its strides are multiples of 16 B.
   c.tmaps = nullptr;
   c.use_tma = 0;
   auto encode = tensor_map_encoder();
   if (encode && h->use_tma) {
-    CUtensorMap map;
-    std::memset(&map, 0, sizeof map);
-    cuuint64_t gdims[4] = {4, (cuuint64_t)s.gdim[0], (cuuint64_t)s.gdim[1], (cuuint64_t)s.gdim[2]};
-    cuuint64_t gstrides[3] = {16, 16ull * s.gdim[0], 16ull * s.gdim[0] * s.gdim[1]};
-    cuuint32_t box[4] = {4, mpm::kWinG, mpm::kWinG, mpm::kWinG};
-    cuuint32_t estr[4] = {1, 1, 1, 1};
-    CUresult r = encode(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, c.g.vel, gdims, gstrides, box, estr,
-                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
-                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-    if (r == CUDA_SUCCESS) {
-      MPM_CUDA(h, cudaMemcpyAsync(tm, &map, sizeof map, cudaMemcpyHostToDevice, h->stream));
+    std::vector<CUtensorMap> maps(ns);
+    bool ok = true;
+    for (int k = 0; k < ns && ok; ++k) {
+      const SceneDev& s = h->scenes[k];
+      std::memset(&maps[k], 0, sizeof(CUtensorMap));
+      cuuint64_t gdims[4] = {4, (cuuint64_t)s.gdim[0], (cuuint64_t)s.gdim[1], (cuuint64_t)s.gdim[2]};
+      cuuint64_t gstrides[3] = {16, 16ull * s.gdim[0], 16ull * s.gdim[0] * s.gdim[1]};
+      cuuint32_t box[4] = {4, mpm::kWinG, mpm::kWinG, mpm::kWinG};
+      cuuint32_t estr[4] = {1, 1, 1, 1};
+      CUresult r = encode(&maps[k], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, c.g.vel + s.node_base, gdims, gstrides, box, estr,
+                          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+      ok = r == CUDA_SUCCESS;
+    }
+    if (ok) {
+      static_assert(sizeof(CUtensorMap) == 128, "tensor map stride");
+      MPM_CUDA(h, cudaMemcpyAsync(tm, maps.data(), sizeof(CUtensorMap) * ns, cudaMemcpyHostToDevice, h->stream));
+      MPM_CUDA(h, cudaStreamSynchronize(h->stream));  // maps is a host temporary
       c.tmaps = tm;
       c.use_tma = 1;
     }
@@ -470,6 +504,7 @@ int mpm_create(const mpm_domain* domain, int64_t capacity, mpm_handle** out) {
   }
   h->dom = *domain;
   h->scene = s;
+  h->scenes.assign(1, s);
   h->cap = capacity;
   h->use_tma = std::getenv("MPM_B200_NO_TMA") ? 0 : 1;  // plain-load gather window when set
   h->mats_host.assign(kMaxMats, mpm_material{});
@@ -521,6 +556,7 @@ int mpm_destroy(mpm_handle* h) {
   if (!h) return MPM_ERR_INVALID_ARG;
   if (h->stream) cudaStreamSynchronize(h->stream);
   for (cudaEvent_t e : h->ev_pool) cudaEventDestroy(e);
+  drop_graph(h);
   free_device(h);
   if (h->stream) cudaStreamDestroy(h->stream);
   delete h;
@@ -535,8 +571,11 @@ int mpm_configure_domain(mpm_handle* h, const mpm_domain* domain) {
   int rc = build_scene(h, *domain, s);
   if (rc != MPM_OK) return rc;
   MPM_CUDA(h, cudaStreamSynchronize(h->stream));
+  if (h->batch) return fail(h, MPM_ERR_STATE, "a batch handle's scenes are fixed at creation");
   h->dom = *domain;
   h->scene = s;
+  h->scenes.assign(1, s);
+  drop_graph(h);
   rc = alloc_grid(h);
   if (rc != MPM_OK) return rc;
   h->uploaded = false;  // positions are relative to the grid origin: upload again
@@ -633,7 +672,15 @@ int mpm_upload_particles(mpm_handle* h, int64_t n, const mpm_particles* p) {
   if (n > 0 && (!p->x || !p->y || !p->z || !p->mass || !p->volume))
     return fail(h, MPM_ERR_INVALID_ARG, "positions, mass and volume are required");
   bool single = true, pinned_any = false;
-  if (p->material) {
+  if (h->batch) {
+    // one material per scene, named at creation; particles come in scene order
+    int64_t total = 0;
+    for (size_t k = 0; k < h->scenes.size(); ++k) {
+      total += h->scenes[k].p_end - h->scenes[k].p_begin;
+      if (!h->mat_set[h->scene_material[k]]) return fail(h, MPM_ERR_INVALID_ARG, "a scene's material is not set");
+    }
+    if (n != total) return fail(h, MPM_ERR_INVALID_ARG, "a batch upload carries exactly the scenes' particle counts");
+  } else if (p->material) {
     for (int64_t i = 0; i < n; ++i) {
       const int m = p->material[i];
       if (m < 0 || m >= kMaxMats || !h->mat_set[m]) return fail(h, MPM_ERR_INVALID_ARG, "particle material not set");
@@ -658,6 +705,7 @@ int mpm_upload_particles(mpm_handle* h, int64_t n, const mpm_particles* p) {
   }
   (void)es;
   MPM_CUDA(h, cudaStreamSynchronize(h->stream));
+  drop_graph(h);  // a captured graph holds the old particle count
   void* ptrs[12];
   const int* mat_dev;
   const unsigned char* pin_dev;
@@ -667,11 +715,26 @@ int mpm_upload_particles(mpm_handle* h, int64_t n, const mpm_particles* p) {
   h->ctx.n = n;
   h->ctx.has_pinned = pinned_any ? 1 : 0;
   h->ctx.single_material = single ? 1 : 0;
+  if (p->temperature) h->ctx.has_thermal = 1;
+  refresh_flags(h);
+  MPM_CUDA(h, cudaMemsetAsync(h->ctx.time_scene, 0, sizeof(double) * h->scenes.size(), h->stream));
+  if (h->batch) {
+    // scene table already on the device (alloc_grid); each particle takes its scene's material
+    { ProfScope ps(h, -1);
+      mpm::launch_upload_convert(h->ctx, h->stream, n, p->dtype, reinterpret_cast<const void* const*>(h->dptr_table),
+                                 nullptr, pin_dev, all, false); }
+    MPM_CUDA(h, cudaGetLastError());
+    h->n = n;
+    h->uploaded = true;
+    h->grid_valid = false;
+    h->reorder_pending = true;
+    MPM_CUDA(h, cudaStreamSynchronize(h->stream));
+    return MPM_OK;
+  }
   h->scene.mat_base = (single && p->material && n > 0) ? p->material[0] : 0;
   h->scene.p_begin = 0;
   h->scene.p_end = n;
-  if (p->temperature) h->ctx.has_thermal = 1;
-  refresh_flags(h);
+  h->scenes[0] = h->scene;
   MPM_CUDA(h, cudaMemcpyAsync(const_cast<SceneDev*>(h->ctx.scenes), &h->scene, sizeof(SceneDev), cudaMemcpyHostToDevice,
                               h->stream));
   // the conversion kernel writes the material index relative to mat_base = 0
@@ -853,6 +916,7 @@ int mpm_step_cfl(mpm_handle* h, int32_t nsteps, double* time_advanced) {
 
 int mpm_step_host(mpm_handle* h, const mpm_particles* io, double dt) {
   if (!h || !io) return MPM_ERR_INVALID_ARG;
+  if (h->batch) return fail(h, MPM_ERR_STATE, "single-scene call on a batch handle");
   if (!h->uploaded) return fail(h, MPM_ERR_STATE, "no particles uploaded");
   if (!(dt > 0)) return fail(h, MPM_ERR_INVALID_ARG, "dt must be positive");
   if (!io->x || !io->y || !io->z || !io->vx || !io->vy || !io->vz)
@@ -1038,6 +1102,7 @@ int mpm_rollback(mpm_handle* h) {
   MPM_CUDA(h, cudaMemcpyAsync(h->pblock, h->snap, h->pblock_bytes, cudaMemcpyDeviceToDevice, h->stream));
   MPM_CUDA(h, cudaMemsetAsync(&h->ctx.ctrl->status, 0, sizeof(unsigned), h->stream));
   MPM_CUDA(h, cudaStreamSynchronize(h->stream));
+  if (h->n != h->snap_n) drop_graph(h);
   h->n = h->snap_n;
   h->grid_valid = false;
   return MPM_OK;
@@ -1054,6 +1119,7 @@ struct CheckpointHeader {
 // the materials (so a load reproduces the state bit for bit).
 int mpm_checkpoint_save(mpm_handle* h, const char* path) {
   if (!h || !path) return MPM_ERR_INVALID_ARG;
+  if (h->batch) return fail(h, MPM_ERR_STATE, "single-scene call on a batch handle");
   if (!h->uploaded) return fail(h, MPM_ERR_STATE, "no particles uploaded");
   FILE* f = std::fopen(path, "wb");
   if (!f) return fail(h, MPM_ERR_INVALID_ARG, std::string("cannot open ") + path);
@@ -1083,6 +1149,7 @@ int mpm_checkpoint_save(mpm_handle* h, const char* path) {
 
 int mpm_checkpoint_load(mpm_handle* h, const char* path) {
   if (!h || !path) return MPM_ERR_INVALID_ARG;
+  if (h->batch) return fail(h, MPM_ERR_STATE, "single-scene call on a batch handle");
   FILE* f = std::fopen(path, "rb");
   if (!f) return fail(h, MPM_ERR_INVALID_ARG, std::string("cannot open ") + path);
   CheckpointHeader hd;
@@ -1136,6 +1203,7 @@ int mpm_checkpoint_load(mpm_handle* h, const char* path) {
   h->scene.mat_base = hd.mat_base;
   h->scene.p_begin = 0;
   h->scene.p_end = hd.n;
+  h->scenes[0] = h->scene;
   MPM_CUDA(h, cudaMemcpyAsync(const_cast<SceneDev*>(h->ctx.scenes), &h->scene, sizeof(SceneDev), cudaMemcpyHostToDevice,
                               h->stream));
   MPM_CUDA(h, cudaStreamSynchronize(h->stream));
@@ -1176,6 +1244,353 @@ int mpm_return_map_batch(const mpm_material* material, int64_t n, const double* 
   if (e == cudaSuccess) e = cudaMemcpy(tau, dtau, 9 * n * sizeof(double), cudaMemcpyDeviceToHost);
   cudaFree(d);
   return e == cudaSuccess ? MPM_OK : MPM_ERR_CUDA;
+}
+
+// ---- per-particle edits (MPM3.resetParticle / MPM3.remove) ----
+
+// Two spare words at the end of the ledger output block hold the slots found on the device.
+static long long* slot_words(mpm_handle* h) { return reinterpret_cast<long long*>(h->ledger_out + 24); }
+
+static int find_slots(mpm_handle* h, int64_t a, int64_t b, long long out[2]) {
+  h->ctx.n = h->n;
+  mpm::launch_find_ids(h->ctx, h->stream, static_cast<unsigned>(a), static_cast<unsigned>(b), slot_words(h));
+  MPM_CUDA(h, cudaGetLastError());
+  MPM_CUDA(h, cudaMemcpyAsync(h->host_ledger + 24, slot_words(h), 2 * sizeof(long long), cudaMemcpyDeviceToHost, h->stream));
+  MPM_CUDA(h, cudaStreamSynchronize(h->stream));
+  std::memcpy(out, h->host_ledger + 24, 2 * sizeof(long long));
+  return MPM_OK;
+}
+
+int mpm_reset_particle(mpm_handle* h, int64_t index) {
+  if (!h) return MPM_ERR_INVALID_ARG;
+  if (!h->uploaded) return fail(h, MPM_ERR_STATE, "no particles uploaded");
+  if (index < 0 || index >= h->n) return fail(h, MPM_ERR_OUT_OF_RANGE, "particle index out of range");
+  long long slots[2];
+  int rc = find_slots(h, index, index, slots);
+  if (rc != MPM_OK) return rc;
+  if (slots[0] < 0) return fail(h, MPM_ERR_STATE, "particle index has no home slot");
+  mpm::launch_edit_particle(h->ctx, h->stream, 0, static_cast<unsigned>(index), slot_words(h));
+  MPM_CUDA(h, cudaGetLastError());
+  MPM_CUDA(h, cudaStreamSynchronize(h->stream));
+  h->grid_valid = false;  // the particle's stress changed
+  return MPM_OK;
+}
+
+int mpm_remove_particle(mpm_handle* h, int64_t index, int64_t last) {
+  if (!h) return MPM_ERR_INVALID_ARG;
+  if (h->batch) return fail(h, MPM_ERR_STATE, "single-scene call on a batch handle");
+  if (!h->uploaded) return fail(h, MPM_ERR_STATE, "no particles uploaded");
+  if (last != h->n - 1) return fail(h, MPM_ERR_INVALID_ARG, "last must be the current count - 1");
+  if (index < 0 || index > last) return fail(h, MPM_ERR_OUT_OF_RANGE, "particle index out of range");
+  long long slots[2];
+  int rc = find_slots(h, index, last, slots);
+  if (rc != MPM_OK) return rc;
+  if (slots[0] < 0 || slots[1] < 0) return fail(h, MPM_ERR_STATE, "particle index has no home slot");
+  mpm::launch_edit_particle(h->ctx, h->stream, 1, static_cast<unsigned>(index), slot_words(h));
+  MPM_CUDA(h, cudaGetLastError());
+  drop_graph(h);
+  h->n -= 1;
+  h->ctx.n = h->n;
+  h->scene.p_end = h->n;
+  h->scenes[0] = h->scene;
+  MPM_CUDA(h, cudaMemcpyAsync(const_cast<SceneDev*>(h->ctx.scenes), &h->scene, sizeof(SceneDev), cudaMemcpyHostToDevice,
+                              h->stream));
+  MPM_CUDA(h, cudaStreamSynchronize(h->stream));
+  h->grid_valid = false;
+  h->reorder_pending = true;
+  return MPM_OK;
+}
+
+// ---- batched ensembles ----
+
+int mpm_batch_create(const mpm_scene_desc* scenes, int32_t nscenes, mpm_handle** out) {
+  if (!out || !scenes || nscenes <= 0 || nscenes > MPM_MAX_SCENES) return MPM_ERR_INVALID_ARG;
+  *out = nullptr;
+  int64_t total = 0;
+  for (int k = 0; k < nscenes; ++k) {
+    if (scenes[k].count < 0 || scenes[k].material < 0 || scenes[k].material >= kMaxMats) return MPM_ERR_INVALID_ARG;
+    total += scenes[k].count;
+  }
+  if (total <= 0 || total > ((int64_t)1 << 31)) return MPM_ERR_INVALID_ARG;
+  mpm_handle* h = nullptr;
+  int rc = mpm_create(&scenes[0].domain, total, &h);
+  if (rc != MPM_OK) return rc;
+  std::vector<SceneDev> list(nscenes);
+  int64_t begin = 0;
+  for (int k = 0; k < nscenes; ++k) {
+    rc = build_scene(h, scenes[k].domain, list[k]);
+    if (rc != MPM_OK) {
+      mpm_destroy(h);
+      return rc;
+    }
+    list[k].p_begin = begin;
+    list[k].p_end = begin + scenes[k].count;
+    list[k].mat_base = scenes[k].material;
+    begin += scenes[k].count;
+    h->scene_material.push_back(scenes[k].material);
+  }
+  h->scenes = list;
+  h->batch = true;
+  h->dom = scenes[0].domain;
+  rc = alloc_grid(h);
+  if (rc == MPM_OK && cudaStreamSynchronize(h->stream) != cudaSuccess) rc = MPM_ERR_CUDA;
+  if (rc != MPM_OK) {
+    mpm_destroy(h);
+    return rc;
+  }
+  *out = h;
+  return MPM_OK;
+}
+
+int mpm_batch_count(const mpm_handle* h, int32_t* nscenes) {
+  if (!h || !nscenes) return MPM_ERR_INVALID_ARG;
+  *nscenes = static_cast<int32_t>(h->scenes.size());
+  return MPM_OK;
+}
+
+// Captures `count` substeps (with the re-sort passes the eager loop would run) into a graph. A
+// graph spans 2 x reorder_interval substeps, so its two permutation passes bring the particle
+// buffers back to the parity they had at capture and every replay sees the same pointers.
+static int capture_graph(mpm_handle* h, int count) {
+  drop_graph(h);
+  const bool prof = h->profiling;
+  h->profiling = false;
+  const int64_t launches0 = h->launches;  // captured launches run on replay, not now
+  MPM_CUDA(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+  for (int i = 0; i < count; ++i) {
+    launch_substep(h, true);
+    if (h->reorder_interval > 0 && ++h->substeps_since_reorder >= h->reorder_interval) {
+      ProfScope ps(h, -1);
+      permute_state(h);
+    }
+  }
+  cudaGraph_t g = nullptr;
+  cudaError_t e = cudaStreamEndCapture(h->stream, &g);
+  h->profiling = prof;
+  h->launches_per_graph = h->launches - launches0;
+  h->launches = launches0;
+  if (e != cudaSuccess) return fail(h, MPM_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+  e = cudaGraphInstantiate(&h->graph, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) {
+    h->graph = nullptr;
+    return fail(h, MPM_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+  }
+  h->graph_substeps = count;
+  return MPM_OK;
+}
+
+static int eager_substep(mpm_handle* h) {
+  launch_substep(h, true);
+  if (h->reorder_interval > 0 && ++h->substeps_since_reorder >= h->reorder_interval) {
+    ProfScope ps(h, -1);
+    return permute_state(h);
+  }
+  return MPM_OK;
+}
+
+int mpm_batch_run(mpm_handle* h, int32_t nsteps, int32_t use_graph) {
+  if (!h) return MPM_ERR_INVALID_ARG;
+  if (nsteps <= 0) return fail(h, MPM_ERR_INVALID_ARG, "nsteps must be positive");
+  if (!h->uploaded) return fail(h, MPM_ERR_STATE, "no particles uploaded");
+  if (h->n == 0) return MPM_OK;
+  if (!use_graph || h->reorder_interval <= 0) return mpm_step_cfl(h, nsteps, nullptr);
+  if (!h->grid_valid) {
+    int rc = prepare_grid(h);
+    if (rc != MPM_OK) return rc;
+  }
+  h->ctx.n = h->n;
+  { ProfScope ps(h, -1); mpm::launch_control_step(h->ctx, h->stream, mpm::kModeCfl, 0.0, nsteps, 0.f); }
+  const int chunk = 2 * h->reorder_interval;
+  int left = nsteps;
+  // eager substeps until the re-sort phase is 0, so every graph replay starts at the same phase
+  while (left > 0 && h->substeps_since_reorder != 0) {
+    const int rc = eager_substep(h);
+    if (rc != MPM_OK) return rc;
+    --left;
+  }
+  if (left >= chunk) {
+    // a graph holds the pointers of the buffer parity it was captured with
+    if (h->graph && (h->graph_substeps != chunk || h->ctx.p.qx != h->graph_parity)) drop_graph(h);
+    if (!h->graph) {
+      h->graph_parity = h->ctx.p.qx;
+      const int rc = capture_graph(h, chunk);
+      if (rc != MPM_OK) return rc;
+    }
+    while (left >= chunk) {
+      MPM_CUDA(h, cudaGraphLaunch(h->graph, h->stream));
+      h->launches += h->launches_per_graph;
+      left -= chunk;
+    }
+  }
+  for (; left > 0; --left) {
+    const int rc = eager_substep(h);
+    if (rc != MPM_OK) return rc;
+  }
+  MPM_CUDA(h, cudaGetLastError());
+  h->pending_grid = true;
+  return check_status(h);
+}
+
+int mpm_batch_times(mpm_handle* h, double* time, double* last_dt) {
+  if (!h) return MPM_ERR_INVALID_ARG;
+  const size_t ns = h->scenes.size();
+  std::vector<float> dts(ns);
+  if (time) MPM_CUDA(h, cudaMemcpyAsync(time, h->ctx.time_scene, ns * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  MPM_CUDA(h, cudaMemcpyAsync(dts.data(), h->ctx.dt_scene, ns * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
+  MPM_CUDA(h, cudaStreamSynchronize(h->stream));
+  if (last_dt)
+    for (size_t k = 0; k < ns; ++k) last_dt[k] = dts[k];
+  return MPM_OK;
+}
+
+int mpm_batch_ledger(mpm_handle* h, int32_t scene, mpm_ledger* out) {
+  if (!h || !out) return MPM_ERR_INVALID_ARG;
+  if (scene < 0 || scene >= (int)h->scenes.size()) return fail(h, MPM_ERR_INVALID_ARG, "scene index out of range");
+  if (!h->uploaded) return fail(h, MPM_ERR_STATE, "no particles uploaded");
+  // the ledger kernel over this scene's home range: particle arrays offset to p_begin, one scene
+  const SceneDev& sc = h->scenes[scene];
+  const long long pb = sc.p_begin;
+  Ctx c = h->ctx;
+  mpm::Particles& p = c.p;
+  p.qx += pb; p.qy += pb; p.qz += pb;
+  p.vx += pb; p.vy += pb; p.vz += pb;
+  p.C += pb; p.D += pb;
+  for (int e = 0; e < 9; ++e) {
+    p.Cc[e] += pb;
+    p.Dc[e] += pb;
+  }
+  p.m += pb; p.V += pb; p.ep += pb; p.T += pb;
+  p.mat += pb; p.pinned += pb; p.id += pb;
+  c.n = sc.p_end - sc.p_begin;
+  c.scenes = h->ctx.scenes + scene;
+  c.nscenes = 1;
+  std::memset(out, 0, sizeof *out);
+  const int blocks = h->num_sms * 4;
+  { ProfScope ps(h, -1); ProfScope ps2(h, -1); mpm::launch_ledger(c, h->stream, h->ledger_partials, blocks, h->ledger_out); }
+  MPM_CUDA(h, cudaGetLastError());
+  MPM_CUDA(h, cudaMemcpyAsync(h->host_ledger, h->ledger_out, 19 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  MPM_CUDA(h, cudaStreamSynchronize(h->stream));
+  const double* r = h->host_ledger;
+  out->mass = r[0];
+  out->kinetic = r[1];
+  out->affine = r[2];
+  out->potential = r[3];
+  out->elastic = r[4];
+  for (int a = 0; a < 3; ++a) {
+    out->momentum[a] = r[5 + a];
+    out->angular[a] = r[8 + a];
+  }
+  out->min_j = c.n ? r[13] : 1.0;
+  out->max_j = c.n ? r[14] : 1.0;
+  out->max_plastic = r[15];
+  out->max_von_mises = r[16];
+  out->nonfinite = static_cast<int64_t>(r[17]);
+  out->invalid_j = static_cast<int64_t>(r[18]);
+  out->count = c.n;
+  return MPM_OK;
+}
+
+int mpm_batch_grid_debug(mpm_handle* h, int32_t scene, double dt, double* mass, double* momentum) {
+  if (!h || !mass || !momentum) return MPM_ERR_INVALID_ARG;
+  if (scene < 0 || scene >= (int)h->scenes.size()) return fail(h, MPM_ERR_INVALID_ARG, "scene index out of range");
+  if (!h->uploaded) return fail(h, MPM_ERR_STATE, "no particles uploaded");
+  if (!h->grid_valid) {
+    const int rc = prepare_grid(h);
+    if (rc != MPM_OK) return rc;
+  }
+  const SceneDev& s = h->scenes[scene];
+  const size_t nodes = (size_t)s.dims[0] * s.dims[1] * s.dims[2];
+  double* dev = nullptr;
+  MPM_CUDA(h, cudaMalloc(&dev, nodes * 4 * sizeof(double)));
+  mpm::launch_grid_debug(h->ctx, h->stream, scene, static_cast<float>(dt), dev, dev + nodes);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpyAsync(mass, dev, nodes * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(momentum, dev + nodes, nodes * 3 * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  cudaFree(dev);
+  if (e != cudaSuccess) return fail(h, MPM_ERR_CUDA, cudaGetErrorString(e));
+  return MPM_OK;
+}
+
+// Times trial substeps of one schedule from the snapshot; returns ms per substep.
+static int time_schedule(mpm_handle* h, int blocks, int interval, int tma, int trial, double* ms) {
+  int rc = mpm_rollback(h);
+  if (rc != MPM_OK) return rc;
+  drop_graph(h);
+  h->g2p2g_blocks = blocks;
+  h->reorder_interval = interval;
+  h->substeps_since_reorder = 0;
+  h->ctx.use_tma = (tma && h->ctx.tmaps) ? 1 : 0;
+  rc = mpm_step_cfl(h, 2, nullptr);  // warm-up: prepares the grid
+  if (rc != MPM_OK) return rc;
+  cudaEvent_t e0, e1;
+  MPM_CUDA(h, cudaEventCreate(&e0));
+  MPM_CUDA(h, cudaEventCreate(&e1));
+  cudaEventRecord(e0, h->stream);
+  rc = mpm_step_cfl(h, trial, nullptr);
+  cudaEventRecord(e1, h->stream);
+  cudaEventSynchronize(e1);
+  float t = 0;
+  cudaEventElapsedTime(&t, e0, e1);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  *ms = t / trial;
+  return rc;
+}
+
+int mpm_batch_autotune(mpm_handle* h, int32_t trial_substeps, mpm_tuning* out) {
+  if (!h || !out) return MPM_ERR_INVALID_ARG;
+  if (!h->uploaded || h->n == 0) return fail(h, MPM_ERR_STATE, "no particles uploaded");
+  if (trial_substeps <= 0) trial_substeps = 8;
+  int rc = mpm_snapshot(h);
+  if (rc != MPM_OK) return rc;
+  // the trials advance the scenes' clocks too: keep them to restore afterwards
+  std::vector<double> clocks(h->scenes.size());
+  MPM_CUDA(h, cudaMemcpyAsync(clocks.data(), h->ctx.time_scene, clocks.size() * sizeof(double), cudaMemcpyDeviceToHost,
+                              h->stream));
+  MPM_CUDA(h, cudaStreamSynchronize(h->stream));
+  const int def_blocks = h->g2p2g_blocks, def_interval = h->reorder_interval, def_tma = h->ctx.use_tma;
+  const int max_per_sm = mpm::g2p2g_blocks_per_sm(true);
+  struct Cand { int per_sm, interval, tma; };
+  std::vector<Cand> cands;
+  for (int per_sm = 1; per_sm <= max_per_sm; ++per_sm)
+    for (int interval : {8, 32, 128})
+      for (int tma : {1, 0}) {
+        if (tma && !h->ctx.tmaps) continue;
+        cands.push_back({per_sm, interval, tma});
+      }
+  double def_ms = 0;
+  Cand pick{std::max(1, def_blocks / h->num_sms), def_interval, def_tma};
+  rc = time_schedule(h, def_blocks, def_interval, def_tma, trial_substeps, &def_ms);
+  if (rc != MPM_OK) return rc;
+  double best = def_ms;
+  for (const Cand& c : cands) {
+    double ms = 0;
+    rc = time_schedule(h, c.per_sm * h->num_sms, c.interval, c.tma, trial_substeps, &ms);
+    if (rc != MPM_OK) return rc;
+    if (ms < best) {
+      best = ms;
+      pick = c;
+    }
+  }
+  rc = mpm_rollback(h);
+  if (rc != MPM_OK) return rc;
+  MPM_CUDA(h, cudaMemcpyAsync(h->ctx.time_scene, clocks.data(), clocks.size() * sizeof(double), cudaMemcpyHostToDevice,
+                              h->stream));
+  MPM_CUDA(h, cudaStreamSynchronize(h->stream));
+  h->g2p2g_blocks = pick.per_sm * h->num_sms;
+  h->reorder_interval = pick.interval;
+  h->substeps_since_reorder = 0;
+  h->ctx.use_tma = pick.tma;
+  drop_graph(h);
+  out->blocks_per_sm = pick.per_sm;
+  out->reorder_interval = pick.interval;
+  out->use_tma = pick.tma;
+  out->trials = static_cast<int32_t>(cands.size()) + 1;
+  out->ms_per_substep = best;
+  out->ms_per_substep_default = def_ms;
+  return MPM_OK;
 }
 
 }  // extern "C"

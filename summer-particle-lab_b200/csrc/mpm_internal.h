@@ -122,6 +122,7 @@ struct Ctx {
   float* dt_scene;      // per scene
   unsigned* wave_max;   // per scene, float bits of max(|v| + c * stretch)
   unsigned* grad_max;   // per scene, float bits of max sum|C|
+  double* time_scene;   // per scene, simulated time accumulated by substeps
   const void* tmaps;    // per scene CUtensorMap (64-byte aligned), or null
   long long n;
   int nscenes;
@@ -152,6 +153,10 @@ void launch_upload_convert(const Ctx& c, cudaStream_t st, long long n, int dtype
 void launch_download_convert(const Ctx& c, cudaStream_t st, long long n, int dtype, void* const* dst,
                              unsigned fields);
 void launch_permute(const Ctx& c, const Particles& dst, cudaStream_t st);
+// home slots of caller indices a and b into slots[0..1] (-1 when absent)
+void launch_find_ids(const Ctx& c, cudaStream_t st, unsigned a, unsigned b, long long* slots);
+// op 0: reset the deformation of slots[0]; op 1: drop slots[0], slots[1] takes caller index a
+void launch_edit_particle(const Ctx& c, cudaStream_t st, int op, unsigned a, const long long* slots);
 void launch_return_map_batch(const MaterialDev& m, long long n, const double* F_in, const double* ep,
                              const double* T, float dt, double* F_out, double* dep, double* tau,
                              cudaStream_t st);

@@ -285,6 +285,7 @@ __global__ void __launch_bounds__(256) k_begin(Ctx c) {
   if (sdone) return;
   for (int s = threadIdx.x; s < c.nscenes; s += blockDim.x) {
     if (ct->mode != kModeCfl) c.dt_scene[s] = sdt;
+    c.time_scene[s] += static_cast<double>(c.dt_scene[s]);
     c.wave_max[s] = 0u;
     c.grad_max[s] = 0u;
   }
@@ -1381,6 +1382,58 @@ void launch_permute(const Ctx& c, const Particles& dst, cudaStream_t st) {
   if (c.n <= 0) return;
   const long long blocks = (c.n + 255) / 256 < 65536 ? (c.n + 255) / 256 : 65536;
   k_permute<<<static_cast<unsigned>(blocks), 256, 0, st>>>(c, dst);
+}
+
+// Home slots of the caller's particle indices a and b (slots[0], slots[1]; -1 when absent).
+__global__ void k_find_ids(Ctx c, unsigned a, unsigned b, long long* slots) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < c.n; i += (long long)gridDim.x * blockDim.x) {
+    const unsigned id = c.p.id[i];
+    if (id == a) slots[0] = i;
+    if (id == b) slots[1] = i;
+  }
+}
+
+__device__ void copy_slot(const Particles& p, long long dst, long long src) {
+  p.qx[dst] = p.qx[src]; p.qy[dst] = p.qy[src]; p.qz[dst] = p.qz[src];
+  p.vx[dst] = p.vx[src]; p.vy[dst] = p.vy[src]; p.vz[dst] = p.vz[src];
+  for (int e = 0; e < 9; ++e) {
+    p.Cc[e][dst] = p.Cc[e][src];
+    p.Dc[e][dst] = p.Dc[e][src];
+  }
+  p.m[dst] = p.m[src]; p.V[dst] = p.V[src]; p.ep[dst] = p.ep[src]; p.T[dst] = p.T[src];
+  p.mat[dst] = p.mat[src]; p.pinned[dst] = p.pinned[src]; p.id[dst] = p.id[src];
+}
+
+// op 0: MPM3.resetParticle of the particle in slots[0] (src/three/mpm.js:21).
+// op 1: MPM3.remove(p, last) (src/three/mpm.js:22-25): the particle in slots[1] (caller index
+// last) takes caller index p, the particle in slots[0] (caller index p) is dropped, and home slot
+// n - 1 moves into the freed slot so the live slots stay [0, n - 1). The host has checked that
+// both slots exist.
+__global__ void k_edit_particle(Ctx c, int op, unsigned new_id, const long long* slots) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const long long sp = slots[0], sl = slots[1];
+  if (sp < 0 || sp >= c.n || (op == 1 && (sl < 0 || sl >= c.n))) return;
+  if (op == 0) {
+    for (int e = 0; e < 9; ++e) {
+      c.p.Cc[e][sp] = 0.f;
+      c.p.Dc[e][sp] = 0.f;
+    }
+    c.p.ep[sp] = 0.f;
+    return;
+  }
+  c.p.id[sl] = new_id;
+  const long long last = c.n - 1;
+  if (sp != last) copy_slot(c.p, sp, last);
+}
+
+void launch_find_ids(const Ctx& c, cudaStream_t st, unsigned a, unsigned b, long long* slots) {
+  cudaMemsetAsync(slots, 0xff, 2 * sizeof(long long), st);
+  const long long blocks = (c.n + 255) / 256 < 4096 ? (c.n + 255) / 256 : 4096;
+  if (blocks > 0) k_find_ids<<<static_cast<unsigned>(blocks), 256, 0, st>>>(c, a, b, slots);
+}
+
+void launch_edit_particle(const Ctx& c, cudaStream_t st, int op, unsigned a, const long long* slots) {
+  k_edit_particle<<<1, 32, 0, st>>>(c, op, a, slots);
 }
 
 template <typename Tdst>

@@ -50,6 +50,15 @@ class MpmLedger(ctypes.Structure):
                 ("nonfinite", _I64), ("invalid_j", _I64)]
 
 
+class MpmSceneDesc(ctypes.Structure):
+    _fields_ = [("domain", MpmDomain), ("material", _I32), ("reserved", _I32), ("count", _I64)]
+
+
+class MpmTuning(ctypes.Structure):
+    _fields_ = [("blocks_per_sm", _I32), ("reorder_interval", _I32), ("use_tma", _I32), ("trials", _I32),
+                ("ms_per_substep", _D), ("ms_per_substep_default", _D)]
+
+
 class SmpmSim(ctypes.Structure):
     _fields_ = [("count", _I32), ("scene", _I32), ("boundary", _I32), ("gravity", _I32),
                 ("solid_stiffness", _D), ("strength", _D), ("x", _P), ("y", _P), ("vx", _P), ("vy", _P),
@@ -102,6 +111,15 @@ SIGNATURES = {
     "mpm_return_map_batch": (ctypes.c_int, [ctypes.POINTER(MpmMaterial), _I64, _P, _P, _P, _D, _P, _P, _P]),
     "mpm_p2g_noalloc": (ctypes.c_int, [ctypes.POINTER(MpmDomain), ctypes.POINTER(MpmMaterial), _I64, _P, _P, _P, _P, _P,
                                         _P, _D, _P, _P, _P]),
+    "mpm_reset_particle": (ctypes.c_int, [_P, _I64]),
+    "mpm_remove_particle": (ctypes.c_int, [_P, _I64, _I64]),
+    "mpm_batch_create": (ctypes.c_int, [ctypes.POINTER(MpmSceneDesc), _I32, ctypes.POINTER(_P)]),
+    "mpm_batch_count": (ctypes.c_int, [_P, ctypes.POINTER(_I32)]),
+    "mpm_batch_run": (ctypes.c_int, [_P, _I32, _I32]),
+    "mpm_batch_times": (ctypes.c_int, [_P, _P, _P]),
+    "mpm_batch_ledger": (ctypes.c_int, [_P, _I32, ctypes.POINTER(MpmLedger)]),
+    "mpm_batch_grid_debug": (ctypes.c_int, [_P, _I32, _D, _P, _P]),
+    "mpm_batch_autotune": (ctypes.c_int, [_P, _I32, ctypes.POINTER(MpmTuning)]),
     "smpm_create": (ctypes.c_int, [_I64, ctypes.POINTER(_P)]),
     "smpm_destroy": (ctypes.c_int, [_P]),
     "smpm_last_error": (ctypes.c_char_p, [_P]),

@@ -9,7 +9,7 @@ import math
 import numpy as np
 
 from . import _lib
-from ._lib import MpmDomain, MpmMaterial, MpmParticles, MpmLedger, check
+from ._lib import MpmDomain, MpmMaterial, MpmParticles, MpmLedger, MpmSceneDesc, MpmTuning, check
 
 _P = ctypes.c_void_p
 
@@ -200,6 +200,88 @@ class Solver:
         s = _P()
         self._check(_lib.lib().mpm_get_stream(self.h, ctypes.byref(s)))
         return s.value
+
+    def reset_particle(self, index):
+        self._check(_lib.lib().mpm_reset_particle(self.h, int(index)))
+
+    def remove_particle(self, index, last):
+        self._check(_lib.lib().mpm_remove_particle(self.h, int(index), int(last)))
+        self.n -= 1
+
+    def autotune(self, trial_substeps=8):
+        t = MpmTuning()
+        self._check(_lib.lib().mpm_batch_autotune(self.h, int(trial_substeps), ctypes.byref(t)))
+        return dict(blocks_per_sm=t.blocks_per_sm, reorder_interval=t.reorder_interval, use_tma=t.use_tma,
+                    trials=t.trials, ms_per_substep=t.ms_per_substep, ms_per_substep_default=t.ms_per_substep_default)
+
+
+class Batch(Solver):
+    """Many independent scenes on one handle (mpm_batch_*): scene k uses its own domain, grid,
+    CFL dt and material (scene.materials[0], stored at material-table index k)."""
+
+    def __init__(self, scenes):
+        self._keep = []
+        self.scenes = list(scenes)
+        descs = (MpmSceneDesc * len(self.scenes))()
+        for k, sc in enumerate(self.scenes):
+            descs[k].domain = domain_struct(sc.domain)
+            descs[k].material = k
+            descs[k].count = sc.n
+        h = _P()
+        check(_lib.lib().mpm_batch_create(descs, len(self.scenes), ctypes.byref(h)))
+        self.h = h
+        self.domain = self.scenes[0].domain
+        self.capacity = sum(sc.n for sc in self.scenes)
+        self.n = 0
+        self.offsets = np.cumsum([0] + [sc.n for sc in self.scenes])
+
+    def upload(self, scene=None, dtype=np.float64):
+        for k, sc in enumerate(self.scenes):
+            self.set_material(k, sc.materials[0])
+        f = np.dtype(dtype)
+
+        def cat(name, shape=None):
+            if any(getattr(sc, name) is None for sc in self.scenes):
+                return None
+            a = np.concatenate([np.asarray(getattr(sc, name)).reshape((sc.n,) + (shape or ())) for sc in self.scenes])
+            return np.ascontiguousarray(a, dtype=np.uint8 if name == "pinned" else f)
+
+        x, v = cat("x", (3,)), cat("v", (3,))
+        cols = [np.ascontiguousarray(x[:, a]) for a in range(3)] + [np.ascontiguousarray(v[:, a]) for a in range(3)]
+        m, V, T, ep = cat("m"), cat("V"), cat("T"), cat("ep")
+        F, C, pin = cat("F", (9,)), cat("C", (9,)), cat("pinned")
+        p = MpmParticles(dtype=_lib.F64 if f == np.float64 else _lib.F32,
+                         x=_ptr(cols[0]), y=_ptr(cols[1]), z=_ptr(cols[2]), vx=_ptr(cols[3]), vy=_ptr(cols[4]),
+                         vz=_ptr(cols[5]), mass=_ptr(m), volume=_ptr(V), temperature=_ptr(T), plastic=_ptr(ep),
+                         F=_ptr(F), C=_ptr(C), material=None, pinned=_ptr(pin))
+        self._check(_lib.lib().mpm_upload_particles(self.h, self.capacity, ctypes.byref(p)))
+        self.n = self.capacity
+
+    def run(self, nsteps, graph=True):
+        self._check(_lib.lib().mpm_batch_run(self.h, int(nsteps), 1 if graph else 0))
+
+    def times(self):
+        t = np.empty(len(self.scenes))
+        dt = np.empty(len(self.scenes))
+        self._check(_lib.lib().mpm_batch_times(self.h, _ptr(t), _ptr(dt)))
+        return t, dt
+
+    def scene_ledger(self, k):
+        L = MpmLedger()
+        self._check(_lib.lib().mpm_batch_ledger(self.h, int(k), ctypes.byref(L)))
+        return L
+
+    def scene_grid_debug(self, k, dt):
+        nodes = int(np.prod(self.scenes[k].domain.dims))
+        m = np.empty(nodes)
+        p = np.empty((nodes, 3))
+        self._check(_lib.lib().mpm_batch_grid_debug(self.h, int(k), dt, _ptr(m), _ptr(p)))
+        return m, p
+
+    def split(self, out):
+        """Per-scene views of a download() result."""
+        o = self.offsets
+        return [{k: v[o[i]:o[i + 1]] for k, v in out.items()} for i in range(len(self.scenes))]
 
 
 def return_map_batch(material, F, ep=None, T=None, dt=0.01):
