@@ -9,6 +9,11 @@ synthetic input. One step = one requested step of dt=2e-6 s, sub-stepped on the 
 (about 4 substeps); the metric counts actual substeps x particles. Multi-GPU runs are independent
 replicas per GPU (weak scaling; the single-scene path has no exchange step).
 
+The line also carries an "ensemble" block: 256 seeded V&V scenes (particle counts log-uniform in
+5e3..2e5, grids 32..96 cells, per-scene CFL dt) on one batch handle per rank, scenes sharded across
+ranks by cost, against the plain form with one handle per scene (--no-ensemble skips it,
+--ensemble-only runs only it).
+
 --impl reference times the reference's CPU algorithm (the FP64 port under oracle/, all host threads,
 because the reference itself is JavaScript and no JS runtime exists here) on a bounded sub-block
 of the same workload and prints the same JSON line with "impl": "reference".
@@ -44,6 +49,10 @@ def parse():
     ap.add_argument("--shape", default="64,64,64")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-ensemble", action="store_true")
+    ap.add_argument("--ensemble-only", action="store_true")
+    ap.add_argument("--ensemble-scenes", type=int, default=256)
+    ap.add_argument("--ensemble-steps", type=int, default=64)
     return ap.parse_args()
 
 
@@ -182,7 +191,7 @@ def run_reference(args, rank, world):
     if rank != 0:
         return
     scene = make_scene(args)
-    sample = sample_scene(scene, 4)
+    sample = sample_scene(scene, 2)
     threads = os.cpu_count() or 1
     dt = 5e-7
     from oracle import oracle as orc
@@ -205,6 +214,98 @@ def run_reference(args, rank, world):
                                        f"{args.steps} substeps of {dt} s"},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+def ensemble_leg(args, rank, world, dist):
+    """The V&V ensemble (seeded scenes with log-uniform particle counts 5e3..2e5, grids 32..96 cells,
+    E, nu, yield drawn per scene, CFL 0.4 dt per scene): scenes sharded across ranks by cost; each
+    rank steps its scenes on one batch handle (autotuned schedule, substeps replayed from a CUDA
+    graph), timed with CUDA events on the library stream. The plain form steps the same scenes
+    with one single-scene handle each, round-robin, one CFL substep per call (wall clock around
+    the loop, synchronized). Both count particles x substeps."""
+    import torch
+    from mpm_b200 import scenes
+    from mpm_b200.ensemble import gather_ledgers, imbalance, ledger_rows, scene_cost, shard_scenes
+    from mpm_b200.solver import Batch, Solver
+    allsc = scenes.ensemble(args.ensemble_scenes)
+    costs = [scene_cost(sc) for sc in allsc]
+    shards = shard_scenes(costs, world)
+    idx = shards[rank]
+    mine = [allsc[k] for k in idx]
+    K = args.ensemble_steps
+
+    def max_sum(ms, parts):
+        t = torch.tensor([ms, parts], dtype=torch.float64, device="cuda")
+        if dist is not None:
+            dist.all_reduce(t[0:1], op=dist.ReduceOp.MAX)
+            dist.all_reduce(t[1:2], op=dist.ReduceOp.SUM)
+        return float(t[0]), float(t[1])
+
+    n_mine = sum(sc.n for sc in mine)
+    b = Batch(mine)
+    b.upload()
+    tune = b.autotune(6)
+    b.run(K, graph=True)  # warm-up, captures the graph
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    ext = torch.cuda.ExternalStream(b.stream())
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    l0 = b.launch_count()
+    e0.record(ext)
+    b.run(K, graph=True)
+    e1.record(ext)
+    torch.cuda.synchronize()
+    launches = b.launch_count() - l0
+    ms, psteps = max_sum(e0.elapsed_time(e1), n_mine * K)
+    batched = {"value": psteps / (ms / 1e3), "ms_per_substep": ms / K, "substeps": K, "cuda_graph": True,
+               "gpu_launches": launches, "tuning": tune}
+    # roofline of the batched G2P2G from an eagerly profiled stretch
+    b.profile(True)
+    b.run(8, graph=False)
+    prof = b.profile_read()
+    b.profile(False)
+    g_ms, g_n = prof["g2p2g"]
+    active = 0
+    for k, sc in enumerate(mine):
+        gm, _ = b.scene_grid_debug(k, 1e-7)
+        active += int(np.count_nonzero(gm > 0))
+    alg = sum(sc.n * BYTES_PER_PARTICLE[sc.materials[0].model] for sc in mine) + BYTES_PER_NODE * active
+    hbm, peak_kind = peaks()
+    ach = alg / (g_ms / g_n / 1e3) / 1e9 if g_n else None
+    ledgers = gather_ledgers(ledger_rows(b, idx), idx, len(allsc), dist)
+    b.close()
+    # plain: one handle per scene
+    handles = []
+    for sc in mine:
+        h = Solver(sc.domain, sc.n)
+        h.upload(sc)
+        h.step_cfl(1)
+        handles.append(h)
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    Kp = max(2, K // 8)
+    t0 = time.perf_counter()
+    for _ in range(Kp):
+        for h in handles:
+            h.step_cfl(1)
+    torch.cuda.synchronize()
+    pms, pp = max_sum((time.perf_counter() - t0) * 1e3, n_mine * Kp)
+    for h in handles:
+        h.close()
+    plain = {"value": pp / (pms / 1e3), "ms_per_substep": pms / Kp, "substeps": Kp, "handles": len(allsc),
+             "timing": "wall clock around the host loop"}
+    return {"workload": f"vv_ensemble_{len(allsc)}_seeds_1000", "scenes": len(allsc),
+            "particles": int(sum(sc.n for sc in allsc)), "ranks": world,
+            "shard_imbalance": imbalance(costs, shards), "batched": batched, "plain": plain,
+            "speedup_batched_vs_plain": batched["value"] / plain["value"],
+            "roofline": {"bound": "hbm", "kernel": "k_g2p2g (all scenes)", "achieved": ach, "peak": hbm,
+                         "unit": "GB/s", "frac": ach / hbm if ach else None,
+                         "algorithmic_bytes_per_launch": alg, "launch_ms": g_ms / g_n if g_n else None,
+                         "peak_source": peak_kind},
+            "ledger_total_mass": float(ledgers[:, 0].sum()), "ledger_min_j": float(ledgers[:, 5].min())}
 
 
 def main():
@@ -230,6 +331,14 @@ def main():
             dist.destroy_process_group()
         return
 
+    if args.ensemble_only:
+        out = ensemble_leg(args, rank, world, dist)
+        if rank == 0:
+            print(json.dumps({"ensemble": out}), flush=True)
+        if dist is not None:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
     from mpm_b200 import _lib
     from mpm_b200.solver import Solver
     scene = make_scene(args)
@@ -339,12 +448,14 @@ def main():
         for p in ptrs:
             _lib.lib().mpm_host_free(p)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        sample = sample_scene(scene, 4)
+        sample = sample_scene(scene, 2)
         threads = os.cpu_count() or 1
-        rate, el = cpu_oracle_rate(sample, 5e-7, 3, threads)
+        rate, el = cpu_oracle_rate(sample, 5e-7, 30, threads)
         line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
-                                "sample": f"{sample.n}-particle sub-block of the workload, 3 substeps "
+                                "sample": f"{sample.n}-particle sub-block (1/8) of the workload, 30 substeps "
                                           f"({el:.1f} s), FP64 oracle with OpenMP"}
+    if not args.no_ensemble:
+        line["ensemble"] = ensemble_leg(args, rank, world, dist)
     if rank == 0:
         print(json.dumps(line), flush=True)
     sol.close()
