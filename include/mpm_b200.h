@@ -278,6 +278,71 @@ int mpm_batch_grid_debug(mpm_handle* h, int32_t scene, double dt, double* mass, 
 int mpm_batch_autotune(mpm_handle* h, int32_t trial_substeps, mpm_tuning* out);
 
 /* ======================================================================================
+ * Learned return map. No counterpart in the reference, whose return maps are closed-form or
+ * bisection code (src/three/metal-plasticity.js:12-38, src/three/thermal-plasticity.js:12-40):
+ * a small MLP (8 -> 64 -> 64 -> 7, ReLU, BF16 tensor-core arithmetic with FP32 accumulation)
+ * trained on the GPU from samples of this library's exact J2 / thermal-J2 return, used behind
+ * a residual gate that sends every particle it cannot vouch for to the exact map.
+ * Inputs (8): the unit direction of the deviatoric trial Hencky strain (Voigt, 6),
+ * (T - 293) / 307 and ep / 0.2. Outputs (7): the return in the units of the elastic predictor,
+ * (tau - tau_trial) / (2 mu sqrt(3/2) dep_est) (Voigt, 6) and dep / dep_est, with
+ * dep_est = (q_trial - sigma_y) J / (3 mu); the projected stress and increment follow exactly
+ * from them. Training rows carry a sample weight in column 7 (1 plastic, 0 elastic).
+ * Parameters: MPM_SURROGATE_PARAMS floats, W1 [64][16] (inputs 8..15 zero), b1 [64],
+ * W2 [64][64], b2 [64], W3 [8][64] (row 7 zero), b3 [8] (entry 7 zero), W[out][in].
+ * ====================================================================================== */
+#define MPM_SURROGATE_PARAMS 5768
+typedef struct mpm_surrogate mpm_surrogate;
+
+typedef struct mpm_surrogate_config {
+  int64_t samples;       /* training set drawn once from the exact map */
+  int32_t batch;         /* minibatch, a multiple of 16 */
+  int32_t steps;         /* AdamW steps */
+  double lr, weight_decay;
+  double dep_weight;     /* loss weight of the dep output (others 1) */
+  int32_t cosine;        /* 1: cosine learning-rate decay */
+  int32_t reserved;
+  uint64_t seed;
+  double strain_min, strain_max; /* log-uniform magnitude of the principal trial log strains */
+  double T_min, T_max, ep_max;   /* uniform temperature and plastic strain */
+} mpm_surrogate_config;
+
+typedef struct mpm_gate_counts {
+  uint32_t elastic;   /* below yield: exact elastic branch */
+  uint32_t learned;   /* prediction accepted by the gate */
+  uint32_t fallback;  /* prediction rejected: exact return */
+  uint32_t reserved;
+} mpm_gate_counts;
+
+int mpm_surrogate_create(const mpm_material* material, uint64_t seed, mpm_surrogate** out);
+int mpm_surrogate_destroy(mpm_surrogate* s);
+const char* mpm_surrogate_last_error(const mpm_surrogate* s);
+int mpm_surrogate_get_weights(mpm_surrogate* s, float* params);
+int mpm_surrogate_set_weights(mpm_surrogate* s, const float* params);
+/* n training rows from the exact map (X n x 8 features, Y n x 8 targets, column 7 zero); with F
+ * non-null also the trial states (F n x 9, ep, T). */
+int mpm_surrogate_samples(mpm_surrogate* s, const mpm_surrogate_config* cfg, int64_t n, float* X, float* Y, double* F,
+                          double* ep, double* T);
+/* Draws cfg->samples rows and runs cfg->steps AdamW steps on the GPU; loss_history (steps
+ * floats, may be NULL) receives the weighted mean squared error of each minibatch. */
+int mpm_surrogate_train(mpm_surrogate* s, const mpm_surrogate_config* cfg, float* loss_history);
+/* Gradient of the weighted mean squared error over n rows (n a multiple of 16) at the current
+ * weights, from the same forward/backward kernel training uses (no update). */
+int mpm_surrogate_grad(mpm_surrogate* s, int64_t n, const float* X, const float* Y, const float* out_weight,
+                       float* grad, double* loss);
+int mpm_surrogate_forward(mpm_surrogate* s, int64_t n, const float* X, float* Y);
+/* Return map of n trial states (F n x 9 row-major, ep, T) through the gate: F_out n x 9,
+ * dep n, tau n x 9 (Kirchhoff), path n (0 elastic, 1 learned, 2 exact fallback; may be NULL).
+ * use_mlp = 0 runs the exact map for every particle through the same kernel. */
+int mpm_return_map_learned(mpm_surrogate* s, int64_t n, const double* F_in, const double* ep, const double* T,
+                           double gate_tol, int32_t use_mlp, double* F_out, double* dep, double* tau, int8_t* path,
+                           mpm_gate_counts* counts);
+/* Device time per call of the gated map and of the exact map on n device-resident random trial
+ * states drawn like cfg's training set (iters calls each, CUDA events). */
+int mpm_surrogate_time(mpm_surrogate* s, const mpm_surrogate_config* cfg, int64_t n, int32_t iters, double gate_tol,
+                       double* ms_exact, double* ms_learned, mpm_gate_counts* counts);
+
+/* ======================================================================================
  * 2D elastic solid: drop-in for the reference's SolidMPM (src/solid-mpm.js:20-116).
  * Fixed 149 x 149 node grid, DX = 8, origin -592 (src/solid-mpm.js:4); fixed-corotated
  * elasticity with E = rho * 16000 * solidStiffness and mu = lambda = 0.4 E. The handle owns

@@ -59,6 +59,20 @@ class MpmTuning(ctypes.Structure):
                 ("ms_per_substep", _D), ("ms_per_substep_default", _D)]
 
 
+class MpmSurrogateConfig(ctypes.Structure):
+    _fields_ = [("samples", _I64), ("batch", _I32), ("steps", _I32), ("lr", _D), ("weight_decay", _D),
+                ("dep_weight", _D), ("cosine", _I32), ("reserved", _I32), ("seed", ctypes.c_uint64),
+                ("strain_min", _D), ("strain_max", _D), ("T_min", _D), ("T_max", _D), ("ep_max", _D)]
+
+
+class MpmGateCounts(ctypes.Structure):
+    _fields_ = [("elastic", ctypes.c_uint32), ("learned", ctypes.c_uint32), ("fallback", ctypes.c_uint32),
+                ("reserved", ctypes.c_uint32)]
+
+
+SURROGATE_PARAMS = 5768
+
+
 class SmpmSim(ctypes.Structure):
     _fields_ = [("count", _I32), ("scene", _I32), ("boundary", _I32), ("gravity", _I32),
                 ("solid_stiffness", _D), ("strength", _D), ("x", _P), ("y", _P), ("vx", _P), ("vy", _P),
@@ -120,6 +134,19 @@ SIGNATURES = {
     "mpm_batch_ledger": (ctypes.c_int, [_P, _I32, ctypes.POINTER(MpmLedger)]),
     "mpm_batch_grid_debug": (ctypes.c_int, [_P, _I32, _D, _P, _P]),
     "mpm_batch_autotune": (ctypes.c_int, [_P, _I32, ctypes.POINTER(MpmTuning)]),
+    "mpm_surrogate_create": (ctypes.c_int, [ctypes.POINTER(MpmMaterial), ctypes.c_uint64, ctypes.POINTER(_P)]),
+    "mpm_surrogate_destroy": (ctypes.c_int, [_P]),
+    "mpm_surrogate_last_error": (ctypes.c_char_p, [_P]),
+    "mpm_surrogate_get_weights": (ctypes.c_int, [_P, _P]),
+    "mpm_surrogate_set_weights": (ctypes.c_int, [_P, _P]),
+    "mpm_surrogate_samples": (ctypes.c_int, [_P, ctypes.POINTER(MpmSurrogateConfig), _I64, _P, _P, _P, _P, _P]),
+    "mpm_surrogate_train": (ctypes.c_int, [_P, ctypes.POINTER(MpmSurrogateConfig), _P]),
+    "mpm_surrogate_grad": (ctypes.c_int, [_P, _I64, _P, _P, _P, _P, ctypes.POINTER(_D)]),
+    "mpm_surrogate_forward": (ctypes.c_int, [_P, _I64, _P, _P]),
+    "mpm_return_map_learned": (ctypes.c_int, [_P, _I64, _P, _P, _P, _D, _I32, _P, _P, _P, _P,
+                                               ctypes.POINTER(MpmGateCounts)]),
+    "mpm_surrogate_time": (ctypes.c_int, [_P, ctypes.POINTER(MpmSurrogateConfig), _I64, _I32, _D, ctypes.POINTER(_D),
+                                           ctypes.POINTER(_D), ctypes.POINTER(MpmGateCounts)]),
     "smpm_create": (ctypes.c_int, [_I64, ctypes.POINTER(_P)]),
     "smpm_destroy": (ctypes.c_int, [_P]),
     "smpm_last_error": (ctypes.c_char_p, [_P]),
