@@ -12,7 +12,8 @@ replicas per GPU (weak scaling; the single-scene path has no exchange step).
 The line also carries an "ensemble" block: 256 seeded V&V scenes (particle counts log-uniform in
 5e3..2e5, grids 32..96 cells, per-scene CFL dt) on one batch handle per rank, scenes sharded across
 ranks by cost, against the plain form with one handle per scene (--no-ensemble skips it,
---ensemble-only runs only it).
+--ensemble-only runs only it), and at N=1 a "surrogate" block: the learned return map trained on
+the GPU and timed, gated, against the exact map (--no-surrogate skips it).
 
 --impl reference times the reference's CPU algorithm (the FP64 port under oracle/, all host threads,
 because the reference itself is JavaScript and no JS runtime exists here) on a bounded sub-block
@@ -50,6 +51,9 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-ensemble", action="store_true")
+    ap.add_argument("--no-surrogate", action="store_true")
+    ap.add_argument("--surrogate-only", action="store_true")
+    ap.add_argument("--surrogate-steps", type=int, default=0, help="training steps (0: the default schedule)")
     ap.add_argument("--ensemble-only", action="store_true")
     ap.add_argument("--ensemble-scenes", type=int, default=256)
     ap.add_argument("--ensemble-steps", type=int, default=64)
@@ -308,6 +312,50 @@ def ensemble_leg(args, rank, world, dist):
             "ledger_total_mass": float(ledgers[:, 0].sum()), "ledger_min_j": float(ledgers[:, 5].min())}
 
 
+def surrogate_leg(steps=0):
+    """Learned return map on the thermo-elastoplastic law (J2, yield 250 MPa softening 0.3 MPa/K):
+    training on the GPU (10M exact-map samples, BF16 tensor-core forward/backward, AdamW), then
+    the gated map against the exact map on 4,096,000 device-resident trial states (trial log
+    strains log-uniform 1e-5..5e-2, random directions, T 293..600 K, ep 0..0.2), CUDA events."""
+    import torch
+    from mpm_b200 import scenes
+    from mpm_b200.params import MODEL_THERMAL_J2
+    from mpm_b200.surrogate import Surrogate, config
+    T_ref, hot = 293.0, 0.001
+    mat = scenes.aluminium_j2(MODEL_THERMAL_J2, T_ref=T_ref, T_hot=T_ref + (1 - hot) * 250e6 / 0.3e6, hot_ratio=hot,
+                              heat_fraction=0.9, specific_heat=900.0)
+    s = Surrogate(mat, seed=5)
+    cfg = config(steps=steps) if steps > 0 else config()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    hist = s.train(cfg)
+    el = time.perf_counter() - t0
+    mlp_flop = 2 * (8 * 64 + 64 * 64 + 64 * 7)  # forward per sample; backward is about twice that
+    train_flops = 3.0 * mlp_flop * cfg.batch * cfg.steps
+    bf16_peak = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["bf16_tflops"] if os.path.exists(
+        os.path.join(ROOT, "MEASURED_PEAKS.json")) else 1590.0
+    n = 4_096_000
+    rows = []
+    for tol in (2e-3, 5e-3, 1e-2):
+        r = s.time(n, iters=10, gate_tol=tol)
+        plastic = r["learned"] + r["fallback"]
+        rows.append({"gate_tol": tol, "stated_stress_error_of_accepted": f"{4 * tol:g} x yield",
+                     "ms_exact": r["ms_exact"], "ms_gated": r["ms_learned"],
+                     "speedup_gated_vs_exact": r["ms_exact"] / r["ms_learned"],
+                     "elastic": r["elastic"], "learned": r["learned"], "fallback": r["fallback"],
+                     "learned_share_of_plastic": r["learned"] / plastic if plastic else None})
+    s.close()
+    return {"law": "thermal J2 (model 10), E 70 GPa, nu 0.33, yield 250 MPa, H 1 GPa, -0.3 MPa/K",
+            "network": "8-64-64-7 ReLU, BF16 mma.sync m16n8k16, FP32 accumulate",
+            "training": {"samples": cfg.samples, "batch": cfg.batch, "steps": cfg.steps, "seconds": el,
+                         "loss_first": float(hist[:10].mean()), "loss_last": float(hist[-100:].mean()),
+                         "mlp_tflops": train_flops / el / 1e12,
+                         "tensor_frac_of_measured_bf16": train_flops / el / 1e12 / bf16_peak,
+                         "note": "wall clock of the whole call, sample generation included"},
+            "return_map_4096000_states": rows,
+            "exact_stress_error": "FP32 exact map: within 1e-5 x yield of the FP64 oracle (tests/test_surrogate.py)"}
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -331,6 +379,13 @@ def main():
             dist.destroy_process_group()
         return
 
+    if args.surrogate_only:
+        if rank == 0:
+            print(json.dumps({"surrogate": surrogate_leg(args.surrogate_steps)}), flush=True)
+        if dist is not None:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
     if args.ensemble_only:
         out = ensemble_leg(args, rank, world, dist)
         if rank == 0:
@@ -456,6 +511,8 @@ def main():
                                           f"({el:.1f} s), FP64 oracle with OpenMP"}
     if not args.no_ensemble:
         line["ensemble"] = ensemble_leg(args, rank, world, dist)
+    if rank == 0 and world == 1 and not args.no_surrogate:
+        line["surrogate"] = surrogate_leg(args.surrogate_steps)
     if rank == 0:
         print(json.dumps(line), flush=True)
     sol.close()
