@@ -251,6 +251,8 @@ typedef struct mpm_scene_desc {
 } mpm_scene_desc;
 
 typedef struct mpm_tuning {
+  int32_t warp_specialised;  /* 1: producer/consumer scatter pass (one 512-thread CTA per SM) */
+  int32_t reserved;
   int32_t blocks_per_sm;     /* resident G2P2G CTAs per SM chosen */
   int32_t reorder_interval;  /* substeps between physical re-sorts of the particle state */
   int32_t use_tma;           /* TMA (1) or plain loads (0) for the gather window */
@@ -272,8 +274,8 @@ int mpm_batch_times(mpm_handle* h, double* time, double* last_dt);
 int mpm_batch_ledger(mpm_handle* h, int32_t scene, mpm_ledger* out);
 /* Grid mass and momentum of one scene after P2G (like mpm_grid_debug). */
 int mpm_batch_grid_debug(mpm_handle* h, int32_t scene, double dt, double* mass, double* momentum);
-/* Autotuner: times trial_substeps substeps for each G2P2G schedule (CTAs per SM, re-sort
- * interval, TMA or plain gather) from the same snapshot of the state, keeps the fastest and
+/* Autotuner: times trial_substeps substeps for each G2P2G schedule (warp-specialised or not,
+ * CTAs per SM, re-sort interval, TMA or plain gather) from the same snapshot of the state, keeps the fastest and
  * restores the state and the scenes' clocks. Works on any handle. */
 int mpm_batch_autotune(mpm_handle* h, int32_t trial_substeps, mpm_tuning* out);
 

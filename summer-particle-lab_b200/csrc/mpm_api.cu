@@ -96,6 +96,7 @@ struct mpm_handle {
   double* host_ledger = nullptr;                         // pinned readback
   Ctx ctx{};
   int g2p2g_blocks = 0, p2g_blocks = 0, grid_blocks = 0;
+  int ws_blocks = 0;  // warp-specialised scatter passes available (CTAs), 0: not available
   // profiling: event pairs around launches while enabled
   bool profiling = false;
   std::vector<cudaEvent_t> ev_pool;
@@ -545,6 +546,12 @@ int mpm_create(const mpm_domain* domain, int64_t capacity, mpm_handle** out) {
   if (alloc_grid(h) != MPM_OK) return bail(MPM_ERR_OUT_OF_MEMORY);
   mpm::g2p2g_blocks_per_sm(false);  // sets the dynamic shared memory limit of the no-scatter pass
   h->g2p2g_blocks = h->num_sms * mpm::g2p2g_blocks_per_sm(true);
+  // The warp-specialised scatter passes (one 512-thread CTA per SM) are an autotuner candidate; on
+  // the 2M-particle J2 drop they measured 0.49 ms per substep against 0.43 ms for the two-CTA
+  // kernel, so they start off (MPM_B200_WS=1 makes them the default).
+  const int ws_per_sm = mpm::ws_blocks_per_sm();
+  h->ws_blocks = ws_per_sm > 0 ? h->num_sms * ws_per_sm : 0;
+  h->ctx.ws_blocks = std::getenv("MPM_B200_WS") ? h->ws_blocks : 0;
   h->p2g_blocks = h->num_sms * mpm::p2g_blocks_per_sm();
   h->grid_blocks = h->num_sms * 8;
   if (cudaStreamSynchronize(h->stream) != cudaSuccess) return bail(MPM_ERR_CUDA);
@@ -1514,10 +1521,11 @@ int mpm_batch_grid_debug(mpm_handle* h, int32_t scene, double dt, double* mass, 
 }
 
 // Times trial substeps of one schedule from the snapshot; returns ms per substep.
-static int time_schedule(mpm_handle* h, int blocks, int interval, int tma, int trial, double* ms) {
+static int time_schedule(mpm_handle* h, int ws, int blocks, int interval, int tma, int trial, double* ms) {
   int rc = mpm_rollback(h);
   if (rc != MPM_OK) return rc;
   drop_graph(h);
+  h->ctx.ws_blocks = ws ? h->ws_blocks : 0;
   h->g2p2g_blocks = blocks;
   h->reorder_interval = interval;
   h->substeps_since_reorder = 0;
@@ -1551,23 +1559,25 @@ int mpm_batch_autotune(mpm_handle* h, int32_t trial_substeps, mpm_tuning* out) {
                               h->stream));
   MPM_CUDA(h, cudaStreamSynchronize(h->stream));
   const int def_blocks = h->g2p2g_blocks, def_interval = h->reorder_interval, def_tma = h->ctx.use_tma;
+  const int def_ws = h->ctx.ws_blocks > 0 ? 1 : 0;
   const int max_per_sm = mpm::g2p2g_blocks_per_sm(true);
-  struct Cand { int per_sm, interval, tma; };
+  struct Cand { int ws, per_sm, interval, tma; };
   std::vector<Cand> cands;
-  for (int per_sm = 1; per_sm <= max_per_sm; ++per_sm)
-    for (int interval : {8, 32, 128})
-      for (int tma : {1, 0}) {
-        if (tma && !h->ctx.tmaps) continue;
-        cands.push_back({per_sm, interval, tma});
-      }
+  for (int ws = (h->ws_blocks > 0 ? 1 : 0); ws >= 0; --ws)
+    for (int per_sm = 1; per_sm <= (ws ? 1 : max_per_sm); ++per_sm)
+      for (int interval : {8, 32, 128})
+        for (int tma : {1, 0}) {
+          if (tma && !h->ctx.tmaps) continue;
+          cands.push_back({ws, ws ? def_blocks / h->num_sms : per_sm, interval, tma});
+        }
   double def_ms = 0;
-  Cand pick{std::max(1, def_blocks / h->num_sms), def_interval, def_tma};
-  rc = time_schedule(h, def_blocks, def_interval, def_tma, trial_substeps, &def_ms);
+  Cand pick{def_ws, std::max(1, def_blocks / h->num_sms), def_interval, def_tma};
+  rc = time_schedule(h, def_ws, def_blocks, def_interval, def_tma, trial_substeps, &def_ms);
   if (rc != MPM_OK) return rc;
   double best = def_ms;
   for (const Cand& c : cands) {
     double ms = 0;
-    rc = time_schedule(h, c.per_sm * h->num_sms, c.interval, c.tma, trial_substeps, &ms);
+    rc = time_schedule(h, c.ws, c.per_sm * h->num_sms, c.interval, c.tma, trial_substeps, &ms);
     if (rc != MPM_OK) return rc;
     if (ms < best) {
       best = ms;
@@ -1583,8 +1593,10 @@ int mpm_batch_autotune(mpm_handle* h, int32_t trial_substeps, mpm_tuning* out) {
   h->reorder_interval = pick.interval;
   h->substeps_since_reorder = 0;
   h->ctx.use_tma = pick.tma;
+  h->ctx.ws_blocks = pick.ws ? h->ws_blocks : 0;
   drop_graph(h);
-  out->blocks_per_sm = pick.per_sm;
+  out->warp_specialised = pick.ws;
+  out->blocks_per_sm = pick.ws ? h->ws_blocks / h->num_sms : pick.per_sm;
   out->reorder_interval = pick.interval;
   out->use_tma = pick.tma;
   out->trials = static_cast<int32_t>(cands.size()) + 1;

@@ -133,6 +133,7 @@ struct Ctx {
   int has_thermal;      // temperature array is read and written
   int has_plastic;      // plastic strain array is read and written
   int use_tma;
+  int ws_blocks;        // > 0: the particle passes that scatter run warp-specialised on this many CTAs
 };
 
 // Launch wrappers (mpm_kernels.cu)
@@ -161,6 +162,7 @@ void launch_return_map_batch(const MaterialDev& m, long long n, const double* F_
                              const double* T, float dt, double* F_out, double* dep, double* tau,
                              cudaStream_t st);
 int g2p2g_blocks_per_sm(bool scatter);
+int ws_blocks_per_sm();
 int p2g_blocks_per_sm();
 
 // field bits of the conversion kernels

@@ -533,30 +533,36 @@ __device__ __noinline__ void scatter_global(const Ctx& c, const SceneDev& sc, co
 
 // Flush the shared scatter window of one tile to the global accumulators (one float4 atomic per
 // touched node and channel group) and clear it; mark the 27 node tiles it covers as active.
-__device__ __forceinline__ void flush_window(const Ctx& c, const SceneDev& sc, PartSmem& sm, int nxt,
-                                             const int tile[3]) {
+// tid / nthreads: this thread's index among the threads that flush.
+__device__ __forceinline__ void flush_window_p(const Ctx& c, const SceneDev& sc, float* acc, int nxt, const int tile[3],
+                                               int tid, int nthreads) {
   const int o0 = tile[0] * kTile - 1, o1 = tile[1] * kTile - 1, o2 = tile[2] * kTile - 1;
-  for (int i = threadIdx.x; i < kWinSNodes; i += kBlock) {
-    const float mass = sm.acc[i];
+  for (int i = tid; i < kWinSNodes; i += nthreads) {
+    const float mass = acc[i];
     if (mass != 0.f) {
       const int x = o0 + (i & 7), y = o1 + ((i >> 3) & 7), z = o2 + (i >> 6);
       if (x >= 0 && y >= 0 && z >= 0) {
         const long long node = sc.node_base + ((long long)z * sc.gdim[1] + y) * sc.gdim[0] + x;
-        atomicAdd(&c.g.acc0[nxt][node], make_float4(mass, sm.acc[1 * kWinSNodes + i], sm.acc[2 * kWinSNodes + i],
-                                                    sm.acc[3 * kWinSNodes + i]));
-        atomicAdd(&c.g.acc1[nxt][node], make_float4(sm.acc[4 * kWinSNodes + i], sm.acc[5 * kWinSNodes + i],
-                                                    sm.acc[6 * kWinSNodes + i], sm.acc[7 * kWinSNodes + i]));
+        atomicAdd(&c.g.acc0[nxt][node], make_float4(mass, acc[1 * kWinSNodes + i], acc[2 * kWinSNodes + i],
+                                                    acc[3 * kWinSNodes + i]));
+        atomicAdd(&c.g.acc1[nxt][node], make_float4(acc[4 * kWinSNodes + i], acc[5 * kWinSNodes + i],
+                                                    acc[6 * kWinSNodes + i], acc[7 * kWinSNodes + i]));
       }
     }
 #pragma unroll
-    for (int ch = 0; ch < kChannels; ++ch) sm.acc[ch * kWinSNodes + i] = 0.f;
+    for (int ch = 0; ch < kChannels; ++ch) acc[ch * kWinSNodes + i] = 0.f;
   }
-  if (threadIdx.x < 27) {
-    const int dx = threadIdx.x % 3 - 1, dy = (threadIdx.x / 3) % 3 - 1, dz = threadIdx.x / 9 - 1;
+  if (tid < 27) {
+    const int dx = tid % 3 - 1, dy = (tid / 3) % 3 - 1, dz = tid / 9 - 1;
     const int tx = tile[0] + dx, ty = tile[1] + dy, tz = tile[2] + dz;
     if (tx >= 0 && ty >= 0 && tz >= 0 && tx < sc.ntiles[0] && ty < sc.ntiles[1] && tz < sc.ntiles[2])
       mark_node_tile(c, sc.node_tile_base + (tz * sc.ntiles[1] + ty) * sc.ntiles[0] + tx, nxt);
   }
+}
+
+__device__ __forceinline__ void flush_window(const Ctx& c, const SceneDev& sc, PartSmem& sm, int nxt,
+                                             const int tile[3]) {
+  flush_window_p(c, sc, sm.acc, nxt, tile, threadIdx.x, kBlock);
 }
 
 // Block reduction of the per-thread CFL maxima and status flags of one tile, then one atomic per
@@ -598,7 +604,8 @@ __device__ __forceinline__ unsigned state_flags(const float v[3], const float D[
 
 // Phase B task: one non-empty base bucket, one z layer of its stencil. Sums the 3x3 nodes x 7
 // channels over the bucket's particles in registers, then adds them to the shared window.
-__device__ __forceinline__ void bucket_layer(PartSmem& sm, int b, int kz) {
+__device__ __forceinline__ void bucket_layer_p(const float* pay, const unsigned short* sidx, const int* bstart,
+                                               float* acc, int b, int kz) {
   const int lx = b % 6, ly = (b / 6) % 6, lz = b / 36;
   float a[3][3][7];
 #pragma unroll
@@ -607,10 +614,10 @@ __device__ __forceinline__ void bucket_layer(PartSmem& sm, int b, int kz) {
     for (int x = 0; x < 3; ++x)
 #pragma unroll
       for (int ch = 0; ch < 7; ++ch) a[y][x][ch] = 0.f;
-  const int i1 = sm.bstart[b + 1];
-  for (int i = sm.bstart[b]; i < i1; ++i) {
-    const int j = sm.sidx[i];
-    const float* P = sm.pay + j;
+  const int i1 = bstart[b + 1];
+  for (int i = bstart[b]; i < i1; ++i) {
+    const int j = sidx[i];
+    const float* P = pay + j;
     const float tx = P[0 * kCap], ty = P[1 * kCap], tz = P[2 * kCap], m = P[3 * kCap];
     const float mv0 = P[4 * kCap], mv1 = P[5 * kCap], mv2 = P[6 * kCap];
     const float c00 = P[7 * kCap], c01 = P[8 * kCap], c02 = P[9 * kCap];
@@ -654,33 +661,42 @@ __device__ __forceinline__ void bucket_layer(PartSmem& sm, int b, int kz) {
     for (int x = 0; x < 3; ++x) {
       const int node = ((lz + kz) * kWinS + (ly + y)) * kWinS + (lx + x);
 #pragma unroll
-      for (int ch = 0; ch < 7; ++ch) atomicAdd(&sm.acc[ch * kWinSNodes + node], a[y][x][ch]);
+      for (int ch = 0; ch < 7; ++ch) atomicAdd(&acc[ch * kWinSNodes + node], a[y][x][ch]);
     }
 }
 
+__device__ __forceinline__ void bucket_layer(PartSmem& sm, int b, int kz) {
+  bucket_layer_p(sm.pay, sm.sidx, sm.bstart, sm.acc, b, kz);
+}
+
 // Exclusive scan of the bucket histogram by warp 0, with the compact list of non-empty buckets.
-__device__ __forceinline__ void scan_buckets(PartSmem& sm) {
-  if (threadIdx.x >= 32) return;
-  const int lane = threadIdx.x;
+// lane: 0..31 of the one warp that scans.
+__device__ __forceinline__ void scan_buckets_p(const int* hist, int* bstart, unsigned short* blist, int* nbuckets,
+                                               int lane) {
   int carry = 0, ncarry = 0;
   for (int b0 = 0; b0 < kBuckets; b0 += 32) {
     const int b = b0 + lane;
-    const int h = b < kBuckets ? sm.hist[b] : 0;
+    const int h = b < kBuckets ? hist[b] : 0;
     int inc = h;
     for (int o = 1; o < 32; o <<= 1) {
       const int y = __shfl_up_sync(0xffffffffu, inc, o);
       if (lane >= o) inc += y;
     }
-    if (b < kBuckets) sm.bstart[b] = carry + inc - h;
+    if (b < kBuckets) bstart[b] = carry + inc - h;
     const unsigned nz = __ballot_sync(0xffffffffu, h > 0);
-    if (h > 0) sm.blist[ncarry + __popc(nz & ((1u << lane) - 1u))] = static_cast<unsigned short>(b);
+    if (h > 0) blist[ncarry + __popc(nz & ((1u << lane) - 1u))] = static_cast<unsigned short>(b);
     carry += __shfl_sync(0xffffffffu, inc, 31);
     ncarry += __popc(nz);
   }
   if (lane == 0) {
-    sm.bstart[kBuckets] = carry;
-    sm.nbuckets = ncarry;
+    bstart[kBuckets] = carry;
+    *nbuckets = ncarry;
   }
+}
+
+__device__ __forceinline__ void scan_buckets(PartSmem& sm) {
+  if (threadIdx.x >= 32) return;
+  scan_buckets_p(sm.hist, sm.bstart, sm.blist, &sm.nbuckets, threadIdx.x);
 }
 
 
@@ -732,6 +748,156 @@ __device__ __forceinline__ void gather27(Ld ld, const float t[3], const float w[
 __device__ __noinline__ void gather_global(const float4* base, int sy, long long sz, const float t[3], const float w[3][3],
                                            float out[12]) {
   gather27([&](int kz, int ky, int kx) { return base[kz * sz + ky * sy + kx]; }, t, w, out);
+}
+
+// Phase A of one particle (home slot `home`, payload row j): G2P from the staged window, F update,
+// fixed-point advection and the constitutive update / return map (src/three/mpm.js:107-131), or,
+// for the P2G pass and pinned particles, the stress of the stored state; then the scatter payload
+// bucketed by its new stencil base in the shared window (pay, meta, hist), and the CFL terms.
+// Writes the particle's new state and returns its next sort key (all ones when not needed).
+template <int PASS>
+__device__ __forceinline__ unsigned particle_phase_a(const Ctx& c, const SceneDev& sc, const TileCtx& tc,
+                                                     const MaterialDev& mt_single, bool single, const float4* vwin,
+                                                     unsigned home, unsigned j, float dt, int nxt, float* pay,
+                                                     unsigned* meta, int* hist, float& wave_acc, float& grad_acc,
+                                                     unsigned& flags_acc, double& work_acc) {
+  constexpr bool SCATTER = PASS != kPassG2P;
+  constexpr bool GATHER = PASS != kPassP2G;
+  unsigned key = 0xffffffffu;
+  unsigned q[3] = {c.p.qx[home], c.p.qy[home], c.p.qz[home]};
+  float D[9];
+#pragma unroll
+  for (int e = 0; e < 9; ++e) D[e] = c.p.Dc[e][home];
+  const float m = c.p.m[home], V = c.p.V[home];
+  const MaterialDev mt = single ? mt_single : c.mats[c.p.mat[home]];
+  const bool pinned = c.has_pinned && c.p.pinned[home];
+  float ep = c.has_plastic ? c.p.ep[home] : 0.f;
+  float T = c.has_thermal ? c.p.T[home] : 0.f;
+  float v[3], C[9];
+  ConstitutiveOut co;
+  unsigned flags = 0;
+  if (GATHER && !pinned) {
+    int b[3];
+    float t[3], w[3][3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      stencil_axis(q[a], tc.dims[a], b[a], t[a]);
+      bspline_weights(t[a], w[a]);
+    }
+    const int l0 = b[0] - tc.tile[0] * kTile, l1 = b[1] - tc.tile[1] * kTile, l2 = b[2] - tc.tile[2] * kTile;
+    // the sort key places the stencil inside the staged window; if it ever does not, the
+    // particle reads the grid from global memory instead (and the step reports it)
+    const bool in_g = l0 >= 0 && l0 <= kWinG - 3 && l1 >= 0 && l1 <= kWinG - 3 && l2 >= 0 && l2 <= kWinG - 3;
+    if (!in_g) flags |= 0x20u;
+    // G2P (src/three/mpm.js:107-118): v = sum w v_i, C = sum w v_i (i - t)^T 4/h
+    float acc12[12];
+    if (in_g) {
+      const float4* win = &vwin[(l2 * kWinG + l1) * kWinG + l0];
+      gather27([&](int kz, int ky, int kx) { return win[(kz * kWinG + ky) * kWinG + kx]; }, t, w, acc12);
+    } else {
+      gather_global(c.g.vel + tc.node_base + ((long long)b[2] * tc.gdim[1] + b[1]) * tc.gdim[0] + b[0], tc.gdim[0],
+                    (long long)tc.gdim[0] * tc.gdim[1], t, w, acc12);
+    }
+    const float v0 = acc12[0], v1 = acc12[1], v2 = acc12[2];
+    const float c0 = acc12[3], c1 = acc12[4], c2 = acc12[5], c3 = acc12[6], c4 = acc12[7], c5 = acc12[8],
+                c6 = acc12[9], c7 = acc12[10], c8 = acc12[11];
+    const float s4 = 4.f * tc.invH;
+    v[0] = v0; v[1] = v1; v[2] = v2;
+    C[0] = c0 * s4; C[1] = c1 * s4; C[2] = c2 * s4;
+    C[3] = c3 * s4; C[4] = c4 * s4; C[5] = c5 * s4;
+    C[6] = c6 * s4; C[7] = c7 * s4; C[8] = c8 * s4;
+    // F <- (I + dt C) F in centred form: D <- D + dt C (I + D) (src/three/mpm.js:119-121)
+    float Dn[9];
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+      for (int bc = 0; bc < 3; ++bc)
+        Dn[a * 3 + bc] = D[a * 3 + bc] + dt * (C[a * 3 + bc] + C[a * 3 + 0] * D[0 * 3 + bc] +
+                                               C[a * 3 + 1] * D[1 * 3 + bc] + C[a * 3 + 2] * D[2 * 3 + bc]);
+#pragma unroll
+    for (int e = 0; e < 9; ++e) D[e] = Dn[e];
+    // x += dt v (src/three/mpm.js:122) in fixed point, clamped into the box
+    const float s = dt * tc.invH * kFixedOne;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      // |dq| stays below 2^30 (a particle moves far less than 256 cells in a substep)
+      long long qn = static_cast<long long>(q[a]) + __float2int_rn(fminf(fmaxf(s * v[a], -1.0e9f), 1.0e9f));
+      if (tc.clamp) {
+        qn = qn < (long long)tc.qlo[a] ? (long long)tc.qlo[a] : qn;
+        qn = qn > (long long)tc.qhi[a] ? (long long)tc.qhi[a] : qn;
+      } else {
+        const long long hi = (static_cast<long long>(tc.dims[a]) - 1) << kFracBits;
+        if (qn < 0 || qn > hi) flags |= 0x4u;
+        qn = qn < 0 ? 0 : (qn > hi ? hi : qn);
+      }
+      q[a] = static_cast<unsigned>(qn);
+    }
+    // return map / stress for the next P2G (src/three/mpm.js:126-131)
+    co = constitutive_update(mt, D, ep, T, V / m, true);
+    ep += co.dep;
+    T += co.dT;
+    c.p.qx[home] = q[0]; c.p.qy[home] = q[1]; c.p.qz[home] = q[2];
+    c.p.vx[home] = v[0]; c.p.vy[home] = v[1]; c.p.vz[home] = v[2];
+#pragma unroll
+    for (int e = 0; e < 9; ++e) {
+      c.p.Cc[e][home] = C[e];
+      c.p.Dc[e][home] = D[e];
+    }
+    if (c.has_plastic) c.p.ep[home] = ep;
+    if (c.has_thermal) c.p.T[home] = T;
+    if (co.dep > 0.f && mt.heat_per_work > 0.f) work_acc += static_cast<double>(co.dT) * m / mt.heat_per_work;
+  } else {
+    // P2G of the stored state, and pinned particles (not moved, src/three/mpm.js:108)
+    v[0] = c.p.vx[home]; v[1] = c.p.vy[home]; v[2] = c.p.vz[home];
+#pragma unroll
+    for (int e = 0; e < 9; ++e) C[e] = c.p.Cc[e][home];
+    float Dc[9];
+#pragma unroll
+    for (int e = 0; e < 9; ++e) Dc[e] = D[e];
+    co = constitutive_update(mt, Dc, ep, T, V / m, false);
+  }
+  if (SCATTER) {
+    // payload of the scatter: fraction t, m, m v, m C h, -4 V / h tau
+    int nb[3];
+    float t[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) stencil_axis(q[a], tc.dims[a], nb[a], t[a]);
+    key = tile_key(sc, nb);
+    if (PASS == kPassG2P2G) c.p.key[home] = key;
+    const float mv[3] = {m * v[0], m * v[1], m * v[2]};
+    const float mH = m * tc.H;
+    float mC[9];
+#pragma unroll
+    for (int e = 0; e < 9; ++e) mC[e] = mH * C[e];
+    const float sv = -4.f * V * tc.invH;
+    const float s6[6] = {sv * co.tau.xx, sv * co.tau.yy, sv * co.tau.zz, sv * co.tau.xy, sv * co.tau.xz, sv * co.tau.yz};
+    const int l0 = nb[0] - (tc.tile[0] * kTile - 1), l1 = nb[1] - (tc.tile[1] * kTile - 1),
+              l2 = nb[2] - (tc.tile[2] * kTile - 1);
+    const bool in_w = l0 >= 0 && l0 <= kWinS - 3 && l1 >= 0 && l1 <= kWinS - 3 && l2 >= 0 && l2 <= kWinS - 3;
+    if (in_w && !pinned) {
+      const int bucket = (l2 * 6 + l1) * 6 + l0;
+      const int rank = atomicAdd(&hist[bucket], 1);
+      meta[j] = static_cast<unsigned>(bucket) | (static_cast<unsigned>(rank) << 8);
+      float* P = pay + j;
+      P[0 * kCap] = t[0]; P[1 * kCap] = t[1]; P[2 * kCap] = t[2]; P[3 * kCap] = m;
+      P[4 * kCap] = mv[0]; P[5 * kCap] = mv[1]; P[6 * kCap] = mv[2];
+#pragma unroll
+      for (int e = 0; e < 9; ++e) P[(7 + e) * kCap] = mC[e];
+#pragma unroll
+      for (int e = 0; e < 6; ++e) P[(16 + e) * kCap] = s6[e];
+    } else {
+      meta[j] = kMetaInvalid;
+      if (!in_w) flags |= 0x10u;
+      scatter_global(c, sc, tc, nxt, nb, t, m, mv, mC, s6, pinned);
+    }
+  }
+  float wave, grad;
+  cfl_terms(mt, D, v, C, m, V, co.Jm1, wave, grad);
+  flags |= state_flags(v, D, co.tau, co.Jm1);
+  flags_acc |= flags;
+  wave_acc = fmaxf(wave_acc, wave);
+  grad_acc = fmaxf(grad_acc, grad);
+  return key;
 }
 
 template <int PASS>
@@ -853,139 +1019,8 @@ __global__ void __launch_bounds__(kBlock, 2) k_particles(const __grid_constant__
         unsigned key = 0xffffffffu;
         if (j < nround) {
           const unsigned home = (r0 == 0 && pf_ok) ? (jj == 0 ? pf[0] : pf[1]) : c.p.perm[it.y + r0 + j];
-          unsigned q[3] = {c.p.qx[home], c.p.qy[home], c.p.qz[home]};
-          float D[9];
-#pragma unroll
-          for (int e = 0; e < 9; ++e) D[e] = c.p.Dc[e][home];
-          const float m = c.p.m[home], V = c.p.V[home];
-          const MaterialDev mt = single ? sm.mt : c.mats[c.p.mat[home]];
-          const bool pinned = c.has_pinned && c.p.pinned[home];
-          float ep = c.has_plastic ? c.p.ep[home] : 0.f;
-          float T = c.has_thermal ? c.p.T[home] : 0.f;
-          float v[3], C[9];
-          ConstitutiveOut co;
-          unsigned flags = 0;
-          if (GATHER && !pinned) {
-            int b[3];
-            float t[3], w[3][3];
-#pragma unroll
-            for (int a = 0; a < 3; ++a) {
-              stencil_axis(q[a], tc.dims[a], b[a], t[a]);
-              bspline_weights(t[a], w[a]);
-            }
-            const int l0 = b[0] - tc.tile[0] * kTile, l1 = b[1] - tc.tile[1] * kTile, l2 = b[2] - tc.tile[2] * kTile;
-            // the sort key places the stencil inside the staged window; if it ever does not, the
-            // particle reads the grid from global memory instead (and the step reports it)
-            const bool in_g = l0 >= 0 && l0 <= kWinG - 3 && l1 >= 0 && l1 <= kWinG - 3 && l2 >= 0 && l2 <= kWinG - 3;
-            if (!in_g) flags |= 0x20u;
-            // G2P (src/three/mpm.js:107-118): v = sum w v_i, C = sum w v_i (i - t)^T 4/h
-            float acc12[12];
-            if (in_g) {
-              const float4* win = &sm.vwin[cb][(l2 * kWinG + l1) * kWinG + l0];
-              gather27([&](int kz, int ky, int kx) { return win[(kz * kWinG + ky) * kWinG + kx]; }, t, w, acc12);
-            } else {
-              gather_global(c.g.vel + tc.node_base + ((long long)b[2] * tc.gdim[1] + b[1]) * tc.gdim[0] + b[0], tc.gdim[0],
-                            (long long)tc.gdim[0] * tc.gdim[1], t, w, acc12);
-            }
-            const float v0 = acc12[0], v1 = acc12[1], v2 = acc12[2];
-            const float c0 = acc12[3], c1 = acc12[4], c2 = acc12[5], c3 = acc12[6], c4 = acc12[7], c5 = acc12[8],
-                        c6 = acc12[9], c7 = acc12[10], c8 = acc12[11];
-            const float s4 = 4.f * tc.invH;
-            v[0] = v0; v[1] = v1; v[2] = v2;
-            C[0] = c0 * s4; C[1] = c1 * s4; C[2] = c2 * s4;
-            C[3] = c3 * s4; C[4] = c4 * s4; C[5] = c5 * s4;
-            C[6] = c6 * s4; C[7] = c7 * s4; C[8] = c8 * s4;
-            // F <- (I + dt C) F in centred form: D <- D + dt C (I + D) (src/three/mpm.js:119-121)
-            float Dn[9];
-#pragma unroll
-            for (int a = 0; a < 3; ++a)
-#pragma unroll
-              for (int bc = 0; bc < 3; ++bc)
-                Dn[a * 3 + bc] = D[a * 3 + bc] + dt * (C[a * 3 + bc] + C[a * 3 + 0] * D[0 * 3 + bc] +
-                                                       C[a * 3 + 1] * D[1 * 3 + bc] + C[a * 3 + 2] * D[2 * 3 + bc]);
-#pragma unroll
-            for (int e = 0; e < 9; ++e) D[e] = Dn[e];
-            // x += dt v (src/three/mpm.js:122) in fixed point, clamped into the box
-            const float s = dt * tc.invH * kFixedOne;
-#pragma unroll
-            for (int a = 0; a < 3; ++a) {
-              // |dq| stays below 2^30 (a particle moves far less than 256 cells in a substep)
-              long long qn = static_cast<long long>(q[a]) + __float2int_rn(fminf(fmaxf(s * v[a], -1.0e9f), 1.0e9f));
-              if (tc.clamp) {
-                qn = qn < (long long)tc.qlo[a] ? (long long)tc.qlo[a] : qn;
-                qn = qn > (long long)tc.qhi[a] ? (long long)tc.qhi[a] : qn;
-              } else {
-                const long long hi = (static_cast<long long>(tc.dims[a]) - 1) << kFracBits;
-                if (qn < 0 || qn > hi) flags |= 0x4u;
-                qn = qn < 0 ? 0 : (qn > hi ? hi : qn);
-              }
-              q[a] = static_cast<unsigned>(qn);
-            }
-            // return map / stress for the next P2G (src/three/mpm.js:126-131)
-            co = constitutive_update(mt, D, ep, T, V / m, true);
-            ep += co.dep;
-            T += co.dT;
-            c.p.qx[home] = q[0]; c.p.qy[home] = q[1]; c.p.qz[home] = q[2];
-            c.p.vx[home] = v[0]; c.p.vy[home] = v[1]; c.p.vz[home] = v[2];
-#pragma unroll
-            for (int e = 0; e < 9; ++e) {
-              c.p.Cc[e][home] = C[e];
-              c.p.Dc[e][home] = D[e];
-            }
-            if (c.has_plastic) c.p.ep[home] = ep;
-            if (c.has_thermal) c.p.T[home] = T;
-            if (co.dep > 0.f && mt.heat_per_work > 0.f) work_acc += static_cast<double>(co.dT) * m / mt.heat_per_work;
-          } else {
-            // P2G of the stored state, and pinned particles (not moved, src/three/mpm.js:108)
-            v[0] = c.p.vx[home]; v[1] = c.p.vy[home]; v[2] = c.p.vz[home];
-#pragma unroll
-            for (int e = 0; e < 9; ++e) C[e] = c.p.Cc[e][home];
-            float Dc[9];
-#pragma unroll
-            for (int e = 0; e < 9; ++e) Dc[e] = D[e];
-            co = constitutive_update(mt, Dc, ep, T, V / m, false);
-          }
-          if (SCATTER) {
-            // payload of the scatter: fraction t, m, m v, m C h, -4 V / h tau
-            int nb[3];
-            float t[3];
-#pragma unroll
-            for (int a = 0; a < 3; ++a) stencil_axis(q[a], tc.dims[a], nb[a], t[a]);
-            key = tile_key(sc, nb);
-            if (PASS == kPassG2P2G) c.p.key[home] = key;
-            const float mv[3] = {m * v[0], m * v[1], m * v[2]};
-            const float mH = m * tc.H;
-            float mC[9];
-#pragma unroll
-            for (int e = 0; e < 9; ++e) mC[e] = mH * C[e];
-            const float sv = -4.f * V * tc.invH;
-            const float s6[6] = {sv * co.tau.xx, sv * co.tau.yy, sv * co.tau.zz, sv * co.tau.xy, sv * co.tau.xz, sv * co.tau.yz};
-            const int l0 = nb[0] - (tc.tile[0] * kTile - 1), l1 = nb[1] - (tc.tile[1] * kTile - 1),
-                      l2 = nb[2] - (tc.tile[2] * kTile - 1);
-            const bool in_w = l0 >= 0 && l0 <= kWinS - 3 && l1 >= 0 && l1 <= kWinS - 3 && l2 >= 0 && l2 <= kWinS - 3;
-            if (in_w && !pinned) {
-              const int bucket = (l2 * 6 + l1) * 6 + l0;
-              const int rank = atomicAdd(&sm.hist[bucket], 1);
-              sm.meta[j] = static_cast<unsigned>(bucket) | (static_cast<unsigned>(rank) << 8);
-              float* P = sm.pay + j;
-              P[0 * kCap] = t[0]; P[1 * kCap] = t[1]; P[2 * kCap] = t[2]; P[3 * kCap] = m;
-              P[4 * kCap] = mv[0]; P[5 * kCap] = mv[1]; P[6 * kCap] = mv[2];
-#pragma unroll
-              for (int e = 0; e < 9; ++e) P[(7 + e) * kCap] = mC[e];
-#pragma unroll
-              for (int e = 0; e < 6; ++e) P[(16 + e) * kCap] = s6[e];
-            } else {
-              sm.meta[j] = kMetaInvalid;
-              if (!in_w) flags |= 0x10u;
-              scatter_global(c, sc, tc, nxt, nb, t, m, mv, mC, s6, pinned);
-            }
-          }
-          float wave, grad;
-          cfl_terms(mt, D, v, C, m, V, co.Jm1, wave, grad);
-          flags |= state_flags(v, D, co.tau, co.Jm1);
-          flags_acc |= flags;
-          wave_acc = fmaxf(wave_acc, wave);
-          grad_acc = fmaxf(grad_acc, grad);
+          key = particle_phase_a<PASS>(c, sc, tc, sm.mt, single, sm.vwin[cb], home, j, dt, nxt, sm.pay, sm.meta,
+                                       sm.hist, wave_acc, grad_acc, flags_acc, work_acc);
         }
         if (PASS == kPassG2P2G) count_key(c, key);
       }
@@ -1040,8 +1075,313 @@ __global__ void __launch_bounds__(kBlock, 2) k_particles(const __grid_constant__
   }
 }
 
+// ---------------------------------------------------------------------------------------------
+// Warp-specialised particle pass (P2G and G2P2G): one CTA of two 256-thread groups per SM.
+//   producer group (warps 0-7): claims tiles, waits for their TMA velocity window, runs phase A
+//     (one thread per particle) into one of two stage buffers (payload, bucket keys, histogram)
+//   consumer group (warps 8-15): scans the buckets of a finished stage, runs phase B (the register
+//     accumulation per bucket and z layer) into the shared scatter window and flushes the window
+//     to HBM after the last stage of a tile
+// so phase A of one tile overlaps phase B of the previous one, and neither group waits at a
+// CTA-wide barrier for the other's slowest thread. Stage hand-off uses mbarriers (full: producer
+// -> consumer, empty: consumer -> producer) with bounded waits; a wait that gives up sets the
+// timeout status and both groups leave through the same sentinel path.
+
+constexpr int kWsGroup = 256;
+constexpr int kWsThreads = 2 * kWsGroup;
+
+struct StageInfo {
+  TileCtx tc;
+  int nround;
+  int flush;     // last round of its tile: the consumer flushes the window after it
+  int scene;
+  int sentinel;  // no more stages
+};
+
+struct __align__(128) WsSmem {
+  float4 vwin[2][kWinG * kWinG * kWinG];  // producer: double-buffered TMA destinations
+  float pay[2][kPay * kCap];              // stage buffers
+  unsigned meta[2][kCap];
+  int hist[2][kBuckets];
+  StageInfo info[2];
+  float acc[kChannels * kWinSNodes];      // consumer: scatter window
+  unsigned short sidx[kCap];
+  int bstart[kBuckets + 1];
+  unsigned short blist[kBuckets];
+  int nbuckets;
+  StageInfo flush_info;                   // consumer copy of the stage it flushes
+  unsigned long long tma_bar[2], full[2], empty[2];
+  uint4 item[2];
+  int abort_flag;                         // producer gave up (its TMA wait timed out)
+  int consumer_exit;                      // consumer gave up waiting for a stage
+  unsigned red[3 * (kWsGroup / 32)];
+  double work[kWsGroup / 32];
+  TileCtx tc;
+  MaterialDev mt;
+};
+
+size_t ws_smem_bytes() { return sizeof(WsSmem); }
+
+__device__ __forceinline__ void group_sync(int id) {
+  asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(kWsGroup) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(unsigned long long* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+
+// Per-tile CFL maxima and status flags over the producer group, then one atomic per tile.
+__device__ __forceinline__ void group_reduce_item(const Ctx& c, int scene, float wave, float grad, unsigned flags,
+                                                  unsigned* red, int tid) {
+  const unsigned wb = __reduce_max_sync(0xffffffffu, fbits(wave));
+  const unsigned gb = __reduce_max_sync(0xffffffffu, fbits(grad));
+  const unsigned fl = __reduce_or_sync(0xffffffffu, flags);
+  const int lane = tid & 31, wid = tid >> 5;
+  if (lane == 0) {
+    red[wid * 3 + 0] = wb;
+    red[wid * 3 + 1] = gb;
+    red[wid * 3 + 2] = fl;
+  }
+  group_sync(1);
+  if (tid == 0) {
+    unsigned w = 0, g = 0, f = 0;
+    for (int k = 0; k < kWsGroup / 32; ++k) {
+      w = max(w, red[k * 3 + 0]);
+      g = max(g, red[k * 3 + 1]);
+      f |= red[k * 3 + 2];
+    }
+    atomicMax(&c.wave_max[scene], w);
+    atomicMax(&c.grad_max[scene], g);
+    if (f) atomicOr(&c.ctrl->status, f);
+  }
+}
+
+template <int PASS>
+__global__ void __launch_bounds__(kWsThreads, 1) k_particles_ws(const __grid_constant__ Ctx c) {
+  static_assert(PASS != kPassG2P, "the warp-specialised pass always scatters");
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  WsSmem& sm = *reinterpret_cast<WsSmem*>(smem_raw);
+  constexpr bool GATHER = PASS != kPassP2G;
+  Ctrl* ct = c.ctrl;
+  if (PASS != kPassP2G && ct->done) return;
+  const unsigned k = ct->step_index;
+  const int lst = PASS == kPassP2G ? (k & 1) : ((k - 1) & 1);
+  const int nxt = k & 1;
+  const bool use_tma = GATHER && c.use_tma;
+  for (int i = threadIdx.x; i < kChannels * kWinSNodes; i += kWsThreads) sm.acc[i] = 0.f;
+  auto issue_window = [&](int buf, const uint4& it) {
+    const SceneDev& sn = c.scenes[it.w];
+    const int lt = static_cast<int>(it.x) - sn.tile_base;
+    fence_proxy_async_smem();
+    mbar_arrive_expect_tx(&sm.tma_bar[buf], sizeof(sm.vwin[0]));
+    tma_load_4d(sm.vwin[buf], static_cast<const char*>(c.tmaps) + 128 * it.w, 0, (lt % sn.tiles[0]) * kTile,
+                ((lt / sn.tiles[0]) % sn.tiles[1]) * kTile, (lt / (sn.tiles[0] * sn.tiles[1])) * kTile,
+                &sm.tma_bar[buf]);
+  };
+  if (threadIdx.x == 0) {
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&sm.tma_bar[b], 1);
+      mbar_init(&sm.full[b], 1);
+      mbar_init(&sm.empty[b], 1);
+    }
+    fence_barrier_init();
+    sm.abort_flag = 0;
+    sm.consumer_exit = 0;
+    const unsigned idx = atomicAdd(&ct->work_next, 1u);
+    sm.item[0] = idx < ct->work_count[lst] ? c.s.work[lst][idx] : make_uint4(0xffffffffu, 0, 0, 0);
+    if (use_tma && sm.item[0].x != 0xffffffffu) issue_window(0, sm.item[0]);
+  }
+  __syncthreads();
+  double work_acc = 0.0;
+  if (threadIdx.x < kWsGroup) {
+    // ================= producer =================
+    const int tid = threadIdx.x;
+    int s = 0, cb = 0;
+    unsigned uses[2] = {0u, 0u}, pe[2] = {0u, 0u}, tph[2] = {0u, 0u};
+    bool in_flight[2] = {tid == 0 && use_tma && sm.item[0].x != 0xffffffffu, false};  // thread 0's TMA copies
+    const bool single = c.single_material != 0;
+    bool stop = false;
+    while (!stop) {
+      group_sync(1);
+      const uint4 it = sm.item[cb];
+      if (it.x == 0xffffffffu) break;
+      const int scene = static_cast<int>(it.w);
+      const SceneDev& sc = c.scenes[scene];
+      if (tid == 0) {
+        if (use_tma) {
+          if (!mbar_wait_bounded(&sm.tma_bar[cb], tph[cb])) {
+            atomicOr(&ct->status, 0x8u);
+            mbar_wait_bounded(&sm.tma_bar[cb], tph[cb]);  // a second bounded chance for the copy in flight
+            sm.abort_flag = 1;
+          }
+          tph[cb] ^= 1u;
+          in_flight[cb] = false;
+        }
+        // claim the next tile now: its window streams in while this tile is processed (the other
+        // window buffer was last read by this group's previous tile)
+        const unsigned idx = atomicAdd(&ct->work_next, 1u);
+        const uint4 nx = idx < ct->work_count[lst] ? c.s.work[lst][idx] : make_uint4(0xffffffffu, 0, 0, 0);
+        sm.item[cb ^ 1] = nx;
+        if (use_tma && nx.x != 0xffffffffu && !sm.abort_flag) {
+          issue_window(cb ^ 1, nx);
+          in_flight[cb ^ 1] = true;
+        }
+        TileCtx tl;
+        const int lt = static_cast<int>(it.x) - sc.tile_base;
+        tl.tile[0] = lt % sc.tiles[0];
+        tl.tile[1] = (lt / sc.tiles[0]) % sc.tiles[1];
+        tl.tile[2] = lt / (sc.tiles[0] * sc.tiles[1]);
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+          tl.dims[a] = sc.dims[a];
+          tl.gdim[a] = sc.gdim[a];
+          tl.qlo[a] = sc.qlo[a];
+          tl.qhi[a] = sc.qhi[a];
+        }
+        tl.node_base = sc.node_base;
+        tl.H = sc.H;
+        tl.invH = sc.invH;
+        tl.clamp = sc.clamp;
+        sm.tc = tl;
+        if (single) sm.mt = c.mats[sc.mat_base];
+      }
+      group_sync(1);
+      if (sm.abort_flag) break;
+      if (GATHER && !use_tma) {
+        const TileCtx& tl = sm.tc;
+        for (int i = tid; i < kWinG * kWinG * kWinG; i += kWsGroup) {
+          const int x = tl.tile[0] * kTile + i % kWinG, y = tl.tile[1] * kTile + (i / kWinG) % kWinG,
+                    z = tl.tile[2] * kTile + i / (kWinG * kWinG);
+          sm.vwin[cb][i] = c.g.vel[tl.node_base + ((long long)z * tl.gdim[1] + y) * tl.gdim[0] + x];
+        }
+        group_sync(1);
+      }
+      const TileCtx& tc = sm.tc;
+      const float dt = GATHER ? c.dt_scene[scene] : 0.f;
+      float wave_acc = 0.f, grad_acc = 0.f;
+      unsigned flags_acc = 0;
+      for (unsigned r0 = 0; r0 < it.z; r0 += kCap) {
+        const unsigned nround = min(static_cast<unsigned>(kCap), it.z - r0);
+        // take stage buffer s once the consumer has finished with it
+        if (tid == 0 && uses[s]) {
+          if (!mbar_wait_bounded(&sm.empty[s], pe[s])) {
+            atomicOr(&ct->status, 0x8u);
+            sm.abort_flag = 1;
+          }
+          pe[s] ^= 1u;
+        }
+        group_sync(1);
+        if (sm.abort_flag) {
+          stop = true;
+          break;
+        }
+        for (int i = tid; i < kBuckets; i += kWsGroup) sm.hist[s][i] = 0;
+        group_sync(1);
+        for (unsigned jj = 0; jj < nround; jj += kWsGroup) {
+          const unsigned j = jj + tid;
+          unsigned key = 0xffffffffu;
+          if (j < nround) {
+            const unsigned home = c.p.perm[it.y + r0 + j];
+            key = particle_phase_a<PASS>(c, sc, tc, sm.mt, single, sm.vwin[cb], home, j, dt, nxt, sm.pay[s],
+                                         sm.meta[s], sm.hist[s], wave_acc, grad_acc, flags_acc, work_acc);
+          }
+          if (PASS == kPassG2P2G) count_key(c, key);
+        }
+        if (tid == 0) {
+          StageInfo inf;
+          inf.tc = tc;
+          inf.nround = static_cast<int>(nround);
+          inf.flush = (r0 + kCap >= it.z) ? 1 : 0;
+          inf.scene = scene;
+          inf.sentinel = 0;
+          sm.info[s] = inf;
+        }
+        group_sync(1);
+        if (tid == 0) {
+          __threadfence_block();
+          mbar_arrive(&sm.full[s]);
+        }
+        ++uses[s];
+        s ^= 1;
+      }
+      if (stop) break;
+      group_reduce_item(c, scene, wave_acc, grad_acc, flags_acc, sm.red, tid);
+      cb ^= 1;
+    }
+    // sentinel stage: the consumer leaves after it. A group that stopped early first lets its own
+    // window copy in flight land (bounded), so no TMA writes into the CTA's memory after it exits.
+    if (tid == 0) {
+      for (int b = 0; b < 2; ++b)
+        if (in_flight[b] && !mbar_wait_bounded(&sm.tma_bar[b], tph[b])) atomicOr(&ct->status, 0x8u);
+      bool ok = true;
+      if (uses[s]) ok = mbar_wait_bounded(&sm.empty[s], pe[s]);
+      if (!ok) atomicOr(&ct->status, 0x8u);
+      sm.info[s].sentinel = 1;
+      __threadfence_block();
+      mbar_arrive(&sm.full[s]);
+    }
+  } else {
+    // ================= consumer =================
+    const int tb = threadIdx.x - kWsGroup;
+    int s = 0;
+    unsigned pf[2] = {0u, 0u};
+    while (true) {
+      if (tb == 0) {
+        if (!mbar_wait_bounded(&sm.full[s], pf[s])) {
+          atomicOr(&ct->status, 0x8u);
+          sm.consumer_exit = 1;
+        }
+        pf[s] ^= 1u;
+      }
+      group_sync(2);
+      if (sm.consumer_exit || sm.info[s].sentinel) break;
+      if (tb < 32) scan_buckets_p(sm.hist[s], sm.bstart, sm.blist, &sm.nbuckets, tb);
+      group_sync(2);
+      const int nround = sm.info[s].nround;
+      for (int j = tb; j < nround; j += kWsGroup) {
+        const unsigned mm = sm.meta[s][j];
+        if (!(mm & kMetaInvalid)) sm.sidx[sm.bstart[mm & 0xffu] + (mm >> 8)] = static_cast<unsigned short>(j);
+      }
+      group_sync(2);
+      const int nbk = sm.nbuckets;
+      for (int task = tb; task < 3 * nbk; task += kWsGroup) {
+        const int kz = task / nbk;
+        bucket_layer_p(sm.pay[s], sm.sidx, sm.bstart, sm.acc, sm.blist[task - kz * nbk], kz);
+      }
+      group_sync(2);
+      if (tb == 0) {
+        sm.flush_info = sm.info[s];  // the producer may reuse the stage once it is released
+        __threadfence_block();
+        mbar_arrive(&sm.empty[s]);
+      }
+      group_sync(2);
+      if (sm.flush_info.flush) {
+        flush_window_p(c, c.scenes[sm.flush_info.scene], sm.acc, nxt, sm.flush_info.tc.tile, tb, kWsGroup);
+        group_sync(2);
+      }
+      s ^= 1;
+    }
+  }
+  // heat from plastic work: one FP64 atomic per CTA (producer threads hold it)
+  __syncthreads();
+  if (GATHER) {
+    const double wsum = warp_sum_d(work_acc);
+    if ((threadIdx.x & 31) == 0 && threadIdx.x < kWsGroup) sm.work[threadIdx.x >> 5] = wsum;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double tsum = 0.0;
+      for (int w = 0; w < kWsGroup / 32; ++w) tsum += sm.work[w];
+      if (tsum != 0.0) atomicAdd(&ct->plastic_work, tsum);
+    }
+  }
+}
+
 template <int PASS>
 static void launch_pass(const Ctx& c, cudaStream_t st, int grid_blocks) {
+  if (PASS != kPassG2P && c.ws_blocks > 0) {
+    k_particles_ws<PASS == kPassG2P ? kPassG2P2G : PASS><<<c.ws_blocks, kWsThreads, sizeof(WsSmem), st>>>(c);
+    return;
+  }
   k_particles<PASS><<<grid_blocks, kBlock, sizeof(PartSmem), st>>>(c);
 }
 
@@ -1060,6 +1400,19 @@ static int blocks_per_sm() {
   int n = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_particles<PASS>, kBlock, sizeof(PartSmem));
   return n > 0 ? n : 1;
+}
+
+// Resident CTAs per SM of the warp-specialised pass (0: it cannot launch here).
+int ws_blocks_per_sm() {
+  int n0 = 0, n1 = 0;
+  if (cudaFuncSetAttribute(k_particles_ws<kPassP2G>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(WsSmem)) !=
+          cudaSuccess ||
+      cudaFuncSetAttribute(k_particles_ws<kPassG2P2G>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)sizeof(WsSmem)) != cudaSuccess)
+    return 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n0, k_particles_ws<kPassP2G>, kWsThreads, sizeof(WsSmem));
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n1, k_particles_ws<kPassG2P2G>, kWsThreads, sizeof(WsSmem));
+  return n0 < n1 ? n0 : n1;
 }
 
 int g2p2g_blocks_per_sm(bool scatter) { return scatter ? blocks_per_sm<kPassG2P2G>() : blocks_per_sm<kPassG2P>(); }

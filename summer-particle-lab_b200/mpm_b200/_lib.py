@@ -55,7 +55,8 @@ class MpmSceneDesc(ctypes.Structure):
 
 
 class MpmTuning(ctypes.Structure):
-    _fields_ = [("blocks_per_sm", _I32), ("reorder_interval", _I32), ("use_tma", _I32), ("trials", _I32),
+    _fields_ = [("warp_specialised", _I32), ("reserved", _I32), ("blocks_per_sm", _I32),
+                ("reorder_interval", _I32), ("use_tma", _I32), ("trials", _I32),
                 ("ms_per_substep", _D), ("ms_per_substep_default", _D)]
 
 

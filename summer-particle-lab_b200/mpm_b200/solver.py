@@ -211,7 +211,7 @@ class Solver:
     def autotune(self, trial_substeps=8):
         t = MpmTuning()
         self._check(_lib.lib().mpm_batch_autotune(self.h, int(trial_substeps), ctypes.byref(t)))
-        return dict(blocks_per_sm=t.blocks_per_sm, reorder_interval=t.reorder_interval, use_tma=t.use_tma,
+        return dict(warp_specialised=t.warp_specialised, blocks_per_sm=t.blocks_per_sm, reorder_interval=t.reorder_interval, use_tma=t.use_tma,
                     trials=t.trials, ms_per_substep=t.ms_per_substep, ms_per_substep_default=t.ms_per_substep_default)
 
 

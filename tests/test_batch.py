@@ -41,7 +41,7 @@ def rel(a, b):
 
 def test_batch_structs_match_header():
     assert ctypes.sizeof(_lib.MpmSceneDesc) == ctypes.sizeof(_lib.MpmDomain) + 16
-    assert ctypes.sizeof(_lib.MpmTuning) == 4 * 4 + 2 * 8
+    assert ctypes.sizeof(_lib.MpmTuning) == 6 * 4 + 2 * 8
 
 
 def test_batch_create_rejects_bad_tables_without_a_device():

@@ -227,6 +227,29 @@ def test_tma_and_plain_gather_agree(monkeypatch):
     assert rel(oa["C"], ob["C"], c_scale(ob["v"], sc.domain.H)) <= 1e-6
 
 
+def test_warp_specialised_pass_matches_oracle(monkeypatch):
+    """The producer/consumer scatter pass (an autotuner candidate): the plastic impact case."""
+    monkeypatch.setenv("MPM_B200_WS", "1")
+    sc = small_j2_scene()
+    dt = 1e-6
+    sol = Solver(sc.domain, sc.n)
+    sol.upload(sc)
+    st = orc.state_from_scene(sc)
+    gm_ref, gp_ref, _ = st.step(dt, want_grid=True)
+    gm, gp = sol.grid_debug(dt)
+    assert rel(gm, gm_ref) <= 1e-6
+    assert rel(gp, gp_ref) <= 1e-6
+    sol.step_fixed(dt, 1)
+    for _ in range(9):
+        st.step(dt)
+    sol.step_fixed(dt, 9)
+    out = sol.download()
+    assert np.max(np.abs(out["x"] - st.x)) <= 1e-6
+    assert np.max(np.abs(out["F"] - st.F)) <= 2e-6
+    assert np.max(np.abs(out["ep"] - st.ep)) <= 2e-6 + 1e-4 * np.max(st.ep)
+    assert sol.status() == 0
+
+
 def test_step_host_drop_in_matches_resident_step():
     sc = small_j2_scene()
     a = Solver(sc.domain, sc.n)
