@@ -24,7 +24,7 @@
 extern "C" {
 #endif
 
-#define MPM_ABI_VERSION 1
+#define MPM_ABI_VERSION 2
 
 /* status codes */
 #define MPM_OK 0
@@ -53,7 +53,10 @@ extern "C" {
 #define MPM_MODEL_NEO_HOOKEAN 1
 #define MPM_MODEL_J2 4
 #define MPM_MODEL_J2_HARDENING 5
+#define MPM_MODEL_JOHNSON_COOK 6        /* rate- and temperature-dependent, bisection return */
+#define MPM_MODEL_JOHNSON_COOK_SIMPLE 7 /* Johnson-Cook without thermal softening */
 #define MPM_MODEL_THERMAL_J2 10
+#define MPM_MODEL_NORTON_CREEP 11       /* Arrhenius power-law creep, bisection return */
 
 /* element type of the floating-point arrays of mpm_particles */
 #define MPM_F64 0
@@ -98,6 +101,13 @@ typedef struct mpm_material {
   double hot_ratio;
   double heat_fraction;  /* beta: share of plastic work converted to heat (gpu/mixed_material.py:150-172) */
   double specific_heat;  /* cp, J/kg/K */
+  /* Johnson-Cook, models 6 and 7 (src/three/metal-plasticity.js:3,12-19): flow stress
+   * (A + B ep^n)(1 + C ln max(1, rate / rate0))(1 - theta^m), theta from T_ref to T_melt (model 6) */
+  double jc_n, jc_C, jc_rate0, T_melt, jc_m;
+  /* Norton creep, model 11 (src/three/thermal-plasticity.js:3,17-21): strain rate
+   * rate exp(clamp(Q/R (1/(T_ref + off) - 1/(T + off)), -60, 60)) (q / stress)^n */
+  double creep_rate, creep_Q, creep_n, creep_stress;
+  double temperature_offset; /* off: 273.15 when temperatures are in deg C like the reference, 0 in K */
 } mpm_material;
 
 /* Host particle arrays (structure of arrays, like Simulation3's Float64Arrays,

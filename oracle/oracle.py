@@ -256,10 +256,18 @@ def material_from(mat):
         return material(mat.model, mu=mat.mu, lam=mat.lam,
                         plasticity=dict(A=mat.yield_stress, B=mat.hardening),
                         beta=mat.heat_fraction, cp=mat.specific_heat)
-    if mat.model == 10:
-        return material(10, mu=mat.mu, lam=mat.lam,
+    if mat.model in (6, 7):
+        return material(mat.model, mu=mat.mu, lam=mat.lam,
+                        plasticity=dict(A=mat.yield_stress, B=mat.hardening, n=mat.jc_n, C=mat.jc_C,
+                                        rate0=mat.jc_rate0, Tref=mat.T_ref, Tm=mat.T_melt, m=mat.jc_m),
+                        beta=mat.heat_fraction, cp=mat.specific_heat)
+    if mat.model in (10, 11):
+        if mat.model == 11 and mat.temperature_offset != 273.15:
+            raise ValueError("the restated creep law takes temperatures in deg C (offset 273.15)")
+        return material(mat.model, mu=mat.mu, lam=mat.lam,
                         thermal=dict(Tref=mat.T_ref, Thot=mat.T_hot, hotRatio=mat.hot_ratio,
-                                     A=mat.yield_stress, H=mat.hardening),
+                                     A=mat.yield_stress, H=mat.hardening, rate=mat.creep_rate, Q=mat.creep_Q,
+                                     n=mat.creep_n, stress=mat.creep_stress),
                         beta=mat.heat_fraction, cp=mat.specific_heat)
     return material(mat.model, mu=mat.mu, lam=mat.lam)
 

@@ -434,13 +434,25 @@ static MaterialDev to_device(const mpm_material& m) {
   d.hot_ratio = static_cast<float>(m.hot_ratio);
   d.heat_per_work = m.specific_heat > 0 ? static_cast<float>(m.heat_fraction / m.specific_heat) : 0.f;
   d.wave_modulus = static_cast<float>(m.lambda + 2 * m.mu);
+  d.jc_n = static_cast<float>(m.jc_n);
+  d.jc_C = static_cast<float>(m.jc_C);
+  d.jc_inv_rate0 = m.jc_rate0 > 0 ? static_cast<float>(1.0 / m.jc_rate0) : 0.f;
+  d.jc_inv_T_span = m.T_melt > m.T_ref ? static_cast<float>(1.0 / (m.T_melt - m.T_ref)) : 0.f;
+  d.jc_m = static_cast<float>(m.jc_m);
+  d.cr_on = m.creep_rate > 0 ? 1 : 0;
+  d.cr_log_rate = m.creep_rate > 0 ? static_cast<float>(std::log(m.creep_rate)) : 0.f;
+  d.cr_Q_over_R = static_cast<float>(m.creep_Q / 8.314462618);
+  d.cr_T_offset = static_cast<float>(m.temperature_offset);
+  d.cr_inv_Tref_abs = static_cast<float>(1.0 / (m.T_ref + m.temperature_offset));
+  d.cr_n = static_cast<float>(m.creep_n);
+  d.cr_inv_stress = m.creep_stress > 0 ? static_cast<float>(1.0 / m.creep_stress) : 0.f;
   return d;
 }
 
 static int validate_material(const mpm_material* m, std::string& why) {
   if (!m) { why = "material is null"; return MPM_ERR_INVALID_ARG; }
-  if (m->model != 0 && m->model != 1 && m->model != 4 && m->model != 5 && m->model != 10) {
-    why = "material model not built (supported: 0, 1, 4, 5, 10)";
+  if (m->model != 0 && m->model != 1 && (m->model < 4 || m->model > 7) && m->model != 10 && m->model != 11) {
+    why = "material model not built (supported: 0, 1, 4, 5, 6, 7, 10, 11)";
     return MPM_ERR_UNSUPPORTED;
   }
   if (!(m->mu > 0) || !(3 * m->lambda + 2 * m->mu > 0) || !std::isfinite(m->mu) || !std::isfinite(m->lambda)) {
@@ -453,6 +465,18 @@ static int validate_material(const mpm_material* m, std::string& why) {
   }
   if (m->model == 10 && !(m->T_hot > m->T_ref)) {
     why = "T_hot must exceed T_ref";
+    return MPM_ERR_INVALID_ARG;
+  }
+  if ((m->model == 6 || m->model == 7) && (!(m->jc_rate0 > 0) || !(m->jc_n >= 0) || !(m->jc_C >= 0))) {
+    why = "Johnson-Cook needs rate0 > 0, n >= 0 and C >= 0";
+    return MPM_ERR_INVALID_ARG;
+  }
+  if (m->model == 6 && (!(m->T_melt > m->T_ref) || !(m->jc_m >= 0))) {
+    why = "Johnson-Cook model 6 needs T_melt > T_ref and m >= 0";
+    return MPM_ERR_INVALID_ARG;
+  }
+  if (m->model == 11 && (!(m->creep_rate >= 0) || !(m->creep_stress > 0) || !(m->T_ref + m->temperature_offset > 0))) {
+    why = "Norton creep needs rate >= 0, stress > 0 and an absolute reference temperature > 0";
     return MPM_ERR_INVALID_ARG;
   }
   if (m->heat_fraction < 0 || m->heat_fraction > 1) {

@@ -833,7 +833,7 @@ __device__ __forceinline__ unsigned particle_phase_a(const Ctx& c, const SceneDe
       q[a] = static_cast<unsigned>(qn);
     }
     // return map / stress for the next P2G (src/three/mpm.js:126-131)
-    co = constitutive_update(mt, D, ep, T, V / m, true);
+    co = constitutive_update(mt, D, ep, T, V / m, true, dt);
     ep += co.dep;
     T += co.dT;
     c.p.qx[home] = q[0]; c.p.qy[home] = q[1]; c.p.qz[home] = q[2];
@@ -1830,12 +1830,12 @@ void launch_download_convert(const Ctx& c, cudaStream_t st, long long n, int dty
 // stateless constitutive batch: projectPlastic + stress (src/three/constitutive.js:52-86)
 
 __global__ void k_return_map(MaterialDev mt, long long n, const double* F_in, const double* ep, const double* T,
-                             double* F_out, double* dep, double* tau) {
+                             float dt, double* F_out, double* dep, double* tau) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
     float D[9];
     for (int e = 0; e < 9; ++e) D[e] = (float)(F_in[i * 9 + e] - ((e % 4 == 0) ? 1.0 : 0.0));
     const float epi = ep ? (float)ep[i] : 0.f, Ti = T ? (float)T[i] : 0.f;
-    const ConstitutiveOut co = constitutive_update(mt, D, epi, Ti, 1.f, true);
+    const ConstitutiveOut co = constitutive_update(mt, D, epi, Ti, 1.f, true, dt);
     for (int e = 0; e < 9; ++e) F_out[i * 9 + e] = (double)D[e] + ((e % 4 == 0) ? 1.0 : 0.0);
     dep[i] = co.dep;
     const float t9[9] = {co.tau.xx, co.tau.xy, co.tau.xz, co.tau.xy, co.tau.yy, co.tau.yz, co.tau.xz, co.tau.yz, co.tau.zz};
@@ -1845,9 +1845,8 @@ __global__ void k_return_map(MaterialDev mt, long long n, const double* F_in, co
 
 void launch_return_map_batch(const MaterialDev& m, long long n, const double* F_in, const double* ep, const double* T,
                              float dt, double* F_out, double* dep, double* tau, cudaStream_t st) {
-  (void)dt;
   const int blocks = static_cast<int>((n + 255) / 256 < 4096 ? (n + 255) / 256 : 4096);
-  if (blocks > 0) k_return_map<<<blocks, 256, 0, st>>>(m, n, F_in, ep, T, F_out, dep, tau);
+  if (blocks > 0) k_return_map<<<blocks, 256, 0, st>>>(m, n, F_in, ep, T, dt, F_out, dep, tau);
 }
 
 }  // namespace mpm

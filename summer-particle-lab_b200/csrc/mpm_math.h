@@ -196,7 +196,71 @@ struct MaterialDev {
   float T_ref, inv_T_span, hot_ratio;
   float heat_per_work;   // heat_fraction / specific_heat (K per J/kg)
   float wave_modulus;    // lambda + 2 mu (CFL wave speed c = sqrt(wave_modulus V / m))
+  // Johnson-Cook, models 6 and 7 (src/three/metal-plasticity.js:12-19): yield_stress = A,
+  // hardening = B, flow = (A + B ep^n)(1 + C ln max(1, rate / rate0))(1 - theta^m), the last
+  // factor for model 6 only, theta = clamp((T - T_ref) / (T_melt - T_ref), 0, 1)
+  float jc_n, jc_C, jc_inv_rate0, jc_inv_T_span, jc_m;
+  // Norton creep, model 11 (src/three/thermal-plasticity.js:17-21): log rate = log A0 +
+  // clamp(Q/R (1/(T_ref + off) - 1/max(1, T + off)), -60, 60) + n log(q / stress)
+  float cr_log_rate, cr_Q_over_R, cr_inv_Tref_abs, cr_T_offset, cr_n, cr_inv_stress;
+  int cr_on;             // creep rate > 0
 };
+
+// Johnson-Cook flow stress (src/three/metal-plasticity.js:12-19).
+MPM_HD float jc_flow(const MaterialDev& mt, float ep, float rate, float T) {
+  const float rf = 1.f + mt.jc_C * logf(fmaxf(1.f, rate * mt.jc_inv_rate0));
+  float f = (mt.yield_stress + mt.hardening * powf(fmaxf(ep, 0.f), mt.jc_n)) * rf;
+  if (mt.model == 6) {
+    const float th = fminf(1.f, fmaxf(0.f, (T - mt.T_ref) * mt.jc_inv_T_span));
+    f *= 1.f - powf(th, mt.jc_m);
+  }
+  return f;
+}
+
+// Norton creep log strain rate at von Mises stress q (src/three/thermal-plasticity.js:17-21).
+MPM_HD float creep_log_rate(const MaterialDev& mt, float q, float T) {
+  if (!mt.cr_on || !(q > 0.f)) return -INFINITY;
+  const float act = fminf(60.f, fmaxf(-60.f, mt.cr_Q_over_R * (mt.cr_inv_Tref_abs - 1.f / fmaxf(1.f, T + mt.cr_T_offset))));
+  return mt.cr_log_rate + act + mt.cr_n * logf(q * mt.cr_inv_stress);
+}
+
+// Plastic strain increment of the J2-type returns for the trial von Mises stress q
+// (src/three/metal-plasticity.js:20-27, src/three/thermal-plasticity.js:22-37): closed form for
+// models 4, 5 and 10, 24 bisections of the consistency condition for Johnson-Cook (6, 7), 32
+// bisections of the creep rate for Norton creep (11), with the reference's brackets.
+MPM_HD float plastic_increment(const MaterialDev& mt, float q, float J, float ep, float T, float dt) {
+  const float slope = 3.f * mt.mu / J;
+  if (mt.model == 6 || mt.model == 7) {
+    if (!(q > jc_flow(mt, ep, 0.f, T))) return 0.f;
+    float lo = 0.f, hi = q / slope;
+    const float inv_dt = 1.f / fmaxf(dt, 1e-12f);
+    for (int it = 0; it < 24; ++it) {
+      const float mid = 0.5f * (lo + hi);
+      if (q - slope * mid > jc_flow(mt, ep + mid, mid * inv_dt, T)) lo = mid;
+      else hi = mid;
+    }
+    return 0.5f * (lo + hi);
+  }
+  if (mt.model == 11) {
+    if (!(dt > 0.f && mt.cr_on && q > 1e-20f)) return 0.f;
+    float lo = 0.f, hi = q / slope;
+    for (int it = 0; it < 32; ++it) {
+      const float mid = 0.5f * (lo + hi);
+      if (logf(mid / dt) < creep_log_rate(mt, fmaxf(0.f, q - slope * mid), T)) lo = mid;
+      else hi = mid;
+    }
+    return 0.5f * (lo + hi);
+  }
+  float soft = 1.f;
+  if (mt.model == 10) {
+    const float theta = fminf(1.f, fmaxf(0.f, (T - mt.T_ref) * mt.inv_T_span));
+    soft = 1.f - (1.f - mt.hot_ratio) * theta;
+  }
+  const float yield = (mt.yield_stress + (mt.model == 4 ? 0.f : mt.hardening * ep)) * soft;
+  if (!(q > yield)) return 0.f;
+  const float hard = mt.model == 4 ? 0.f : mt.hardening * soft;
+  return (q - yield) / (slope + hard);
+}
 
 struct ConstitutiveOut {
   Sym3 tau;       // Kirchhoff stress for the next P2G
@@ -214,7 +278,7 @@ MPM_HD float hencky_strain(float beta) {
 // Large-strain path (|B| > 0.15): Jacobi eigen-decomposition of B. Out of line so its registers do
 // not count against the series path that almost every particle takes.
 MPM_NOINLINE ConstitutiveOut constitutive_eigen(const MaterialDev& mt, const Sym3& B, float D[9], float ep,
-                                                float T, float inv_rho0, bool do_return) {
+                                                float T, float inv_rho0, bool do_return, float dt) {
   ConstitutiveOut out;
   out.dep = 0.f;
   out.dT = 0.f;
@@ -245,17 +309,7 @@ MPM_NOINLINE ConstitutiveOut constitutive_eigen(const MaterialDev& mt, const Sym
   const float len = sqrtf(dev[0] * dev[0] + dev[1] * dev[1] + dev[2] * dev[2]);
   const float J = fmaxf(1e-6f, expf(tr));
   const float q = 2.449489742783178f * mt.mu * len / J;
-  float soft = 1.f;
-  if (mt.model == 10) {
-    const float theta = fminf(1.f, fmaxf(0.f, (T - mt.T_ref) * mt.inv_T_span));
-    soft = 1.f - (1.f - mt.hot_ratio) * theta;
-  }
-  const float yield = (mt.yield_stress + (mt.model == 4 ? 0.f : mt.hardening * ep)) * soft;
-  float dep = 0.f;
-  if (do_return && q > yield) {
-    const float hard = mt.model == 4 ? 0.f : mt.hardening * soft;
-    dep = (q - yield) / (3.f * mt.mu / J + hard);
-  }
+  const float dep = do_return ? plastic_increment(mt, q, J, ep, T, dt) : 0.f;
   float scale = 1.f;
   if (dep > 0.f) {
     scale = fmaxf(0.f, 1.f - 1.224744871391589f * dep / fmaxf(len, 1e-20f));
@@ -287,15 +341,16 @@ MPM_NOINLINE ConstitutiveOut constitutive_eigen(const MaterialDev& mt, const Sym
 }
 
 // Constitutive update of one particle after the F update, in place on D (= F - I):
-// models 4/5/10 run the J2 radial return (src/three/metal-plasticity.js:20-27,
-// src/three/thermal-plasticity.js:22-29) and give the Hencky stress of the returned state
+// models 4-7, 10 and 11 run the J2-type radial return (src/three/metal-plasticity.js:20-38,
+// src/three/thermal-plasticity.js:22-40; dt is the substep, used by the rate-dependent laws 6,
+// 7 and 11) and give the Hencky stress of the returned state
 // (src/three/constitutive.js:81-86); models 0 and 1 give the elastic stress of F
 // (src/three/math.js:25-32, src/three/constitutive.js:94-100).
 // ep is the accumulated plastic strain, T the temperature; rho0 = m / V for the heat term.
 // With do_return false the J2 models give the stress of F without a return (the reference's
 // updateStress when no cached stress exists, src/three/mpm.js:36).
 MPM_HD ConstitutiveOut constitutive_update(const MaterialDev& mt, float D[9], float ep, float T,
-                                           float inv_rho0, bool do_return) {
+                                           float inv_rho0, bool do_return, float dt = 0.f) {
   ConstitutiveOut out;
   out.dep = 0.f;
   out.dT = 0.f;
@@ -343,16 +398,9 @@ MPM_HD ConstitutiveOut constitutive_update(const MaterialDev& mt, float D[9], fl
     const float len = sym_norm(dv);
     const float J = fmaxf(1e-6f, expf(trL));
     const float q = 2.449489742783178f * mt.mu * len / J;
-    float soft = 1.f;
-    if (mt.model == 10) {
-      const float theta = fminf(1.f, fmaxf(0.f, (T - mt.T_ref) * mt.inv_T_span));
-      soft = 1.f - (1.f - mt.hot_ratio) * theta;
-    }
-    const float yield = (mt.yield_stress + (mt.model == 4 ? 0.f : mt.hardening * ep)) * soft;
-    float dep = 0.f, scale = 1.f;
-    if (do_return && q > yield) {
-      const float hard = mt.model == 4 ? 0.f : mt.hardening * soft;
-      dep = (q - yield) / (3.f * mt.mu / J + hard);
+    const float dep = do_return ? plastic_increment(mt, q, J, ep, T, dt) : 0.f;
+    float scale = 1.f;
+    if (dep > 0.f) {
       scale = fmaxf(0.f, 1.f - 1.224744871391589f * dep / fmaxf(len, 1e-20f));
       const float g = scale - 1.f;
       const Sym3 M{g * dv.xx, g * dv.yy, g * dv.zz, g * dv.xy, g * dv.xz, g * dv.yz};
@@ -382,7 +430,7 @@ MPM_HD ConstitutiveOut constitutive_update(const MaterialDev& mt, float D[9], fl
     out.Jm1 = expm1f(trL);
     return out;
   }
-  return constitutive_eigen(mt, B, D, ep, T, inv_rho0, do_return);
+  return constitutive_eigen(mt, B, D, ep, T, inv_rho0, do_return, dt);
 }
 
 }  // namespace mpm

@@ -34,7 +34,10 @@ class MpmDomain(ctypes.Structure):
 class MpmMaterial(ctypes.Structure):
     _fields_ = [("model", _I32), ("reserved", _I32), ("mu", _D), ("lam", _D), ("yield_stress", _D),
                 ("hardening", _D), ("T_ref", _D), ("T_hot", _D), ("hot_ratio", _D),
-                ("heat_fraction", _D), ("specific_heat", _D)]
+                ("heat_fraction", _D), ("specific_heat", _D),
+                ("jc_n", _D), ("jc_C", _D), ("jc_rate0", _D), ("T_melt", _D), ("jc_m", _D),
+                ("creep_rate", _D), ("creep_Q", _D), ("creep_n", _D), ("creep_stress", _D),
+                ("temperature_offset", _D)]
 
 
 class MpmParticles(ctypes.Structure):

@@ -19,7 +19,10 @@ MODEL_NEO_HOOKEAN = 1
 MODEL_J2 = 4
 MODEL_J2_HARDENING = 5
 MODEL_THERMAL_J2 = 10
-SUPPORTED_MODELS = (0, 1, 4, 5, 10)
+MODEL_JOHNSON_COOK = 6
+MODEL_JOHNSON_COOK_SIMPLE = 7
+MODEL_NORTON_CREEP = 11
+SUPPORTED_MODELS = (0, 1, 4, 5, 6, 7, 10, 11)
 
 # Positions are held on the device as unsigned 32-bit fixed point in cell units relative to the
 # grid origin, with this many fractional bits (grids up to 1023 cells per axis).
@@ -77,6 +80,18 @@ class Material:
     hot_ratio: float = 0.08        # strength fraction left at T_hot
     heat_fraction: float = 0.0     # beta: share of plastic work converted to heat
     specific_heat: float = 1.0     # cp (J/kg/K)
+    # Johnson-Cook (models 6, 7): (A + B ep^n)(1 + C ln max(1, rate/rate0))(1 - theta^m)
+    jc_n: float = 0.35
+    jc_C: float = 0.025
+    jc_rate0: float = 1.0
+    T_melt: float = 1000.0
+    jc_m: float = 1.0
+    # Norton creep (model 11): rate exp(Q/R (1/T_ref,abs - 1/T_abs)) (q / stress)^n
+    creep_rate: float = 0.0
+    creep_Q: float = 0.0
+    creep_n: float = 1.0
+    creep_stress: float = 1.0
+    temperature_offset: float = 0.0  # added to T for the Arrhenius term (273.15 for deg C)
 
     def __post_init__(self):
         if self.model not in SUPPORTED_MODELS:
@@ -98,11 +113,19 @@ class Material:
         kw = dict(model=model, mu=.4 * E, lam=.4 * E, density=density)
         if model in (4, 5):
             kw.update(yield_stress=A * E, hardening=(B * E if model == 5 else 0.0))
-        if model == 10:
-            t = dict(Tref=20, Thot=180, hotRatio=.08, A=.04, H=.04)
+        if model in (6, 7):
+            # src/three/metal-plasticity.js:3 defaults, temperatures in deg C
+            kw.update(yield_stress=A * E, hardening=B * E, jc_n=.35, jc_C=.025, jc_rate0=1.0, T_ref=20.0,
+                      T_melt=1000.0, jc_m=1.0)
+        if model in (10, 11):
+            # src/three/thermal-plasticity.js:3 defaults, temperatures in deg C
+            t = dict(Tref=20, Thot=180, hotRatio=.08, A=.04, H=.04, rate=.0005, Q=35000, n=3, stress=.04)
             t.update(thermal or {})
             kw.update(yield_stress=t["A"] * E, hardening=t["H"] * E, T_ref=t["Tref"],
                       T_hot=t["Thot"], hot_ratio=t["hotRatio"])
+            if model == 11:
+                kw.update(creep_rate=t["rate"], creep_Q=t["Q"], creep_n=t["n"], creep_stress=t["stress"] * E,
+                          temperature_offset=273.15)
         return Material(**kw)
 
     @property

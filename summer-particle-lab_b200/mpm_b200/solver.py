@@ -34,7 +34,10 @@ def domain_struct(d):
 def material_struct(m):
     return MpmMaterial(model=m.model, mu=m.mu, lam=m.lam, yield_stress=m.yield_stress,
                        hardening=m.hardening, T_ref=m.T_ref, T_hot=m.T_hot, hot_ratio=m.hot_ratio,
-                       heat_fraction=m.heat_fraction, specific_heat=m.specific_heat)
+                       heat_fraction=m.heat_fraction, specific_heat=m.specific_heat, jc_n=m.jc_n, jc_C=m.jc_C,
+                       jc_rate0=m.jc_rate0, T_melt=m.T_melt, jc_m=m.jc_m, creep_rate=m.creep_rate,
+                       creep_Q=m.creep_Q, creep_n=m.creep_n, creep_stress=m.creep_stress,
+                       temperature_offset=m.temperature_offset)
 
 
 def _ptr(a):

@@ -25,6 +25,43 @@ extern "C" void harness_constitutive(int model, double mu, double lam, double A,
   }
 }
 
+// Every material field (in the order of mpm_material from mu on) and the substep dt, for the
+// rate-dependent laws: prm = {mu, lam, A, B, Tref, Thot, hot, jc_n, jc_C, jc_rate0, T_melt, jc_m,
+// creep_rate, creep_Q, creep_n, creep_stress, T_offset}.
+extern "C" void harness_constitutive_full(int model, const double* prm, double dt, int n, const double* F,
+                                          const double* ep, const double* T, double* Fout, double* dep, double* tau) {
+  mpm::MaterialDev m{};
+  m.model = model;
+  m.mu = (float)prm[0];
+  m.lam = (float)prm[1];
+  m.yield_stress = (float)prm[2];
+  m.hardening = (float)prm[3];
+  m.T_ref = (float)prm[4];
+  m.inv_T_span = prm[5] > prm[4] ? (float)(1.0 / (prm[5] - prm[4])) : 0.f;
+  m.hot_ratio = (float)prm[6];
+  m.jc_n = (float)prm[7];
+  m.jc_C = (float)prm[8];
+  m.jc_inv_rate0 = prm[9] > 0 ? (float)(1.0 / prm[9]) : 0.f;
+  m.jc_inv_T_span = prm[10] > prm[4] ? (float)(1.0 / (prm[10] - prm[4])) : 0.f;
+  m.jc_m = (float)prm[11];
+  m.cr_on = prm[12] > 0;
+  m.cr_log_rate = prm[12] > 0 ? (float)std::log(prm[12]) : 0.f;
+  m.cr_Q_over_R = (float)(prm[13] / 8.314462618);
+  m.cr_n = (float)prm[14];
+  m.cr_inv_stress = (float)(1.0 / prm[15]);
+  m.cr_T_offset = (float)prm[16];
+  m.cr_inv_Tref_abs = (float)(1.0 / (prm[4] + prm[16]));
+  for (int i = 0; i < n; ++i) {
+    float D[9];
+    for (int e = 0; e < 9; ++e) D[e] = (float)(F[i * 9 + e] - (e % 4 == 0 ? 1.0 : 0.0));
+    mpm::ConstitutiveOut o = mpm::constitutive_update(m, D, (float)ep[i], (float)T[i], 1.f, true, (float)dt);
+    for (int e = 0; e < 9; ++e) Fout[i * 9 + e] = (double)D[e] + (e % 4 == 0 ? 1.0 : 0.0);
+    dep[i] = o.dep;
+    const float t9[9] = {o.tau.xx, o.tau.xy, o.tau.xz, o.tau.xy, o.tau.yy, o.tau.yz, o.tau.xz, o.tau.yz, o.tau.zz};
+    for (int e = 0; e < 9; ++e) tau[i * 9 + e] = t9[e];
+  }
+}
+
 extern "C" void harness_eig(int n, const double* S6, double* lam, double* U) {
   for (int i = 0; i < n; ++i) {
     mpm::Sym3 a{(float)S6[i * 6 + 0], (float)S6[i * 6 + 1], (float)S6[i * 6 + 2],

@@ -155,3 +155,69 @@ def test_thermal_series_path_with_softening(harness):
         assert abs(dep[i] - inc) < 1e-5
         n_yield += inc > 0
     assert n_yield > 20
+
+
+# ---- rate-dependent laws: Johnson-Cook (6, 7) and Norton creep (11), bisection returns ----------
+
+def _full(L, mat, dt, F, ep, T):
+    L.harness_constitutive_full.argtypes = [ctypes.c_int, P, ctypes.c_double, ctypes.c_int, P, P, P, P, P, P]
+    prm = np.array([mat.mu, mat.lam, mat.yield_stress, mat.hardening, mat.T_ref, mat.T_hot, mat.hot_ratio, mat.jc_n,
+                    mat.jc_C, mat.jc_rate0, mat.T_melt, mat.jc_m, mat.creep_rate, mat.creep_Q, mat.creep_n,
+                    mat.creep_stress, mat.temperature_offset])
+    F = np.ascontiguousarray(np.asarray(F, dtype=np.float64).reshape(-1, 9))
+    n = F.shape[0]
+    ep = np.ascontiguousarray(np.broadcast_to(np.asarray(ep, dtype=np.float64), (n,)))
+    T = np.ascontiguousarray(np.broadcast_to(np.asarray(T, dtype=np.float64), (n,)))
+    Fo, dep, tau = np.empty((n, 9)), np.empty(n), np.empty((n, 9))
+    c = lambda a: a.ctypes.data_as(P)
+    L.harness_constitutive_full(mat.model, c(prm), dt, n, c(F), c(ep), c(T), c(Fo), c(dep), c(tau))
+    return Fo, dep, tau
+
+
+@pytest.mark.parametrize("model", [6, 7])
+def test_johnson_cook_matches_oracle(harness, model):
+    from mpm_b200.params import Material
+    # gpu/metal_reference.mjs:1-9: T in {20, 650, 1100}, dt in {.001, .02}, F preset, ep .15, A .03, B .12
+    mat = Material.reference_units(model, A=.03, B=.12)
+    omat = orc.material_from(mat)
+    F = [1.3, .1, 0, 0, .8, 0, 0, 0, 1 / 1.04]
+    for T in (20, 650, 1100):
+        for dt in (.001, .02):
+            Fo_ref, inc_ref, _ = orc.project(F, omat, ep=.15, dt=dt, T=T)
+            Fo, dep, _ = _full(harness, mat, dt, [F], .15, T)
+            np.testing.assert_allclose(Fo[0], Fo_ref, atol=4e-6, rtol=4e-5)
+            assert abs(dep[0] - inc_ref) < 1e-5, (T, dt, dep[0], inc_ref)
+    # random trial states: yielding and elastic, several temperatures and strain rates
+    rng = np.random.default_rng(11)
+    Fs = random_F(300, .05, 12)
+    eps = rng.uniform(0, .3, 300)
+    Ts = rng.uniform(0, 900, 300)
+    Fo, dep, tau = _full(harness, mat, .005, Fs, eps, Ts)
+    yielded = 0
+    for i in range(300):
+        Fo_ref, inc_ref, _ = orc.project(Fs[i], omat, ep=eps[i], dt=.005, T=Ts[i])
+        np.testing.assert_allclose(Fo[i], Fo_ref, atol=4e-6, rtol=4e-5)
+        assert abs(dep[i] - inc_ref) < 1e-5
+        np.testing.assert_allclose(tau[i], orc.constitutive_stress(Fo_ref, model, mat.mu, mat.lam), atol=3e-6, rtol=5e-4)
+        yielded += inc_ref > 0
+    assert yielded > 50
+
+
+def test_norton_creep_matches_oracle(harness):
+    from mpm_b200.params import Material
+    # gpu/thermal_reference.mjs:1-9 for model 11: T in {-100, 20, 180, 800}, two F, ep .05, dt .01
+    mat = Material.reference_units(11)
+    omat = orc.material_from(mat)
+    for T in (-100, 20, 180, 800):
+        for F in ([1, .2, 0, 0, 1, 0, 0, 0, 1], [.9, 0, 0, 0, 1.05, 0, 0, 0, 1]):
+            Fo_ref, inc_ref, _ = orc.project(F, omat, ep=.05, dt=.01, T=T)
+            Fo, dep, _ = _full(harness, mat, .01, [F], .05, T)
+            np.testing.assert_allclose(Fo[0], Fo_ref, atol=4e-6, rtol=5e-5)
+            assert abs(dep[0] - inc_ref) <= 1e-5 + 1e-4 * inc_ref, (T, F, dep[0], inc_ref)
+    # the n = 1 closed form of tests/thermal-plasticity.test.mjs:28-31 on the device math:
+    # dep = dt rate q/s / (1 + dt rate 1.2/s) at T = Tref (activation term zero)
+    lin = Material.reference_units(11, thermal=dict(n=1))
+    F = [1.02, 0, 0, 0, 1 / 1.02, 0, 0, 0, 1]
+    _, dep, _ = _full(harness, lin, .01, [F], 0.0, 20.0)
+    Fo_ref, inc_ref, _ = orc.project(F, orc.material_from(lin), ep=0.0, dt=.01, T=20.0)
+    assert abs(dep[0] - inc_ref) <= 1e-6 + 1e-4 * inc_ref
