@@ -218,6 +218,22 @@ int mpm_checkpoint_load(mpm_handle* h, const char* path);
 int mpm_host_alloc(size_t bytes, void** out);
 int mpm_host_free(void* p);
 
+/* ---- viewer frame (gpu/solver.py:985-1035, the Taichi service's `pack` + `snapshot`) ----
+ * One deterministic sample per block of `stride` = ceil(count / preview_limit) caller indices,
+ * chosen by the reference's integer hash so previews show no lattice stripes, written as 8 floats
+ * per row: x, y, z (m), material index, temperature, pinned, von Mises Kirchhoff stress / J,
+ * plastic strain. rows = ceil(count / stride); data holds max_rows x 8 floats. The frame
+ * reductions are FP64 on the device. Returns MPM_ERR_NONFINITE, like the reference's snapshot,
+ * when any particle's state is not finite. */
+typedef struct mpm_frame_info {
+  int64_t count, rows, stride;
+  double mass, thermal_energy;   /* sum m, sum m cp T */
+  double min_T, max_T, min_j, max_von_mises, max_plastic;
+  int64_t nonfinite;
+  int64_t per_material[256];     /* particles per material index */
+} mpm_frame_info;
+int mpm_pack_frame(mpm_handle* h, int64_t preview_limit, float* data, int64_t max_rows, mpm_frame_info* info);
+
 /* ---- constitutive batch on the device (projectPlastic + stress, src/three/constitutive.js:52-106)
  * F_in/F_out n x 9, ep/T/dep n, tau n x 9 (Kirchhoff). Stateless; runs on the default stream. */
 int mpm_return_map_batch(const mpm_material* material, int64_t n, const double* F_in,

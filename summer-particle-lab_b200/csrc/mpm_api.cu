@@ -433,6 +433,7 @@ static MaterialDev to_device(const mpm_material& m) {
   d.inv_T_span = m.T_hot > m.T_ref ? static_cast<float>(1.0 / (m.T_hot - m.T_ref)) : 0.f;
   d.hot_ratio = static_cast<float>(m.hot_ratio);
   d.heat_per_work = m.specific_heat > 0 ? static_cast<float>(m.heat_fraction / m.specific_heat) : 0.f;
+  d.cp = static_cast<float>(m.specific_heat);
   d.wave_modulus = static_cast<float>(m.lambda + 2 * m.mu);
   d.jc_n = static_cast<float>(m.jc_n);
   d.jc_C = static_cast<float>(m.jc_C);
@@ -1275,6 +1276,66 @@ int mpm_return_map_batch(const mpm_material* material, int64_t n, const double* 
   if (e == cudaSuccess) e = cudaMemcpy(tau, dtau, 9 * n * sizeof(double), cudaMemcpyDeviceToHost);
   cudaFree(d);
   return e == cudaSuccess ? MPM_OK : MPM_ERR_CUDA;
+}
+
+// ---- viewer frame ----
+
+int mpm_pack_frame(mpm_handle* h, int64_t preview_limit, float* data, int64_t max_rows, mpm_frame_info* info) {
+  if (!h || !info || preview_limit <= 0 || max_rows < 0 || (max_rows > 0 && !data)) return MPM_ERR_INVALID_ARG;
+  if (!h->uploaded) return fail(h, MPM_ERR_STATE, "no particles uploaded");
+  std::memset(info, 0, sizeof *info);
+  const int64_t n = h->n;
+  const int64_t stride = std::max<int64_t>(1, (n + preview_limit - 1) / preview_limit);
+  const int64_t rows = (n + stride - 1) / stride;
+  info->count = n;
+  info->stride = stride;
+  info->rows = rows;
+  if (rows > max_rows) return fail(h, MPM_ERR_CAPACITY, "data holds fewer rows than the frame needs");
+  mpm_ledger L;
+  int rc = mpm_ledger_compute(h, &L);
+  if (rc != MPM_OK) return rc;
+  info->mass = L.mass;
+  info->min_j = L.min_j;
+  info->max_von_mises = L.max_von_mises;
+  info->max_plastic = L.max_plastic;
+  info->nonfinite = L.nonfinite;
+  if (n == 0) return MPM_OK;
+  const size_t data_bytes = align_up(rows * 8 * sizeof(float), 256);
+  rc = ensure_staging(h, data_bytes + 256 + 256 * sizeof(unsigned));
+  if (rc != MPM_OK) return rc;
+  char* base = static_cast<char*>(h->staging);
+  float* d_data = reinterpret_cast<float*>(base);
+  double* d_energy = reinterpret_cast<double*>(base + data_bytes);
+  unsigned* d_tkey = reinterpret_cast<unsigned*>(base + data_bytes + 8);
+  unsigned* d_counts = reinterpret_cast<unsigned*>(base + data_bytes + 256);
+  const unsigned tinit[2] = {0xffffffffu, 0u};
+  MPM_CUDA(h, cudaMemsetAsync(d_energy, 0, 8, h->stream));
+  MPM_CUDA(h, cudaMemcpyAsync(d_tkey, tinit, sizeof tinit, cudaMemcpyHostToDevice, h->stream));
+  MPM_CUDA(h, cudaMemsetAsync(d_counts, 0, 256 * sizeof(unsigned), h->stream));
+  h->ctx.n = n;
+  { ProfScope ps(h, -1); mpm::launch_pack_frame(h->ctx, h->stream, stride, d_data, d_energy, d_tkey, d_counts); }
+  MPM_CUDA(h, cudaGetLastError());
+  double energy = 0;
+  unsigned tkey[2], counts[256];
+  MPM_CUDA(h, cudaMemcpyAsync(data, d_data, rows * 8 * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
+  MPM_CUDA(h, cudaMemcpyAsync(&energy, d_energy, 8, cudaMemcpyDeviceToHost, h->stream));
+  MPM_CUDA(h, cudaMemcpyAsync(tkey, d_tkey, sizeof tkey, cudaMemcpyDeviceToHost, h->stream));
+  MPM_CUDA(h, cudaMemcpyAsync(counts, d_counts, sizeof counts, cudaMemcpyDeviceToHost, h->stream));
+  MPM_CUDA(h, cudaStreamSynchronize(h->stream));
+  auto unkey = [](unsigned k) {
+    const unsigned u = (k & 0x80000000u) ? (k & 0x7fffffffu) : ~k;
+    float f;
+    std::memcpy(&f, &u, 4);
+    return static_cast<double>(f);
+  };
+  info->thermal_energy = energy;
+  info->min_T = unkey(tkey[0]);
+  info->max_T = unkey(tkey[1]);
+  for (int k = 0; k < 256; ++k) info->per_material[k] = counts[k];
+  bool finite = L.nonfinite == 0 && std::isfinite(L.mass) && std::isfinite(energy) && std::isfinite(L.min_j);
+  for (int64_t i = 0; i < rows * 8 && finite; ++i) finite = std::isfinite(data[i]);
+  if (!finite) return fail(h, MPM_ERR_NONFINITE, "non-finite particle state in the frame");
+  return MPM_OK;
 }
 
 // ---- per-particle edits (MPM3.resetParticle / MPM3.remove) ----

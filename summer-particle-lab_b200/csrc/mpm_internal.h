@@ -154,6 +154,9 @@ void launch_upload_convert(const Ctx& c, cudaStream_t st, long long n, int dtype
 void launch_download_convert(const Ctx& c, cudaStream_t st, long long n, int dtype, void* const* dst,
                              unsigned fields);
 void launch_permute(const Ctx& c, const Particles& dst, cudaStream_t st);
+// viewer frame: sampled rows (8 floats) and energy / temperature-range / per-material reductions
+void launch_pack_frame(const Ctx& c, cudaStream_t st, long long stride, float* data, double* energy, unsigned* tkey,
+                       unsigned* counts);
 // home slots of caller indices a and b into slots[0..1] (-1 when absent)
 void launch_find_ids(const Ctx& c, cudaStream_t st, unsigned a, unsigned b, long long* slots);
 // op 0: reset the deformation of slots[0]; op 1: drop slots[0], slots[1] takes caller index a

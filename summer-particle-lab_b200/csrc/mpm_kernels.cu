@@ -1827,6 +1827,80 @@ void launch_download_convert(const Ctx& c, cudaStream_t st, long long n, int dty
 }
 
 // ---------------------------------------------------------------------------------------------
+// Frame packing for a viewer (gpu/solver.py:985-1035): one deterministic sample per block of
+// `stride` caller indices, chosen by the reference's integer hash so previews show no lattice
+// stripes, as 8 floats (x, y, z, material, T, pinned, von Mises stress, plastic strain), plus the
+// frame reductions the ledger does not carry. stats: [0] sum m cp T (FP64), [1] ordered-key
+// min T, [2] ordered-key max T (as doubles holding the keys), counts[256]: particles per material.
+
+__device__ __forceinline__ unsigned preview_pick(unsigned row, unsigned span) {
+  unsigned h = row * 747796405u + 2891336453u;
+  h = ((h >> ((h >> 28) + 4u)) ^ h) * 277803737u;
+  h = (h >> 22) ^ h;
+  return h % span;
+}
+
+__device__ __forceinline__ unsigned ordered_key(float f) {
+  const unsigned u = __float_as_uint(f);
+  return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+
+__global__ void k_pack_frame(Ctx c, long long stride, float* data, double* energy, unsigned* tkey, unsigned* counts) {
+  double e_acc = 0.0;
+  unsigned tmin = 0xffffffffu, tmax = 0u;
+  for (long long h = blockIdx.x * (long long)blockDim.x + threadIdx.x; h < c.n; h += (long long)gridDim.x * blockDim.x) {
+    const long long id = c.p.id[h];
+    const int s = c.nscenes == 1 ? 0 : find_scene_by_particle(c.scenes, c.nscenes, h);
+    const SceneDev& sc = c.scenes[s];
+    const int mi = c.single_material ? sc.mat_base : c.p.mat[h];
+    const MaterialDev& mt = c.mats[mi];
+    const float T = c.has_thermal ? c.p.T[h] : 0.f;
+    const float m = c.p.m[h];
+    e_acc += (double)m * mt.cp * T;
+    tmin = min(tmin, ordered_key(T));
+    tmax = max(tmax, ordered_key(T));
+    {  // one atomic per distinct material in the warp
+      const unsigned peers = __match_any_sync(__activemask(), mi);
+      if ((threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&counts[mi], __popc(peers));
+    }
+    const long long row = id / stride;
+    const long long span = min(stride, c.n - row * stride);
+    if ((id % stride) != (long long)preview_pick(static_cast<unsigned>(row), static_cast<unsigned>(span))) continue;
+    float D[9];
+    for (int e = 0; e < 9; ++e) D[e] = c.p.D[e * c.p.cap + h];
+    const float Jm1 = det_minus_one(D);
+    const ConstitutiveOut co = constitutive_update(mt, D, 0.f, T, c.p.V[h] / m, false);
+    const float dxy = co.tau.xx - co.tau.yy, dyz = co.tau.yy - co.tau.zz, dzx = co.tau.zz - co.tau.xx;
+    const float vm = sqrtf(fmaxf(0.f, 0.5f * (dxy * dxy + dyz * dyz + dzx * dzx) +
+                                          3.f * (co.tau.xy * co.tau.xy + co.tau.xz * co.tau.xz + co.tau.yz * co.tau.yz))) /
+                     fmaxf(1e-6f, 1.f + Jm1);
+    float* r = data + row * 8;
+    const double Hs = sc.H;
+    r[0] = (float)(sc.origin[0] + c.p.qx[h] * (Hs / 4194304.0));
+    r[1] = (float)(sc.origin[1] + c.p.qy[h] * (Hs / 4194304.0));
+    r[2] = (float)(sc.origin[2] + c.p.qz[h] * (Hs / 4194304.0));
+    r[3] = (float)mi;
+    r[4] = T;
+    r[5] = c.has_pinned ? (float)c.p.pinned[h] : 0.f;
+    r[6] = vm;
+    r[7] = c.has_plastic ? c.p.ep[h] : 0.f;
+  }
+  const double es = warp_sum_d(e_acc);
+  const unsigned mn = __reduce_min_sync(0xffffffffu, tmin), mx = __reduce_max_sync(0xffffffffu, tmax);
+  if ((threadIdx.x & 31) == 0) {
+    if (es != 0.0) atomicAdd(energy, es);
+    atomicMin(&tkey[0], mn);
+    atomicMax(&tkey[1], mx);
+  }
+}
+
+void launch_pack_frame(const Ctx& c, cudaStream_t st, long long stride, float* data, double* energy, unsigned* tkey,
+                       unsigned* counts) {
+  const long long blocks = (c.n + 255) / 256 < 4096 ? (c.n + 255) / 256 : 4096;
+  if (blocks > 0) k_pack_frame<<<static_cast<unsigned>(blocks), 256, 0, st>>>(c, stride, data, energy, tkey, counts);
+}
+
+// ---------------------------------------------------------------------------------------------
 // stateless constitutive batch: projectPlastic + stress (src/three/constitutive.js:52-86)
 
 __global__ void k_return_map(MaterialDev mt, long long n, const double* F_in, const double* ep, const double* T,

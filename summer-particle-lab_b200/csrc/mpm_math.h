@@ -195,6 +195,7 @@ struct MaterialDev {
   float yield_stress, hardening;
   float T_ref, inv_T_span, hot_ratio;
   float heat_per_work;   // heat_fraction / specific_heat (K per J/kg)
+  float cp;              // specific heat (J/kg/K)
   float wave_modulus;    // lambda + 2 mu (CFL wave speed c = sqrt(wave_modulus V / m))
   // Johnson-Cook, models 6 and 7 (src/three/metal-plasticity.js:12-19): yield_stress = A,
   // hardening = B, flow = (A + B ep^n)(1 + C ln max(1, rate / rate0))(1 - theta^m), the last

@@ -77,6 +77,12 @@ class MpmGateCounts(ctypes.Structure):
 SURROGATE_PARAMS = 5768
 
 
+class MpmFrameInfo(ctypes.Structure):
+    _fields_ = [("count", _I64), ("rows", _I64), ("stride", _I64), ("mass", _D), ("thermal_energy", _D),
+                ("min_T", _D), ("max_T", _D), ("min_j", _D), ("max_von_mises", _D), ("max_plastic", _D),
+                ("nonfinite", _I64), ("per_material", _I64 * 256)]
+
+
 class SmpmSim(ctypes.Structure):
     _fields_ = [("count", _I32), ("scene", _I32), ("boundary", _I32), ("gravity", _I32),
                 ("solid_stiffness", _D), ("strength", _D), ("x", _P), ("y", _P), ("vx", _P), ("vy", _P),
@@ -129,6 +135,7 @@ SIGNATURES = {
     "mpm_return_map_batch": (ctypes.c_int, [ctypes.POINTER(MpmMaterial), _I64, _P, _P, _P, _D, _P, _P, _P]),
     "mpm_p2g_noalloc": (ctypes.c_int, [ctypes.POINTER(MpmDomain), ctypes.POINTER(MpmMaterial), _I64, _P, _P, _P, _P, _P,
                                         _P, _D, _P, _P, _P]),
+    "mpm_pack_frame": (ctypes.c_int, [_P, _I64, _P, _I64, ctypes.POINTER(MpmFrameInfo)]),
     "mpm_reset_particle": (ctypes.c_int, [_P, _I64]),
     "mpm_remove_particle": (ctypes.c_int, [_P, _I64, _I64]),
     "mpm_batch_create": (ctypes.c_int, [ctypes.POINTER(MpmSceneDesc), _I32, ctypes.POINTER(_P)]),
