@@ -218,6 +218,16 @@ int mpm_checkpoint_load(mpm_handle* h, const char* path);
 int mpm_host_alloc(size_t bytes, void** out);
 int mpm_host_free(void* p);
 
+/* ---- grid heat conduction ----
+ * No counterpart in the reference's solid step (its particles exchange heat pairwise,
+ * gpu/solver.py:775-811); this is the grid conduction of the coupled scene: each substep P2G
+ * also scatters sum w m T, node temperatures T_i follow, face-neighbour nodes that both hold
+ * mass exchange Q_ij = G_ij (T_j - T_i) with G_ij = k h dt min(1, min(m_i, m_j) / (rho h^3)),
+ * and G2P adds the interpolated node increments Q_i / (m_i cp) to the particles' temperatures.
+ * The heat sum m cp T is conserved; dt is limited to 0.9 rho cp h^2 / (6 k). conductivity <= 0
+ * turns it off. Applies to scene `scene` (0 for a single-scene handle); not saved in checkpoints. */
+int mpm_set_conduction(mpm_handle* h, int32_t scene, double conductivity, double density, double specific_heat);
+
 /* ---- viewer frame (gpu/solver.py:985-1035, the Taichi service's `pack` + `snapshot`) ----
  * One deterministic sample per block of `stride` = ceil(count / preview_limit) caller indices,
  * chosen by the reference's integer hash so previews show no lattice stripes, written as 8 floats

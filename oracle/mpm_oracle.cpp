@@ -60,6 +60,10 @@ struct OracleScene {
   // CFL rule (src/three/mpm.js:43-55): dt <= min(dt_max, cfl*H/max(1, |v|+c*max(1,row*col,compr)),
   // grad_limit/max(1, sum|C|)) with c = sqrt((lambda+2mu)/rho)
   double cfl, dt_max, grad_limit;
+  // grid heat conduction (this project's coupled-scene extension, no reference counterpart):
+  // off when cond_k <= 0; conductance k H dt min(1, min(m_i, m_j) / (rho H^3)) between face
+  // neighbours that both hold mass, node increments Q_i / (m_i cp) added to particles in G2P
+  double cond_k, cond_rho, cond_cp;
 };
 
 struct OracleLedger {
@@ -393,6 +397,8 @@ int oracle_step(const OracleScene* sc, const OracleMaterial* mats, int32_t nmat,
   const int64_t nodes = (int64_t)sc->dims[0] * sc->dims[1] * sc->dims[2];
   const double H = sc->H;
   std::vector<double> gm(nodes, 0.0), gv(nodes * 3, 0.0);
+  const bool conduct = sc->cond_k > 0;
+  std::vector<double> gh(conduct ? nodes : 0, 0.0), gdT(conduct ? nodes : 0, 0.0);
   std::vector<uint8_t> fixed(nodes, 0);
   std::vector<double> tau((size_t)n * 9);
   for (int64_t p = 0; p < n; ++p)
@@ -432,6 +438,15 @@ int oracle_step(const OracleScene* sc, const OracleMaterial* mats, int32_t nmat,
           const double add[4] = {w * mp, w * (mp * v[p * 3 + 0] + A[0] * dx + A[1] * dy + A[2] * dz),
                                  w * (mp * v[p * 3 + 1] + A[3] * dx + A[4] * dy + A[5] * dz),
                                  w * (mp * v[p * 3 + 2] + A[6] * dx + A[7] * dy + A[8] * dz)};
+          if (conduct) {
+            const double hq = w * mp * T[p];
+            if (atomic) {
+#pragma omp atomic
+              gh[nd] += hq;
+            } else {
+              gh[nd] += hq;
+            }
+          }
           if (atomic) {
 #pragma omp atomic
             gm[nd] += add[0];
@@ -484,6 +499,30 @@ int oracle_step(const OracleScene* sc, const OracleMaterial* mats, int32_t nmat,
     }
   }
   if (grid_vel) std::memcpy(grid_vel, gv.data(), nodes * 3 * sizeof(double));
+  // grid heat conduction between face-neighbour nodes that both hold mass
+  if (conduct) {
+    std::vector<double> Tn(nodes, 0.0);
+    for (int64_t nd = 0; nd < nodes; ++nd)
+      if (gm[nd] > sc->mass_eps) Tn[nd] = gh[nd] / gm[nd];
+    const double g0 = sc->cond_k * H * dt, mfull = sc->cond_rho * H * H * H;
+    const int64_t stride[3] = {1, sc->dims[0], (int64_t)sc->dims[0] * sc->dims[1]};
+#pragma omp parallel for schedule(static)
+    for (int64_t nd = 0; nd < nodes; ++nd) {
+      if (!(gm[nd] > sc->mass_eps)) continue;
+      const int idx[3] = {(int)(nd % sc->dims[0]), (int)((nd / sc->dims[0]) % sc->dims[1]),
+                          (int)(nd / ((int64_t)sc->dims[0] * sc->dims[1]))};
+      double q = 0;
+      for (int a = 0; a < 3; ++a)
+        for (int d = -1; d <= 1; d += 2) {
+          const int pp = idx[a] + d;
+          if (pp < 0 || pp >= sc->dims[a]) continue;
+          const int64_t nj = nd + d * stride[a];
+          if (!(gm[nj] > sc->mass_eps)) continue;
+          q += g0 * std::min(1.0, std::min(gm[nd], gm[nj]) / mfull) * (Tn[nj] - Tn[nd]);
+        }
+      gdT[nd] = q / (gm[nd] * sc->cond_cp);
+    }
+  }
   // G2P + F update (mpm.js:107-123), then the return map (mpm.js:126-131)
   int status = 0;
 #pragma omp parallel for schedule(static) reduction(min : status)
@@ -514,6 +553,22 @@ int oracle_step(const OracleScene* sc, const OracleMaterial* mats, int32_t nmat,
         F[p * 9 + a * 3 + b] = val;
       }
     std::memcpy(&C[p * 9], c, sizeof c);
+    if (conduct) {
+      // node temperature increments, interpolated like the velocity, and relaxation of the particle's
+      // offset from the interpolated node temperature at the rate of the finest unresolved mode
+      // (wavelength 2H): beta = 1 - exp(-pi^2 alpha dt / H^2). Both parts keep sum m T.
+      double dT = 0, Tint = 0;
+      for (int k = 0; k < 3; ++k)
+        for (int j = 0; j < 3; ++j)
+          for (int i = 0; i < 3; ++i) {
+            const int64_t nd = node_index(sc, st.base[0] + i, st.base[1] + j, st.base[2] + k);
+            const double w = st.w[0][i] * st.w[1][j] * st.w[2][k];
+            dT += w * gdT[nd];
+            Tint += w * (gm[nd] > sc->mass_eps ? gh[nd] / gm[nd] : 0.0);
+          }
+      const double beta = 1 - std::exp(-9.869604401089358 * sc->cond_k * dt / (sc->cond_rho * sc->cond_cp * H * H));
+      T[p] += dT + beta * (Tint - T[p]);
+    }
     v[p * 3] = vx; v[p * 3 + 1] = vy; v[p * 3 + 2] = vz;
     x[p * 3] += dt * vx; x[p * 3 + 1] += dt * vy; x[p * 3 + 2] += dt * vz;
     if (sc->clamp_positions)
@@ -572,7 +627,9 @@ double oracle_stable_dt(const OracleScene* sc, const OracleMaterial* mats, int64
     maxw = std::max(maxw, speed + c * std::max(1.0, std::max(row * col, compression)));
     grad = std::max(grad, g);
   }
-  return std::min(sc->dt_max, std::min(sc->cfl * sc->H / maxw, sc->grad_limit / grad));
+  double dt = std::min(sc->dt_max, std::min(sc->cfl * sc->H / maxw, sc->grad_limit / grad));
+  if (sc->cond_k > 0) dt = std::min(dt, 0.9 * sc->cond_rho * sc->cond_cp * sc->H * sc->H / (6 * sc->cond_k));
+  return dt;
 }
 
 // src/simulation/mechanical-diagnostics.js:9-37 (SI: no sandbox length factor) and

@@ -32,7 +32,8 @@ class OracleScene(ctypes.Structure):
                 ("sticky_floor", ctypes.c_int32), ("lower", _D * 3), ("upper", _D * 3),
                 ("gravity", _D * 3), ("gravity_on_grid", ctypes.c_int32),
                 ("clamp_positions", ctypes.c_int32), ("clamp_lo", _D * 3), ("clamp_hi", _D * 3),
-                ("mass_eps", _D), ("cfl", _D), ("dt_max", _D), ("grad_limit", _D)]
+                ("mass_eps", _D), ("cfl", _D), ("dt_max", _D), ("grad_limit", _D),
+                ("cond_k", _D), ("cond_rho", _D), ("cond_cp", _D)]
 
 
 class OracleLedger(ctypes.Structure):
@@ -237,6 +238,10 @@ class OracleState:
             raise RuntimeError(f"oracle_step failed: {rc}")
         return (gm, gp, gv) if want_grid else None
 
+    def set_conduction(self, k, rho, cp):
+        """Grid heat conduction (k W/m/K, density, specific heat); k <= 0 turns it off."""
+        self.sc.cond_k, self.sc.cond_rho, self.sc.cond_cp = k, rho, cp
+
     def stable_dt(self):
         return lib().oracle_stable_dt(ctypes.byref(self.sc), self.mats, self.n, _ptr(self.v),
                                       _ptr(self.C), _ptr(self.F), _ptr(self.m), _ptr(self.V),
@@ -273,5 +278,9 @@ def material_from(mat):
 
 
 def state_from_scene(scene):
-    """OracleState for a mpm_b200.scenes.Scene."""
-    return OracleState(scene, [material_from(m) for m in scene.materials])
+    """OracleState for a mpm_b200.scenes.Scene (with its grid heat conduction, if any)."""
+    st = OracleState(scene, [material_from(m) for m in scene.materials])
+    cond = scene.meta.get("conduction") if scene.meta else None
+    if cond:
+        st.set_conduction(cond["k"], cond["rho"], cond["cp"])
+    return st

@@ -286,7 +286,11 @@ static int alloc_grid(mpm_handle* h) {
     for (int k = 0; k < 2; ++k) {
       c.g.acc0[k] = cv.take<float4>(nodes);
       c.g.acc1[k] = cv.take<float4>(nodes);
+      c.g.heat[k] = cv.take<float>(nodes);
     }
+    c.g.tnode = cv.take<float>(nodes);
+    c.g.mnode = cv.take<float>(nodes);
+    c.g.tile_epoch = cv.take<unsigned>(ntiles);
     c.g.vel = cv.take<float4>(nodes);
     c.g.tile_flag = cv.take<unsigned>(ntiles);
     c.g.active[0] = cv.take<unsigned>(ntiles);
@@ -415,6 +419,10 @@ static void launch_substep(mpm_handle* h, bool scatter) {
   Ctx& c = h->ctx;
   { ProfScope ps(h, 0); mpm::launch_begin(c, h->stream); }
   { ProfScope ps(h, 1); mpm::launch_grid_update(c, h->stream, h->grid_blocks); }
+  if (c.conduct) {
+    ProfScope ps(h, -1);
+    mpm::launch_conduct(c, h->stream, h->grid_blocks);
+  }
   { ProfScope ps(h, 2); mpm::launch_g2p2g(c, h->stream, h->g2p2g_blocks, scatter); }
   if (scatter) {
     { ProfScope ps(h, 3); mpm::launch_scan(c, h->stream); }
@@ -1276,6 +1284,46 @@ int mpm_return_map_batch(const mpm_material* material, int64_t n, const double* 
   if (e == cudaSuccess) e = cudaMemcpy(tau, dtau, 9 * n * sizeof(double), cudaMemcpyDeviceToHost);
   cudaFree(d);
   return e == cudaSuccess ? MPM_OK : MPM_ERR_CUDA;
+}
+
+// ---- grid heat conduction ----
+
+int mpm_set_conduction(mpm_handle* h, int32_t scene, double conductivity, double density, double specific_heat) {
+  if (!h) return MPM_ERR_INVALID_ARG;
+  if (scene < 0 || scene >= (int)h->scenes.size()) return fail(h, MPM_ERR_INVALID_ARG, "scene index out of range");
+  if (!(conductivity >= 0) || !std::isfinite(conductivity))
+    return fail(h, MPM_ERR_INVALID_ARG, "conductivity must be finite and >= 0");
+  SceneDev& s = h->scenes[scene];
+  if (conductivity > 0) {
+    if (!(density > 0) || !(specific_heat > 0)) return fail(h, MPM_ERR_INVALID_ARG, "density and specific heat must be > 0");
+    const double H = s.H;
+    s.cond_G = static_cast<float>(conductivity * H);
+    s.cond_inv_mfull = static_cast<float>(1.0 / (density * H * H * H));
+    s.cond_inv_cp = static_cast<float>(1.0 / specific_heat);
+    s.cond_dt_max = static_cast<float>(0.9 * density * specific_heat * H * H / (6.0 * conductivity));
+  } else {
+    s.cond_G = s.cond_inv_mfull = s.cond_inv_cp = 0.f;
+    s.cond_dt_max = 0.f;
+  }
+  if (scene == 0) {
+    // keep the single-scene copy (and its particle range) in step
+    SceneDev s0 = s;
+    s0.p_begin = h->scene.p_begin;
+    s0.p_end = h->scene.p_end;
+    s0.mat_base = h->scene.mat_base;
+    h->scene = s0;
+    s = s0;
+  }
+  MPM_CUDA(h, cudaMemcpyAsync(const_cast<SceneDev*>(h->ctx.scenes) + scene, &s, sizeof(SceneDev), cudaMemcpyHostToDevice,
+                              h->stream));
+  MPM_CUDA(h, cudaStreamSynchronize(h->stream));
+  int any = 0;
+  for (const SceneDev& x : h->scenes) any |= x.cond_G > 0.f;
+  h->ctx.conduct = any;
+  if (any) h->ctx.has_thermal = 1;  // temperatures are read and written
+  drop_graph(h);
+  h->grid_valid = false;  // the next scatter carries the heat channel
+  return MPM_OK;
 }
 
 // ---- viewer frame ----

@@ -59,6 +59,12 @@ struct SceneDev {
   int mat_base, nmat;
   long long p_begin, p_end;  // home particle range
   double origin[3];
+  // grid heat conduction between face-neighbour nodes (off when cond_G == 0):
+  // conductance k h dt min(1, min(m_i, m_j) / (rho h^3)), node heat capacity m cp
+  float cond_G;          // k h (W/K)
+  float cond_inv_mfull;  // 1 / (rho h^3)
+  float cond_inv_cp;     // 1 / cp
+  float cond_dt_max;     // explicit-diffusion limit 0.9 rho cp h^2 / (6 k)
 };
 
 struct Ctrl {
@@ -100,7 +106,11 @@ struct Particles {
 struct Grid {
   float4* acc0[2];
   float4* acc1[2];
-  float4* vel;
+  float* heat[2];        // sum w m T (conduction only)
+  float* tnode;          // node temperature of the last grid update (conduction only)
+  float* mnode;          // node mass of the last grid update (conduction only)
+  unsigned* tile_epoch;  // step index of a node tile's last grid update (conduction only)
+  float4* vel;           // (vx, vy, vz, m), or (vx, vy, vz, dT) after a conduction pass
   unsigned* tile_flag;   // per node tile
   unsigned* active[2];   // active node-tile lists
 };
@@ -134,6 +144,7 @@ struct Ctx {
   int has_plastic;      // plastic strain array is read and written
   int use_tma;
   int ws_blocks;        // > 0: the particle passes that scatter run warp-specialised on this many CTAs
+  int conduct;          // a scene conducts heat on the grid: heat channel, conduction pass, dT gather
 };
 
 // Launch wrappers (mpm_kernels.cu)
@@ -146,6 +157,7 @@ void launch_control_step(const Ctx& c, cudaStream_t st, int mode, double dt_req,
 void launch_begin(const Ctx& c, cudaStream_t st);
 void launch_grid_clear(const Ctx& c, cudaStream_t st, int grid_blocks);
 void launch_grid_update(const Ctx& c, cudaStream_t st, int grid_blocks);
+void launch_conduct(const Ctx& c, cudaStream_t st, int grid_blocks);
 void launch_g2p2g(const Ctx& c, cudaStream_t st, int grid_blocks, bool scatter);
 void launch_ledger(const Ctx& c, cudaStream_t st, double* partials, int blocks, double* out);
 void launch_grid_debug(const Ctx& c, cudaStream_t st, int scene, float dt, double* mass, double* mom);

@@ -242,7 +242,8 @@ __global__ void __launch_bounds__(256) k_begin(Ctx c) {
     const SceneDev& sc = c.scenes[s];
     const float wave = fmaxf(1.f, __uint_as_float(c.wave_max[s]));
     const float grad = fmaxf(1.f, __uint_as_float(c.grad_max[s]));
-    const float dt = fminf(sc.dt_max, fminf(sc.cfl * sc.H / wave, sc.grad_limit / grad));
+    float dt = fminf(sc.dt_max, fminf(sc.cfl * sc.H / wave, sc.grad_limit / grad));
+    if (sc.cond_G > 0.f) dt = fminf(dt, sc.cond_dt_max);
     c.dt_scene[s] = dt;  // provisional: the scene's own stable dt
     local = fminf(local, dt);
   }
@@ -465,7 +466,7 @@ void launch_sort_scatter(const Ctx& c, cudaStream_t st, bool initial) {
 // then one float4 atomic per touched node and channel group flushes the window to HBM.
 
 constexpr int kCap = 512;      // particles per scatter round
-constexpr int kPay = 22;       // payload floats per particle
+constexpr int kPay = 23;       // payload floats per particle (the last, m T, only with conduction)
 constexpr int kBuckets = 216;  // 6^3 possible stencil bases in the scatter window
 constexpr unsigned kMetaInvalid = 0x80000000u;
 
@@ -485,7 +486,7 @@ struct TileCtx {
 struct __align__(128) PartSmem {
   float4 vwin[2][kWinG * kWinG * kWinG];  // double-buffered TMA destinations (3456 B each)
   float acc[kChannels * kWinSNodes];      // 16 KiB scatter window
-  float pay[kPay * kCap];                 // 44 KiB payloads, structure of arrays
+  float pay[kPay * kCap];                 // 46 KiB payloads, structure of arrays
   unsigned meta[kCap];                    // bucket | rank << 8 (or kMetaInvalid)
   unsigned short sidx[kCap];              // slots sorted by bucket
   int hist[kBuckets];
@@ -507,7 +508,7 @@ size_t particle_smem_bytes() { return sizeof(PartSmem); }
 // channel atomics straight to the accumulators, and the node tiles they touch become active.
 __device__ __noinline__ void scatter_global(const Ctx& c, const SceneDev& sc, const TileCtx& tc, int nxt,
                                                const int b[3], const float t[3], float m, const float mv[3],
-                                               const float mC[9], const float s6[6], bool pinned) {
+                                               const float mC[9], const float s6[6], bool pinned, float mT) {
   float w[3][3];
 #pragma unroll
   for (int a = 0; a < 3; ++a) bspline_weights(t[a], w[a]);
@@ -527,6 +528,7 @@ __device__ __noinline__ void scatter_global(const Ctx& c, const SceneDev& sc, co
         atomicAdd(a1 + 1, wt * (s6[3] * dx + s6[1] * dy + s6[5] * dz));
         atomicAdd(a1 + 2, wt * (s6[4] * dx + s6[5] * dy + s6[2] * dz));
         if (pinned && wt > 1e-8f) atomicAdd(a1 + 3, wt * m);
+        if (c.conduct) atomicAdd(&c.g.heat[nxt][node], wt * mT);
       }
   mark_node_tiles_of(c, sc, b[0], b[1], b[2], nxt);
 }
@@ -545,8 +547,12 @@ __device__ __forceinline__ void flush_window_p(const Ctx& c, const SceneDev& sc,
         const long long node = sc.node_base + ((long long)z * sc.gdim[1] + y) * sc.gdim[0] + x;
         atomicAdd(&c.g.acc0[nxt][node], make_float4(mass, acc[1 * kWinSNodes + i], acc[2 * kWinSNodes + i],
                                                     acc[3 * kWinSNodes + i]));
+        // channel 7 of the window is pinned mass without conduction (always zero there: pinned particles
+        // scatter globally) and the heat sum w m T with it
+        const float ch7 = acc[7 * kWinSNodes + i];
         atomicAdd(&c.g.acc1[nxt][node], make_float4(acc[4 * kWinSNodes + i], acc[5 * kWinSNodes + i],
-                                                    acc[6 * kWinSNodes + i], acc[7 * kWinSNodes + i]));
+                                                    acc[6 * kWinSNodes + i], c.conduct ? 0.f : ch7));
+        if (c.conduct) atomicAdd(&c.g.heat[nxt][node], ch7);
       }
     }
 #pragma unroll
@@ -604,6 +610,7 @@ __device__ __forceinline__ unsigned state_flags(const float v[3], const float D[
 
 // Phase B task: one non-empty base bucket, one z layer of its stencil. Sums the 3x3 nodes x 7
 // channels over the bucket's particles in registers, then adds them to the shared window.
+template <bool HEAT>
 __device__ __forceinline__ void bucket_layer_p(const float* pay, const unsigned short* sidx, const int* bstart,
                                                float* acc, int b, int kz) {
   const int lx = b % 6, ly = (b / 6) % 6, lz = b / 36;
@@ -663,10 +670,35 @@ __device__ __forceinline__ void bucket_layer_p(const float* pay, const unsigned 
 #pragma unroll
       for (int ch = 0; ch < 7; ++ch) atomicAdd(&acc[ch * kWinSNodes + node], a[y][x][ch]);
     }
+  if (HEAT) {  // sum w m T into channel 7 (conduction)
+    float hsum[3][3];
+#pragma unroll
+    for (int y = 0; y < 3; ++y)
+#pragma unroll
+      for (int x = 0; x < 3; ++x) hsum[y][x] = 0.f;
+    for (int i = bstart[b]; i < i1; ++i) {
+      const float* P = pay + sidx[i];
+      float wx[3], wy[3], wzv[3];
+      bspline_weights(P[0 * kCap], wx);
+      bspline_weights(P[1 * kCap], wy);
+      bspline_weights(P[2 * kCap], wzv);
+      const float wmt = (kz == 0 ? wzv[0] : (kz == 1 ? wzv[1] : wzv[2])) * P[22 * kCap];
+#pragma unroll
+      for (int y = 0; y < 3; ++y)
+#pragma unroll
+        for (int x = 0; x < 3; ++x) hsum[y][x] += wx[x] * wy[y] * wmt;
+    }
+#pragma unroll
+    for (int y = 0; y < 3; ++y)
+#pragma unroll
+      for (int x = 0; x < 3; ++x)
+        atomicAdd(&acc[7 * kWinSNodes + ((lz + kz) * kWinS + (ly + y)) * kWinS + (lx + x)], hsum[y][x]);
+  }
 }
 
+template <bool HEAT>
 __device__ __forceinline__ void bucket_layer(PartSmem& sm, int b, int kz) {
-  bucket_layer_p(sm.pay, sm.sidx, sm.bstart, sm.acc, b, kz);
+  bucket_layer_p<HEAT>(sm.pay, sm.sidx, sm.bstart, sm.acc, b, kz);
 }
 
 // Exclusive scan of the bucket histogram by warp 0, with the compact list of non-empty buckets.
@@ -744,6 +776,25 @@ __device__ __forceinline__ void gather27(Ld ld, const float t[3], const float w[
   out[9] = cx2; out[10] = cy2; out[11] = cz2;
 }
 
+// Weighted sum of the nodes' fourth channel (the conduction temperature increment).
+template <typename Ld>
+__device__ __forceinline__ float gather_w27(Ld ld, const float w[3][3]) {
+  float sz = 0.f;
+#pragma unroll
+  for (int kz = 0; kz < 3; ++kz) {
+    float sy = 0.f;
+#pragma unroll
+    for (int ky = 0; ky < 3; ++ky) {
+      float sx = 0.f;
+#pragma unroll
+      for (int kx = 0; kx < 3; ++kx) sx = fmaf(w[0][kx], ld(kz, ky, kx).w, sx);
+      sy = fmaf(w[1][ky], sx, sy);
+    }
+    sz = fmaf(w[2][kz], sy, sz);
+  }
+  return sz;
+}
+
 // Gather straight from global memory (a particle whose stencil is outside the staged window).
 __device__ __noinline__ void gather_global(const float4* base, int sy, long long sz, const float t[3], const float w[3][3],
                                            float out[12]) {
@@ -755,7 +806,7 @@ __device__ __noinline__ void gather_global(const float4* base, int sy, long long
 // for the P2G pass and pinned particles, the stress of the stored state; then the scatter payload
 // bucketed by its new stencil base in the shared window (pay, meta, hist), and the CFL terms.
 // Writes the particle's new state and returns its next sort key (all ones when not needed).
-template <int PASS>
+template <int PASS, bool HEAT>
 __device__ __forceinline__ unsigned particle_phase_a(const Ctx& c, const SceneDev& sc, const TileCtx& tc,
                                                      const MaterialDev& mt_single, bool single, const float4* vwin,
                                                      unsigned home, unsigned j, float dt, int nxt, float* pay,
@@ -797,6 +848,27 @@ __device__ __forceinline__ unsigned particle_phase_a(const Ctx& c, const SceneDe
     } else {
       gather_global(c.g.vel + tc.node_base + ((long long)b[2] * tc.gdim[1] + b[1]) * tc.gdim[0] + b[0], tc.gdim[0],
                     (long long)tc.gdim[0] * tc.gdim[1], t, w, acc12);
+    }
+    // grid heat conduction: the node temperature increments, interpolated like the velocity, and
+    // relaxation of the particle's offset from the interpolated node temperature at the rate of the
+    // finest unresolved mode (wavelength 2h): beta = 1 - exp(-pi^2 alpha dt / h^2); both parts keep
+    // the heat sum, and the relaxation lets a body reach a uniform temperature
+    if (HEAT && sc.cond_G > 0.f) {
+      const long long o = tc.node_base + ((long long)b[2] * tc.gdim[1] + b[1]) * tc.gdim[0] + b[0];
+      const long long sz = (long long)tc.gdim[0] * tc.gdim[1];
+      float dTc;
+      if (in_g) {
+        const float4* win = &vwin[(l2 * kWinG + l1) * kWinG + l0];
+        dTc = gather_w27([&](int kz, int ky, int kx) { return win[(kz * kWinG + ky) * kWinG + kx]; }, w);
+      } else {
+        const float4* base = c.g.vel + o;
+        dTc = gather_w27([&](int kz, int ky, int kx) { return base[kz * sz + ky * tc.gdim[0] + kx]; }, w);
+      }
+      const float* tn = c.g.tnode + o;
+      const float Tint = gather_w27([&](int kz, int ky, int kx) {
+        return make_float4(0.f, 0.f, 0.f, tn[kz * sz + ky * tc.gdim[0] + kx]); }, w);
+      const float beta = 1.f - expf(-9.8696044f * sc.cond_G * sc.cond_inv_mfull * sc.cond_inv_cp * dt);
+      T += dTc + beta * (Tint - T);
     }
     const float v0 = acc12[0], v1 = acc12[1], v2 = acc12[2];
     const float c0 = acc12[3], c1 = acc12[4], c2 = acc12[5], c3 = acc12[6], c4 = acc12[7], c5 = acc12[8],
@@ -885,10 +957,11 @@ __device__ __forceinline__ unsigned particle_phase_a(const Ctx& c, const SceneDe
       for (int e = 0; e < 9; ++e) P[(7 + e) * kCap] = mC[e];
 #pragma unroll
       for (int e = 0; e < 6; ++e) P[(16 + e) * kCap] = s6[e];
+      if (HEAT) P[22 * kCap] = m * T;
     } else {
       meta[j] = kMetaInvalid;
       if (!in_w) flags |= 0x10u;
-      scatter_global(c, sc, tc, nxt, nb, t, m, mv, mC, s6, pinned);
+      scatter_global(c, sc, tc, nxt, nb, t, m, mv, mC, s6, pinned, m * T);
     }
   }
   float wave, grad;
@@ -900,7 +973,7 @@ __device__ __forceinline__ unsigned particle_phase_a(const Ctx& c, const SceneDe
   return key;
 }
 
-template <int PASS>
+template <int PASS, bool HEAT>
 __global__ void __launch_bounds__(kBlock, 2) k_particles(const __grid_constant__ Ctx c) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   PartSmem& sm = *reinterpret_cast<PartSmem*>(smem_raw);
@@ -1019,7 +1092,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_particles(const __grid_constant__
         unsigned key = 0xffffffffu;
         if (j < nround) {
           const unsigned home = (r0 == 0 && pf_ok) ? (jj == 0 ? pf[0] : pf[1]) : c.p.perm[it.y + r0 + j];
-          key = particle_phase_a<PASS>(c, sc, tc, sm.mt, single, sm.vwin[cb], home, j, dt, nxt, sm.pay, sm.meta,
+          key = particle_phase_a<PASS, HEAT>(c, sc, tc, sm.mt, single, sm.vwin[cb], home, j, dt, nxt, sm.pay, sm.meta,
                                        sm.hist, wave_acc, grad_acc, flags_acc, work_acc);
         }
         if (PASS == kPassG2P2G) count_key(c, key);
@@ -1040,7 +1113,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_particles(const __grid_constant__
         const int nbk = sm.nbuckets;
         for (int task = threadIdx.x; task < 3 * nbk; task += kBlock) {
           const int kz = task / nbk;
-          bucket_layer(sm, sm.blist[task - kz * nbk], kz);
+          bucket_layer<HEAT>(sm, sm.blist[task - kz * nbk], kz);
         }
         __syncthreads();
         if (r0 == 0) {  // perm of the next tile's first round, consumed there
@@ -1156,7 +1229,7 @@ __device__ __forceinline__ void group_reduce_item(const Ctx& c, int scene, float
   }
 }
 
-template <int PASS>
+template <int PASS, bool HEAT>
 __global__ void __launch_bounds__(kWsThreads, 1) k_particles_ws(const __grid_constant__ Ctx c) {
   static_assert(PASS != kPassG2P, "the warp-specialised pass always scatters");
   extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -1282,7 +1355,7 @@ __global__ void __launch_bounds__(kWsThreads, 1) k_particles_ws(const __grid_con
           unsigned key = 0xffffffffu;
           if (j < nround) {
             const unsigned home = c.p.perm[it.y + r0 + j];
-            key = particle_phase_a<PASS>(c, sc, tc, sm.mt, single, sm.vwin[cb], home, j, dt, nxt, sm.pay[s],
+            key = particle_phase_a<PASS, HEAT>(c, sc, tc, sm.mt, single, sm.vwin[cb], home, j, dt, nxt, sm.pay[s],
                                          sm.meta[s], sm.hist[s], wave_acc, grad_acc, flags_acc, work_acc);
           }
           if (PASS == kPassG2P2G) count_key(c, key);
@@ -1346,7 +1419,7 @@ __global__ void __launch_bounds__(kWsThreads, 1) k_particles_ws(const __grid_con
       const int nbk = sm.nbuckets;
       for (int task = tb; task < 3 * nbk; task += kWsGroup) {
         const int kz = task / nbk;
-        bucket_layer_p(sm.pay[s], sm.sidx, sm.bstart, sm.acc, sm.blist[task - kz * nbk], kz);
+        bucket_layer_p<HEAT>(sm.pay[s], sm.sidx, sm.bstart, sm.acc, sm.blist[task - kz * nbk], kz);
       }
       group_sync(2);
       if (tb == 0) {
@@ -1376,13 +1449,22 @@ __global__ void __launch_bounds__(kWsThreads, 1) k_particles_ws(const __grid_con
   }
 }
 
-template <int PASS>
-static void launch_pass(const Ctx& c, cudaStream_t st, int grid_blocks) {
+template <int PASS, bool HEAT>
+static void launch_pass_t(const Ctx& c, cudaStream_t st, int grid_blocks) {
   if (PASS != kPassG2P && c.ws_blocks > 0) {
-    k_particles_ws<PASS == kPassG2P ? kPassG2P2G : PASS><<<c.ws_blocks, kWsThreads, sizeof(WsSmem), st>>>(c);
+    k_particles_ws<PASS == kPassG2P ? kPassG2P2G : PASS, HEAT><<<c.ws_blocks, kWsThreads, sizeof(WsSmem), st>>>(c);
     return;
   }
-  k_particles<PASS><<<grid_blocks, kBlock, sizeof(PartSmem), st>>>(c);
+  k_particles<PASS, HEAT><<<grid_blocks, kBlock, sizeof(PartSmem), st>>>(c);
+}
+
+// The heat channel and the conduction gather are compiled only into the conducting instances.
+template <int PASS>
+static void launch_pass(const Ctx& c, cudaStream_t st, int grid_blocks) {
+  if (c.conduct)
+    launch_pass_t<PASS, true>(c, st, grid_blocks);
+  else
+    launch_pass_t<PASS, false>(c, st, grid_blocks);
 }
 
 void launch_p2g(const Ctx& c, cudaStream_t st, int grid_blocks) { launch_pass<kPassP2G>(c, st, grid_blocks); }
@@ -1396,22 +1478,24 @@ void launch_g2p2g(const Ctx& c, cudaStream_t st, int grid_blocks, bool scatter) 
 
 template <int PASS>
 static int blocks_per_sm() {
-  cudaFuncSetAttribute(k_particles<PASS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(PartSmem));
+  cudaFuncSetAttribute(k_particles<PASS, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(PartSmem));
+  cudaFuncSetAttribute(k_particles<PASS, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(PartSmem));
   int n = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_particles<PASS>, kBlock, sizeof(PartSmem));
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_particles<PASS, false>, kBlock, sizeof(PartSmem));
   return n > 0 ? n : 1;
 }
 
 // Resident CTAs per SM of the warp-specialised pass (0: it cannot launch here).
 int ws_blocks_per_sm() {
   int n0 = 0, n1 = 0;
-  if (cudaFuncSetAttribute(k_particles_ws<kPassP2G>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(WsSmem)) !=
-          cudaSuccess ||
-      cudaFuncSetAttribute(k_particles_ws<kPassG2P2G>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)sizeof(WsSmem)) != cudaSuccess)
+  const int bytes = (int)sizeof(WsSmem);
+  if (cudaFuncSetAttribute(k_particles_ws<kPassP2G, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) != cudaSuccess ||
+      cudaFuncSetAttribute(k_particles_ws<kPassG2P2G, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) != cudaSuccess ||
+      cudaFuncSetAttribute(k_particles_ws<kPassP2G, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) != cudaSuccess ||
+      cudaFuncSetAttribute(k_particles_ws<kPassG2P2G, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) != cudaSuccess)
     return 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n0, k_particles_ws<kPassP2G>, kWsThreads, sizeof(WsSmem));
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n1, k_particles_ws<kPassG2P2G>, kWsThreads, sizeof(WsSmem));
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n0, k_particles_ws<kPassP2G, true>, kWsThreads, sizeof(WsSmem));
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n1, k_particles_ws<kPassG2P2G, true>, kWsThreads, sizeof(WsSmem));
   return n0 < n1 ? n0 : n1;
 }
 
@@ -1455,9 +1539,68 @@ __global__ void __launch_bounds__(256) k_grid_update(Ctx c) {
     c.g.vel[node] = out;
     c.g.acc0[cur][node] = make_float4(0.f, 0.f, 0.f, 0.f);
     c.g.acc1[cur][node] = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (c.conduct) {  // node temperature and mass for the conduction pass
+      const bool has = a0.x > sc.mass_eps;
+      c.g.tnode[node] = has ? c.g.heat[cur][node] / a0.x : 0.f;
+      c.g.mnode[node] = has ? a0.x : 0.f;
+      c.g.heat[cur][node] = 0.f;
+      if (lid == 0) c.g.tile_epoch[tile] = k;
+    }
     if (lid == 0) c.g.tile_flag[tile] = 0u;
   }
 }
+
+// Grid heat conduction (explicit, between face-neighbour nodes that both hold mass this substep):
+// Q_ij = G_ij (T_j - T_i), G_ij = k h dt min(1, min(m_i, m_j) / (rho h^3)); dT_i = sum_j Q_ij /
+// (m_i cp), written to the node's fourth velocity channel for the gather. G is symmetric, so the
+// nodes' heat sum m cp T is unchanged; the mass factor keeps partly filled nodes under the same
+// stability limit as full ones (6 k dt / (rho cp h^2) < 1). A neighbour counts only if its node
+// tile was updated in this substep (its stored mass and temperature are current).
+__global__ void __launch_bounds__(256) k_conduct(Ctx c) {
+  Ctrl* ct = c.ctrl;
+  if (ct->done) return;
+  const unsigned k = ct->step_index;
+  const int cur = (k - 1) & 1;
+  const unsigned count = ct->active_count[cur];
+  const int sub = threadIdx.x >> 6, lid = threadIdx.x & 63;
+  for (unsigned ti = blockIdx.x * 4 + sub; ti < count; ti += gridDim.x * 4) {
+    const unsigned tile = c.g.active[cur][ti];
+    const int s = c.nscenes == 1 ? 0 : find_scene_by_node_tile(c.scenes, c.nscenes, static_cast<int>(tile));
+    const SceneDev& sc = c.scenes[s];
+    const int lt = static_cast<int>(tile) - sc.node_tile_base;
+    const int ntx = lt % sc.ntiles[0], nty = (lt / sc.ntiles[0]) % sc.ntiles[1], ntz = lt / (sc.ntiles[0] * sc.ntiles[1]);
+    const int x = ntx * 4 + (lid & 3), y = nty * 4 + ((lid >> 2) & 3), z = ntz * 4 + (lid >> 4);
+    const long long node = sc.node_base + ((long long)z * sc.gdim[1] + y) * sc.gdim[0] + x;
+    const float mi = c.g.mnode[node];
+    float dT = 0.f;
+    if (sc.cond_G > 0.f && mi > sc.mass_eps) {
+      const float Ti = c.g.tnode[node];
+      const float g0 = sc.cond_G * c.dt_scene[s];
+      float q = 0.f;
+      const int xyz[3] = {x, y, z};
+      const long long stride[3] = {1, sc.gdim[0], (long long)sc.gdim[0] * sc.gdim[1]};
+#pragma unroll
+      for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int d = -1; d <= 1; d += 2) {
+          const int p = xyz[a] + d;
+          if (p < 0 || p >= sc.gdim[a]) continue;
+          int nt[3] = {x >> 2, y >> 2, z >> 2};
+          nt[a] = p >> 2;
+          const unsigned jt = static_cast<unsigned>(sc.node_tile_base + (nt[2] * sc.ntiles[1] + nt[1]) * sc.ntiles[0] + nt[0]);
+          if (c.g.tile_epoch[jt] != k) continue;
+          const long long nj = node + d * stride[a];
+          const float mj = c.g.mnode[nj];
+          if (!(mj > sc.mass_eps)) continue;
+          q += g0 * fminf(1.f, fminf(mi, mj) * sc.cond_inv_mfull) * (c.g.tnode[nj] - Ti);
+        }
+      dT = q * sc.cond_inv_cp / mi;
+    }
+    c.g.vel[node].w = dT;
+  }
+}
+
+void launch_conduct(const Ctx& c, cudaStream_t st, int grid_blocks) { k_conduct<<<grid_blocks, 256, 0, st>>>(c); }
 
 // Clears a pending scattered grid (acc[step_index & 1] over its active list) without using it.
 __global__ void __launch_bounds__(256) k_grid_clear(Ctx c) {
@@ -1475,6 +1618,7 @@ __global__ void __launch_bounds__(256) k_grid_clear(Ctx c) {
     const long long node = sc.node_base + ((long long)z * sc.gdim[1] + y) * sc.gdim[0] + x;
     c.g.acc0[par][node] = make_float4(0.f, 0.f, 0.f, 0.f);
     c.g.acc1[par][node] = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (c.conduct) c.g.heat[par][node] = 0.f;
     if (lid == 0) c.g.tile_flag[tile] = 0u;
   }
 }

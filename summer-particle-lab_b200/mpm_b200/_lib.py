@@ -136,6 +136,7 @@ SIGNATURES = {
     "mpm_p2g_noalloc": (ctypes.c_int, [ctypes.POINTER(MpmDomain), ctypes.POINTER(MpmMaterial), _I64, _P, _P, _P, _P, _P,
                                         _P, _D, _P, _P, _P]),
     "mpm_pack_frame": (ctypes.c_int, [_P, _I64, _P, _I64, ctypes.POINTER(MpmFrameInfo)]),
+    "mpm_set_conduction": (ctypes.c_int, [_P, _I32, _D, _D, _D]),
     "mpm_reset_particle": (ctypes.c_int, [_P, _I64]),
     "mpm_remove_particle": (ctypes.c_int, [_P, _I64, _I64]),
     "mpm_batch_create": (ctypes.c_int, [ctypes.POINTER(MpmSceneDesc), _I32, ctypes.POINTER(_P)]),

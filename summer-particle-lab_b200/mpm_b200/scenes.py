@@ -179,7 +179,8 @@ def coupled_collision(scale=1, seed=5):
     v[a.shape[0]:, 0] = -20.0
     T = np.full(n, 293.0)
     s = _scene("coupled_collision", d, [mat], x, (0, 0, 0), T=T,
-               meta=dict(dt=1e-6, steps=2000, workload=f"coupled_collision_{n}_grid{grid}"))
+               meta=dict(dt=1e-6, steps=2000, workload=f"coupled_collision_{n}_grid{grid}",
+                         conduction=dict(k=150.0, rho=2700.0, cp=900.0)))
     s.v = v
     return s
 

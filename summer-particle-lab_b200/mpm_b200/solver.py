@@ -92,6 +92,13 @@ class Solver:
                          F=_ptr(F), C=_ptr(C), material=_ptr(mat), pinned=_ptr(pin))
         self._check(_lib.lib().mpm_upload_particles(self.h, n, ctypes.byref(p)))
         self.n = n
+        cond = scene.meta.get("conduction") if scene.meta else None
+        if cond:
+            self.set_conduction(cond["k"], cond["rho"], cond["cp"])
+
+    def set_conduction(self, k, rho, cp, scene=0):
+        """Grid heat conduction (W/m/K, kg/m^3, J/kg/K); k <= 0 turns it off."""
+        self._check(_lib.lib().mpm_set_conduction(self.h, int(scene), float(k), float(rho), float(cp)))
 
     def download(self, fields=("x", "v", "F", "C", "ep", "T"), dtype=np.float64):
         n = self.n
