@@ -24,7 +24,7 @@
 extern "C" {
 #endif
 
-#define MPM_ABI_VERSION 2
+#define MPM_ABI_VERSION 3
 
 /* status codes */
 #define MPM_OK 0
@@ -51,11 +51,15 @@ extern "C" {
 /* material models (src/three/constitutive.js:6-19 numbering) */
 #define MPM_MODEL_FIXED_COROTATED 0
 #define MPM_MODEL_NEO_HOOKEAN 1
+#define MPM_MODEL_SNOW 2                /* clamped principal stretches, compaction hardening */
+#define MPM_MODEL_SAND 3                /* non-cohesive Drucker-Prager with a dilation history */
 #define MPM_MODEL_J2 4
 #define MPM_MODEL_J2_HARDENING 5
 #define MPM_MODEL_JOHNSON_COOK 6        /* rate- and temperature-dependent, bisection return */
 #define MPM_MODEL_JOHNSON_COOK_SIMPLE 7 /* Johnson-Cook without thermal softening */
 #define MPM_MODEL_THERMAL_J2 10
+#define MPM_MODEL_COHESIVE_DP 8         /* cohesive Drucker-Prager: dilatancy, tension cutoff */
+#define MPM_MODEL_FOAM 9                /* Deshpande-Fleck foam: pressure-dependent yield, bisection return */
 #define MPM_MODEL_NORTON_CREEP 11       /* Arrhenius power-law creep, bisection return */
 
 /* element type of the floating-point arrays of mpm_particles */
@@ -108,12 +112,21 @@ typedef struct mpm_material {
    * rate exp(clamp(Q/R (1/(T_ref + off) - 1/(T + off)), -60, 60)) (q / stress)^n */
   double creep_rate, creep_Q, creep_n, creep_stress;
   double temperature_offset; /* off: 273.15 when temperatures are in deg C like the reference, 0 in K */
+  /* Snow, model 2 (src/three/constitutive.js:48,58-60): principal stretches clamped to
+   * [1 - yield_strain, 1 + 0.3 yield_strain], Jp = clamp(Jp det F / det F', 0.6, 20), moduli
+   * scaled by clamp(exp(10 (1 - Jp)), 0.25, 4). Sand, model 3 (constitutive.js:66-74): friction
+   * angle in degrees. The reference takes both per particle; here they are per material. */
+  double yield_strain, friction_deg;
+  /* Cohesive Drucker-Prager, model 8, and Deshpande-Fleck foam, model 9
+   * (src/three/pressure-plasticity.js:2,11-48): strengths in Pa (Cauchy, tension positive). */
+  double dp_cohesion, dp_slope, dp_dilatancy, dp_tension;
+  double df_alpha, df_plateau, df_gamma, df_densify, df_beta, df_eps_d;
 } mpm_material;
 
 /* Host particle arrays (structure of arrays, like Simulation3's Float64Arrays,
  * src/three/simulation.js:27-30; F and C are n x 9 row-major like MPM3.F, src/three/mpm.js:9).
  * Any pointer may be NULL: on upload NULL means the default (v = 0, F = I, C = 0, ep = 0,
- * T = 0, material 0, not pinned); on download NULL arrays are skipped. */
+ * T = 0, material 0, not pinned, Jp = 1, dilation = 0); on download NULL arrays are skipped. */
 typedef struct mpm_particles {
   int32_t dtype;         /* MPM_F64 or MPM_F32 for every floating-point array below */
   int32_t reserved;
@@ -127,6 +140,8 @@ typedef struct mpm_particles {
   void* C;               /* n x 9 */
   int32_t* material;     /* index into the materials set with mpm_set_material */
   uint8_t* pinned;       /* pinned particles scatter but are not moved (src/three/mpm.js:84,108) */
+  void* jp;              /* plastic volume ratio MPM3.Jp (models 2, 8, 9; 1 otherwise) */
+  void* dilation;        /* MPM3.dilation (model 3; 0 otherwise) */
 } mpm_particles;
 
 /* FP64 ledger, reduced on the device (src/simulation/mechanical-diagnostics.js:16-37 and
@@ -151,6 +166,10 @@ const char* mpm_last_error(const mpm_handle* h);
 int mpm_configure_domain(mpm_handle* h, const mpm_domain* domain);
 int mpm_grid_dims(const mpm_handle* h, int32_t dims[3], double origin[3]);
 int mpm_set_material(mpm_handle* h, int32_t index, const mpm_material* material);
+/* The checks mpm_set_material applies, on the host without a handle (like the reference's
+ * pressureParameters, src/three/pressure-plasticity.js:4-10): MPM_OK, MPM_ERR_INVALID_ARG or
+ * MPM_ERR_UNSUPPORTED. */
+int mpm_validate_material(const mpm_material* material);
 int mpm_get_stream(mpm_handle* h, void** cuda_stream);
 
 /* ---- state (Simulation3 arrays + MPM3.F/C/plastic) ---- */
@@ -245,7 +264,8 @@ typedef struct mpm_frame_info {
 int mpm_pack_frame(mpm_handle* h, int64_t preview_limit, float* data, int64_t max_rows, mpm_frame_info* info);
 
 /* ---- constitutive batch on the device (projectPlastic + stress, src/three/constitutive.js:52-106)
- * F_in/F_out n x 9, ep/T/dep n, tau n x 9 (Kirchhoff). Stateless; runs on the default stream. */
+ * F_in/F_out n x 9, ep/T/dep n, tau n x 9 (Kirchhoff). Stateless; runs on the default stream.
+ * Models 2, 3, 8 and 9 carry Jp / dilation between steps and return MPM_ERR_UNSUPPORTED here. */
 int mpm_return_map_batch(const mpm_material* material, int64_t n, const double* F_in,
                          const double* ep, const double* T, double dt, double* F_out,
                          double* dep, double* tau);
@@ -255,7 +275,7 @@ int mpm_return_map_batch(const mpm_material* material, int64_t n, const double* 
  * host that owns every device byte through its own pool and passes this library only buffers it
  * already holds, or code running where cudaMalloc is not allowed. Scatters caller-owned device
  * particle arrays onto the domain's grid (stress from F without a return, like the first P2G of an
- * uploaded state) and writes, for every node in ((z*ny)+y)*nx+x order, the mass (nx*ny*nz doubles)
+ * uploaded state: Jp = 1 for snow) and writes, for every node in ((z*ny)+y)*nx+x order, the mass (nx*ny*nz doubles)
  * and the momentum including dt * (stress force + m g) (3*nx*ny*nz doubles): the values
  * mpm_grid_debug returns for the same state. Device pointers: x (n x 3) and F (n x 9 row-major)
  * double; v (n x 3), C (n x 9), m and V float.

@@ -32,8 +32,9 @@
 extern "C" {
 
 // Material parameters. model follows src/three/constitutive.js:6-19:
-// 0 fixed-corotated, 1 Neo-Hookean, 4 ideal J2, 5 linear-hardening J2,
-// 6 Johnson-Cook, 7 simplified Johnson-Cook, 10 thermal J2, 11 Norton creep.
+// 0 fixed-corotated, 1 Neo-Hookean, 2 snow, 3 sand, 4 ideal J2, 5 linear-hardening J2,
+// 6 Johnson-Cook, 7 simplified Johnson-Cook, 8 cohesive Drucker-Prager, 9 Deshpande-Fleck foam,
+// 10 thermal J2, 11 Norton creep.
 struct OracleMaterial {
   int32_t model;
   int32_t pad;
@@ -44,6 +45,11 @@ struct OracleMaterial {
   double tTref, tThot, tHotRatio, tA, tH, tRate, tQ, tN, tStress;
   // plastic heating: heat fraction beta and specific heat cp (gpu/mixed_material.py:150-172)
   double beta, cp;
+  // snow yield strain and sand friction angle in degrees (per particle in the reference,
+  // src/three/simulation.js:40; defaults .025 and 35)
+  double yieldStrain, friction;
+  // pressure models (src/three/pressure-plasticity.js:2): strengths in the stress unit of mu
+  double cohesion, slope, dilatancy, tension, alpha, plateau, gamma, densify, pbeta, epsD;
 };
 
 struct OracleScene {
@@ -327,29 +333,149 @@ void oracle_thermal_return(const double* sigma, int model, double ep, double dt,
   *increment = inc;
 }
 
-// constitutive.js:52-78 (projectPlastic) for the in-scope models 4-7, 10, 11; models 0, 1 return F
-// unchanged. Outputs the projected F, the plastic increment, and the cached Kirchhoff stress of
-// constitutive.js:81-86 (principalStress with mu, lambda). Returns -1 for models out of scope.
-int oracle_project(const double* F, const OracleMaterial* p, double ep, double dt, double T,
-                   double* Fout, double* increment, double* tau_cache) {
+// constitutive.js:48
+double oracle_hardening(double jp) { return std::max(0.25, std::min(4.0, std::exp(10 * (1 - jp)))); }
+
+// pressure-plasticity.js:11-14. Fully densified foam (ep >= epsD) has strength 1e30 here (1e20 in
+// the reference's E units): both stand for "cannot yield".
+double oracle_foam_strength(double ep, const OracleMaterial* p) {
+  const double r = ep / p->epsD;
+  return r >= 1 ? 1e30
+                : p->plateau + p->gamma * r - p->densify * std::log(std::max(1e-30, 1 - std::pow(r, p->pbeta)));
+}
+
+// pressure-plasticity.js:15-48 (models 8 and 9). The reference's G = 0.4 / J and K = (2/3) / J
+// are mu / J and (lambda + 2 mu / 3) / J at mu = lambda = 0.4.
+void oracle_pressure_return(const double* sigma, int model, double jp, double ep, const OracleMaterial* p,
+                            double* out, double* jp_out, double* increment) {
+  double e[3], dev[3];
+  for (int k = 0; k < 3; ++k) e[k] = std::log(std::max(sigma[k], 1e-6));
+  const double trace = e[0] + e[1] + e[2];
+  for (int k = 0; k < 3; ++k) dev[k] = e[k] - trace / 3;
+  const double length = std::sqrt(dev[0] * dev[0] + dev[1] * dev[1] + dev[2] * dev[2]);
+  const double J = std::max(1e-6, std::exp(trace) * jp), G = p->mu / J, K = (p->lambda + 2 * p->mu / 3) / J;
+  const double mean = K * trace, q = std::sqrt(6.0) * G * length;
+  double meanNew = mean, qNew = q, inc = 0;
+  if (model == 8) {
+    const double t = q / std::sqrt(3.0), c = p->cohesion, a = p->slope, b = p->dilatancy, T = p->tension;
+    if (mean > T && t + a * T <= c) {
+      meanNew = T;
+    } else if (t + a * mean > c) {
+      const double dl = (t + a * mean - c) / (G + a * K * b);
+      meanNew = mean - K * b * dl;
+      qNew = std::sqrt(3.0) * std::max(0.0, t - G * dl);
+      if (meanNew > T) {
+        meanNew = T;
+        qNew = std::sqrt(3.0) * std::max(0.0, c - a * T);
+      }
+    }
+  } else {
+    const double a2 = p->alpha * p->alpha, B = 1 + a2 / 9, trial = std::sqrt((q * q + a2 * mean * mean) / B);
+    if (trial > oracle_foam_strength(ep, p)) {
+      auto state = [&](double eta, double& qn, double& mn, double& dl) {
+        qn = q / (1 + 3 * G * eta);
+        mn = mean / (1 + K * a2 * eta);
+        const double hat = std::sqrt((qn * qn + a2 * mn * mn) / B);
+        dl = eta * B * hat;
+        return hat - oracle_foam_strength(ep + dl, p);
+      };
+      double qn, mn, dl, lo = 0, hi = 1 / G;
+      for (int k = 0; k < 32 && state(hi, qn, mn, dl) > 0; ++k) hi *= 2;
+      for (int k = 0; k < 28; ++k) {
+        const double mid = (lo + hi) / 2;
+        if (state(mid, qn, mn, dl) > 0) lo = mid;
+        else hi = mid;
+      }
+      state((lo + hi) / 2, qn, mn, dl);
+      qNew = qn;
+      meanNew = mn;
+      inc = dl;
+    }
+  }
+  const double traceNew = meanNew / K, scale = q > 1e-20 ? qNew / q : 1;
+  double newE[3];
+  for (int k = 0; k < 3; ++k) newE[k] = traceNew / 3 + scale * dev[k];
+  if (model == 8) {
+    double d2 = 0;
+    for (int k = 0; k < 3; ++k) d2 += (e[k] - newE[k]) * (e[k] - newE[k]);
+    inc = std::sqrt(2.0 / 3.0) * std::sqrt(d2);
+  }
+  for (int k = 0; k < 3; ++k) out[k] = std::exp(newE[k]);
+  *jp_out = jp * std::exp(trace - traceNew);
+  *increment = inc;
+}
+
+// constitutive.js:52-78 (projectPlastic); models 0, 1 return F unchanged. jp and dilation are
+// MPM3.Jp and MPM3.dilation, read and updated (either may be null: 1 and 0, not returned).
+// Outputs the projected F, the plastic increment (metal, thermal and pressure returns give their
+// own; snow and sand |log(s / s')|), and the cached Kirchhoff stress of constitutive.js:81-86
+// (principalStress with mu, lambda: snow's fixed-corotated form, Hencky for the others).
+int oracle_project(const double* F, const OracleMaterial* p, double ep, double dt, double T, double* jp,
+                   double* dilation, double* Fout, double* increment, double* tau_cache) {
   const int model = p->model;
+  if (model < 0 || model > 11) return -1;
   if (model < 2) {
     std::memcpy(Fout, F, 9 * sizeof(double));
     *increment = 0;
     oracle_constitutive_stress(F, model, p->mu, p->lambda, tau_cache);
     return 0;
   }
-  double u[9], v[9], s[3], proj[3], inc = 0;
+  double jpv = jp ? *jp : 1.0, dil = dilation ? *dilation : 0.0;
+  double u[9], v[9], s[3], proj[3], inc = -1;
   oracle_svd3(F, u, v, s);
-  if (model >= 10 && model <= 11)
+  if (model == 2) {
+    double ds = 1, dp = 1;
+    for (int k = 0; k < 3; ++k) {
+      proj[k] = std::max(1 - p->yieldStrain, std::min(1 + p->yieldStrain * .3, s[k]));
+      ds *= s[k];
+      dp *= proj[k];
+    }
+    jpv = std::max(.6, std::min(20.0, jpv * ds / dp));
+  } else if (model >= 10) {
     oracle_thermal_return(s, model, ep, dt, T, p, proj, &inc);
-  else if (model >= 4 && model <= 7)
+  } else if (model >= 8) {
+    oracle_pressure_return(s, model, jpv, ep, p, proj, &jpv, &inc);
+  } else if (model >= 4) {
     oracle_metal_return(s, model, ep, dt, T, p, proj, &inc);
-  else
-    return -1;
+  } else {  // sand
+    double e[3];
+    for (int k = 0; k < 3; ++k) e[k] = std::log(std::max(s[k], 1e-6));
+    const double trace = e[0] + e[1] + e[2] + dil;
+    if (trace >= 0) {
+      proj[0] = proj[1] = proj[2] = 1;
+      dil = trace;
+    } else {
+      dil = 0;
+      double dev[3];
+      for (int k = 0; k < 3; ++k) dev[k] = e[k] - trace / 3;
+      const double length = std::sqrt(dev[0] * dev[0] + dev[1] * dev[1] + dev[2] * dev[2]);
+      const double sn = std::sin(p->friction * 3.14159265358979323846 / 180), alpha = std::sqrt(2.0 / 3) * 2 * sn / (3 - sn);
+      // the reference's 2.5 = (3 lambda + 2 mu) / (2 mu) at lambda = mu
+      const double delta = std::max(0.0, length + (3 * p->lambda + 2 * p->mu) / (2 * p->mu) * trace * alpha);
+      for (int k = 0; k < 3; ++k) proj[k] = std::exp(e[k] - delta / (length > 0 ? length : 1) * dev[k]);
+    }
+  }
+  if (inc < 0) {  // snow and sand: |log(s / s')|
+    double d2 = 0;
+    for (int k = 0; k < 3; ++k) d2 += std::log(s[k] / proj[k]) * std::log(s[k] / proj[k]);
+    inc = std::sqrt(d2);
+  }
   oracle_compose(u, v, proj, Fout);
   *increment = inc;
-  oracle_principal_stress(u, proj, p->mu, p->lambda, tau_cache);
+  if (jp) *jp = jpv;
+  if (dilation) *dilation = dil;
+  if (model == 2) {  // principalStress of snow: 2 mu (s - 1) s + lambda (J - 1) J
+    const double Jp = proj[0] * proj[1] * proj[2];
+    for (int a = 0; a < 3; ++a)
+      for (int b = 0; b < 3; ++b) {
+        double t = 0;
+        for (int k = 0; k < 3; ++k)
+          t += u[a * 3 + k] * (2 * p->mu * (proj[k] - 1) * proj[k] + p->lambda * (Jp - 1) * Jp) * u[b * 3 + k];
+        tau_cache[a * 3 + b] = t;
+      }
+  } else {
+    oracle_principal_stress(u, proj, p->mu, p->lambda, tau_cache);
+  }
   return 0;
 }
 
@@ -385,7 +511,7 @@ static inline void stencil(const OracleScene* sc, const double* x, Stencil& st) 
 }
 
 int oracle_step(const OracleScene* sc, const OracleMaterial* mats, int32_t nmat, int64_t n,
-                double* x, double* v, double* C, double* F, double* ep, double* T,
+                double* x, double* v, double* C, double* F, double* ep, double* T, double* jp, double* dilation,
                 const double* m, const double* V, const int32_t* mat, const uint8_t* pinned,
                 double* tau_cache, uint8_t* cache_valid, double dt, double* grid_mass,
                 double* grid_mom, double* grid_vel, int32_t threads) {
@@ -420,6 +546,10 @@ int oracle_step(const OracleScene* sc, const OracleMaterial* mats, int32_t nmat,
       std::memcpy(&tau[p * 9], &tau_cache[p * 9], 9 * sizeof(double));
     else
       oracle_constitutive_stress(&F[p * 9], mp->model, mp->mu, mp->lambda, &tau[p * 9]);
+    if (mp->model == 2) {  // snow's compaction hardening scales the stress (mpm.js:35-37)
+      const double h = oracle_hardening(jp ? jp[p] : 1.0);
+      for (int k = 0; k < 9; ++k) tau[p * 9 + k] *= h;
+    }
   }
   // P2G (mpm.js:66-85). With threads == 1 it is serial, so the summation order is the
   // particle order; with more threads the scatter uses atomic adds (CPU baseline timing).
@@ -577,7 +707,8 @@ int oracle_step(const OracleScene* sc, const OracleMaterial* mats, int32_t nmat,
     const OracleMaterial* mp = &mats[mat[p]];
     if (mp->model >= 2) {
       double Fn[9], inc = 0, tc[9];
-      if (oracle_project(&F[p * 9], mp, ep[p], dt, T[p], Fn, &inc, tc) != 0) {
+      if (oracle_project(&F[p * 9], mp, ep[p], dt, T[p], jp ? &jp[p] : nullptr, dilation ? &dilation[p] : nullptr, Fn,
+                         &inc, tc) != 0) {
         status = -2;
         continue;
       }
@@ -587,7 +718,7 @@ int oracle_step(const OracleScene* sc, const OracleMaterial* mats, int32_t nmat,
       if (cache_valid) cache_valid[p] = 1;
       // plastic-work heating: dT = beta * tau_eq(returned) * dep / (rho0 * cp), tau_eq the
       // Kirchhoff von Mises stress sqrt(6) mu |dev e_returned| (gpu/mixed_material.py:150-172)
-      if (mp->beta > 0 && inc > 0) {
+      if (mp->beta > 0 && inc > 0 && ((mp->model >= 4 && mp->model <= 7) || mp->model >= 10)) {
         double u[9], vv[9], s[3], e[3];
         oracle_svd3(&F[p * 9], u, vv, s);
         for (int k = 0; k < 3; ++k) e[k] = std::log(std::max(s[k], 1e-6));
@@ -606,7 +737,7 @@ int oracle_step(const OracleScene* sc, const OracleMaterial* mats, int32_t nmat,
 // (reference units: sqrt(19200 stiffness) since lambda + 2mu = 1.2 E = 1.2*16000*stiffness*rho)
 double oracle_stable_dt(const OracleScene* sc, const OracleMaterial* mats, int64_t n,
                         const double* v, const double* C, const double* F, const double* m,
-                        const double* V, const int32_t* mat) {
+                        const double* V, const int32_t* mat, const double* jp) {
   double maxw = 1, grad = 1;
   for (int64_t p = 0; p < n; ++p) {
     double row = 0, col = 0, g = 0;
@@ -621,8 +752,12 @@ double oracle_stable_dt(const OracleScene* sc, const OracleMaterial* mats, int64
       col = std::max(col, c);
     }
     const OracleMaterial* mp = &mats[mat[p]];
-    const double compression = mp->model == 1 ? 1 / std::max(0.05, det3(&F[p * 9])) : 1;
-    const double c = std::sqrt((mp->lambda + 2 * mp->mu) * V[p] / m[p]);
+    const double jpp = jp ? jp[p] : 1.0;
+    const bool press = mp->model == 8 || mp->model == 9;
+    const double compression =
+        mp->model == 1 || press ? 1 / std::max(0.05, det3(&F[p * 9]) * (press ? jpp : 1.0)) : 1;
+    const double hard = mp->model == 2 ? oracle_hardening(jpp) : 1.0;
+    const double c = std::sqrt((mp->lambda + 2 * mp->mu) * hard * V[p] / m[p]);
     const double speed = std::sqrt(v[p * 3] * v[p * 3] + v[p * 3 + 1] * v[p * 3 + 1] + v[p * 3 + 2] * v[p * 3 + 2]);
     maxw = std::max(maxw, speed + c * std::max(1.0, std::max(row * col, compression)));
     grad = std::max(grad, g);
@@ -638,7 +773,7 @@ double oracle_stable_dt(const OracleScene* sc, const OracleMaterial* mats, int64
 // Hencky models (an extension; the reference reports them unsupported) mu|e|^2 + lambda/2 tr^2 e.
 void oracle_ledger(const OracleScene* sc, const OracleMaterial* mats, int64_t n, const double* x,
                    const double* v, const double* C, const double* F, const double* ep,
-                   const double* m, const double* V, const int32_t* mat, OracleLedger* out) {
+                   const double* m, const double* V, const int32_t* mat, const double* jp, OracleLedger* out) {
   OracleLedger L{};
   L.min_j = INFINITY;
   L.max_j = -INFINITY;
@@ -679,12 +814,13 @@ void oracle_ledger(const OracleScene* sc, const OracleMaterial* mats, int64_t n,
     double W = 0;
     if (!(J > 0)) {
       L.unsupported_elastic++;
-    } else if (mt->model == 0) {
+    } else if (mt->model == 0 || mt->model == 2) {  // snow with its hardened moduli
       double R[9];
       oracle_rotation(Fp, R);
       double s = 0;
       for (int k = 0; k < 9; ++k) s += (Fp[k] - R[k]) * (Fp[k] - R[k]);
-      W = mt->mu * s + 0.5 * mt->lambda * (J - 1) * (J - 1);
+      W = (mt->model == 2 ? oracle_hardening(jp ? jp[p] : 1.0) : 1.0) *
+          (mt->mu * s + 0.5 * mt->lambda * (J - 1) * (J - 1));
     } else if (mt->model == 1) {
       double s = 0;
       for (int k = 0; k < 9; ++k) s += Fp[k] * Fp[k];
@@ -700,8 +836,12 @@ void oracle_ledger(const OracleScene* sc, const OracleMaterial* mats, int64_t n,
     L.elastic += V[p] * W;
     if (ep) L.max_plastic = std::max(L.max_plastic, ep[p]);
     double tau[9];
-    oracle_constitutive_stress(Fp, mt->model == 0 || mt->model == 1 ? mt->model : 4, mt->mu, mt->lambda, tau);
-    L.max_von_mises = std::max(L.max_von_mises, oracle_von_mises(tau, J));
+    oracle_constitutive_stress(Fp, mt->model <= 2 ? mt->model : 4, mt->mu, mt->lambda, tau);
+    const double jpp = jp ? jp[p] : 1.0;
+    if (mt->model == 2)
+      for (int k = 0; k < 9; ++k) tau[k] *= oracle_hardening(jpp);
+    // Cauchy von Mises over the total volume ratio J Jp for the pressure models (mpm.js:38)
+    L.max_von_mises = std::max(L.max_von_mises, oracle_von_mises(tau, J * (mt->model == 8 || mt->model == 9 ? jpp : 1.0)));
   }
   *out = L;
 }

@@ -3,8 +3,8 @@
 Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg import this module, and
 only as the checker: the product path (mpm_b200) never calls into it.
 The C sources restate src/three/mpm.js:25-134, src/three/constitutive.js:22-106,
-src/three/metal-plasticity.js:12-38, src/three/thermal-plasticity.js:12-40 and
-src/three/math.js:9-32 of the reference.
+src/three/metal-plasticity.js:12-38, src/three/thermal-plasticity.js:12-40,
+src/three/pressure-plasticity.js:11-48 and src/three/math.js:9-32 of the reference.
 """
 import ctypes
 import os
@@ -24,7 +24,9 @@ class OracleMaterial(ctypes.Structure):
                 ("Tm", _D), ("m", _D),
                 ("tTref", _D), ("tThot", _D), ("tHotRatio", _D), ("tA", _D), ("tH", _D),
                 ("tRate", _D), ("tQ", _D), ("tN", _D), ("tStress", _D),
-                ("beta", _D), ("cp", _D)]
+                ("beta", _D), ("cp", _D), ("yieldStrain", _D), ("friction", _D),
+                ("cohesion", _D), ("slope", _D), ("dilatancy", _D), ("tension", _D), ("alpha", _D),
+                ("plateau", _D), ("gamma", _D), ("densify", _D), ("pbeta", _D), ("epsD", _D)]
 
 
 class OracleScene(ctypes.Structure):
@@ -48,6 +50,9 @@ class OracleLedger(ctypes.Structure):
 PLASTICITY_DEFAULTS = dict(A=.025, B=.08, n=.35, C=.025, rate0=1, Tref=20, Tm=1000, m=1)
 THERMAL_DEFAULTS = dict(Tref=20, Thot=180, hotRatio=.08, A=.04, H=.04, rate=.0005, Q=35000, n=3,
                         stress=.04)
+# src/three/pressure-plasticity.js:2 (strengths / E)
+PRESSURE_DEFAULTS = dict(cohesion=.025, slope=.6, dilatancy=.15, tension=.01, alpha=1.5, plateau=.015, gamma=.01,
+                         densify=.02, beta=2, epsD=.7)
 
 _lib = None
 
@@ -74,17 +79,21 @@ def lib():
         L.oracle_creep_log_rate.restype = _D
         L.oracle_metal_return.argtypes = [_P, ctypes.c_int, _D, _D, _D, P(OracleMaterial), _P, _P]
         L.oracle_thermal_return.argtypes = [_P, ctypes.c_int, _D, _D, _D, P(OracleMaterial), _P, _P]
-        L.oracle_project.argtypes = [_P, P(OracleMaterial), _D, _D, _D, _P, _P, _P]
+        L.oracle_project.argtypes = [_P, P(OracleMaterial), _D, _D, _D, _P, _P, _P, _P, _P]
         L.oracle_project.restype = ctypes.c_int
+        L.oracle_hardening.argtypes = [_D]
+        L.oracle_hardening.restype = _D
+        L.oracle_foam_strength.argtypes = [_D, P(OracleMaterial)]
+        L.oracle_foam_strength.restype = _D
         L.oracle_step.argtypes = [P(OracleScene), P(OracleMaterial), ctypes.c_int32, ctypes.c_int64,
-                                  _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _D, _P, _P, _P,
+                                  _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _D, _P, _P, _P,
                                   ctypes.c_int32]
         L.oracle_step.restype = ctypes.c_int
         L.oracle_stable_dt.argtypes = [P(OracleScene), P(OracleMaterial), ctypes.c_int64,
-                                       _P, _P, _P, _P, _P, _P]
+                                       _P, _P, _P, _P, _P, _P, _P]
         L.oracle_stable_dt.restype = _D
         L.oracle_ledger.argtypes = [P(OracleScene), P(OracleMaterial), ctypes.c_int64, _P, _P, _P,
-                                    _P, _P, _P, _P, _P, P(OracleLedger)]
+                                    _P, _P, _P, _P, _P, _P, P(OracleLedger)]
         _lib = L
     return _lib
 
@@ -98,15 +107,28 @@ def _f64(a, shape=None):
     return a.reshape(shape) if shape is not None else a
 
 
-def material(model, mu=.4, lam=.4, plasticity=None, thermal=None, beta=0.0, cp=1.0):
+def material(model, mu=.4, lam=.4, plasticity=None, thermal=None, beta=0.0, cp=1.0, yield_strain=.025,
+             friction=35.0, pressure=None):
     """Oracle material. Defaults are the reference's units: mu = lambda = 0.4 (E = 1)."""
     p = dict(PLASTICITY_DEFAULTS, **(plasticity or {}))
     t = dict(THERMAL_DEFAULTS, **(thermal or {}))
+    q = dict(PRESSURE_DEFAULTS, **(pressure or {}))
     return OracleMaterial(model=model, mu=mu, lam=lam, A=p["A"], B=p["B"], n=p["n"], C=p["C"],
                           rate0=p["rate0"], Tref=p["Tref"], Tm=p["Tm"], m=p["m"],
                           tTref=t["Tref"], tThot=t["Thot"], tHotRatio=t["hotRatio"], tA=t["A"],
                           tH=t["H"], tRate=t["rate"], tQ=t["Q"], tN=t["n"], tStress=t["stress"],
-                          beta=beta, cp=cp)
+                          beta=beta, cp=cp, yieldStrain=yield_strain, friction=friction,
+                          cohesion=q["cohesion"], slope=q["slope"], dilatancy=q["dilatancy"], tension=q["tension"],
+                          alpha=q["alpha"], plateau=q["plateau"], gamma=q["gamma"], densify=q["densify"],
+                          pbeta=q["beta"], epsD=q["epsD"])
+
+
+def hardening(jp):
+    return lib().oracle_hardening(jp)
+
+
+def foam_strength(ep, mat):
+    return lib().oracle_foam_strength(ep, ctypes.byref(mat))
 
 
 def svd3(F):
@@ -172,11 +194,19 @@ def thermal_return(sigma, model, ep, dt, T, mat):
 
 def project(F, mat, ep=0.0, dt=.01, T=20.0):
     """projectPlastic (constitutive.js:52-78): returns (F_out, increment, cached tau)."""
+    r = project_state(F, mat, ep=ep, dt=dt, T=T)
+    return r["F"], r["increment"], r["tau"]
+
+
+def project_state(F, mat, jp=1.0, dilation=0.0, ep=0.0, dt=.01, T=20.0):
+    """projectPlastic with the history scalars: dict(F, jp, dilation, increment, tau)."""
     Fo, inc, tau = np.zeros(9), np.zeros(1), np.zeros(9)
-    rc = lib().oracle_project(_ptr(_f64(F, (9,))), ctypes.byref(mat), ep, dt, T, _ptr(Fo), _ptr(inc), _ptr(tau))
+    j, d = np.array([float(jp)]), np.array([float(dilation)])
+    rc = lib().oracle_project(_ptr(_f64(F, (9,))), ctypes.byref(mat), ep, dt, T, _ptr(j), _ptr(d), _ptr(Fo),
+                              _ptr(inc), _ptr(tau))
     if rc != 0:
         raise ValueError("model out of scope")
-    return Fo, float(inc[0]), tau
+    return dict(F=Fo, jp=float(j[0]), dilation=float(d[0]), increment=float(inc[0]), tau=tau)
 
 
 def scene_struct(domain):
@@ -217,6 +247,8 @@ class OracleState:
         self.F = _f64(scene.F, (n, 9)).copy() if scene.F is not None else np.tile(np.eye(3).ravel(), (n, 1))
         self.ep = _f64(scene.ep).copy() if scene.ep is not None else np.zeros(n)
         self.T = _f64(scene.T).copy() if scene.T is not None else np.zeros(n)
+        self.jp = _f64(scene.jp).copy() if getattr(scene, "jp", None) is not None else np.ones(n)
+        self.dilation = _f64(scene.dilation).copy() if getattr(scene, "dilation", None) is not None else np.zeros(n)
         self.m = _f64(scene.m).copy()
         self.V = _f64(scene.V).copy()
         self.mat = np.ascontiguousarray(np.asarray(scene.mat, dtype=np.int32))
@@ -231,7 +263,8 @@ class OracleState:
         gv = np.zeros((nodes, 3)) if want_grid else None
         rc = lib().oracle_step(ctypes.byref(self.sc), self.mats, self.nmat, self.n,
                                _ptr(self.x), _ptr(self.v), _ptr(self.C), _ptr(self.F), _ptr(self.ep),
-                               _ptr(self.T), _ptr(self.m), _ptr(self.V), _ptr(self.mat),
+                               _ptr(self.T), _ptr(self.jp), _ptr(self.dilation), _ptr(self.m), _ptr(self.V),
+                               _ptr(self.mat),
                                _ptr(self.pinned), _ptr(self.tau_cache), _ptr(self.cache_valid), dt,
                                _ptr(gm), _ptr(gp), _ptr(gv), threads)
         if rc != 0:
@@ -245,13 +278,13 @@ class OracleState:
     def stable_dt(self):
         return lib().oracle_stable_dt(ctypes.byref(self.sc), self.mats, self.n, _ptr(self.v),
                                       _ptr(self.C), _ptr(self.F), _ptr(self.m), _ptr(self.V),
-                                      _ptr(self.mat))
+                                      _ptr(self.mat), _ptr(self.jp))
 
     def ledger(self):
         L = OracleLedger()
         lib().oracle_ledger(ctypes.byref(self.sc), self.mats, self.n, _ptr(self.x), _ptr(self.v),
                             _ptr(self.C), _ptr(self.F), _ptr(self.ep), _ptr(self.m), _ptr(self.V),
-                            _ptr(self.mat), ctypes.byref(L))
+                            _ptr(self.mat), _ptr(self.jp), ctypes.byref(L))
         return L
 
 
@@ -274,6 +307,14 @@ def material_from(mat):
                                      A=mat.yield_stress, H=mat.hardening, rate=mat.creep_rate, Q=mat.creep_Q,
                                      n=mat.creep_n, stress=mat.creep_stress),
                         beta=mat.heat_fraction, cp=mat.specific_heat)
+    if mat.model in (2, 3):
+        return material(mat.model, mu=mat.mu, lam=mat.lam, yield_strain=mat.yield_strain, friction=mat.friction_deg)
+    if mat.model in (8, 9):
+        return material(mat.model, mu=mat.mu, lam=mat.lam,
+                        pressure=dict(cohesion=mat.dp_cohesion, slope=mat.dp_slope, dilatancy=mat.dp_dilatancy,
+                                      tension=mat.dp_tension, alpha=mat.df_alpha, plateau=mat.df_plateau,
+                                      gamma=mat.df_gamma, densify=mat.df_densify, beta=mat.df_beta,
+                                      epsD=mat.df_eps_d))
     return material(mat.model, mu=mat.mu, lam=mat.lam)
 
 

@@ -23,7 +23,7 @@ namespace {
 
 constexpr int kMaxMats = 256;
 constexpr uint32_t kCheckpointMagic = 0x3242504du;  // "MPB2"
-constexpr uint32_t kCheckpointVersion = 2;  // 2: home-slot id array saved
+constexpr uint32_t kCheckpointVersion = 3;  // 2: home-slot id array saved; 3: aux (Jp / dilation) saved
 
 size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
@@ -70,6 +70,7 @@ struct mpm_handle {
   int64_t launches_per_graph = 0;
   std::vector<mpm_material> mats_host;
   std::vector<MaterialDev> mats_dev;
+  std::vector<mpm::MaterialExt> mats_ext;
   std::vector<char> mat_set;
   int64_t cap = 0;
   int64_t n = 0;
@@ -239,6 +240,7 @@ static size_t carve_particles(char* base, int64_t cap, mpm::Particles& p) {
   }
   p.m = c.take<float>(cap); p.V = c.take<float>(cap);
   p.ep = c.take<float>(cap); p.T = c.take<float>(cap);
+  p.aux = c.take<float>(cap);
   p.mat = c.take<unsigned short>(cap);
   p.pinned = c.take<unsigned char>(cap);
   p.id = c.take<unsigned>(cap);
@@ -307,6 +309,7 @@ static int alloc_grid(mpm_handle* h) {
     c.time_scene = cv.take<double>(ns);
     *scenes = cv.take<SceneDev>(ns);
     *mats = cv.take<MaterialDev>(kMaxMats);
+    c.mats_ext = cv.take<mpm::MaterialExt>(kMaxMats);
     *tmaps = cv.take<char>(128 * (size_t)ns);
     return align_up(cv.off, 256);
   };
@@ -331,6 +334,8 @@ static int alloc_grid(mpm_handle* h) {
   MPM_CUDA(h, cudaMemcpyAsync(scenes, h->scenes.data(), sizeof(SceneDev) * ns, cudaMemcpyHostToDevice, h->stream));
   MPM_CUDA(h, cudaMemcpyAsync(mats, h->mats_dev.data(), sizeof(MaterialDev) * kMaxMats, cudaMemcpyHostToDevice,
                               h->stream));
+  MPM_CUDA(h, cudaMemcpyAsync(const_cast<mpm::MaterialExt*>(c.mats_ext), h->mats_ext.data(),
+                              sizeof(mpm::MaterialExt) * kMaxMats, cudaMemcpyHostToDevice, h->stream));
   // TMA descriptor of each scene's velocity grid: 4D {channel 4, x, y, z}, box {4, 6, 6, 6}, fp32.
   // A scene's grid starts at a float4 node (16-byte aligned) and its strides are multiples of 16 B.
   c.tmaps = nullptr;
@@ -365,14 +370,16 @@ static int alloc_grid(mpm_handle* h) {
 }
 
 static void refresh_flags(mpm_handle* h) {
-  bool plastic = false, thermal = false;
+  bool plastic = false, thermal = false, aux = false;
   for (size_t i = 0; i < h->mats_host.size(); ++i) {
     if (!h->mat_set[i]) continue;
     const int m = h->mats_host[i].model;
-    if (m >= 4) plastic = true;
+    if (m >= 2) plastic = true;
     if (m == 10) thermal = true;
+    if (mpm::aux_model(m)) aux = true;
   }
   h->ctx.has_plastic = plastic ? 1 : 0;
+  h->ctx.has_aux = aux ? 1 : 0;
   h->ctx.has_thermal = thermal || h->ctx.has_thermal ? 1 : 0;
 }
 
@@ -458,10 +465,31 @@ static MaterialDev to_device(const mpm_material& m) {
   return d;
 }
 
+static mpm::MaterialExt to_device_ext(const mpm_material& m) {
+  mpm::MaterialExt d{};
+  d.snow_lo = static_cast<float>(-m.yield_strain);
+  d.snow_hi = static_cast<float>(0.3 * m.yield_strain);
+  const double sn = std::sin(m.friction_deg * 3.14159265358979323846 / 180.0);
+  d.sand_k = static_cast<float>(std::sqrt(2.0 / 3.0) * 2 * sn / (3 - sn) * (3 * m.lambda + 2 * m.mu) / (2 * m.mu));
+  d.bulk = static_cast<float>(m.lambda + 2 * m.mu / 3);
+  d.dp_c = static_cast<float>(m.dp_cohesion);
+  d.dp_a = static_cast<float>(m.dp_slope);
+  d.dp_b = static_cast<float>(m.dp_dilatancy);
+  d.dp_T = static_cast<float>(m.dp_tension);
+  d.df_a2 = static_cast<float>(m.df_alpha * m.df_alpha);
+  d.df_B = static_cast<float>(1 + m.df_alpha * m.df_alpha / 9);
+  d.df_plateau = static_cast<float>(m.df_plateau);
+  d.df_gamma = static_cast<float>(m.df_gamma);
+  d.df_densify = static_cast<float>(m.df_densify);
+  d.df_beta = static_cast<float>(m.df_beta);
+  d.df_inv_epsd = m.df_eps_d > 0 ? static_cast<float>(1.0 / m.df_eps_d) : 0.f;
+  return d;
+}
+
 static int validate_material(const mpm_material* m, std::string& why) {
   if (!m) { why = "material is null"; return MPM_ERR_INVALID_ARG; }
-  if (m->model != 0 && m->model != 1 && (m->model < 4 || m->model > 7) && m->model != 10 && m->model != 11) {
-    why = "material model not built (supported: 0, 1, 4, 5, 6, 7, 10, 11)";
+  if (m->model < 0 || m->model > 11) {
+    why = "material model not built (supported: 0-11)";
     return MPM_ERR_UNSUPPORTED;
   }
   if (!(m->mu > 0) || !(3 * m->lambda + 2 * m->mu > 0) || !std::isfinite(m->mu) || !std::isfinite(m->lambda)) {
@@ -488,6 +516,28 @@ static int validate_material(const mpm_material* m, std::string& why) {
     why = "Norton creep needs rate >= 0, stress > 0 and an absolute reference temperature > 0";
     return MPM_ERR_INVALID_ARG;
   }
+  if (m->model == 2 && !(m->yield_strain > 0 && m->yield_strain < 1)) {
+    why = "snow needs 0 < yield_strain < 1";
+    return MPM_ERR_INVALID_ARG;
+  }
+  if (m->model == 3 && !(m->friction_deg > 0 && m->friction_deg < 90)) {
+    why = "sand needs a friction angle in (0, 90) degrees";
+    return MPM_ERR_INVALID_ARG;
+  }
+  // src/three/pressure-plasticity.js:2-10: the reference's limits on the dimensionless
+  // parameters, non-negative strengths, dilatancy <= slope and slope * tension <= cohesion
+  if (m->model == 8 && (!(m->dp_cohesion >= 0) || !(m->dp_slope >= 0 && m->dp_slope <= 2) ||
+                        !(m->dp_dilatancy >= 0 && m->dp_dilatancy <= m->dp_slope) || !(m->dp_tension >= 0) ||
+                        !(m->dp_slope * m->dp_tension <= m->dp_cohesion * (1 + 1e-12) + 1e-300))) {
+    why = "cohesive Drucker-Prager needs cohesion, tension >= 0, 0 <= dilatancy <= slope <= 2 and slope * tension <= cohesion";
+    return MPM_ERR_INVALID_ARG;
+  }
+  if (m->model == 9 && (!(m->df_alpha >= 0.05 && m->df_alpha <= std::sqrt(4.5)) || !(m->df_plateau > 0) ||
+                        !(m->df_gamma >= 0) || !(m->df_densify > 0) || !(m->df_beta >= 1 && m->df_beta <= 5) ||
+                        !(m->df_eps_d >= 0.05 && m->df_eps_d <= 3))) {
+    why = "Deshpande-Fleck foam needs alpha in [0.05, sqrt(4.5)], plateau, densify > 0, gamma >= 0, beta in [1, 5], eps_D in [0.05, 3]";
+    return MPM_ERR_INVALID_ARG;
+  }
   if (m->heat_fraction < 0 || m->heat_fraction > 1) {
     why = "heat_fraction must lie in [0, 1]";
     return MPM_ERR_INVALID_ARG;
@@ -498,6 +548,11 @@ static int validate_material(const mpm_material* m, std::string& why) {
 extern "C" {
 
 int mpm_abi_version(void) { return MPM_ABI_VERSION; }
+
+int mpm_validate_material(const mpm_material* material) {
+  std::string why;
+  return validate_material(material, why);
+}
 
 const char* mpm_error_string(int status) {
   switch (status) {
@@ -543,6 +598,7 @@ int mpm_create(const mpm_domain* domain, int64_t capacity, mpm_handle** out) {
   h->use_tma = std::getenv("MPM_B200_NO_TMA") ? 0 : 1;  // plain-load gather window when set
   h->mats_host.assign(kMaxMats, mpm_material{});
   h->mats_dev.assign(kMaxMats, MaterialDev{});
+  h->mats_ext.assign(kMaxMats, mpm::MaterialExt{});
   h->mat_set.assign(kMaxMats, 0);
   mpm::Particles p{};
   const size_t pbytes = carve_particles(nullptr, capacity, p);
@@ -640,9 +696,12 @@ int mpm_set_material(mpm_handle* h, int32_t index, const mpm_material* material)
   if (rc != MPM_OK) return fail(h, rc, why);
   h->mats_host[index] = *material;
   h->mats_dev[index] = to_device(*material);
+  h->mats_ext[index] = to_device_ext(*material);
   h->mat_set[index] = 1;
   MPM_CUDA(h, cudaMemcpyAsync(const_cast<MaterialDev*>(h->ctx.mats) + index, &h->mats_dev[index], sizeof(MaterialDev),
                               cudaMemcpyHostToDevice, h->stream));
+  MPM_CUDA(h, cudaMemcpyAsync(const_cast<mpm::MaterialExt*>(h->ctx.mats_ext) + index, &h->mats_ext[index],
+                              sizeof(mpm::MaterialExt), cudaMemcpyHostToDevice, h->stream));
   refresh_flags(h);
   h->grid_valid = false;  // stresses change
   return MPM_OK;
@@ -665,26 +724,31 @@ static int ensure_staging(mpm_handle* h, size_t bytes) {
 }
 
 // Copies the caller's host arrays into device staging; fills ptrs with device addresses (or null).
-static int stage_in(mpm_handle* h, int64_t n, const mpm_particles* p, void* ptrs[12], const int** mat_dev,
+// Staged arrays: 0-2 x, y, z; 3-5 v; 6 mass; 7 volume; 8 T; 9 plastic; 10 F; 11 C; 12 Jp; 13 dilation.
+constexpr int kStaged = 14;
+static inline int staged_comps(int k) { return k == 10 || k == 11 ? 9 : 1; }
+
+static int stage_in(mpm_handle* h, int64_t n, const mpm_particles* p, void* ptrs[kStaged], const int** mat_dev,
                     const unsigned char** pin_dev, unsigned fields) {
   const size_t es = p->dtype == MPM_F32 ? 4 : 8;
-  const void* src[12] = {p->x, p->y, p->z, p->vx, p->vy, p->vz, p->mass, p->volume, p->temperature, p->plastic, p->F, p->C};
-  const unsigned need[12] = {mpm::kFieldPos, mpm::kFieldPos, mpm::kFieldPos, mpm::kFieldVel, mpm::kFieldVel,
-                             mpm::kFieldVel, mpm::kFieldMass, mpm::kFieldVolume, mpm::kFieldTemp, mpm::kFieldPlastic,
-                             mpm::kFieldF, mpm::kFieldC};
+  const void* src[kStaged] = {p->x, p->y, p->z, p->vx, p->vy, p->vz, p->mass, p->volume, p->temperature, p->plastic,
+                              p->F, p->C, p->jp, p->dilation};
+  const unsigned need[kStaged] = {mpm::kFieldPos, mpm::kFieldPos, mpm::kFieldPos, mpm::kFieldVel, mpm::kFieldVel,
+                                  mpm::kFieldVel, mpm::kFieldMass, mpm::kFieldVolume, mpm::kFieldTemp,
+                                  mpm::kFieldPlastic, mpm::kFieldF, mpm::kFieldC, mpm::kFieldAux, mpm::kFieldAux};
   size_t total = 0;
-  for (int k = 0; k < 12; ++k)
-    if (src[k] && (fields & need[k])) total += align_up((k >= 10 ? 9 : 1) * n * es, 256);
+  for (int k = 0; k < kStaged; ++k)
+    if (src[k] && (fields & need[k])) total += align_up(staged_comps(k) * n * es, 256);
   if ((fields & mpm::kFieldMass) && p->material) total += align_up(n * 4, 256);
   if ((fields & mpm::kFieldMass) && p->pinned) total += align_up(n, 256);
   int rc = ensure_staging(h, std::max<size_t>(total, 256));
   if (rc != MPM_OK) return rc;
   char* base = static_cast<char*>(h->staging);
   size_t off = 0;
-  for (int k = 0; k < 12; ++k) {
+  for (int k = 0; k < kStaged; ++k) {
     ptrs[k] = nullptr;
     if (!src[k] || !(fields & need[k])) continue;
-    const size_t bytes = (k >= 10 ? 9 : 1) * n * es;
+    const size_t bytes = staged_comps(k) * n * es;
     ptrs[k] = base + off;
     MPM_CUDA(h, cudaMemcpyAsync(ptrs[k], src[k], bytes, cudaMemcpyHostToDevice, h->stream));
     off += align_up(bytes, 256);
@@ -701,7 +765,7 @@ static int stage_in(mpm_handle* h, int64_t n, const mpm_particles* p, void* ptrs
     MPM_CUDA(h, cudaMemcpyAsync(base + off, p->pinned, n, cudaMemcpyHostToDevice, h->stream));
     off += align_up(n, 256);
   }
-  MPM_CUDA(h, cudaMemcpyAsync(h->dptr_table, ptrs, 12 * sizeof(void*), cudaMemcpyHostToDevice, h->stream));
+  MPM_CUDA(h, cudaMemcpyAsync(h->dptr_table, ptrs, kStaged * sizeof(void*), cudaMemcpyHostToDevice, h->stream));
   return MPM_OK;
 }
 
@@ -746,10 +810,10 @@ int mpm_upload_particles(mpm_handle* h, int64_t n, const mpm_particles* p) {
   (void)es;
   MPM_CUDA(h, cudaStreamSynchronize(h->stream));
   drop_graph(h);  // a captured graph holds the old particle count
-  void* ptrs[12];
+  void* ptrs[kStaged];
   const int* mat_dev;
   const unsigned char* pin_dev;
-  const unsigned all = 0xffu;
+  const unsigned all = 0x1ffu;
   int rc = stage_in(h, n, p, ptrs, &mat_dev, &pin_dev, all);
   if (rc != MPM_OK) return rc;
   h->ctx.n = n;
@@ -805,6 +869,7 @@ static unsigned download_fields(const mpm_particles* p) {
   if (p->plastic) f |= mpm::kFieldPlastic;
   if (p->F) f |= mpm::kFieldF;
   if (p->C) f |= mpm::kFieldC;
+  if (p->jp || p->dilation) f |= mpm::kFieldAux;
   return f;
 }
 
@@ -815,26 +880,27 @@ int mpm_download_particles(mpm_handle* h, const mpm_particles* p) {
   if (n == 0) return MPM_OK;
   const size_t es = p->dtype == MPM_F32 ? 4 : 8;
   const unsigned fields = download_fields(p);
-  void* dst[12] = {p->x, p->y, p->z, p->vx, p->vy, p->vz, p->mass, p->volume, p->temperature, p->plastic, p->F, p->C};
+  void* dst[kStaged] = {p->x, p->y, p->z, p->vx, p->vy, p->vz, p->mass, p->volume, p->temperature, p->plastic,
+                        p->F, p->C, p->jp, p->dilation};
   size_t total = 0;
-  for (int k = 0; k < 12; ++k)
-    if (dst[k]) total += align_up((k >= 10 ? 9 : 1) * n * es, 256);
+  for (int k = 0; k < kStaged; ++k)
+    if (dst[k]) total += align_up(staged_comps(k) * n * es, 256);
   int rc = ensure_staging(h, std::max<size_t>(total, 256));
   if (rc != MPM_OK) return rc;
-  void* dev[12];
+  void* dev[kStaged];
   char* base = static_cast<char*>(h->staging);
   size_t off = 0;
-  for (int k = 0; k < 12; ++k) {
+  for (int k = 0; k < kStaged; ++k) {
     dev[k] = nullptr;
     if (!dst[k]) continue;
     dev[k] = base + off;
-    off += align_up((k >= 10 ? 9 : 1) * n * es, 256);
+    off += align_up(staged_comps(k) * n * es, 256);
   }
-  MPM_CUDA(h, cudaMemcpyAsync(h->dptr_table, dev, 12 * sizeof(void*), cudaMemcpyHostToDevice, h->stream));
+  MPM_CUDA(h, cudaMemcpyAsync(h->dptr_table, dev, kStaged * sizeof(void*), cudaMemcpyHostToDevice, h->stream));
   { ProfScope ps(h, -1); mpm::launch_download_convert(h->ctx, h->stream, n, p->dtype, reinterpret_cast<void* const*>(h->dptr_table), fields); }
   MPM_CUDA(h, cudaGetLastError());
-  for (int k = 0; k < 12; ++k)
-    if (dst[k]) MPM_CUDA(h, cudaMemcpyAsync(dst[k], dev[k], (k >= 10 ? 9 : 1) * n * es, cudaMemcpyDeviceToHost, h->stream));
+  for (int k = 0; k < kStaged; ++k)
+    if (dst[k]) MPM_CUDA(h, cudaMemcpyAsync(dst[k], dev[k], staged_comps(k) * n * es, cudaMemcpyDeviceToHost, h->stream));
   MPM_CUDA(h, cudaStreamSynchronize(h->stream));
   return MPM_OK;
 }
@@ -851,6 +917,7 @@ int mpm_reset_deformation(mpm_handle* h) {
   MPM_CUDA(h, cudaMemsetAsync(p.C, 0, sizeof(float) * 9 * p.cap, h->stream));
   MPM_CUDA(h, cudaMemsetAsync(p.D, 0, sizeof(float) * 9 * p.cap, h->stream));
   MPM_CUDA(h, cudaMemsetAsync(p.ep, 0, sizeof(float) * p.cap, h->stream));
+  MPM_CUDA(h, cudaMemsetAsync(p.aux, 0, sizeof(float) * p.cap, h->stream));  // Jp = 1, dilation = 0
   h->grid_valid = false;
   MPM_CUDA(h, cudaStreamSynchronize(h->stream));
   return MPM_OK;
@@ -963,7 +1030,7 @@ int mpm_step_host(mpm_handle* h, const mpm_particles* io, double dt) {
     return fail(h, MPM_ERR_INVALID_ARG, "positions and velocities are required");
   const int64_t n = h->n;
   if (n == 0) return MPM_OK;
-  void* ptrs[12];
+  void* ptrs[kStaged];
   const int* mat_dev;
   const unsigned char* pin_dev;
   const unsigned fields = mpm::kFieldPos | mpm::kFieldVel;
@@ -998,7 +1065,7 @@ int mpm_frame_host(mpm_handle* h, const mpm_particles* io, double dt_requested, 
     return fail(h, MPM_ERR_INVALID_ARG, "positions and velocities are required");
   const int64_t n = h->n;
   if (n == 0) return MPM_OK;
-  void* ptrs[12];
+  void* ptrs[kStaged];
   const int* mat_dev;
   const unsigned char* pin_dev;
   const unsigned fields = mpm::kFieldPos | mpm::kFieldVel;
@@ -1152,7 +1219,7 @@ struct CheckpointHeader {
   uint32_t magic, version;
   int64_t n;
   mpm_domain dom;
-  int32_t has_pinned, single_material, has_thermal, has_plastic, mat_base, reserved;
+  int32_t has_pinned, single_material, has_thermal, has_plastic, mat_base, has_aux;
 };
 
 // Raw device state of the n live particles, array by array, after a header with the domain and
@@ -1164,14 +1231,15 @@ int mpm_checkpoint_save(mpm_handle* h, const char* path) {
   FILE* f = std::fopen(path, "wb");
   if (!f) return fail(h, MPM_ERR_INVALID_ARG, std::string("cannot open ") + path);
   CheckpointHeader hd{kCheckpointMagic, kCheckpointVersion, h->n, h->dom, h->ctx.has_pinned, h->ctx.single_material,
-                      h->ctx.has_thermal, h->ctx.has_plastic, h->scene.mat_base, 0};
+                      h->ctx.has_thermal, h->ctx.has_plastic, h->scene.mat_base, h->ctx.has_aux};
   bool ok = std::fwrite(&hd, sizeof hd, 1, f) == 1;
   ok = ok && std::fwrite(h->mat_set.data(), 1, kMaxMats, f) == (size_t)kMaxMats;
   ok = ok && std::fwrite(h->mats_host.data(), sizeof(mpm_material), kMaxMats, f) == (size_t)kMaxMats;
   const mpm::Particles& p = h->ctx.p;
   struct Arr { const void* d; size_t es; int comps; } arrs[] = {
       {p.qx, 4, 1}, {p.qy, 4, 1}, {p.qz, 4, 1}, {p.vx, 4, 1}, {p.vy, 4, 1}, {p.vz, 4, 1}, {p.C, 4, 9}, {p.D, 4, 9},
-      {p.m, 4, 1}, {p.V, 4, 1}, {p.ep, 4, 1}, {p.T, 4, 1}, {p.mat, 2, 1}, {p.pinned, 1, 1}, {p.id, 4, 1}};
+      {p.m, 4, 1}, {p.V, 4, 1}, {p.ep, 4, 1}, {p.T, 4, 1}, {p.aux, 4, 1}, {p.mat, 2, 1}, {p.pinned, 1, 1},
+      {p.id, 4, 1}};
   std::vector<char> buf;
   cudaStreamSynchronize(h->stream);
   for (const Arr& a : arrs) {
@@ -1220,7 +1288,8 @@ int mpm_checkpoint_load(mpm_handle* h, const char* path) {
   const mpm::Particles& p = h->ctx.p;
   struct Arr { void* d; size_t es; int comps; } arrs[] = {
       {p.qx, 4, 1}, {p.qy, 4, 1}, {p.qz, 4, 1}, {p.vx, 4, 1}, {p.vy, 4, 1}, {p.vz, 4, 1}, {p.C, 4, 9}, {p.D, 4, 9},
-      {p.m, 4, 1}, {p.V, 4, 1}, {p.ep, 4, 1}, {p.T, 4, 1}, {p.mat, 2, 1}, {p.pinned, 1, 1}, {p.id, 4, 1}};
+      {p.m, 4, 1}, {p.V, 4, 1}, {p.ep, 4, 1}, {p.T, 4, 1}, {p.aux, 4, 1}, {p.mat, 2, 1}, {p.pinned, 1, 1},
+      {p.id, 4, 1}};
   std::vector<char> buf;
   cudaStreamSynchronize(h->stream);
   for (const Arr& a : arrs) {
@@ -1240,6 +1309,7 @@ int mpm_checkpoint_load(mpm_handle* h, const char* path) {
   h->ctx.single_material = hd.single_material;
   h->ctx.has_thermal = hd.has_thermal;
   h->ctx.has_plastic = hd.has_plastic;
+  h->ctx.has_aux = hd.has_aux;
   h->scene.mat_base = hd.mat_base;
   h->scene.p_begin = 0;
   h->scene.p_end = hd.n;
@@ -1261,6 +1331,7 @@ int mpm_host_free(void* p) { return cudaFreeHost(p) == cudaSuccess ? MPM_OK : MP
 
 int mpm_return_map_batch(const mpm_material* material, int64_t n, const double* F_in, const double* ep, const double* T,
                          double dt, double* F_out, double* dep, double* tau) {
+  if (material && mpm::aux_model(material->model)) return MPM_ERR_UNSUPPORTED;  // needs Jp / dilation in and out
   std::string why;
   int rc = validate_material(material, why);
   if (rc != MPM_OK) return rc;
@@ -1600,7 +1671,7 @@ int mpm_batch_ledger(mpm_handle* h, int32_t scene, mpm_ledger* out) {
     p.Cc[e] += pb;
     p.Dc[e] += pb;
   }
-  p.m += pb; p.V += pb; p.ep += pb; p.T += pb;
+  p.m += pb; p.V += pb; p.ep += pb; p.T += pb; p.aux += pb;
   p.mat += pb; p.pinned += pb; p.id += pb;
   c.n = sc.p_end - sc.p_begin;
   c.scenes = h->ctx.scenes + scene;

@@ -95,6 +95,7 @@ struct Particles {
   float* Cc[9];  // the same component arrays as separate pointers (32-bit indexing in kernels)
   float* Dc[9];
   float *m, *V, *ep, *T;
+  float* aux;       // Jp - 1 (snow, pressure models) or the dilation (sand); 0 for the other laws
   unsigned short* mat;
   unsigned char* pinned;
   unsigned* id;     // caller's index of the particle in this home slot
@@ -128,6 +129,7 @@ struct Ctx {
   SortBufs s;
   const SceneDev* scenes;
   const MaterialDev* mats;
+  const MaterialExt* mats_ext;  // the constants of snow, sand and the pressure laws, same rows
   Ctrl* ctrl;
   float* dt_scene;      // per scene
   unsigned* wave_max;   // per scene, float bits of max(|v| + c * stretch)
@@ -142,6 +144,7 @@ struct Ctx {
   int single_material;
   int has_thermal;      // temperature array is read and written
   int has_plastic;      // plastic strain array is read and written
+  int has_aux;          // aux array is read and written (a snow, sand or pressure material is set)
   int use_tma;
   int ws_blocks;        // > 0: the particle passes that scatter run warp-specialised on this many CTAs
   int conduct;          // a scene conducts heat on the grid: heat channel, conduction pass, dT gather
@@ -183,7 +186,8 @@ int p2g_blocks_per_sm();
 // field bits of the conversion kernels
 enum Field : unsigned {
   kFieldPos = 1u << 0, kFieldVel = 1u << 1, kFieldMass = 1u << 2, kFieldVolume = 1u << 3,
-  kFieldTemp = 1u << 4, kFieldPlastic = 1u << 5, kFieldF = 1u << 6, kFieldC = 1u << 7
+  kFieldTemp = 1u << 4, kFieldPlastic = 1u << 5, kFieldF = 1u << 6, kFieldC = 1u << 7,
+  kFieldAux = 1u << 8
 };
 
 }  // namespace mpm

@@ -154,8 +154,9 @@ struct StepOut {
 };
 
 // CFL terms of src/three/mpm.js:43-54 for one particle (F = I + D)
+template <bool AUX>
 __device__ __forceinline__ void cfl_terms(const MaterialDev& mt, const float D[9], const float v[3],
-                                          const float C[9], float m, float V, float Jm1, float& wave,
+                                          const float C[9], float m, float V, float Jm1, float aux, float& wave,
                                           float& grad) {
   float row = 0.f, col = 0.f, g = 0.f;
 #pragma unroll
@@ -170,8 +171,11 @@ __device__ __forceinline__ void cfl_terms(const MaterialDev& mt, const float D[9
     row = fmaxf(row, r);
     col = fmaxf(col, cc);
   }
-  const float compression = mt.model == 1 ? 1.f / fmaxf(0.05f, 1.f + Jm1) : 1.f;
-  const float c = sqrtf(mt.wave_modulus * V / m);
+  // Neo-Hookean and the pressure models stiffen in compression (by J, or J Jp for 8 and 9); snow's
+  // moduli carry its hardening
+  const bool press = AUX && (mt.model == 8 || mt.model == 9);
+  const float compression = mt.model == 1 || press ? 1.f / fmaxf(0.05f, (1.f + Jm1) * (press ? 1.f + aux : 1.f)) : 1.f;
+  const float c = sqrtf(mt.wave_modulus * (AUX && mt.model == 2 ? snow_hardening(aux) : 1.f) * V / m);
   const float speed = sqrtf(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
   wave = speed + c * fmaxf(1.f, fmaxf(row * col, compression));
   grad = g;
@@ -481,6 +485,7 @@ struct TileCtx {
   long long node_base;
   float H, invH;
   int clamp;
+  int mat;  // material row of a single-material scene
 };
 
 struct __align__(128) PartSmem {
@@ -806,7 +811,7 @@ __device__ __noinline__ void gather_global(const float4* base, int sy, long long
 // for the P2G pass and pinned particles, the stress of the stored state; then the scatter payload
 // bucketed by its new stencil base in the shared window (pay, meta, hist), and the CFL terms.
 // Writes the particle's new state and returns its next sort key (all ones when not needed).
-template <int PASS, bool HEAT>
+template <int PASS, bool HEAT, bool AUX>
 __device__ __forceinline__ unsigned particle_phase_a(const Ctx& c, const SceneDev& sc, const TileCtx& tc,
                                                      const MaterialDev& mt_single, bool single, const float4* vwin,
                                                      unsigned home, unsigned j, float dt, int nxt, float* pay,
@@ -821,9 +826,11 @@ __device__ __forceinline__ unsigned particle_phase_a(const Ctx& c, const SceneDe
   for (int e = 0; e < 9; ++e) D[e] = c.p.Dc[e][home];
   const float m = c.p.m[home], V = c.p.V[home];
   const MaterialDev mt = single ? mt_single : c.mats[c.p.mat[home]];
+  const MaterialExt* xp = AUX ? &c.mats_ext[single ? tc.mat : c.p.mat[home]] : nullptr;
   const bool pinned = c.has_pinned && c.p.pinned[home];
   float ep = c.has_plastic ? c.p.ep[home] : 0.f;
   float T = c.has_thermal ? c.p.T[home] : 0.f;
+  float aux = AUX ? c.p.aux[home] : 0.f;
   float v[3], C[9];
   ConstitutiveOut co;
   unsigned flags = 0;
@@ -905,7 +912,7 @@ __device__ __forceinline__ unsigned particle_phase_a(const Ctx& c, const SceneDe
       q[a] = static_cast<unsigned>(qn);
     }
     // return map / stress for the next P2G (src/three/mpm.js:126-131)
-    co = constitutive_update(mt, D, ep, T, V / m, true, dt);
+    co = constitutive_update_t<AUX>(mt, D, ep, aux, T, V / m, true, dt, xp);
     ep += co.dep;
     T += co.dT;
     c.p.qx[home] = q[0]; c.p.qy[home] = q[1]; c.p.qz[home] = q[2];
@@ -917,6 +924,7 @@ __device__ __forceinline__ unsigned particle_phase_a(const Ctx& c, const SceneDe
     }
     if (c.has_plastic) c.p.ep[home] = ep;
     if (c.has_thermal) c.p.T[home] = T;
+    if (AUX) c.p.aux[home] = aux;
     if (co.dep > 0.f && mt.heat_per_work > 0.f) work_acc += static_cast<double>(co.dT) * m / mt.heat_per_work;
   } else {
     // P2G of the stored state, and pinned particles (not moved, src/three/mpm.js:108)
@@ -926,7 +934,7 @@ __device__ __forceinline__ unsigned particle_phase_a(const Ctx& c, const SceneDe
     float Dc[9];
 #pragma unroll
     for (int e = 0; e < 9; ++e) Dc[e] = D[e];
-    co = constitutive_update(mt, Dc, ep, T, V / m, false);
+    co = constitutive_update_t<AUX>(mt, Dc, ep, aux, T, V / m, false, 0.f, xp);
   }
   if (SCATTER) {
     // payload of the scatter: fraction t, m, m v, m C h, -4 V / h tau
@@ -965,7 +973,7 @@ __device__ __forceinline__ unsigned particle_phase_a(const Ctx& c, const SceneDe
     }
   }
   float wave, grad;
-  cfl_terms(mt, D, v, C, m, V, co.Jm1, wave, grad);
+  cfl_terms<AUX>(mt, D, v, C, m, V, co.Jm1, aux, wave, grad);
   flags |= state_flags(v, D, co.tau, co.Jm1);
   flags_acc |= flags;
   wave_acc = fmaxf(wave_acc, wave);
@@ -973,7 +981,7 @@ __device__ __forceinline__ unsigned particle_phase_a(const Ctx& c, const SceneDe
   return key;
 }
 
-template <int PASS, bool HEAT>
+template <int PASS, bool HEAT, bool AUX>
 __global__ void __launch_bounds__(kBlock, 2) k_particles(const __grid_constant__ Ctx c) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   PartSmem& sm = *reinterpret_cast<PartSmem*>(smem_raw);
@@ -1061,6 +1069,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_particles(const __grid_constant__
       tl.H = sc.H;
       tl.invH = sc.invH;
       tl.clamp = sc.clamp;
+      tl.mat = sc.mat_base;
       sm.tc = tl;
       if (c.single_material) sm.mt = c.mats[sc.mat_base];
     }
@@ -1092,7 +1101,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_particles(const __grid_constant__
         unsigned key = 0xffffffffu;
         if (j < nround) {
           const unsigned home = (r0 == 0 && pf_ok) ? (jj == 0 ? pf[0] : pf[1]) : c.p.perm[it.y + r0 + j];
-          key = particle_phase_a<PASS, HEAT>(c, sc, tc, sm.mt, single, sm.vwin[cb], home, j, dt, nxt, sm.pay, sm.meta,
+          key = particle_phase_a<PASS, HEAT, AUX>(c, sc, tc, sm.mt, single, sm.vwin[cb], home, j, dt, nxt, sm.pay, sm.meta,
                                        sm.hist, wave_acc, grad_acc, flags_acc, work_acc);
         }
         if (PASS == kPassG2P2G) count_key(c, key);
@@ -1229,7 +1238,7 @@ __device__ __forceinline__ void group_reduce_item(const Ctx& c, int scene, float
   }
 }
 
-template <int PASS, bool HEAT>
+template <int PASS, bool HEAT, bool AUX>
 __global__ void __launch_bounds__(kWsThreads, 1) k_particles_ws(const __grid_constant__ Ctx c) {
   static_assert(PASS != kPassG2P, "the warp-specialised pass always scatters");
   extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -1315,6 +1324,7 @@ __global__ void __launch_bounds__(kWsThreads, 1) k_particles_ws(const __grid_con
         tl.H = sc.H;
         tl.invH = sc.invH;
         tl.clamp = sc.clamp;
+        tl.mat = sc.mat_base;
         sm.tc = tl;
         if (single) sm.mt = c.mats[sc.mat_base];
       }
@@ -1355,7 +1365,7 @@ __global__ void __launch_bounds__(kWsThreads, 1) k_particles_ws(const __grid_con
           unsigned key = 0xffffffffu;
           if (j < nround) {
             const unsigned home = c.p.perm[it.y + r0 + j];
-            key = particle_phase_a<PASS, HEAT>(c, sc, tc, sm.mt, single, sm.vwin[cb], home, j, dt, nxt, sm.pay[s],
+            key = particle_phase_a<PASS, HEAT, AUX>(c, sc, tc, sm.mt, single, sm.vwin[cb], home, j, dt, nxt, sm.pay[s],
                                          sm.meta[s], sm.hist[s], wave_acc, grad_acc, flags_acc, work_acc);
           }
           if (PASS == kPassG2P2G) count_key(c, key);
@@ -1449,22 +1459,26 @@ __global__ void __launch_bounds__(kWsThreads, 1) k_particles_ws(const __grid_con
   }
 }
 
-template <int PASS, bool HEAT>
+template <int PASS, bool HEAT, bool AUX>
 static void launch_pass_t(const Ctx& c, cudaStream_t st, int grid_blocks) {
   if (PASS != kPassG2P && c.ws_blocks > 0) {
-    k_particles_ws<PASS == kPassG2P ? kPassG2P2G : PASS, HEAT><<<c.ws_blocks, kWsThreads, sizeof(WsSmem), st>>>(c);
+    k_particles_ws<PASS == kPassG2P ? kPassG2P2G : PASS, HEAT, AUX><<<c.ws_blocks, kWsThreads, sizeof(WsSmem), st>>>(c);
     return;
   }
-  k_particles<PASS, HEAT><<<grid_blocks, kBlock, sizeof(PartSmem), st>>>(c);
+  k_particles<PASS, HEAT, AUX><<<grid_blocks, kBlock, sizeof(PartSmem), st>>>(c);
 }
 
-// The heat channel and the conduction gather are compiled only into the conducting instances.
+// The heat channel and the conduction gather are compiled only into the conducting instances, the
+// history scalar of snow, sand and the pressure laws only into the instances for those materials.
 template <int PASS>
 static void launch_pass(const Ctx& c, cudaStream_t st, int grid_blocks) {
-  if (c.conduct)
-    launch_pass_t<PASS, true>(c, st, grid_blocks);
-  else
-    launch_pass_t<PASS, false>(c, st, grid_blocks);
+  if (c.conduct) {
+    if (c.has_aux) launch_pass_t<PASS, true, true>(c, st, grid_blocks);
+    else launch_pass_t<PASS, true, false>(c, st, grid_blocks);
+  } else {
+    if (c.has_aux) launch_pass_t<PASS, false, true>(c, st, grid_blocks);
+    else launch_pass_t<PASS, false, false>(c, st, grid_blocks);
+  }
 }
 
 void launch_p2g(const Ctx& c, cudaStream_t st, int grid_blocks) { launch_pass<kPassP2G>(c, st, grid_blocks); }
@@ -1478,10 +1492,13 @@ void launch_g2p2g(const Ctx& c, cudaStream_t st, int grid_blocks, bool scatter) 
 
 template <int PASS>
 static int blocks_per_sm() {
-  cudaFuncSetAttribute(k_particles<PASS, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(PartSmem));
-  cudaFuncSetAttribute(k_particles<PASS, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(PartSmem));
+  const int bytes = (int)sizeof(PartSmem);
+  cudaFuncSetAttribute(k_particles<PASS, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  cudaFuncSetAttribute(k_particles<PASS, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  cudaFuncSetAttribute(k_particles<PASS, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  cudaFuncSetAttribute(k_particles<PASS, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
   int n = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_particles<PASS, false>, kBlock, sizeof(PartSmem));
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_particles<PASS, false, false>, kBlock, sizeof(PartSmem));
   return n > 0 ? n : 1;
 }
 
@@ -1489,13 +1506,16 @@ static int blocks_per_sm() {
 int ws_blocks_per_sm() {
   int n0 = 0, n1 = 0;
   const int bytes = (int)sizeof(WsSmem);
-  if (cudaFuncSetAttribute(k_particles_ws<kPassP2G, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) != cudaSuccess ||
-      cudaFuncSetAttribute(k_particles_ws<kPassG2P2G, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) != cudaSuccess ||
-      cudaFuncSetAttribute(k_particles_ws<kPassP2G, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) != cudaSuccess ||
-      cudaFuncSetAttribute(k_particles_ws<kPassG2P2G, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) != cudaSuccess)
+  auto set = [&](const void* fn) {
+    return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) == cudaSuccess;
+  };
+  if (!set((const void*)k_particles_ws<kPassP2G, false, false>) || !set((const void*)k_particles_ws<kPassG2P2G, false, false>) ||
+      !set((const void*)k_particles_ws<kPassP2G, true, false>) || !set((const void*)k_particles_ws<kPassG2P2G, true, false>) ||
+      !set((const void*)k_particles_ws<kPassP2G, false, true>) || !set((const void*)k_particles_ws<kPassG2P2G, false, true>) ||
+      !set((const void*)k_particles_ws<kPassP2G, true, true>) || !set((const void*)k_particles_ws<kPassG2P2G, true, true>))
     return 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n0, k_particles_ws<kPassP2G, true>, kWsThreads, sizeof(WsSmem));
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n1, k_particles_ws<kPassG2P2G, true>, kWsThreads, sizeof(WsSmem));
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n0, k_particles_ws<kPassP2G, true, true>, kWsThreads, sizeof(WsSmem));
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n1, k_particles_ws<kPassG2P2G, true, true>, kWsThreads, sizeof(WsSmem));
   return n0 < n1 ? n0 : n1;
 }
 
@@ -1686,7 +1706,9 @@ __global__ void __launch_bounds__(256) k_ledger(Ctx c, double* partials) {
     float Dc[9];
 #pragma unroll
     for (int e = 0; e < 9; ++e) Dc[e] = D[e];
-    const ConstitutiveOut co = constitutive_update(mt, Dc, 0.f, c.has_thermal ? c.p.T[i] : 0.f, (float)(V / m), false);
+    float aux = c.has_aux ? c.p.aux[i] : 0.f;
+    const ConstitutiveOut co =
+        constitutive_update_aux(mt, nullptr, Dc, 0.f, aux, c.has_thermal ? c.p.T[i] : 0.f, (float)(V / m), false);
     double W = 0.0;
     if (J > 0.0) {
       const Sym3 B = cauchy_green_minus_identity(D);
@@ -1696,13 +1718,13 @@ __global__ void __launch_bounds__(256) k_ledger(Ctx c, double* partials) {
       } else {
         float beta[3], U[9];
         sym_eig3(B, beta, U);
-        if (mt.model == 0) {
+        if (mt.model == 0 || mt.model == 2) {  // snow: fixed-corotated with its hardened moduli
           double s2 = 0.0;
           for (int kk = 0; kk < 3; ++kk) {
             const double sm1 = beta[kk] / (1.0 + sqrt(fmax(1.0 + beta[kk], 0.0)));
             s2 += sm1 * sm1;
           }
-          W = mt.mu * s2 + 0.5 * mt.lam * (double)Jm1 * Jm1;
+          W = (mt.model == 2 ? snow_hardening(aux) : 1.0) * (mt.mu * s2 + 0.5 * mt.lam * (double)Jm1 * Jm1);
         } else {
           double e2 = 0.0, tr = 0.0;
           for (int kk = 0; kk < 3; ++kk) {
@@ -1719,7 +1741,9 @@ __global__ void __launch_bounds__(256) k_ledger(Ctx c, double* partials) {
                               (double)(co.tau.yy - co.tau.zz) * (co.tau.yy - co.tau.zz) +
                               (double)(co.tau.zz - co.tau.xx) * (co.tau.zz - co.tau.xx)) +
                        3.0 * ((double)co.tau.xy * co.tau.xy + (double)co.tau.xz * co.tau.xz + (double)co.tau.yz * co.tau.yz);
-    const double vm = sqrt(fmax(0.0, tvm)) / fmax(1e-6, J);
+    // Cauchy von Mises; the pressure models divide by the total volume ratio J Jp (src/three/mpm.js:38)
+    const double Jv = J * ((mt.model == 8 || mt.model == 9) ? 1.0 + (double)aux : 1.0);
+    const double vm = sqrt(fmax(0.0, tvm)) / fmax(1e-6, Jv);
     bool finite = isfinite(m) && isfinite(v[0] + v[1] + v[2]) && isfinite(J) && isfinite(c2);
 #pragma unroll
     for (int e = 0; e < 9; ++e) finite = finite && isfinite(D[e]);
@@ -1831,6 +1855,14 @@ __global__ void k_upload(Ctx c, long long n, const Tsrc* const* src, const int* 
     if (fields & kFieldVolume) c.p.V[h] = (float)src[7][i];
     if (fields & kFieldTemp) c.p.T[h] = src[8] ? (float)src[8][i] : 0.f;
     if (fields & kFieldPlastic) c.p.ep[h] = src[9] ? (float)src[9][i] : 0.f;
+    if (fields & kFieldAux) {
+      // aux = Jp - 1 (models 2, 8, 9) or the dilation (model 3)
+      const int model = c.mats[material ? sc.mat_base + material[i] : sc.mat_base].model;
+      float a = 0.f;
+      if ((model == 2 || model == 8 || model == 9) && src[12]) a = (float)((double)src[12][i] - 1.0);
+      if (model == 3 && src[13]) a = (float)src[13][i];
+      c.p.aux[h] = a;
+    }
     if (fields & kFieldF)
       for (int e = 0; e < 9; ++e)
         c.p.D[e * cap + h] = src[10] ? (float)((double)src[10][i * 9 + e] - ((e % 4 == 0) ? 1.0 : 0.0)) : 0.f;
@@ -1869,7 +1901,7 @@ __global__ void k_permute(Ctx c, Particles d) {
       d.Cc[e][i] = s.Cc[e][h];
       d.Dc[e][i] = s.Dc[e][h];
     }
-    d.m[i] = s.m[h]; d.V[i] = s.V[h]; d.ep[i] = s.ep[h]; d.T[i] = s.T[h];
+    d.m[i] = s.m[h]; d.V[i] = s.V[h]; d.ep[i] = s.ep[h]; d.T[i] = s.T[h]; d.aux[i] = s.aux[h];
     d.mat[i] = s.mat[h]; d.pinned[i] = s.pinned[h]; d.id[i] = s.id[h];
     s.perm[i] = static_cast<unsigned>(i);
   }
@@ -1897,7 +1929,7 @@ __device__ void copy_slot(const Particles& p, long long dst, long long src) {
     p.Cc[e][dst] = p.Cc[e][src];
     p.Dc[e][dst] = p.Dc[e][src];
   }
-  p.m[dst] = p.m[src]; p.V[dst] = p.V[src]; p.ep[dst] = p.ep[src]; p.T[dst] = p.T[src];
+  p.m[dst] = p.m[src]; p.V[dst] = p.V[src]; p.ep[dst] = p.ep[src]; p.T[dst] = p.T[src]; p.aux[dst] = p.aux[src];
   p.mat[dst] = p.mat[src]; p.pinned[dst] = p.pinned[src]; p.id[dst] = p.id[src];
 }
 
@@ -1916,6 +1948,7 @@ __global__ void k_edit_particle(Ctx c, int op, unsigned new_id, const long long*
       c.p.Dc[e][sp] = 0.f;
     }
     c.p.ep[sp] = 0.f;
+    c.p.aux[sp] = 0.f;  // Jp = 1, dilation = 0
     return;
   }
   c.p.id[sl] = new_id;
@@ -1953,6 +1986,12 @@ __global__ void k_download(Ctx c, long long n, Tdst* const* dst, unsigned fields
     if (fields & kFieldVolume) dst[7][i] = (Tdst)c.p.V[h];
     if (fields & kFieldTemp) dst[8][i] = (Tdst)c.p.T[h];
     if (fields & kFieldPlastic) dst[9][i] = (Tdst)c.p.ep[h];
+    if (fields & kFieldAux) {
+      const int model = c.mats[c.single_material ? sc.mat_base : c.p.mat[h]].model;
+      const double a = c.p.aux[h];
+      if (dst[12]) dst[12][i] = (Tdst)((model == 2 || model == 8 || model == 9) ? 1.0 + a : 1.0);
+      if (dst[13]) dst[13][i] = (Tdst)(model == 3 ? a : 0.0);
+    }
     for (int e = 0; e < 9; ++e) {
       const double ident = (e % 4 == 0) ? 1.0 : 0.0;
       if (fields & kFieldF) dst[10][i * 9 + e] = (Tdst)((double)c.p.D[e * cap + h] + ident);
@@ -2013,11 +2052,12 @@ __global__ void k_pack_frame(Ctx c, long long stride, float* data, double* energ
     float D[9];
     for (int e = 0; e < 9; ++e) D[e] = c.p.D[e * c.p.cap + h];
     const float Jm1 = det_minus_one(D);
-    const ConstitutiveOut co = constitutive_update(mt, D, 0.f, T, c.p.V[h] / m, false);
+    float aux = c.has_aux ? c.p.aux[h] : 0.f;
+    const ConstitutiveOut co = constitutive_update_aux(mt, nullptr, D, 0.f, aux, T, c.p.V[h] / m, false);
     const float dxy = co.tau.xx - co.tau.yy, dyz = co.tau.yy - co.tau.zz, dzx = co.tau.zz - co.tau.xx;
     const float vm = sqrtf(fmaxf(0.f, 0.5f * (dxy * dxy + dyz * dyz + dzx * dzx) +
                                           3.f * (co.tau.xy * co.tau.xy + co.tau.xz * co.tau.xz + co.tau.yz * co.tau.yz))) /
-                     fmaxf(1e-6f, 1.f + Jm1);
+                     fmaxf(1e-6f, (1.f + Jm1) * ((mt.model == 8 || mt.model == 9) ? 1.f + aux : 1.f));
     float* r = data + row * 8;
     const double Hs = sc.H;
     r[0] = (float)(sc.origin[0] + c.p.qx[h] * (Hs / 4194304.0));

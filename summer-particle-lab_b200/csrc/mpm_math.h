@@ -207,6 +207,26 @@ struct MaterialDev {
   int cr_on;             // creep rate > 0
 };
 
+// Constants of the laws with a second history scalar, in their own table so the row the hot J2
+// path copies stays small.
+struct MaterialExt {
+  // snow, model 2 (src/three/constitutive.js:48,58-60): s - 1 clamped to [snow_lo, snow_hi]
+  float snow_lo, snow_hi;
+  // sand, model 3 (constitutive.js:66-74): alpha (3 lambda + 2 mu) / (2 mu) with
+  // alpha = sqrt(2/3) 2 sin(phi) / (3 - sin(phi))
+  float sand_k;
+  // pressure models 8 and 9 (src/three/pressure-plasticity.js:11-48): bulk modulus lambda + 2 mu / 3,
+  // cohesive Drucker-Prager cohesion, slope, dilatancy and tension cutoff; Deshpande-Fleck alpha^2,
+  // 1 + alpha^2 / 9, plateau, gamma, densification, beta and 1 / eps_D
+  float bulk;
+  float dp_c, dp_a, dp_b, dp_T;
+  float df_a2, df_B, df_plateau, df_gamma, df_densify, df_beta, df_inv_epsd;
+};
+
+// Models whose state carries a second history scalar (aux): Jp - 1 for snow and the pressure
+// models (the plastic volume ratio, src/three/mpm.js:9), the dilation for sand.
+MPM_HD bool aux_model(int model) { return model == 2 || model == 3 || model == 8 || model == 9; }
+
 // Johnson-Cook flow stress (src/three/metal-plasticity.js:12-19).
 MPM_HD float jc_flow(const MaterialDev& mt, float ep, float rate, float T) {
   const float rf = 1.f + mt.jc_C * logf(fmaxf(1.f, rate * mt.jc_inv_rate0));
@@ -269,6 +289,18 @@ struct ConstitutiveOut {
   float dT;       // temperature increment from plastic work
   float Jm1;      // det F - 1 after the return
 };
+
+// Deshpande-Fleck foam strength (src/three/pressure-plasticity.js:11-14); fully densified
+// (ep >= eps_D) is given an effectively infinite strength.
+MPM_HD float foam_strength(const MaterialExt& mt, float ep) {
+  const float r = ep * mt.df_inv_epsd;
+  if (r >= 1.f) return 1e30f;
+  return mt.df_plateau + mt.df_gamma * r - mt.df_densify * logf(fmaxf(1e-30f, 1.f - powf(r, mt.df_beta)));
+}
+
+// Snow's compaction hardening clamp(exp(10 (1 - Jp)), 0.25, 4) with aux = Jp - 1
+// (src/three/constitutive.js:48).
+MPM_HD float snow_hardening(float aux) { return fminf(4.f, fmaxf(0.25f, expf(-10.f * aux))); }
 
 // Hencky strains e_k = log(max(s_k, 1e-6)) from beta_k = s_k^2 - 1 (constitutive.js:58,
 // metal-plasticity.js:21)
@@ -341,6 +373,160 @@ MPM_NOINLINE ConstitutiveOut constitutive_eigen(const MaterialDev& mt, const Sym
   return out;
 }
 
+// Snow (2), sand (3), cohesive Drucker-Prager (8) and Deshpande-Fleck foam (9): the returns of
+// src/three/constitutive.js:58-74 and src/three/pressure-plasticity.js:15-48 on the principal
+// stretches s_k of F (eigenvalues beta_k = s_k^2 - 1 of B), then F' = U diag(s'/s) U^T F and the
+// cached stress of the returned state (constitutive.js:81-86; snow: fixed-corotated scaled by
+// its hardening). aux is Jp - 1 (models 2, 8, 9) or the dilation (model 3), updated in place.
+// Always on the eigen-decomposition: the snow clamp acts per principal stretch, and these laws
+// are not on the benchmark path whose registers the series path keeps small. Without the law's
+// constants (xp null) only the stress of the stored state is available (no return).
+MPM_NOINLINE ConstitutiveOut constitutive_pressure(const MaterialDev& mt, const MaterialExt* xp, const Sym3& B,
+                                                   float D[9], float ep, float& aux, bool do_return) {
+  if (!xp) do_return = false;
+  const MaterialExt none{};
+  const MaterialExt& xt = xp ? *xp : none;
+  ConstitutiveOut out;
+  out.dep = 0.f;
+  out.dT = 0.f;
+  float beta[3], U[9];
+  sym_eig3(B, beta, U);
+  float sm1[3], e[3], r[3] = {0.f, 0.f, 0.f};
+  for (int k = 0; k < 3; ++k) {
+    sm1[k] = beta[k] / (1.f + sqrtf(fmaxf(1.f + beta[k], 0.f)));  // s - 1
+    e[k] = hencky_strain(beta[k]);
+  }
+  bool moved = false;
+  float d[3];
+  if (mt.model == 2) {
+    float sn[3] = {sm1[0], sm1[1], sm1[2]};  // returned s - 1
+    if (do_return) {
+      float lr = 0.f, inc2 = 0.f;
+      for (int k = 0; k < 3; ++k) {
+        sn[k] = fminf(xt.snow_hi, fmaxf(xt.snow_lo, sm1[k]));
+        r[k] = (sn[k] - sm1[k]) / (1.f + sm1[k]);
+        const float dl = -log1pf(r[k]);  // log(s / s')
+        lr += dl;
+        inc2 += dl * dl;
+      }
+      // Jp <- clamp(Jp det F / det F', 0.6, 20)
+      aux = fminf(19.f, fmaxf(-0.4f, aux * expf(lr) + expm1f(lr)));
+      out.dep = sqrtf(inc2);
+      moved = out.dep > 0.f;
+    }
+    const float h = snow_hardening(aux);
+    const float Jm1 = expm1f(log1pf(sn[0]) + log1pf(sn[1]) + log1pf(sn[2]));
+    const float vol = h * mt.lam * Jm1 * (1.f + Jm1);
+    for (int k = 0; k < 3; ++k) d[k] = 2.f * h * mt.mu * sn[k] * (1.f + sn[k]) + vol;
+    out.Jm1 = Jm1;
+  } else {
+    float en[3] = {e[0], e[1], e[2]};  // returned log stretches
+    if (do_return && mt.model == 3) {
+      const float tr = e[0] + e[1] + e[2] + aux;
+      if (tr >= 0.f) {  // no tensile strength: back to the unstretched state, dilation kept
+        en[0] = en[1] = en[2] = 0.f;
+        aux = tr;
+      } else {
+        aux = 0.f;
+        float dev[3];
+        for (int k = 0; k < 3; ++k) dev[k] = e[k] - tr * (1.f / 3.f);
+        const float len = sqrtf(dev[0] * dev[0] + dev[1] * dev[1] + dev[2] * dev[2]);
+        const float delta = fmaxf(0.f, len + xt.sand_k * tr);
+        const float f = delta / (len > 0.f ? len : 1.f);
+        for (int k = 0; k < 3; ++k) en[k] = e[k] - f * dev[k];
+      }
+    } else if (do_return) {  // models 8, 9
+      const float tr = e[0] + e[1] + e[2];
+      float dev[3];
+      for (int k = 0; k < 3; ++k) dev[k] = e[k] - tr * (1.f / 3.f);
+      const float len = sqrtf(dev[0] * dev[0] + dev[1] * dev[1] + dev[2] * dev[2]);
+      const float J = fmaxf(1e-6f, expf(tr) * (1.f + aux));
+      const float G = mt.mu / J, K = xt.bulk / J;
+      const float mean = K * tr, q = 2.449489742783178f * G * len;
+      float mean_n = mean, q_n = q, inc = 0.f;
+      if (mt.model == 8) {
+        const float t = q * 0.5773502691896258f;
+        const float c = xt.dp_c, a = xt.dp_a, b = xt.dp_b, T = xt.dp_T;
+        if (mean > T && t + a * T <= c) {
+          mean_n = T;
+        } else if (t + a * mean > c) {
+          const float dl = (t + a * mean - c) / (G + a * K * b);
+          mean_n = mean - K * b * dl;
+          q_n = 1.7320508075688772f * fmaxf(0.f, t - G * dl);
+          if (mean_n > T) {
+            mean_n = T;
+            q_n = 1.7320508075688772f * fmaxf(0.f, c - a * T);
+          }
+        }
+      } else {
+        const float a2 = xt.df_a2, Bf = xt.df_B;
+        const float trial = sqrtf((q * q + a2 * mean * mean) / Bf);
+        if (trial > foam_strength(xt, ep)) {
+          // residual of the consistency condition at plastic multiplier eta (decreasing in eta)
+          auto residual = [&](float eta, float& qn, float& mn, float& dl) {
+            qn = q / (1.f + 3.f * G * eta);
+            mn = mean / (1.f + K * a2 * eta);
+            const float hat = sqrtf((qn * qn + a2 * mn * mn) / Bf);
+            dl = eta * Bf * hat;
+            return hat - foam_strength(xt, ep + dl);
+          };
+          float qn, mn, dl;
+          float lo = 0.f, hi = 1.f / G;
+          for (int k = 0; k < 32 && residual(hi, qn, mn, dl) > 0.f; ++k) hi *= 2.f;
+          for (int k = 0; k < 28; ++k) {
+            const float mid = 0.5f * (lo + hi);
+            if (residual(mid, qn, mn, dl) > 0.f) lo = mid;
+            else hi = mid;
+          }
+          residual(0.5f * (lo + hi), qn, mn, dl);
+          q_n = qn;
+          mean_n = mn;
+          inc = dl;
+        }
+      }
+      const float tr_n = mean_n / K, scale = q > 1e-20f ? q_n / q : 1.f;
+      for (int k = 0; k < 3; ++k) en[k] = tr_n * (1.f / 3.f) + scale * dev[k];
+      if (mt.model == 8) {
+        const float d0 = e[0] - en[0], d1 = e[1] - en[1], d2 = e[2] - en[2];
+        inc = 0.816496580927726f * sqrtf(d0 * d0 + d1 * d1 + d2 * d2);
+      }
+      // Jp <- Jp exp(tr - tr')
+      const float dv = tr - tr_n;
+      aux = aux * expf(dv) + expm1f(dv);
+      out.dep = inc;
+    }
+    if (do_return) {
+      float inc2 = 0.f;
+      for (int k = 0; k < 3; ++k) {
+        const float dk = en[k] - e[k];
+        r[k] = expm1f(dk);
+        inc2 += dk * dk;
+        moved = moved || dk != 0.f;
+      }
+      if (mt.model == 3) out.dep = sqrtf(inc2);  // |log(s / s')| (constitutive.js:76)
+    }
+    const float tr = en[0] + en[1] + en[2];
+    for (int k = 0; k < 3; ++k) d[k] = 2.f * mt.mu * en[k] + mt.lam * tr;
+    out.Jm1 = expm1f(tr);
+  }
+  if (moved) {
+    // D' = M + M D + D with M = U diag(s'/s - 1) U^T
+    const Sym3 M = rotate_diag(U, r);
+    float Dn[9];
+    for (int b = 0; b < 3; ++b) {
+      Dn[0 * 3 + b] = M.xx * D[0 * 3 + b] + M.xy * D[1 * 3 + b] + M.xz * D[2 * 3 + b];
+      Dn[1 * 3 + b] = M.xy * D[0 * 3 + b] + M.yy * D[1 * 3 + b] + M.yz * D[2 * 3 + b];
+      Dn[2 * 3 + b] = M.xz * D[0 * 3 + b] + M.yz * D[1 * 3 + b] + M.zz * D[2 * 3 + b];
+    }
+    Dn[0] += M.xx; Dn[1] += M.xy; Dn[2] += M.xz;
+    Dn[3] += M.xy; Dn[4] += M.yy; Dn[5] += M.yz;
+    Dn[6] += M.xz; Dn[7] += M.yz; Dn[8] += M.zz;
+    for (int k = 0; k < 9; ++k) D[k] += Dn[k];
+  }
+  out.tau = rotate_diag(U, d);
+  return out;
+}
+
 // Constitutive update of one particle after the F update, in place on D (= F - I):
 // models 4-7, 10 and 11 run the J2-type radial return (src/three/metal-plasticity.js:20-38,
 // src/three/thermal-plasticity.js:22-40; dt is the substep, used by the rate-dependent laws 6,
@@ -350,12 +536,17 @@ MPM_NOINLINE ConstitutiveOut constitutive_eigen(const MaterialDev& mt, const Sym
 // ep is the accumulated plastic strain, T the temperature; rho0 = m / V for the heat term.
 // With do_return false the J2 models give the stress of F without a return (the reference's
 // updateStress when no cached stress exists, src/three/mpm.js:36).
-MPM_HD ConstitutiveOut constitutive_update(const MaterialDev& mt, float D[9], float ep, float T,
-                                           float inv_rho0, bool do_return, float dt = 0.f) {
+// Models 2, 3, 8 and 9 also read and update aux with the constants xp (see constitutive_pressure).
+// AUX = false compiles their branch out, for kernels that know no such material is in use.
+template <bool AUX>
+MPM_HD ConstitutiveOut constitutive_update_t(const MaterialDev& mt, float D[9], float ep, float& aux, float T,
+                                             float inv_rho0, bool do_return, float dt = 0.f,
+                                             const MaterialExt* xp = nullptr) {
   ConstitutiveOut out;
   out.dep = 0.f;
   out.dT = 0.f;
   const Sym3 B = cauchy_green_minus_identity(D);
+  if (AUX && aux_model(mt.model)) return constitutive_pressure(mt, xp, B, D, ep, aux, do_return);
   if (mt.model == 1) {  // Neo-Hookean: mu (F F^T - I) + lambda log J I
     const float Jm1 = det_minus_one(D);
     const float J = 1.f + Jm1;
@@ -432,6 +623,20 @@ MPM_HD ConstitutiveOut constitutive_update(const MaterialDev& mt, float D[9], fl
     return out;
   }
   return constitutive_eigen(mt, B, D, ep, T, inv_rho0, do_return, dt);
+}
+
+MPM_HD ConstitutiveOut constitutive_update_aux(const MaterialDev& mt, const MaterialExt* xp, float D[9], float ep,
+                                               float& aux, float T, float inv_rho0, bool do_return, float dt = 0.f) {
+  return constitutive_update_t<true>(mt, D, ep, aux, T, inv_rho0, do_return, dt, xp);
+}
+
+// Every law with its history scalar at the default (Jp = 1, dilation = 0), not returned; snow,
+// sand and the pressure laws give the stress of the stored state only (their constants are not
+// passed).
+MPM_HD ConstitutiveOut constitutive_update(const MaterialDev& mt, float D[9], float ep, float T, float inv_rho0,
+                                           bool do_return, float dt = 0.f) {
+  float aux = 0.f;
+  return constitutive_update_t<true>(mt, D, ep, aux, T, inv_rho0, do_return, dt);
 }
 
 }  // namespace mpm

@@ -117,7 +117,7 @@ extern "C" int mpm_p2g_noalloc(const mpm_domain* domain, const mpm_material* mat
   if (n > 0 && (!x || !v || !F || !C || !m || !V)) return MPM_ERR_INVALID_ARG;
   if (!mass || !momentum) return MPM_ERR_INVALID_ARG;
   const int model = material->model;
-  if (model != 0 && model != 1 && (model < 4 || model > 7) && model != 10 && model != 11) return MPM_ERR_UNSUPPORTED;
+  if (model < 0 || model > 11) return MPM_ERR_UNSUPPORTED;
   if (!(material->mu > 0) || !(3 * material->lambda + 2 * material->mu > 0)) return MPM_ERR_INVALID_ARG;
   // grid geometry as mpm_create derives it (src/three/discretization.js:12-14)
   const double H = domain->cell_size;

@@ -37,13 +37,17 @@ class MpmMaterial(ctypes.Structure):
                 ("heat_fraction", _D), ("specific_heat", _D),
                 ("jc_n", _D), ("jc_C", _D), ("jc_rate0", _D), ("T_melt", _D), ("jc_m", _D),
                 ("creep_rate", _D), ("creep_Q", _D), ("creep_n", _D), ("creep_stress", _D),
-                ("temperature_offset", _D)]
+                ("temperature_offset", _D), ("yield_strain", _D), ("friction_deg", _D),
+                ("dp_cohesion", _D), ("dp_slope", _D), ("dp_dilatancy", _D), ("dp_tension", _D),
+                ("df_alpha", _D), ("df_plateau", _D), ("df_gamma", _D), ("df_densify", _D), ("df_beta", _D),
+                ("df_eps_d", _D)]
 
 
 class MpmParticles(ctypes.Structure):
     _fields_ = [("dtype", _I32), ("reserved", _I32), ("x", _P), ("y", _P), ("z", _P), ("vx", _P),
                 ("vy", _P), ("vz", _P), ("mass", _P), ("volume", _P), ("temperature", _P),
-                ("plastic", _P), ("F", _P), ("C", _P), ("material", _P), ("pinned", _P)]
+                ("plastic", _P), ("F", _P), ("C", _P), ("material", _P), ("pinned", _P), ("jp", _P),
+                ("dilation", _P)]
 
 
 class MpmLedger(ctypes.Structure):
@@ -107,6 +111,7 @@ SIGNATURES = {
     "mpm_configure_domain": (ctypes.c_int, [_P, ctypes.POINTER(MpmDomain)]),
     "mpm_grid_dims": (ctypes.c_int, [_P, ctypes.POINTER(_I32), ctypes.POINTER(_D)]),
     "mpm_set_material": (ctypes.c_int, [_P, _I32, ctypes.POINTER(MpmMaterial)]),
+    "mpm_validate_material": (ctypes.c_int, [ctypes.POINTER(MpmMaterial)]),
     "mpm_get_stream": (ctypes.c_int, [_P, ctypes.POINTER(_P)]),
     "mpm_upload_particles": (ctypes.c_int, [_P, _I64, ctypes.POINTER(MpmParticles)]),
     "mpm_download_particles": (ctypes.c_int, [_P, ctypes.POINTER(MpmParticles)]),

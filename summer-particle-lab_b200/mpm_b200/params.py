@@ -6,7 +6,9 @@ The reference describes its grid by a domain box and a cell size
 separating slip on all six faces (src/three/mpm.js:93). The sticky floor is an added option.
 
 Materials follow the reference's model numbering (src/three/constitutive.js:6-19):
-0 fixed-corotated, 1 Neo-Hookean, 4 ideal J2, 5 linear-hardening J2, 10 thermal-softening J2.
+0 fixed-corotated, 1 Neo-Hookean, 2 snow, 3 sand (Drucker-Prager), 4 ideal J2, 5 linear-hardening
+J2, 6 Johnson-Cook, 7 simplified Johnson-Cook, 8 cohesive Drucker-Prager, 9 Deshpande-Fleck foam,
+10 thermal-softening J2, 11 Norton creep.
 The reference fixes mu = lambda = 0.4 E and gives strengths as stress / E
 (src/three/mpm.js:34-37, src/three/metal-plasticity.js:1-2); here every parameter is SI and
 ``Material.reference_units`` rebuilds the reference's convention.
@@ -22,7 +24,14 @@ MODEL_THERMAL_J2 = 10
 MODEL_JOHNSON_COOK = 6
 MODEL_JOHNSON_COOK_SIMPLE = 7
 MODEL_NORTON_CREEP = 11
-SUPPORTED_MODELS = (0, 1, 4, 5, 6, 7, 10, 11)
+MODEL_SNOW = 2
+MODEL_SAND = 3
+MODEL_COHESIVE_DP = 8
+MODEL_FOAM = 9
+SUPPORTED_MODELS = tuple(range(12))
+# src/three/pressure-plasticity.js:2, strengths as stress / E
+PRESSURE_DEFAULTS = dict(cohesion=.025, slope=.6, dilatancy=.15, tension=.01, alpha=1.5, plateau=.015, gamma=.01,
+                         densify=.02, beta=2.0, epsD=.7)
 
 # Positions are held on the device as unsigned 32-bit fixed point in cell units relative to the
 # grid origin, with this many fractional bits (grids up to 1023 cells per axis).
@@ -92,6 +101,21 @@ class Material:
     creep_n: float = 1.0
     creep_stress: float = 1.0
     temperature_offset: float = 0.0  # added to T for the Arrhenius term (273.15 for deg C)
+    # snow (2): principal stretches clamped to [1 - yield_strain, 1 + 0.3 yield_strain];
+    # sand (3): friction angle (degrees)
+    yield_strain: float = 0.025
+    friction_deg: float = 35.0
+    # cohesive Drucker-Prager (8) and Deshpande-Fleck foam (9), strengths in Pa
+    dp_cohesion: float = 0.0
+    dp_slope: float = 0.6
+    dp_dilatancy: float = 0.15
+    dp_tension: float = 0.0
+    df_alpha: float = 1.5
+    df_plateau: float = 1.0
+    df_gamma: float = 0.0
+    df_densify: float = 1.0
+    df_beta: float = 2.0
+    df_eps_d: float = 0.7
 
     def __post_init__(self):
         if self.model not in SUPPORTED_MODELS:
@@ -108,9 +132,17 @@ class Material:
         return Material(model=model, mu=mu, lam=lam, **kw)
 
     @staticmethod
-    def reference_units(model, E=1.0, A=.025, B=.08, thermal=None, density=1000.0):
+    def reference_units(model, E=1.0, A=.025, B=.08, thermal=None, density=1000.0, pressure=None,
+                        yield_strain=.025, friction=35.0):
         """The reference's convention: mu = lambda = 0.4 E, strengths given as stress / E."""
         kw = dict(model=model, mu=.4 * E, lam=.4 * E, density=density)
+        if model in (2, 3):
+            kw.update(yield_strain=yield_strain, friction_deg=friction)
+        if model in (8, 9):
+            q = dict(PRESSURE_DEFAULTS, **(pressure or {}))
+            kw.update(dp_cohesion=q["cohesion"] * E, dp_slope=q["slope"], dp_dilatancy=q["dilatancy"],
+                      dp_tension=q["tension"] * E, df_alpha=q["alpha"], df_plateau=q["plateau"] * E,
+                      df_gamma=q["gamma"] * E, df_densify=q["densify"] * E, df_beta=q["beta"], df_eps_d=q["epsD"])
         if model in (4, 5):
             kw.update(yield_stress=A * E, hardening=(B * E if model == 5 else 0.0))
         if model in (6, 7):

@@ -54,6 +54,8 @@ class Scene:
     C: np.ndarray = None     # (n, 9) APIC affine matrix (default zero)
     ep: np.ndarray = None    # (n,) plastic strain (default zero)
     pinned: np.ndarray = None
+    jp: np.ndarray = None    # (n,) plastic volume ratio Jp of snow / pressure materials (default one)
+    dilation: np.ndarray = None  # (n,) sand dilation history (default zero)
     meta: dict = field(default_factory=dict)
 
     @property

@@ -37,7 +37,11 @@ def material_struct(m):
                        heat_fraction=m.heat_fraction, specific_heat=m.specific_heat, jc_n=m.jc_n, jc_C=m.jc_C,
                        jc_rate0=m.jc_rate0, T_melt=m.T_melt, jc_m=m.jc_m, creep_rate=m.creep_rate,
                        creep_Q=m.creep_Q, creep_n=m.creep_n, creep_stress=m.creep_stress,
-                       temperature_offset=m.temperature_offset)
+                       temperature_offset=m.temperature_offset, yield_strain=m.yield_strain,
+                       friction_deg=m.friction_deg, dp_cohesion=m.dp_cohesion, dp_slope=m.dp_slope,
+                       dp_dilatancy=m.dp_dilatancy, dp_tension=m.dp_tension, df_alpha=m.df_alpha,
+                       df_plateau=m.df_plateau, df_gamma=m.df_gamma, df_densify=m.df_densify, df_beta=m.df_beta,
+                       df_eps_d=m.df_eps_d)
 
 
 def _ptr(a):
@@ -82,6 +86,7 @@ class Solver:
         cols = [np.ascontiguousarray(x[:, a]) for a in range(3)] + [np.ascontiguousarray(v[:, a]) for a in range(3)]
         m, V = arr(scene.m), arr(scene.V)
         T, ep = arr(scene.T), arr(scene.ep)
+        jp, dil = arr(getattr(scene, "jp", None)), arr(getattr(scene, "dilation", None))
         F = None if scene.F is None else np.ascontiguousarray(np.asarray(scene.F).reshape(n, 9), dtype=f)
         C = None if scene.C is None else np.ascontiguousarray(np.asarray(scene.C).reshape(n, 9), dtype=f)
         mat = np.ascontiguousarray(scene.mat, dtype=np.int32)
@@ -89,7 +94,7 @@ class Solver:
         p = MpmParticles(dtype=_lib.F64 if f == np.float64 else _lib.F32,
                          x=_ptr(cols[0]), y=_ptr(cols[1]), z=_ptr(cols[2]), vx=_ptr(cols[3]), vy=_ptr(cols[4]),
                          vz=_ptr(cols[5]), mass=_ptr(m), volume=_ptr(V), temperature=_ptr(T), plastic=_ptr(ep),
-                         F=_ptr(F), C=_ptr(C), material=_ptr(mat), pinned=_ptr(pin))
+                         F=_ptr(F), C=_ptr(C), material=_ptr(mat), pinned=_ptr(pin), jp=_ptr(jp), dilation=_ptr(dil))
         self._check(_lib.lib().mpm_upload_particles(self.h, n, ctypes.byref(p)))
         self.n = n
         cond = scene.meta.get("conduction") if scene.meta else None
@@ -114,7 +119,7 @@ class Solver:
             for k in ("vx", "vy", "vz"):
                 cols[k] = np.empty(n, dtype=f)
                 setattr(p, k, _ptr(cols[k]))
-        one = {"m": "mass", "V": "volume", "T": "temperature", "ep": "plastic"}
+        one = {"m": "mass", "V": "volume", "T": "temperature", "ep": "plastic", "jp": "jp", "dilation": "dilation"}
         for k, name in one.items():
             if k in fields:
                 out[k] = np.empty(n, dtype=f)

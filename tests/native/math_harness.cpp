@@ -62,6 +62,46 @@ extern "C" void harness_constitutive_full(int model, const double* prm, double d
   }
 }
 
+// Snow, sand and the pressure models with their history scalar: prm = {mu, lam, yield_strain,
+// friction_deg, cohesion, slope, dilatancy, tension, alpha, plateau, gamma, densify, beta, eps_D}
+// (the fields of mpm_material), hist = Jp (models 2, 8, 9) or the dilation (model 3), updated.
+extern "C" void harness_constitutive_aux(int model, const double* prm, int n, const double* F, const double* ep,
+                                         double* hist, int do_return, double* Fout, double* dep, double* tau) {
+  mpm::MaterialDev m{};
+  m.model = model;
+  m.mu = (float)prm[0];
+  m.lam = (float)prm[1];
+  m.wave_modulus = (float)(prm[1] + 2 * prm[0]);
+  mpm::MaterialExt x{};
+  x.snow_lo = (float)(-prm[2]);
+  x.snow_hi = (float)(0.3 * prm[2]);
+  const double sn = std::sin(prm[3] * 3.14159265358979323846 / 180.0);
+  x.sand_k = (float)(std::sqrt(2.0 / 3.0) * 2 * sn / (3 - sn) * (3 * prm[1] + 2 * prm[0]) / (2 * prm[0]));
+  x.bulk = (float)(prm[1] + 2 * prm[0] / 3);
+  x.dp_c = (float)prm[4];
+  x.dp_a = (float)prm[5];
+  x.dp_b = (float)prm[6];
+  x.dp_T = (float)prm[7];
+  x.df_a2 = (float)(prm[8] * prm[8]);
+  x.df_B = (float)(1 + prm[8] * prm[8] / 9);
+  x.df_plateau = (float)prm[9];
+  x.df_gamma = (float)prm[10];
+  x.df_densify = (float)prm[11];
+  x.df_beta = (float)prm[12];
+  x.df_inv_epsd = (float)(1.0 / prm[13]);
+  for (int i = 0; i < n; ++i) {
+    float D[9];
+    for (int e = 0; e < 9; ++e) D[e] = (float)(F[i * 9 + e] - (e % 4 == 0 ? 1.0 : 0.0));
+    float aux = model == 3 ? (float)hist[i] : (float)(hist[i] - 1.0);
+    mpm::ConstitutiveOut o = mpm::constitutive_update_aux(m, &x, D, (float)ep[i], aux, 0.f, 1.f, do_return != 0, 0.01f);
+    for (int e = 0; e < 9; ++e) Fout[i * 9 + e] = (double)D[e] + (e % 4 == 0 ? 1.0 : 0.0);
+    dep[i] = o.dep;
+    hist[i] = model == 3 ? (double)aux : 1.0 + (double)aux;
+    const float t9[9] = {o.tau.xx, o.tau.xy, o.tau.xz, o.tau.xy, o.tau.yy, o.tau.yz, o.tau.xz, o.tau.yz, o.tau.zz};
+    for (int e = 0; e < 9; ++e) tau[i * 9 + e] = t9[e];
+  }
+}
+
 extern "C" void harness_eig(int n, const double* S6, double* lam, double* U) {
   for (int i = 0; i < n; ++i) {
     mpm::Sym3 a{(float)S6[i * 6 + 0], (float)S6[i * 6 + 1], (float)S6[i * 6 + 2],

@@ -27,7 +27,7 @@ def test_library_exports_every_declared_symbol():
 
 def test_abi_version_and_error_strings_need_no_gpu():
     L = _lib.lib()
-    assert L.mpm_abi_version() == 2
+    assert L.mpm_abi_version() == 3
     assert L.mpm_error_string(-4) == b"non-finite particle state"
     assert L.mpm_error_string(0) == b"ok"
 
@@ -35,8 +35,8 @@ def test_abi_version_and_error_strings_need_no_gpu():
 def test_struct_layouts_match_header_sizes():
     # sizes follow from the header's field lists (all 8-byte aligned)
     assert ctypes.sizeof(_lib.MpmDomain) == 8 * 3 * 2 + 8 + 24 + 4 + 4 + 8 * 4 + 8
-    assert ctypes.sizeof(_lib.MpmMaterial) == 8 + 19 * 8
-    assert ctypes.sizeof(_lib.MpmParticles) == 8 + 14 * 8
+    assert ctypes.sizeof(_lib.MpmMaterial) == 8 + 31 * 8
+    assert ctypes.sizeof(_lib.MpmParticles) == 8 + 16 * 8
     assert ctypes.sizeof(_lib.MpmLedger) == 5 * 8 + 6 * 8 + 5 * 8 + 3 * 8
     assert ctypes.sizeof(_lib.SmpmSim) == 4 * 4 + 2 * 8 + 8 * 8
     assert ctypes.sizeof(_lib.SmpmStats) == 4 * 4 + 3 * 8
@@ -49,5 +49,7 @@ def test_invalid_arguments_are_rejected_without_touching_a_device():
     assert L.mpm_destroy(None) == -1
     assert L.smpm_create(0, ctypes.byref(h)) == -1
     assert L.smpm_destroy(None) == -1
-    m = _lib.MpmMaterial(model=3, mu=1, lam=1)
+    m = _lib.MpmMaterial(model=12, mu=1, lam=1)
+    assert L.mpm_return_map_batch(ctypes.byref(m), 0, None, None, None, 0.0, None, None, None) == -10
+    m = _lib.MpmMaterial(model=2, mu=1, lam=1, yield_strain=.025)  # carries Jp between steps
     assert L.mpm_return_map_batch(ctypes.byref(m), 0, None, None, None, 0.0, None, None, None) == -10
