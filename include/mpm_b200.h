@@ -336,6 +336,36 @@ int mpm_batch_grid_debug(mpm_handle* h, int32_t scene, double dt, double* mass, 
 int mpm_batch_autotune(mpm_handle* h, int32_t trial_substeps, mpm_tuning* out);
 
 /* ======================================================================================
+ * Solid position regularisation (src/three/solid-sampling.js:5-42, regularizeSolids): pairs of
+ * particles of one material closer than the mean of their target spacings are pushed apart,
+ * weighted by inverse mass (pinned particles do not move and have none), with
+ *   spacing_i = spacing * cbrt(clamp(V_i det F_i Jp_i / volume_unit, 1/64, 8))
+ *   shift     = (x_i - x_j) (target - r) (1 - exp(-rate dt)) / (r (1/m_i + 1/m_j))
+ * (coincident pairs along the reference's hashed direction of their indices), every shift of a
+ * scene scaled by 1 / max(1, largest |shift| / (max_speed dt)), positions clamped to the domain.
+ * Only positions change: v, C, F and the plastic history are kept. The reference's values in its
+ * own units are spacing 2.8, volume_unit 1, max_speed 8, rate 40; the reference runs it after
+ * every substep unless its solidAntiClump setting is off. Parts are material indices here.
+ * ====================================================================================== */
+typedef struct mpm_regularizer {
+  int32_t enabled;     /* 0: off (the default; mpm_regularize then changes nothing) */
+  int32_t reserved;
+  double spacing;      /* target spacing (m) of a particle whose V det F Jp equals volume_unit */
+  double volume_unit;  /* m^3 */
+  double max_speed;    /* displacement budget per second (m/s) */
+  double rate;         /* relaxation rate (1/s) */
+} mpm_regularizer;
+/* Stores the parameters; while enabled, mpm_step / mpm_step_fixed / mpm_step_cfl / mpm_frame_host
+ * and batch runs regularise after every substep (as Simulation3.substep does), which splits the
+ * fused particle pass into a gather pass, the regularisation and a re-sorted scatter pass. */
+int mpm_set_regularizer(mpm_handle* h, const mpm_regularizer* r);
+/* One pass now with time step dt (the reference's regularizeSolids(s, dt) after MPM3.step). */
+int mpm_regularize(mpm_handle* h, double dt);
+/* The same on the caller's positions (x, y, z required; the regularizeSolids(s, dt) drop-in for a
+ * host that owns them, like mpm_step_host): copied in, regularised, copied back. */
+int mpm_regularize_host(mpm_handle* h, const mpm_particles* io, double dt);
+
+/* ======================================================================================
  * Learned return map. No counterpart in the reference, whose return maps are closed-form or
  * bisection code (src/three/metal-plasticity.js:12-38, src/three/thermal-plasticity.js:12-40):
  * a small MLP (8 -> 64 -> 64 -> 7, ReLU, BF16 tensor-core arithmetic with FP32 accumulation)

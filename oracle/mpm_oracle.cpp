@@ -846,4 +846,90 @@ void oracle_ledger(const OracleScene* sc, const OracleMaterial* mats, int64_t n,
   *out = L;
 }
 
+// ---------------------------------------------------------------------------
+// Solid position regularisation, src/three/solid-sampling.js:5-42 (regularizeSolids), in SI:
+// spacing_i = spacing cbrt(clamp(V_i J_i Jp_i / volume_unit, 1/64, 8)) (the reference's 2.8 and
+// volume 1), pairs of one part (here: one material index) closer than the mean of their spacings
+// pushed apart by (target - r) gain / (r (1/m_i + 1/m_j)) along x_i - x_j, weighted by the inverse
+// masses (pinned particles have none), coincident pairs (r below 1e-8 of the reference's units, i.e.
+// spacing * 1e-8 / 2.8) along a hashed direction of their indices; gain = 1 - exp(-rate dt); every
+// shift scaled by 1 / max(1, max_i |shift_i| / (max_speed dt)), applied to unpinned particles and
+// clamped to [lo, hi]. Pairs are visited i < j in index order like the reference's loop over cells
+// (the order changes only the rounding of the sums). jp may be null (1).
+struct OracleRegularizer {
+  double spacing, volume_unit, max_speed, rate;
+};
+
+void oracle_regularize(const OracleRegularizer* rg, const OracleMaterial* mats, int64_t n, double* x,
+                       const double* F, const double* jp, const double* V, const double* m, const int32_t* mat,
+                       const uint8_t* pinned, double dt, const double* lo, const double* hi) {
+  std::vector<double> target(n), inv(n), dx((size_t)n * 3, 0.0);
+  for (int64_t i = 0; i < n; ++i) {
+    const int model = mats[mat[i]].model;
+    const double j = (model == 2 || model == 8 || model == 9) && jp ? jp[i] : 1.0;
+    const double vol = std::max(.015625, std::min(8.0, V[i] * det3(&F[i * 9]) * j / rg->volume_unit));
+    target[i] = rg->spacing * std::cbrt(vol);
+    inv[i] = pinned && pinned[i] ? 0.0 : 1.0 / m[i];
+  }
+  // cell list with cells as large as the largest possible target (2 spacing)
+  const double hc = 2 * rg->spacing;
+  double lo_c[3] = {INFINITY, INFINITY, INFINITY};
+  for (int64_t i = 0; i < n; ++i)
+    for (int a = 0; a < 3; ++a) lo_c[a] = std::min(lo_c[a], x[i * 3 + a]);
+  std::vector<std::vector<int64_t>> cells;
+  std::vector<int64_t> cell_of(n);
+  int dims[3] = {1, 1, 1};
+  for (int64_t i = 0; i < n; ++i)
+    for (int a = 0; a < 3; ++a) dims[a] = std::max(dims[a], (int)std::floor((x[i * 3 + a] - lo_c[a]) / hc) + 1);
+  cells.resize((size_t)dims[0] * dims[1] * dims[2]);
+  auto coord = [&](int64_t i, int a) { return (int)std::floor((x[i * 3 + a] - lo_c[a]) / hc); };
+  for (int64_t i = 0; i < n; ++i) {
+    const int64_t c = ((int64_t)coord(i, 2) * dims[1] + coord(i, 1)) * dims[0] + coord(i, 0);
+    cell_of[i] = c;
+    cells[c].push_back(i);
+  }
+  const double gain = 1 - std::exp(-rg->rate * dt), eps = rg->spacing * 1e-8 / 2.8;
+  for (int64_t i = 0; i < n; ++i) {
+    const int ci[3] = {coord(i, 0), coord(i, 1), coord(i, 2)};
+    for (int z = -1; z <= 1; ++z)
+      for (int y = -1; y <= 1; ++y)
+        for (int xx = -1; xx <= 1; ++xx) {
+          const int cz = ci[2] + z, cy = ci[1] + y, cx = ci[0] + xx;
+          if (cz < 0 || cy < 0 || cx < 0 || cz >= dims[2] || cy >= dims[1] || cx >= dims[0]) continue;
+          for (int64_t j : cells[((int64_t)cz * dims[1] + cy) * dims[0] + cx]) {
+            if (j <= i || mat[i] != mat[j]) continue;
+            const double total = inv[i] + inv[j];
+            if (!(total > 0)) continue;
+            double d[3] = {x[i * 3] - x[j * 3], x[i * 3 + 1] - x[j * 3 + 1], x[i * 3 + 2] - x[j * 3 + 2]};
+            double r = std::sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+            const double t = (target[i] + target[j]) * .5;
+            if (r >= t) continue;
+            double q;
+            if (r < eps) {
+              const uint32_t h = (uint32_t)(i + 1) * 73856093u ^ (uint32_t)(j + 1) * 19349663u;
+              d[0] = (h & 1023) / 511.5 - 1;
+              d[1] = ((h >> 10) & 1023) / 511.5 - 1;
+              d[2] = ((h >> 20) & 1023) / 511.5 - 1;
+              r = std::sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+              q = t * gain / (r * total);
+            } else {
+              q = (t - r) * gain / (r * total);
+            }
+            for (int a = 0; a < 3; ++a) {
+              dx[i * 3 + a] += d[a] * q * inv[i];
+              dx[j * 3 + a] -= d[a] * q * inv[j];
+            }
+          }
+        }
+  }
+  double scale = 1;
+  const double budget = rg->max_speed * dt;
+  for (int64_t i = 0; i < n; ++i)
+    scale = std::max(scale, std::sqrt(dx[i * 3] * dx[i * 3] + dx[i * 3 + 1] * dx[i * 3 + 1] + dx[i * 3 + 2] * dx[i * 3 + 2]) / budget);
+  for (int64_t i = 0; i < n; ++i) {
+    if (pinned && pinned[i]) continue;
+    for (int a = 0; a < 3; ++a) x[i * 3 + a] = std::max(lo[a], std::min(hi[a], x[i * 3 + a] + dx[i * 3 + a] / scale));
+  }
+}
+
 }  // extern "C"

@@ -38,6 +38,11 @@ class OracleScene(ctypes.Structure):
                 ("cond_k", _D), ("cond_rho", _D), ("cond_cp", _D)]
 
 
+class OracleRegularizer(ctypes.Structure):
+    """regularizeSolids parameters (src/three/solid-sampling.js:5-42); reference units: 2.8, 1, 8, 40."""
+    _fields_ = [("spacing", _D), ("volume_unit", _D), ("max_speed", _D), ("rate", _D)]
+
+
 class OracleLedger(ctypes.Structure):
     _fields_ = [("mass", _D), ("kinetic", _D), ("affine", _D), ("potential", _D),
                 ("elastic", _D), ("momentum", _D * 3), ("angular", _D * 3), ("min_j", _D),
@@ -94,6 +99,8 @@ def lib():
         L.oracle_stable_dt.restype = _D
         L.oracle_ledger.argtypes = [P(OracleScene), P(OracleMaterial), ctypes.c_int64, _P, _P, _P,
                                     _P, _P, _P, _P, _P, _P, P(OracleLedger)]
+        L.oracle_regularize.argtypes = [P(OracleRegularizer), P(OracleMaterial), ctypes.c_int64, _P, _P, _P, _P, _P,
+                                        _P, _P, _D, _P, _P]
         _lib = L
     return _lib
 
@@ -279,6 +286,16 @@ class OracleState:
         return lib().oracle_stable_dt(ctypes.byref(self.sc), self.mats, self.n, _ptr(self.v),
                                       _ptr(self.C), _ptr(self.F), _ptr(self.m), _ptr(self.V),
                                       _ptr(self.mat), _ptr(self.jp))
+
+    def regularize(self, dt, spacing=2.8, volume_unit=1.0, max_speed=8.0, rate=40.0):
+        """regularizeSolids after a step: moves x only, clamped to the domain's clamp box."""
+        rg = OracleRegularizer(spacing=spacing, volume_unit=volume_unit, max_speed=max_speed, rate=rate)
+        d = self.domain
+        lo = np.array(d.clamp_lo if d.clamp_positions else d.origin, dtype=np.float64)
+        hi = np.array(d.clamp_hi if d.clamp_positions else
+                      [o + (n - 1) * d.H for o, n in zip(d.origin, d.dims)], dtype=np.float64)
+        lib().oracle_regularize(ctypes.byref(rg), self.mats, self.n, _ptr(self.x), _ptr(self.F), _ptr(self.jp),
+                                _ptr(self.V), _ptr(self.m), _ptr(self.mat), _ptr(self.pinned), dt, _ptr(lo), _ptr(hi))
 
     def ledger(self):
         L = OracleLedger()

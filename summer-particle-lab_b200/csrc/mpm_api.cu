@@ -14,6 +14,7 @@
 
 #include "mpm_b200.h"
 #include "mpm_internal.h"
+#include "regularize.h"
 
 using mpm::Ctx;
 using mpm::MaterialDev;
@@ -98,6 +99,12 @@ struct mpm_handle {
   Ctx ctx{};
   int g2p2g_blocks = 0, p2g_blocks = 0, grid_blocks = 0;
   int ws_blocks = 0;  // warp-specialised scatter passes available (CTAs), 0: not available
+  // solid position regularisation: parameters and scratch (cells, sort, shifts), built on use
+  mpm_regularizer reg{};
+  void* rblock = nullptr;  size_t rblock_bytes = 0;
+  mpm::RegBufs rbufs{};
+  mpm::RegDev rdev{};
+  bool reg_dirty = true;   // domain, scenes or spacing changed since the scratch was laid out
   // profiling: event pairs around launches while enabled
   bool profiling = false;
   std::vector<cudaEvent_t> ev_pool;
@@ -217,6 +224,10 @@ static int free_device(mpm_handle* h) {
   if (h->staging) cudaFree(h->staging);
   if (h->dptr_table) cudaFree(h->dptr_table);
   if (h->ledger_partials) cudaFree(h->ledger_partials);
+  if (h->rblock) cudaFree(h->rblock);
+  h->rblock = nullptr;
+  h->rblock_bytes = 0;
+  h->reg_dirty = true;
   if (h->host_ctrl) cudaFreeHost(h->host_ctrl);
   if (h->host_ledger) cudaFreeHost(h->host_ledger);
   h->pblock = h->gblock = h->snap = h->staging = nullptr;
@@ -313,6 +324,7 @@ static int alloc_grid(mpm_handle* h) {
     *tmaps = cv.take<char>(128 * (size_t)ns);
     return align_up(cv.off, 256);
   };
+  h->reg_dirty = true;  // neighbour cells follow the scenes' grids
   Ctx probe{};
   void* t;
   SceneDev* sp;
@@ -946,6 +958,120 @@ int mpm_stable_dt(mpm_handle* h, double* dt) {
   return MPM_OK;
 }
 
+// Lays out the regularisation scratch for the current scenes and spacing: neighbour cells two
+// spacings wide over each scene's grid, the cell sort and the per-particle shifts.
+static int ensure_regularizer(mpm_handle* h) {
+  if (!h->reg_dirty && h->rblock) return MPM_OK;
+  const double hc = 2 * h->reg.spacing;
+  const int ns = static_cast<int>(h->scenes.size());
+  std::vector<mpm::RegScene> rs(ns);
+  long long cells = 0;
+  for (int s = 0; s < ns; ++s) {
+    const SceneDev& sc = h->scenes[s];
+    long long k = 1;
+    for (int a = 0; a < 3; ++a) {
+      const double ext = (sc.dims[a] - 1) * static_cast<double>(sc.H);
+      rs[s].nc[a] = static_cast<int>(std::min(1.0e9, std::floor(ext / hc))) + 1;
+      k *= rs[s].nc[a];
+    }
+    rs[s].cell_base = cells;
+    cells += k;
+    if (cells > (1ll << 30)) return fail(h, MPM_ERR_INVALID_ARG, "regularisation spacing too small for the grid");
+  }
+  const int64_t cap = h->cap;
+  const size_t nb = mpm::reg_scan_blocks(cells);
+  auto lay = [&](char* base, mpm::RegBufs& b, mpm::RegScene** scenes) {
+    Carver cv{base};
+    *scenes = cv.take<mpm::RegScene>(ns);
+    b.count = cv.take<unsigned>(cells);
+    b.start = cv.take<unsigned>(cells);
+    b.cursor = cv.take<unsigned>(cells);
+    b.block_sums = cv.take<unsigned>(nb + 1);
+    b.largest = cv.take<unsigned>(ns);
+    b.cell_of = cv.take<unsigned>(cap);
+    b.sorted = cv.take<unsigned>(cap);
+    b.target = cv.take<float>(cap);
+    b.inv_mass = cv.take<float>(cap);
+    b.shift = cv.take<float4>(cap);
+    return align_up(cv.off, 256);
+  };
+  mpm::RegBufs probe{};
+  mpm::RegScene* sp = nullptr;
+  const size_t bytes = lay(nullptr, probe, &sp);
+  if (h->rblock) cudaFree(h->rblock);
+  h->rblock = nullptr;
+  if (cudaMalloc(&h->rblock, bytes) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(h, MPM_ERR_OUT_OF_MEMORY, "regularisation scratch");
+  }
+  h->rblock_bytes = bytes;
+  lay(static_cast<char*>(h->rblock), h->rbufs, &sp);
+  MPM_CUDA(h, cudaMemcpyAsync(sp, rs.data(), sizeof(mpm::RegScene) * ns, cudaMemcpyHostToDevice, h->stream));
+  MPM_CUDA(h, cudaStreamSynchronize(h->stream));  // rs is a host temporary
+  mpm::RegDev& r = h->rdev;
+  r.scenes = sp;
+  r.cells = cells;
+  r.spacing = static_cast<float>(h->reg.spacing);
+  r.inv_volume_unit = static_cast<float>(1.0 / h->reg.volume_unit);
+  r.max_speed = static_cast<float>(h->reg.max_speed);
+  r.rate = static_cast<float>(h->reg.rate);
+  r.eps = static_cast<float>(h->reg.spacing * 1e-8 / 2.8);  // 1e-8 in the reference's units (spacing 2.8)
+  r.inv_hc = static_cast<float>(1.0 / hc);
+  h->reg_dirty = false;
+  return MPM_OK;
+}
+
+// One regularisation pass over the current state; dt_scene (device, per scene) or dt.
+static int regularize_now(mpm_handle* h, const float* dt_scene, double dt) {
+  int rc = ensure_regularizer(h);
+  if (rc != MPM_OK) return rc;
+  mpm::RegDev r = h->rdev;
+  r.dt_scene = dt_scene;
+  r.dt = static_cast<float>(dt);
+  h->ctx.n = h->n;
+  { ProfScope ps(h, -1); mpm::launch_regularize(h->ctx, r, h->rbufs, h->stream); }
+  MPM_CUDA(h, cudaGetLastError());
+  h->grid_valid = false;  // positions moved: the next scatter re-sorts
+  return MPM_OK;
+}
+
+// Substeps with the regularisation after each one (Simulation3.substep): a gather-only pass, the
+// regularisation at the substep's dt, then the sort and scatter of the regularised state. The
+// host reads the control block after each substep to stop when the call is done.
+static int run_substeps_regularized(mpm_handle* h, int mode, double dt_req, int max_substeps, float dt_fixed,
+                                    int* substeps, double* advanced) {
+  if (!h->grid_valid) {
+    int rc = prepare_grid(h);
+    if (rc != MPM_OK) return rc;
+  }
+  h->ctx.n = h->n;
+  { ProfScope ps(h, -1); mpm::launch_control_step(h->ctx, h->stream, mode, dt_req, max_substeps, dt_fixed); }
+  for (int i = 0; i < max_substeps; ++i) {
+    launch_substep(h, false);
+    MPM_CUDA(h, cudaGetLastError());
+    MPM_CUDA(h, cudaMemcpyAsync(h->host_ctrl, h->ctx.ctrl, sizeof(mpm::Ctrl), cudaMemcpyDeviceToHost, h->stream));
+    MPM_CUDA(h, cudaStreamSynchronize(h->stream));
+    const mpm::Ctrl ct = *h->host_ctrl;
+    if (ct.done || (ct.status & (MPM_STATUS_NONFINITE | MPM_STATUS_TIMEOUT))) break;  // nothing ran
+    h->grid_valid = false;
+    h->pending_grid = false;  // the grid update consumed the scatter; the gather pass made none
+    int rc = regularize_now(h, h->ctx.dt_scene, 0.0);
+    if (rc != MPM_OK) return rc;
+    if (h->reorder_interval > 0 && ++h->substeps_since_reorder >= h->reorder_interval) {
+      h->reorder_pending = true;
+      h->substeps_since_reorder = 0;
+    }
+    rc = prepare_grid(h);  // keeps the call's counters; clears only the lists and the done flag
+    if (rc != MPM_OK) return rc;
+    if (ct.substeps >= max_substeps || (mode == mpm::kModeRequested && !(ct.remaining > 1e-6 * dt_req))) break;
+  }
+  const mpm::Ctrl& ct = *h->host_ctrl;
+  if (substeps) *substeps = ct.substeps;
+  if (advanced) *advanced = ct.advanced;
+  h->last_estimate = ct.substeps;
+  return check_status(h);
+}
+
 static int run_substeps(mpm_handle* h, int mode, double dt_req, int max_substeps, float dt_fixed, int* substeps,
                         double* advanced) {
   if (!h->uploaded) return fail(h, MPM_ERR_STATE, "no particles uploaded");
@@ -954,6 +1080,7 @@ static int run_substeps(mpm_handle* h, int mode, double dt_req, int max_substeps
     if (advanced) *advanced = 0;
     return MPM_OK;
   }
+  if (h->reg.enabled) return run_substeps_regularized(h, mode, dt_req, max_substeps, dt_fixed, substeps, advanced);
   if (!h->grid_valid) {
     int rc = prepare_grid(h);
     if (rc != MPM_OK) return rc;
@@ -1082,6 +1209,53 @@ int mpm_frame_host(mpm_handle* h, const mpm_particles* io, double dt_requested, 
   out.dtype = io->dtype;
   out.x = io->x; out.y = io->y; out.z = io->z;
   out.vx = io->vx; out.vy = io->vy; out.vz = io->vz;
+  return mpm_download_particles(h, &out);
+}
+
+int mpm_set_regularizer(mpm_handle* h, const mpm_regularizer* r) {
+  if (!h || !r) return MPM_ERR_INVALID_ARG;
+  if (r->enabled && (!(r->spacing > 0) || !(r->volume_unit > 0) || !(r->max_speed > 0) || !(r->rate >= 0) ||
+                     !std::isfinite(r->spacing) || !std::isfinite(r->volume_unit) || !std::isfinite(r->max_speed) ||
+                     !std::isfinite(r->rate)))
+    return fail(h, MPM_ERR_INVALID_ARG, "regulariser needs spacing, volume_unit, max_speed > 0 and rate >= 0");
+  if (r->enabled && r->spacing != h->reg.spacing) h->reg_dirty = true;
+  h->reg = *r;
+  drop_graph(h);  // a captured graph holds the fused (unregularised) substeps
+  return MPM_OK;
+}
+
+int mpm_regularize(mpm_handle* h, double dt) {
+  if (!h) return MPM_ERR_INVALID_ARG;
+  if (!h->uploaded) return fail(h, MPM_ERR_STATE, "no particles uploaded");
+  if (!(dt > 0) || !std::isfinite(dt)) return fail(h, MPM_ERR_INVALID_ARG, "dt must be positive");
+  if (!h->reg.enabled || h->n == 0) return MPM_OK;  // solidAntiClump off: nothing moves
+  const int rc = regularize_now(h, nullptr, dt);
+  if (rc != MPM_OK) return rc;
+  MPM_CUDA(h, cudaStreamSynchronize(h->stream));
+  return MPM_OK;
+}
+
+int mpm_regularize_host(mpm_handle* h, const mpm_particles* io, double dt) {
+  if (!h || !io) return MPM_ERR_INVALID_ARG;
+  if (h->batch) return fail(h, MPM_ERR_STATE, "single-scene call on a batch handle");
+  if (!h->uploaded) return fail(h, MPM_ERR_STATE, "no particles uploaded");
+  if (!io->x || !io->y || !io->z) return fail(h, MPM_ERR_INVALID_ARG, "positions are required");
+  if (!(dt > 0) || !std::isfinite(dt)) return fail(h, MPM_ERR_INVALID_ARG, "dt must be positive");
+  if (!h->reg.enabled || h->n == 0) return MPM_OK;
+  void* ptrs[kStaged];
+  const int* mat_dev;
+  const unsigned char* pin_dev;
+  int rc = stage_in(h, h->n, io, ptrs, &mat_dev, &pin_dev, mpm::kFieldPos);
+  if (rc != MPM_OK) return rc;
+  { ProfScope ps(h, -1);
+    mpm::launch_upload_convert(h->ctx, h->stream, h->n, io->dtype, reinterpret_cast<const void* const*>(h->dptr_table),
+                               nullptr, nullptr, mpm::kFieldPos, true); }
+  MPM_CUDA(h, cudaGetLastError());
+  rc = regularize_now(h, nullptr, dt);
+  if (rc != MPM_OK) return rc;
+  mpm_particles out{};
+  out.dtype = io->dtype;
+  out.x = io->x; out.y = io->y; out.z = io->z;
   return mpm_download_particles(h, &out);
 }
 
@@ -1605,7 +1779,7 @@ int mpm_batch_run(mpm_handle* h, int32_t nsteps, int32_t use_graph) {
   if (nsteps <= 0) return fail(h, MPM_ERR_INVALID_ARG, "nsteps must be positive");
   if (!h->uploaded) return fail(h, MPM_ERR_STATE, "no particles uploaded");
   if (h->n == 0) return MPM_OK;
-  if (!use_graph || h->reorder_interval <= 0) return mpm_step_cfl(h, nsteps, nullptr);
+  if (!use_graph || h->reorder_interval <= 0 || h->reg.enabled) return mpm_step_cfl(h, nsteps, nullptr);
   if (!h->grid_valid) {
     int rc = prepare_grid(h);
     if (rc != MPM_OK) return rc;

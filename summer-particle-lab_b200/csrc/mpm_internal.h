@@ -150,6 +150,18 @@ struct Ctx {
   int conduct;          // a scene conducts heat on the grid: heat channel, conduction pass, dT gather
 };
 
+#ifdef __CUDACC__
+// Scene of home particle slot i (scenes hold contiguous slot ranges in order).
+__device__ __forceinline__ int find_scene_by_particle(const SceneDev* sc, int ns, long long i) {
+  int lo = 0, hi = ns - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (sc[mid].p_begin <= i) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+#endif
+
 // Launch wrappers (mpm_kernels.cu)
 void launch_control_init(const Ctx& c, cudaStream_t st);
 void launch_keys(const Ctx& c, cudaStream_t st);

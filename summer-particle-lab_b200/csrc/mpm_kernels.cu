@@ -76,15 +76,6 @@ __device__ __forceinline__ void tma_load_4d(void* dst, const void* tmap, int c0,
       : "memory");
 }
 
-__device__ __forceinline__ int find_scene_by_particle(const SceneDev* sc, int ns, long long i) {
-  int lo = 0, hi = ns - 1;
-  while (lo < hi) {
-    const int mid = (lo + hi + 1) >> 1;
-    if (sc[mid].p_begin <= i) lo = mid; else hi = mid - 1;
-  }
-  return lo;
-}
-
 __device__ __forceinline__ int find_scene_by_tile(const SceneDev* sc, int ns, int t) {
   int lo = 0, hi = ns - 1;
   while (lo < hi) {

@@ -1,0 +1,39 @@
+// Device side of the solid position regularisation (regularize.cu); internal, not part of the C ABI.
+#pragma once
+#include <cstddef>
+
+#include "mpm_internal.h"
+
+namespace mpm {
+
+// Neighbour cells of one scene: nc cells per axis from the scene's grid origin, global ids from
+// cell_base.
+struct RegScene {
+  int nc[3];
+  int pad;
+  long long cell_base;
+};
+
+struct RegDev {
+  const RegScene* scenes;
+  long long cells;        // total over scenes
+  float spacing;          // target spacing at volume_unit (m)
+  float inv_volume_unit;
+  float max_speed;        // displacement budget per second (m/s)
+  float rate;             // gain = 1 - exp(-rate dt)
+  float eps;              // coincident pairs: r < eps
+  float inv_hc;           // 1 / neighbour cell size (cells are two spacings wide)
+  const float* dt_scene;  // per-scene dt of the substep just taken, or null: dt
+  float dt;
+};
+
+struct RegBufs {
+  unsigned *cell_of, *count, *start, *cursor, *sorted, *block_sums, *largest;
+  float *target, *inv_mass;
+  float4* shift;
+};
+
+size_t reg_scan_blocks(long long cells);
+void launch_regularize(const Ctx& c, const RegDev& r, const RegBufs& b, cudaStream_t st);
+
+}  // namespace mpm

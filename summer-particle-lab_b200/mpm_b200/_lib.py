@@ -43,6 +43,11 @@ class MpmMaterial(ctypes.Structure):
                 ("df_eps_d", _D)]
 
 
+class MpmRegularizer(ctypes.Structure):
+    _fields_ = [("enabled", _I32), ("reserved", _I32), ("spacing", _D), ("volume_unit", _D), ("max_speed", _D),
+                ("rate", _D)]
+
+
 class MpmParticles(ctypes.Structure):
     _fields_ = [("dtype", _I32), ("reserved", _I32), ("x", _P), ("y", _P), ("z", _P), ("vx", _P),
                 ("vy", _P), ("vz", _P), ("mass", _P), ("volume", _P), ("temperature", _P),
@@ -112,6 +117,9 @@ SIGNATURES = {
     "mpm_grid_dims": (ctypes.c_int, [_P, ctypes.POINTER(_I32), ctypes.POINTER(_D)]),
     "mpm_set_material": (ctypes.c_int, [_P, _I32, ctypes.POINTER(MpmMaterial)]),
     "mpm_validate_material": (ctypes.c_int, [ctypes.POINTER(MpmMaterial)]),
+    "mpm_set_regularizer": (ctypes.c_int, [_P, ctypes.POINTER(MpmRegularizer)]),
+    "mpm_regularize": (ctypes.c_int, [_P, _D]),
+    "mpm_regularize_host": (ctypes.c_int, [_P, ctypes.POINTER(MpmParticles), _D]),
     "mpm_get_stream": (ctypes.c_int, [_P, ctypes.POINTER(_P)]),
     "mpm_upload_particles": (ctypes.c_int, [_P, _I64, ctypes.POINTER(MpmParticles)]),
     "mpm_download_particles": (ctypes.c_int, [_P, ctypes.POINTER(MpmParticles)]),

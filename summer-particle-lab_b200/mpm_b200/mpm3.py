@@ -127,6 +127,19 @@ class MPM3:
                                               ctypes.byref(sub)))
         return sub.value
 
+    def setRegularizer(self, enabled=True, spacing=2.8, volume_unit=1.0, max_speed=8.0, rate=40.0):
+        """Parameters of regularizeSolids (the reference's settings.solidAntiClump and its constants,
+        src/three/solid-sampling.js:5-42); `frame` then regularises after every substep."""
+        self.solver.set_regularizer(enabled, spacing, volume_unit, max_speed, rate)
+
+    def regularizeSolids(self, s, dt):
+        """regularizeSolids(s, dt) (src/three/solid-sampling.js:10-42) on the caller's positions,
+        in place, as Simulation3.substep runs it after `step`."""
+        self._sync(s)
+        if s.count == 0:
+            return
+        self._check(_lib.lib().mpm_regularize_host(self.solver.h, ctypes.byref(s.particles("xv")), float(dt)))
+
     def refreshDiagnostics(self, s):
         """The ledger the V&V panel reads (src/simulation/mechanical-diagnostics.js:16-37), FP64."""
         self._sync(s)

@@ -223,6 +223,16 @@ class Solver:
         self._check(_lib.lib().mpm_remove_particle(self.h, int(index), int(last)))
         self.n -= 1
 
+    def set_regularizer(self, enabled=True, spacing=2.8, volume_unit=1.0, max_speed=8.0, rate=40.0):
+        """Solid position regularisation (regularizeSolids); defaults are the reference's units."""
+        r = _lib.MpmRegularizer(enabled=int(bool(enabled)), spacing=spacing, volume_unit=volume_unit,
+                                max_speed=max_speed, rate=rate)
+        self._check(_lib.lib().mpm_set_regularizer(self.h, ctypes.byref(r)))
+
+    def regularize(self, dt):
+        """One regularisation pass now (regularizeSolids(s, dt) after a step)."""
+        self._check(_lib.lib().mpm_regularize(self.h, float(dt)))
+
     def autotune(self, trial_substeps=8):
         t = MpmTuning()
         self._check(_lib.lib().mpm_batch_autotune(self.h, int(trial_substeps), ctypes.byref(t)))

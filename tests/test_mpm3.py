@@ -81,3 +81,25 @@ def test_mpm3_state_methods():
     assert 0.9 < m.minJ(s) <= 1.0 + 1e-3
     assert m.frame(s, 1e-3) >= 1
     m.close()
+
+
+@pytest.mark.gpu
+def test_mpm3_regularize_solids_on_caller_positions():
+    """regularizeSolids(s, dt) through the facade: tests/solid-sampling.test.mjs:7-15 on Sim3 arrays."""
+    from mpm_b200.mpm3 import MPM3
+    from mpm_b200.params import Material
+    s = Sim3(8)
+    s.add(-.5, 0, 0, mass=2.7, volume=1)
+    s.add(.5, 0, 0, mass=3.0, volume=1)
+    s.vx[:2] = 7
+    m = MPM3(s.capacity, materials={0: Material.reference_units(0)})
+    m.setRegularizer(True)
+    for _ in range(60):
+        m.regularizeSolids(s, 1 / 120)
+    assert s.x[1] - s.x[0] > 2.79
+    assert list(s.vx[:2]) == [7, 7]
+    m.setRegularizer(False)
+    x = s.x[:2].copy()
+    m.regularizeSolids(s, 1 / 120)
+    assert np.array_equal(s.x[:2], x)
+    m.close()
