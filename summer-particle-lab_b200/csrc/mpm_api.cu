@@ -993,6 +993,9 @@ static int ensure_regularizer(mpm_handle* h) {
     b.target = cv.take<float>(cap);
     b.inv_mass = cv.take<float>(cap);
     b.shift = cv.take<float4>(cap);
+    b.pos_sorted = cv.take<uint4>(cap);
+    b.inv_sorted = cv.take<uint2>(cap);
+    b.mat_sorted = cv.take<unsigned short>(cap);
     return align_up(cv.off, 256);
   };
   mpm::RegBufs probe{};

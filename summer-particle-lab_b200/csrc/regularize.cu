@@ -6,14 +6,16 @@
 //                  spacings, so every pair closer than its target lies in the 27 surrounding
 //                  cells), target spacing from V J Jp, cell population
 //   scan           exclusive prefix sum of the populations (k_scan_blocks / k_scan_top / k_scan_add)
-//   k_reg_scatter  particle slots grouped by cell
-//   k_reg_pairs    thread per particle: its own shift, gathered over the 27 cells. The reference
-//                  visits each pair once (i < j) and adds +shift to i and -shift to j; the pair
+//   k_reg_scatter  particle slots grouped by cell, with a packed copy of what the pair test reads
+//                  (position, target, inverse mass, index, material) in cell order, so neighbour
+//                  candidates are read as contiguous runs
+//   k_reg_pairs    thread per particle in cell order: its own shift, gathered over the 27 cells.
+//                  The reference visits each pair once (i < j) and adds +shift to i and -shift to j; the pair
 //                  term is antisymmetric, so gathering every neighbour from each side gives the
 //                  same sums without atomics. The largest shift of each scene over its budget.
 //   k_reg_apply    x += shift / max(1, largest / budget) for unpinned particles, clamped to the box
-// HBM traffic per particle: about 60 B (position, D, V, m, aux, id reads; cell, target, shift
-// scratch) plus the neighbour reads, which hit L1/L2 because slots are tile-sorted.
+// HBM traffic per particle: about 110 B (position, D, V, m, aux, id reads; the cell, target, shift
+// and packed scratch) plus the neighbour reads, contiguous runs of the packed copy that L1/L2 serve.
 #include "mpm_internal.h"
 #include "regularize.h"
 
@@ -52,29 +54,37 @@ __global__ void k_reg_count(Ctx c, RegDev r, unsigned* cell_of, float* target, f
   }
 }
 
-__global__ void k_reg_scatter(long long n, const unsigned* cell_of, const unsigned* start, unsigned* cursor,
-                              unsigned* sorted) {
-  for (long long h = blockIdx.x * (long long)blockDim.x + threadIdx.x; h < n; h += (long long)gridDim.x * blockDim.x) {
+__global__ void k_reg_scatter(Ctx c, const unsigned* cell_of, const unsigned* start, unsigned* cursor,
+                              const float* target, const float* inv_mass, unsigned* sorted, uint4* pos_sorted,
+                              uint2* inv_sorted, unsigned short* mat_sorted) {
+  for (long long h = blockIdx.x * (long long)blockDim.x + threadIdx.x; h < c.n; h += (long long)gridDim.x * blockDim.x) {
     const unsigned cell = cell_of[h];
-    sorted[start[cell] + atomicAdd(&cursor[cell], 1u)] = static_cast<unsigned>(h);
+    const unsigned k = start[cell] + atomicAdd(&cursor[cell], 1u);
+    sorted[k] = static_cast<unsigned>(h);
+    pos_sorted[k] = make_uint4(c.p.qx[h], c.p.qy[h], c.p.qz[h], __float_as_uint(target[h]));
+    inv_sorted[k] = make_uint2(__float_as_uint(inv_mass[h]), c.p.id[h]);
+    if (!c.single_material) mat_sorted[k] = c.p.mat[h];
   }
 }
 
 __device__ __forceinline__ float scene_dt(const RegDev& r, int s) { return r.dt_scene ? r.dt_scene[s] : r.dt; }
 
-__global__ void k_reg_pairs(Ctx c, RegDev r, const unsigned* cell_of, const float* target, const float* inv_mass,
-                            const unsigned* start, const unsigned* count, const unsigned* sorted, float4* shift,
-                            unsigned* largest) {
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < c.n; i += (long long)gridDim.x * blockDim.x) {
+__global__ void k_reg_pairs(Ctx c, RegDev r, const unsigned* cell_of, const unsigned* start, const unsigned* count,
+                            const unsigned* sorted, const uint4* pos_sorted, const uint2* inv_sorted,
+                            const unsigned short* mat_sorted, float4* shift, unsigned* largest) {
+  for (long long ks = blockIdx.x * (long long)blockDim.x + threadIdx.x; ks < c.n; ks += (long long)gridDim.x * blockDim.x) {
+    const unsigned i = sorted[ks];  // home slot
     const int s = c.nscenes == 1 ? 0 : find_scene_by_particle(c.scenes, c.nscenes, i);
     const SceneDev& sc = c.scenes[s];
     const RegScene& rs = r.scenes[s];
     const float dt = scene_dt(r, s);
     const float gain = -expm1f(-r.rate * dt);
-    const unsigned qi[3] = {c.p.qx[i], c.p.qy[i], c.p.qz[i]};
-    const float ti = target[i], inv_i = inv_mass[i];
-    const unsigned id_i = c.p.id[i];
-    const int mat_i = c.single_material ? 0 : c.p.mat[i];
+    const uint4 pi = pos_sorted[ks];
+    const uint2 bi = inv_sorted[ks];
+    const unsigned qi[3] = {pi.x, pi.y, pi.z};
+    const float ti = __uint_as_float(pi.w), inv_i = __uint_as_float(bi.x);
+    const unsigned id_i = bi.y;
+    const int mat_i = c.single_material ? 0 : mat_sorted[ks];
     const float to_m = sc.H * kInvFixedOne;
     const long long local = (long long)cell_of[i] - rs.cell_base;
     const int cx = static_cast<int>(local % rs.nc[0]), cy = static_cast<int>((local / rs.nc[0]) % rs.nc[1]),
@@ -87,21 +97,22 @@ __global__ void k_reg_pairs(Ctx c, RegDev r, const unsigned* cell_of, const floa
             const long long cell = rs.cell_base + ((long long)z * rs.nc[1] + y) * rs.nc[0] + x;
             const unsigned b = start[cell], e = b + count[cell];
             for (unsigned k = b; k < e; ++k) {
-              const unsigned j = sorted[k];
-              if (j == i) continue;
-              if (!c.single_material && c.p.mat[j] != mat_i) continue;  // one part
-              const float total = inv_i + inv_mass[j];
+              if (k == ks) continue;
+              if (!c.single_material && mat_sorted[k] != mat_i) continue;  // one part
+              const uint4 pj = pos_sorted[k];
               // exact fixed-point differences, then metres
-              float d[3] = {static_cast<float>(static_cast<int>(qi[0] - c.p.qx[j])) * to_m,
-                            static_cast<float>(static_cast<int>(qi[1] - c.p.qy[j])) * to_m,
-                            static_cast<float>(static_cast<int>(qi[2] - c.p.qz[j])) * to_m};
+              float d[3] = {static_cast<float>(static_cast<int>(qi[0] - pj.x)) * to_m,
+                            static_cast<float>(static_cast<int>(qi[1] - pj.y)) * to_m,
+                            static_cast<float>(static_cast<int>(qi[2] - pj.z)) * to_m};
               float rr = sqrtf(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
-              const float t = 0.5f * (ti + target[j]);
+              const float t = 0.5f * (ti + __uint_as_float(pj.w));
               if (!(rr < t)) continue;
+              const uint2 bj = inv_sorted[k];
+              const float total = inv_i + __uint_as_float(bj.x);
               float q;
               if (rr < r.eps) {
                 // the reference's hashed direction of the pair (lower index first), +/- by side
-                const unsigned id_j = c.p.id[j];
+                const unsigned id_j = bj.y;
                 const unsigned lo = min(id_i, id_j), hi = max(id_i, id_j);
                 const unsigned hsh = (lo + 1u) * 73856093u ^ (hi + 1u) * 19349663u;
                 const float sign = id_i < id_j ? 1.f : -1.f;
@@ -243,9 +254,10 @@ void launch_regularize(const Ctx& c, const RegDev& r, const RegBufs& b, cudaStre
   k_scan_blocks<<<nb, kScanThreads, 0, st>>>(b.count, r.cells, b.start, b.block_sums);
   k_scan_top<<<1, kScanThreads, 0, st>>>(b.block_sums, static_cast<int>(nb));
   k_scan_add<<<nb, 256, 0, st>>>(b.start, r.cells, b.block_sums);
-  k_reg_scatter<<<blocks, 256, 0, st>>>(n, b.cell_of, b.start, b.cursor, b.sorted);
-  k_reg_pairs<<<blocks, 256, 0, st>>>(c, r, b.cell_of, b.target, b.inv_mass, b.start, b.count, b.sorted, b.shift,
-                                      b.largest);
+  k_reg_scatter<<<blocks, 256, 0, st>>>(c, b.cell_of, b.start, b.cursor, b.target, b.inv_mass, b.sorted,
+                                        b.pos_sorted, b.inv_sorted, b.mat_sorted);
+  k_reg_pairs<<<blocks, 256, 0, st>>>(c, r, b.cell_of, b.start, b.count, b.sorted, b.pos_sorted, b.inv_sorted,
+                                      b.mat_sorted, b.shift, b.largest);
   k_reg_apply<<<blocks, 256, 0, st>>>(c, r, b.shift, b.largest);
 }
 

@@ -31,6 +31,9 @@ struct RegBufs {
   unsigned *cell_of, *count, *start, *cursor, *sorted, *block_sums, *largest;
   float *target, *inv_mass;
   float4* shift;
+  uint4* pos_sorted;             // cell order: (qx, qy, qz, target bits)
+  uint2* inv_sorted;             // cell order: (inverse mass bits, caller index)
+  unsigned short* mat_sorted;    // cell order: material (multi-material scenes)
 };
 
 size_t reg_scan_blocks(long long cells);
