@@ -121,6 +121,12 @@ typedef struct mpm_material {
    * (src/three/pressure-plasticity.js:2,11-48): strengths in Pa (Cauchy, tension positive). */
   double dp_cohesion, dp_slope, dp_dilatancy, dp_tension;
   double df_alpha, df_plateau, df_gamma, df_densify, df_beta, df_eps_d;
+  /* Particle-pair heat exchange (src/thermal.js:35-56): conductivity k (W/m/K). Enthalpy phase
+   * change of the custom MPM material (src/three/phase-change.js:4-18): enabled when
+   * latent_heat > 0 (J/kg), melting at melting_point; h = specific_heat T (+ latent_heat once
+   * molten), the temperature sits at melting_point on the plateau, and a particle switches phase
+   * only at complete melting or freezing. */
+  double conductivity, melting_point, latent_heat;
 } mpm_material;
 
 /* Host particle arrays (structure of arrays, like Simulation3's Float64Arrays,
@@ -142,6 +148,8 @@ typedef struct mpm_particles {
   uint8_t* pinned;       /* pinned particles scatter but are not moved (src/three/mpm.js:84,108) */
   void* jp;              /* plastic volume ratio MPM3.Jp (models 2, 8, 9; 1 otherwise) */
   void* dilation;        /* MPM3.dilation (model 3; 0 otherwise) */
+  void* enthalpy;        /* Simulation3.enthalpy (J/kg); on upload it sets the temperature (and phase) */
+  uint8_t* melted;       /* Simulation3.melted: 1 once a phase-change material has fully melted */
 } mpm_particles;
 
 /* FP64 ledger, reduced on the device (src/simulation/mechanical-diagnostics.js:16-37 and
@@ -364,6 +372,33 @@ int mpm_regularize(mpm_handle* h, double dt);
 /* The same on the caller's positions (x, y, z required; the regularizeSolids(s, dt) drop-in for a
  * host that owns them, like mpm_step_host): copied in, regularised, copied back. */
 int mpm_regularize_host(mpm_handle* h, const mpm_particles* io, double dt);
+
+/* ======================================================================================
+ * Particle-pair heat exchange and phase change (src/thermal.js:35-56, exchangeHeat, with the
+ * pairs of Simulation3.near, src/three/simulation.js:168-174, and the phase change of
+ * src/three/phase-change.js:4-18). Every pair of particles of a scene closer than `radius` (and
+ * farther than radius * 1.25e-7, the reference's 1e-6 of its 8-unit radius) exchanges
+ *   Q = (T_j - T_i) g dt min(b_i, b_j),  g = (1 - r / radius) geometry heat_rate 2 k_i k_j / (k_i + k_j)
+ * with b_i = min(1, 0.45 m_i cp_i / (dt sum_j g_ij)) (1 without contacts), applied as +Q / -Q;
+ * then h_i += heat_i / m_i, optional ambient loss (T_i - ambient_T) cp_i dt ambient_rate, and the
+ * phase decode. A particle that melts or freezes gets the reference's resetParticle (F = I,
+ * C = 0, plastic history cleared) and a melted one is unpinned; melted particles keep taking part
+ * in the MPM solve here (the reference hands them to its fluid solver; a host does the same with
+ * mpm_remove_particle). Reference values in its own units: radius 8 (the neighbour cell),
+ * geometry 20, heat_rate 20 (settings.heatRate), ambient_T 15, ambient_rate 0.003.
+ * ====================================================================================== */
+typedef struct mpm_heat_exchange {
+  double radius;        /* m */
+  double geometry;      /* m: contact length of the conductance */
+  double heat_rate;     /* acceleration factor */
+  int32_t ambient;      /* 1: cool toward ambient_T */
+  int32_t reserved;
+  double ambient_T;
+  double ambient_rate;  /* 1/s */
+} mpm_heat_exchange;
+/* One exchange over the time dt (the reference calls it once per frame with the time advanced).
+ * exchanged (may be null): sum over pairs of |Q| (Simulation3.exchangedHeat), FP64. */
+int mpm_exchange_heat(mpm_handle* h, const mpm_heat_exchange* x, double dt, double* exchanged);
 
 /* ======================================================================================
  * Learned return map. No counterpart in the reference, whose return maps are closed-form or

@@ -50,6 +50,9 @@ struct OracleMaterial {
   double yieldStrain, friction;
   // pressure models (src/three/pressure-plasticity.js:2): strengths in the stress unit of mu
   double cohesion, slope, dilatancy, tension, alpha, plateau, gamma, densify, pbeta, epsD;
+  // heat exchange and phase change (src/thermal.js:35-56, src/three/phase-change.js:4-18):
+  // conductivity, melting point and latent heat (phase change enabled when latent > 0)
+  double kcond, Tphase, latent;
 };
 
 struct OracleScene {
@@ -930,6 +933,109 @@ void oracle_regularize(const OracleRegularizer* rg, const OracleMaterial* mats, 
     if (pinned && pinned[i]) continue;
     for (int a = 0; a < 3; ++a) x[i * 3 + a] = std::max(lo[a], std::min(hi[a], x[i * 3 + a] + dx[i * 3 + a] / scale));
   }
+}
+
+// ---------------------------------------------------------------------------
+// Particle-pair heat exchange, src/thermal.js:35-56 (exchangeHeat), over the pairs of
+// src/three/simulation.js:168-174 (r in (1e-6, H) of the reference's units: here
+// (radius * 1.25e-7, radius)), then the phase decode of src/three/phase-change.js:12-18 for
+// materials with latent > 0 (h <= cp Tm: solid at h / cp; h >= cp Tm + L: molten at (h - L) / cp;
+// between: Tm with the previous phase) and h / cp otherwise. A phase switch resets the
+// particle's deformation (MPM3.resetParticle) and unpins a molten one. Enthalpy h (J/kg) and the
+// molten flags are the state; T is written from them. Returns the sum of |Q| over pairs.
+struct OracleHeat {
+  double radius, geometry, heat_rate;
+  int32_t ambient, pad;
+  double ambient_T, ambient_rate;
+};
+
+// phaseEnthalpy (src/three/phase-change.js:11)
+double oracle_phase_enthalpy(double T, const OracleMaterial* p) {
+  return p->cp * T + (p->latent > 0 && T > p->Tphase ? p->latent : 0.0);
+}
+
+double oracle_exchange_heat(const OracleHeat* x, const OracleMaterial* mats, int64_t n, const double* pos, double* T,
+                            double* h, uint8_t* melted, const double* m, const int32_t* mat, uint8_t* pinned,
+                            double* F, double* C, double* ep, double* jp, double* dilation, double dt) {
+  const double R = x->radius, eps = R * 1.25e-7;
+  // pairs i < j in index order (the reference collects them over neighbour cells; the pair set and
+  // each pair's terms are the same)
+  struct Pair { int64_t i, j; double g; };
+  std::vector<Pair> pairs;
+  std::vector<std::vector<int64_t>> cells;
+  double lo[3] = {INFINITY, INFINITY, INFINITY};
+  for (int64_t i = 0; i < n; ++i)
+    for (int a = 0; a < 3; ++a) lo[a] = std::min(lo[a], pos[i * 3 + a]);
+  int dims[3] = {1, 1, 1};
+  auto coord = [&](int64_t i, int a) { return (int)std::floor((pos[i * 3 + a] - lo[a]) / R); };
+  for (int64_t i = 0; i < n; ++i)
+    for (int a = 0; a < 3; ++a) dims[a] = std::max(dims[a], coord(i, a) + 1);
+  cells.resize((size_t)dims[0] * dims[1] * dims[2]);
+  for (int64_t i = 0; i < n; ++i) cells[((int64_t)coord(i, 2) * dims[1] + coord(i, 1)) * dims[0] + coord(i, 0)].push_back(i);
+  for (int64_t i = 0; i < n; ++i) {
+    const int ci[3] = {coord(i, 0), coord(i, 1), coord(i, 2)};
+    for (int z = -1; z <= 1; ++z)
+      for (int y = -1; y <= 1; ++y)
+        for (int xx = -1; xx <= 1; ++xx) {
+          const int cz = ci[2] + z, cy = ci[1] + y, cx = ci[0] + xx;
+          if (cz < 0 || cy < 0 || cx < 0 || cz >= dims[2] || cy >= dims[1] || cx >= dims[0]) continue;
+          for (int64_t j : cells[((int64_t)cz * dims[1] + cy) * dims[0] + cx]) {
+            if (j <= i) continue;
+            const double d[3] = {pos[i * 3] - pos[j * 3], pos[i * 3 + 1] - pos[j * 3 + 1], pos[i * 3 + 2] - pos[j * 3 + 2]};
+            const double r = std::sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+            if (!(r > eps && r < R)) continue;
+            const double ki = mats[mat[i]].kcond, kj = mats[mat[j]].kcond;
+            const double kh = ki + kj > 0 ? 2 * ki * kj / (ki + kj) : 0.0;
+            pairs.push_back({i, j, (1 - r / R) * x->geometry * x->heat_rate * kh});
+          }
+        }
+  }
+  std::vector<double> budget(n, 0.0), heat(n, 0.0);
+  for (const Pair& p : pairs) {
+    budget[p.i] += p.g;
+    budget[p.j] += p.g;
+  }
+  for (int64_t i = 0; i < n; ++i)
+    budget[i] = budget[i] ? std::min(1.0, .45 * m[i] * mats[mat[i]].cp / (dt * budget[i])) : 1.0;
+  double exchanged = 0;
+  for (const Pair& p : pairs) {
+    const double q = (T[p.j] - T[p.i]) * p.g * dt * std::min(budget[p.i], budget[p.j]);
+    exchanged += std::fabs(q);
+    heat[p.i] += q;
+    heat[p.j] -= q;
+  }
+  for (int64_t i = 0; i < n; ++i) {
+    const OracleMaterial* mp = &mats[mat[i]];
+    h[i] += heat[i] / m[i];
+    if (x->ambient) h[i] -= (T[i] - x->ambient_T) * mp->cp * dt * x->ambient_rate;
+    bool liquid = false;
+    if (mp->latent > 0) {
+      const double start = mp->cp * mp->Tphase, end = start + mp->latent;
+      if (h[i] <= start) {
+        T[i] = h[i] / mp->cp;
+      } else if (h[i] >= end) {
+        liquid = true;
+        T[i] = (h[i] - mp->latent) / mp->cp;
+      } else {
+        liquid = melted[i] != 0;
+        T[i] = mp->Tphase;
+      }
+    } else {
+      T[i] = h[i] / mp->cp;
+    }
+    if (liquid != (melted[i] != 0)) {
+      melted[i] = liquid ? 1 : 0;
+      for (int k = 0; k < 9; ++k) {
+        F[i * 9 + k] = (k % 4 == 0) ? 1.0 : 0.0;
+        C[i * 9 + k] = 0.0;
+      }
+      ep[i] = 0;
+      if (jp) jp[i] = 1;
+      if (dilation) dilation[i] = 0;
+      if (liquid && pinned) pinned[i] = 0;
+    }
+  }
+  return exchanged;
 }
 
 }  // extern "C"

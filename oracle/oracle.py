@@ -26,7 +26,8 @@ class OracleMaterial(ctypes.Structure):
                 ("tRate", _D), ("tQ", _D), ("tN", _D), ("tStress", _D),
                 ("beta", _D), ("cp", _D), ("yieldStrain", _D), ("friction", _D),
                 ("cohesion", _D), ("slope", _D), ("dilatancy", _D), ("tension", _D), ("alpha", _D),
-                ("plateau", _D), ("gamma", _D), ("densify", _D), ("pbeta", _D), ("epsD", _D)]
+                ("plateau", _D), ("gamma", _D), ("densify", _D), ("pbeta", _D), ("epsD", _D),
+                ("kcond", _D), ("Tphase", _D), ("latent", _D)]
 
 
 class OracleScene(ctypes.Structure):
@@ -41,6 +42,12 @@ class OracleScene(ctypes.Structure):
 class OracleRegularizer(ctypes.Structure):
     """regularizeSolids parameters (src/three/solid-sampling.js:5-42); reference units: 2.8, 1, 8, 40."""
     _fields_ = [("spacing", _D), ("volume_unit", _D), ("max_speed", _D), ("rate", _D)]
+
+
+class OracleHeat(ctypes.Structure):
+    """exchangeHeat parameters; the reference's units: radius 8, geometry 20, heatRate 20."""
+    _fields_ = [("radius", _D), ("geometry", _D), ("heat_rate", _D), ("ambient", ctypes.c_int32),
+                ("pad", ctypes.c_int32), ("ambient_T", _D), ("ambient_rate", _D)]
 
 
 class OracleLedger(ctypes.Structure):
@@ -101,6 +108,11 @@ def lib():
                                     _P, _P, _P, _P, _P, _P, P(OracleLedger)]
         L.oracle_regularize.argtypes = [P(OracleRegularizer), P(OracleMaterial), ctypes.c_int64, _P, _P, _P, _P, _P,
                                         _P, _P, _D, _P, _P]
+        L.oracle_phase_enthalpy.argtypes = [_D, P(OracleMaterial)]
+        L.oracle_phase_enthalpy.restype = _D
+        L.oracle_exchange_heat.argtypes = [P(OracleHeat), P(OracleMaterial), ctypes.c_int64, _P, _P, _P, _P, _P, _P,
+                                           _P, _P, _P, _P, _P, _P, _D]
+        L.oracle_exchange_heat.restype = _D
         _lib = L
     return _lib
 
@@ -115,7 +127,7 @@ def _f64(a, shape=None):
 
 
 def material(model, mu=.4, lam=.4, plasticity=None, thermal=None, beta=0.0, cp=1.0, yield_strain=.025,
-             friction=35.0, pressure=None):
+             friction=35.0, pressure=None, conductivity=0.0, melting_point=0.0, latent_heat=0.0):
     """Oracle material. Defaults are the reference's units: mu = lambda = 0.4 (E = 1)."""
     p = dict(PLASTICITY_DEFAULTS, **(plasticity or {}))
     t = dict(THERMAL_DEFAULTS, **(thermal or {}))
@@ -127,7 +139,8 @@ def material(model, mu=.4, lam=.4, plasticity=None, thermal=None, beta=0.0, cp=1
                           beta=beta, cp=cp, yieldStrain=yield_strain, friction=friction,
                           cohesion=q["cohesion"], slope=q["slope"], dilatancy=q["dilatancy"], tension=q["tension"],
                           alpha=q["alpha"], plateau=q["plateau"], gamma=q["gamma"], densify=q["densify"],
-                          pbeta=q["beta"], epsD=q["epsD"])
+                          pbeta=q["beta"], epsD=q["epsD"], kcond=conductivity, Tphase=melting_point,
+                          latent=latent_heat)
 
 
 def hardening(jp):
@@ -297,6 +310,28 @@ class OracleState:
         lib().oracle_regularize(ctypes.byref(rg), self.mats, self.n, _ptr(self.x), _ptr(self.F), _ptr(self.jp),
                                 _ptr(self.V), _ptr(self.m), _ptr(self.mat), _ptr(self.pinned), dt, _ptr(lo), _ptr(hi))
 
+    def init_enthalpy(self):
+        """Simulation3's enthalpy and molten flags from the temperatures (phaseEnthalpy)."""
+        L = lib()
+        self.h = np.array([L.oracle_phase_enthalpy(float(self.T[i]), ctypes.byref(self.mats[self.mat[i]]))
+                           for i in range(self.n)])
+        self.melted = np.array([1 if (self.mats[self.mat[i]].latent > 0 and self.T[i] > self.mats[self.mat[i]].Tphase)
+                                else 0 for i in range(self.n)], dtype=np.uint8)
+
+    def exchange_heat(self, dt, radius=8.0, geometry=20.0, heat_rate=20.0, ambient=False, ambient_T=15.0,
+                      ambient_rate=.003):
+        """exchangeHeat over the pairs closer than radius; returns the exchanged heat (sum |Q|)."""
+        if not hasattr(self, "h"):
+            self.init_enthalpy()
+        x = OracleHeat(radius=radius, geometry=geometry, heat_rate=heat_rate, ambient=int(ambient),
+                       ambient_T=ambient_T, ambient_rate=ambient_rate)
+        if self.pinned is None:
+            self.pinned = np.zeros(self.n, dtype=np.uint8)
+        return lib().oracle_exchange_heat(ctypes.byref(x), self.mats, self.n, _ptr(self.x), _ptr(self.T), _ptr(self.h),
+                                          _ptr(self.melted), _ptr(self.m), _ptr(self.mat), _ptr(self.pinned),
+                                          _ptr(self.F), _ptr(self.C), _ptr(self.ep), _ptr(self.jp),
+                                          _ptr(self.dilation), dt)
+
     def ledger(self):
         L = OracleLedger()
         lib().oracle_ledger(ctypes.byref(self.sc), self.mats, self.n, _ptr(self.x), _ptr(self.v),
@@ -335,9 +370,17 @@ def material_from(mat):
     return material(mat.model, mu=mat.mu, lam=mat.lam)
 
 
+def _with_heat(om, mat):
+    om.cp = getattr(mat, "specific_heat", om.cp)
+    om.kcond = getattr(mat, "conductivity", 0.0)
+    om.Tphase = getattr(mat, "melting_point", 0.0)
+    om.latent = getattr(mat, "latent_heat", 0.0)
+    return om
+
+
 def state_from_scene(scene):
     """OracleState for a mpm_b200.scenes.Scene (with its grid heat conduction, if any)."""
-    st = OracleState(scene, [material_from(m) for m in scene.materials])
+    st = OracleState(scene, [_with_heat(material_from(m), m) for m in scene.materials])
     cond = scene.meta.get("conduction") if scene.meta else None
     if cond:
         st.set_conduction(cond["k"], cond["rho"], cond["cp"])

@@ -14,7 +14,7 @@
 
 #include "mpm_b200.h"
 #include "mpm_internal.h"
-#include "regularize.h"
+#include "pairs.h"
 
 using mpm::Ctx;
 using mpm::MaterialDev;
@@ -105,6 +105,12 @@ struct mpm_handle {
   mpm::RegBufs rbufs{};
   mpm::RegDev rdev{};
   bool reg_dirty = true;   // domain, scenes or spacing changed since the scratch was laid out
+  // particle-pair heat exchange scratch, laid out for heat_radius
+  void* hblock = nullptr;  size_t hblock_bytes = 0;
+  mpm::HeatBufs hbufs{};
+  mpm::HeatDev hdev{};
+  double heat_radius = 0;
+  double* host_exchanged = nullptr;  // pinned readback
   // profiling: event pairs around launches while enabled
   bool profiling = false;
   std::vector<cudaEvent_t> ev_pool;
@@ -228,6 +234,12 @@ static int free_device(mpm_handle* h) {
   h->rblock = nullptr;
   h->rblock_bytes = 0;
   h->reg_dirty = true;
+  if (h->hblock) cudaFree(h->hblock);
+  h->hblock = nullptr;
+  h->hblock_bytes = 0;
+  h->heat_radius = 0;
+  if (h->host_exchanged) cudaFreeHost(h->host_exchanged);
+  h->host_exchanged = nullptr;
   if (h->host_ctrl) cudaFreeHost(h->host_ctrl);
   if (h->host_ledger) cudaFreeHost(h->host_ledger);
   h->pblock = h->gblock = h->snap = h->staging = nullptr;
@@ -252,6 +264,8 @@ static size_t carve_particles(char* base, int64_t cap, mpm::Particles& p) {
   p.m = c.take<float>(cap); p.V = c.take<float>(cap);
   p.ep = c.take<float>(cap); p.T = c.take<float>(cap);
   p.aux = c.take<float>(cap);
+  p.latent = c.take<float>(cap);
+  p.melted = c.take<unsigned char>(cap);
   p.mat = c.take<unsigned short>(cap);
   p.pinned = c.take<unsigned char>(cap);
   p.id = c.take<unsigned>(cap);
@@ -325,6 +339,7 @@ static int alloc_grid(mpm_handle* h) {
     return align_up(cv.off, 256);
   };
   h->reg_dirty = true;  // neighbour cells follow the scenes' grids
+  h->heat_radius = 0;
   Ctx probe{};
   void* t;
   SceneDev* sp;
@@ -495,6 +510,9 @@ static mpm::MaterialExt to_device_ext(const mpm_material& m) {
   d.df_densify = static_cast<float>(m.df_densify);
   d.df_beta = static_cast<float>(m.df_beta);
   d.df_inv_epsd = m.df_eps_d > 0 ? static_cast<float>(1.0 / m.df_eps_d) : 0.f;
+  d.conductivity = static_cast<float>(m.conductivity);
+  d.melting_point = static_cast<float>(m.melting_point);
+  d.latent = m.latent_heat > 0 ? static_cast<float>(m.latent_heat) : 0.f;
   return d;
 }
 
@@ -548,6 +566,17 @@ static int validate_material(const mpm_material* m, std::string& why) {
                         !(m->df_gamma >= 0) || !(m->df_densify > 0) || !(m->df_beta >= 1 && m->df_beta <= 5) ||
                         !(m->df_eps_d >= 0.05 && m->df_eps_d <= 3))) {
     why = "Deshpande-Fleck foam needs alpha in [0.05, sqrt(4.5)], plateau, densify > 0, gamma >= 0, beta in [1, 5], eps_D in [0.05, 3]";
+    return MPM_ERR_INVALID_ARG;
+  }
+  // src/three/phase-change.js:4-9 (melting point in [-100, 2000], latent heat in [1000, 2e6] when
+  // enabled) in the caller's units; here: finite, latent heat >= 0, conductivity >= 0
+  if (!(m->conductivity >= 0) || !std::isfinite(m->conductivity) || !(m->latent_heat >= 0) ||
+      !std::isfinite(m->latent_heat) || !std::isfinite(m->melting_point)) {
+    why = "conductivity and latent heat must be finite and >= 0, the melting point finite";
+    return MPM_ERR_INVALID_ARG;
+  }
+  if (m->latent_heat > 0 && !(m->specific_heat > 0)) {
+    why = "phase change needs a specific heat > 0";
     return MPM_ERR_INVALID_ARG;
   }
   if (m->heat_fraction < 0 || m->heat_fraction > 1) {
@@ -736,23 +765,26 @@ static int ensure_staging(mpm_handle* h, size_t bytes) {
 }
 
 // Copies the caller's host arrays into device staging; fills ptrs with device addresses (or null).
-// Staged arrays: 0-2 x, y, z; 3-5 v; 6 mass; 7 volume; 8 T; 9 plastic; 10 F; 11 C; 12 Jp; 13 dilation.
-constexpr int kStaged = 14;
+// Staged arrays: 0-2 x, y, z; 3-5 v; 6 mass; 7 volume; 8 T; 9 plastic; 10 F; 11 C; 12 Jp; 13 dilation;
+// 14 enthalpy.
+constexpr int kStaged = 15;
 static inline int staged_comps(int k) { return k == 10 || k == 11 ? 9 : 1; }
 
 static int stage_in(mpm_handle* h, int64_t n, const mpm_particles* p, void* ptrs[kStaged], const int** mat_dev,
-                    const unsigned char** pin_dev, unsigned fields) {
+                    const unsigned char** pin_dev, unsigned fields, const unsigned char** melt_dev = nullptr) {
   const size_t es = p->dtype == MPM_F32 ? 4 : 8;
   const void* src[kStaged] = {p->x, p->y, p->z, p->vx, p->vy, p->vz, p->mass, p->volume, p->temperature, p->plastic,
-                              p->F, p->C, p->jp, p->dilation};
+                              p->F, p->C, p->jp, p->dilation, p->enthalpy};
   const unsigned need[kStaged] = {mpm::kFieldPos, mpm::kFieldPos, mpm::kFieldPos, mpm::kFieldVel, mpm::kFieldVel,
                                   mpm::kFieldVel, mpm::kFieldMass, mpm::kFieldVolume, mpm::kFieldTemp,
-                                  mpm::kFieldPlastic, mpm::kFieldF, mpm::kFieldC, mpm::kFieldAux, mpm::kFieldAux};
+                                  mpm::kFieldPlastic, mpm::kFieldF, mpm::kFieldC, mpm::kFieldAux, mpm::kFieldAux,
+                                  mpm::kFieldTemp};
   size_t total = 0;
   for (int k = 0; k < kStaged; ++k)
     if (src[k] && (fields & need[k])) total += align_up(staged_comps(k) * n * es, 256);
   if ((fields & mpm::kFieldMass) && p->material) total += align_up(n * 4, 256);
   if ((fields & mpm::kFieldMass) && p->pinned) total += align_up(n, 256);
+  if ((fields & mpm::kFieldTemp) && p->melted && melt_dev) total += align_up(n, 256);
   int rc = ensure_staging(h, std::max<size_t>(total, 256));
   if (rc != MPM_OK) return rc;
   char* base = static_cast<char*>(h->staging);
@@ -775,6 +807,12 @@ static int stage_in(mpm_handle* h, int64_t n, const mpm_particles* p, void* ptrs
   if ((fields & mpm::kFieldMass) && p->pinned) {
     *pin_dev = reinterpret_cast<const unsigned char*>(base + off);
     MPM_CUDA(h, cudaMemcpyAsync(base + off, p->pinned, n, cudaMemcpyHostToDevice, h->stream));
+    off += align_up(n, 256);
+  }
+  if (melt_dev) *melt_dev = nullptr;
+  if ((fields & mpm::kFieldTemp) && p->melted && melt_dev) {
+    *melt_dev = reinterpret_cast<const unsigned char*>(base + off);
+    MPM_CUDA(h, cudaMemcpyAsync(base + off, p->melted, n, cudaMemcpyHostToDevice, h->stream));
     off += align_up(n, 256);
   }
   MPM_CUDA(h, cudaMemcpyAsync(h->dptr_table, ptrs, kStaged * sizeof(void*), cudaMemcpyHostToDevice, h->stream));
@@ -825,8 +863,9 @@ int mpm_upload_particles(mpm_handle* h, int64_t n, const mpm_particles* p) {
   void* ptrs[kStaged];
   const int* mat_dev;
   const unsigned char* pin_dev;
+  const unsigned char* melt_dev;
   const unsigned all = 0x1ffu;
-  int rc = stage_in(h, n, p, ptrs, &mat_dev, &pin_dev, all);
+  int rc = stage_in(h, n, p, ptrs, &mat_dev, &pin_dev, all, &melt_dev);
   if (rc != MPM_OK) return rc;
   h->ctx.n = n;
   h->ctx.has_pinned = pinned_any ? 1 : 0;
@@ -838,7 +877,7 @@ int mpm_upload_particles(mpm_handle* h, int64_t n, const mpm_particles* p) {
     // scene table already on the device (alloc_grid); each particle takes its scene's material
     { ProfScope ps(h, -1);
       mpm::launch_upload_convert(h->ctx, h->stream, n, p->dtype, reinterpret_cast<const void* const*>(h->dptr_table),
-                                 nullptr, pin_dev, all, false); }
+                                 nullptr, pin_dev, all, false, melt_dev); }
     MPM_CUDA(h, cudaGetLastError());
     h->n = n;
     h->uploaded = true;
@@ -859,7 +898,7 @@ int mpm_upload_particles(mpm_handle* h, int64_t n, const mpm_particles* p) {
   MPM_CUDA(h, cudaMemcpyAsync(const_cast<SceneDev*>(h->ctx.scenes), &tmp, sizeof(SceneDev), cudaMemcpyHostToDevice, h->stream));
   { ProfScope ps(h, -1);
     mpm::launch_upload_convert(h->ctx, h->stream, n, p->dtype, reinterpret_cast<const void* const*>(h->dptr_table), mat_dev,
-                               pin_dev, all, false); }
+                               pin_dev, all, false, melt_dev); }
   MPM_CUDA(h, cudaGetLastError());
   MPM_CUDA(h, cudaMemcpyAsync(const_cast<SceneDev*>(h->ctx.scenes), &h->scene, sizeof(SceneDev), cudaMemcpyHostToDevice,
                               h->stream));
@@ -882,6 +921,7 @@ static unsigned download_fields(const mpm_particles* p) {
   if (p->F) f |= mpm::kFieldF;
   if (p->C) f |= mpm::kFieldC;
   if (p->jp || p->dilation) f |= mpm::kFieldAux;
+  if (p->enthalpy || p->melted) f |= mpm::kFieldTemp;
   return f;
 }
 
@@ -893,10 +933,11 @@ int mpm_download_particles(mpm_handle* h, const mpm_particles* p) {
   const size_t es = p->dtype == MPM_F32 ? 4 : 8;
   const unsigned fields = download_fields(p);
   void* dst[kStaged] = {p->x, p->y, p->z, p->vx, p->vy, p->vz, p->mass, p->volume, p->temperature, p->plastic,
-                        p->F, p->C, p->jp, p->dilation};
+                        p->F, p->C, p->jp, p->dilation, p->enthalpy};
   size_t total = 0;
   for (int k = 0; k < kStaged; ++k)
     if (dst[k]) total += align_up(staged_comps(k) * n * es, 256);
+  if (p->melted) total += align_up(n, 256);
   int rc = ensure_staging(h, std::max<size_t>(total, 256));
   if (rc != MPM_OK) return rc;
   void* dev[kStaged];
@@ -913,6 +954,12 @@ int mpm_download_particles(mpm_handle* h, const mpm_particles* p) {
   MPM_CUDA(h, cudaGetLastError());
   for (int k = 0; k < kStaged; ++k)
     if (dst[k]) MPM_CUDA(h, cudaMemcpyAsync(dst[k], dev[k], staged_comps(k) * n * es, cudaMemcpyDeviceToHost, h->stream));
+  if (p->melted) {  // molten flags by caller index (u8 in the staging tail)
+    unsigned char* mdev = static_cast<unsigned char*>(h->staging) + off;
+    MPM_CUDA(h, cudaMemsetAsync(mdev, 0, n, h->stream));
+    { ProfScope ps(h, -1); mpm::launch_download_melted(h->ctx, h->stream, n, mdev); }
+    MPM_CUDA(h, cudaMemcpyAsync(p->melted, mdev, n, cudaMemcpyDeviceToHost, h->stream));
+  }
   MPM_CUDA(h, cudaStreamSynchronize(h->stream));
   return MPM_OK;
 }
@@ -1238,6 +1285,94 @@ int mpm_regularize(mpm_handle* h, double dt) {
   return MPM_OK;
 }
 
+// Lays out the heat-exchange scratch for cells one radius wide over each scene's grid.
+static int ensure_heat(mpm_handle* h, double radius) {
+  if (h->hblock && h->heat_radius == radius) return MPM_OK;
+  const int ns = static_cast<int>(h->scenes.size());
+  std::vector<mpm::RegScene> rs(ns);
+  long long cells = 0;
+  for (int s = 0; s < ns; ++s) {
+    const SceneDev& sc = h->scenes[s];
+    long long k = 1;
+    for (int a = 0; a < 3; ++a) {
+      const double ext = (sc.dims[a] - 1) * static_cast<double>(sc.H);
+      rs[s].nc[a] = static_cast<int>(std::min(1.0e9, std::floor(ext / radius))) + 1;
+      k *= rs[s].nc[a];
+    }
+    rs[s].cell_base = cells;
+    cells += k;
+    if (cells > (1ll << 30)) return fail(h, MPM_ERR_INVALID_ARG, "heat-exchange radius too small for the grid");
+  }
+  const int64_t cap = h->cap;
+  const size_t nb = mpm::reg_scan_blocks(cells);
+  auto lay = [&](char* base, mpm::HeatBufs& b, mpm::RegScene** scenes) {
+    Carver cv{base};
+    *scenes = cv.take<mpm::RegScene>(ns);
+    b.count = cv.take<unsigned>(cells);
+    b.start = cv.take<unsigned>(cells);
+    b.cursor = cv.take<unsigned>(cells);
+    b.block_sums = cv.take<unsigned>(nb + 1);
+    b.exchanged = cv.take<double>(1);
+    b.cell_of = cv.take<unsigned>(cap);
+    b.sorted = cv.take<unsigned>(cap);
+    b.pos_sorted = cv.take<uint4>(cap);
+    b.prop_sorted = cv.take<float2>(cap);
+    b.budget = cv.take<float>(cap);
+    return align_up(cv.off, 256);
+  };
+  mpm::HeatBufs probe{};
+  mpm::RegScene* sp = nullptr;
+  const size_t bytes = lay(nullptr, probe, &sp);
+  if (h->hblock) cudaFree(h->hblock);
+  h->hblock = nullptr;
+  h->heat_radius = 0;
+  if (cudaMalloc(&h->hblock, bytes) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(h, MPM_ERR_OUT_OF_MEMORY, "heat-exchange scratch");
+  }
+  if (!h->host_exchanged && cudaMallocHost(&h->host_exchanged, sizeof(double)) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(h, MPM_ERR_OUT_OF_MEMORY, "heat-exchange readback");
+  }
+  h->hblock_bytes = bytes;
+  lay(static_cast<char*>(h->hblock), h->hbufs, &sp);
+  MPM_CUDA(h, cudaMemcpyAsync(sp, rs.data(), sizeof(mpm::RegScene) * ns, cudaMemcpyHostToDevice, h->stream));
+  MPM_CUDA(h, cudaStreamSynchronize(h->stream));  // rs is a host temporary
+  h->hdev.scenes = sp;
+  h->hdev.cells = cells;
+  h->heat_radius = radius;
+  return MPM_OK;
+}
+
+int mpm_exchange_heat(mpm_handle* h, const mpm_heat_exchange* x, double dt, double* exchanged) {
+  if (!h || !x) return MPM_ERR_INVALID_ARG;
+  if (!h->uploaded) return fail(h, MPM_ERR_STATE, "no particles uploaded");
+  if (!(x->radius > 0) || !std::isfinite(x->radius) || !(x->geometry >= 0) || !(x->heat_rate >= 0) ||
+      !(dt >= 0) || !std::isfinite(dt) || !std::isfinite(x->ambient_T) || !(x->ambient_rate >= 0))
+    return fail(h, MPM_ERR_INVALID_ARG, "heat exchange needs radius > 0, geometry, heat_rate, dt >= 0");
+  if (exchanged) *exchanged = 0;
+  if (h->n == 0) return MPM_OK;
+  int rc = ensure_heat(h, x->radius);
+  if (rc != MPM_OK) return rc;
+  mpm::HeatDev hd = h->hdev;
+  hd.inv_hc = static_cast<float>(1.0 / x->radius);
+  hd.radius = static_cast<float>(x->radius);
+  hd.eps = static_cast<float>(x->radius * 1.25e-7);  // 1e-6 of the reference's 8-unit radius
+  hd.geom_rate = static_cast<float>(x->geometry * x->heat_rate);
+  hd.dt = static_cast<float>(dt);
+  hd.ambient = x->ambient ? 1 : 0;
+  hd.ambient_T = static_cast<float>(x->ambient_T);
+  hd.ambient_rate = static_cast<float>(x->ambient_rate);
+  h->ctx.n = h->n;
+  { ProfScope ps(h, -1); mpm::launch_exchange_heat(h->ctx, hd, h->hbufs, h->stream); }
+  MPM_CUDA(h, cudaGetLastError());
+  MPM_CUDA(h, cudaMemcpyAsync(h->host_exchanged, h->hbufs.exchanged, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  MPM_CUDA(h, cudaStreamSynchronize(h->stream));
+  if (exchanged) *exchanged = *h->host_exchanged;
+  h->grid_valid = false;   // temperatures and possibly deformation changed: the next step re-scatters
+  return MPM_OK;
+}
+
 int mpm_regularize_host(mpm_handle* h, const mpm_particles* io, double dt) {
   if (!h || !io) return MPM_ERR_INVALID_ARG;
   if (h->batch) return fail(h, MPM_ERR_STATE, "single-scene call on a batch handle");
@@ -1415,8 +1550,8 @@ int mpm_checkpoint_save(mpm_handle* h, const char* path) {
   const mpm::Particles& p = h->ctx.p;
   struct Arr { const void* d; size_t es; int comps; } arrs[] = {
       {p.qx, 4, 1}, {p.qy, 4, 1}, {p.qz, 4, 1}, {p.vx, 4, 1}, {p.vy, 4, 1}, {p.vz, 4, 1}, {p.C, 4, 9}, {p.D, 4, 9},
-      {p.m, 4, 1}, {p.V, 4, 1}, {p.ep, 4, 1}, {p.T, 4, 1}, {p.aux, 4, 1}, {p.mat, 2, 1}, {p.pinned, 1, 1},
-      {p.id, 4, 1}};
+      {p.m, 4, 1}, {p.V, 4, 1}, {p.ep, 4, 1}, {p.T, 4, 1}, {p.aux, 4, 1}, {p.latent, 4, 1}, {p.melted, 1, 1},
+      {p.mat, 2, 1}, {p.pinned, 1, 1}, {p.id, 4, 1}};
   std::vector<char> buf;
   cudaStreamSynchronize(h->stream);
   for (const Arr& a : arrs) {
@@ -1465,8 +1600,8 @@ int mpm_checkpoint_load(mpm_handle* h, const char* path) {
   const mpm::Particles& p = h->ctx.p;
   struct Arr { void* d; size_t es; int comps; } arrs[] = {
       {p.qx, 4, 1}, {p.qy, 4, 1}, {p.qz, 4, 1}, {p.vx, 4, 1}, {p.vy, 4, 1}, {p.vz, 4, 1}, {p.C, 4, 9}, {p.D, 4, 9},
-      {p.m, 4, 1}, {p.V, 4, 1}, {p.ep, 4, 1}, {p.T, 4, 1}, {p.aux, 4, 1}, {p.mat, 2, 1}, {p.pinned, 1, 1},
-      {p.id, 4, 1}};
+      {p.m, 4, 1}, {p.V, 4, 1}, {p.ep, 4, 1}, {p.T, 4, 1}, {p.aux, 4, 1}, {p.latent, 4, 1}, {p.melted, 1, 1},
+      {p.mat, 2, 1}, {p.pinned, 1, 1}, {p.id, 4, 1}};
   std::vector<char> buf;
   cudaStreamSynchronize(h->stream);
   for (const Arr& a : arrs) {

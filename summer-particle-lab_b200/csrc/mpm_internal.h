@@ -96,6 +96,8 @@ struct Particles {
   float* Dc[9];
   float *m, *V, *ep, *T;
   float* aux;       // Jp - 1 (snow, pressure models) or the dilation (sand); 0 for the other laws
+  float* latent;    // molten fraction of a phase-change material on its latent plateau (0..1)
+  unsigned char* melted;  // 1 once a phase-change material has fully melted
   unsigned short* mat;
   unsigned char* pinned;
   unsigned* id;     // caller's index of the particle in this home slot
@@ -177,7 +179,9 @@ void launch_g2p2g(const Ctx& c, cudaStream_t st, int grid_blocks, bool scatter);
 void launch_ledger(const Ctx& c, cudaStream_t st, double* partials, int blocks, double* out);
 void launch_grid_debug(const Ctx& c, cudaStream_t st, int scene, float dt, double* mass, double* mom);
 void launch_upload_convert(const Ctx& c, cudaStream_t st, long long n, int dtype, const void* const* src,
-                           const int* material, const unsigned char* pinned, unsigned fields, bool by_id);
+                           const int* material, const unsigned char* pinned, unsigned fields, bool by_id,
+                           const unsigned char* melted = nullptr);
+void launch_download_melted(const Ctx& c, cudaStream_t st, long long n, unsigned char* out);
 void launch_download_convert(const Ctx& c, cudaStream_t st, long long n, int dtype, void* const* dst,
                              unsigned fields);
 void launch_permute(const Ctx& c, const Particles& dst, cudaStream_t st);

@@ -1822,7 +1822,7 @@ void launch_grid_debug(const Ctx& c, cudaStream_t st, int scene, float dt, doubl
 // caller's order (id = i); with by_id the caller's particle id[i] is read into home slot i.
 template <typename Tsrc>
 __global__ void k_upload(Ctx c, long long n, const Tsrc* const* src, const int* material,
-                         const unsigned char* pinned, unsigned fields, int by_id) {
+                         const unsigned char* pinned, unsigned fields, int by_id, const unsigned char* melted) {
   const long long cap = c.p.cap;
   for (long long h = blockIdx.x * (long long)blockDim.x + threadIdx.x; h < n; h += (long long)gridDim.x * blockDim.x) {
     const long long i = by_id ? (long long)c.p.id[h] : h;
@@ -1844,7 +1844,33 @@ __global__ void k_upload(Ctx c, long long n, const Tsrc* const* src, const int* 
     }
     if (fields & kFieldMass) c.p.m[h] = (float)src[6][i];
     if (fields & kFieldVolume) c.p.V[h] = (float)src[7][i];
-    if (fields & kFieldTemp) c.p.T[h] = src[8] ? (float)src[8][i] : 0.f;
+    if (fields & kFieldTemp) {
+      // temperature, or the decode of the enthalpy (src/three/phase-change.js:12-18); the molten
+      // flag is the hint on a latent plateau, else follows from T > melting point (phaseEnthalpy)
+      const int mi = material ? sc.mat_base + material[i] : sc.mat_base;
+      const MaterialExt& xt = c.mats_ext[mi];
+      const double cp = c.mats[mi].cp;
+      double T = src[8] ? (double)src[8][i] : 0.0;
+      float f = 0.f;
+      unsigned char mol = melted ? melted[i] : 0;
+      if (src[14] && xt.latent > 0.f) {
+        const double hh = (double)src[14][i], start = cp * xt.melting_point, end = start + xt.latent;
+        if (hh <= start) { T = hh / cp; f = 0.f; mol = 0; }
+        else if (hh >= end) { T = (hh - xt.latent) / cp; f = 1.f; mol = 1; }
+        else { T = xt.melting_point; f = (float)((hh - start) / xt.latent); }
+      } else if (src[14] && cp > 0.0) {
+        T = (double)src[14][i] / cp;
+        mol = 0;
+      } else if (xt.latent > 0.f) {
+        mol = T > xt.melting_point ? 1 : 0;
+        f = mol ? 1.f : 0.f;
+      } else {
+        mol = 0;
+      }
+      c.p.T[h] = (float)T;
+      c.p.latent[h] = f;
+      c.p.melted[h] = mol;
+    }
     if (fields & kFieldPlastic) c.p.ep[h] = src[9] ? (float)src[9][i] : 0.f;
     if (fields & kFieldAux) {
       // aux = Jp - 1 (models 2, 8, 9) or the dilation (model 3)
@@ -1868,15 +1894,16 @@ __global__ void k_upload(Ctx c, long long n, const Tsrc* const* src, const int* 
 }
 
 void launch_upload_convert(const Ctx& c, cudaStream_t st, long long n, int dtype, const void* const* src,
-                           const int* material, const unsigned char* pinned, unsigned fields, bool by_id) {
+                           const int* material, const unsigned char* pinned, unsigned fields, bool by_id,
+                           const unsigned char* melted) {
   if (n <= 0) return;
   const int blocks = static_cast<int>((n + 255) / 256 < 65536 ? (n + 255) / 256 : 65536);
   if (dtype == 0)
     k_upload<double><<<blocks, 256, 0, st>>>(c, n, reinterpret_cast<const double* const*>(src), material, pinned, fields,
-                                             by_id ? 1 : 0);
+                                             by_id ? 1 : 0, melted);
   else
     k_upload<float><<<blocks, 256, 0, st>>>(c, n, reinterpret_cast<const float* const*>(src), material, pinned, fields,
-                                            by_id ? 1 : 0);
+                                            by_id ? 1 : 0, melted);
 }
 
 // Rewrites the state in sort order: dst[i] = current[perm[i]] for every field, then perm = identity,
@@ -1893,6 +1920,7 @@ __global__ void k_permute(Ctx c, Particles d) {
       d.Dc[e][i] = s.Dc[e][h];
     }
     d.m[i] = s.m[h]; d.V[i] = s.V[h]; d.ep[i] = s.ep[h]; d.T[i] = s.T[h]; d.aux[i] = s.aux[h];
+    d.latent[i] = s.latent[h]; d.melted[i] = s.melted[h];
     d.mat[i] = s.mat[h]; d.pinned[i] = s.pinned[h]; d.id[i] = s.id[h];
     s.perm[i] = static_cast<unsigned>(i);
   }
@@ -1921,6 +1949,7 @@ __device__ void copy_slot(const Particles& p, long long dst, long long src) {
     p.Dc[e][dst] = p.Dc[e][src];
   }
   p.m[dst] = p.m[src]; p.V[dst] = p.V[src]; p.ep[dst] = p.ep[src]; p.T[dst] = p.T[src]; p.aux[dst] = p.aux[src];
+  p.latent[dst] = p.latent[src]; p.melted[dst] = p.melted[src];
   p.mat[dst] = p.mat[src]; p.pinned[dst] = p.pinned[src]; p.id[dst] = p.id[src];
 }
 
@@ -1975,7 +2004,13 @@ __global__ void k_download(Ctx c, long long n, Tdst* const* dst, unsigned fields
     }
     if (fields & kFieldMass) dst[6][i] = (Tdst)c.p.m[h];
     if (fields & kFieldVolume) dst[7][i] = (Tdst)c.p.V[h];
-    if (fields & kFieldTemp) dst[8][i] = (Tdst)c.p.T[h];
+    if (fields & kFieldTemp) {
+      if (dst[8]) dst[8][i] = (Tdst)c.p.T[h];
+      if (dst[14]) {  // h = cp T (+ the molten fraction of the latent heat)
+        const int mi = c.single_material ? sc.mat_base : c.p.mat[h];
+        dst[14][i] = (Tdst)((double)c.mats[mi].cp * c.p.T[h] + (double)c.p.latent[h] * c.mats_ext[mi].latent);
+      }
+    }
     if (fields & kFieldPlastic) dst[9][i] = (Tdst)c.p.ep[h];
     if (fields & kFieldAux) {
       const int model = c.mats[c.single_material ? sc.mat_base : c.p.mat[h]].model;
@@ -1989,6 +2024,17 @@ __global__ void k_download(Ctx c, long long n, Tdst* const* dst, unsigned fields
       if (fields & kFieldC) dst[11][i * 9 + e] = (Tdst)c.p.C[e * cap + h];
     }
   }
+}
+
+__global__ void k_download_melted(Ctx c, long long n, unsigned char* out) {
+  for (long long h = blockIdx.x * (long long)blockDim.x + threadIdx.x; h < n; h += (long long)gridDim.x * blockDim.x)
+    out[c.p.id[h]] = c.p.melted[h];
+}
+
+void launch_download_melted(const Ctx& c, cudaStream_t st, long long n, unsigned char* out) {
+  if (n <= 0) return;
+  const int blocks = static_cast<int>((n + 255) / 256 < 65536 ? (n + 255) / 256 : 65536);
+  k_download_melted<<<blocks, 256, 0, st>>>(c, n, out);
 }
 
 void launch_download_convert(const Ctx& c, cudaStream_t st, long long n, int dtype, void* const* dst, unsigned fields) {

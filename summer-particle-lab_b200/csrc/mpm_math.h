@@ -221,6 +221,9 @@ struct MaterialExt {
   float bulk;
   float dp_c, dp_a, dp_b, dp_T;
   float df_a2, df_B, df_plateau, df_gamma, df_densify, df_beta, df_inv_epsd;
+  // particle-pair heat exchange and enthalpy phase change (src/thermal.js:35-56,
+  // src/three/phase-change.js:4-18): conductivity, melting point, latent heat (0: no phase change)
+  float conductivity, melting_point, latent;
 };
 
 // Models whose state carries a second history scalar (aux): Jp - 1 for snow and the pressure

@@ -1,7 +1,9 @@
-// Solid position regularisation on the device (src/three/solid-sampling.js:5-42, regularizeSolids;
-// the reference's GPU twin is gpu/solver.py:565-648).
+// Particle-pair passes over a cell sort of the particles: the solid position regularisation
+// (src/three/solid-sampling.js:5-42, regularizeSolids; the reference's GPU twin is
+// gpu/solver.py:565-648) and the particle-pair heat exchange with the enthalpy phase change
+// (src/thermal.js:35-56, src/three/phase-change.js:12-18; GPU twin gpu/solver.py:775-811).
 //
-// Per pass:
+// Regularisation pass:
 //   k_reg_count    thread per particle: neighbour cell (cells as large as the largest target, two
 //                  spacings, so every pair closer than its target lies in the 27 surrounding
 //                  cells), target spacing from V J Jp, cell population
@@ -17,7 +19,7 @@
 // HBM traffic per particle: about 110 B (position, D, V, m, aux, id reads; the cell, target, shift
 // and packed scratch) plus the neighbour reads, contiguous runs of the packed copy that L1/L2 serve.
 #include "mpm_internal.h"
-#include "regularize.h"
+#include "pairs.h"
 
 namespace mpm {
 
@@ -238,7 +240,162 @@ __global__ void k_scan_add(unsigned* out, long long n, const unsigned* block_sum
     if (i + k < n) out[i + k] += add;
 }
 
+// ---- particle-pair heat exchange -------------------------------------------------------------
+// k_heat_count / scan / k_heat_scatter: cell sort (cells one radius wide) with a packed copy of
+//   position, temperature, conductivity and heat capacity in cell order
+// k_heat_budget: per particle the sum of its conductances g over pairs (eps < r < radius), and its
+//   budget min(1, 0.45 m cp / (dt sum g)) (1 without contacts)
+// k_heat_flow: per particle heat_i = sum_j (T_j - T_i) g dt min(b_i, b_j) — each pair's +Q / -Q
+//   gathered from both sides — then the enthalpy update, ambient loss and phase decode of the
+//   particle; |Q| summed over pairs (each seen twice: halved) in FP64.
+
+__global__ void k_heat_count(Ctx c, HeatDev hd, unsigned* cell_of, unsigned* count) {
+  for (long long h = blockIdx.x * (long long)blockDim.x + threadIdx.x; h < c.n; h += (long long)gridDim.x * blockDim.x) {
+    const int s = c.nscenes == 1 ? 0 : find_scene_by_particle(c.scenes, c.nscenes, h);
+    const SceneDev& sc = c.scenes[s];
+    const RegScene& rs = hd.scenes[s];
+    float x[3];
+    position(c.p, h, sc, x);
+    int cc[3];
+    for (int a = 0; a < 3; ++a) cc[a] = min(rs.nc[a] - 1, max(0, static_cast<int>(floorf(x[a] * hd.inv_hc))));
+    const unsigned cell = static_cast<unsigned>(rs.cell_base + ((long long)cc[2] * rs.nc[1] + cc[1]) * rs.nc[0] + cc[0]);
+    cell_of[h] = cell;
+    atomicAdd(&count[cell], 1u);
+  }
+}
+
+__global__ void k_heat_scatter(Ctx c, const unsigned* cell_of, const unsigned* start, unsigned* cursor, unsigned* sorted,
+                               uint4* pos_sorted, float2* prop_sorted) {
+  for (long long h = blockIdx.x * (long long)blockDim.x + threadIdx.x; h < c.n; h += (long long)gridDim.x * blockDim.x) {
+    const unsigned cell = cell_of[h];
+    const unsigned k = start[cell] + atomicAdd(&cursor[cell], 1u);
+    const int s = c.nscenes == 1 ? 0 : find_scene_by_particle(c.scenes, c.nscenes, h);
+    const int mi = c.single_material ? c.scenes[s].mat_base : c.p.mat[h];
+    sorted[k] = static_cast<unsigned>(h);
+    pos_sorted[k] = make_uint4(c.p.qx[h], c.p.qy[h], c.p.qz[h], __float_as_uint(c.p.T[h]));
+    prop_sorted[k] = make_float2(c.mats_ext[mi].conductivity, c.p.m[h] * c.mats[mi].cp);
+  }
+}
+
+// Visits the neighbours j of sorted particle ks within (eps, radius): fn(k, g) with the pair's
+// conductance g = (1 - r / radius) geometry heat_rate 2 k_i k_j / (k_i + k_j).
+template <typename Fn>
+__device__ __forceinline__ void heat_pairs(const Ctx& c, const HeatDev& hd, const unsigned* cell_of,
+                                           const unsigned* start, const unsigned* count, const uint4* pos_sorted,
+                                           const float2* prop_sorted, long long ks, unsigned i, Fn&& fn) {
+  const int s = c.nscenes == 1 ? 0 : find_scene_by_particle(c.scenes, c.nscenes, i);
+  const SceneDev& sc = c.scenes[s];
+  const RegScene& rs = hd.scenes[s];
+  const uint4 pi = pos_sorted[ks];
+  const float ki = prop_sorted[ks].x;
+  const float to_m = sc.H * kInvFixedOne;
+  const long long local = (long long)cell_of[i] - rs.cell_base;
+  const int cx = static_cast<int>(local % rs.nc[0]), cy = static_cast<int>((local / rs.nc[0]) % rs.nc[1]),
+            cz = static_cast<int>(local / ((long long)rs.nc[0] * rs.nc[1]));
+  for (int z = max(0, cz - 1); z <= min(rs.nc[2] - 1, cz + 1); ++z)
+    for (int y = max(0, cy - 1); y <= min(rs.nc[1] - 1, cy + 1); ++y)
+      for (int x = max(0, cx - 1); x <= min(rs.nc[0] - 1, cx + 1); ++x) {
+        const long long cell = rs.cell_base + ((long long)z * rs.nc[1] + y) * rs.nc[0] + x;
+        const unsigned b = start[cell], e = b + count[cell];
+        for (unsigned k = b; k < e; ++k) {
+          if (k == ks) continue;
+          const uint4 pj = pos_sorted[k];
+          const float dx = static_cast<float>(static_cast<int>(pi.x - pj.x)) * to_m;
+          const float dy = static_cast<float>(static_cast<int>(pi.y - pj.y)) * to_m;
+          const float dz = static_cast<float>(static_cast<int>(pi.z - pj.z)) * to_m;
+          const float r = sqrtf(dx * dx + dy * dy + dz * dz);
+          if (!(r > hd.eps && r < hd.radius)) continue;
+          const float kj = prop_sorted[k].x;
+          const float kh = ki + kj > 0.f ? 2.f * ki * kj / (ki + kj) : 0.f;
+          fn(k, (1.f - r / hd.radius) * hd.geom_rate * kh);
+        }
+      }
+}
+
+__global__ void k_heat_budget(Ctx c, HeatDev hd, const unsigned* cell_of, const unsigned* start, const unsigned* count,
+                              const unsigned* sorted, const uint4* pos_sorted, const float2* prop_sorted, float* budget) {
+  for (long long ks = blockIdx.x * (long long)blockDim.x + threadIdx.x; ks < c.n; ks += (long long)gridDim.x * blockDim.x) {
+    const unsigned i = sorted[ks];
+    double gsum = 0.0;
+    heat_pairs(c, hd, cell_of, start, count, pos_sorted, prop_sorted, ks, i, [&](unsigned, float g) { gsum += g; });
+    const double mcp = prop_sorted[ks].y;
+    budget[ks] = gsum > 0.0 ? static_cast<float>(fmin(1.0, 0.45 * mcp / (hd.dt * gsum))) : 1.f;
+  }
+}
+
+__global__ void k_heat_flow(Ctx c, HeatDev hd, const unsigned* cell_of, const unsigned* start, const unsigned* count,
+                            const unsigned* sorted, const uint4* pos_sorted, const float2* prop_sorted,
+                            const float* budget, double* exchanged) {
+  double absq = 0.0;
+  for (long long ks = blockIdx.x * (long long)blockDim.x + threadIdx.x; ks < c.n; ks += (long long)gridDim.x * blockDim.x) {
+    const unsigned i = sorted[ks];
+    const double Ti = __uint_as_float(pos_sorted[ks].w);
+    const float bi = budget[ks];
+    double heat = 0.0;
+    heat_pairs(c, hd, cell_of, start, count, pos_sorted, prop_sorted, ks, i, [&](unsigned k, float g) {
+      const double q = ((double)__uint_as_float(pos_sorted[k].w) - Ti) * g * hd.dt * fminf(bi, budget[k]);
+      heat += q;
+      absq += fabs(q);
+    });
+    // enthalpy update, ambient loss and the phase decode (src/thermal.js:51-55,
+    // src/three/phase-change.js:12-18, src/three/simulation.js:260-270)
+    const int s = c.nscenes == 1 ? 0 : find_scene_by_particle(c.scenes, c.nscenes, i);
+    const int mi = c.single_material ? c.scenes[s].mat_base : c.p.mat[i];
+    const MaterialExt& xt = c.mats_ext[mi];
+    const double cp = c.mats[mi].cp, L = xt.latent;
+    double hh = cp * Ti + (double)c.p.latent[i] * L + heat / c.p.m[i];
+    if (hd.ambient) hh -= (Ti - hd.ambient_T) * cp * hd.dt * hd.ambient_rate;
+    const unsigned char was = c.p.melted[i];
+    unsigned char liquid = 0;
+    double T;
+    float f = 0.f;
+    if (L > 0.0) {
+      const double st = cp * xt.melting_point, en = st + L;
+      if (hh <= st) { T = hh / cp; }
+      else if (hh >= en) { T = (hh - L) / cp; f = 1.f; liquid = 1; }
+      else { T = xt.melting_point; f = static_cast<float>((hh - st) / L); liquid = was; }
+    } else {
+      T = cp > 0.0 ? hh / cp : Ti;
+    }
+    c.p.T[i] = static_cast<float>(T);
+    c.p.latent[i] = f;
+    if (liquid != was) {
+      // MPM3.resetParticle on a phase switch; a molten particle is released (Simulation3.pin(i, false))
+      c.p.melted[i] = liquid;
+      for (int e = 0; e < 9; ++e) {
+        c.p.Cc[e][i] = 0.f;
+        c.p.Dc[e][i] = 0.f;
+      }
+      c.p.ep[i] = 0.f;
+      c.p.aux[i] = 0.f;
+      if (liquid) c.p.pinned[i] = 0;
+    }
+  }
+  // each pair was seen from both sides
+  for (int o = 16; o > 0; o >>= 1) absq += __shfl_xor_sync(0xffffffffu, absq, o);
+  if ((threadIdx.x & 31) == 0 && absq != 0.0) atomicAdd(exchanged, 0.5 * absq);
+}
+
 }  // namespace
+
+void launch_exchange_heat(const Ctx& c, const HeatDev& hd, const HeatBufs& b, cudaStream_t st) {
+  if (c.n <= 0) return;
+  const long long n = c.n;
+  const unsigned blocks = static_cast<unsigned>((n + 255) / 256 < 65536 ? (n + 255) / 256 : 65536);
+  cudaMemsetAsync(b.count, 0, sizeof(unsigned) * hd.cells, st);
+  cudaMemsetAsync(b.cursor, 0, sizeof(unsigned) * hd.cells, st);
+  cudaMemsetAsync(b.exchanged, 0, sizeof(double), st);
+  k_heat_count<<<blocks, 256, 0, st>>>(c, hd, b.cell_of, b.count);
+  const unsigned nb = static_cast<unsigned>(reg_scan_blocks(hd.cells));
+  k_scan_blocks<<<nb, kScanThreads, 0, st>>>(b.count, hd.cells, b.start, b.block_sums);
+  k_scan_top<<<1, kScanThreads, 0, st>>>(b.block_sums, static_cast<int>(nb));
+  k_scan_add<<<nb, 256, 0, st>>>(b.start, hd.cells, b.block_sums);
+  k_heat_scatter<<<blocks, 256, 0, st>>>(c, b.cell_of, b.start, b.cursor, b.sorted, b.pos_sorted, b.prop_sorted);
+  k_heat_budget<<<blocks, 256, 0, st>>>(c, hd, b.cell_of, b.start, b.count, b.sorted, b.pos_sorted, b.prop_sorted,
+                                        b.budget);
+  k_heat_flow<<<blocks, 256, 0, st>>>(c, hd, b.cell_of, b.start, b.count, b.sorted, b.pos_sorted, b.prop_sorted,
+                                      b.budget, b.exchanged);
+}
 
 size_t reg_scan_blocks(long long cells) { return static_cast<size_t>((cells + kScanSpan - 1) / kScanSpan); }
 

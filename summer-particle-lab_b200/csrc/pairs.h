@@ -1,4 +1,4 @@
-// Device side of the solid position regularisation (regularize.cu); internal, not part of the C ABI.
+// Device side of the particle-pair passes (pairs.cu): solid regularisation and heat exchange; internal.
 #pragma once
 #include <cstddef>
 
@@ -38,5 +38,28 @@ struct RegBufs {
 
 size_t reg_scan_blocks(long long cells);
 void launch_regularize(const Ctx& c, const RegDev& r, const RegBufs& b, cudaStream_t st);
+
+// Particle-pair heat exchange: neighbour cells one radius wide (RegScene layout), conductance
+// factor geometry * heat_rate, optional ambient loss.
+struct HeatDev {
+  const RegScene* scenes;
+  long long cells;
+  float inv_hc;         // 1 / radius
+  float radius, eps;    // pairs with eps < r < radius
+  float geom_rate;      // geometry * heat_rate
+  float dt;
+  int ambient;
+  float ambient_T, ambient_rate;
+};
+
+struct HeatBufs {
+  unsigned *cell_of, *count, *start, *cursor, *sorted, *block_sums;
+  uint4* pos_sorted;    // cell order: (qx, qy, qz, T bits)
+  float2* prop_sorted;  // cell order: (conductivity, m cp)
+  float* budget;        // cell order
+  double* exchanged;    // 1: sum over pairs of |Q|
+};
+
+void launch_exchange_heat(const Ctx& c, const HeatDev& hd, const HeatBufs& b, cudaStream_t st);
 
 }  // namespace mpm

@@ -40,7 +40,7 @@ class MpmMaterial(ctypes.Structure):
                 ("temperature_offset", _D), ("yield_strain", _D), ("friction_deg", _D),
                 ("dp_cohesion", _D), ("dp_slope", _D), ("dp_dilatancy", _D), ("dp_tension", _D),
                 ("df_alpha", _D), ("df_plateau", _D), ("df_gamma", _D), ("df_densify", _D), ("df_beta", _D),
-                ("df_eps_d", _D)]
+                ("df_eps_d", _D), ("conductivity", _D), ("melting_point", _D), ("latent_heat", _D)]
 
 
 class MpmRegularizer(ctypes.Structure):
@@ -52,7 +52,12 @@ class MpmParticles(ctypes.Structure):
     _fields_ = [("dtype", _I32), ("reserved", _I32), ("x", _P), ("y", _P), ("z", _P), ("vx", _P),
                 ("vy", _P), ("vz", _P), ("mass", _P), ("volume", _P), ("temperature", _P),
                 ("plastic", _P), ("F", _P), ("C", _P), ("material", _P), ("pinned", _P), ("jp", _P),
-                ("dilation", _P)]
+                ("dilation", _P), ("enthalpy", _P), ("melted", _P)]
+
+
+class MpmHeatExchange(ctypes.Structure):
+    _fields_ = [("radius", _D), ("geometry", _D), ("heat_rate", _D), ("ambient", _I32), ("reserved", _I32),
+                ("ambient_T", _D), ("ambient_rate", _D)]
 
 
 class MpmLedger(ctypes.Structure):
@@ -120,6 +125,7 @@ SIGNATURES = {
     "mpm_set_regularizer": (ctypes.c_int, [_P, ctypes.POINTER(MpmRegularizer)]),
     "mpm_regularize": (ctypes.c_int, [_P, _D]),
     "mpm_regularize_host": (ctypes.c_int, [_P, ctypes.POINTER(MpmParticles), _D]),
+    "mpm_exchange_heat": (ctypes.c_int, [_P, ctypes.POINTER(MpmHeatExchange), _D, ctypes.POINTER(_D)]),
     "mpm_get_stream": (ctypes.c_int, [_P, ctypes.POINTER(_P)]),
     "mpm_upload_particles": (ctypes.c_int, [_P, _I64, ctypes.POINTER(MpmParticles)]),
     "mpm_download_particles": (ctypes.c_int, [_P, ctypes.POINTER(MpmParticles)]),

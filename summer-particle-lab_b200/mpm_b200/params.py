@@ -116,6 +116,10 @@ class Material:
     df_densify: float = 1.0
     df_beta: float = 2.0
     df_eps_d: float = 0.7
+    # particle-pair heat exchange (W/m/K) and enthalpy phase change (enabled when latent_heat > 0)
+    conductivity: float = 0.0
+    melting_point: float = 0.0
+    latent_heat: float = 0.0
 
     def __post_init__(self):
         if self.model not in SUPPORTED_MODELS:

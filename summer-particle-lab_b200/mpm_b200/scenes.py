@@ -56,6 +56,8 @@ class Scene:
     pinned: np.ndarray = None
     jp: np.ndarray = None    # (n,) plastic volume ratio Jp of snow / pressure materials (default one)
     dilation: np.ndarray = None  # (n,) sand dilation history (default zero)
+    enthalpy: np.ndarray = None  # (n,) J/kg; when given it sets T (and the phase of phase-change materials)
+    melted: np.ndarray = None    # (n,) u8 molten flags of phase-change materials
     meta: dict = field(default_factory=dict)
 
     @property

@@ -41,7 +41,8 @@ def material_struct(m):
                        friction_deg=m.friction_deg, dp_cohesion=m.dp_cohesion, dp_slope=m.dp_slope,
                        dp_dilatancy=m.dp_dilatancy, dp_tension=m.dp_tension, df_alpha=m.df_alpha,
                        df_plateau=m.df_plateau, df_gamma=m.df_gamma, df_densify=m.df_densify, df_beta=m.df_beta,
-                       df_eps_d=m.df_eps_d)
+                       df_eps_d=m.df_eps_d, conductivity=m.conductivity, melting_point=m.melting_point,
+                       latent_heat=m.latent_heat)
 
 
 def _ptr(a):
@@ -87,6 +88,8 @@ class Solver:
         m, V = arr(scene.m), arr(scene.V)
         T, ep = arr(scene.T), arr(scene.ep)
         jp, dil = arr(getattr(scene, "jp", None)), arr(getattr(scene, "dilation", None))
+        enth = arr(getattr(scene, "enthalpy", None))
+        mel = None if getattr(scene, "melted", None) is None else np.ascontiguousarray(scene.melted, dtype=np.uint8)
         F = None if scene.F is None else np.ascontiguousarray(np.asarray(scene.F).reshape(n, 9), dtype=f)
         C = None if scene.C is None else np.ascontiguousarray(np.asarray(scene.C).reshape(n, 9), dtype=f)
         mat = np.ascontiguousarray(scene.mat, dtype=np.int32)
@@ -94,7 +97,8 @@ class Solver:
         p = MpmParticles(dtype=_lib.F64 if f == np.float64 else _lib.F32,
                          x=_ptr(cols[0]), y=_ptr(cols[1]), z=_ptr(cols[2]), vx=_ptr(cols[3]), vy=_ptr(cols[4]),
                          vz=_ptr(cols[5]), mass=_ptr(m), volume=_ptr(V), temperature=_ptr(T), plastic=_ptr(ep),
-                         F=_ptr(F), C=_ptr(C), material=_ptr(mat), pinned=_ptr(pin), jp=_ptr(jp), dilation=_ptr(dil))
+                         F=_ptr(F), C=_ptr(C), material=_ptr(mat), pinned=_ptr(pin), jp=_ptr(jp), dilation=_ptr(dil),
+                         enthalpy=_ptr(enth), melted=_ptr(mel))
         self._check(_lib.lib().mpm_upload_particles(self.h, n, ctypes.byref(p)))
         self.n = n
         cond = scene.meta.get("conduction") if scene.meta else None
@@ -119,7 +123,8 @@ class Solver:
             for k in ("vx", "vy", "vz"):
                 cols[k] = np.empty(n, dtype=f)
                 setattr(p, k, _ptr(cols[k]))
-        one = {"m": "mass", "V": "volume", "T": "temperature", "ep": "plastic", "jp": "jp", "dilation": "dilation"}
+        one = {"m": "mass", "V": "volume", "T": "temperature", "ep": "plastic", "jp": "jp", "dilation": "dilation",
+               "enthalpy": "enthalpy"}
         for k, name in one.items():
             if k in fields:
                 out[k] = np.empty(n, dtype=f)
@@ -128,6 +133,9 @@ class Solver:
             if k in fields:
                 out[k] = np.empty((n, 9), dtype=f)
                 setattr(p, k, _ptr(out[k]))
+        if "melted" in fields:
+            out["melted"] = np.empty(n, dtype=np.uint8)
+            p.melted = _ptr(out["melted"])
         self._check(_lib.lib().mpm_download_particles(self.h, ctypes.byref(p)))
         if "x" in fields:
             out["x"] = np.stack([cols["x"], cols["y"], cols["z"]], axis=1)
@@ -228,6 +236,15 @@ class Solver:
         r = _lib.MpmRegularizer(enabled=int(bool(enabled)), spacing=spacing, volume_unit=volume_unit,
                                 max_speed=max_speed, rate=rate)
         self._check(_lib.lib().mpm_set_regularizer(self.h, ctypes.byref(r)))
+
+    def exchange_heat(self, dt, radius, geometry=20.0, heat_rate=20.0, ambient=False, ambient_T=15.0,
+                      ambient_rate=.003):
+        """Particle-pair heat exchange (exchangeHeat) over dt; returns the exchanged heat (sum |Q|)."""
+        x = _lib.MpmHeatExchange(radius=radius, geometry=geometry, heat_rate=heat_rate, ambient=int(bool(ambient)),
+                                 ambient_T=ambient_T, ambient_rate=ambient_rate)
+        q = ctypes.c_double()
+        self._check(_lib.lib().mpm_exchange_heat(self.h, ctypes.byref(x), float(dt), ctypes.byref(q)))
+        return q.value
 
     def regularize(self, dt):
         """One regularisation pass now (regularizeSolids(s, dt) after a step)."""

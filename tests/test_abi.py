@@ -35,8 +35,8 @@ def test_abi_version_and_error_strings_need_no_gpu():
 def test_struct_layouts_match_header_sizes():
     # sizes follow from the header's field lists (all 8-byte aligned)
     assert ctypes.sizeof(_lib.MpmDomain) == 8 * 3 * 2 + 8 + 24 + 4 + 4 + 8 * 4 + 8
-    assert ctypes.sizeof(_lib.MpmMaterial) == 8 + 31 * 8
-    assert ctypes.sizeof(_lib.MpmParticles) == 8 + 16 * 8
+    assert ctypes.sizeof(_lib.MpmMaterial) == 8 + 34 * 8
+    assert ctypes.sizeof(_lib.MpmParticles) == 8 + 18 * 8
     assert ctypes.sizeof(_lib.MpmLedger) == 5 * 8 + 6 * 8 + 5 * 8 + 3 * 8
     assert ctypes.sizeof(_lib.SmpmSim) == 4 * 4 + 2 * 8 + 8 * 8
     assert ctypes.sizeof(_lib.SmpmStats) == 4 * 4 + 3 * 8
