@@ -28,10 +28,11 @@ class Sim3:
 
     def __init__(self, capacity=CAPACITY3):
         self.capacity = capacity
-        for k in ("x", "y", "z", "vx", "vy", "vz", "mass", "volume", "temperature"):
+        for k in ("x", "y", "z", "vx", "vy", "vz", "mass", "volume", "temperature", "enthalpy"):
             setattr(self, k, np.zeros(capacity))
         self.material = np.zeros(capacity, np.int32)
         self.pinned = np.zeros(capacity, np.uint8)
+        self.melted = np.zeros(capacity, np.uint8)
         self.count = 0
 
     def add(self, x, y, z, mass, volume, material=0, v=(0.0, 0.0, 0.0), temperature=0.0):
@@ -48,7 +49,8 @@ class Sim3:
     def remove(self, i):
         """Simulation3.remove(i) for these arrays (src/three/simulation.js:114); pair with MPM3.remove."""
         last = self.count - 1
-        for k in ("x", "y", "z", "vx", "vy", "vz", "mass", "volume", "temperature", "material", "pinned"):
+        for k in ("x", "y", "z", "vx", "vy", "vz", "mass", "volume", "temperature", "enthalpy", "material", "pinned",
+                  "melted"):
             a = getattr(self, k)
             a[i] = a[last]
         self.count = last
@@ -139,6 +141,22 @@ class MPM3:
         if s.count == 0:
             return
         self._check(_lib.lib().mpm_regularize_host(self.solver.h, ctypes.byref(s.particles("xv")), float(dt)))
+
+    def exchangeHeat(self, s, dt, radius=8.0, geometry=20.0, heat_rate=20.0, ambient=False):
+        """exchangeHeat(s, pairs, dt) (src/thermal.js:35-56) over the pairs closer than `radius`
+        (Simulation3.near's H), on the device state; s.temperature, s.enthalpy and s.melted are
+        updated from it. Returns the exchanged heat (Simulation3.exchangedHeat)."""
+        self._sync(s)
+        if s.count == 0:
+            return 0.0
+        q = self.solver.exchange_heat(dt, radius, geometry, heat_rate, ambient)
+        n = s.count
+        d = lambda a: a.ctypes.data_as(ctypes.c_void_p)
+        p = _lib.MpmParticles(dtype=_lib.F64, temperature=d(s.temperature), enthalpy=d(s.enthalpy),
+                              melted=d(s.melted))
+        self._check(_lib.lib().mpm_download_particles(self.solver.h, ctypes.byref(p)))
+        assert n == s.count
+        return q
 
     def refreshDiagnostics(self, s):
         """The ledger the V&V panel reads (src/simulation/mechanical-diagnostics.js:16-37), FP64."""

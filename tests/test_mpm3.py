@@ -103,3 +103,26 @@ def test_mpm3_regularize_solids_on_caller_positions():
     m.regularizeSolids(s, 1 / 120)
     assert np.array_equal(s.x[:2], x)
     m.close()
+
+
+@pytest.mark.gpu
+def test_mpm3_exchange_heat_updates_caller_temperatures():
+    """exchangeHeat through the facade: tests/three.test.mjs:27-31 (contact by 3D distance)."""
+    from mpm_b200.mpm3 import MPM3
+    from mpm_b200.params import Material
+    s = Sim3(8)
+    s.add(0, 0, 0, mass=1.0, volume=1, temperature=80.0)
+    s.add(0, 0, 20, mass=1.0, volume=1, temperature=20.0)
+    water = Material(model=0, mu=.4, lam=.4, specific_heat=4180.0, conductivity=.6)
+    m = MPM3(s.capacity, materials={0: water})
+    assert m.exchangeHeat(s, 1 / 60) == 0.0
+    assert s.temperature[0] == 80 and s.temperature[1] == 20
+    m.close()
+    s.z[1] = 5
+    m = MPM3(s.capacity, materials={0: water})
+    e0 = 4180.0 * (80 + 20)
+    for _ in range(30):
+        m.exchangeHeat(s, 1 / 60)
+    assert s.temperature[0] < 80 and s.temperature[1] > 20
+    assert abs(float(np.sum(s.enthalpy[:2])) - e0) <= 1e-6 * e0
+    m.close()
