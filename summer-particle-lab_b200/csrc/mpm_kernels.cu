@@ -489,6 +489,7 @@ struct __align__(128) PartSmem {
   int bstart[kBuckets + 1];
   unsigned short blist[kBuckets];
   int nbuckets;
+  int wsum[kBlock / 32], wnz[kBlock / 32];  // per-warp bucket totals of the block-wide scan
   unsigned long long mbar[2];
   uint4 item[2];
   int abort_flag;
@@ -722,9 +723,38 @@ __device__ __forceinline__ void scan_buckets_p(const int* hist, int* bstart, uns
   }
 }
 
+// The same scan over the whole block: thread t takes bucket t, warps scan their 32 buckets, and
+// each thread adds the totals of the warps before it (one barrier). A one-warp scan here left the
+// other seven warps of the CTA idle for a quarter of the pass. The histogram is cleared for the
+// next round on the way (it is not read after the scan).
+static_assert(kBlock >= kBuckets, "one thread per bucket");
 __device__ __forceinline__ void scan_buckets(PartSmem& sm) {
-  if (threadIdx.x >= 32) return;
-  scan_buckets_p(sm.hist, sm.bstart, sm.blist, &sm.nbuckets, threadIdx.x);
+  const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+  const int h = t < kBuckets ? sm.hist[t] : 0;
+  if (t < kBuckets) sm.hist[t] = 0;
+  int inc = h;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, inc, o);
+    if (lane >= o) inc += y;
+  }
+  const unsigned nz = __ballot_sync(0xffffffffu, h > 0);
+  if (lane == 31) {
+    sm.wsum[w] = inc;
+    sm.wnz[w] = __popc(nz);
+  }
+  __syncthreads();
+  int base = 0, nbase = 0;
+  for (int k = 0; k < w; ++k) {
+    base += sm.wsum[k];
+    nbase += sm.wnz[k];
+  }
+  if (t < kBuckets) sm.bstart[t] = base + inc - h;
+  if (h > 0) sm.blist[nbase + __popc(nz & ((1u << lane) - 1u))] = static_cast<unsigned short>(t);
+  if (t == kBlock - 1) {
+    sm.bstart[kBuckets] = base + inc;
+    sm.nbuckets = nbase + __popc(nz);
+  }
 }
 
 
@@ -986,8 +1016,10 @@ __global__ void __launch_bounds__(kBlock, 2) k_particles(const __grid_constant__
   const int lst = PASS == kPassP2G ? (k & 1) : ((k - 1) & 1);
   const int nxt = k & 1;
   const bool use_tma = GATHER && c.use_tma;
-  if (SCATTER)
+  if (SCATTER) {
     for (int i = threadIdx.x; i < kChannels * kWinSNodes; i += kBlock) sm.acc[i] = 0.f;
+    for (int i = threadIdx.x; i < kBuckets; i += kBlock) sm.hist[i] = 0;
+  }
   if (threadIdx.x == 0) {
     mbar_init(&sm.mbar[0], 1);
     mbar_init(&sm.mbar[1], 1);
@@ -1008,7 +1040,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_particles(const __grid_constant__
   double work_acc = 0.0;
   int cb = 0;
   // perm entries of the next tile's first round (j = tid, tid + kBlock), loaded one tile ahead
-  unsigned pf[kCap / kBlock] = {0u, 0u};
+  unsigned pf[kCap / kBlock] = {};
   bool pf_ok = false;
   while (true) {
     __syncthreads();
@@ -1082,16 +1114,13 @@ __global__ void __launch_bounds__(kBlock, 2) k_particles(const __grid_constant__
     unsigned flags_acc = 0;
     for (unsigned r0 = 0; r0 < it.z; r0 += kCap) {
       const unsigned nround = min(static_cast<unsigned>(kCap), it.z - r0);
-      if (SCATTER) {
-        for (int i = threadIdx.x; i < kBuckets; i += kBlock) sm.hist[i] = 0;
-        __syncthreads();
-      }
-      // ---- phase A: one thread per particle ----
+      // ---- phase A: one thread per particle (the bucket histogram is zero: cleared at the start
+      // and by each round's scan) ----
       for (unsigned jj = 0; jj < nround; jj += kBlock) {
         const unsigned j = jj + threadIdx.x;
         unsigned key = 0xffffffffu;
         if (j < nround) {
-          const unsigned home = (r0 == 0 && pf_ok) ? (jj == 0 ? pf[0] : pf[1]) : c.p.perm[it.y + r0 + j];
+          const unsigned home = (r0 == 0 && pf_ok) ? pf[jj / kBlock] : c.p.perm[it.y + r0 + j];
           key = particle_phase_a<PASS, HEAT, AUX>(c, sc, tc, sm.mt, single, sm.vwin[cb], home, j, dt, nxt, sm.pay, sm.meta,
                                        sm.hist, wave_acc, grad_acc, flags_acc, work_acc);
         }
