@@ -698,40 +698,18 @@ __device__ __forceinline__ void bucket_layer(PartSmem& sm, int b, int kz) {
   bucket_layer_p<HEAT>(sm.pay, sm.sidx, sm.bstart, sm.acc, b, kz);
 }
 
-// Exclusive scan of the bucket histogram by warp 0, with the compact list of non-empty buckets.
-// lane: 0..31 of the one warp that scans.
-__device__ __forceinline__ void scan_buckets_p(const int* hist, int* bstart, unsigned short* blist, int* nbuckets,
-                                               int lane) {
-  int carry = 0, ncarry = 0;
-  for (int b0 = 0; b0 < kBuckets; b0 += 32) {
-    const int b = b0 + lane;
-    const int h = b < kBuckets ? hist[b] : 0;
-    int inc = h;
-    for (int o = 1; o < 32; o <<= 1) {
-      const int y = __shfl_up_sync(0xffffffffu, inc, o);
-      if (lane >= o) inc += y;
-    }
-    if (b < kBuckets) bstart[b] = carry + inc - h;
-    const unsigned nz = __ballot_sync(0xffffffffu, h > 0);
-    if (h > 0) blist[ncarry + __popc(nz & ((1u << lane) - 1u))] = static_cast<unsigned short>(b);
-    carry += __shfl_sync(0xffffffffu, inc, 31);
-    ncarry += __popc(nz);
-  }
-  if (lane == 0) {
-    bstart[kBuckets] = carry;
-    *nbuckets = ncarry;
-  }
-}
-
-// The same scan over the whole block: thread t takes bucket t, warps scan their 32 buckets, and
-// each thread adds the totals of the warps before it (one barrier). A one-warp scan here left the
-// other seven warps of the CTA idle for a quarter of the pass. The histogram is cleared for the
-// next round on the way (it is not read after the scan).
-static_assert(kBlock >= kBuckets, "one thread per bucket");
-__device__ __forceinline__ void scan_buckets(PartSmem& sm) {
-  const int t = threadIdx.x, lane = t & 31, w = t >> 5;
-  const int h = t < kBuckets ? sm.hist[t] : 0;
-  if (t < kBuckets) sm.hist[t] = 0;
+// Exclusive scan of the bucket histogram over a group of NT >= kBuckets threads, with the compact
+// list of non-empty buckets: thread t takes bucket t, warps scan their 32 buckets, and each thread
+// adds the totals of the warps before it (one group barrier, `sync`). A one-warp scan here left the
+// other warps of the group idle for a quarter of the pass. With clear, the histogram is zeroed for
+// the next round on the way (it is not read after the scan).
+template <int NT, typename Sync>
+__device__ __forceinline__ void scan_buckets_group(int* hist, int* bstart, unsigned short* blist, int* nbuckets,
+                                                   int* wsum, int* wnz, int t, bool clear, Sync&& sync) {
+  static_assert(NT >= kBuckets && NT % 32 == 0, "one thread per bucket");
+  const int lane = t & 31, w = t >> 5;
+  const int h = t < kBuckets ? hist[t] : 0;
+  if (clear && t < kBuckets) hist[t] = 0;
   int inc = h;
 #pragma unroll
   for (int o = 1; o < 32; o <<= 1) {
@@ -740,21 +718,26 @@ __device__ __forceinline__ void scan_buckets(PartSmem& sm) {
   }
   const unsigned nz = __ballot_sync(0xffffffffu, h > 0);
   if (lane == 31) {
-    sm.wsum[w] = inc;
-    sm.wnz[w] = __popc(nz);
+    wsum[w] = inc;
+    wnz[w] = __popc(nz);
   }
-  __syncthreads();
+  sync();
   int base = 0, nbase = 0;
   for (int k = 0; k < w; ++k) {
-    base += sm.wsum[k];
-    nbase += sm.wnz[k];
+    base += wsum[k];
+    nbase += wnz[k];
   }
-  if (t < kBuckets) sm.bstart[t] = base + inc - h;
-  if (h > 0) sm.blist[nbase + __popc(nz & ((1u << lane) - 1u))] = static_cast<unsigned short>(t);
-  if (t == kBlock - 1) {
-    sm.bstart[kBuckets] = base + inc;
-    sm.nbuckets = nbase + __popc(nz);
+  if (t < kBuckets) bstart[t] = base + inc - h;
+  if (h > 0) blist[nbase + __popc(nz & ((1u << lane) - 1u))] = static_cast<unsigned short>(t);
+  if (t == NT - 1) {
+    bstart[kBuckets] = base + inc;
+    *nbuckets = nbase + __popc(nz);
   }
+}
+
+__device__ __forceinline__ void scan_buckets(PartSmem& sm) {
+  scan_buckets_group<kBlock>(sm.hist, sm.bstart, sm.blist, &sm.nbuckets, sm.wsum, sm.wnz, threadIdx.x, true,
+                             [] { __syncthreads(); });
 }
 
 
@@ -1211,6 +1194,7 @@ struct __align__(128) WsSmem {
   int bstart[kBuckets + 1];
   unsigned short blist[kBuckets];
   int nbuckets;
+  int wsum[kWsGroup / 32], wnz[kWsGroup / 32];  // per-warp bucket totals of the consumer scan
   StageInfo flush_info;                   // consumer copy of the stage it flushes
   unsigned long long tma_bar[2], full[2], empty[2];
   uint4 item[2];
@@ -1438,7 +1422,8 @@ __global__ void __launch_bounds__(kWsThreads, 1) k_particles_ws(const __grid_con
       }
       group_sync(2);
       if (sm.consumer_exit || sm.info[s].sentinel) break;
-      if (tb < 32) scan_buckets_p(sm.hist[s], sm.bstart, sm.blist, &sm.nbuckets, tb);
+      scan_buckets_group<kWsGroup>(sm.hist[s], sm.bstart, sm.blist, &sm.nbuckets, sm.wsum, sm.wnz, tb, false,
+                                   [] { group_sync(2); });
       group_sync(2);
       const int nround = sm.info[s].nround;
       for (int j = tb; j < nround; j += kWsGroup) {
