@@ -175,7 +175,8 @@ def read_traffic_per_particle():
     if not os.path.exists(path):
         return None
     for line in open(path):
-        if line.strip().startswith("dram_bytes_per_particle:"):
+        line = line.strip().lstrip("-").strip()  # the summary lists it as a bullet
+        if line.startswith("dram_bytes_per_particle:"):
             try:
                 return float(line.split(":", 1)[1].split()[0])
             except ValueError:
