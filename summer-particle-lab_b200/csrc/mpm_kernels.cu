@@ -463,6 +463,11 @@ void launch_sort_scatter(const Ctx& c, cudaStream_t st, bool initial) {
 constexpr int kCap = 512;      // particles per scatter round
 constexpr int kPay = 23;       // payload floats per particle (the last, m T, only with conduction)
 constexpr int kBuckets = 216;  // 6^3 possible stencil bases in the scatter window
+// Payload slot of particle j: one extra word every 32 slots, so the slots phase B reads at a
+// stride of a bucket's size (8 for the particles of one cell in consecutive slots) fall in
+// different shared-memory banks; phase A's consecutive slots stay conflict-free.
+constexpr int kPayStride = kCap + kCap / 32;
+__device__ __forceinline__ int pay_slot(int j) { return j + (j >> 5); }
 constexpr unsigned kMetaInvalid = 0x80000000u;
 
 enum Pass : int { kPassP2G = 0, kPassG2P2G = 1, kPassG2P = 2 };
@@ -482,7 +487,7 @@ struct TileCtx {
 struct __align__(128) PartSmem {
   float4 vwin[2][kWinG * kWinG * kWinG];  // double-buffered TMA destinations (3456 B each)
   float acc[kChannels * kWinSNodes];      // 16 KiB scatter window
-  float pay[kPay * kCap];                 // 46 KiB payloads, structure of arrays
+  float pay[kPay * kPayStride];           // 47 KiB payloads, structure of arrays (swizzled slots)
   unsigned meta[kCap];                    // bucket | rank << 8 (or kMetaInvalid)
   unsigned short sidx[kCap];              // slots sorted by bucket
   int hist[kBuckets];
@@ -621,14 +626,14 @@ __device__ __forceinline__ void bucket_layer_p(const float* pay, const unsigned 
   const int i1 = bstart[b + 1];
   for (int i = bstart[b]; i < i1; ++i) {
     const int j = sidx[i];
-    const float* P = pay + j;
-    const float tx = P[0 * kCap], ty = P[1 * kCap], tz = P[2 * kCap], m = P[3 * kCap];
-    const float mv0 = P[4 * kCap], mv1 = P[5 * kCap], mv2 = P[6 * kCap];
-    const float c00 = P[7 * kCap], c01 = P[8 * kCap], c02 = P[9 * kCap];
-    const float c10 = P[10 * kCap], c11 = P[11 * kCap], c12 = P[12 * kCap];
-    const float c20 = P[13 * kCap], c21 = P[14 * kCap], c22 = P[15 * kCap];
-    const float s00 = P[16 * kCap], s11 = P[17 * kCap], s22 = P[18 * kCap];
-    const float s01 = P[19 * kCap], s02 = P[20 * kCap], s12 = P[21 * kCap];
+    const float* P = pay + pay_slot(j);
+    const float tx = P[0 * kPayStride], ty = P[1 * kPayStride], tz = P[2 * kPayStride], m = P[3 * kPayStride];
+    const float mv0 = P[4 * kPayStride], mv1 = P[5 * kPayStride], mv2 = P[6 * kPayStride];
+    const float c00 = P[7 * kPayStride], c01 = P[8 * kPayStride], c02 = P[9 * kPayStride];
+    const float c10 = P[10 * kPayStride], c11 = P[11 * kPayStride], c12 = P[12 * kPayStride];
+    const float c20 = P[13 * kPayStride], c21 = P[14 * kPayStride], c22 = P[15 * kPayStride];
+    const float s00 = P[16 * kPayStride], s11 = P[17 * kPayStride], s22 = P[18 * kPayStride];
+    const float s01 = P[19 * kPayStride], s02 = P[20 * kPayStride], s12 = P[21 * kPayStride];
     float wx[3], wy[3], wzv[3];
     bspline_weights(tx, wx);
     bspline_weights(ty, wy);
@@ -674,12 +679,12 @@ __device__ __forceinline__ void bucket_layer_p(const float* pay, const unsigned 
 #pragma unroll
       for (int x = 0; x < 3; ++x) hsum[y][x] = 0.f;
     for (int i = bstart[b]; i < i1; ++i) {
-      const float* P = pay + sidx[i];
+      const float* P = pay + pay_slot(sidx[i]);
       float wx[3], wy[3], wzv[3];
-      bspline_weights(P[0 * kCap], wx);
-      bspline_weights(P[1 * kCap], wy);
-      bspline_weights(P[2 * kCap], wzv);
-      const float wmt = (kz == 0 ? wzv[0] : (kz == 1 ? wzv[1] : wzv[2])) * P[22 * kCap];
+      bspline_weights(P[0 * kPayStride], wx);
+      bspline_weights(P[1 * kPayStride], wy);
+      bspline_weights(P[2 * kPayStride], wzv);
+      const float wmt = (kz == 0 ? wzv[0] : (kz == 1 ? wzv[1] : wzv[2])) * P[22 * kPayStride];
 #pragma unroll
       for (int y = 0; y < 3; ++y)
 #pragma unroll
@@ -960,16 +965,23 @@ __device__ __forceinline__ unsigned particle_phase_a(const Ctx& c, const SceneDe
     const bool in_w = l0 >= 0 && l0 <= kWinS - 3 && l1 >= 0 && l1 <= kWinS - 3 && l2 >= 0 && l2 <= kWinS - 3;
     if (in_w && !pinned) {
       const int bucket = (l2 * 6 + l1) * 6 + l0;
-      const int rank = atomicAdd(&hist[bucket], 1);
+      // one shared atomic per bucket among the warp's converged lanes (particles of one cell share
+      // buckets), each lane's rank from its position among them
+      const unsigned act = __activemask();
+      const unsigned peers = __match_any_sync(act, bucket);
+      const int leader = __ffs(peers) - 1, lane = threadIdx.x & 31;
+      int rank0 = 0;
+      if (lane == leader) rank0 = atomicAdd(&hist[bucket], __popc(peers));
+      const int rank = __shfl_sync(peers, rank0, leader) + __popc(peers & ((1u << lane) - 1u));
       meta[j] = static_cast<unsigned>(bucket) | (static_cast<unsigned>(rank) << 8);
-      float* P = pay + j;
-      P[0 * kCap] = t[0]; P[1 * kCap] = t[1]; P[2 * kCap] = t[2]; P[3 * kCap] = m;
-      P[4 * kCap] = mv[0]; P[5 * kCap] = mv[1]; P[6 * kCap] = mv[2];
+      float* P = pay + pay_slot(j);
+      P[0 * kPayStride] = t[0]; P[1 * kPayStride] = t[1]; P[2 * kPayStride] = t[2]; P[3 * kPayStride] = m;
+      P[4 * kPayStride] = mv[0]; P[5 * kPayStride] = mv[1]; P[6 * kPayStride] = mv[2];
 #pragma unroll
-      for (int e = 0; e < 9; ++e) P[(7 + e) * kCap] = mC[e];
+      for (int e = 0; e < 9; ++e) P[(7 + e) * kPayStride] = mC[e];
 #pragma unroll
-      for (int e = 0; e < 6; ++e) P[(16 + e) * kCap] = s6[e];
-      if (HEAT) P[22 * kCap] = m * T;
+      for (int e = 0; e < 6; ++e) P[(16 + e) * kPayStride] = s6[e];
+      if (HEAT) P[22 * kPayStride] = m * T;
     } else {
       meta[j] = kMetaInvalid;
       if (!in_w) flags |= 0x10u;
@@ -1185,7 +1197,7 @@ struct StageInfo {
 
 struct __align__(128) WsSmem {
   float4 vwin[2][kWinG * kWinG * kWinG];  // producer: double-buffered TMA destinations
-  float pay[2][kPay * kCap];              // stage buffers
+  float pay[2][kPay * kPayStride];        // stage buffers
   unsigned meta[2][kCap];
   int hist[2][kBuckets];
   StageInfo info[2];
@@ -1940,8 +1952,61 @@ __global__ void k_permute(Ctx c, Particles d) {
   }
 }
 
+// Before a permutation: orders each tile's perm range by the particle's stencil base cell within
+// the tile (64 cells; counting sort in shared memory, one CTA per tile of the current work list),
+// so after the permutation the particles of one cell sit in consecutive home slots and a warp of
+// consecutive particles touches few cells. Tiles above kCellSortMax particles keep their order.
+constexpr int kCellSortMax = 4096;
+
+__global__ void __launch_bounds__(256) k_cell_order(Ctx c) {
+  __shared__ unsigned ids[kCellSortMax];
+  __shared__ unsigned char cell[kCellSortMax];
+  __shared__ int cursor[64];
+  const unsigned list = c.ctrl->step_index & 1u;
+  const unsigned nwork = min(c.ctrl->work_count[list], static_cast<unsigned>(c.total_tiles));
+  for (unsigned w = blockIdx.x; w < nwork; w += gridDim.x) {
+    const uint4 it = c.s.work[list][w];  // (tile, start, count, scene)
+    if (it.z > static_cast<unsigned>(kCellSortMax) || it.y + it.z > static_cast<unsigned long long>(c.n)) continue;
+    const SceneDev& sc = c.scenes[it.w];
+    if (threadIdx.x < 64) cursor[threadIdx.x] = 0;
+    __syncthreads();
+    for (unsigned j = threadIdx.x; j < it.z; j += blockDim.x) {
+      const unsigned h = c.p.perm[it.y + j];
+      int b0, b1, b2;
+      float t;
+      stencil_axis(c.p.qx[h], sc.dims[0], b0, t);
+      stencil_axis(c.p.qy[h], sc.dims[1], b1, t);
+      stencil_axis(c.p.qz[h], sc.dims[2], b2, t);
+      const int local = ((b2 & 3) * 4 + (b1 & 3)) * 4 + (b0 & 3);
+      ids[j] = h;
+      cell[j] = static_cast<unsigned char>(local);
+      atomicAdd(&cursor[local], 1);
+    }
+    __syncthreads();
+    if (threadIdx.x < 32) {  // exclusive scan of the 64 cell counts by one warp (two per lane)
+      const int a0 = cursor[2 * threadIdx.x], a1 = cursor[2 * threadIdx.x + 1];
+      int inc = a0 + a1;
+      for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, inc, o);
+        if (threadIdx.x >= o) inc += y;
+      }
+      const int ex = inc - a0 - a1;
+      cursor[2 * threadIdx.x] = ex;
+      cursor[2 * threadIdx.x + 1] = ex + a0;
+    }
+    __syncthreads();
+    for (unsigned j = threadIdx.x; j < it.z; j += blockDim.x) {
+      const int pos = atomicAdd(&cursor[cell[j]], 1);
+      c.p.perm[it.y + pos] = ids[j];
+    }
+    __syncthreads();
+  }
+}
+
 void launch_permute(const Ctx& c, const Particles& dst, cudaStream_t st) {
   if (c.n <= 0) return;
+  const int tiles = c.total_tiles < 4096 ? c.total_tiles : 4096;
+  if (tiles > 0) k_cell_order<<<tiles, 256, 0, st>>>(c);
   const long long blocks = (c.n + 255) / 256 < 65536 ? (c.n + 255) / 256 : 65536;
   k_permute<<<static_cast<unsigned>(blocks), 256, 0, st>>>(c, dst);
 }
