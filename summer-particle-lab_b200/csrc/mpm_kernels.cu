@@ -1034,6 +1034,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_particles(const __grid_constant__
   unsigned phase0 = 0, phase1 = 0;
   double work_acc = 0.0;
   int cb = 0;
+  int mt_row = -1;  // material row held in sm.mt
   // perm entries of the next tile's first round (j = tid, tid + kBlock), loaded one tile ahead
   unsigned pf[kCap / kBlock] = {};
   bool pf_ok = false;
@@ -1089,7 +1090,15 @@ __global__ void __launch_bounds__(kBlock, 2) k_particles(const __grid_constant__
       tl.clamp = sc.clamp;
       tl.mat = sc.mat_base;
       sm.tc = tl;
-      if (c.single_material) sm.mt = c.mats[sc.mat_base];
+    }
+    // the material row of a single-material scene, copied word by word by the whole block, and
+    // only when it changes (every tile of a one-scene handle shares it)
+    if (c.single_material && sc.mat_base != mt_row) {
+      static_assert(sizeof(MaterialDev) % 4 == 0, "word copy");
+      const unsigned* src = reinterpret_cast<const unsigned*>(c.mats + sc.mat_base);
+      unsigned* dst = reinterpret_cast<unsigned*>(&sm.mt);
+      for (int i = threadIdx.x; i < static_cast<int>(sizeof(MaterialDev) / 4); i += kBlock) dst[i] = src[i];
+      mt_row = sc.mat_base;
     }
     __syncthreads();
     if (sm.abort_flag) return;
