@@ -283,19 +283,21 @@ class Batch(Solver):
         f = np.dtype(dtype)
 
         def cat(name, shape=None):
-            if any(getattr(sc, name) is None for sc in self.scenes):
+            if any(getattr(sc, name, None) is None for sc in self.scenes):
                 return None
             a = np.concatenate([np.asarray(getattr(sc, name)).reshape((sc.n,) + (shape or ())) for sc in self.scenes])
-            return np.ascontiguousarray(a, dtype=np.uint8 if name == "pinned" else f)
+            return np.ascontiguousarray(a, dtype=np.uint8 if name in ("pinned", "melted") else f)
 
         x, v = cat("x", (3,)), cat("v", (3,))
         cols = [np.ascontiguousarray(x[:, a]) for a in range(3)] + [np.ascontiguousarray(v[:, a]) for a in range(3)]
         m, V, T, ep = cat("m"), cat("V"), cat("T"), cat("ep")
         F, C, pin = cat("F", (9,)), cat("C", (9,)), cat("pinned")
+        jp, dil, enth, mel = cat("jp"), cat("dilation"), cat("enthalpy"), cat("melted")
         p = MpmParticles(dtype=_lib.F64 if f == np.float64 else _lib.F32,
                          x=_ptr(cols[0]), y=_ptr(cols[1]), z=_ptr(cols[2]), vx=_ptr(cols[3]), vy=_ptr(cols[4]),
                          vz=_ptr(cols[5]), mass=_ptr(m), volume=_ptr(V), temperature=_ptr(T), plastic=_ptr(ep),
-                         F=_ptr(F), C=_ptr(C), material=None, pinned=_ptr(pin))
+                         F=_ptr(F), C=_ptr(C), material=None, pinned=_ptr(pin), jp=_ptr(jp), dilation=_ptr(dil),
+                         enthalpy=_ptr(enth), melted=_ptr(mel))
         self._check(_lib.lib().mpm_upload_particles(self.h, self.capacity, ctypes.byref(p)))
         self.n = self.capacity
 
