@@ -401,6 +401,32 @@ typedef struct mpm_heat_exchange {
 int mpm_exchange_heat(mpm_handle* h, const mpm_heat_exchange* x, double dt, double* exchanged);
 
 /* ======================================================================================
+ * One domain split into slabs along z (the halo-exchange form of one large scene; no
+ * counterpart in the reference, which runs one scene in one worker). Neighbouring slabs hold the
+ * same `planes` node planes; after every scatter both copies of a shared node get the sum of both
+ * slabs' contributions (only in node tiles the slab has active), so both grid updates give the same
+ * velocity there and particles near the seam need no copy. Faces where the domain continues have
+ * no wall, no sticky floor and no position clamp. Particles must stay at least 3 node planes inside
+ * their slab's grid (no migration here: a host re-partitions by download and upload when needed).
+ * ====================================================================================== */
+/* On one handle: consecutive scenes of a batch are the slabs (scene s + 1's first `planes` z
+ * nodes are scene s's last), every scene takes the same dt (the smallest), and the overlap sum runs
+ * after each scatter on the device. */
+int mpm_batch_set_slabs(mpm_handle* h, int32_t planes);
+/* Across ranks (one single-scene handle per rank): open faces (bit 2 axis + side; z low = 16,
+ * z high = 32), a scatter of the current state without stepping, and the overlap planes of the
+ * fresh scatter exported to / added from a device buffer of mpm_halo_bytes bytes (16-byte aligned;
+ * acc planes then heat planes). A rank exports its side, exchanges buffers with the neighbour,
+ * adds what it received, then steps (mpm_step_fixed, one substep, dt = the smallest
+ * mpm_stable_dt over ranks). Export and add return after their copy is complete; the caller makes
+ * the received buffer ready before mpm_halo_add. */
+int mpm_set_open_faces(mpm_handle* h, int32_t faces);
+int mpm_prepare(mpm_handle* h);
+int mpm_halo_bytes(const mpm_handle* h, int32_t planes, int64_t* bytes);
+int mpm_halo_export(mpm_handle* h, int32_t side, int32_t planes, void* device_buffer);
+int mpm_halo_add(mpm_handle* h, int32_t side, int32_t planes, const void* device_buffer);
+
+/* ======================================================================================
  * Learned return map. No counterpart in the reference, whose return maps are closed-form or
  * bisection code (src/three/metal-plasticity.js:12-38, src/three/thermal-plasticity.js:12-40):
  * a small MLP (8 -> 64 -> 64 -> 7, ReLU, BF16 tensor-core arithmetic with FP32 accumulation)

@@ -111,6 +111,7 @@ struct mpm_handle {
   mpm::HeatDev hdev{};
   double heat_radius = 0;
   double* host_exchanged = nullptr;  // pinned readback
+  int slab_planes = 0;     // batch of slabs along z: node planes shared by consecutive scenes
   // profiling: event pairs around launches while enabled
   bool profiling = false;
   std::vector<cudaEvent_t> ev_pool;
@@ -443,6 +444,7 @@ static int prepare_grid(mpm_handle* h) {
     h->reorder_pending = false;
   }
   { ProfScope ps(h, 5); mpm::launch_p2g(h->ctx, h->stream, h->p2g_blocks); }
+  if (h->slab_planes) { ProfScope ps(h, -1); mpm::launch_halo_sum(h->ctx, h->stream, h->slab_planes); }
   MPM_CUDA(h, cudaGetLastError());
   h->grid_valid = true;
   h->pending_grid = true;
@@ -458,6 +460,7 @@ static void launch_substep(mpm_handle* h, bool scatter) {
     mpm::launch_conduct(c, h->stream, h->grid_blocks);
   }
   { ProfScope ps(h, 2); mpm::launch_g2p2g(c, h->stream, h->g2p2g_blocks, scatter); }
+  if (scatter && h->slab_planes) { ProfScope ps(h, -1); mpm::launch_halo_sum(c, h->stream, h->slab_planes); }
   if (scatter) {
     { ProfScope ps(h, 3); mpm::launch_scan(c, h->stream); }
     { ProfScope ps(h, 4); mpm::launch_sort_scatter(c, h->stream, false); }
@@ -1395,6 +1398,113 @@ int mpm_regularize_host(mpm_handle* h, const mpm_particles* io, double dt) {
   out.dtype = io->dtype;
   out.x = io->x; out.y = io->y; out.z = io->z;
   return mpm_download_particles(h, &out);
+}
+
+// Opens the given faces of every scene (bit 2 axis + side): no separating-slip wall, no sticky
+// floor and no position clamp there, because the domain continues in another scene or rank.
+static void open_faces(mpm_handle* h, SceneDev& s, int faces) {
+  for (int a = 0; a < 3; ++a) {
+    const unsigned qmax = static_cast<unsigned>((static_cast<long long>(s.dims[a]) - 1) << mpm::kFracBits);
+    if (faces & (1 << (2 * a))) {
+      s.wall_lo[a] = -1;
+      s.qlo[a] = 0;
+      if (a == 1) s.sticky = 0;
+    }
+    if (faces & (1 << (2 * a + 1))) {
+      s.wall_hi[a] = 1 << 30;
+      s.qhi[a] = qmax;
+    }
+  }
+  (void)h;
+}
+
+int mpm_batch_set_slabs(mpm_handle* h, int32_t planes) {
+  if (!h) return MPM_ERR_INVALID_ARG;
+  const int ns = static_cast<int>(h->scenes.size());
+  if (!h->batch || ns < 2) return fail(h, MPM_ERR_STATE, "slabs need a batch handle of two or more scenes");
+  if (h->slab_planes) return fail(h, MPM_ERR_STATE, "slabs are already set");
+  if (planes < 4) return fail(h, MPM_ERR_INVALID_ARG, "slabs share at least 4 node planes");
+  for (int s = 0; s + 1 < ns; ++s) {
+    const SceneDev& a = h->scenes[s];
+    const SceneDev& b = h->scenes[s + 1];
+    const double H = a.H;
+    bool ok = a.H == b.H && a.dims[0] == b.dims[0] && a.dims[1] == b.dims[1] && planes * 2 <= a.dims[2] &&
+              planes * 2 <= b.dims[2];
+    for (int k = 0; k < 2 && ok; ++k) ok = std::fabs(a.origin[k] - b.origin[k]) <= 1e-9 * H;
+    ok = ok && std::fabs(b.origin[2] - (a.origin[2] + (a.dims[2] - planes) * H)) <= 1e-6 * H;
+    if (!ok)
+      return fail(h, MPM_ERR_INVALID_ARG,
+                  "consecutive scenes must be slabs of one grid along z that share the given node planes");
+  }
+  for (int s = 0; s < ns; ++s) open_faces(h, h->scenes[s], (s > 0 ? 1 << 4 : 0) | (s + 1 < ns ? 1 << 5 : 0));
+  h->scene = h->scenes[0];
+  MPM_CUDA(h, cudaMemcpyAsync(const_cast<SceneDev*>(h->ctx.scenes), h->scenes.data(), sizeof(SceneDev) * ns,
+                              cudaMemcpyHostToDevice, h->stream));
+  MPM_CUDA(h, cudaStreamSynchronize(h->stream));
+  h->slab_planes = planes;
+  h->ctx.uniform_dt = 1;
+  drop_graph(h);
+  h->grid_valid = false;
+  return MPM_OK;
+}
+
+int mpm_set_open_faces(mpm_handle* h, int32_t faces) {
+  if (!h || faces < 0 || faces > 63) return MPM_ERR_INVALID_ARG;
+  if (h->batch) return fail(h, MPM_ERR_STATE, "single-scene call on a batch handle");
+  open_faces(h, h->scene, faces);
+  h->scenes[0] = h->scene;
+  MPM_CUDA(h, cudaMemcpyAsync(const_cast<SceneDev*>(h->ctx.scenes), &h->scene, sizeof(SceneDev), cudaMemcpyHostToDevice,
+                              h->stream));
+  MPM_CUDA(h, cudaStreamSynchronize(h->stream));
+  h->grid_valid = false;
+  return MPM_OK;
+}
+
+int mpm_prepare(mpm_handle* h) {
+  if (!h) return MPM_ERR_INVALID_ARG;
+  if (!h->uploaded) return fail(h, MPM_ERR_STATE, "no particles uploaded");
+  if (h->n == 0 || h->grid_valid) return MPM_OK;
+  const int rc = prepare_grid(h);
+  if (rc != MPM_OK) return rc;
+  MPM_CUDA(h, cudaStreamSynchronize(h->stream));
+  return MPM_OK;
+}
+
+static int halo_check(mpm_handle* h, int side, int planes, const void* buf) {
+  if (h->batch) return fail(h, MPM_ERR_STATE, "single-scene call on a batch handle");
+  if (!h->uploaded) return fail(h, MPM_ERR_STATE, "no particles uploaded");
+  if ((side != 0 && side != 1) || planes < 1 || planes * 2 > h->scene.dims[2])
+    return fail(h, MPM_ERR_INVALID_ARG, "side 0 or 1 and 1 <= planes <= half the z nodes");
+  if (!buf || (reinterpret_cast<uintptr_t>(buf) & 15u)) return fail(h, MPM_ERR_INVALID_ARG, "buffer must be 16-byte aligned");
+  if (!h->grid_valid) return fail(h, MPM_ERR_STATE, "no fresh scatter: call mpm_prepare or a step first");
+  return MPM_OK;
+}
+
+int mpm_halo_bytes(const mpm_handle* h, int32_t planes, int64_t* bytes) {
+  if (!h || !bytes || planes < 1) return MPM_ERR_INVALID_ARG;
+  const long long per = (long long)h->scene.gdim[0] * h->scene.gdim[1] * planes;
+  *bytes = per * (32 + (h->ctx.conduct ? 4 : 0));
+  return MPM_OK;
+}
+
+int mpm_halo_export(mpm_handle* h, int32_t side, int32_t planes, void* device_buffer) {
+  if (!h) return MPM_ERR_INVALID_ARG;
+  int rc = halo_check(h, side, planes, device_buffer);
+  if (rc != MPM_OK) return rc;
+  { ProfScope ps(h, -1); mpm::launch_halo_export(h->ctx, h->stream, side, planes, static_cast<float*>(device_buffer)); }
+  MPM_CUDA(h, cudaGetLastError());
+  MPM_CUDA(h, cudaStreamSynchronize(h->stream));
+  return MPM_OK;
+}
+
+int mpm_halo_add(mpm_handle* h, int32_t side, int32_t planes, const void* device_buffer) {
+  if (!h) return MPM_ERR_INVALID_ARG;
+  int rc = halo_check(h, side, planes, device_buffer);
+  if (rc != MPM_OK) return rc;
+  { ProfScope ps(h, -1); mpm::launch_halo_add(h->ctx, h->stream, side, planes, static_cast<const float*>(device_buffer)); }
+  MPM_CUDA(h, cudaGetLastError());
+  MPM_CUDA(h, cudaStreamSynchronize(h->stream));
+  return MPM_OK;
 }
 
 int mpm_profile_enable(mpm_handle* h, int32_t on) {

@@ -150,6 +150,7 @@ struct Ctx {
   int use_tma;
   int ws_blocks;        // > 0: the particle passes that scatter run warp-specialised on this many CTAs
   int conduct;          // a scene conducts heat on the grid: heat channel, conduction pass, dT gather
+  int uniform_dt;       // every scene takes the smallest scene dt (slabs of one domain)
 };
 
 #ifdef __CUDACC__
@@ -175,6 +176,13 @@ void launch_begin(const Ctx& c, cudaStream_t st);
 void launch_grid_clear(const Ctx& c, cudaStream_t st, int grid_blocks);
 void launch_grid_update(const Ctx& c, cudaStream_t st, int grid_blocks);
 void launch_conduct(const Ctx& c, cudaStream_t st, int grid_blocks);
+// Slab decomposition along z: consecutive scenes share `planes` node planes; after a scatter both
+// copies of every shared node hold the sum (only in node tiles the scene has active).
+void launch_halo_sum(const Ctx& c, cudaStream_t st, int planes);
+// One scene's low (side 0) or high (side 1) `planes` node planes of the fresh scatter, to or from
+// a device buffer: acc0 planes, acc1 planes, then heat planes when conducting.
+void launch_halo_export(const Ctx& c, cudaStream_t st, int side, int planes, float* buf);
+void launch_halo_add(const Ctx& c, cudaStream_t st, int side, int planes, const float* buf);
 void launch_g2p2g(const Ctx& c, cudaStream_t st, int grid_blocks, bool scatter);
 void launch_ledger(const Ctx& c, cudaStream_t st, double* partials, int blocks, double* out);
 void launch_grid_debug(const Ctx& c, cudaStream_t st, int scene, float dt, double* mass, double* mom);

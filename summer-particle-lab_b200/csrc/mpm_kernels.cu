@@ -280,7 +280,7 @@ __global__ void __launch_bounds__(256) k_begin(Ctx c) {
   __syncthreads();
   if (sdone) return;
   for (int s = threadIdx.x; s < c.nscenes; s += blockDim.x) {
-    if (ct->mode != kModeCfl) c.dt_scene[s] = sdt;
+    if (ct->mode != kModeCfl || c.uniform_dt) c.dt_scene[s] = sdt;
     c.time_scene[s] += static_cast<double>(c.dt_scene[s]);
     c.wave_max[s] = 0u;
     c.grad_max[s] = 0u;
@@ -1647,6 +1647,93 @@ __global__ void __launch_bounds__(256) k_conduct(Ctx c) {
 }
 
 void launch_conduct(const Ctx& c, cudaStream_t st, int grid_blocks) { k_conduct<<<grid_blocks, 256, 0, st>>>(c); }
+
+// ---------------------------------------------------------------------------------------------
+// Slab decomposition of one domain along z. Scenes s and s+1 (or two ranks' scenes) hold the same
+// `planes` node planes: the top planes of s are the bottom planes of s+1. After each scatter (the
+// fresh grid is acc[step_index & 1]) both copies of a shared node must hold the sum of both
+// slabs' contributions, so both grid updates give the same velocity there; a copy is written only
+// where its node tile is active this substep (inactive tiles are never read by the grid update,
+// which would also never clear them).
+
+__device__ __forceinline__ bool node_active(const Ctx& c, const SceneDev& sc, int x, int y, int z) {
+  const unsigned tile = sc.node_tile_base + ((z >> 2) * sc.ntiles[1] + (y >> 2)) * sc.ntiles[0] + (x >> 2);
+  return c.g.tile_flag[tile] != 0u;
+}
+
+__global__ void k_halo_sum(Ctx c, int planes) {
+  if (c.ctrl->done) return;
+  const int par = c.ctrl->step_index & 1;
+  for (int s = 0; s + 1 < c.nscenes; ++s) {
+    const SceneDev& lo = c.scenes[s];
+    const SceneDev& hi = c.scenes[s + 1];
+    const long long per = (long long)lo.gdim[0] * lo.gdim[1];
+    const long long total = per * planes;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x) {
+      const int zr = static_cast<int>(i / per);
+      const int rem = static_cast<int>(i - (long long)zr * per);
+      const int y = rem / lo.gdim[0], x = rem - y * lo.gdim[0];
+      const int zl = lo.dims[2] - planes + zr;
+      const long long nl = lo.node_base + ((long long)zl * lo.gdim[1] + y) * lo.gdim[0] + x;
+      const long long nh = hi.node_base + ((long long)zr * hi.gdim[1] + y) * hi.gdim[0] + x;
+      const bool al = node_active(c, lo, x, y, zl), ah = node_active(c, hi, x, y, zr);
+      if (!al && !ah) continue;
+      const float4 a0 = c.g.acc0[par][nl], b0 = c.g.acc0[par][nh];
+      const float4 a1 = c.g.acc1[par][nl], b1 = c.g.acc1[par][nh];
+      const float4 s0 = make_float4(a0.x + b0.x, a0.y + b0.y, a0.z + b0.z, a0.w + b0.w);
+      const float4 s1 = make_float4(a1.x + b1.x, a1.y + b1.y, a1.z + b1.z, a1.w + b1.w);
+      if (al) { c.g.acc0[par][nl] = s0; c.g.acc1[par][nl] = s1; }
+      if (ah) { c.g.acc0[par][nh] = s0; c.g.acc1[par][nh] = s1; }
+      if (c.conduct) {
+        const float hs = c.g.heat[par][nl] + c.g.heat[par][nh];
+        if (al) c.g.heat[par][nl] = hs;
+        if (ah) c.g.heat[par][nh] = hs;
+      }
+    }
+  }
+}
+
+void launch_halo_sum(const Ctx& c, cudaStream_t st, int planes) {
+  if (c.nscenes < 2 || planes <= 0) return;
+  k_halo_sum<<<1184, 256, 0, st>>>(c, planes);
+}
+
+__global__ void k_halo_copy(Ctx c, int side, int planes, float* out, const float* in) {
+  if (c.ctrl->done) return;
+  const int par = c.ctrl->step_index & 1;
+  const SceneDev& sc = c.scenes[0];
+  const long long per = (long long)sc.gdim[0] * sc.gdim[1];
+  const long long total = per * planes;
+  const int z0 = side == 0 ? 0 : sc.dims[2] - planes;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x) {
+    const int zr = static_cast<int>(i / per);
+    const int rem = static_cast<int>(i - (long long)zr * per);
+    const int y = rem / sc.gdim[0], x = rem - y * sc.gdim[0];
+    const long long node = sc.node_base + ((long long)(z0 + zr) * sc.gdim[1] + y) * sc.gdim[0] + x;
+    float4* b0 = reinterpret_cast<float4*>(out ? out : const_cast<float*>(in));
+    float4* b1 = b0 + total;
+    float* bh = reinterpret_cast<float*>(b1 + total);
+    if (out) {
+      b0[i] = c.g.acc0[par][node];
+      b1[i] = c.g.acc1[par][node];
+      if (c.conduct) bh[i] = c.g.heat[par][node];
+    } else if (node_active(c, sc, x, y, z0 + zr)) {
+      const float4 p = c.g.acc0[par][node], q = b0[i];
+      c.g.acc0[par][node] = make_float4(p.x + q.x, p.y + q.y, p.z + q.z, p.w + q.w);
+      const float4 r = c.g.acc1[par][node], t = b1[i];
+      c.g.acc1[par][node] = make_float4(r.x + t.x, r.y + t.y, r.z + t.z, r.w + t.w);
+      if (c.conduct) c.g.heat[par][node] += bh[i];
+    }
+  }
+}
+
+void launch_halo_export(const Ctx& c, cudaStream_t st, int side, int planes, float* buf) {
+  k_halo_copy<<<592, 256, 0, st>>>(c, side, planes, buf, nullptr);
+}
+
+void launch_halo_add(const Ctx& c, cudaStream_t st, int side, int planes, const float* buf) {
+  k_halo_copy<<<592, 256, 0, st>>>(c, side, planes, nullptr, buf);
+}
 
 // Clears a pending scattered grid (acc[step_index & 1] over its active list) without using it.
 __global__ void __launch_bounds__(256) k_grid_clear(Ctx c) {

@@ -126,6 +126,12 @@ SIGNATURES = {
     "mpm_regularize": (ctypes.c_int, [_P, _D]),
     "mpm_regularize_host": (ctypes.c_int, [_P, ctypes.POINTER(MpmParticles), _D]),
     "mpm_exchange_heat": (ctypes.c_int, [_P, ctypes.POINTER(MpmHeatExchange), _D, ctypes.POINTER(_D)]),
+    "mpm_batch_set_slabs": (ctypes.c_int, [_P, _I32]),
+    "mpm_set_open_faces": (ctypes.c_int, [_P, _I32]),
+    "mpm_prepare": (ctypes.c_int, [_P]),
+    "mpm_halo_bytes": (ctypes.c_int, [_P, _I32, ctypes.POINTER(_I64)]),
+    "mpm_halo_export": (ctypes.c_int, [_P, _I32, _I32, _P]),
+    "mpm_halo_add": (ctypes.c_int, [_P, _I32, _I32, _P]),
     "mpm_get_stream": (ctypes.c_int, [_P, ctypes.POINTER(_P)]),
     "mpm_upload_particles": (ctypes.c_int, [_P, _I64, ctypes.POINTER(MpmParticles)]),
     "mpm_download_particles": (ctypes.c_int, [_P, ctypes.POINTER(MpmParticles)]),

@@ -1,0 +1,89 @@
+"""One scene split into slabs along z (mpm_b200.slabs): grid alignment, the particle partition and
+the overlap-exchange protocol between ranks, on the CPU (gloo, world size 2 and 3, over numpy
+stand-ins for the device planes). GPU tests of the device paths: tests/test_gpu_slabs.py."""
+import os
+
+import numpy as np
+import pytest
+import torch.distributed as dist
+import torch.multiprocessing as mp
+
+from mpm_b200 import scenes
+from mpm_b200.slabs import halo_exchange, partition, slab_domains
+
+
+def test_slab_grids_align_and_share_the_planes():
+    sc = scenes.j2_drop(shape=(16, 16, 16), grid=48)
+    for nslabs in (2, 3):
+        slabs = slab_domains(sc.domain, nslabs, 6)
+        d = sc.domain
+        assert slabs[0].nodes[0] == 0 and slabs[-1].nodes[1] == d.dims[2]
+        for k, s in enumerate(slabs):
+            assert s.domain.dims[:2] == d.dims[:2] and s.domain.origin[:2] == d.origin[:2]
+            assert abs(s.domain.origin[2] - (d.origin[2] + s.nodes[0] * d.H)) < 1e-12
+            assert s.domain.dims[2] == s.nodes[1] - s.nodes[0]
+            if k > 0:
+                assert slabs[k - 1].nodes[1] - s.nodes[0] == 6  # the shared planes
+                assert s.own[0] - s.nodes[0] == 3 and slabs[k - 1].nodes[1] - slabs[k - 1].own[1] == 3
+        parts = partition(sc, slabs)
+        idx = np.sort(np.concatenate([i for _, i in parts]))
+        assert np.array_equal(idx, np.arange(sc.n))  # every particle in exactly one slab
+        for k, ((p, _), s) in enumerate(zip(parts, slabs)):
+            zq = (p.x[:, 2] - s.domain.origin[2]) / d.H
+            # own range: 3 planes (half the shared ones) inside the slab's grid at each seam
+            lo = 3 if k > 0 else 0
+            hi = s.domain.dims[2] - (3 if k < nslabs - 1 else 0)
+            assert p.n == 0 or (zq.min() >= lo and zq.max() < hi)
+
+
+def test_bad_slab_requests_are_rejected():
+    sc = scenes.elastic_cube()
+    with pytest.raises(ValueError):
+        slab_domains(sc.domain, 2, 5)  # odd
+    with pytest.raises(ValueError):
+        slab_domains(sc.domain, 20, 6)  # too thin
+
+
+def _worker(rank, world, port, out):
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    import torch
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    rng = np.random.default_rng(rank)
+    planes = {0: rng.normal(size=8), 1: rng.normal(size=8)}  # this rank's own seam contributions
+    send, recv, held = {}, {}, {0: planes[0].copy(), 1: planes[1].copy()}
+
+    def export(s):
+        send[s] = torch.from_numpy(held[s].copy())
+
+    def swap(s, peer):
+        recv[s] = torch.empty(8, dtype=torch.float64)
+        ops = [dist.P2POp(dist.isend, send[s], peer), dist.P2POp(dist.irecv, recv[s], peer)]
+        for r in dist.batch_isend_irecv(ops):
+            r.wait()
+
+    def add(s):
+        held[s] = held[s] + recv[s].numpy()
+
+    sides = halo_exchange(rank, world, export, add, swap)
+    out[rank] = (sides, {s: held[s].tolist() for s in sides}, {s: planes[s].tolist() for s in (0, 1)})
+    dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_rank_exchange_sums_both_sides_of_every_seam(world):
+    port = 29600 + world
+    with mp.Manager() as m:
+        out = m.dict()
+        mp.spawn(_worker, args=(world, port, out), nprocs=world, join=True)
+        res = dict(out)
+    for r in range(world):
+        sides, held, own = res[r]
+        assert sides == [s for s, p in ((0, r - 1), (1, r + 1)) if 0 <= p < world]
+        for s in sides:
+            peer = r - 1 if s == 0 else r + 1
+            other = res[peer][2][1 - s]  # the neighbour's contribution on the same seam
+            np.testing.assert_allclose(held[s], np.add(own[s], other), rtol=0, atol=0)
+    # both copies of a seam hold the same sum (addition is commutative in floating point)
+    for r in range(world - 1):
+        np.testing.assert_array_equal(res[r][1][1], res[r + 1][1][0])
