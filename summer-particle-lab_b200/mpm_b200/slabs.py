@@ -152,5 +152,17 @@ class SlabRank:
             self.solver.step_fixed(dt, 1)
             self.exchange()
 
+    def advance(self, duration):
+        """Substeps until `duration` seconds have passed, each at the smallest stable dt over ranks
+        (cut to the time left), so every rank takes the same substeps; returns their number."""
+        t, n = 0.0, 0
+        while duration - t > 1e-9 * duration:
+            dt = self.reduce_min(min(self.solver.stable_dt(), duration - t))
+            self.solver.step_fixed(dt, 1)
+            self.exchange()
+            t += dt
+            n += 1
+        return n
+
     def close(self):
         self.solver.close()

@@ -87,3 +87,50 @@ def test_rank_exchange_sums_both_sides_of_every_seam(world):
     # both copies of a seam hold the same sum (addition is commutative in floating point)
     for r in range(world - 1):
         np.testing.assert_array_equal(res[r][1][1], res[r + 1][1][0])
+
+
+class _FakeSolver:
+    """Stands in for a slab's single-scene handle: a stable dt of its own, a log of fixed substeps."""
+
+    def __init__(self, dt):
+        self.dt, self.taken = dt, []
+
+    def stable_dt(self):
+        return self.dt
+
+    def step_fixed(self, dt, n):
+        self.taken += [dt] * n
+
+
+def _advance_worker(rank, world, port, out):
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    import torch
+    from mpm_b200.slabs import SlabRank
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+
+    def reduce_min(x):
+        t = torch.tensor([x], dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MIN)
+        return float(t.item())
+
+    sr = SlabRank.__new__(SlabRank)
+    sr.rank, sr.world, sr.reduce_min = rank, world, reduce_min
+    sr.solver = _FakeSolver(dt=3e-4 * (1 + rank))  # rank 0 is the slowest to stay stable
+    exchanges = []
+    sr.exchange = lambda: exchanges.append(len(sr.solver.taken))
+    n = sr.advance(1e-3)
+    out[rank] = (n, sr.solver.taken, exchanges)
+    dist.destroy_process_group()
+
+
+def test_ranks_advance_with_the_same_substeps():
+    world = 2
+    with mp.Manager() as m:
+        out = m.dict()
+        mp.spawn(_advance_worker, args=(world, 29610, out), nprocs=world, join=True)
+        res = dict(out)
+    n0, taken0, ex0 = res[0]
+    assert n0 == 4 and ex0 == [1, 2, 3, 4]  # 3 x 3e-4 and the 1e-4 left; one exchange after each
+    np.testing.assert_allclose(taken0, [3e-4, 3e-4, 3e-4, 1e-4], rtol=1e-12)
+    assert res[1] == res[0]
