@@ -79,7 +79,8 @@ struct mpm_handle {
   bool grid_valid = false;   // acc[step_index & 1] holds the scatter of the current state
   bool pending_grid = false; // a scatter sits in acc[step_index & 1] (valid or stale)
   int use_tma = 1;
-  int last_estimate = 0;
+  int last_estimate = 0;           // substeps the last requested-dt call took (0: query the CFL dt first)
+  double last_dt_requested = 0;
   // device memory
   void* pblock = nullptr;  size_t pblock_bytes = 0;   // particle arrays (current home order)
   void* pblock_alt = nullptr;                           // the other buffer of the permutation pass
@@ -748,6 +749,7 @@ int mpm_set_material(mpm_handle* h, int32_t index, const mpm_material* material)
                               sizeof(mpm::MaterialExt), cudaMemcpyHostToDevice, h->stream));
   refresh_flags(h);
   h->grid_valid = false;  // stresses change
+  h->last_estimate = 0;
   return MPM_OK;
 }
 
@@ -884,6 +886,7 @@ int mpm_upload_particles(mpm_handle* h, int64_t n, const mpm_particles* p) {
     MPM_CUDA(h, cudaGetLastError());
     h->n = n;
     h->uploaded = true;
+    h->last_estimate = 0;
     h->grid_valid = false;
     h->reorder_pending = true;
     MPM_CUDA(h, cudaStreamSynchronize(h->stream));
@@ -907,6 +910,7 @@ int mpm_upload_particles(mpm_handle* h, int64_t n, const mpm_particles* p) {
                               h->stream));
   h->n = n;
   h->uploaded = true;
+  h->last_estimate = 0;
   h->grid_valid = false;
   h->reorder_pending = true;
   MPM_CUDA(h, cudaStreamSynchronize(h->stream));
@@ -1142,7 +1146,11 @@ static int run_substeps(mpm_handle* h, int mode, double dt_req, int max_substeps
   { ProfScope ps(h, -1); mpm::launch_control_step(h->ctx, h->stream, mode, dt_req, max_substeps, dt_fixed); }
   int launched = 0;
   int est;
-  if (mode == mpm::kModeRequested) {
+  if (mode == mpm::kModeRequested && h->last_estimate > 0 && h->last_dt_requested == dt_req) {
+    // the previous call's substep count for the same requested dt: no host round trip before the
+    // launches (substeps past the end return at once; a short estimate is topped up below)
+    est = std::min(h->last_estimate, max_substeps);
+  } else if (mode == mpm::kModeRequested) {
     double dt = 0;
     int rc = mpm_stable_dt(h, &dt);
     if (rc != MPM_OK) return rc;
@@ -1169,13 +1177,19 @@ static int run_substeps(mpm_handle* h, int mode, double dt_req, int max_substeps
     const bool finished = ct.done || ct.substeps >= max_substeps ||
                           (mode == mpm::kModeRequested && !(ct.remaining > 1e-6 * dt_req)) || launched >= max_substeps;
     if (finished || (ct.status & (MPM_STATUS_NONFINITE | MPM_STATUS_TIMEOUT))) break;
+    // the substeps still needed at this call's mean dt so far
     est = 1;
+    if (mode == mpm::kModeRequested && ct.substeps > 0 && ct.advanced > 0) {
+      const double need = std::ceil(ct.remaining / (ct.advanced / ct.substeps) - 1e-9);
+      est = static_cast<int>(std::max(1.0, std::min(need, static_cast<double>(max_substeps - launched))));
+    }
   }
   h->pending_grid = true;
   const mpm::Ctrl& ct = *h->host_ctrl;
   if (substeps) *substeps = ct.substeps;
   if (advanced) *advanced = ct.advanced;
-  h->last_estimate = ct.substeps;
+  h->last_estimate = mode == mpm::kModeRequested ? ct.substeps : 0;
+  h->last_dt_requested = dt_req;
   return check_status(h);
 }
 
@@ -1740,6 +1754,7 @@ int mpm_checkpoint_load(mpm_handle* h, const char* path) {
                               h->stream));
   MPM_CUDA(h, cudaStreamSynchronize(h->stream));
   h->uploaded = true;
+  h->last_estimate = 0;
   h->grid_valid = false;
   return MPM_OK;
 }

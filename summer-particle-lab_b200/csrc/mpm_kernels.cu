@@ -997,6 +997,37 @@ __device__ __forceinline__ unsigned particle_phase_a(const Ctx& c, const SceneDe
   return key;
 }
 
+// L2 prefetch of the particle state a claimed tile will read. Between physical re-sorts a tile's
+// particles keep the contiguous home range the last re-sort gave them (apart from the few that
+// changed tiles since), and the tile's perm lists them in about that order; one perm entry from the
+// middle places the range, and one bulk prefetch per state array covers it with a margin. Only a
+// hint: the range is clipped to the live particles and a wrong guess costs bandwidth, not results.
+template <bool AUX>
+__device__ __forceinline__ void prefetch_tile_state(const Ctx& c, uint4 it) {
+  const long long cnt = it.z;
+  if (cnt == 0) return;
+  const long long mid = c.p.perm[it.y + it.z / 2];
+  const long long lo = max(0ll, mid - (3 * cnt) / 4 - 32), hi = min(static_cast<long long>(c.n), mid + (3 * cnt) / 4 + 32);
+  if (hi <= lo) return;
+  auto pf = [&](const void* base, int esize) {
+    const unsigned long long a = (reinterpret_cast<unsigned long long>(base) + lo * esize) & ~15ull;
+    const unsigned long long b = (reinterpret_cast<unsigned long long>(base) + hi * esize + 15) & ~15ull;
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(a), "r"(static_cast<unsigned>(b - a)) : "memory");
+  };
+  pf(c.p.qx, 4);
+  pf(c.p.qy, 4);
+  pf(c.p.qz, 4);
+#pragma unroll
+  for (int e = 0; e < 9; ++e) pf(c.p.Dc[e], 4);
+  pf(c.p.m, 4);
+  pf(c.p.V, 4);
+  if (c.has_plastic) pf(c.p.ep, 4);
+  if (c.has_thermal) pf(c.p.T, 4);
+  if (AUX) pf(c.p.aux, 4);
+  if (!c.single_material) pf(c.p.mat, 2);
+  if (c.has_pinned) pf(c.p.pinned, 1);
+}
+
 template <int PASS, bool HEAT, bool AUX>
 __global__ void __launch_bounds__(kBlock, 2) k_particles(const __grid_constant__ Ctx c) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -1068,6 +1099,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_particles(const __grid_constant__
                     ((lt / sn.tiles[0]) % sn.tiles[1]) * kTile, (lt / (sn.tiles[0] * sn.tiles[1])) * kTile,
                     &sm.mbar[cb ^ 1]);
       }
+      if (nx.x != 0xffffffffu) prefetch_tile_state<AUX>(c, nx);
     };
     const int scene = static_cast<int>(it.w);
     const SceneDev& sc = c.scenes[scene];
