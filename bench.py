@@ -43,7 +43,7 @@ BYTES_PER_NODE = 56
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=500)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="j2_drop")
@@ -109,25 +109,58 @@ def cpu_oracle_rate(scene, dt, steps, threads):
 
 
 class Clocks:
+    """SM clocks, power and clock-event reasons sampled during the run: an NVML thread every 20 ms
+    (read-only queries), or `nvidia-smi -lms 100` when NVML is unavailable. Samples are written to
+    gpurun_out/clocks_bench_<pid>.csv with their host time."""
     QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NAMES = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
 
     def __init__(self, index):
         self.index = index
         self.proc = None
+        self.thread = None
+        self.rows = []  # (time, sm_mhz, max_mhz, power_w, [active reason names])
         self.path = os.path.join(ROOT, "gpurun_out", f"clocks_bench_{os.getpid()}.csv")
 
     def wait_first_sample(self, timeout=5.0):
         t0 = time.time()
-        while self.proc is not None and time.time() - t0 < timeout:
-            if os.path.exists(self.path) and os.path.getsize(self.path) > 0:
+        while time.time() - t0 < timeout:
+            if self.rows or (self.proc is not None and os.path.exists(self.path) and os.path.getsize(self.path) > 0):
                 return
-            time.sleep(0.05)
+            if self.thread is None and self.proc is None:
+                return
+            time.sleep(0.02)
+
+    def _nvml_loop(self, nv, h):
+        bits = [nv.nvmlClocksEventReasonHwSlowdown, nv.nvmlClocksEventReasonHwThermalSlowdown,
+                nv.nvmlClocksEventReasonSwThermalSlowdown, nv.nvmlClocksEventReasonSwPowerCap]
+        while not self.stop:
+            try:
+                sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+                pw = nv.nvmlDeviceGetPowerUsage(h) / 1e3
+                rs = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                self.rows.append((time.time(), float(sm), float(mx), pw, [n for n, b in zip(self.NAMES, bits) if rs & b]))
+            except Exception:
+                pass
+            time.sleep(0.02)
 
     def __enter__(self):
+        os.makedirs(os.path.dirname(self.path), exist_ok=True)
         try:
-            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            import threading
+            import pynvml as nv
+            nv.nvmlInit()
+            h = nv.nvmlDeviceGetHandleByIndex(self.index)
+            self.stop = False
+            self.thread = threading.Thread(target=self._nvml_loop, args=(nv, h), daemon=True)
+            self.thread.start()
+            return self
+        except Exception:
+            self.thread = None
+        try:
             self.f = open(self.path, "w")
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}",
                                           "--format=csv,noheader,nounits", "-lms", "100"],
@@ -138,6 +171,13 @@ class Clocks:
         return self
 
     def __exit__(self, *a):
+        if self.thread is not None:
+            self.stop = True
+            self.thread.join(timeout=2)
+            with open(self.path, "w") as f:
+                f.write("time,sm_mhz,max_sm_mhz,power_w,reasons\n")
+                for t, sm, mx, pw, rs in self.rows:
+                    f.write(f"{t:.3f},{sm:.0f},{mx:.0f},{pw:.1f},{'|'.join(rs) or 'none'}\n")
         if self.proc is not None:
             self.proc.terminate()
             try:
@@ -147,8 +187,20 @@ class Clocks:
             self.f.close()
 
     def summary(self, t_start=None, t_end=None):
-        """Samples taken during [t_start, t_end] (the timed region), widened by one sampling period
-        on each side when the region is shorter than the sampling interval."""
+        """Median SM clock, max clock and the reasons seen in the samples taken during [t_start,
+        t_end] (the timed region)."""
+        if self.thread is not None:
+            rows = [r for r in self.rows if t_start is None or t_start <= r[0] <= t_end]
+            if not rows:  # a region shorter than the sampling period: the samples on either side
+                before = [r for r in self.rows if r[0] < t_start][-1:]
+                after = [r for r in self.rows if r[0] > t_end][:1]
+                rows = before + after
+            if not rows:
+                return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+            sm = sorted(r[1] for r in rows)
+            return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": max(r[2] for r in rows),
+                    "reasons": sorted({n for r in rows for n in r[4]}), "samples": len(rows),
+                    "power_w_median": sorted(r[3] for r in rows)[len(rows) // 2], "source": "nvml"}
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         rows_all = []
@@ -166,10 +218,9 @@ class Clocks:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
         sm = sorted(float(r[1]) for r in rows if r[1].replace(".", "").isdigit())
         mx = max(float(r[2]) for r in rows if r[2].replace(".", "").isdigit())
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[k] for r in rows for k in range(4) if "Active" in r[5 + k] and "Not" not in r[5 + k]})
+        reasons = sorted({self.NAMES[k] for r in rows for k in range(4) if "Active" in r[5 + k] and "Not" not in r[5 + k]})
         return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": mx, "reasons": reasons,
-                "samples": len(rows)}
+                "samples": len(rows), "source": "nvidia-smi"}
 
 
 def read_traffic_per_particle():
@@ -466,7 +517,7 @@ def main():
     sol = Solver(scene.domain, scene.n)
     sol.upload(scene)
     ext = torch.cuda.ExternalStream(sol.stream())
-    clk = Clocks(local if world == 1 else 0)
+    clk = Clocks(local)
     clk.__enter__()  # sampling starts before warm-up so the timed region is covered
     for _ in range(args.warmup):
         sol.step(dt_req)
@@ -474,7 +525,6 @@ def main():
     clk.wait_first_sample()
     if dist is not None:
         dist.barrier()
-    sol.profile(True)
     launches0 = sol.launch_count()
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
@@ -488,12 +538,28 @@ def main():
     ev1.record(ext)
     torch.cuda.synchronize()
     t_end = time.time()
-    time.sleep(0.25)
-    clk.__exit__()
     launches = sol.launch_count() - launches0
+    ms = ev0.elapsed_time(ev1)
+    # the same K steps again with a CUDA event pair around every kernel launch (on the library's
+    # stream) for the per-kernel durations of the roofline; events between the launches of the
+    # headline pass would add about 5% to it
+    if dist is not None:
+        dist.barrier()
+    sol.profile(True)
+    torch.cuda.synchronize()
+    kp0 = torch.cuda.Event(enable_timing=True)
+    kp1 = torch.cuda.Event(enable_timing=True)
+    kp0.record(ext)
+    for _ in range(args.steps):
+        sol.step(dt_req)
+    kp1.record(ext)
+    torch.cuda.synchronize()
+    t_end2 = time.time()
     prof = sol.profile_read()
     sol.profile(False)
-    ms = ev0.elapsed_time(ev1)
+    kernel_pass_ms = kp0.elapsed_time(kp1) / args.steps
+    time.sleep(0.25)
+    clk.__exit__()
     el_t = torch.tensor([ms, scene.n * substeps], dtype=torch.float64, device="cuda")
     if dist is not None:
         mx = el_t.clone()
@@ -516,7 +582,10 @@ def main():
                 "traffic": (traffic_pp * scene.n if traffic_pp else None),
                 "kernel": "k_g2p2g", "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind,
                 "algorithmic_bytes_per_launch": alg_bytes, "launch_ms": g_ms / g_n if g_n else None,
-                "share_of_step": g_ms / sum(v[0] for v in prof.values()) if g_n else None}
+                "share_of_step": g_ms / sum(v[0] for v in prof.values()) if g_n else None,
+                "timing": f"CUDA events around each launch in a second pass of the same {args.steps} steps "
+                          f"({kernel_pass_ms:.3f} ms per step with the events)",
+                "clocks": clk.summary(t_end, t_end2)}
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_all / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
@@ -569,9 +638,9 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         sample = sample_scene(scene, 2)
         threads = os.cpu_count() or 1
-        rate, el = cpu_oracle_rate(sample, 5e-7, 30, threads)
+        rate, el = cpu_oracle_rate(sample, 5e-7, 200, threads)
         line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
-                                "sample": f"{sample.n}-particle sub-block (1/8) of the workload, 30 substeps "
+                                "sample": f"{sample.n}-particle sub-block (1/8) of the workload, 200 substeps "
                                           f"({el:.1f} s), FP64 oracle with OpenMP"}
     if not args.no_ensemble:
         line["ensemble"] = ensemble_leg(args, rank, world, dist)

@@ -460,7 +460,11 @@ void launch_sort_scatter(const Ctx& c, cudaStream_t st, bool initial) {
 //      63 shared atomics per bucket and layer (about 24 per particle instead of 189)
 // then one float4 atomic per touched node and channel group flushes the window to HBM.
 
-constexpr int kCap = 512;      // particles per scatter round
+// Particles per scatter round. A full tile holds 512 (64 cells x 8), but a block that drifts by a
+// fraction of a cell leaves a third of its tiles a few particles over 512 (up to ~530); at
+// kCap = 512 those took a second round (every phase and barrier again for a handful of particles).
+constexpr int kCap = 768;
+constexpr int kPf = 2;         // perm entries of the next tile's first round held in registers per thread
 constexpr int kPay = 23;       // payload floats per particle (the last, m T, only with conduction)
 constexpr int kBuckets = 216;  // 6^3 possible stencil bases in the scatter window
 // Payload slot of particle j: one extra word every 32 slots, so the slots phase B reads at a
@@ -505,6 +509,7 @@ struct __align__(128) PartSmem {
 };
 
 size_t particle_smem_bytes() { return sizeof(PartSmem); }
+static_assert(sizeof(PartSmem) <= 112 * 1024, "two CTAs per SM");
 
 // Direct global scatter (rare: particles that left the window, pinned particles): 27 nodes x
 // channel atomics straight to the accumulators, and the node tiles they touch become active.
@@ -1067,7 +1072,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_particles(const __grid_constant__
   int cb = 0;
   int mt_row = -1;  // material row held in sm.mt
   // perm entries of the next tile's first round (j = tid, tid + kBlock), loaded one tile ahead
-  unsigned pf[kCap / kBlock] = {};
+  unsigned pf[kPf] = {};
   bool pf_ok = false;
   while (true) {
     __syncthreads();
@@ -1156,7 +1161,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_particles(const __grid_constant__
         const unsigned j = jj + threadIdx.x;
         unsigned key = 0xffffffffu;
         if (j < nround) {
-          const unsigned home = (r0 == 0 && pf_ok) ? pf[jj / kBlock] : c.p.perm[it.y + r0 + j];
+          const unsigned home = (r0 == 0 && pf_ok && jj < kPf * kBlock) ? pf[jj / kBlock] : c.p.perm[it.y + r0 + j];
           key = particle_phase_a<PASS, HEAT, AUX>(c, sc, tc, sm.mt, single, sm.vwin[cb], home, j, dt, nxt, sm.pay, sm.meta,
                                        sm.hist, wave_acc, grad_acc, flags_acc, work_acc);
         }
@@ -1186,7 +1191,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_particles(const __grid_constant__
           pf_ok = nx.x != 0xffffffffu;
           if (pf_ok) {
 #pragma unroll
-            for (int k = 0; k < kCap / kBlock; ++k) {
+            for (int k = 0; k < kPf; ++k) {
               const unsigned j = k * kBlock + threadIdx.x;
               pf[k] = j < nx.z ? c.p.perm[nx.y + j] : 0u;
             }
