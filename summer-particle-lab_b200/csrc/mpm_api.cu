@@ -1129,8 +1129,11 @@ static int run_substeps_regularized(mpm_handle* h, int mode, double dt_req, int 
   return check_status(h);
 }
 
+// final_gather: the caller replaces the particle state after the call (mpm_frame_host), so the
+// estimated last substep runs the gather-only pass; the scatter it would make is never used. If
+// more substeps turn out to be needed, the state is scattered again (prepare_grid) first.
 static int run_substeps(mpm_handle* h, int mode, double dt_req, int max_substeps, float dt_fixed, int* substeps,
-                        double* advanced) {
+                        double* advanced, bool final_gather = false) {
   if (!h->uploaded) return fail(h, MPM_ERR_STATE, "no particles uploaded");
   if (h->n == 0) {
     if (substeps) *substeps = 0;
@@ -1161,7 +1164,7 @@ static int run_substeps(mpm_handle* h, int mode, double dt_req, int max_substeps
   }
   while (true) {
     for (int i = 0; i < est; ++i) {
-      launch_substep(h, true);
+      launch_substep(h, !(final_gather && i == est - 1));
       // keep tiles contiguous in memory: a permutation pass after every reorder_interval substeps
       if (h->reorder_interval > 0 && ++h->substeps_since_reorder >= h->reorder_interval) {
         ProfScope ps(h, -1);
@@ -1177,6 +1180,11 @@ static int run_substeps(mpm_handle* h, int mode, double dt_req, int max_substeps
     const bool finished = ct.done || ct.substeps >= max_substeps ||
                           (mode == mpm::kModeRequested && !(ct.remaining > 1e-6 * dt_req)) || launched >= max_substeps;
     if (finished || (ct.status & (MPM_STATUS_NONFINITE | MPM_STATUS_TIMEOUT))) break;
+    if (final_gather) {  // the last substep ran and made no scatter: scatter the state again
+      h->pending_grid = false;
+      const int rc = prepare_grid(h);
+      if (rc != MPM_OK) return rc;
+    }
     // the substeps still needed at this call's mean dt so far
     est = 1;
     if (mode == mpm::kModeRequested && ct.substeps > 0 && ct.advanced > 0) {
@@ -1184,8 +1192,14 @@ static int run_substeps(mpm_handle* h, int mode, double dt_req, int max_substeps
       est = static_cast<int>(std::max(1.0, std::min(need, static_cast<double>(max_substeps - launched))));
     }
   }
-  h->pending_grid = true;
   const mpm::Ctrl& ct = *h->host_ctrl;
+  h->pending_grid = true;
+  if (final_gather) {
+    // every launch of the last batch ran (none returned at the done flag): the last one was the
+    // gather-only pass and left no scatter; otherwise an earlier scatter pass was the last to run
+    h->grid_valid = false;
+    h->pending_grid = ct.substeps < launched;
+  }
   if (substeps) *substeps = ct.substeps;
   if (advanced) *advanced = ct.advanced;
   h->last_estimate = mode == mpm::kModeRequested ? ct.substeps : 0;
@@ -1270,7 +1284,10 @@ int mpm_frame_host(mpm_handle* h, const mpm_particles* io, double dt_requested, 
                                nullptr, fields, true); }
   MPM_CUDA(h, cudaGetLastError());
   h->grid_valid = false;
-  rc = mpm_step(h, dt_requested, max_substeps, substeps, nullptr);
+  if (!(dt_requested > 0) || !std::isfinite(dt_requested)) return fail(h, MPM_ERR_INVALID_ARG, "dt must be positive");
+  if (max_substeps <= 0) max_substeps = 48;  // the reference's cap (src/three/simulation.js:308)
+  // the next frame replaces positions and velocities again: the last substep needs no scatter
+  rc = run_substeps(h, mpm::kModeRequested, dt_requested, max_substeps, 0.f, substeps, nullptr, true);
   if (rc != MPM_OK) return rc;
   mpm_particles out{};
   out.dtype = io->dtype;

@@ -126,3 +126,55 @@ def test_mpm3_exchange_heat_updates_caller_temperatures():
     assert s.temperature[0] < 80 and s.temperature[1] > 20
     assert abs(float(np.sum(s.enthalpy[:2])) - e0) <= 1e-6 * e0
     m.close()
+
+
+def oracle_frame(st, dt_frame, max_substeps=48):
+    """Simulation3.step's sub-stepping (src/three/simulation.js:305-311) on the oracle: substeps of
+    the stable dt, the last one taking exactly what is left."""
+    left, n = dt_frame, 0
+    while left > 1e-6 * dt_frame and n < max_substeps:
+        dt = min(st.stable_dt(), left)
+        if left - dt <= 1e-6 * dt_frame:
+            dt = left
+        st.step(dt)
+        left -= dt
+        n += 1
+    return n
+
+
+@pytest.mark.gpu
+def test_mpm3_frames_match_oracle_substeps():
+    """MPM3.frame (mpm_frame_host) over four frames against the oracle's sub-stepping: the same
+    substep counts, x within 1e-5 m and v within 1e-5 relative after every frame. The frame's last
+    substep skips the scatter the next upload would discard; the third frame multiplies the
+    caller's velocities by 30, so the substep count carried over from the previous frame falls
+    short and the call scatters the state again and tops the count up."""
+    from mpm_b200.mpm3 import MPM3
+    from oracle import oracle as orc
+    sc = moving_cube()
+    s = sim_from_scene(sc)
+    m = MPM3(s.capacity, sc.domain, {0: sc.materials[0]})
+    st = orc.state_from_scene(sc)
+    n = s.count
+    dt_frame = 3.5 * st.stable_dt()
+    subs = []
+    for frame in range(4):
+        if frame == 2:
+            s.vx[:n] *= 30.0
+            s.vy[:n] *= 30.0
+            s.vz[:n] *= 30.0
+            st.v = np.ascontiguousarray(np.stack([s.vx[:n], s.vy[:n], s.vz[:n]], 1))
+        sub = m.frame(s, dt_frame)
+        sub_ref = oracle_frame(st, dt_frame)
+        assert sub == sub_ref, (frame, sub, sub_ref)
+        if frame == 2:
+            assert sub > subs[-1]  # more substeps than the carried-over count
+        subs.append(sub)
+        x = np.stack([s.x[:n], s.y[:n], s.z[:n]], 1)
+        v = np.stack([s.vx[:n], s.vy[:n], s.vz[:n]], 1)
+        assert np.max(np.abs(x - st.x)) <= 1e-5, frame
+        assert np.max(np.abs(v - st.v)) <= 1e-5 * np.max(np.abs(st.v)), frame
+        # the device F and C of the frame's final gather-only substep match the oracle too
+        out = m.solver.download(("F", "C"))
+        assert np.max(np.abs(out["F"] - st.F)) <= 1e-5, frame
+    m.close()
