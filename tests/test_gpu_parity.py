@@ -315,3 +315,48 @@ def test_nonfinite_input_reports_error():
         a.step_fixed(2e-7, 1)
     assert e.value.code == -4
     assert a.status() & 1
+
+
+def dense_j2_scene(ppc_axis=3, grid=32, block=(8, 8, 8), v0=-60.0, seed=11):
+    """A block with ppc_axis^3 particles per cell (27 by default): a 4^3-cell tile then holds 1,728
+    particles, more than one scatter round of the fused pass takes, so its tiles run several rounds."""
+    d = scenes.Domain(lower=(0, 0, 0), upper=(1, 1, 1), H=1 / grid, gravity=(0, -9.8, 0), sticky_floor=True)
+    rng = np.random.default_rng(seed)
+    lo = np.array([10, 1, 10])
+    cells = np.stack(np.meshgrid(*[np.arange(b) for b in block], indexing="ij"), -1).reshape(-1, 3) + lo
+    sub = (np.stack(np.meshgrid(*[np.arange(ppc_axis)] * 3, indexing="ij"), -1).reshape(-1, 3) + 0.5) / ppc_axis
+    q = (cells[:, None, :] + sub[None, :, :]).reshape(-1, 3)
+    q += rng.uniform(-0.2, 0.2, q.shape) / ppc_axis
+    x = np.asarray(d.lower) + q * d.H
+    sc = scenes._scene("j2_dense", d, [scenes.aluminium_j2(5)], x, (0, v0, 0))
+    sc.m = sc.m * 8 / ppc_axis ** 3
+    sc.V = sc.V * 8 / ppc_axis ** 3
+    return sc
+
+
+def test_tiles_over_one_scatter_round_match_oracle():
+    """27 particles per cell (1,728 per full tile, three scatter rounds of the fused pass per tile):
+    grid after the first scatter, then one and ten J2 impact steps, within the one-step bounds."""
+    sc = dense_j2_scene()
+    dt = 1e-6
+    sol = Solver(sc.domain, sc.n)
+    sol.upload(sc)
+    st = orc.state_from_scene(sc)
+    gm_ref, gp_ref, _ = st.step(dt, want_grid=True)
+    gm, gp = sol.grid_debug(dt)
+    assert rel(gm, gm_ref) <= 1e-6
+    assert rel(gp, gp_ref) <= 1e-6
+    sol.step_fixed(dt, 1)
+    out = sol.download()
+    assert np.max(np.abs(out["x"] - st.x)) <= 1e-6
+    assert np.max(np.abs(out["F"] - st.F)) <= 1e-6
+    for _ in range(9):
+        st.step(dt)
+    sol.step_fixed(dt, 9)
+    out = sol.download()
+    assert np.max(st.ep) > 0  # the impact yields
+    assert np.max(np.abs(out["x"] - st.x)) <= 1e-6
+    assert np.max(np.abs(out["F"] - st.F)) <= 2e-6
+    assert np.max(np.abs(out["ep"] - st.ep)) <= 2e-6 + 1e-4 * np.max(st.ep)
+    assert sol.status() == 0
+    sol.close()
