@@ -59,6 +59,11 @@ PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
 struct mpm_handle {
   std::string err;
   cudaStream_t stream = nullptr;
+  // The tile sort after a scatter pass runs on `side` beside the next substep's k_begin and grid
+  // update; `main_ev` orders it after the pass, `side_ev` orders the next pass after it.
+  cudaStream_t side = nullptr;
+  cudaEvent_t main_ev = nullptr, side_ev = nullptr;
+  bool side_pending = false;
   int num_sms = 148;
   mpm_domain dom{};
   SceneDev scene{};                  // scene 0 (the only scene of a single-scene handle)
@@ -127,7 +132,8 @@ struct ProfScope {
   int id;
   size_t idx = 0;
   bool on;
-  ProfScope(mpm_handle* hh, int kid) : h(hh), id(kid), on(hh->profiling) {
+  cudaStream_t st;
+  ProfScope(mpm_handle* hh, int kid, cudaStream_t s = nullptr) : h(hh), id(kid), on(hh->profiling), st(s ? s : hh->stream) {
     ++h->launches;
     if (!on) return;
     if (h->ev_next + 2 > h->ev_pool.size()) {
@@ -139,11 +145,11 @@ struct ProfScope {
     }
     idx = h->ev_next;
     h->ev_next += 2;
-    cudaEventRecord(h->ev_pool[idx], h->stream);
+    cudaEventRecord(h->ev_pool[idx], st);
   }
   ~ProfScope() {
     if (!on) return;
-    cudaEventRecord(h->ev_pool[idx + 1], h->stream);
+    cudaEventRecord(h->ev_pool[idx + 1], st);
     h->ev_used.push_back({id, static_cast<int>(idx)});
   }
 };
@@ -276,7 +282,15 @@ static size_t carve_particles(char* base, int64_t cap, mpm::Particles& p) {
 }
 
 // Permutation pass: rewrite the state in sort order into the other buffer and make it current.
+// The main stream waits for a tile sort still running on the side stream.
+static void join_side(mpm_handle* h) {
+  if (!h->side_pending) return;
+  cudaStreamWaitEvent(h->stream, h->side_ev, 0);
+  h->side_pending = false;
+}
+
 static int permute_state(mpm_handle* h) {
+  join_side(h);
   h->ctx.n = h->n;
   mpm::launch_permute(h->ctx, h->palt, h->stream);
   MPM_CUDA(h, cudaGetLastError());
@@ -413,6 +427,7 @@ static void refresh_flags(mpm_handle* h) {
 }
 
 static int check_status(mpm_handle* h) {
+  join_side(h);
   MPM_CUDA(h, cudaMemcpyAsync(h->host_ctrl, h->ctx.ctrl, sizeof(mpm::Ctrl), cudaMemcpyDeviceToHost, h->stream));
   MPM_CUDA(h, cudaStreamSynchronize(h->stream));
   const unsigned st = h->host_ctrl->status;
@@ -426,6 +441,7 @@ static int check_status(mpm_handle* h) {
 
 // Counting sort of the current state by tile and the dt-free P2G into acc[step_index & 1].
 static int prepare_grid(mpm_handle* h) {
+  join_side(h);
   Ctx& c = h->ctx;
   c.n = h->n;
   if (h->pending_grid) {
@@ -436,7 +452,7 @@ static int prepare_grid(mpm_handle* h) {
   { ProfScope ps(h, -1); mpm::launch_control_init(c, h->stream); }
   MPM_CUDA(h, cudaMemsetAsync(c.s.count, 0, sizeof(unsigned) * (c.total_tiles + 1), h->stream));
   { ProfScope ps(h, 6); mpm::launch_keys(c, h->stream); }
-  { ProfScope ps(h, 3); mpm::launch_scan(c, h->stream); }
+  { ProfScope ps(h, 3); mpm::launch_scan(c, h->stream, true); }
   { ProfScope ps(h, 4); mpm::launch_sort_scatter(c, h->stream, true); }
   if (h->reorder_pending) {
     ProfScope ps(h, -1);
@@ -452,6 +468,12 @@ static int prepare_grid(mpm_handle* h) {
   return MPM_OK;
 }
 
+// One substep: k_begin and the grid update (beside the previous pass's tile sort, if that is still
+// running on the side stream), then the particle pass; a scatter pass forks its tile sort (scan +
+// counting sort of the keys it wrote) onto the side stream, where it overlaps the next substep's
+// k_begin and grid update. The two never touch the same data: the sort works on the keys, counts,
+// perm and the work list of the pass's parity, k_begin and the grid update on the control block's
+// step fields, the other list's counters and the grid.
 static void launch_substep(mpm_handle* h, bool scatter) {
   Ctx& c = h->ctx;
   { ProfScope ps(h, 0); mpm::launch_begin(c, h->stream); }
@@ -460,11 +482,16 @@ static void launch_substep(mpm_handle* h, bool scatter) {
     ProfScope ps(h, -1);
     mpm::launch_conduct(c, h->stream, h->grid_blocks);
   }
+  join_side(h);
   { ProfScope ps(h, 2); mpm::launch_g2p2g(c, h->stream, h->g2p2g_blocks, scatter); }
   if (scatter && h->slab_planes) { ProfScope ps(h, -1); mpm::launch_halo_sum(c, h->stream, h->slab_planes); }
   if (scatter) {
-    { ProfScope ps(h, 3); mpm::launch_scan(c, h->stream); }
-    { ProfScope ps(h, 4); mpm::launch_sort_scatter(c, h->stream, false); }
+    cudaEventRecord(h->main_ev, h->stream);
+    cudaStreamWaitEvent(h->side, h->main_ev, 0);
+    { ProfScope ps(h, 3, h->side); mpm::launch_scan(c, h->side, false); }
+    { ProfScope ps(h, 4, h->side); mpm::launch_sort_scatter(c, h->side, false); }
+    cudaEventRecord(h->side_ev, h->side);
+    h->side_pending = true;
   }
 }
 
@@ -636,6 +663,15 @@ int mpm_create(const mpm_domain* domain, int64_t capacity, mpm_handle** out) {
     delete h;
     return MPM_ERR_CUDA;
   }
+  if (cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&h->main_ev, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&h->side_ev, cudaEventDisableTiming) != cudaSuccess) {
+    if (h->main_ev) cudaEventDestroy(h->main_ev);
+    if (h->side) cudaStreamDestroy(h->side);
+    cudaStreamDestroy(h->stream);
+    delete h;
+    return MPM_ERR_CUDA;
+  }
   h->dom = *domain;
   h->scene = s;
   h->scenes.assign(1, s);
@@ -649,6 +685,9 @@ int mpm_create(const mpm_domain* domain, int64_t capacity, mpm_handle** out) {
   const size_t pbytes = carve_particles(nullptr, capacity, p);
   auto bail = [&](int code) {
     free_device(h);
+    cudaEventDestroy(h->main_ev);
+    cudaEventDestroy(h->side_ev);
+    cudaStreamDestroy(h->side);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
     return code;
@@ -695,10 +734,15 @@ int mpm_create(const mpm_domain* domain, int64_t capacity, mpm_handle** out) {
 
 int mpm_destroy(mpm_handle* h) {
   if (!h) return MPM_ERR_INVALID_ARG;
+  join_side(h);
   if (h->stream) cudaStreamSynchronize(h->stream);
+  if (h->side) cudaStreamSynchronize(h->side);
   for (cudaEvent_t e : h->ev_pool) cudaEventDestroy(e);
   drop_graph(h);
   free_device(h);
+  if (h->main_ev) cudaEventDestroy(h->main_ev);
+  if (h->side_ev) cudaEventDestroy(h->side_ev);
+  if (h->side) cudaStreamDestroy(h->side);
   if (h->stream) cudaStreamDestroy(h->stream);
   delete h;
   return MPM_OK;
@@ -1173,6 +1217,7 @@ static int run_substeps(mpm_handle* h, int mode, double dt_req, int max_substeps
       }
     }
     launched += est;
+    join_side(h);
     MPM_CUDA(h, cudaGetLastError());
     MPM_CUDA(h, cudaMemcpyAsync(h->host_ctrl, h->ctx.ctrl, sizeof(mpm::Ctrl), cudaMemcpyDeviceToHost, h->stream));
     MPM_CUDA(h, cudaStreamSynchronize(h->stream));
@@ -1550,6 +1595,7 @@ int mpm_profile_enable(mpm_handle* h, int32_t on) {
 int mpm_profile_read(mpm_handle* h, double ms[MPM_PROFILE_KERNELS], int64_t launches[MPM_PROFILE_KERNELS]) {
   if (!h || !ms || !launches) return MPM_ERR_INVALID_ARG;
   MPM_CUDA(h, cudaStreamSynchronize(h->stream));
+  MPM_CUDA(h, cudaStreamSynchronize(h->side));  // the sort kernels' events
   for (int k = 0; k < MPM_PROFILE_KERNELS; ++k) {
     ms[k] = 0;
     launches[k] = 0;
@@ -2021,6 +2067,7 @@ static int capture_graph(mpm_handle* h, int count) {
   const bool prof = h->profiling;
   h->profiling = false;
   const int64_t launches0 = h->launches;  // captured launches run on replay, not now
+  join_side(h);  // the graph starts with nothing pending on the side stream
   MPM_CUDA(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
   for (int i = 0; i < count; ++i) {
     launch_substep(h, true);
@@ -2029,6 +2076,7 @@ static int capture_graph(mpm_handle* h, int count) {
       permute_state(h);
     }
   }
+  join_side(h);  // and ends with the side stream joined back
   cudaGraph_t g = nullptr;
   cudaError_t e = cudaStreamEndCapture(h->stream, &g);
   h->profiling = prof;
@@ -2082,6 +2130,7 @@ int mpm_batch_run(mpm_handle* h, int32_t nsteps, int32_t use_graph) {
       const int rc = capture_graph(h, chunk);
       if (rc != MPM_OK) return rc;
     }
+    join_side(h);
     while (left >= chunk) {
       MPM_CUDA(h, cudaGraphLaunch(h->graph, h->stream));
       h->launches += h->launches_per_graph;
@@ -2092,6 +2141,7 @@ int mpm_batch_run(mpm_handle* h, int32_t nsteps, int32_t use_graph) {
     const int rc = eager_substep(h);
     if (rc != MPM_OK) return rc;
   }
+  join_side(h);
   MPM_CUDA(h, cudaGetLastError());
   h->pending_grid = true;
   return check_status(h);

@@ -84,7 +84,8 @@ struct Ctrl {
   unsigned active_count[2];
   unsigned grid_next;
   unsigned scan_ticket;
-  unsigned pad[2];
+  unsigned sort_list;    // work list the sort after a scatter pass appends to (written by that pass)
+  unsigned sort_active;  // 1 if that pass ran (the sort and scan skip a pass that returned at done)
 };
 
 struct Particles {
@@ -168,7 +169,7 @@ __device__ __forceinline__ int find_scene_by_particle(const SceneDev* sc, int ns
 // Launch wrappers (mpm_kernels.cu)
 void launch_control_init(const Ctx& c, cudaStream_t st);
 void launch_keys(const Ctx& c, cudaStream_t st);
-void launch_scan(const Ctx& c, cudaStream_t st);
+void launch_scan(const Ctx& c, cudaStream_t st, bool initial);
 void launch_sort_scatter(const Ctx& c, cudaStream_t st, bool initial);
 void launch_p2g(const Ctx& c, cudaStream_t st, int grid_blocks);
 void launch_control_step(const Ctx& c, cudaStream_t st, int mode, double dt_req, int max_substeps, float dt_fixed);

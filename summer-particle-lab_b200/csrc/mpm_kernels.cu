@@ -320,8 +320,10 @@ constexpr int kScanChunk = kScanThreads * kScanPer;  // 4096 tiles per block
 
 // Exclusive scan of count[0..T] into start (block-local) + block_off (per 4096 tiles).
 // The last block to finish scans the block sums (threadfence + ticket).
-__global__ void __launch_bounds__(kScanThreads) k_scan(Ctx c) {
-  if (c.ctrl->done) return;
+// initial: the scan of a first sort (done is clear); otherwise the scan after a scatter pass, which
+// may run beside the next substep's opening kernels and so reads the pass's own flag, not done.
+__global__ void __launch_bounds__(kScanThreads) k_scan(Ctx c, int initial) {
+  if (initial ? c.ctrl->done != 0 : c.ctrl->sort_active == 0) return;
   if (c.ctrl->status & 0x8u) return;
   __shared__ unsigned warp_sums[32];
   __shared__ bool last;
@@ -399,9 +401,9 @@ __global__ void __launch_bounds__(kScanThreads) k_scan(Ctx c) {
   if (threadIdx.x == 0) c.ctrl->scan_ticket = 0;
 }
 
-void launch_scan(const Ctx& c, cudaStream_t st) {
+void launch_scan(const Ctx& c, cudaStream_t st, bool initial) {
   const int blocks = (c.total_tiles + 1 + kScanChunk - 1) / kScanChunk;
-  k_scan<<<blocks, kScanThreads, 0, st>>>(c);
+  k_scan<<<blocks, kScanThreads, 0, st>>>(c, initial ? 1 : 0);
 }
 
 __device__ __forceinline__ unsigned tile_start(const Ctx& c, unsigned k) {
@@ -409,8 +411,11 @@ __device__ __forceinline__ unsigned tile_start(const Ctx& c, unsigned k) {
 }
 
 // perm[start(k) + rank] = home slot; the group that claims a tile first appends the work item.
+// After a scatter pass the sort may run beside the next substep's k_begin and grid update, so it
+// takes its list and its go-ahead from the fields that pass wrote (sort_list, sort_active), which
+// k_begin does not touch.
 __global__ void __launch_bounds__(256) k_sort_scatter(Ctx c, int initial) {
-  if (!initial && c.ctrl->done) return;
+  if (!initial && c.ctrl->sort_active == 0) return;
   if (c.ctrl->status & 0x8u) return;  // a bounded wait gave up this substep
   const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   const unsigned key = i < c.n ? c.p.key[i] : 0xffffffffu;
@@ -432,7 +437,7 @@ __global__ void __launch_bounds__(256) k_sort_scatter(Ctx c, int initial) {
   }
   c.p.perm[s0 + old - 1 - below] = static_cast<unsigned>(i);
   if (lane == leader && old == cnt) {
-    const unsigned list = c.ctrl->step_index & 1u;
+    const unsigned list = initial ? (c.ctrl->step_index & 1u) : c.ctrl->sort_list;
     const unsigned idx = atomicAdd(&c.ctrl->work_count[list], 1u);
     const int s = c.nscenes == 1 ? 0 : find_scene_by_tile(c.scenes, c.nscenes, static_cast<int>(key));
     if (idx < static_cast<unsigned>(c.total_tiles)) c.s.work[list][idx] = make_uint4(key, s0, cnt, static_cast<unsigned>(s));
@@ -1040,6 +1045,10 @@ __global__ void __launch_bounds__(kBlock, 2) k_particles(const __grid_constant__
   constexpr bool SCATTER = PASS != kPassG2P;
   constexpr bool GATHER = PASS != kPassP2G;
   Ctrl* ct = c.ctrl;
+  if (PASS == kPassG2P2G && blockIdx.x == 0 && threadIdx.x == 0) {  // for the sort that follows
+    ct->sort_list = ct->step_index & 1u;
+    ct->sort_active = ct->done ? 0u : 1u;
+  }
   if (PASS != kPassP2G && ct->done) return;
   const unsigned k = ct->step_index;
   // lists: the P2G pass reads the list its sort just wrote (k & 1) and scatters into acc[k & 1];
@@ -1307,6 +1316,10 @@ __global__ void __launch_bounds__(kWsThreads, 1) k_particles_ws(const __grid_con
   WsSmem& sm = *reinterpret_cast<WsSmem*>(smem_raw);
   constexpr bool GATHER = PASS != kPassP2G;
   Ctrl* ct = c.ctrl;
+  if (PASS == kPassG2P2G && blockIdx.x == 0 && threadIdx.x == 0) {  // for the sort that follows
+    ct->sort_list = ct->step_index & 1u;
+    ct->sort_active = ct->done ? 0u : 1u;
+  }
   if (PASS != kPassP2G && ct->done) return;
   const unsigned k = ct->step_index;
   const int lst = PASS == kPassP2G ? (k & 1) : ((k - 1) & 1);
