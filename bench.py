@@ -639,9 +639,12 @@ def main():
         sample = sample_scene(scene, 2)
         threads = os.cpu_count() or 1
         rate, el = cpu_oracle_rate(sample, 5e-7, 200, threads)
+        rate1, el1 = cpu_oracle_rate(sample, 5e-7, 10, 1)  # the reference runs in one worker thread
         line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
+                                "value_1_thread": rate1,
                                 "sample": f"{sample.n}-particle sub-block (1/8) of the workload, 200 substeps "
-                                          f"({el:.1f} s), FP64 oracle with OpenMP"}
+                                          f"({el:.1f} s) on {threads} threads and 10 substeps ({el1:.1f} s) on one, "
+                                          f"FP64 oracle with OpenMP"}
     if not args.no_ensemble:
         line["ensemble"] = ensemble_leg(args, rank, world, dist)
     if rank == 0 and world == 1 and not args.no_surrogate:
