@@ -212,7 +212,9 @@ int mpm_step_host(mpm_handle* h, const mpm_particles* io, double dt);
 
 /* Simulation3.step(dt) drop-in for the solid path (src/three/simulation.js:305-311): positions and
  * velocities come from the caller's host arrays, the step advances dt_requested in CFL substeps on
- * the device, and positions and velocities are written back. */
+ * the device, and positions and velocities are written back. The call's last substep skips the
+ * scatter that the next call's upload would replace, so a following mpm_step scatters the state
+ * again first (same results, one extra scatter pass). */
 int mpm_frame_host(mpm_handle* h, const mpm_particles* io, double dt_requested, int32_t max_substeps,
                    int32_t* substeps);
 
