@@ -223,6 +223,11 @@ int mpm_ledger_compute(mpm_handle* h, mpm_ledger* out);
 /* MPM3.minJ(s) (src/three/mpm.js:135) */
 int mpm_min_j(mpm_handle* h, double* out);
 int mpm_status(mpm_handle* h, uint32_t* flags);
+/* Self-check of the device's bounded waits (the TMA window waits of the particle pass give up
+ * after about a second, set MPM_STATUS_TIMEOUT and leave the context usable): waits on a barrier
+ * that nothing completes for limit_cycles SM cycles on the handle's stream and reports
+ * *timed_out = 1 when the wait gave up. No other state changes. */
+int mpm_check_bounded_wait(mpm_handle* h, int64_t limit_cycles, int32_t* timed_out);
 int mpm_clear_status(mpm_handle* h);
 /* Grid after P2G of the current state with a step of dt: node mass and momentum including
  * dt * (stress force + m g), in node order ((z*ny)+y)*nx+x. Arrays of nx*ny*nz and 3*nx*ny*nz. */

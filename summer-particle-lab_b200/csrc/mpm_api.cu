@@ -1610,6 +1610,24 @@ int mpm_profile_read(mpm_handle* h, double ms[MPM_PROFILE_KERNELS], int64_t laun
   return MPM_OK;
 }
 
+int mpm_check_bounded_wait(mpm_handle* h, int64_t limit_cycles, int32_t* timed_out) {
+  if (!h || !timed_out) return MPM_ERR_INVALID_ARG;
+  if (limit_cycles <= 0 || limit_cycles > (1ll << 33))
+    return fail(h, MPM_ERR_INVALID_ARG, "limit_cycles must be in (0, 2^33]");
+  join_side(h);
+  unsigned* dev = nullptr;
+  MPM_CUDA(h, cudaMalloc(&dev, sizeof(unsigned)));
+  unsigned host = 0;
+  mpm::launch_wait_probe(h->stream, dev, limit_cycles);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&host, dev, sizeof(unsigned), cudaMemcpyDeviceToHost, h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  cudaFree(dev);
+  if (e != cudaSuccess) return fail(h, MPM_ERR_CUDA, cudaGetErrorString(e));
+  *timed_out = static_cast<int32_t>(host);
+  return MPM_OK;
+}
+
 int mpm_launch_count(mpm_handle* h, int64_t* count) {
   if (!h || !count) return MPM_ERR_INVALID_ARG;
   *count = h->launches;

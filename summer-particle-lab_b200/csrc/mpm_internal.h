@@ -170,6 +170,7 @@ __device__ __forceinline__ int find_scene_by_particle(const SceneDev* sc, int ns
 void launch_control_init(const Ctx& c, cudaStream_t st);
 void launch_keys(const Ctx& c, cudaStream_t st);
 void launch_scan(const Ctx& c, cudaStream_t st, bool initial);
+void launch_wait_probe(cudaStream_t st, unsigned* out, long long limit);
 void launch_sort_scatter(const Ctx& c, cudaStream_t st, bool initial);
 void launch_p2g(const Ctx& c, cudaStream_t st, int grid_blocks);
 void launch_control_step(const Ctx& c, cudaStream_t st, int mode, double dt_req, int max_substeps, float dt_fixed);

@@ -56,14 +56,27 @@ __device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned 
   return ok != 0;
 }
 
-// Bounded wait: gives up after about 2^31 SM cycles (~1 s) and reports false.
-__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsigned parity) {
+// Bounded wait: gives up after `limit` SM cycles (default 2^31, about 1 s) and reports false.
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsigned parity,
+                                                  long long limit = 1ll << 31) {
   const long long t0 = clock64();
   while (!mbar_try_wait(bar, parity)) {
-    if (clock64() - t0 > (1ll << 31)) return false;
+    if (clock64() - t0 > limit) return false;
   }
   return true;
 }
+
+// Self-check of the bounded wait: one thread waits on an mbarrier that nothing arrives on, gives
+// up after `limit` cycles and reports 1 in out[0] (0 would mean the wait completed).
+__global__ void k_wait_probe(unsigned* out, long long limit) {
+  __shared__ __align__(8) unsigned long long bar;
+  if (threadIdx.x != 0) return;
+  mbar_init(&bar, 1);
+  fence_barrier_init();
+  out[0] = mbar_wait_bounded(&bar, 0, limit) ? 0u : 1u;
+}
+
+void launch_wait_probe(cudaStream_t st, unsigned* out, long long limit) { k_wait_probe<<<1, 32, 0, st>>>(out, limit); }
 
 // 4D tiled TMA load (no multicast): box {4 channels, 6, 6, 6} of the grid velocity array.
 // The innermost coordinate is the channel index 0, so the 16-byte alignment rule holds.

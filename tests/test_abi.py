@@ -53,3 +53,5 @@ def test_invalid_arguments_are_rejected_without_touching_a_device():
     assert L.mpm_return_map_batch(ctypes.byref(m), 0, None, None, None, 0.0, None, None, None) == -10
     m = _lib.MpmMaterial(model=2, mu=1, lam=1, yield_strain=.025)  # carries Jp between steps
     assert L.mpm_return_map_batch(ctypes.byref(m), 0, None, None, None, 0.0, None, None, None) == -10
+    t = ctypes.c_int32()
+    assert L.mpm_check_bounded_wait(None, 1 << 20, ctypes.byref(t)) == -1
