@@ -426,17 +426,21 @@ static void refresh_flags(mpm_handle* h) {
   h->ctx.has_thermal = thermal || h->ctx.has_thermal ? 1 : 0;
 }
 
-static int check_status(mpm_handle* h) {
-  join_side(h);
-  MPM_CUDA(h, cudaMemcpyAsync(h->host_ctrl, h->ctx.ctrl, sizeof(mpm::Ctrl), cudaMemcpyDeviceToHost, h->stream));
-  MPM_CUDA(h, cudaStreamSynchronize(h->stream));
-  const unsigned st = h->host_ctrl->status;
+// The error for the device status flags st (MPM_OK when none is set).
+static int status_error(mpm_handle* h, unsigned st) {
   if (st & MPM_STATUS_TIMEOUT) return fail(h, MPM_ERR_TIMEOUT, "a bounded device wait gave up (TMA copy did not complete)");
   if (st & MPM_STATUS_NONFINITE) return fail(h, MPM_ERR_NONFINITE, "non-finite particle state");
   if (st & MPM_STATUS_INVALID_J) return fail(h, MPM_ERR_INVALID_J, "det F <= 0 in a particle");
   if (st & MPM_STATUS_OUT_OF_RANGE) return fail(h, MPM_ERR_OUT_OF_RANGE, "a particle left the grid");
   if (st & MPM_STATUS_SORT_MISMATCH) return fail(h, MPM_ERR_STATE, "tile sort keys and counts disagreed");
   return MPM_OK;
+}
+
+static int check_status(mpm_handle* h) {
+  join_side(h);
+  MPM_CUDA(h, cudaMemcpyAsync(h->host_ctrl, h->ctx.ctrl, sizeof(mpm::Ctrl), cudaMemcpyDeviceToHost, h->stream));
+  MPM_CUDA(h, cudaStreamSynchronize(h->stream));
+  return status_error(h, h->host_ctrl->status);
 }
 
 // Counting sort of the current state by tile and the dt-free P2G into acc[step_index & 1].
@@ -1249,7 +1253,7 @@ static int run_substeps(mpm_handle* h, int mode, double dt_req, int max_substeps
   if (advanced) *advanced = ct.advanced;
   h->last_estimate = mode == mpm::kModeRequested ? ct.substeps : 0;
   h->last_dt_requested = dt_req;
-  return check_status(h);
+  return status_error(h, ct.status);  // the control block was read after the last launch
 }
 
 int mpm_step(mpm_handle* h, double dt_requested, int32_t max_substeps, int32_t* substeps, double* advanced) {
