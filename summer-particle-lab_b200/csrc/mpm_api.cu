@@ -341,6 +341,8 @@ static int alloc_grid(mpm_handle* h) {
     c.s.count = cv.take<unsigned>(tiles + 1);
     c.s.start = cv.take<unsigned>(tiles + 1);
     c.s.block_off = cv.take<unsigned>(scan_blocks + 1);
+    c.s.rank = cv.take<unsigned>(tiles + 1);
+    c.s.block_rank = cv.take<unsigned>(scan_blocks + 1);
     c.s.work[0] = cv.take<uint4>(tiles);
     c.s.work[1] = cv.take<uint4>(tiles);
     c.ctrl = cv.take<mpm::Ctrl>(1);

@@ -123,7 +123,9 @@ struct SortBufs {
   unsigned* count;      // per particle tile, total_tiles + 1
   unsigned* start;      // block-local exclusive scan, total_tiles + 1
   unsigned* block_off;  // exclusive scan of block sums
-  uint4* work[2];       // (tile, start, count, scene)
+  unsigned* rank;       // block-local exclusive count of non-empty tiles before each tile
+  unsigned* block_rank; // exclusive scan of the blocks' non-empty tile counts
+  uint4* work[2];       // (tile, start, count, scene), non-empty tiles in tile-key order
 };
 
 struct Ctx {

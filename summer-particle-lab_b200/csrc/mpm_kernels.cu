@@ -331,50 +331,65 @@ constexpr int kScanThreads = 1024;
 constexpr int kScanPer = 4;
 constexpr int kScanChunk = kScanThreads * kScanPer;  // 4096 tiles per block
 
-// Exclusive scan of count[0..T] into start (block-local) + block_off (per 4096 tiles).
-// The last block to finish scans the block sums (threadfence + ticket).
+// Exclusive scans of count[0..T] into start (block-local) + block_off (per 4096 tiles), and of the
+// non-empty flags into rank + block_rank (a tile's place in the work list, which so comes out in
+// tile-key order). The last block to finish scans the block sums (threadfence + ticket) and sets
+// the work list's length.
 // initial: the scan of a first sort (done is clear); otherwise the scan after a scatter pass, which
 // may run beside the next substep's opening kernels and so reads the pass's own flag, not done.
+__device__ __forceinline__ uint2 warp_incl_scan2(uint2 v, int lane) {
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const unsigned a = __shfl_up_sync(0xffffffffu, v.x, o);
+    const unsigned b = __shfl_up_sync(0xffffffffu, v.y, o);
+    if (lane >= o) {
+      v.x += a;
+      v.y += b;
+    }
+  }
+  return v;
+}
+
 __global__ void __launch_bounds__(kScanThreads) k_scan(Ctx c, int initial) {
   if (initial ? c.ctrl->done != 0 : c.ctrl->sort_active == 0) return;
   if (c.ctrl->status & 0x8u) return;
-  __shared__ unsigned warp_sums[32];
+  __shared__ uint2 warp_sums[32];
   __shared__ bool last;
   const int T = c.total_tiles + 1;
   const int base = blockIdx.x * kScanChunk + threadIdx.x * kScanPer;
   unsigned v[kScanPer];
-  unsigned sum = 0;
+  uint2 sum = make_uint2(0u, 0u);
 #pragma unroll
   for (int k = 0; k < kScanPer; ++k) {
     v[k] = (base + k < c.total_tiles) ? c.s.count[base + k] : 0u;
-    sum += v[k];
+    sum.x += v[k];
+    sum.y += v[k] > 0u ? 1u : 0u;
   }
   // block exclusive scan of per-thread sums
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  unsigned incl = sum;
-  for (int o = 1; o < 32; o <<= 1) {
-    const unsigned y = __shfl_up_sync(0xffffffffu, incl, o);
-    if (lane >= o) incl += y;
-  }
+  const uint2 incl = warp_incl_scan2(sum, lane);
   if (lane == 31) warp_sums[wid] = incl;
   __syncthreads();
   if (wid == 0) {
-    unsigned ws = warp_sums[lane];
-    unsigned wi = ws;
-    for (int o = 1; o < 32; o <<= 1) {
-      const unsigned y = __shfl_up_sync(0xffffffffu, wi, o);
-      if (lane >= o) wi += y;
-    }
-    warp_sums[lane] = wi - ws;
+    const uint2 ws = warp_sums[lane];
+    const uint2 wi = warp_incl_scan2(ws, lane);
+    warp_sums[lane] = make_uint2(wi.x - ws.x, wi.y - ws.y);
   }
   __syncthreads();
-  unsigned run = warp_sums[wid] + incl - sum;
+  uint2 run = make_uint2(warp_sums[wid].x + incl.x - sum.x, warp_sums[wid].y + incl.y - sum.y);
 #pragma unroll
   for (int k = 0; k < kScanPer; ++k) {
-    if (base + k < T) c.s.start[base + k] = run;
-    run += v[k];
+    if (base + k < T) {
+      c.s.start[base + k] = run.x;
+      c.s.rank[base + k] = run.y;
+    }
+    run.x += v[k];
+    run.y += v[k] > 0u ? 1u : 0u;
   }
-  if (threadIdx.x == kScanThreads - 1) c.s.block_off[blockIdx.x] = run;  // block total
+  if (threadIdx.x == kScanThreads - 1) {  // block totals
+    c.s.block_off[blockIdx.x] = run.x;
+    c.s.block_rank[blockIdx.x] = run.y;
+  }
   __threadfence();
   __syncthreads();
   if (threadIdx.x == 0) last = (atomicAdd(&c.ctrl->scan_ticket, 1u) == gridDim.x - 1);
@@ -382,36 +397,37 @@ __global__ void __launch_bounds__(kScanThreads) k_scan(Ctx c, int initial) {
   if (!last) return;
   __threadfence();
   // last block: exclusive scan of the block totals (gridDim.x <= 1024 * 64 blocks)
-  __shared__ unsigned carry;
-  if (threadIdx.x == 0) carry = 0;
+  __shared__ uint2 carry;
+  if (threadIdx.x == 0) carry = make_uint2(0u, 0u);
   __syncthreads();
   for (int b0 = 0; b0 < (int)gridDim.x; b0 += kScanThreads) {
     const int b = b0 + threadIdx.x;
-    const unsigned x = (b < (int)gridDim.x) ? *((volatile unsigned*)&c.s.block_off[b]) : 0u;
-    unsigned inc = x;
-    for (int o = 1; o < 32; o <<= 1) {
-      const unsigned y = __shfl_up_sync(0xffffffffu, inc, o);
-      if (lane >= o) inc += y;
-    }
+    const uint2 x = (b < (int)gridDim.x)
+                        ? make_uint2(*((volatile unsigned*)&c.s.block_off[b]), *((volatile unsigned*)&c.s.block_rank[b]))
+                        : make_uint2(0u, 0u);
+    const uint2 inc = warp_incl_scan2(x, lane);
     if (lane == 31) warp_sums[wid] = inc;
     __syncthreads();
     if (wid == 0) {
-      unsigned ws = warp_sums[lane];
-      unsigned wi = ws;
-      for (int o = 1; o < 32; o <<= 1) {
-        const unsigned y = __shfl_up_sync(0xffffffffu, wi, o);
-        if (lane >= o) wi += y;
-      }
-      warp_sums[lane] = wi - ws;
+      const uint2 ws = warp_sums[lane];
+      const uint2 wi = warp_incl_scan2(ws, lane);
+      warp_sums[lane] = make_uint2(wi.x - ws.x, wi.y - ws.y);
     }
     __syncthreads();
-    const unsigned excl = carry + warp_sums[wid] + inc - x;
-    if (b < (int)gridDim.x) c.s.block_off[b] = excl;
+    const uint2 excl = make_uint2(carry.x + warp_sums[wid].x + inc.x - x.x, carry.y + warp_sums[wid].y + inc.y - x.y);
+    if (b < (int)gridDim.x) {
+      c.s.block_off[b] = excl.x;
+      c.s.block_rank[b] = excl.y;
+    }
     __syncthreads();
-    if (threadIdx.x == kScanThreads - 1) carry = excl + x;
+    if (threadIdx.x == kScanThreads - 1) carry = make_uint2(excl.x + x.x, excl.y + x.y);
     __syncthreads();
   }
-  if (threadIdx.x == 0) c.ctrl->scan_ticket = 0;
+  if (threadIdx.x == 0) {
+    const unsigned list = initial ? (c.ctrl->step_index & 1u) : c.ctrl->sort_list;
+    c.ctrl->work_count[list] = carry.y;  // non-empty tiles
+    c.ctrl->scan_ticket = 0;
+  }
 }
 
 void launch_scan(const Ctx& c, cudaStream_t st, bool initial) {
@@ -423,7 +439,7 @@ __device__ __forceinline__ unsigned tile_start(const Ctx& c, unsigned k) {
   return c.s.start[k] + c.s.block_off[k / kScanChunk];
 }
 
-// perm[start(k) + rank] = home slot; the group that claims a tile first appends the work item.
+// perm[start(k) + rank] = home slot; the group that claims a tile first writes its work item.
 // After a scatter pass the sort may run beside the next substep's k_begin and grid update, so it
 // takes its list and its go-ahead from the fields that pass wrote (sort_list, sort_active), which
 // k_begin does not touch.
@@ -449,9 +465,9 @@ __global__ void __launch_bounds__(256) k_sort_scatter(Ctx c, int initial) {
     return;
   }
   c.p.perm[s0 + old - 1 - below] = static_cast<unsigned>(i);
-  if (lane == leader && old == cnt) {
+  if (lane == leader && old == cnt) {  // the tile's first group writes its work item at the tile's rank
     const unsigned list = initial ? (c.ctrl->step_index & 1u) : c.ctrl->sort_list;
-    const unsigned idx = atomicAdd(&c.ctrl->work_count[list], 1u);
+    const unsigned idx = c.s.rank[key] + c.s.block_rank[key / kScanChunk];
     const int s = c.nscenes == 1 ? 0 : find_scene_by_tile(c.scenes, c.nscenes, static_cast<int>(key));
     if (idx < static_cast<unsigned>(c.total_tiles)) c.s.work[list][idx] = make_uint4(key, s0, cnt, static_cast<unsigned>(s));
   }
