@@ -144,6 +144,15 @@ MPM_HD int series_terms(float r) {
   return r <= 1e-3f ? 3 : r <= 1e-2f ? 4 : r <= 3e-2f ? 5 : r <= 6e-2f ? 6 : r <= 0.1f ? 8 : r <= kSeriesMaxNorm ? 10 : 0;
 }
 
+// The same choice from the squared norm (no square root on the per-particle path).
+MPM_HD float sym_norm2(const Sym3& a) {
+  return a.xx * a.xx + a.yy * a.yy + a.zz * a.zz + 2.f * (a.xy * a.xy + a.xz * a.xz + a.yz * a.yz);
+}
+MPM_HD int series_terms_sq(float r2) {
+  return r2 <= 1e-6f ? 3 : r2 <= 1e-4f ? 4 : r2 <= 9e-4f ? 5 : r2 <= 3.6e-3f ? 6 : r2 <= 1e-2f ? 8
+       : r2 <= kSeriesMaxNorm * kSeriesMaxNorm ? 10 : 0;
+}
+
 // Coefficient c_k of x^(k+1) in the series (Taylor coefficients, exact rationals):
 //   kind 0  log(1 + x)      = x - x^2/2 + x^3/3 - ...          c_k = (-1)^k / (k + 1)
 //   kind 1  sqrt(1 + x) - 1 = x/2 - x^2/8 + x^3/16 - ...       c_k = binom(1/2, k + 1)
@@ -567,7 +576,7 @@ MPM_HD ConstitutiveOut constitutive_update_t(const MaterialDev& mt, float D[9], 
   // fixed-corotated: V_l = sqrt(I + B), (F - R) F^T = (V_l - I) V_l;  Hencky: L = log(V_l) =
   // log(I + B)/2, |dev e| = |dev L|_F, returned L' = tr L/3 I + scale dev L, and the return
   // F' = U diag(s'/s) U^T F = exp((scale - 1) dev L) F.
-  const int nt = series_terms(sym_norm(B));
+  const int nt = series_terms_sq(sym_norm2(B));
   if (nt > 0) {
     if (mt.model == 0) {
       const Sym3 S1 = matrix_series<1>(B, nt);  // sqrt(I + B) - I
@@ -591,7 +600,8 @@ MPM_HD ConstitutiveOut constitutive_update_t(const MaterialDev& mt, float D[9], 
     Sym3 dv = L;
     dv.xx -= tr3; dv.yy -= tr3; dv.zz -= tr3;
     const float len = sym_norm(dv);
-    const float J = fmaxf(1e-6f, expf(trL));
+    const float em1 = expm1f(trL);  // J - 1
+    const float J = fmaxf(1e-6f, 1.f + em1);
     const float q = 2.449489742783178f * mt.mu * len / J;
     const float dep = do_return ? plastic_increment(mt, q, J, ep, T, dt) : 0.f;
     float scale = 1.f;
@@ -622,7 +632,7 @@ MPM_HD ConstitutiveOut constitutive_update_t(const MaterialDev& mt, float D[9], 
     out.tau.xz = m2s * dv.xz;
     out.tau.yz = m2s * dv.yz;
     out.dep = dep;
-    out.Jm1 = expm1f(trL);
+    out.Jm1 = em1;
     return out;
   }
   return constitutive_eigen(mt, B, D, ep, T, inv_rho0, do_return, dt);
