@@ -201,6 +201,12 @@ int mpm_stable_dt(mpm_handle* h, double* dt);
  * substeps of min(remaining, stable dt), at most max_substeps; the state stays on the device. */
 int mpm_step(mpm_handle* h, double dt_requested, int32_t max_substeps, int32_t* substeps,
              double* advanced);
+/* nsteps consecutive mpm_step calls in one call: every requested-dt step sub-steps to the CFL
+ * limit as mpm_step does (at most max_substeps each), the step boundaries are taken on the
+ * device and the host synchronises once at the end. *substeps is the total over all steps,
+ * *advanced the time advanced (nsteps x dt_requested unless a step hit max_substeps). */
+int mpm_run(mpm_handle* h, double dt_requested, int32_t nsteps, int32_t max_substeps, int32_t* substeps,
+            double* advanced);
 /* nsteps substeps of exactly dt each (no CFL control) */
 int mpm_step_fixed(mpm_handle* h, double dt, int32_t nsteps);
 /* nsteps substeps, each of the scene's own stable dt (ensemble / CFL mode) */

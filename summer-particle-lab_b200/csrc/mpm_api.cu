@@ -1182,8 +1182,10 @@ static int run_substeps_regularized(mpm_handle* h, int mode, double dt_req, int 
 // final_gather: the caller replaces the particle state after the call (mpm_frame_host), so the
 // estimated last substep runs the gather-only pass; the scatter it would make is never used. If
 // more substeps turn out to be needed, the state is scattered again (prepare_grid) first.
+// nsteps (requested mode): requested-dt steps in this call, each of up to max_substeps substeps,
+// with the step boundaries taken on the device (mpm_run).
 static int run_substeps(mpm_handle* h, int mode, double dt_req, int max_substeps, float dt_fixed, int* substeps,
-                        double* advanced, bool final_gather = false) {
+                        double* advanced, bool final_gather = false, int nsteps = 1) {
   if (!h->uploaded) return fail(h, MPM_ERR_STATE, "no particles uploaded");
   if (h->n == 0) {
     if (substeps) *substeps = 0;
@@ -1196,24 +1198,27 @@ static int run_substeps(mpm_handle* h, int mode, double dt_req, int max_substeps
     if (rc != MPM_OK) return rc;
   }
   h->ctx.n = h->n;
-  { ProfScope ps(h, -1); mpm::launch_control_step(h->ctx, h->stream, mode, dt_req, max_substeps, dt_fixed); }
-  int launched = 0;
-  int est;
+  if (mode != mpm::kModeRequested) nsteps = 1;
+  { ProfScope ps(h, -1); mpm::launch_control_step(h->ctx, h->stream, mode, dt_req, max_substeps, dt_fixed, nsteps); }
+  // launches are bounded by max_substeps per requested step
+  const long long max_total = static_cast<long long>(max_substeps) * nsteps;
+  long long launched = 0;
+  long long est;
   if (mode == mpm::kModeRequested && h->last_estimate > 0 && h->last_dt_requested == dt_req) {
-    // the previous call's substep count for the same requested dt: no host round trip before the
-    // launches (substeps past the end return at once; a short estimate is topped up below)
-    est = std::min(h->last_estimate, max_substeps);
+    // the previous call's substep count per step for the same requested dt: no host round trip
+    // before the launches (substeps past the end return at once; a short estimate is topped up)
+    est = static_cast<long long>(std::min(h->last_estimate, max_substeps)) * nsteps;
   } else if (mode == mpm::kModeRequested) {
     double dt = 0;
     int rc = mpm_stable_dt(h, &dt);
     if (rc != MPM_OK) return rc;
-    est = static_cast<int>(std::ceil(dt_req / std::max(dt, 1e-30) - 1e-9));
-    est = std::max(1, std::min(est, max_substeps));
+    est = static_cast<long long>(std::ceil(dt_req / std::max(dt, 1e-30) - 1e-9));
+    est = std::max(1ll, std::min(est, static_cast<long long>(max_substeps))) * nsteps;
   } else {
     est = max_substeps;
   }
   while (true) {
-    for (int i = 0; i < est; ++i) {
+    for (long long i = 0; i < est; ++i) {
       launch_substep(h, !(final_gather && i == est - 1));
       // keep tiles contiguous in memory: a permutation pass after every reorder_interval substeps
       if (h->reorder_interval > 0 && ++h->substeps_since_reorder >= h->reorder_interval) {
@@ -1228,19 +1233,24 @@ static int run_substeps(mpm_handle* h, int mode, double dt_req, int max_substeps
     MPM_CUDA(h, cudaMemcpyAsync(h->host_ctrl, h->ctx.ctrl, sizeof(mpm::Ctrl), cudaMemcpyDeviceToHost, h->stream));
     MPM_CUDA(h, cudaStreamSynchronize(h->stream));
     const mpm::Ctrl& ct = *h->host_ctrl;
-    const bool finished = ct.done || ct.substeps >= max_substeps ||
-                          (mode == mpm::kModeRequested && !(ct.remaining > 1e-6 * dt_req)) || launched >= max_substeps;
+    const bool finished =
+        ct.done || launched >= max_total ||
+        (mode == mpm::kModeRequested
+             ? ct.steps_left <= 1 && (!(ct.remaining > 1e-6 * dt_req) || ct.step_substeps >= max_substeps)
+             : ct.substeps >= max_substeps);
     if (finished || (ct.status & (MPM_STATUS_NONFINITE | MPM_STATUS_TIMEOUT))) break;
     if (final_gather) {  // the last substep ran and made no scatter: scatter the state again
       h->pending_grid = false;
       const int rc = prepare_grid(h);
       if (rc != MPM_OK) return rc;
     }
-    // the substeps still needed at this call's mean dt so far
+    // the substeps still needed at this call's mean dt so far: the rest of the current step and
+    // the steps not yet started
     est = 1;
     if (mode == mpm::kModeRequested && ct.substeps > 0 && ct.advanced > 0) {
-      const double need = std::ceil(ct.remaining / (ct.advanced / ct.substeps) - 1e-9);
-      est = static_cast<int>(std::max(1.0, std::min(need, static_cast<double>(max_substeps - launched))));
+      const double mean = ct.advanced / ct.substeps;
+      const double need = std::ceil(ct.remaining / mean - 1e-9) + (ct.steps_left - 1) * std::ceil(dt_req / mean - 1e-9);
+      est = static_cast<long long>(std::max(1.0, std::min(need, static_cast<double>(max_total - launched))));
     }
   }
   const mpm::Ctrl& ct = *h->host_ctrl;
@@ -1253,9 +1263,36 @@ static int run_substeps(mpm_handle* h, int mode, double dt_req, int max_substeps
   }
   if (substeps) *substeps = ct.substeps;
   if (advanced) *advanced = ct.advanced;
-  h->last_estimate = mode == mpm::kModeRequested ? ct.substeps : 0;
+  h->last_estimate = mode == mpm::kModeRequested ? (ct.substeps + nsteps - 1) / nsteps : 0;
   h->last_dt_requested = dt_req;
   return status_error(h, ct.status);  // the control block was read after the last launch
+}
+
+int mpm_run(mpm_handle* h, double dt_requested, int32_t nsteps, int32_t max_substeps, int32_t* substeps,
+            double* advanced) {
+  if (!h) return MPM_ERR_INVALID_ARG;
+  if (!(dt_requested > 0) || !std::isfinite(dt_requested)) return fail(h, MPM_ERR_INVALID_ARG, "dt must be positive");
+  if (nsteps <= 0) return fail(h, MPM_ERR_INVALID_ARG, "nsteps must be positive");
+  if (max_substeps <= 0) max_substeps = 48;  // the reference's cap per step (src/three/simulation.js:308)
+  if (h->reg.enabled) {  // the regulariser runs between substeps on the host's schedule: step by step
+    int total = 0;
+    double adv = 0;
+    for (int k = 0; k < nsteps; ++k) {
+      int sub = 0;
+      double a = 0;
+      const int rc = run_substeps(h, mpm::kModeRequested, dt_requested, max_substeps, 0.f, &sub, &a);
+      if (rc != MPM_OK) return rc;
+      total += sub;
+      adv += a;
+    }
+    if (substeps) *substeps = total;
+    if (advanced) *advanced = adv;
+    return MPM_OK;
+  }
+  int sub = 0;
+  const int rc = run_substeps(h, mpm::kModeRequested, dt_requested, max_substeps, 0.f, &sub, advanced, false, nsteps);
+  if (substeps) *substeps = sub;
+  return rc;
 }
 
 int mpm_step(mpm_handle* h, double dt_requested, int32_t max_substeps, int32_t* substeps, double* advanced) {

@@ -84,6 +84,8 @@ struct Ctrl {
   unsigned active_count[2];
   unsigned grid_next;
   unsigned scan_ticket;
+  int steps_left;        // requested-dt steps of this call still to start after the current one, + 1
+  int step_substeps;     // substeps of the current requested-dt step
   unsigned sort_list;    // work list the sort after a scatter pass appends to (written by that pass)
   unsigned sort_active;  // 1 if that pass ran (the sort and scan skip a pass that returned at done)
 };
@@ -175,7 +177,8 @@ void launch_scan(const Ctx& c, cudaStream_t st, bool initial);
 void launch_wait_probe(cudaStream_t st, unsigned* out, long long limit);
 void launch_sort_scatter(const Ctx& c, cudaStream_t st, bool initial);
 void launch_p2g(const Ctx& c, cudaStream_t st, int grid_blocks);
-void launch_control_step(const Ctx& c, cudaStream_t st, int mode, double dt_req, int max_substeps, float dt_fixed);
+void launch_control_step(const Ctx& c, cudaStream_t st, int mode, double dt_req, int max_substeps, float dt_fixed,
+                         int nsteps = 1);
 void launch_begin(const Ctx& c, cudaStream_t st);
 void launch_grid_clear(const Ctx& c, cudaStream_t st, int grid_blocks);
 void launch_grid_update(const Ctx& c, cudaStream_t st, int grid_blocks);

@@ -192,8 +192,9 @@ struct ControlOp {
   int op;           // 0: reset lists for an initial sort + P2G, 1: start a step call
   int mode;
   double dt_requested;
-  int max_substeps;
+  int max_substeps;  // per requested-dt step in requested mode, per call otherwise
   float dt_fixed;
+  int nsteps;        // requested-dt steps in this call
 };
 
 __global__ void k_control(Ctx c, ControlOp op) {
@@ -214,6 +215,8 @@ __global__ void k_control(Ctx c, ControlOp op) {
       ct->done = 0;
       ct->mode = op.mode;
       ct->dt_fixed = op.dt_fixed;
+      ct->steps_left = op.nsteps > 1 ? op.nsteps : 1;
+      ct->step_substeps = 0;
     }
   }
   if (op.op == 0) {
@@ -225,12 +228,13 @@ __global__ void k_control(Ctx c, ControlOp op) {
 }
 
 void launch_control_init(const Ctx& c, cudaStream_t st) {
-  ControlOp op{0, 0, 0.0, 0, 0.f};
+  ControlOp op{0, 0, 0.0, 0, 0.f, 1};
   k_control<<<1, 256, 0, st>>>(c, op);
 }
 
-void launch_control_step(const Ctx& c, cudaStream_t st, int mode, double dt_req, int max_substeps, float dt_fixed) {
-  ControlOp op{1, mode, dt_req, max_substeps, dt_fixed};
+void launch_control_step(const Ctx& c, cudaStream_t st, int mode, double dt_req, int max_substeps, float dt_fixed,
+                         int nsteps) {
+  ControlOp op{1, mode, dt_req, max_substeps, dt_fixed, nsteps};
   k_control<<<1, 32, 0, st>>>(c, op);
 }
 
@@ -263,22 +267,32 @@ __global__ void __launch_bounds__(256) k_begin(Ctx c) {
     for (int w = 1; w < (int)(blockDim.x >> 5); ++w) m = fminf(m, smin[w]);
     int done = 0;
     float dt = m;
-    if (ct->substeps >= ct->max_substeps) done = 1;
     if (ct->mode == kModeRequested) {
-      if (!(ct->remaining > 1e-6 * ct->dt_requested)) done = 1;
+      // a requested-dt step ends when its time is used up or it has taken max_substeps; the
+      // call's next step (mpm_run) then starts with the full requested dt
+      bool over = !(ct->remaining > 1e-6 * ct->dt_requested) || ct->step_substeps >= ct->max_substeps;
+      if (over && ct->steps_left > 1) {
+        ct->steps_left -= 1;
+        ct->remaining = ct->dt_requested;
+        ct->step_substeps = 0;
+        over = false;
+      }
+      if (over) done = 1;
       dt = static_cast<float>(fmin(ct->remaining, static_cast<double>(m)));
       if (!done) {
         // the last substep takes exactly what is left (src/three/simulation.js:309)
         if (ct->remaining - dt <= 1e-6 * ct->dt_requested) dt = static_cast<float>(ct->remaining);
         ct->remaining -= dt;
       }
-    } else if (ct->mode == kModeFixed) {
-      dt = ct->dt_fixed;
+    } else {
+      if (ct->substeps >= ct->max_substeps) done = 1;
+      if (ct->mode == kModeFixed) dt = ct->dt_fixed;
     }
     if (done) {
       ct->done = 1;
     } else {
       ct->substeps += 1;
+      ct->step_substeps += 1;
       ct->advanced += dt;
       const unsigned k = ct->step_index + 1;
       ct->step_index = k;

@@ -144,6 +144,7 @@ SIGNATURES = {
     "mpm_step_host": (ctypes.c_int, [_P, ctypes.POINTER(MpmParticles), _D]),
     "mpm_frame_host": (ctypes.c_int, [_P, ctypes.POINTER(MpmParticles), _D, _I32, ctypes.POINTER(_I32)]),
     "mpm_check_bounded_wait": (ctypes.c_int, [_P, ctypes.c_int64, ctypes.POINTER(_I32)]),
+    "mpm_run": (ctypes.c_int, [_P, _D, _I32, _I32, ctypes.POINTER(_I32), ctypes.POINTER(_D)]),
     "mpm_profile_enable": (ctypes.c_int, [_P, _I32]),
     "mpm_profile_read": (ctypes.c_int, [_P, ctypes.POINTER(_D), ctypes.POINTER(_I64)]),
     "mpm_launch_count": (ctypes.c_int, [_P, ctypes.POINTER(_I64)]),

@@ -149,6 +149,14 @@ class Solver:
         self._check(_lib.lib().mpm_step(self.h, dt_requested, max_substeps, ctypes.byref(sub), ctypes.byref(adv)))
         return sub.value, adv.value
 
+    def run(self, dt_requested, nsteps, max_substeps=48):
+        """nsteps requested-dt steps in one call (mpm_run); returns (total substeps, time advanced)."""
+        sub = ctypes.c_int32()
+        adv = ctypes.c_double()
+        self._check(_lib.lib().mpm_run(self.h, dt_requested, int(nsteps), max_substeps, ctypes.byref(sub),
+                                       ctypes.byref(adv)))
+        return sub.value, adv.value
+
     def step_fixed(self, dt, nsteps=1):
         self._check(_lib.lib().mpm_step_fixed(self.h, dt, nsteps))
 
