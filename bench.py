@@ -6,8 +6,10 @@
 Workload (default): the 2,097,152-particle J2 linear-hardening drop (64x64x64-cell block, 8 particles
 per cell, 128^3 grid, aluminium E=70 GPa, nu=0.33, yield 250 MPa, hardening 1 GPa), seeded
 synthetic input. One step = one requested step of dt=2e-6 s, sub-stepped on the device to CFL 0.4
-(about 4 substeps); the metric counts actual substeps x particles. Multi-GPU runs are independent
-replicas per GPU (weak scaling; the single-scene path has no exchange step).
+(about 4 substeps); the metric counts actual substeps x particles. The K timed steps go through
+mpm_run (one call, the step boundaries taken on the device); "step_per_call" gives the same steps as
+K mpm_step calls. Multi-GPU runs are independent replicas per GPU (weak scaling), or with --slabs
+one scene split into z slabs (strong scaling).
 
 The line also carries an "ensemble" block: 256 seeded V&V scenes (particle counts log-uniform in
 5e3..2e5, grids 32..96 cells, per-scene CFL dt) on one batch handle per rank, scenes sharded across
@@ -529,21 +531,30 @@ def main():
     clk.wait_first_sample()
     if dist is not None:
         dist.barrier()
+    # headline: the K requested steps through mpm_run (one call; the step boundaries are taken on
+    # the device and the host synchronises once)
     launches0 = sol.launch_count()
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
-    substeps = 0
     torch.cuda.synchronize()
     t_start = time.time()
     ev0.record(ext)
-    for _ in range(args.steps):
-        s, _adv = sol.step(dt_req)
-        substeps += s
+    substeps, _adv = sol.run(dt_req, args.steps)
     ev1.record(ext)
     torch.cuda.synchronize()
     t_end = time.time()
     launches = sol.launch_count() - launches0
     ms = ev0.elapsed_time(ev1)
+    # the same K steps as K mpm_step calls (one host round trip each), for comparison
+    pc0 = torch.cuda.Event(enable_timing=True)
+    pc1 = torch.cuda.Event(enable_timing=True)
+    pc_sub = 0
+    pc0.record(ext)
+    for _ in range(args.steps):
+        pc_sub += sol.step(dt_req)[0]
+    pc1.record(ext)
+    torch.cuda.synchronize()
+    per_call_ms = pc0.elapsed_time(pc1)
     # the same K steps again with a CUDA event pair around every kernel launch (on the library's
     # stream) for the per-kernel durations of the roofline; events between the launches of the
     # headline pass would add about 5% to it
@@ -554,8 +565,7 @@ def main():
     kp0 = torch.cuda.Event(enable_timing=True)
     kp1 = torch.cuda.Event(enable_timing=True)
     kp0.record(ext)
-    for _ in range(args.steps):
-        sol.step(dt_req)
+    sol.run(dt_req, args.steps)
     kp1.record(ext)
     torch.cuda.synchronize()
     t_end2 = time.time()
@@ -597,8 +607,11 @@ def main():
                        "dt_requested": dt_req, "substeps_per_step": substeps / args.steps,
                        "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                        "l2": f"particle state {scene.n * 160 / 1e6:.0f} MB > 126 MB L2 (no flush)",
-                       "active_nodes": active_nodes},
+                       "active_nodes": active_nodes,
+                       "api": "mpm_run (all requested steps in one call)"},
             "roofline": roofline, "gpu_launches": launches,
+            "step_per_call": {"value": scene.n * pc_sub / (per_call_ms / 1e3), "ms_per_step": per_call_ms / args.steps,
+                              "api": "mpm_step once per requested step (a host round trip each)"},
             "kernel_ms": {k: v[0] for k, v in prof.items()}, "clocks": clk.summary(t_start, t_end)}
     # end to end through the C ABI with pinned host buffers (x, v in and out every step)
     if not args.no_e2e:
