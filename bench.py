@@ -51,6 +51,7 @@ def parse():
     ap.add_argument("--workload", default="j2_drop")
     ap.add_argument("--shape", default="64,64,64")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--clocks-csv", default=None, help="also write the clock samples to this CSV file")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-ensemble", action="store_true")
     ap.add_argument("--no-surrogate", action="store_true")
@@ -98,33 +99,59 @@ def sample_scene(scene, factor=2):
     return s
 
 
-def cpu_oracle_rate(scene, dt, steps, threads):
-    """Oracle particle-steps/s on the given scene (steps of dt, OpenMP threads)."""
+def oracle_requested_step(st, dt_req, threads, max_substeps=48):
+    """One requested step on the oracle, sub-stepped as Simulation3.step does
+    (src/three/simulation.js:305-311): substeps of the stable dt, the last one taking what is left."""
+    left, n = dt_req, 0
+    while left > 1e-6 * dt_req and n < max_substeps:
+        dt = min(st.stable_dt(), left)
+        if left - dt <= 1e-6 * dt_req:
+            dt = left
+        st.step(dt, threads=threads)
+        left -= dt
+        n += 1
+    return n
+
+
+def cpu_oracle_rate(scene, dt_req, steps, threads, budget_s=None):
+    """Oracle particle-steps/s on the given scene: `steps` requested steps of dt_req sub-stepped to
+    the stable dt (OpenMP threads), stopping early once budget_s seconds have passed. Returns
+    (rate, seconds, requested steps timed, substeps)."""
     from oracle import oracle as orc
     st = orc.state_from_scene(scene)
-    st.step(dt, threads=threads)  # warm-up
+    oracle_requested_step(st, dt_req, threads)  # warm-up
     t0 = time.perf_counter()
-    for _ in range(steps):
-        st.step(dt, threads=threads)
+    done = subs = 0
+    while done < steps:
+        subs += oracle_requested_step(st, dt_req, threads)
+        done += 1
+        if budget_s is not None and time.perf_counter() - t0 > budget_s:
+            break
     el = time.perf_counter() - t0
-    return scene.n * steps / el, el
+    return scene.n * subs / el, el, done, subs
 
 
 class Clocks:
     """SM clocks, power and clock-event reasons sampled during the run: an NVML thread every 20 ms
-    (read-only queries), or `nvidia-smi -lms 100` when NVML is unavailable. Samples are written to
-    gpurun_out/clocks_bench_<pid>.csv with their host time."""
+    (read-only queries), or `nvidia-smi -lms 100` when NVML is unavailable. Samples stay in memory;
+    with --clocks-csv PATH they are also written there with their host time (nvidia-smi writes its
+    rows to that path, or to a temporary file)."""
     QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
     NAMES = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
 
-    def __init__(self, index):
+    def __init__(self, index, path=None):
         self.index = index
         self.proc = None
         self.thread = None
         self.rows = []  # (time, sm_mhz, max_mhz, power_w, [active reason names])
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_bench_{os.getpid()}.csv")
+        self.keep = path is not None
+        if path is None:
+            import tempfile
+            fd, path = tempfile.mkstemp(prefix="clocks_bench_", suffix=".csv")
+            os.close(fd)
+        self.path = path
 
     def wait_first_sample(self, timeout=5.0):
         t0 = time.time()
@@ -150,7 +177,8 @@ class Clocks:
             time.sleep(0.02)
 
     def __enter__(self):
-        os.makedirs(os.path.dirname(self.path), exist_ok=True)
+        if os.path.dirname(self.path):
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
         try:
             import threading
             import pynvml as nv
@@ -176,10 +204,13 @@ class Clocks:
         if self.thread is not None:
             self.stop = True
             self.thread.join(timeout=2)
-            with open(self.path, "w") as f:
-                f.write("time,sm_mhz,max_sm_mhz,power_w,reasons\n")
-                for t, sm, mx, pw, rs in self.rows:
-                    f.write(f"{t:.3f},{sm:.0f},{mx:.0f},{pw:.1f},{'|'.join(rs) or 'none'}\n")
+            if self.keep:
+                with open(self.path, "w") as f:
+                    f.write("time,sm_mhz,max_sm_mhz,power_w,reasons\n")
+                    for t, sm, mx, pw, rs in self.rows:
+                        f.write(f"{t:.3f},{sm:.0f},{mx:.0f},{pw:.1f},{'|'.join(rs) or 'none'}\n")
+            elif os.path.exists(self.path):
+                os.remove(self.path)
         if self.proc is not None:
             self.proc.terminate()
             try:
@@ -225,19 +256,11 @@ class Clocks:
                 "samples": len(rows), "source": "nvidia-smi"}
 
 
-def read_traffic_per_particle():
-    """DRAM bytes per particle of one g2p2g launch from the committed ncu summary, if present."""
-    path = os.path.join(ROOT, "profiles", "g2p2g_j2_drop.md")
-    if not os.path.exists(path):
-        return None
-    for line in open(path):
-        line = line.strip().lstrip("-").strip()  # the summary lists it as a bullet
-        if line.startswith("dram_bytes_per_particle:"):
-            try:
-                return float(line.split(":", 1)[1].split()[0])
-            except ValueError:
-                return None
-    return None
+# DRAM bytes per particle of one fused G2P2G launch (dram__bytes_read.sum + dram__bytes_write.sum of
+# one ncu --set full capture of k_particles<1,0,0> on the 2M-particle J2 drop, divided by the particle
+# count), set by hand from that capture; bench.py scales it to the timed workload's particle count.
+TRAFFIC_PER_PARTICLE = 196.8
+TRAFFIC_SOURCE = "ncu --set full capture of k_particles<1,0,0>, j2_drop 2,097,152 particles (412.8 MB per launch)"
 
 
 def peaks():
@@ -249,30 +272,40 @@ def peaks():
 
 
 def run_reference(args, rank, world):
+    """The reference's CPU algorithm (the FP64 port of src/three/mpm.js under oracle/, built with
+    -march=native on this host, all host threads) on a 1/8 sub-block of the same workload, each step
+    a requested step of the workload's dt sub-stepped to the stable dt like Simulation3.step; the
+    metric counts particles x substeps like the GPU arm. Bounded to about 90 s of timed work."""
     if rank != 0:
         return
+    from oracle import oracle as orc
+    isa = orc.use_native()
     scene = make_scene(args)
     sample = sample_scene(scene, 2)
     threads = os.cpu_count() or 1
-    dt = 5e-7
-    from oracle import oracle as orc
+    dt_req = scene.meta.get("dt", 2e-6)
     st = orc.state_from_scene(sample)
     for _ in range(max(1, args.warmup)):
-        st.step(dt, threads=threads)
+        oracle_requested_step(st, dt_req, threads)
     t0 = time.perf_counter()
-    for _ in range(args.steps):
-        st.step(dt, threads=threads)
+    done = subs = 0
+    while done < args.steps:
+        subs += oracle_requested_step(st, dt_req, threads)
+        done += 1
+        if time.perf_counter() - t0 > 90.0:
+            break
     el = time.perf_counter() - t0
-    value = sample.n * args.steps / el
+    value = sample.n * subs / el
+    sample_desc = (f"{sample.n}-particle sub-block (1/8) of {scene.meta['workload']}, {done} requested steps of "
+                   f"{dt_req} s ({subs} CFL substeps) in {el:.1f} s")
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps, "higher_is_better": True,
+            "warmup": args.warmup, "ms_per_step": 1e3 * el / max(done, 1), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "impl": "reference",
             "config": {"workload": scene.meta["workload"], "sample_particles": sample.n,
-                       "dt_substep": dt},
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
-                             "sample": f"{sample.n}-particle sub-block of {scene.meta['workload']}, "
-                                       f"{args.steps} substeps of {dt} s"},
+                       "dt_requested": dt_req, "steps_timed": done, "substeps_timed": subs},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "isa": isa,
+                             "sample": sample_desc},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -354,14 +387,30 @@ def ensemble_leg(args, rank, world, dist):
             h.step_cfl(1)
     torch.cuda.synchronize()
     pms, pp = max_sum((time.perf_counter() - t0) * 1e3, n_mine * Kp)
+    # the same substeps again with CUDA events around every launch on each handle's stream: the sum
+    # of the kernel durations is the device time the plain form needs without its host loop
+    for h in handles:
+        h.profile(True)
+    for _ in range(Kp):
+        for h in handles:
+            h.step_cfl(1)
+    torch.cuda.synchronize()
+    dev_ms = 0.0
+    for h in handles:
+        dev_ms += sum(v[0] for v in h.profile_read().values())
+        h.profile(False)
+    dms, _ = max_sum(dev_ms, 0.0)
     for h in handles:
         h.close()
     plain = {"value": pp / (pms / 1e3), "ms_per_substep": pms / Kp, "substeps": Kp, "handles": len(allsc),
-             "timing": "wall clock around the host loop"}
+             "timing": "wall clock around the host loop",
+             "device_value": pp / (dms / 1e3), "device_ms_per_substep": dms / Kp,
+             "device_timing": "sum of CUDA-event kernel durations on every handle's stream (no host loop)"}
     return {"workload": f"vv_ensemble_{len(allsc)}_seeds_1000", "scenes": len(allsc),
             "particles": int(sum(sc.n for sc in allsc)), "ranks": world,
             "shard_imbalance": imbalance(costs, shards), "batched": batched, "plain": plain,
             "speedup_batched_vs_plain": batched["value"] / plain["value"],
+            "speedup_batched_vs_plain_device": batched["value"] / plain["device_value"],
             "roofline": {"bound": "hbm", "kernel": "k_g2p2g (all scenes)", "achieved": ach, "peak": hbm,
                          "unit": "GB/s", "frac": ach / hbm if ach else None,
                          "algorithmic_bytes_per_launch": alg, "launch_ms": g_ms / g_n if g_n else None,
@@ -472,6 +521,53 @@ def slab_leg(args, rank, world, dist):
         "status": status}), flush=True)
 
 
+def e2e_leg(args, sol, scene, dt_req, ext, dist, dtype):
+    """K requested steps through mpm_frame_host with the caller's positions and velocities in pinned
+    host arrays of `dtype`: every step copies them to the device, steps, and copies them back inside
+    the timed region (CUDA events on the handle's stream, max over ranks)."""
+    import ctypes
+    import torch
+    from mpm_b200 import _lib
+    n = scene.n
+    es = np.dtype(dtype).itemsize
+    ctype = ctypes.c_double if es == 8 else ctypes.c_float
+    ptrs = []
+    for k in range(6):
+        p = ctypes.c_void_p()
+        _lib.check(_lib.lib().mpm_host_alloc(n * es, ctypes.byref(p)))
+        arr = np.ctypeslib.as_array((ctype * n).from_address(p.value))
+        arr[:] = (scene.x[:, k] if k < 3 else scene.v[:, k - 3])
+        ptrs.append(p)
+    io = _lib.MpmParticles(dtype=_lib.F64 if es == 8 else _lib.F32, x=ptrs[0], y=ptrs[1], z=ptrs[2], vx=ptrs[3],
+                           vy=ptrs[4], vz=ptrs[5])
+    sub = ctypes.c_int32()
+    for _ in range(max(1, args.warmup)):
+        _lib.check(_lib.lib().mpm_frame_host(sol.h, ctypes.byref(io), dt_req, 48, ctypes.byref(sub)), sol.h)
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    sub_total = 0
+    e0.record(ext)
+    for _ in range(args.steps):
+        _lib.check(_lib.lib().mpm_frame_host(sol.h, ctypes.byref(io), dt_req, 48, ctypes.byref(sub)), sol.h)
+        sub_total += sub.value
+    e1.record(ext)
+    torch.cuda.synchronize()
+    ems = e0.elapsed_time(e1)
+    et = torch.tensor([ems, n * sub_total], dtype=torch.float64, device="cuda")
+    if dist is not None:
+        dist.all_reduce(et[0:1], op=dist.ReduceOp.MAX)
+        dist.all_reduce(et[1:2], op=dist.ReduceOp.SUM)
+    for p in ptrs:
+        _lib.lib().mpm_host_free(p)
+    return {"value": float(et[1]) / (float(et[0]) / 1e3), "unit": UNIT,
+            "h2d_bytes_per_step": 6 * es * n, "d2h_bytes_per_step": 6 * es * n,
+            "ms_per_step": float(et[0]) / args.steps,
+            "api": f"mpm_frame_host ({'f64' if es == 8 else 'f32'} pinned host arrays x, y, z, vx, vy, vz)"}
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -523,7 +619,7 @@ def main():
     sol = Solver(scene.domain, scene.n)
     sol.upload(scene)
     ext = torch.cuda.ExternalStream(sol.stream())
-    clk = Clocks(local)
+    clk = Clocks(local, args.clocks_csv)
     clk.__enter__()  # sampling starts before warm-up so the timed region is covered
     for _ in range(args.warmup):
         sol.step(dt_req)
@@ -565,7 +661,7 @@ def main():
     kp0 = torch.cuda.Event(enable_timing=True)
     kp1 = torch.cuda.Event(enable_timing=True)
     kp0.record(ext)
-    sol.run(dt_req, args.steps)
+    prof_substeps, _ = sol.run(dt_req, args.steps)
     kp1.record(ext)
     torch.cuda.synchronize()
     t_end2 = time.time()
@@ -589,13 +685,18 @@ def main():
     g_ms, g_n = prof["g2p2g"]
     alg_bytes = scene.n * BYTES_PER_PARTICLE[model] + BYTES_PER_NODE * active_nodes
     hbm, peak_kind = peaks()
-    achieved = alg_bytes / (g_ms / g_n / 1e3) / 1e9 if g_n else None
-    traffic_pp = read_traffic_per_particle()
+    # launches of the profile pass past the call's last substep return at once (the call launches
+    # its substep estimate); their few microseconds stay in g_ms, but only the substeps that ran
+    # count as launches, so the mean launch time is not understated
+    ran = min(int(prof_substeps), int(g_n)) if g_n else 0
+    launch_ms = g_ms / ran if ran else None
+    achieved = alg_bytes / (launch_ms / 1e3) / 1e9 if launch_ms else None
     roofline = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                 "frac": achieved / hbm if achieved else None,
-                "traffic": (traffic_pp * scene.n if traffic_pp else None),
+                "traffic": TRAFFIC_PER_PARTICLE * scene.n, "traffic_source": TRAFFIC_SOURCE,
                 "kernel": "k_g2p2g", "peak_source": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind,
-                "algorithmic_bytes_per_launch": alg_bytes, "launch_ms": g_ms / g_n if g_n else None,
+                "algorithmic_bytes_per_launch": alg_bytes, "launch_ms": launch_ms,
+                "launches_profiled": int(g_n), "substeps_ran": int(prof_substeps),
                 "share_of_step": g_ms / sum(v[0] for v in prof.values()) if g_n else None,
                 "timing": f"CUDA events around each launch in a second pass of the same {args.steps} steps "
                           f"({kernel_pass_ms:.3f} ms per step with the events)",
@@ -613,55 +714,25 @@ def main():
             "step_per_call": {"value": scene.n * pc_sub / (per_call_ms / 1e3), "ms_per_step": per_call_ms / args.steps,
                               "api": "mpm_step once per requested step (a host round trip each)"},
             "kernel_ms": {k: v[0] for k, v in prof.items()}, "clocks": clk.summary(t_start, t_end)}
-    # end to end through the C ABI with pinned host buffers (x, v in and out every step)
+    # end to end through the C ABI with pinned host buffers (x, v in and out every step): FP64, the
+    # type of the reference's particle arrays (Simulation3's Float64Arrays), is the headline; FP32
+    # arrays are reported beside it
     if not args.no_e2e:
-        import ctypes
-        n = scene.n
-        bufs = []
-        ptrs = []
-        for k in range(6):
-            p = ctypes.c_void_p()
-            _lib.check(_lib.lib().mpm_host_alloc(n * 4, ctypes.byref(p)))
-            arr = np.ctypeslib.as_array((ctypes.c_float * n).from_address(p.value))
-            arr[:] = (scene.x[:, k] if k < 3 else scene.v[:, k - 3])
-            bufs.append(arr)
-            ptrs.append(p)
-        io = _lib.MpmParticles(dtype=_lib.F32, x=ptrs[0], y=ptrs[1], z=ptrs[2], vx=ptrs[3], vy=ptrs[4], vz=ptrs[5])
-        sub = ctypes.c_int32()
-        for _ in range(max(1, args.warmup)):
-            _lib.check(_lib.lib().mpm_frame_host(sol.h, ctypes.byref(io), dt_req, 48, ctypes.byref(sub)), sol.h)
-        torch.cuda.synchronize()
-        if dist is not None:
-            dist.barrier()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        sub_total = 0
-        e0.record(ext)
-        for _ in range(args.steps):
-            _lib.check(_lib.lib().mpm_frame_host(sol.h, ctypes.byref(io), dt_req, 48, ctypes.byref(sub)), sol.h)
-            sub_total += sub.value
-        e1.record(ext)
-        torch.cuda.synchronize()
-        ems = e0.elapsed_time(e1)
-        et = torch.tensor([ems, n * sub_total], dtype=torch.float64, device="cuda")
-        if dist is not None:
-            dist.all_reduce(et[0:1], op=dist.ReduceOp.MAX)
-            dist.all_reduce(et[1:2], op=dist.ReduceOp.SUM)
-        line["e2e"] = {"value": float(et[1]) / (float(et[0]) / 1e3), "unit": UNIT,
-                       "h2d_bytes_per_step": 6 * 4 * n, "d2h_bytes_per_step": 6 * 4 * n,
-                       "api": "mpm_frame_host (f32 pinned host arrays)"}
-        for p in ptrs:
-            _lib.lib().mpm_host_free(p)
+        line["e2e"] = e2e_leg(args, sol, scene, dt_req, ext, dist, np.float64)
+        line["e2e_f32"] = e2e_leg(args, sol, scene, dt_req, ext, dist, np.float32)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        from oracle import oracle as orc
+        isa = orc.use_native()
         sample = sample_scene(scene, 2)
         threads = os.cpu_count() or 1
-        rate, el = cpu_oracle_rate(sample, 5e-7, 200, threads)
-        rate1, el1 = cpu_oracle_rate(sample, 5e-7, 10, 1)  # the reference runs in one worker thread
-        line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
+        rate, el, done, subs = cpu_oracle_rate(sample, dt_req, 50, threads, budget_s=20.0)
+        rate1, el1, done1, subs1 = cpu_oracle_rate(sample, dt_req, 2, 1, budget_s=5.0)  # one worker thread
+        line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": threads, "kind": "port", "isa": isa,
                                 "value_1_thread": rate1,
-                                "sample": f"{sample.n}-particle sub-block (1/8) of the workload, 200 substeps "
-                                          f"({el:.1f} s) on {threads} threads and 10 substeps ({el1:.1f} s) on one, "
-                                          f"FP64 oracle with OpenMP"}
+                                "sample": f"{sample.n}-particle sub-block (1/8) of the workload: {done} requested "
+                                          f"steps of {dt_req} s ({subs} CFL substeps, {el:.1f} s) on {threads} "
+                                          f"threads and {done1} ({subs1} substeps, {el1:.1f} s) on one; FP64 oracle "
+                                          f"built {isa} with OpenMP"}
     if not args.no_ensemble:
         line["ensemble"] = ensemble_leg(args, rank, world, dist)
     if rank == 0 and world == 1 and not args.no_surrogate:

@@ -302,8 +302,9 @@ int mpm_return_map_batch(const mpm_material* material, int64_t n, const double* 
  * double; v (n x 3), C (n x 9), m and V float.
  * The intermediate grid lives in one fixed device array of 262,144 nodes (8 MiB) that every GPU
  * which loads the library holds until the process exits; larger grids return MPM_ERR_CAPACITY.
- * The call allocates and frees no device memory. Its first call on a device looks up that array's
- * device address once (make this first call before any stream capture). Every call reuses the same
+ * The call allocates and frees no device memory. Every call looks up that array's device address
+ * on the current device (it stays valid across a device reset); the first call on a device may also
+ * load the library's device code, so make it before any stream capture. Every call reuses the same
  * array and clears the nodes it needs first; calls that overlap on the GPU race on it.
  * Launches on `stream` (NULL: the default stream) and returns without waiting. */
 int mpm_p2g_noalloc(const mpm_domain* domain, const mpm_material* material, int64_t n, const double* x,

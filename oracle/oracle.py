@@ -69,52 +69,63 @@ PRESSURE_DEFAULTS = dict(cohesion=.025, slope=.6, dilatancy=.15, tension=.01, al
 _lib = None
 
 
+def use_native():
+    """Switch this process to the -march=native build of the oracle (compiled here on first use).
+    Only the CPU-baseline timing calls it; the tests use the portable build."""
+    global _lib
+    _lib = _load(build_oracle.build(native=True))
+    return build_oracle.NATIVE_ISA
+
+
 def lib():
     global _lib
     if _lib is None:
-        path = build_oracle.build()
-        L = ctypes.CDLL(path)
-        P = ctypes.POINTER
-        L.oracle_svd3.argtypes = [_P, _P, _P, _P]
-        L.oracle_compose.argtypes = [_P, _P, _P, _P]
-        L.oracle_rotation.argtypes = [_P, _P]
-        L.oracle_stress3.argtypes = [_P, _D, _D, _P]
-        L.oracle_von_mises.argtypes = [_P, _D]
-        L.oracle_von_mises.restype = _D
-        L.oracle_constitutive_stress.argtypes = [_P, ctypes.c_int, _D, _D, _P]
-        L.oracle_constitutive_stress.restype = ctypes.c_int
-        L.oracle_flow_stress.argtypes = [ctypes.c_int, _D, _D, _D, P(OracleMaterial)]
-        L.oracle_flow_stress.restype = _D
-        L.oracle_thermal_strength.argtypes = [_D, _D, P(OracleMaterial)]
-        L.oracle_thermal_strength.restype = _D
-        L.oracle_creep_log_rate.argtypes = [_D, _D, P(OracleMaterial)]
-        L.oracle_creep_log_rate.restype = _D
-        L.oracle_metal_return.argtypes = [_P, ctypes.c_int, _D, _D, _D, P(OracleMaterial), _P, _P]
-        L.oracle_thermal_return.argtypes = [_P, ctypes.c_int, _D, _D, _D, P(OracleMaterial), _P, _P]
-        L.oracle_project.argtypes = [_P, P(OracleMaterial), _D, _D, _D, _P, _P, _P, _P, _P]
-        L.oracle_project.restype = ctypes.c_int
-        L.oracle_hardening.argtypes = [_D]
-        L.oracle_hardening.restype = _D
-        L.oracle_foam_strength.argtypes = [_D, P(OracleMaterial)]
-        L.oracle_foam_strength.restype = _D
-        L.oracle_step.argtypes = [P(OracleScene), P(OracleMaterial), ctypes.c_int32, ctypes.c_int64,
-                                  _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _D, _P, _P, _P,
-                                  ctypes.c_int32]
-        L.oracle_step.restype = ctypes.c_int
-        L.oracle_stable_dt.argtypes = [P(OracleScene), P(OracleMaterial), ctypes.c_int64,
-                                       _P, _P, _P, _P, _P, _P, _P]
-        L.oracle_stable_dt.restype = _D
-        L.oracle_ledger.argtypes = [P(OracleScene), P(OracleMaterial), ctypes.c_int64, _P, _P, _P,
-                                    _P, _P, _P, _P, _P, _P, P(OracleLedger)]
-        L.oracle_regularize.argtypes = [P(OracleRegularizer), P(OracleMaterial), ctypes.c_int64, _P, _P, _P, _P, _P,
-                                        _P, _P, _D, _P, _P]
-        L.oracle_phase_enthalpy.argtypes = [_D, P(OracleMaterial)]
-        L.oracle_phase_enthalpy.restype = _D
-        L.oracle_exchange_heat.argtypes = [P(OracleHeat), P(OracleMaterial), ctypes.c_int64, _P, _P, _P, _P, _P, _P,
-                                           _P, _P, _P, _P, _P, _P, _D]
-        L.oracle_exchange_heat.restype = _D
-        _lib = L
+        _lib = _load(build_oracle.build())
     return _lib
+
+
+def _load(path):
+    L = ctypes.CDLL(path)
+    P = ctypes.POINTER
+    L.oracle_svd3.argtypes = [_P, _P, _P, _P]
+    L.oracle_compose.argtypes = [_P, _P, _P, _P]
+    L.oracle_rotation.argtypes = [_P, _P]
+    L.oracle_stress3.argtypes = [_P, _D, _D, _P]
+    L.oracle_von_mises.argtypes = [_P, _D]
+    L.oracle_von_mises.restype = _D
+    L.oracle_constitutive_stress.argtypes = [_P, ctypes.c_int, _D, _D, _P]
+    L.oracle_constitutive_stress.restype = ctypes.c_int
+    L.oracle_flow_stress.argtypes = [ctypes.c_int, _D, _D, _D, P(OracleMaterial)]
+    L.oracle_flow_stress.restype = _D
+    L.oracle_thermal_strength.argtypes = [_D, _D, P(OracleMaterial)]
+    L.oracle_thermal_strength.restype = _D
+    L.oracle_creep_log_rate.argtypes = [_D, _D, P(OracleMaterial)]
+    L.oracle_creep_log_rate.restype = _D
+    L.oracle_metal_return.argtypes = [_P, ctypes.c_int, _D, _D, _D, P(OracleMaterial), _P, _P]
+    L.oracle_thermal_return.argtypes = [_P, ctypes.c_int, _D, _D, _D, P(OracleMaterial), _P, _P]
+    L.oracle_project.argtypes = [_P, P(OracleMaterial), _D, _D, _D, _P, _P, _P, _P, _P]
+    L.oracle_project.restype = ctypes.c_int
+    L.oracle_hardening.argtypes = [_D]
+    L.oracle_hardening.restype = _D
+    L.oracle_foam_strength.argtypes = [_D, P(OracleMaterial)]
+    L.oracle_foam_strength.restype = _D
+    L.oracle_step.argtypes = [P(OracleScene), P(OracleMaterial), ctypes.c_int32, ctypes.c_int64,
+                              _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _D, _P, _P, _P,
+                              ctypes.c_int32]
+    L.oracle_step.restype = ctypes.c_int
+    L.oracle_stable_dt.argtypes = [P(OracleScene), P(OracleMaterial), ctypes.c_int64,
+                                   _P, _P, _P, _P, _P, _P, _P]
+    L.oracle_stable_dt.restype = _D
+    L.oracle_ledger.argtypes = [P(OracleScene), P(OracleMaterial), ctypes.c_int64, _P, _P, _P,
+                                _P, _P, _P, _P, _P, _P, P(OracleLedger)]
+    L.oracle_regularize.argtypes = [P(OracleRegularizer), P(OracleMaterial), ctypes.c_int64, _P, _P, _P, _P, _P,
+                                    _P, _P, _D, _P, _P]
+    L.oracle_phase_enthalpy.argtypes = [_D, P(OracleMaterial)]
+    L.oracle_phase_enthalpy.restype = _D
+    L.oracle_exchange_heat.argtypes = [P(OracleHeat), P(OracleMaterial), ctypes.c_int64, _P, _P, _P, _P, _P, _P,
+                                       _P, _P, _P, _P, _P, _P, _D]
+    L.oracle_exchange_heat.restype = _D
+    return L
 
 
 def _ptr(a):

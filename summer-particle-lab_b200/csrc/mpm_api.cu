@@ -1274,6 +1274,9 @@ int mpm_run(mpm_handle* h, double dt_requested, int32_t nsteps, int32_t max_subs
   if (!(dt_requested > 0) || !std::isfinite(dt_requested)) return fail(h, MPM_ERR_INVALID_ARG, "dt must be positive");
   if (nsteps <= 0) return fail(h, MPM_ERR_INVALID_ARG, "nsteps must be positive");
   if (max_substeps <= 0) max_substeps = 48;  // the reference's cap per step (src/three/simulation.js:308)
+  // the call's substep counters (device control block, the returned count) are 32-bit
+  if (static_cast<long long>(nsteps) * max_substeps > 0x7fffffffll)
+    return fail(h, MPM_ERR_INVALID_ARG, "nsteps x max_substeps must stay below 2^31");
   if (h->reg.enabled) {  // the regulariser runs between substeps on the host's schedule: step by step
     int total = 0;
     double adv = 0;

@@ -11,13 +11,14 @@
 // The scratch array is kNoAllocMaxNodes nodes x 2 float4 = 8 MiB per GPU that loads the library and
 // lives until the process exits. Every call shares it and it keeps the previous call's contents:
 // each call clears the nodes it uses before scattering, and calls that overlap on the GPU (on
-// different streams, or from several threads) race on it.
+// different streams, or from several threads) race on it. Each call looks up the array's device
+// address for the current device; the first call on a device may also load the library's device
+// code there, so make it before any stream capture on that device.
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <cmath>
 #include <cstring>
-#include <mutex>
 
 #include "mpm_b200.h"
 #include "mpm_math.h"
@@ -25,13 +26,9 @@
 namespace {
 
 constexpr long long kNoAllocMaxNodes = 1ll << 18;  // 262,144 nodes, e.g. a 64^3-node grid
-constexpr int kMaxDevices = 64;
 
 // (m, px, py, pz) and (fx, fy, fz, unused) per node
 static __device__ __align__(256) float4 g_noalloc_grid[2 * kNoAllocMaxNodes];
-
-std::mutex g_setup_mutex;
-float4* g_grid_addr[kMaxDevices] = {};
 
 struct NaGrid {
   double origin[3];
@@ -138,20 +135,13 @@ extern "C" int mpm_p2g_noalloc(const mpm_domain* domain, const mpm_material* mat
   g.invH = static_cast<float>(1.0 / H);
   const long long nodes = (long long)g.dims[0] * g.dims[1] * g.dims[2];
   if (nodes > kNoAllocMaxNodes) return MPM_ERR_CAPACITY;  // grid larger than the fixed scratch
-  // set-up, once per device with that device current: the device address of the scratch array
-  // (in host code the array's name is only a host-side stand-in, not a device address)
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return MPM_ERR_CUDA;
-  float4* grid = nullptr;
-  {
-    std::lock_guard<std::mutex> lock(g_setup_mutex);
-    if (!g_grid_addr[dev]) {
-      void* p = nullptr;
-      if (cudaGetSymbolAddress(&p, g_noalloc_grid) != cudaSuccess || !p) return MPM_ERR_CUDA;
-      g_grid_addr[dev] = static_cast<float4*>(p);
-    }
-    grid = g_grid_addr[dev];
-  }
+  // set-up with the caller's device current: the device address of the scratch array on that
+  // device (in host code the array's name is only a host-side stand-in, not a device address). It
+  // is looked up on every call rather than cached, so a context re-created after a device reset
+  // (or a change of current device) never gets a stale address; the lookup allocates nothing.
+  void* scratch = nullptr;
+  if (cudaGetSymbolAddress(&scratch, g_noalloc_grid) != cudaSuccess || !scratch) return MPM_ERR_CUDA;
+  float4* grid = static_cast<float4*>(scratch);
   mpm::MaterialDev mt{};
   mt.model = model;
   mt.mu = static_cast<float>(material->mu);

@@ -64,3 +64,43 @@ def test_run_tops_up_a_short_estimate():
     assert a.status() == 0 and b.status() == 0
     a.close()
     b.close()
+
+
+def test_run_with_regularisation_matches_consecutive_steps():
+    """The regularised branch of mpm_run (solid regularisation after every substep, run step by step
+    on the host's schedule) against the same requested steps as single mpm_step calls."""
+    sc = impact_scene()
+    a, b = pair(sc)
+    for s in (a, b):
+        s.set_regularizer(True)
+    dt_req = 3 * a.stable_dt()
+    total = sum(a.step(dt_req)[0] for _ in range(4))
+    s_run, adv_run = b.run(dt_req, 4)
+    assert s_run == total and total >= 8
+    assert abs(adv_run - 4 * dt_req) <= 1e-6 * dt_req
+    oa, ob = a.download(("x", "F")), b.download(("x", "F"))
+    assert np.max(np.abs(oa["x"] - ob["x"])) <= 1e-6
+    assert np.max(np.abs(oa["F"] - ob["F"])) <= 1e-6
+    a.close()
+    b.close()
+
+
+def test_run_stops_at_a_nonfinite_state():
+    """Fault injection on the host: one particle uploaded with a NaN velocity. mpm_run over 20 steps
+    stops with MPM_ERR_NONFINITE and the non-finite flag in the status, and a clean handle stepped
+    the same way afterwards is unaffected."""
+    from mpm_b200._lib import MpmError
+    sc = impact_scene()
+    good = Solver(sc.domain, sc.n)
+    good.upload(sc)
+    sc.v[17, 0] = float("nan")
+    a = Solver(sc.domain, sc.n)
+    a.upload(sc)
+    with pytest.raises(MpmError) as e:
+        a.run(2e-7, 20)
+    assert e.value.code == -4
+    assert a.status() & 1
+    sub, _ = good.run(2e-7, 3)
+    assert sub >= 3 and good.status() == 0
+    a.close()
+    good.close()

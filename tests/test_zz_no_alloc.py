@@ -1,11 +1,12 @@
-"""The allocation-free P2G entry point against the handle path (GPU, through the C ABI).
+"""The allocation-free P2G entry point against the oracle and the handle path (GPU, through the C ABI).
 
 mpm_p2g_noalloc serves callers that cannot allocate device memory themselves (a host that owns all
 device memory through its own pool, or code running where cudaMalloc is not allowed): the caller
 passes device inputs and outputs and the library's only intermediate is a fixed device array. This
 test allocates the caller's buffers with torch, calls the entry point twice in a row, and checks
-both results against mpm_grid_debug of a handle holding the same state, within the grid tolerance of
-the other parity tests (1e-6 normwise relative). It sits in a file of its own, collected last.
+both results against the FP64 oracle's grid after P2G of the same state and against mpm_grid_debug
+of a handle holding it, within the grid tolerance of the other parity tests (1e-6 normwise
+relative). It sits in a file of its own, collected last.
 """
 import ctypes
 
@@ -13,6 +14,7 @@ import numpy as np
 import pytest
 
 from mpm_b200 import _lib, scenes
+from oracle import oracle as orc
 from mpm_b200.solver import Solver, domain_struct, material_struct
 
 pytestmark = pytest.mark.gpu
@@ -33,13 +35,14 @@ def deformed_j2_block():
     return sc
 
 
-def test_noalloc_p2g_matches_handle_path_twice():
+def test_noalloc_p2g_matches_oracle_and_handle_path_twice():
     import torch
     sc = deformed_j2_block()
     dt = 1e-6
     sol = Solver(sc.domain, sc.n)
     sol.upload(sc)
-    gm_ref, gp_ref = sol.grid_debug(dt)
+    gm_dev, gp_dev = sol.grid_debug(dt)
+    gm_ref, gp_ref, _ = orc.state_from_scene(sc).step(dt, want_grid=True)
     dims, _ = sol.grid_dims()
     nodes = int(np.prod(dims))
     dev = torch.device("cuda", 0)
@@ -67,6 +70,9 @@ def test_noalloc_p2g_matches_handle_path_twice():
         gp = mom.cpu().numpy().reshape(-1, 3)
         assert rel(gm, gm_ref) <= 1e-6, call
         assert rel(gp, gp_ref) <= 1e-6, call
+        assert rel(gm, gm_dev) <= 1e-6, call
+        assert rel(gp, gp_dev) <= 1e-6, call
+    sol.close()
 
 
 def test_noalloc_rejects_grids_beyond_the_scratch_size():
