@@ -88,6 +88,9 @@ struct Ctrl {
   int step_substeps;     // substeps of the current requested-dt step
   unsigned sort_list;    // work list the sort after a scatter pass appends to (written by that pass)
   unsigned sort_active;  // 1 if that pass ran (the sort and scan skip a pass that returned at done)
+  unsigned last_substep; // 1 when the current substep is the call's last (set by k_begin): only then
+                         // does the fused pass store particle velocities and APIC matrices, which no
+                         // later substep of the call reads
 };
 
 struct Particles {

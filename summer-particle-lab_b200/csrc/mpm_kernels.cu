@@ -107,6 +107,12 @@ __device__ __forceinline__ int find_scene_by_node_tile(const SceneDev* sc, int n
   return lo;
 }
 
+// Paired FP32 arithmetic of sm_100 (FFMA2 / FMUL2): two independent lanes per instruction, each
+// rounded exactly like a scalar fmaf / multiply, so the results are bitwise those of the scalar form.
+__device__ __forceinline__ float2 ffma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 fmul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 dup2(float x) { return make_float2(x, x); }
+
 // Stencil along one axis from a fixed-point position (src/three/mpm.js:25-32):
 // base = clamp(floor(q - 0.5), 0, N - 3), t = q - base (exact: integer below 2^24 times 2^-22).
 __device__ __forceinline__ void stencil_axis(unsigned q, int dim, int& base, float& t) {
@@ -201,6 +207,7 @@ __global__ void k_control(Ctx c, ControlOp op) {
   Ctrl* ct = c.ctrl;
   if (threadIdx.x == 0) {
     const unsigned k = ct->step_index;
+    ct->last_substep = 1u;
     if (op.op == 0) {
       ct->work_count[k & 1] = 0;
       ct->active_count[k & 1] = 0;
@@ -294,6 +301,14 @@ __global__ void __launch_bounds__(256) k_begin(Ctx c) {
       ct->substeps += 1;
       ct->step_substeps += 1;
       ct->advanced += dt;
+      // the next k_begin ends the call after this substep (the same tests it will make)
+      bool last;
+      if (ct->mode == kModeRequested)
+        last = ct->steps_left <= 1 &&
+               (!(ct->remaining > 1e-6 * ct->dt_requested) || ct->step_substeps >= ct->max_substeps);
+      else
+        last = ct->substeps >= ct->max_substeps;
+      ct->last_substep = last ? 1u : 0u;
       const unsigned k = ct->step_index + 1;
       ct->step_index = k;
       ct->work_count[k & 1] = 0;
@@ -513,7 +528,12 @@ void launch_sort_scatter(const Ctx& c, cudaStream_t st, bool initial) {
 // kCap = 512 those took a second round (every phase and barrier again for a handful of particles).
 constexpr int kCap = 768;
 constexpr int kPf = 2;         // perm entries of the next tile's first round held in registers per thread
-constexpr int kPay = 23;       // payload floats per particle (the last, m T, only with conduction)
+// Payload of one particle: 12 float pairs, laid out for the paired FMAs of phase B:
+//   0 (tx, ty)   1 (tz, m)    2 (mv0, mv1)  3 (mv2, m T)  [m T only with conduction, else 0]
+//   4 (c02, c12) 5 (c22, s02) 6 (s12, s22)  7 (c01, c11)  8 (c21, s01)  9 (c00, c10)  10 (c20, s00)
+//   11 (s11, 0)
+// with c = m h C and s = -4 V / h tau (symmetric).
+constexpr int kPayRows = 12;
 constexpr int kBuckets = 216;  // 6^3 possible stencil bases in the scatter window
 // Payload slot of particle j: one extra word every 32 slots, so the slots phase B reads at a
 // stride of a bucket's size (8 for the particles of one cell in consecutive slots) fall in
@@ -539,7 +559,7 @@ struct TileCtx {
 struct __align__(128) PartSmem {
   float4 vwin[2][kWinG * kWinG * kWinG];  // double-buffered TMA destinations (3456 B each)
   float acc[kChannels * kWinSNodes];      // 16 KiB scatter window
-  float pay[kPay * kPayStride];           // 47 KiB payloads, structure of arrays (swizzled slots)
+  float2 pay[kPayRows * kPayStride];      // 74 KiB payloads, structure of pair arrays (swizzled slots)
   unsigned meta[kCap];                    // bucket | rank << 8 (or kMetaInvalid)
   unsigned short sidx[kCap];              // slots sorted by bucket
   int hist[kBuckets];
@@ -664,56 +684,55 @@ __device__ __forceinline__ unsigned state_flags(const float v[3], const float D[
 }
 
 // Phase B task: one non-empty base bucket, one z layer of its stencil. Sums the 3x3 nodes x 7
-// channels over the bucket's particles in registers, then adds them to the shared window.
+// channels over the bucket's particles in registers, then adds them to the shared window. The
+// channels run as one scalar (mass) and three pairs (p0, p1), (p2, f0), (f1, f2) of paired FMAs.
 template <bool HEAT>
-__device__ __forceinline__ void bucket_layer_p(const float* pay, const unsigned short* sidx, const int* bstart,
+__device__ __forceinline__ void bucket_layer_p(const float2* pay, const unsigned short* sidx, const int* bstart,
                                                float* acc, int b, int kz) {
   const int lx = b % 6, ly = (b / 6) % 6, lz = b / 36;
-  float a[3][3][7];
+  float a0[3][3];
+  float2 a12[3][3], a34[3][3], a56[3][3];
 #pragma unroll
   for (int y = 0; y < 3; ++y)
 #pragma unroll
-    for (int x = 0; x < 3; ++x)
-#pragma unroll
-      for (int ch = 0; ch < 7; ++ch) a[y][x][ch] = 0.f;
+    for (int x = 0; x < 3; ++x) {
+      a0[y][x] = 0.f;
+      a12[y][x] = a34[y][x] = a56[y][x] = dup2(0.f);
+    }
   const int i1 = bstart[b + 1];
   for (int i = bstart[b]; i < i1; ++i) {
     const int j = sidx[i];
-    const float* P = pay + pay_slot(j);
-    const float tx = P[0 * kPayStride], ty = P[1 * kPayStride], tz = P[2 * kPayStride], m = P[3 * kPayStride];
-    const float mv0 = P[4 * kPayStride], mv1 = P[5 * kPayStride], mv2 = P[6 * kPayStride];
-    const float c00 = P[7 * kPayStride], c01 = P[8 * kPayStride], c02 = P[9 * kPayStride];
-    const float c10 = P[10 * kPayStride], c11 = P[11 * kPayStride], c12 = P[12 * kPayStride];
-    const float c20 = P[13 * kPayStride], c21 = P[14 * kPayStride], c22 = P[15 * kPayStride];
-    const float s00 = P[16 * kPayStride], s11 = P[17 * kPayStride], s22 = P[18 * kPayStride];
-    const float s01 = P[19 * kPayStride], s02 = P[20 * kPayStride], s12 = P[21 * kPayStride];
+    const float2* P = pay + pay_slot(j);
+    const float2 txy = P[0 * kPayStride], tzm = P[1 * kPayStride], mv01 = P[2 * kPayStride];
+    const float2 mv2h = P[3 * kPayStride], E = P[4 * kPayStride], Fz = P[5 * kPayStride];
+    const float2 G = P[6 * kPayStride], H = P[7 * kPayStride], I = P[8 * kPayStride];
+    const float2 K = P[9 * kPayStride], L = P[10 * kPayStride], S11 = P[11 * kPayStride];
+    const float2 J = make_float2(S11.x, G.x);  // (s11, s12)
+    const float2 M = make_float2(I.y, Fz.y);   // (s01, s02)
     float wx[3], wy[3], wzv[3];
-    bspline_weights(tx, wx);
-    bspline_weights(ty, wy);
-    bspline_weights(tz, wzv);
+    bspline_weights(txy.x, wx);
+    bspline_weights(txy.y, wy);
+    bspline_weights(tzm.x, wzv);
     const float wz = kz == 0 ? wzv[0] : (kz == 1 ? wzv[1] : wzv[2]);
-    const float dz = static_cast<float>(kz) - tz;
-    const float q0 = mv0 + c02 * dz, q1 = mv1 + c12 * dz, q2 = mv2 + c22 * dz;
-    const float g0 = s02 * dz, g1 = s12 * dz, g2 = s22 * dz;
-    const float mwz = m * wz;
+    const float2 dz2 = dup2(static_cast<float>(kz) - tzm.x);
+    const float2 q01 = ffma2(E, dz2, mv01);                        // (mv0 + c02 dz, mv1 + c12 dz)
+    const float2 q2g0 = ffma2(Fz, dz2, make_float2(mv2h.x, 0.f));  // (mv2 + c22 dz, s02 dz)
+    const float2 g12 = fmul2(G, dz2);                              // (s12 dz, s22 dz)
+    const float mwz = tzm.y * wz;
 #pragma unroll
     for (int y = 0; y < 3; ++y) {
-      const float dy = static_cast<float>(y) - ty;
+      const float2 dy2 = dup2(static_cast<float>(y) - txy.y);
       const float wyz = wy[y] * wz;
-      const float p0 = q0 + c01 * dy, p1 = q1 + c11 * dy, p2 = q2 + c21 * dy;
-      const float f0 = g0 + s01 * dy, f1 = g1 + s11 * dy, f2 = g2 + s12 * dy;
+      const float2 p01 = ffma2(H, dy2, q01), p2f0 = ffma2(I, dy2, q2g0), f12 = ffma2(J, dy2, g12);
       const float mwyz = mwz * wy[y];
 #pragma unroll
       for (int x = 0; x < 3; ++x) {
-        const float dx = static_cast<float>(x) - tx;
-        const float wt = wx[x] * wyz;
-        a[y][x][0] += wx[x] * mwyz;
-        a[y][x][1] += wt * (p0 + c00 * dx);
-        a[y][x][2] += wt * (p1 + c10 * dx);
-        a[y][x][3] += wt * (p2 + c20 * dx);
-        a[y][x][4] += wt * (f0 + s00 * dx);
-        a[y][x][5] += wt * (f1 + s01 * dx);
-        a[y][x][6] += wt * (f2 + s02 * dx);
+        const float2 dx2 = dup2(static_cast<float>(x) - txy.x);
+        const float2 wt = dup2(wx[x] * wyz);
+        a0[y][x] = fmaf(wx[x], mwyz, a0[y][x]);
+        a12[y][x] = ffma2(wt, ffma2(K, dx2, p01), a12[y][x]);
+        a34[y][x] = ffma2(wt, ffma2(L, dx2, p2f0), a34[y][x]);
+        a56[y][x] = ffma2(wt, ffma2(M, dx2, f12), a56[y][x]);
       }
     }
   }
@@ -721,9 +740,14 @@ __device__ __forceinline__ void bucket_layer_p(const float* pay, const unsigned 
   for (int y = 0; y < 3; ++y)
 #pragma unroll
     for (int x = 0; x < 3; ++x) {
-      const int node = ((lz + kz) * kWinS + (ly + y)) * kWinS + (lx + x);
-#pragma unroll
-      for (int ch = 0; ch < 7; ++ch) atomicAdd(&acc[ch * kWinSNodes + node], a[y][x][ch]);
+      float* A = acc + ((lz + kz) * kWinS + (ly + y)) * kWinS + (lx + x);
+      atomicAdd(A + 0 * kWinSNodes, a0[y][x]);
+      atomicAdd(A + 1 * kWinSNodes, a12[y][x].x);
+      atomicAdd(A + 2 * kWinSNodes, a12[y][x].y);
+      atomicAdd(A + 3 * kWinSNodes, a34[y][x].x);
+      atomicAdd(A + 4 * kWinSNodes, a34[y][x].y);
+      atomicAdd(A + 5 * kWinSNodes, a56[y][x].x);
+      atomicAdd(A + 6 * kWinSNodes, a56[y][x].y);
     }
   if (HEAT) {  // sum w m T into channel 7 (conduction)
     float hsum[3][3];
@@ -732,12 +756,13 @@ __device__ __forceinline__ void bucket_layer_p(const float* pay, const unsigned 
 #pragma unroll
       for (int x = 0; x < 3; ++x) hsum[y][x] = 0.f;
     for (int i = bstart[b]; i < i1; ++i) {
-      const float* P = pay + pay_slot(sidx[i]);
+      const float2* P = pay + pay_slot(sidx[i]);
+      const float2 txy = P[0 * kPayStride];
       float wx[3], wy[3], wzv[3];
-      bspline_weights(P[0 * kPayStride], wx);
-      bspline_weights(P[1 * kPayStride], wy);
-      bspline_weights(P[2 * kPayStride], wzv);
-      const float wmt = (kz == 0 ? wzv[0] : (kz == 1 ? wzv[1] : wzv[2])) * P[22 * kPayStride];
+      bspline_weights(txy.x, wx);
+      bspline_weights(txy.y, wy);
+      bspline_weights(P[1 * kPayStride].x, wzv);
+      const float wmt = (kz == 0 ? wzv[0] : (kz == 1 ? wzv[1] : wzv[2])) * P[3 * kPayStride].y;
 #pragma unroll
       for (int y = 0; y < 3; ++y)
 #pragma unroll
@@ -876,9 +901,9 @@ __device__ __noinline__ void gather_global(const float4* base, int sy, long long
 template <int PASS, bool HEAT, bool AUX>
 __device__ __forceinline__ unsigned particle_phase_a(const Ctx& c, const SceneDev& sc, const TileCtx& tc,
                                                      const MaterialDev& mt_single, bool single, const float4* vwin,
-                                                     unsigned home, unsigned j, float dt, int nxt, float* pay,
+                                                     unsigned home, unsigned j, float dt, int nxt, float2* pay,
                                                      unsigned* meta, int* hist, float& wave_acc, float& grad_acc,
-                                                     unsigned& flags_acc, double& work_acc) {
+                                                     unsigned& flags_acc, double& work_acc, bool store_vc) {
   constexpr bool SCATTER = PASS != kPassG2P;
   constexpr bool GATHER = PASS != kPassP2G;
   unsigned key = 0xffffffffu;
@@ -978,11 +1003,15 @@ __device__ __forceinline__ unsigned particle_phase_a(const Ctx& c, const SceneDe
     ep += co.dep;
     T += co.dT;
     c.p.qx[home] = q[0]; c.p.qy[home] = q[1]; c.p.qz[home] = q[2];
-    c.p.vx[home] = v[0]; c.p.vy[home] = v[1]; c.p.vz[home] = v[2];
 #pragma unroll
-    for (int e = 0; e < 9; ++e) {
-      c.p.Cc[e][home] = C[e];
-      c.p.Dc[e][home] = D[e];
+    for (int e = 0; e < 9; ++e) c.p.Dc[e][home] = D[e];
+    // v and C: the fused pass scatters the ones it just gathered and never reads the stored copies,
+    // so it stores them only on the call's last substep (downloads, ledgers, frames, regularisation
+    // and a later P2G of the stored state read them after the call); the gather-only pass always does
+    if (PASS != kPassG2P2G || store_vc) {
+      c.p.vx[home] = v[0]; c.p.vy[home] = v[1]; c.p.vz[home] = v[2];
+#pragma unroll
+      for (int e = 0; e < 9; ++e) c.p.Cc[e][home] = C[e];
     }
     if (c.has_plastic) c.p.ep[home] = ep;
     if (c.has_thermal) c.p.T[home] = T;
@@ -1027,14 +1056,19 @@ __device__ __forceinline__ unsigned particle_phase_a(const Ctx& c, const SceneDe
       if (lane == leader) rank0 = atomicAdd(&hist[bucket], __popc(peers));
       const int rank = __shfl_sync(peers, rank0, leader) + __popc(peers & ((1u << lane) - 1u));
       meta[j] = static_cast<unsigned>(bucket) | (static_cast<unsigned>(rank) << 8);
-      float* P = pay + pay_slot(j);
-      P[0 * kPayStride] = t[0]; P[1 * kPayStride] = t[1]; P[2 * kPayStride] = t[2]; P[3 * kPayStride] = m;
-      P[4 * kPayStride] = mv[0]; P[5 * kPayStride] = mv[1]; P[6 * kPayStride] = mv[2];
-#pragma unroll
-      for (int e = 0; e < 9; ++e) P[(7 + e) * kPayStride] = mC[e];
-#pragma unroll
-      for (int e = 0; e < 6; ++e) P[(16 + e) * kPayStride] = s6[e];
-      if (HEAT) P[22 * kPayStride] = m * T;
+      float2* P = pay + pay_slot(j);
+      P[0 * kPayStride] = make_float2(t[0], t[1]);
+      P[1 * kPayStride] = make_float2(t[2], m);
+      P[2 * kPayStride] = make_float2(mv[0], mv[1]);
+      P[3 * kPayStride] = make_float2(mv[2], HEAT ? m * T : 0.f);
+      P[4 * kPayStride] = make_float2(mC[2], mC[5]);
+      P[5 * kPayStride] = make_float2(mC[8], s6[4]);
+      P[6 * kPayStride] = make_float2(s6[5], s6[2]);
+      P[7 * kPayStride] = make_float2(mC[1], mC[4]);
+      P[8 * kPayStride] = make_float2(mC[7], s6[3]);
+      P[9 * kPayStride] = make_float2(mC[0], mC[3]);
+      P[10 * kPayStride] = make_float2(mC[6], s6[0]);
+      P[11 * kPayStride] = make_float2(s6[1], 0.f);
     } else {
       meta[j] = kMetaInvalid;
       if (!in_w) flags |= 0x10u;
@@ -1094,6 +1128,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_particles(const __grid_constant__
   }
   if (PASS != kPassP2G && ct->done) return;
   const unsigned k = ct->step_index;
+  const bool store_vc = ct->last_substep != 0u;
   // lists: the P2G pass reads the list its sort just wrote (k & 1) and scatters into acc[k & 1];
   // a substep (after k_begin advanced k) reads list (k - 1) & 1 and scatters into acc[k & 1]
   const int lst = PASS == kPassP2G ? (k & 1) : ((k - 1) & 1);
@@ -1215,7 +1250,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_particles(const __grid_constant__
         if (j < nround) {
           const unsigned home = (r0 == 0 && pf_ok && jj < kPf * kBlock) ? pf[jj / kBlock] : c.p.perm[it.y + r0 + j];
           key = particle_phase_a<PASS, HEAT, AUX>(c, sc, tc, sm.mt, single, sm.vwin[cb], home, j, dt, nxt, sm.pay, sm.meta,
-                                       sm.hist, wave_acc, grad_acc, flags_acc, work_acc);
+                                       sm.hist, wave_acc, grad_acc, flags_acc, work_acc, store_vc);
         }
         if (PASS == kPassG2P2G) count_key(c, key);
       }
@@ -1295,7 +1330,7 @@ struct StageInfo {
 
 struct __align__(128) WsSmem {
   float4 vwin[2][kWinG * kWinG * kWinG];  // producer: double-buffered TMA destinations
-  float pay[2][kPay * kPayStride];        // stage buffers
+  float2 pay[2][kPayRows * kPayStride];   // stage buffers
   unsigned meta[2][kCap];
   int hist[2][kBuckets];
   StageInfo info[2];
@@ -1365,6 +1400,7 @@ __global__ void __launch_bounds__(kWsThreads, 1) k_particles_ws(const __grid_con
   }
   if (PASS != kPassP2G && ct->done) return;
   const unsigned k = ct->step_index;
+  const bool store_vc = ct->last_substep != 0u;
   const int lst = PASS == kPassP2G ? (k & 1) : ((k - 1) & 1);
   const int nxt = k & 1;
   const bool use_tma = GATHER && c.use_tma;
@@ -1484,7 +1520,7 @@ __global__ void __launch_bounds__(kWsThreads, 1) k_particles_ws(const __grid_con
           if (j < nround) {
             const unsigned home = c.p.perm[it.y + r0 + j];
             key = particle_phase_a<PASS, HEAT, AUX>(c, sc, tc, sm.mt, single, sm.vwin[cb], home, j, dt, nxt, sm.pay[s],
-                                         sm.meta[s], sm.hist[s], wave_acc, grad_acc, flags_acc, work_acc);
+                                         sm.meta[s], sm.hist[s], wave_acc, grad_acc, flags_acc, work_acc, store_vc);
           }
           if (PASS == kPassG2P2G) count_key(c, key);
         }
