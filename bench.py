@@ -38,7 +38,7 @@ for _p in (ROOT, PKG):
 METRIC = "particle-steps/s, 2M-particle J2 MPM: surrogate+batched vs exact, same stress err"
 UNIT = "particle-steps/s"
 # algorithmic bytes per particle-step (FP32 state read once and written once) and per active node
-BYTES_PER_PARTICLE = {0: 200, 1: 200, 4: 208, 5: 208, 10: 216}
+BYTES_PER_PARTICLE = {0: 200, 1: 200, 4: 208, 5: 208, 6: 216, 7: 208, 10: 216}
 BYTES_PER_NODE = 56
 
 
@@ -56,6 +56,8 @@ def parse():
     ap.add_argument("--no-ensemble", action="store_true")
     ap.add_argument("--no-surrogate", action="store_true")
     ap.add_argument("--surrogate-only", action="store_true")
+    ap.add_argument("--learned-newton", type=int, default=4, help="most Newton steps after the network's prediction")
+    ap.add_argument("--learned-gate", type=float, default=1e-5, help="gate: consistency residual / trial stress")
     ap.add_argument("--surrogate-steps", type=int, default=0, help="training steps (0: the default schedule)")
     ap.add_argument("--ensemble-only", action="store_true")
     ap.add_argument("--ensemble-scenes", type=int, default=256)
@@ -80,6 +82,8 @@ def make_scene(args):
         return scenes.thermal_j2()
     if args.workload == "coupled_collision":
         return scenes.coupled_collision()
+    if args.workload == "jc_impact":
+        return scenes.jc_impact()
     raise SystemExit(f"unknown workload {args.workload}")
 
 
@@ -452,7 +456,8 @@ def surrogate_leg(steps=0):
                      "learned_share_of_plastic": r["learned"] / plastic if plastic else None})
     s.close()
     return {"law": "thermal J2 (model 10), E 70 GPa, nu 0.33, yield 250 MPa, H 1 GPa, -0.3 MPa/K",
-            "network": "8-64-64-7 ReLU, BF16 mma.sync m16n8k16, FP32 accumulate",
+            "network": "8-64-64-7 ReLU, BF16 operands, FP32 accumulate; training and the gated map on tcgen05 "
+                       "(TMEM accumulators, 128 samples per tile)",
             "training": {"samples": cfg.samples, "batch": cfg.batch, "steps": cfg.steps, "seconds": el,
                          "loss_first": float(hist[:10].mean()), "loss_last": float(hist[-100:].mean()),
                          "mlp_tflops": train_flops / el / 1e12,
@@ -460,6 +465,119 @@ def surrogate_leg(steps=0):
                          "note": "wall clock of the whole call, sample generation included"},
             "return_map_4096000_states": rows,
             "exact_stress_error": "FP32 exact map: within 1e-5 x yield of the FP64 oracle (tests/test_surrogate.py)"}
+
+
+def learned_step_leg(args):
+    """The learned return map inside the fused step, on the law whose exact return iterates: a
+    Johnson-Cook network (8-64-64-7, BF16 tensor cores, FP32 accumulation) trained on the GPU from
+    the exact bisection's roots, then
+      - the 2M-particle Johnson-Cook impact (64^3-cell block, 8 ppc, 128^3 grid, 60 m/s) stepped K
+        requested steps through mpm_run in exact and in learned mode from the same initial state
+        (CUDA events on the handle's stream), and
+      - the 256-scene V&V ensemble with Johnson-Cook materials on one batch handle with graph replay,
+        exact and learned,
+    both at one stated stress error: the gate accepts a prediction only when its consistency
+    residual is at most gate_tol x the trial stress (the bisection's own FP32 residual is below it);
+    the end states of the two modes are compared."""
+    import torch
+    from mpm_b200 import scenes
+    from mpm_b200.solver import Batch, Solver
+    from mpm_b200.surrogate import Surrogate, jc_config
+    gate_tol, newton = args.learned_gate, args.learned_newton
+    mat = scenes.johnson_cook_metal(7)
+    s = Surrogate(mat, seed=11)
+    cfg = jc_config(newton=newton)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    hist = s.train(cfg)
+    train_s = time.perf_counter() - t0
+    kern = s.time(4_096_000, iters=10, gate_tol=gate_tol, cfg=cfg)
+    plastic_k = kern["learned"] + kern["fallback"]
+    scene = scenes.jc_impact()
+    dt_req = scene.meta["dt"]
+    K = args.steps
+
+    def timed(learned):
+        sol = Solver(scene.domain, scene.n)
+        sol.upload(scene)
+        if learned:
+            sol.set_return_mode(s, gate_tol=gate_tol, newton=newton)
+        ext = torch.cuda.ExternalStream(sol.stream())
+        sol.run(dt_req, max(1, args.warmup))
+        sol.gate_counts(reset=True)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(ext)
+        sub, _ = sol.run(dt_req, K)
+        e1.record(ext)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        counts = sol.gate_counts()
+        out = sol.download(("x", "ep", "F"))
+        st = sol.status()
+        sol.close()
+        return {"value": scene.n * sub / (ms / 1e3), "ms_per_step": ms / K, "substeps": sub, "status": st,
+                "gate_learned": counts[0], "gate_fallback": counts[1]}, out
+
+    ex, ox = timed(False)
+    le, ol = timed(True)
+    served = le["gate_learned"] / max(1, le["gate_learned"] + le["gate_fallback"])
+    step = {"workload": scene.meta["workload"], "particles": scene.n, "requested_steps": K, "dt_requested": dt_req,
+            "exact": ex, "learned": le, "speedup_learned_vs_exact": le["value"] / ex["value"],
+            "learned_share_of_returns": served,
+            "end_state_difference": {"x_m": float(np.max(np.abs(ox["x"] - ol["x"]))),
+                                     "ep": float(np.max(np.abs(ox["ep"] - ol["ep"]))),
+                                     "F": float(np.max(np.abs(ox["F"] - ol["F"]))),
+                                     "max_ep": float(np.max(ox["ep"]))}}
+    # the V&V ensemble with Johnson-Cook materials on one batch handle, exact and learned
+    ens = scenes.ensemble(args.ensemble_scenes, model=7)
+    Ke = args.ensemble_steps
+    n_all = sum(sc.n for sc in ens)
+
+    def batch_run(learned):
+        b = Batch(ens)
+        b.upload()
+        if learned:
+            b.set_return_mode(s, gate_tol=gate_tol, newton=newton)
+        b.run(Ke, graph=True)  # warm-up, captures the graph
+        b.gate_counts(reset=True)
+        torch.cuda.synchronize()
+        ext = torch.cuda.ExternalStream(b.stream())
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(ext)
+        b.run(Ke, graph=True)
+        e1.record(ext)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        counts = b.gate_counts()
+        st = b.status()
+        b.close()
+        return {"value": n_all * Ke / (ms / 1e3), "ms_per_substep": ms / Ke, "status": st,
+                "gate_learned": counts[0], "gate_fallback": counts[1]}
+
+    bex = batch_run(False)
+    ble = batch_run(True)
+    s.close()
+    mlp_flop = 2 * (8 * 64 + 64 * 64 + 64 * 7)
+    return {"law": "Johnson-Cook model 7 (A = B = yield, n 0.35, C 0.025, rate0 1/s; src/three/metal-plasticity.js:28-34, "
+                   "24 bisection halvings)",
+            "network": "8-64-64-7 ReLU: training on tcgen05 (TMEM accumulators); in-step inference as warp-wide "
+                       "mma.sync m16n8k16 tiles inside the fused pass, FP32 accumulate",
+            "gate": {"tol": gate_tol, "newton_steps_max": newton,
+                     "stated_stress_error": f"consistency residual <= {gate_tol:g} x trial stress for every accepted "
+                                            f"return"},
+            "training": {"samples": cfg.samples, "batch": cfg.batch, "steps": cfg.steps, "seconds": train_s,
+                         "loss_first": float(hist[:10].mean()), "loss_last": float(hist[-100:].mean()),
+                         "mlp_tflops": 3.0 * mlp_flop * cfg.batch * cfg.steps / train_s / 1e12,
+                         "note": "wall clock of the whole call, sample generation included"},
+            "return_map_4096000_states": {"ms_exact": kern["ms_exact"], "ms_learned": kern["ms_learned"],
+                                          "speedup": kern["ms_exact"] / kern["ms_learned"],
+                                          "learned_share_of_plastic": kern["learned"] / max(1, plastic_k),
+                                          "plastic": plastic_k},
+            "step": step,
+            "ensemble": {"workload": f"vv_ensemble_jc_{len(ens)}_seeds_1000", "particles": n_all, "substeps": Ke,
+                         "exact_batched": bex, "learned_batched": ble,
+                         "speedup_learned_vs_exact": ble["value"] / bex["value"]}}
 
 
 def slab_leg(args, rank, world, dist):
@@ -593,7 +711,8 @@ def main():
 
     if args.surrogate_only:
         if rank == 0:
-            print(json.dumps({"surrogate": surrogate_leg(args.surrogate_steps)}), flush=True)
+            print(json.dumps({"surrogate": surrogate_leg(args.surrogate_steps),
+                              "learned_return": learned_step_leg(args)}), flush=True)
         if dist is not None:
             dist.barrier()
             dist.destroy_process_group()
@@ -737,6 +856,7 @@ def main():
         line["ensemble"] = ensemble_leg(args, rank, world, dist)
     if rank == 0 and world == 1 and not args.no_surrogate:
         line["surrogate"] = surrogate_leg(args.surrogate_steps)
+        line["learned_return"] = learned_step_leg(args)
     if rank == 0:
         print(json.dumps(line), flush=True)
     sol.close()

@@ -464,10 +464,11 @@ typedef struct mpm_surrogate_config {
   double lr, weight_decay;
   double dep_weight;     /* loss weight of the dep output (others 1) */
   int32_t cosine;        /* 1: cosine learning-rate decay */
-  int32_t reserved;
+  int32_t newton;        /* Johnson-Cook: most Newton steps after the prediction (0: 4) */
   uint64_t seed;
   double strain_min, strain_max; /* log-uniform magnitude of the principal trial log strains */
   double T_min, T_max, ep_max;   /* uniform temperature and plastic strain */
+  double dt_min, dt_max;         /* Johnson-Cook: log-uniform substep (0, 0: 1e-7 .. 1e-5 s) */
 } mpm_surrogate_config;
 
 typedef struct mpm_gate_counts {
@@ -500,6 +501,27 @@ int mpm_surrogate_forward(mpm_surrogate* s, int64_t n, const float* X, float* Y)
 int mpm_return_map_learned(mpm_surrogate* s, int64_t n, const double* F_in, const double* ep, const double* T,
                            double gate_tol, int32_t use_mlp, double* F_out, double* dep, double* tau, int8_t* path,
                            mpm_gate_counts* counts);
+/* ---- learned return map inside the step ----
+ * The reference's per-particle return (src/three/mpm.js:126-131 calling projectPlastic,
+ * src/three/constitutive.js:52-78) with the Johnson-Cook plastic increment
+ * (src/three/metal-plasticity.js:28-34, 24 bisection halvings of the consistency condition) taken from a
+ * network trained for models 6 / 7 (mpm_surrogate_create with such a material, mpm_surrogate_train):
+ * the fused particle pass evaluates it on the tensor cores for every particle whose trial stress
+ * exceeds the initial flow stress, refines the predicted increment by at most `newton` Newton steps
+ * on the consistency condition (stopping once the gate passes) and accepts it only when the
+ * dimensionless residual |q - 3 mu / J dep - flow(ep + dep, dep / dt, T)| / q is at most gate_tol
+ * (the stress residual is then at most gate_tol x the trial stress); every other particle takes the
+ * exact bisection. The handle keeps its own copy of the weights (the surrogate may be destroyed
+ * afterwards). MPM_RETURN_EXACT restores the reference's map. Scenes with grid conduction or with
+ * snow, sand or pressure materials run the exact map (MPM_ERR_UNSUPPORTED when set on such a
+ * handle). Batch handles take it for all their scenes. */
+#define MPM_RETURN_EXACT 0
+#define MPM_RETURN_LEARNED_GATED 1
+int mpm_set_return_mode(mpm_handle* h, int32_t mode, mpm_surrogate* s, double gate_tol, int32_t newton);
+/* Returns served by the network (learned) and sent to the exact map (fallback) since the mode was
+ * set or the counts were last reset (reset != 0 clears them after the read); elastic is 0. */
+int mpm_gate_counts_read(mpm_handle* h, mpm_gate_counts* out, int32_t reset);
+
 /* Device time per call of the gated map and of the exact map on n device-resident random trial
  * states drawn like cfg's training set (iters calls each, CUDA events). */
 int mpm_surrogate_time(mpm_surrogate* s, const mpm_surrogate_config* cfg, int64_t n, int32_t iters, double gate_tol,

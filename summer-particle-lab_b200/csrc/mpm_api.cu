@@ -14,6 +14,7 @@
 
 #include "mpm_b200.h"
 #include "mpm_internal.h"
+#include "surrogate_net.h"
 #include "pairs.h"
 
 using mpm::Ctx;
@@ -118,6 +119,10 @@ struct mpm_handle {
   double heat_radius = 0;
   double* host_exchanged = nullptr;  // pinned readback
   int slab_planes = 0;     // batch of slabs along z: node planes shared by consecutive scenes
+  // learned return mode: the network's BF16 tensor-core weights, its FP32 parameters and the gate
+  // counts, one device block owned by the handle (a copy: the surrogate may be destroyed after)
+  int return_mode = MPM_RETURN_EXACT;
+  void* mlp_block = nullptr;
   // profiling: event pairs around launches while enabled
   bool profiling = false;
   std::vector<cudaEvent_t> ev_pool;
@@ -250,6 +255,10 @@ static int free_device(mpm_handle* h) {
   h->host_exchanged = nullptr;
   if (h->host_ctrl) cudaFreeHost(h->host_ctrl);
   if (h->host_ledger) cudaFreeHost(h->host_ledger);
+  if (h->mlp_block) cudaFree(h->mlp_block);
+  h->mlp_block = nullptr;
+  h->return_mode = MPM_RETURN_EXACT;
+  h->ctx.learned = 0;
   h->pblock = h->gblock = h->snap = h->staging = nullptr;
   h->dptr_table = nullptr;
   h->ledger_partials = nullptr;
@@ -414,6 +423,13 @@ static int alloc_grid(mpm_handle* h) {
   return MPM_OK;
 }
 
+// The learned instances of the particle pass serve scenes without grid conduction and without the
+// history laws (snow, sand, pressure); anything else runs the exact return map.
+static void apply_return_mode(mpm_handle* h) {
+  h->ctx.learned = h->return_mode == MPM_RETURN_LEARNED_GATED && h->mlp_block && !h->ctx.has_aux && !h->ctx.conduct
+                       ? 1 : 0;
+}
+
 static void refresh_flags(mpm_handle* h) {
   bool plastic = false, thermal = false, aux = false;
   for (size_t i = 0; i < h->mats_host.size(); ++i) {
@@ -426,6 +442,7 @@ static void refresh_flags(mpm_handle* h) {
   h->ctx.has_plastic = plastic ? 1 : 0;
   h->ctx.has_aux = aux ? 1 : 0;
   h->ctx.has_thermal = thermal || h->ctx.has_thermal ? 1 : 0;
+  apply_return_mode(h);
 }
 
 // The error for the device status flags st (MPM_OK when none is set).
@@ -501,7 +518,7 @@ static void launch_substep(mpm_handle* h, bool scatter) {
   }
 }
 
-static MaterialDev to_device(const mpm_material& m) {
+MaterialDev mpm::material_to_device(const mpm_material& m) {
   MaterialDev d{};
   d.model = m.model;
   d.mu = static_cast<float>(m.mu);
@@ -721,7 +738,7 @@ int mpm_create(const mpm_domain* domain, int64_t capacity, mpm_handle** out) {
   def.mu = 1;
   def.lambda = 1;
   h->mats_host[0] = def;
-  h->mats_dev[0] = to_device(def);
+  h->mats_dev[0] = mpm::material_to_device(def);
   if (alloc_grid(h) != MPM_OK) return bail(MPM_ERR_OUT_OF_MEMORY);
   mpm::g2p2g_blocks_per_sm(false);  // sets the dynamic shared memory limit of the no-scatter pass
   h->g2p2g_blocks = h->num_sms * mpm::g2p2g_blocks_per_sm(true);
@@ -790,7 +807,7 @@ int mpm_set_material(mpm_handle* h, int32_t index, const mpm_material* material)
   const int rc = validate_material(material, why);
   if (rc != MPM_OK) return fail(h, rc, why);
   h->mats_host[index] = *material;
-  h->mats_dev[index] = to_device(*material);
+  h->mats_dev[index] = mpm::material_to_device(*material);
   h->mats_ext[index] = to_device_ext(*material);
   h->mat_set[index] = 1;
   MPM_CUDA(h, cudaMemcpyAsync(const_cast<MaterialDev*>(h->ctx.mats) + index, &h->mats_dev[index], sizeof(MaterialDev),
@@ -1873,6 +1890,7 @@ int mpm_checkpoint_load(mpm_handle* h, const char* path) {
   h->ctx.has_thermal = hd.has_thermal;
   h->ctx.has_plastic = hd.has_plastic;
   h->ctx.has_aux = hd.has_aux;
+  apply_return_mode(h);
   h->scene.mat_base = hd.mat_base;
   h->scene.p_begin = 0;
   h->scene.p_end = hd.n;
@@ -1901,7 +1919,7 @@ int mpm_return_map_batch(const mpm_material* material, int64_t n, const double* 
   if (rc != MPM_OK) return rc;
   if (n < 0 || (n > 0 && (!F_in || !F_out || !dep || !tau))) return MPM_ERR_INVALID_ARG;
   if (n == 0) return MPM_OK;
-  const MaterialDev md = to_device(*material);
+  const MaterialDev md = mpm::material_to_device(*material);
   double* d = nullptr;
   const size_t bytes = (size_t)n * (9 + 1 + 1 + 9 + 1 + 9) * sizeof(double);
   if (cudaMalloc(&d, bytes) != cudaSuccess) return MPM_ERR_OUT_OF_MEMORY;
@@ -1922,6 +1940,59 @@ int mpm_return_map_batch(const mpm_material* material, int64_t n, const double* 
 }
 
 // ---- grid heat conduction ----
+
+int mpm_set_return_mode(mpm_handle* h, int32_t mode, mpm_surrogate* s, double gate_tol, int32_t newton) {
+  if (!h) return MPM_ERR_INVALID_ARG;
+  if (mode == MPM_RETURN_EXACT) {
+    h->return_mode = MPM_RETURN_EXACT;
+    apply_return_mode(h);
+    drop_graph(h);
+    return MPM_OK;
+  }
+  if (mode != MPM_RETURN_LEARNED_GATED || !s) return fail(h, MPM_ERR_INVALID_ARG, "mode must be exact or learned_gated with a network");
+  if (!mpm::learned_model(surr::surrogate_model(s)))
+    return fail(h, MPM_ERR_UNSUPPORTED, "the learned return mode serves networks trained for Johnson-Cook (models 6, 7)");
+  if (!(gate_tol > 0) || !(gate_tol < 1)) return fail(h, MPM_ERR_INVALID_ARG, "gate_tol must lie in (0, 1)");
+  if (newton < 0 || newton > 8) return fail(h, MPM_ERR_INVALID_ARG, "newton must lie in [0, 8]");
+  if (h->ctx.has_aux || h->ctx.conduct)
+    return fail(h, MPM_ERR_UNSUPPORTED, "the learned return mode serves scenes without conduction and without snow, sand "
+                                        "or pressure materials");
+  const size_t wbytes = surr::weights_bytes();
+  if (!h->mlp_block) {
+    MPM_CUDA(h, cudaMalloc(&h->mlp_block, wbytes + surr::kParams * sizeof(float) + 16));
+  }
+  char* base = static_cast<char*>(h->mlp_block);
+  float* params = reinterpret_cast<float*>(base + wbytes);
+  unsigned* counts = reinterpret_cast<unsigned*>(params + surr::kParams);
+  const int rc = surr::export_weights(s, base, params, h->stream);
+  if (rc != MPM_OK) return fail(h, rc, "copying the network's weights failed");
+  MPM_CUDA(h, cudaMemsetAsync(counts, 0, 16, h->stream));
+  MPM_CUDA(h, cudaStreamSynchronize(h->stream));
+  h->ctx.mlp_w = base;
+  h->ctx.mlp_params = params;
+  h->ctx.gate_counts = counts;
+  h->ctx.gate_tol = static_cast<float>(gate_tol);
+  h->ctx.learned_newton = newton;
+  h->return_mode = MPM_RETURN_LEARNED_GATED;
+  apply_return_mode(h);
+  drop_graph(h);
+  return MPM_OK;
+}
+
+int mpm_gate_counts_read(mpm_handle* h, mpm_gate_counts* out, int32_t reset) {
+  if (!h || !out) return MPM_ERR_INVALID_ARG;
+  *out = mpm_gate_counts{};
+  if (!h->mlp_block) return MPM_OK;
+  unsigned* counts = h->ctx.gate_counts;
+  unsigned hc[2] = {0, 0};
+  join_side(h);
+  MPM_CUDA(h, cudaMemcpyAsync(hc, counts, sizeof hc, cudaMemcpyDeviceToHost, h->stream));
+  if (reset) MPM_CUDA(h, cudaMemsetAsync(counts, 0, sizeof hc, h->stream));
+  MPM_CUDA(h, cudaStreamSynchronize(h->stream));
+  out->learned = hc[0];
+  out->fallback = hc[1];
+  return MPM_OK;
+}
 
 int mpm_set_conduction(mpm_handle* h, int32_t scene, double conductivity, double density, double specific_heat) {
   if (!h) return MPM_ERR_INVALID_ARG;
@@ -1956,6 +2027,7 @@ int mpm_set_conduction(mpm_handle* h, int32_t scene, double conductivity, double
   for (const SceneDev& x : h->scenes) any |= x.cond_G > 0.f;
   h->ctx.conduct = any;
   if (any) h->ctx.has_thermal = 1;  // temperatures are read and written
+  apply_return_mode(h);
   drop_graph(h);
   h->grid_valid = false;  // the next scatter carries the heat channel
   return MPM_OK;

@@ -22,6 +22,7 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include "mpm_b200.h"
 #include "mpm_math.h"
 
 namespace mpm {
@@ -159,7 +160,19 @@ struct Ctx {
   int ws_blocks;        // > 0: the particle passes that scatter run warp-specialised on this many CTAs
   int conduct;          // a scene conducts heat on the grid: heat channel, conduction pass, dT gather
   int uniform_dt;       // every scene takes the smallest scene dt (slabs of one domain)
+  // learned return mode (Johnson-Cook laws): the network's BF16 weights and FP32 parameters (the
+  // handle's own copy), the gate's residual tolerance, the most Newton steps after the prediction,
+  // and the counts of returns the gate accepted and sent to the exact map (2 unsigned)
+  int learned;
+  int learned_newton;
+  float gate_tol;
+  const void* mlp_w;
+  const float* mlp_params;
+  unsigned* gate_counts;
 };
+
+// Johnson-Cook returns the learned mode serves (src/three/metal-plasticity.js:28-34)
+__host__ __device__ inline bool learned_model(int model) { return model == 6 || model == 7; }
 
 #ifdef __CUDACC__
 // Scene of home particle slot i (scenes hold contiguous slot ranges in order).
@@ -172,6 +185,9 @@ __device__ __forceinline__ int find_scene_by_particle(const SceneDev* sc, int ns
   return lo;
 }
 #endif
+
+// Device constants of a material (mpm_api.cu)
+MaterialDev material_to_device(const mpm_material& m);
 
 // Launch wrappers (mpm_kernels.cu)
 void launch_control_init(const Ctx& c, cudaStream_t st);

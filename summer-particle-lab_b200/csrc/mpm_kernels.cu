@@ -19,6 +19,7 @@
 #include <cstdint>
 
 #include "mpm_internal.h"
+#include "surrogate_net.h"
 
 namespace mpm {
 
@@ -1084,6 +1085,200 @@ __device__ __forceinline__ unsigned particle_phase_a(const Ctx& c, const SceneDe
   return key;
 }
 
+// Phase A of the learned return mode (fused or gather-only pass; scenes without conduction and
+// without the history laws). The same particle update as particle_phase_a, with the plastic
+// increment of Johnson-Cook trial states (src/three/metal-plasticity.js:28-34) taken from the
+// network: the warp evaluates it on the tensor cores for its lanes whose trial stress exceeds the
+// initial flow stress, each such lane refines the prediction by Newton steps and keeps it if the
+// consistency residual passes the gate (|g| <= gate_tol, i.e. the stress residual is at most
+// gate_tol x the trial stress), and every other lane runs the exact bisection. Every lane of the
+// warp calls it: lanes past the end of the round (live false) read the round's first particle,
+// take part in the network evaluation and write nothing.
+template <int PASS>
+__device__ __forceinline__ unsigned particle_phase_a_learned(const Ctx& c, const SceneDev& sc, const TileCtx& tc,
+                                                             const MaterialDev& mt_single, bool single,
+                                                             const float4* vwin, bool live, unsigned home, unsigned j,
+                                                             float dt, int nxt, float2* pay, unsigned* meta, int* hist,
+                                                             float& wave_acc, float& grad_acc, unsigned& flags_acc,
+                                                             double& work_acc, bool store_vc, unsigned& n_learned,
+                                                             unsigned& n_exact) {
+  constexpr bool SCATTER = PASS != kPassG2P;
+  static_assert(PASS != kPassP2G, "the learned mode changes only returns");
+  unsigned key = 0xffffffffu;
+  unsigned q[3] = {c.p.qx[home], c.p.qy[home], c.p.qz[home]};
+  float D[9];
+#pragma unroll
+  for (int e = 0; e < 9; ++e) D[e] = c.p.Dc[e][home];
+  const float m = c.p.m[home], V = c.p.V[home];
+  const MaterialDev mt = single ? mt_single : c.mats[c.p.mat[home]];
+  const bool pinned = c.has_pinned && c.p.pinned[home];
+  float ep = c.has_plastic ? c.p.ep[home] : 0.f;
+  float T = c.has_thermal ? c.p.T[home] : 0.f;
+  float aux = 0.f;
+  float v[3], C[9];
+  unsigned flags = 0;
+  const bool moving = !pinned;
+  J2Trial tr{};
+  bool series = false;
+  if (moving) {
+    int b[3];
+    float t[3], w[3][3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      stencil_axis(q[a], tc.dims[a], b[a], t[a]);
+      bspline_weights(t[a], w[a]);
+    }
+    const int l0 = b[0] - tc.tile[0] * kTile, l1 = b[1] - tc.tile[1] * kTile, l2 = b[2] - tc.tile[2] * kTile;
+    const bool in_g = l0 >= 0 && l0 <= kWinG - 3 && l1 >= 0 && l1 <= kWinG - 3 && l2 >= 0 && l2 <= kWinG - 3;
+    if (!in_g) flags |= 0x20u;
+    float acc12[12];
+    if (in_g) {
+      const float4* win = &vwin[(l2 * kWinG + l1) * kWinG + l0];
+      gather27([&](int kz, int ky, int kx) { return win[(kz * kWinG + ky) * kWinG + kx]; }, t, w, acc12);
+    } else {
+      gather_global(c.g.vel + tc.node_base + ((long long)b[2] * tc.gdim[1] + b[1]) * tc.gdim[0] + b[0], tc.gdim[0],
+                    (long long)tc.gdim[0] * tc.gdim[1], t, w, acc12);
+    }
+    const float s4 = 4.f * tc.invH;
+    v[0] = acc12[0]; v[1] = acc12[1]; v[2] = acc12[2];
+#pragma unroll
+    for (int e = 0; e < 9; ++e) C[e] = acc12[3 + e] * s4;
+    float Dn[9];
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+      for (int bc = 0; bc < 3; ++bc)
+        Dn[a * 3 + bc] = D[a * 3 + bc] + dt * (C[a * 3 + bc] + C[a * 3 + 0] * D[0 * 3 + bc] +
+                                               C[a * 3 + 1] * D[1 * 3 + bc] + C[a * 3 + 2] * D[2 * 3 + bc]);
+#pragma unroll
+    for (int e = 0; e < 9; ++e) D[e] = Dn[e];
+    const float s = dt * tc.invH * kFixedOne;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      long long qn = static_cast<long long>(q[a]) + __float2int_rn(fminf(fmaxf(s * v[a], -1.0e9f), 1.0e9f));
+      if (tc.clamp) {
+        qn = qn < (long long)tc.qlo[a] ? (long long)tc.qlo[a] : qn;
+        qn = qn > (long long)tc.qhi[a] ? (long long)tc.qhi[a] : qn;
+      } else {
+        const long long hi = (static_cast<long long>(tc.dims[a]) - 1) << kFracBits;
+        if (qn < 0 || qn > hi) flags |= 0x4u;
+        qn = qn < 0 ? 0 : (qn > hi ? hi : qn);
+      }
+      q[a] = static_cast<unsigned>(qn);
+    }
+    // trial invariants of the J2-type laws on the series path
+    if (mt.model >= 4 && mt.model != 8 && mt.model != 9) {
+      const Sym3 B = cauchy_green_minus_identity(D);
+      const int nt = series_terms_sq(sym_norm2(B));
+      if (nt > 0) {
+        tr = j2_trial_series(mt, B, nt);
+        series = true;
+      }
+    }
+  } else {
+    v[0] = c.p.vx[home]; v[1] = c.p.vy[home]; v[2] = c.p.vz[home];
+#pragma unroll
+    for (int e = 0; e < 9; ++e) C[e] = c.p.Cc[e][home];
+  }
+  // the warp's network evaluation (every lane arrives here)
+  const bool need = live && series && learned_model(mt.model) && tr.q > jc_flow(mt, ep, 0.f, T);
+  float x[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+  if (need) jc_features(mt, tr.q, tr.J, ep, T, dt, x);
+  const float u = surr::warp_predict_first(static_cast<const surr::WeightsBf16*>(c.mlp_w), c.mlp_params, x, need);
+  ConstitutiveOut co;
+  if (moving) {
+    if (series) {
+      float dep = 0.f;
+      if (need) {  // a Johnson-Cook trial stress above the initial flow stress
+        if (jc_refine(mt, tr.q, tr.J, ep, T, dt, u, c.gate_tol, c.learned_newton, dep)) {
+          ++n_learned;
+        } else {
+          dep = jc_bisect(mt, tr.q, tr.J, ep, T, dt);
+          ++n_exact;
+        }
+      } else if (!learned_model(mt.model)) {  // the other J2-type laws (a Johnson-Cook state below yield: 0)
+        dep = plastic_increment(mt, tr.q, tr.J, ep, T, dt);
+      }
+      co = j2_finish(mt, tr, D, dep, V / m);
+    } else {
+      co = constitutive_update_t<false>(mt, D, ep, aux, T, V / m, true, dt);
+    }
+    ep += co.dep;
+    T += co.dT;
+    if (live) {
+      c.p.qx[home] = q[0]; c.p.qy[home] = q[1]; c.p.qz[home] = q[2];
+#pragma unroll
+      for (int e = 0; e < 9; ++e) c.p.Dc[e][home] = D[e];
+      if (PASS != kPassG2P2G || store_vc) {
+        c.p.vx[home] = v[0]; c.p.vy[home] = v[1]; c.p.vz[home] = v[2];
+#pragma unroll
+        for (int e = 0; e < 9; ++e) c.p.Cc[e][home] = C[e];
+      }
+      if (c.has_plastic) c.p.ep[home] = ep;
+      if (c.has_thermal) c.p.T[home] = T;
+      if (co.dep > 0.f && mt.heat_per_work > 0.f) work_acc += static_cast<double>(co.dT) * m / mt.heat_per_work;
+    }
+  } else {
+    float Dc[9];
+#pragma unroll
+    for (int e = 0; e < 9; ++e) Dc[e] = D[e];
+    co = constitutive_update_t<false>(mt, Dc, ep, aux, T, V / m, false, 0.f);
+  }
+  if (!live) return key;
+  if (SCATTER) {
+    int nb[3];
+    float t[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) stencil_axis(q[a], tc.dims[a], nb[a], t[a]);
+    key = tile_key(sc, nb);
+    if (PASS == kPassG2P2G) c.p.key[home] = key;
+    const float mv[3] = {m * v[0], m * v[1], m * v[2]};
+    const float mH = m * tc.H;
+    float mC[9];
+#pragma unroll
+    for (int e = 0; e < 9; ++e) mC[e] = mH * C[e];
+    const float sv = -4.f * V * tc.invH;
+    const float s6[6] = {sv * co.tau.xx, sv * co.tau.yy, sv * co.tau.zz, sv * co.tau.xy, sv * co.tau.xz, sv * co.tau.yz};
+    const int l0 = nb[0] - (tc.tile[0] * kTile - 1), l1 = nb[1] - (tc.tile[1] * kTile - 1),
+              l2 = nb[2] - (tc.tile[2] * kTile - 1);
+    const bool in_w = l0 >= 0 && l0 <= kWinS - 3 && l1 >= 0 && l1 <= kWinS - 3 && l2 >= 0 && l2 <= kWinS - 3;
+    if (in_w && !pinned) {
+      const int bucket = (l2 * 6 + l1) * 6 + l0;
+      const unsigned act = __activemask();
+      const unsigned peers = __match_any_sync(act, bucket);
+      const int leader = __ffs(peers) - 1, lane = threadIdx.x & 31;
+      int rank0 = 0;
+      if (lane == leader) rank0 = atomicAdd(&hist[bucket], __popc(peers));
+      const int rank = __shfl_sync(peers, rank0, leader) + __popc(peers & ((1u << lane) - 1u));
+      meta[j] = static_cast<unsigned>(bucket) | (static_cast<unsigned>(rank) << 8);
+      float2* P = pay + pay_slot(j);
+      P[0 * kPayStride] = make_float2(t[0], t[1]);
+      P[1 * kPayStride] = make_float2(t[2], m);
+      P[2 * kPayStride] = make_float2(mv[0], mv[1]);
+      P[3 * kPayStride] = make_float2(mv[2], 0.f);
+      P[4 * kPayStride] = make_float2(mC[2], mC[5]);
+      P[5 * kPayStride] = make_float2(mC[8], s6[4]);
+      P[6 * kPayStride] = make_float2(s6[5], s6[2]);
+      P[7 * kPayStride] = make_float2(mC[1], mC[4]);
+      P[8 * kPayStride] = make_float2(mC[7], s6[3]);
+      P[9 * kPayStride] = make_float2(mC[0], mC[3]);
+      P[10 * kPayStride] = make_float2(mC[6], s6[0]);
+      P[11 * kPayStride] = make_float2(s6[1], 0.f);
+    } else {
+      meta[j] = kMetaInvalid;
+      if (!in_w) flags |= 0x10u;
+      scatter_global(c, sc, tc, nxt, nb, t, m, mv, mC, s6, pinned, 0.f);
+    }
+  }
+  float wave, grad;
+  cfl_terms<false>(mt, D, v, C, m, V, co.Jm1, aux, wave, grad);
+  flags |= state_flags(v, D, co.tau, co.Jm1);
+  flags_acc |= flags;
+  wave_acc = fmaxf(wave_acc, wave);
+  grad_acc = fmaxf(grad_acc, grad);
+  return key;
+}
+
 // L2 prefetch of the particle state a claimed tile will read. Between physical re-sorts a tile's
 // particles keep the contiguous home range the last re-sort gave them (apart from the few that
 // changed tiles since), and the tile's perm lists them in about that order; one perm entry from the
@@ -1115,8 +1310,9 @@ __device__ __forceinline__ void prefetch_tile_state(const Ctx& c, uint4 it) {
   if (c.has_pinned) pf(c.p.pinned, 1);
 }
 
-template <int PASS, bool HEAT, bool AUX>
+template <int PASS, bool HEAT, bool AUX, bool LEARNED = false>
 __global__ void __launch_bounds__(kBlock, 2) k_particles(const __grid_constant__ Ctx c) {
+  static_assert(!LEARNED || (!HEAT && !AUX && PASS != kPassP2G), "learned instances: no conduction, no history laws");
   extern __shared__ __align__(128) unsigned char smem_raw[];
   PartSmem& sm = *reinterpret_cast<PartSmem*>(smem_raw);
   constexpr bool SCATTER = PASS != kPassG2P;
@@ -1156,6 +1352,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_particles(const __grid_constant__
   }
   unsigned phase0 = 0, phase1 = 0;
   double work_acc = 0.0;
+  unsigned n_learned = 0, n_exact = 0;  // learned mode: returns the gate accepted / sent to the exact map
   int cb = 0;
   int mt_row = -1;  // material row held in sm.mt
   // perm entries of the next tile's first round (j = tid, tid + kBlock), loaded one tile ahead
@@ -1247,7 +1444,18 @@ __global__ void __launch_bounds__(kBlock, 2) k_particles(const __grid_constant__
       for (unsigned jj = 0; jj < nround; jj += kBlock) {
         const unsigned j = jj + threadIdx.x;
         unsigned key = 0xffffffffu;
-        if (j < nround) {
+        if constexpr (LEARNED) {
+          // every lane of a warp with a live particle takes part in its network evaluation (warps
+          // past the end of the round skip as a whole)
+          if (jj + (threadIdx.x & ~31u) >= nround) continue;
+          const bool live = j < nround;
+          const unsigned home = !live ? c.p.perm[it.y + r0]
+                                      : (r0 == 0 && pf_ok && jj < kPf * kBlock) ? pf[jj / kBlock]
+                                                                                 : c.p.perm[it.y + r0 + j];
+          key = particle_phase_a_learned<PASS>(c, sc, tc, sm.mt, single, sm.vwin[cb], live, home, j, dt, nxt, sm.pay,
+                                               sm.meta, sm.hist, wave_acc, grad_acc, flags_acc, work_acc, store_vc,
+                                               n_learned, n_exact);
+        } else if (j < nround) {
           const unsigned home = (r0 == 0 && pf_ok && jj < kPf * kBlock) ? pf[jj / kBlock] : c.p.perm[it.y + r0 + j];
           key = particle_phase_a<PASS, HEAT, AUX>(c, sc, tc, sm.mt, single, sm.vwin[cb], home, j, dt, nxt, sm.pay, sm.meta,
                                        sm.hist, wave_acc, grad_acc, flags_acc, work_acc, store_vc);
@@ -1290,6 +1498,13 @@ __global__ void __launch_bounds__(kBlock, 2) k_particles(const __grid_constant__
     __syncthreads();
     if (SCATTER) flush_window(c, sc, sm, nxt, tc.tile);
     cb ^= 1;
+  }
+  if (LEARNED) {  // gate counts: one atomic per warp
+    const unsigned nl = __reduce_add_sync(0xffffffffu, n_learned), ne = __reduce_add_sync(0xffffffffu, n_exact);
+    if ((threadIdx.x & 31) == 0 && (nl | ne)) {
+      atomicAdd(&c.gate_counts[0], nl);
+      atomicAdd(&c.gate_counts[1], ne);
+    }
   }
   // heat from plastic work: one FP64 atomic per CTA
   if (GATHER) {
@@ -1616,6 +1831,12 @@ __global__ void __launch_bounds__(kWsThreads, 1) k_particles_ws(const __grid_con
 
 template <int PASS, bool HEAT, bool AUX>
 static void launch_pass_t(const Ctx& c, cudaStream_t st, int grid_blocks) {
+  if constexpr (PASS != kPassP2G && !HEAT && !AUX) {
+    if (c.learned) {
+      k_particles<PASS, false, false, true><<<grid_blocks, kBlock, sizeof(PartSmem), st>>>(c);
+      return;
+    }
+  }
   if (PASS != kPassG2P && c.ws_blocks > 0) {
     k_particles_ws<PASS == kPassG2P ? kPassG2P2G : PASS, HEAT, AUX><<<c.ws_blocks, kWsThreads, sizeof(WsSmem), st>>>(c);
     return;
@@ -1652,6 +1873,8 @@ static int blocks_per_sm() {
   cudaFuncSetAttribute(k_particles<PASS, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
   cudaFuncSetAttribute(k_particles<PASS, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
   cudaFuncSetAttribute(k_particles<PASS, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if constexpr (PASS != kPassP2G)
+    cudaFuncSetAttribute(k_particles<PASS, false, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
   int n = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_particles<PASS, false, false>, kBlock, sizeof(PartSmem));
   return n > 0 ? n : 1;

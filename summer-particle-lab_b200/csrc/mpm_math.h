@@ -257,6 +257,21 @@ MPM_HD float creep_log_rate(const MaterialDev& mt, float q, float T) {
   return mt.cr_log_rate + act + mt.cr_n * logf(q * mt.cr_inv_stress);
 }
 
+// The Johnson-Cook consistency condition q - 3 mu / J dep = flow(ep + dep, dep / dt, T) for a trial
+// stress above the initial flow stress: 24 bisections of [0, q J / (3 mu)], the reference's bracket
+// and count (src/three/metal-plasticity.js:28-34).
+MPM_HD float jc_bisect(const MaterialDev& mt, float q, float J, float ep, float T, float dt) {
+  const float slope = 3.f * mt.mu / J;
+  float lo = 0.f, hi = q / slope;
+  const float inv_dt = 1.f / fmaxf(dt, 1e-12f);
+  for (int it = 0; it < 24; ++it) {
+    const float mid = 0.5f * (lo + hi);
+    if (q - slope * mid > jc_flow(mt, ep + mid, mid * inv_dt, T)) lo = mid;
+    else hi = mid;
+  }
+  return 0.5f * (lo + hi);
+}
+
 // Plastic strain increment of the J2-type returns for the trial von Mises stress q
 // (src/three/metal-plasticity.js:20-27, src/three/thermal-plasticity.js:22-37): closed form for
 // models 4, 5 and 10, 24 bisections of the consistency condition for Johnson-Cook (6, 7), 32
@@ -265,14 +280,7 @@ MPM_HD float plastic_increment(const MaterialDev& mt, float q, float J, float ep
   const float slope = 3.f * mt.mu / J;
   if (mt.model == 6 || mt.model == 7) {
     if (!(q > jc_flow(mt, ep, 0.f, T))) return 0.f;
-    float lo = 0.f, hi = q / slope;
-    const float inv_dt = 1.f / fmaxf(dt, 1e-12f);
-    for (int it = 0; it < 24; ++it) {
-      const float mid = 0.5f * (lo + hi);
-      if (q - slope * mid > jc_flow(mt, ep + mid, mid * inv_dt, T)) lo = mid;
-      else hi = mid;
-    }
-    return 0.5f * (lo + hi);
+    return jc_bisect(mt, q, J, ep, T, dt);
   }
   if (mt.model == 11) {
     if (!(dt > 0.f && mt.cr_on && q > 1e-20f)) return 0.f;
@@ -293,6 +301,107 @@ MPM_HD float plastic_increment(const MaterialDev& mt, float q, float J, float ep
   if (!(q > yield)) return 0.f;
   const float hard = mt.model == 4 ? 0.f : mt.hardening * soft;
   return (q - yield) / (slope + hard);
+}
+
+// ---- Learned Johnson-Cook return (models 6 and 7) ------------------------------------------
+// The consistency condition of src/three/metal-plasticity.js:28-34 in dimensionless form: with
+// slope = 3 mu / J, the bracket s = q / slope and dep = u s (u in [0, 1]),
+//   g(u) = 1 - u - flow(ep + u s, u s / dt, T) / q,
+// decreasing in u, zero at the return. The reference bisects it 24 times. The learned form takes a
+// network's guess of u, refines it by Newton steps on g and accepts the result only if |g| <= tol
+// (the stress residual |q - slope dep - flow| is then at most tol q); otherwise the caller runs the
+// exact bisection.
+
+// Flow stress and its derivative with respect to dep at dep = d (d > 0).
+MPM_HD float jc_flow_d(const MaterialDev& mt, float ep, float d, float inv_dt, float soft, float& dflow) {
+  const float e = fmaxf(ep + d, 1e-30f);
+  const float pw = powf(e, mt.jc_n);
+  const float hard = mt.yield_stress + mt.hardening * pw;
+  const float r = d * inv_dt * mt.jc_inv_rate0;
+  const bool rate_on = r > 1.f;
+  const float rf = 1.f + (rate_on ? mt.jc_C * logf(r) : 0.f);
+  dflow = soft * (mt.hardening * mt.jc_n * pw / e * rf + (rate_on ? hard * mt.jc_C / d : 0.f));
+  return soft * hard * rf;
+}
+
+// Thermal softening factor of model 6 (1 for model 7).
+MPM_HD float jc_soft(const MaterialDev& mt, float T) {
+  if (mt.model != 6) return 1.f;
+  const float th = fminf(1.f, fmaxf(0.f, (T - mt.T_ref) * mt.jc_inv_T_span));
+  return 1.f - powf(th, mt.jc_m);
+}
+
+// The eight network inputs of a plastic Johnson-Cook trial state (q > flow(ep, 0, T)); all are
+// dimensionless, so one network serves every material with the same B / A, n and C:
+//   a = A soft / q, the hardening at ep and at ep + s relative to q, C ln max(1, s / (dt rate0)),
+//   log10 of the bracket s, ep, 1 - a - h0 and the network's bias input.
+MPM_NOINLINE void jc_features(const MaterialDev& mt, float q, float J, float ep, float T, float dt, float x[8]) {
+  const float slope = 3.f * mt.mu / J;
+  const float s = q / slope;
+  const float soft = jc_soft(mt, T);
+  const float iq = 1.f / q;
+  const float a = mt.yield_stress * soft * iq;
+  const float h0 = mt.hardening * soft * powf(fmaxf(ep, 0.f), mt.jc_n) * iq;
+  const float h1 = mt.hardening * soft * powf(fmaxf(ep, 0.f) + s, mt.jc_n) * iq;
+  const float L = logf(fmaxf(1.f, s / fmaxf(dt, 1e-30f) * mt.jc_inv_rate0));
+  x[0] = a;
+  x[1] = h0;
+  x[2] = h1 - h0;
+  x[3] = mt.jc_C * L;
+  x[4] = 0.25f * log10f(fmaxf(s, 1e-12f)) + 1.5f;
+  x[5] = ep;
+  x[6] = 1.f - a - h0;
+  x[7] = 1.f;
+}
+
+// Newton refinement of a predicted root u and the gate. The rate factor max(1, rate / rate0) has a
+// kink at u_k = dt rate0 / s, where the slope of g jumps; g is smooth on either side, so when the
+// kink lies inside the bracket the refinement first finds the side of the root (the sign of g(u_k)).
+// Left of the kink Newton runs on u; right of it on w = ln(u / u_k), in which the logarithmic rate
+// term is linear (the curvature that slows Newton on u just past the kink). At most `newton` steps,
+// stopping as soon as |g| <= tol; a step that would leave the side is replaced by the midpoint toward
+// its end. Returns true with dep = u s when the final |g(u)| <= tol.
+MPM_NOINLINE bool jc_refine(const MaterialDev& mt, float q, float J, float ep, float T, float dt, float u_pred, float tol,
+                            int newton, float& dep) {
+  const float slope = 3.f * mt.mu / J;
+  const float s = q / slope;
+  const float soft = jc_soft(mt, T);
+  const float inv_dt = 1.f / fmaxf(dt, 1e-12f);
+  const float iq = 1.f / q;
+  float df;
+  const float uk = mt.jc_C > 0.f ? 1.f / (s * inv_dt * mt.jc_inv_rate0) : 2.f;
+  bool right = false;  // the root lies past the kink (the rate term is on)
+  if (uk > 0.f && uk < 1.f) right = 1.f - uk - jc_flow_d(mt, ep, uk * s, inv_dt, soft, df) * iq > 0.f;
+  float u, g;
+  if (right) {
+    const float whi = -logf(uk);
+    float w = fminf(whi, fmaxf(0.f, logf(fmaxf(u_pred, uk) / uk)));
+    u = uk * expf(w);
+    g = 1.f - u - jc_flow_d(mt, ep, u * s, inv_dt, soft, df) * iq;
+    for (int k = 0; k < newton && !(fabsf(g) <= tol); ++k) {
+      const float dgw = (-1.f - df * s * iq) * u;  // dg / dw
+      float wn = w - g / dgw;
+      if (!(wn > 0.f)) wn = 0.5f * w;
+      if (!(wn < whi)) wn = 0.5f * (w + whi);
+      w = wn;
+      u = uk * expf(w);
+      g = 1.f - u - jc_flow_d(mt, ep, u * s, inv_dt, soft, df) * iq;
+    }
+  } else {
+    const float hi = fminf(1.f, uk);
+    u = fminf(hi, fmaxf(0.f, u_pred));
+    g = 1.f - u - jc_flow_d(mt, ep, u * s, inv_dt, soft, df) * iq;
+    for (int k = 0; k < newton && !(fabsf(g) <= tol); ++k) {
+      const float dg = -1.f - df * s * iq;
+      float un = u - g / dg;
+      if (!(un > 0.f)) un = 0.5f * u;
+      if (!(un < hi)) un = 0.5f * (u + hi);
+      u = un;
+      g = 1.f - u - jc_flow_d(mt, ep, u * s, inv_dt, soft, df) * iq;
+    }
+  }
+  dep = u * s;
+  return fabsf(g) <= tol;
 }
 
 struct ConstitutiveOut {
@@ -539,6 +648,67 @@ MPM_NOINLINE ConstitutiveOut constitutive_pressure(const MaterialDev& mt, const 
   return out;
 }
 
+// Trial invariants of the J2-type returns on the small-strain series path (|B - I| <= 0.15):
+// L = log(I + B) / 2 = log V_l, its deviator, |dev L|, J - 1 and the trial von Mises stress q.
+struct J2Trial {
+  Sym3 dv;
+  float len, trL, tr3, em1, J, q;
+};
+
+MPM_HD J2Trial j2_trial_series(const MaterialDev& mt, const Sym3& B, int nt) {
+  J2Trial t;
+  Sym3 L = matrix_series<0>(B, nt);  // log(I + B) = 2 log V_l
+  L.xx *= 0.5f; L.yy *= 0.5f; L.zz *= 0.5f; L.xy *= 0.5f; L.xz *= 0.5f; L.yz *= 0.5f;
+  t.trL = L.xx + L.yy + L.zz;
+  t.tr3 = t.trL * (1.f / 3.f);
+  t.dv = L;
+  t.dv.xx -= t.tr3; t.dv.yy -= t.tr3; t.dv.zz -= t.tr3;
+  t.len = sym_norm(t.dv);
+  t.em1 = expm1f(t.trL);  // J - 1
+  t.J = fmaxf(1e-6f, 1.f + t.em1);
+  t.q = 2.449489742783178f * mt.mu * t.len / t.J;
+  return t;
+}
+
+// The return for a plastic strain increment dep (0: elastic) and the Hencky stress of the
+// returned state: F' = exp((scale - 1) dev L) F with scale = 1 - sqrt(3/2) dep / |dev L|
+// (src/three/metal-plasticity.js:24-26, src/three/constitutive.js:77-86), plastic-work heating.
+MPM_HD ConstitutiveOut j2_finish(const MaterialDev& mt, const J2Trial& t, float D[9], float dep, float inv_rho0) {
+  ConstitutiveOut out;
+  out.dT = 0.f;
+  const Sym3& dv = t.dv;
+  float scale = 1.f;
+  if (dep > 0.f) {
+    scale = fmaxf(0.f, 1.f - 1.224744871391589f * dep / fmaxf(t.len, 1e-20f));
+    const float g = scale - 1.f;
+    const Sym3 M{g * dv.xx, g * dv.yy, g * dv.zz, g * dv.xy, g * dv.xz, g * dv.yz};
+    const int nm = series_terms(sym_norm(M));
+    const Sym3 E = matrix_series<2>(M, nm > 0 ? nm : 10);  // exp(M) - I
+    float Dn[9];
+#pragma unroll
+    for (int b = 0; b < 3; ++b) {
+      Dn[0 * 3 + b] = E.xx * D[0 * 3 + b] + E.xy * D[1 * 3 + b] + E.xz * D[2 * 3 + b];
+      Dn[1 * 3 + b] = E.xy * D[0 * 3 + b] + E.yy * D[1 * 3 + b] + E.yz * D[2 * 3 + b];
+      Dn[2 * 3 + b] = E.xz * D[0 * 3 + b] + E.yz * D[1 * 3 + b] + E.zz * D[2 * 3 + b];
+    }
+    D[0] += Dn[0] + E.xx; D[1] += Dn[1] + E.xy; D[2] += Dn[2] + E.xz;
+    D[3] += Dn[3] + E.xy; D[4] += Dn[4] + E.yy; D[5] += Dn[5] + E.yz;
+    D[6] += Dn[6] + E.xz; D[7] += Dn[7] + E.yz; D[8] += Dn[8] + E.zz;
+    out.dT = mt.heat_per_work * 2.449489742783178f * mt.mu * scale * t.len * dep * inv_rho0;
+  }
+  const float m2s = 2.f * mt.mu * scale;
+  const float iso = 2.f * mt.mu * t.tr3 + mt.lam * t.trL;
+  out.tau.xx = m2s * dv.xx + iso;
+  out.tau.yy = m2s * dv.yy + iso;
+  out.tau.zz = m2s * dv.zz + iso;
+  out.tau.xy = m2s * dv.xy;
+  out.tau.xz = m2s * dv.xz;
+  out.tau.yz = m2s * dv.yz;
+  out.dep = dep;
+  out.Jm1 = t.em1;
+  return out;
+}
+
 // Constitutive update of one particle after the F update, in place on D (= F - I):
 // models 4-7, 10 and 11 run the J2-type radial return (src/three/metal-plasticity.js:20-38,
 // src/three/thermal-plasticity.js:22-40; dt is the substep, used by the rate-dependent laws 6,
@@ -593,47 +763,9 @@ MPM_HD ConstitutiveOut constitutive_update_t(const MaterialDev& mt, float D[9], 
       out.Jm1 = Jm1;
       return out;
     }
-    Sym3 L = matrix_series<0>(B, nt);  // log(I + B) = 2 log V_l
-    L.xx *= 0.5f; L.yy *= 0.5f; L.zz *= 0.5f; L.xy *= 0.5f; L.xz *= 0.5f; L.yz *= 0.5f;
-    const float trL = L.xx + L.yy + L.zz;
-    const float tr3 = trL * (1.f / 3.f);
-    Sym3 dv = L;
-    dv.xx -= tr3; dv.yy -= tr3; dv.zz -= tr3;
-    const float len = sym_norm(dv);
-    const float em1 = expm1f(trL);  // J - 1
-    const float J = fmaxf(1e-6f, 1.f + em1);
-    const float q = 2.449489742783178f * mt.mu * len / J;
-    const float dep = do_return ? plastic_increment(mt, q, J, ep, T, dt) : 0.f;
-    float scale = 1.f;
-    if (dep > 0.f) {
-      scale = fmaxf(0.f, 1.f - 1.224744871391589f * dep / fmaxf(len, 1e-20f));
-      const float g = scale - 1.f;
-      const Sym3 M{g * dv.xx, g * dv.yy, g * dv.zz, g * dv.xy, g * dv.xz, g * dv.yz};
-      const int nm = series_terms(sym_norm(M));
-      const Sym3 E = matrix_series<2>(M, nm > 0 ? nm : 10);  // exp(M) - I
-      float Dn[9];
-#pragma unroll
-      for (int b = 0; b < 3; ++b) {
-        Dn[0 * 3 + b] = E.xx * D[0 * 3 + b] + E.xy * D[1 * 3 + b] + E.xz * D[2 * 3 + b];
-        Dn[1 * 3 + b] = E.xy * D[0 * 3 + b] + E.yy * D[1 * 3 + b] + E.yz * D[2 * 3 + b];
-        Dn[2 * 3 + b] = E.xz * D[0 * 3 + b] + E.yz * D[1 * 3 + b] + E.zz * D[2 * 3 + b];
-      }
-      D[0] += Dn[0] + E.xx; D[1] += Dn[1] + E.xy; D[2] += Dn[2] + E.xz;
-      D[3] += Dn[3] + E.xy; D[4] += Dn[4] + E.yy; D[5] += Dn[5] + E.yz;
-      D[6] += Dn[6] + E.xz; D[7] += Dn[7] + E.yz; D[8] += Dn[8] + E.zz;
-      out.dT = mt.heat_per_work * 2.449489742783178f * mt.mu * scale * len * dep * inv_rho0;
-    }
-    const float m2s = 2.f * mt.mu * scale;
-    const float iso = 2.f * mt.mu * tr3 + mt.lam * trL;
-    out.tau.xx = m2s * dv.xx + iso;
-    out.tau.yy = m2s * dv.yy + iso;
-    out.tau.zz = m2s * dv.zz + iso;
-    out.tau.xy = m2s * dv.xy;
-    out.tau.xz = m2s * dv.xz;
-    out.tau.yz = m2s * dv.yz;
-    out.dep = dep;
-    out.Jm1 = em1;
-    return out;
+    const J2Trial tr = j2_trial_series(mt, B, nt);
+    const float dep = do_return ? plastic_increment(mt, tr.q, tr.J, ep, T, dt) : 0.f;
+    return j2_finish(mt, tr, D, dep, inv_rho0);
   }
   return constitutive_eigen(mt, B, D, ep, T, inv_rho0, do_return, dt);
 }

@@ -13,13 +13,18 @@
 // carry errors of several per cent of sigma_y. Only plastic states train the network (column 7
 // of a target row is its sample weight: 1 plastic, 0 elastic); elastic states never reach it.
 //
-// Arithmetic. Weights and activations enter the tensor cores as BF16 (mma.sync m16n8k16,
-// FP32 accumulation); the optimizer keeps FP32 master weights. One warp owns 16 samples: the
-// accumulator fragment of one layer is the A fragment of the next (two 8-column tiles make one
-// 16-wide K step), so activations never leave registers in the forward pass. Weight gradients
-// are GEMMs over the sample axis: each warp stages its activations and gradients transposed in
-// shared memory (BF16) and runs them through the same mma shape; warps sum into FP32 shared
-// accumulators and each CTA adds its sums to the global gradient once.
+// Arithmetic. Weights and activations enter the tensor cores as BF16 with FP32 accumulation; the
+// optimizer keeps FP32 master weights. Training (k_train_tc) and the gated map over particle arrays
+// (k_gated) run on the 5th-generation tensor cores: tcgen05.mma with operands in shared memory and
+// accumulators in tensor memory, 128 samples per tile, the weight gradients as GEMMs over the
+// sample axis accumulated in tensor memory. The per-particle inference inside other kernels
+// (k_gated_jc, the fused particle pass in learned return mode) runs warp-wide mma.sync tiles of 16
+// rows, where the accumulator fragment of one layer is the A fragment of the next, so activations
+// never leave registers.
+//
+// Johnson-Cook (models 6, 7). The network maps the dimensionless trial state to the root of the
+// consistency condition the reference bisects (see k_samples_jc); mpm::jc_refine polishes the
+// prediction by Newton steps and gates it on the consistency residual.
 //
 // Gate. A particle whose trial von Mises stress is at or below yield takes the exact elastic
 // branch (no return exists). Otherwise the prediction is accepted only if (a) dep >= 0,
@@ -37,174 +42,11 @@
 #include <vector>
 
 #include "mpm_b200.h"
+#include "mpm_internal.h"
 #include "mpm_math.h"
+#include "surrogate_net.h"
 
 namespace surr {
-
-constexpr int kIn = 8, kHid = 64, kOut = 7;
-// FP32 parameter vector (out-major weights: W[o][i])
-constexpr int kW1 = 0;                   // [64][16] (inputs 8..15 zero)
-constexpr int kB1 = kW1 + kHid * 16;     // [64]
-constexpr int kW2 = kB1 + kHid;          // [64][64]
-constexpr int kB2 = kW2 + kHid * kHid;   // [64]
-constexpr int kW3 = kB2 + kHid;          // [8][64] (row 7 zero)
-constexpr int kB3 = kW3 + 8 * kHid;      // [8] (entry 7 zero)
-constexpr int kParams = kB3 + 8;         // 5768
-static_assert(kParams == MPM_SURROGATE_PARAMS, "parameter count");
-
-// BF16 copies for the tensor cores
-struct __align__(16) WeightsBf16 {
-  __nv_bfloat16 w1f[kHid * 16];   // forward B operand, out-major [o][i]
-  __nv_bfloat16 w2f[kHid * kHid];
-  __nv_bfloat16 w3f[8 * kHid];
-  __nv_bfloat16 w2b[kHid * kHid]; // backward B operand, in-major [i][o]
-  __nv_bfloat16 w3b[kHid * 16];   // in-major [i][o], o padded to 16
-};
-
-struct Scales {
-  float T_lo, T_span, ep;
-};
-
-__device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
-  __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
-  return *reinterpret_cast<uint32_t*>(&v);
-}
-
-__device__ __forceinline__ uint32_t ld32(const __nv_bfloat16* p) { return *reinterpret_cast<const uint32_t*>(p); }
-
-__device__ __forceinline__ void mma(float c[4], const uint32_t a[4], uint32_t b0, uint32_t b1) {
-  asm volatile(
-      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
-      "{%0,%1,%2,%3};\n"
-      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
-      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
-}
-
-// A fragment of K columns [16 kc, 16 kc + 16) from two accumulator tiles (2 kc, 2 kc + 1).
-__device__ __forceinline__ void chain(const float t[][4], int kc, uint32_t a[4]) {
-  a[0] = pack_bf16(t[2 * kc][0], t[2 * kc][1]);
-  a[1] = pack_bf16(t[2 * kc][2], t[2 * kc][3]);
-  a[2] = pack_bf16(t[2 * kc + 1][0], t[2 * kc + 1][1]);
-  a[3] = pack_bf16(t[2 * kc + 1][2], t[2 * kc + 1][3]);
-}
-
-// Forward pass of one warp's 16 samples. xa: A fragment of the inputs (K = 16, 8 real).
-// h1, h2: post-ReLU activations (accumulator layout, 8 tiles of 8 columns); y: outputs (1 tile).
-__device__ __forceinline__ void forward(const WeightsBf16& w, const float* bias, const uint32_t xa[4], float h1[8][4],
-                                        float h2[8][4], float y[4], int g, int tig) {
-#pragma unroll
-  for (int nt = 0; nt < 8; ++nt) {
-    const float b0 = bias[kB1 + nt * 8 + tig * 2], b1 = bias[kB1 + nt * 8 + tig * 2 + 1];
-    h1[nt][0] = b0; h1[nt][1] = b1; h1[nt][2] = b0; h1[nt][3] = b1;
-    const __nv_bfloat16* wr = w.w1f + (nt * 8 + g) * 16 + tig * 2;
-    mma(h1[nt], xa, ld32(wr), ld32(wr + 8));
-#pragma unroll
-    for (int j = 0; j < 4; ++j) h1[nt][j] = fmaxf(h1[nt][j], 0.f);
-  }
-#pragma unroll
-  for (int nt = 0; nt < 8; ++nt) {
-    const float b0 = bias[kB2 + nt * 8 + tig * 2], b1 = bias[kB2 + nt * 8 + tig * 2 + 1];
-    h2[nt][0] = b0; h2[nt][1] = b1; h2[nt][2] = b0; h2[nt][3] = b1;
-  }
-#pragma unroll
-  for (int kc = 0; kc < 4; ++kc) {
-    uint32_t a[4];
-    chain(h1, kc, a);
-#pragma unroll
-    for (int nt = 0; nt < 8; ++nt) {
-      const __nv_bfloat16* wr = w.w2f + (nt * 8 + g) * kHid + kc * 16 + tig * 2;
-      mma(h2[nt], a, ld32(wr), ld32(wr + 8));
-    }
-  }
-#pragma unroll
-  for (int nt = 0; nt < 8; ++nt)
-#pragma unroll
-    for (int j = 0; j < 4; ++j) h2[nt][j] = fmaxf(h2[nt][j], 0.f);
-  {
-    const float b0 = bias[kB3 + tig * 2], b1 = bias[kB3 + tig * 2 + 1];
-    y[0] = b0; y[1] = b1; y[2] = b0; y[3] = b1;
-  }
-#pragma unroll
-  for (int kc = 0; kc < 4; ++kc) {
-    uint32_t a[4];
-    chain(h2, kc, a);
-    const __nv_bfloat16* wr = w.w3f + g * kHid + kc * 16 + tig * 2;
-    mma(y, a, ld32(wr), ld32(wr + 8));
-  }
-}
-
-// Per-warp shared staging for the weight-gradient GEMMs: transposed BF16 tiles [feature][sample].
-struct WarpStage {
-  __nv_bfloat16 xT[16][16];    // inputs (8 real rows)
-  __nv_bfloat16 h1T[kHid][16];
-  __nv_bfloat16 h2T[kHid][16];
-  __nv_bfloat16 d1T[kHid][16]; // dL/d(pre-activation 1)
-  __nv_bfloat16 d2T[kHid][16]; // dL/d(pre-activation 2)
-  __nv_bfloat16 dyT[16][16];   // dL/dy (7 real rows)
-};
-
-constexpr int kTrainThreads = 256;
-constexpr int kTrainWarps = kTrainThreads / 32;
-
-struct TrainSmem {
-  WeightsBf16 w;
-  float bias[kParams];   // only the bias entries are read
-  float grad[kParams];   // CTA gradient sums
-  WarpStage stage[kTrainWarps];
-  float loss[kTrainWarps];
-};
-
-// Stores an accumulator tile (16 samples x 8 columns starting at col0) transposed into T[col][s].
-__device__ __forceinline__ void store_t(__nv_bfloat16 (*T)[16], const float c[4], int col0, int g, int tig) {
-  T[col0 + tig * 2][g] = __float2bfloat16_rn(c[0]);
-  T[col0 + tig * 2 + 1][g] = __float2bfloat16_rn(c[1]);
-  T[col0 + tig * 2][g + 8] = __float2bfloat16_rn(c[2]);
-  T[col0 + tig * 2 + 1][g + 8] = __float2bfloat16_rn(c[3]);
-}
-
-// grad[base + o * ld + i] += sum_s A[o][s] B[i][s] for o in [0, M), i in [0, N) (M, N multiples
-// of 16 / 8; K = the warp's 16 samples), adding into the CTA's shared accumulators.
-template <int M, int N>
-__device__ __forceinline__ void wgrad(const __nv_bfloat16 (*A)[16], const __nv_bfloat16 (*B)[16], float* grad, int base,
-                                      int ld, int mvalid, int g, int tig) {
-#pragma unroll
-  for (int mt = 0; mt < M / 16; ++mt) {
-    uint32_t a[4];
-    a[0] = ld32(&A[mt * 16 + g][tig * 2]);
-    a[1] = ld32(&A[mt * 16 + g + 8][tig * 2]);
-    a[2] = ld32(&A[mt * 16 + g][tig * 2 + 8]);
-    a[3] = ld32(&A[mt * 16 + g + 8][tig * 2 + 8]);
-#pragma unroll
-    for (int nt = 0; nt < N / 8; ++nt) {
-      float c[4] = {0.f, 0.f, 0.f, 0.f};
-      mma(c, a, ld32(&B[nt * 8 + g][tig * 2]), ld32(&B[nt * 8 + g][tig * 2 + 8]));
-      const int o0 = mt * 16 + g, o1 = o0 + 8, i0 = nt * 8 + tig * 2;
-      if (o0 < mvalid) {
-        atomicAdd(&grad[base + o0 * ld + i0], c[0]);
-        atomicAdd(&grad[base + o0 * ld + i0 + 1], c[1]);
-      }
-      if (o1 < mvalid) {
-        atomicAdd(&grad[base + o1 * ld + i0], c[2]);
-        atomicAdd(&grad[base + o1 * ld + i0 + 1], c[3]);
-      }
-    }
-  }
-}
-
-// Column sums of an accumulator tile over the warp's 16 samples, added to grad[base + col].
-__device__ __forceinline__ void bias_grad(const float c[4], float* grad, int base, int col0, int g, int tig,
-                                          int valid) {
-  float s0 = c[0] + c[2], s1 = c[1] + c[3];
-#pragma unroll
-  for (int o = 4; o < 32; o <<= 1) {
-    s0 += __shfl_xor_sync(0xffffffffu, s0, o);
-    s1 += __shfl_xor_sync(0xffffffffu, s1, o);
-  }
-  if (g == 0) {
-    if (col0 + tig * 2 < valid) atomicAdd(&grad[base + col0 + tig * 2], s0);
-    if (col0 + tig * 2 + 1 < valid) atomicAdd(&grad[base + col0 + tig * 2 + 1], s1);
-  }
-}
 
 __device__ __forceinline__ void load_weights(WeightsBf16& dst, const WeightsBf16* src) {
   const uint4* s = reinterpret_cast<const uint4*>(src);
@@ -212,127 +54,361 @@ __device__ __forceinline__ void load_weights(WeightsBf16& dst, const WeightsBf16
   for (int i = threadIdx.x; i < (int)(sizeof(WeightsBf16) / 16); i += blockDim.x) d[i] = s[i];
 }
 
-// Loss = sum over samples and outputs of wout[o] (y - t)^2 / n_total; gradient into grad_out.
-// Samples are rows of X (n x 8) and Y (n x 8, column 7 unused); sample r of this call is row
-// (first + r * stride) mod n_data, a strided walk that visits every row once per epoch when
-// stride and n_data are coprime.
-__global__ void __launch_bounds__(kTrainThreads) k_train(const WeightsBf16* wg, const float* params, const float* X,
-                                                         const float* Y, long long n_data, long long first,
-                                                         long long stride, int batch, float inv_batch, const float* wout,
-                                                         float* grad_out, float* loss_out) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  TrainSmem& sm = *reinterpret_cast<TrainSmem*>(smem_raw);
-  load_weights(sm.w, wg);
-  for (int i = threadIdx.x; i < kParams; i += blockDim.x) {
-    sm.bias[i] = params[i];
-    sm.grad[i] = 0.f;
+// ---------------------------------------------------------------------------------------------
+// Training step on the 5th-generation tensor cores (tcgen05, accumulators in tensor memory).
+//
+// One CTA of 4 warps per SM takes tiles of 128 samples (the MMA's M); tile row r is thread r and
+// TMEM lane r. Every GEMM of the step is one chain of tcgen05.mma (kind::f16, BF16 operands in
+// shared memory, FP32 accumulation in TMEM) issued by thread 0 and completed through an mbarrier:
+//   forward   H1 = X W1^T, H2 = relu(H1) W2^T, Y = relu(H2) W3^T
+//   backward  dH2 = dY W3, dH1 = (dH2 . relu'(H2)) W2
+//   weights   [dW2 ; dW1] += [d2^T ; d1^T] [h1^T | x^T | 1]^T  (M = 128: o of layer 2, then of layer 1)
+//             dW3 += dy^T [h2^T | 1]^T, whose columns of ones give the bias gradients.
+// Between the GEMMs the threads read their accumulator row (tcgen05.ld), apply bias, ReLU, loss or
+// mask, and write the next operands to shared memory in the canonical K-major layout without
+// swizzle (8 x 8 core matrices of 128 bytes; an 8-row group holds its K chunks back to back), both
+// as rows (A of the next layer) and transposed (the sample axis as K of the weight GEMMs). The
+// weight-gradient accumulators stay in TMEM across the CTA's tiles and leave once per CTA.
+
+constexpr int kTcRows = 128;
+constexpr int kTcThreads = 128;
+constexpr int kTmemCols = 512;
+// accumulator columns (32-bit) in the CTA's tensor memory
+constexpr int kColH1 = 0, kColH2 = 64, kColY = 128, kColD2 = 144, kColD1 = 208, kColW21 = 272, kColW3 = 368;
+
+struct __align__(1024) TcSmem {
+  __nv_bfloat16 w1[64 * 16];    // B of H1:  [N 64 outputs][K 16 inputs]
+  __nv_bfloat16 w2[64 * 64];    // B of H2:  [64][64]
+  __nv_bfloat16 w3[16 * 64];    // B of Y:   [N 16][K 64] (rows 7..15 zero)
+  __nv_bfloat16 w3t[64 * 16];   // B of dH2: [N 64][K 16] (W3 transposed, K 7..15 zero)
+  __nv_bfloat16 w2t[64 * 64];   // B of dH1: [N 64][K 64] (W2 transposed)
+  __nv_bfloat16 x[128 * 16];    // A: inputs (columns 8..15 zero)
+  __nv_bfloat16 h1[128 * 64];   // A: layer-1 activations
+  __nv_bfloat16 h2[128 * 64];   // A: layer-2 activations
+  __nv_bfloat16 dy[128 * 16];   // A: output gradient (columns 7..15 zero)
+  __nv_bfloat16 d2[128 * 64];   // A: layer-2 pre-activation gradient
+  __nv_bfloat16 dyT[16 * 128];  // A of dW3; as an M = 128 operand its rows 16..127 run into dT (not read back)
+  __nv_bfloat16 dT[128 * 128];  // A of [dW2; dW1]: rows 0..63 d2^T, rows 64..127 d1^T (K = samples)
+  __nv_bfloat16 hxT[96 * 128];  // B of [dW2; dW1]: rows 0..63 h1^T, 64..79 x^T, 80 ones, 81..95 zero
+  __nv_bfloat16 h2T[80 * 128];  // B of dW3: rows 0..63 h2^T, 64 ones, 65..79 zero
+  float bias[64 + 64 + 16];
+  unsigned long long mbar;
+  unsigned tmem_base;
+};
+
+// Element offset of (row r, column k) in a K-major no-swizzle bf16 matrix with K columns.
+__device__ __forceinline__ int km_off(int r, int k, int K) { return (r & 7) * 8 + (r >> 3) * (K * 8) + (k & 7) + (k >> 3) * 64; }
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return static_cast<uint32_t>(__cvta_generic_to_shared(p)); }
+
+// Shared-memory matrix descriptor of K-major operand rows (K columns) for the MMA's K step ks
+// (16 columns): start, leading byte offset 128 (the next 8 columns), stride byte offset 16 K (the
+// next 8 rows), descriptor version 1, no swizzle.
+__device__ __forceinline__ uint64_t kdesc(const void* base, int K, int ks) {
+  const uint32_t a = smem_u32(base) + ks * 256;
+  return static_cast<uint64_t>((a >> 4) & 0x3FFFu) | (static_cast<uint64_t>(128 >> 4) << 16) |
+         (static_cast<uint64_t>((K * 16) >> 4) << 32) | (1ull << 46);
+}
+
+// Instruction descriptor: kind::f16, BF16 A and B (K-major), FP32 D, M = 128, N.
+__device__ __forceinline__ uint32_t idesc_bf16(int N) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | (static_cast<uint32_t>(N >> 3) << 17) | ((128u >> 4) << 24);
+}
+
+__device__ __forceinline__ void umma_f16(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc, uint32_t acc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d_tmem),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(acc));
+}
+
+// D (+)= A B^T over K columns (A: 128 rows, B: N rows, both K-major).
+__device__ __forceinline__ void tc_gemm(uint32_t d_tmem, const void* A, const void* B, int K, int N, bool accumulate) {
+  const uint32_t id = idesc_bf16(N);
+  for (int ks = 0; ks < K / 16; ++ks) umma_f16(d_tmem, kdesc(A, K, ks), kdesc(B, K, ks), id, (accumulate || ks > 0) ? 1u : 0u);
+}
+
+__device__ __forceinline__ void tc_commit(unsigned long long* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+               : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void proxy_fence() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+// Waits for the mbarrier phase with the given parity for at most 2^31 SM cycles (about 1 s); false
+// if it gave up.
+__device__ __forceinline__ bool tc_wait(unsigned long long* bar, uint32_t parity) {
+  const uint32_t a = smem_u32(bar);
+  const long long t0 = clock64();
+  while (clock64() - t0 < (1ll << 31)) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(done)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (done) return true;
   }
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, tig = lane & 3;
-  if (lane == 0) sm.loss[warp] = 0.f;
+  return false;
+}
+
+// 16 consecutive FP32 accumulator columns of this thread's TMEM lane.
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float v[16]) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, "
+      "[%16];\n"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int j = 0; j < 16; ++j) v[j] = __uint_as_float(r[j]);
+}
+
+__device__ __forceinline__ void st_pair(__nv_bfloat16* m, int off, float a, float b) {
+  *reinterpret_cast<uint32_t*>(m + off) = pack_bf16(a, b);
+}
+
+// Operands written by this CTA's threads become visible to the tensor cores before thread 0 issues.
+__device__ __forceinline__ void tc_handoff() {
+  proxy_fence();
+  tc_fence_before();
   __syncthreads();
-  WarpStage& st = sm.stage[warp];
-  const int tiles = batch / 16;
-  float wo0 = wout[tig * 2], wo1 = wout[tig * 2 + 1];
-  for (int tile = blockIdx.x * kTrainWarps + warp; tile < tiles; tile += gridDim.x * kTrainWarps) {
-    const long long r0 = (first + (long long)(tile * 16 + g) * stride) % n_data;
-    const long long r1 = (first + (long long)(tile * 16 + g + 8) * stride) % n_data;
-    uint32_t xa[4];
-    {
-      const float2 x0 = *reinterpret_cast<const float2*>(X + r0 * kIn + tig * 2);
-      const float2 x1 = *reinterpret_cast<const float2*>(X + r1 * kIn + tig * 2);
-      xa[0] = pack_bf16(x0.x, x0.y);
-      xa[1] = pack_bf16(x1.x, x1.y);
-      xa[2] = 0u;
-      xa[3] = 0u;
-      st.xT[tig * 2][g] = __float2bfloat16_rn(x0.x);
-      st.xT[tig * 2 + 1][g] = __float2bfloat16_rn(x0.y);
-      st.xT[tig * 2][g + 8] = __float2bfloat16_rn(x1.x);
-      st.xT[tig * 2 + 1][g + 8] = __float2bfloat16_rn(x1.y);
+}
+
+// One MMA group: thread 0 issues it after the hand-off and commits it to the mbarrier, every thread
+// waits for its completion (bounded). Returns false for the whole CTA if a wait gave up.
+template <typename Issue>
+__device__ __forceinline__ bool tc_run(unsigned long long* bar, uint32_t& phase, Issue issue) {
+  tc_handoff();
+  if (threadIdx.x == 0) {
+    tc_fence_after();
+    issue();
+    tc_commit(bar);
+  }
+  const bool done = tc_wait(bar, phase);
+  phase ^= 1u;
+  tc_fence_after();
+  return __syncthreads_and(done) != 0;
+}
+
+__device__ __forceinline__ void tc_alloc(unsigned* dst, int cols) {
+  asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(dst)), "r"(cols)
+               : "memory");
+  asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+
+__device__ __forceinline__ void tc_dealloc(uint32_t taddr, int cols) {
+  asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(cols) : "memory");
+}
+
+__device__ __forceinline__ void mbar_init1(unsigned long long* bar) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar)) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+// Loss = sum over samples and outputs of wout[o] ws (y - t)^2 / batch, with ws = Y[row][7] the
+// sample weight; its gradient is added to grad_out and the loss to loss_out. Sample r of this call
+// is row (first + r * stride) mod n_data, a strided walk that visits every row once per epoch when
+// stride and n_data are coprime. err: set when a completion wait gave up.
+__global__ void __launch_bounds__(kTcThreads, 1)
+    k_train_tc(const WeightsBf16* wg, const float* params, const float* X, const float* Y, long long n_data,
+               long long first, long long stride, int batch, float inv_batch, const float* wout, float* grad_out,
+               float* loss_out, unsigned* err) {
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  TcSmem& sm = *reinterpret_cast<TcSmem*>(smem_raw);
+  const int r = threadIdx.x, warp = r >> 5;
+  // weights into the K-major layouts, constant rows, biases
+  for (int i = r; i < 64 * 16; i += kTcThreads) {
+    const int o = i / 16, k = i % 16;
+    sm.w1[km_off(o, k, 16)] = wg->w1f[o * 16 + k];
+    sm.w3t[km_off(o, k, 16)] = wg->w3b[o * 16 + k];  // w3b is [i][o], o padded to 16
+  }
+  for (int i = r; i < 64 * 64; i += kTcThreads) {
+    const int o = i / 64, k = i % 64;
+    sm.w2[km_off(o, k, 64)] = wg->w2f[i];
+    sm.w2t[km_off(o, k, 64)] = wg->w2b[i];
+  }
+  for (int i = r; i < 16 * 64; i += kTcThreads) {
+    const int o = i / 64, k = i % 64;
+    sm.w3[km_off(o, k, 64)] = o < 8 ? wg->w3f[o * 64 + k] : __float2bfloat16_rn(0.f);
+  }
+  for (int i = r; i < 144; i += kTcThreads)
+    sm.bias[i] = i < 64 ? params[kB1 + i] : i < 128 ? params[kB2 + i - 64] : (i - 128 < 8 ? params[kB3 + i - 128] : 0.f);
+  for (int n = 72; n < 96; ++n) sm.hxT[km_off(n, r, 128)] = __float2bfloat16_rn(n == 80 ? 1.f : 0.f);
+  for (int n = 64; n < 80; ++n) sm.h2T[km_off(n, r, 128)] = __float2bfloat16_rn(n == 64 ? 1.f : 0.f);
+  if (r == 0) mbar_init1(&sm.mbar);
+  if (warp == 0) tc_alloc(&sm.tmem_base, kTmemCols);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tm = sm.tmem_base;
+  const uint32_t lane = static_cast<uint32_t>(warp * 32) << 16;  // this warp's TMEM lane quarter
+  float wo[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) wo[k] = k < 7 ? wout[k] : 0.f;
+  uint32_t phase = 0;
+  float loss = 0.f;
+  int ntile = 0;
+  bool ok = true;
+  const int tiles = (batch + kTcRows - 1) / kTcRows;
+  for (int tile = blockIdx.x; tile < tiles && ok; tile += gridDim.x, ++ntile) {
+    const int srow = tile * kTcRows + r;
+    const bool valid = srow < batch;
+    const long long row = valid ? (first + static_cast<long long>(srow) * stride) % n_data : 0;
+    float xv[8], tv[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      xv[k] = valid ? X[row * 8 + k] : 0.f;
+      tv[k] = valid ? Y[row * 8 + k] : 0.f;
     }
-    float h1[8][4], h2[8][4], y[4];
-    forward(sm.w, sm.bias, xa, h1, h2, y, g, tig);
-    // dL/dy = 2 w (y - t) / batch; output 7 is padding
-    float dy[4];
-    {
-      const float2 t0 = *reinterpret_cast<const float2*>(Y + r0 * 8 + tig * 2);
-      const float2 t1 = *reinterpret_cast<const float2*>(Y + r1 * 8 + tig * 2);
-      // column 7 of a target row is the sample weight (held by the lane with tig 3)
-      const float ws0 = __shfl_sync(0xffffffffu, t0.y, (lane & ~3) | 3);
-      const float ws1 = __shfl_sync(0xffffffffu, t1.y, (lane & ~3) | 3);
-      const float e0 = y[0] - t0.x, e1 = y[1] - t0.y, e2 = y[2] - t1.x, e3 = y[3] - t1.y;
-      const bool pad = tig == 3;  // column 7
-      const float w1m = pad ? 0.f : wo1;
-      dy[0] = 2.f * wo0 * ws0 * e0 * inv_batch;
-      dy[1] = 2.f * w1m * ws0 * e1 * inv_batch;
-      dy[2] = 2.f * wo0 * ws1 * e2 * inv_batch;
-      dy[3] = 2.f * w1m * ws1 * e3 * inv_batch;
-      float l = ws0 * (wo0 * e0 * e0 + w1m * e1 * e1) + ws1 * (wo0 * e2 * e2 + w1m * e3 * e3);
+    const float ws = tv[7];  // sample weight (0 for the rows past the batch)
 #pragma unroll
-      for (int o = 1; o < 32; o <<= 1) l += __shfl_xor_sync(0xffffffffu, l, o);
-      if (lane == 0) sm.loss[warp] += l * inv_batch;
-    }
-    // dL/dh2 = dy W3 (K = outputs, 8 of 16), masked by ReLU
-    float d2[8][4];
-    {
-      uint32_t a[4] = {pack_bf16(dy[0], dy[1]), pack_bf16(dy[2], dy[3]), 0u, 0u};
+    for (int k = 0; k < 16; k += 2) st_pair(sm.x, km_off(r, k, 16), k < 8 ? xv[k] : 0.f, k < 8 ? xv[k + 1] : 0.f);
 #pragma unroll
-      for (int nt = 0; nt < 8; ++nt) {
-        d2[nt][0] = d2[nt][1] = d2[nt][2] = d2[nt][3] = 0.f;
-        mma(d2[nt], a, ld32(sm.w.w3b + (nt * 8 + g) * 16 + tig * 2), 0u);
+    for (int k = 0; k < 8; ++k) sm.hxT[km_off(64 + k, r, 128)] = __float2bfloat16_rn(xv[k]);
+    // layer 1
+    ok = tc_run(&sm.mbar, phase, [&] { tc_gemm(tm + kColH1, sm.x, sm.w1, 16, 64, false); });
+    if (!ok) break;
+    uint32_t m1[2] = {0u, 0u}, m2[2] = {0u, 0u};
 #pragma unroll
-        for (int j = 0; j < 4; ++j) d2[nt][j] = h2[nt][j] > 0.f ? d2[nt][j] : 0.f;
+    for (int c = 0; c < 4; ++c) {
+      float v[16];
+      tmem_ld16(tm + lane + kColH1 + 16 * c, v);
+#pragma unroll
+      for (int j = 0; j < 16; j += 2) {
+        const int o = 16 * c + j;
+        const float a = fmaxf(v[j] + sm.bias[o], 0.f), b = fmaxf(v[j + 1] + sm.bias[o + 1], 0.f);
+        m1[o >> 5] |= (a > 0.f ? 1u : 0u) << (o & 31);
+        m1[(o + 1) >> 5] |= (b > 0.f ? 1u : 0u) << ((o + 1) & 31);
+        st_pair(sm.h1, km_off(r, o, 64), a, b);
+        sm.hxT[km_off(o, r, 128)] = __float2bfloat16_rn(a);
+        sm.hxT[km_off(o + 1, r, 128)] = __float2bfloat16_rn(b);
       }
     }
-    // dL/dh1 = d2 W2, masked
-    float d1[8][4];
+    // layer 2
+    ok = tc_run(&sm.mbar, phase, [&] { tc_gemm(tm + kColH2, sm.h1, sm.w2, 64, 64, false); });
+    if (!ok) break;
 #pragma unroll
-    for (int nt = 0; nt < 8; ++nt) d1[nt][0] = d1[nt][1] = d1[nt][2] = d1[nt][3] = 0.f;
+    for (int c = 0; c < 4; ++c) {
+      float v[16];
+      tmem_ld16(tm + lane + kColH2 + 16 * c, v);
 #pragma unroll
-    for (int kc = 0; kc < 4; ++kc) {
-      uint32_t a[4];
-      chain(d2, kc, a);
-#pragma unroll
-      for (int nt = 0; nt < 8; ++nt) {
-        const __nv_bfloat16* wr = sm.w.w2b + (nt * 8 + g) * kHid + kc * 16 + tig * 2;
-        mma(d1[nt], a, ld32(wr), ld32(wr + 8));
+      for (int j = 0; j < 16; j += 2) {
+        const int o = 16 * c + j;
+        const float a = fmaxf(v[j] + sm.bias[64 + o], 0.f), b = fmaxf(v[j + 1] + sm.bias[64 + o + 1], 0.f);
+        m2[o >> 5] |= (a > 0.f ? 1u : 0u) << (o & 31);
+        m2[(o + 1) >> 5] |= (b > 0.f ? 1u : 0u) << ((o + 1) & 31);
+        st_pair(sm.h2, km_off(r, o, 64), a, b);
+        sm.h2T[km_off(o, r, 128)] = __float2bfloat16_rn(a);
+        sm.h2T[km_off(o + 1, r, 128)] = __float2bfloat16_rn(b);
       }
     }
+    // output layer, loss and dL/dy = 2 w (y - t) / batch (output 7 is padding)
+    ok = tc_run(&sm.mbar, phase, [&] { tc_gemm(tm + kColY, sm.h2, sm.w3, 64, 16, false); });
+    if (!ok) break;
+    {
+      float v[16];
+      tmem_ld16(tm + lane + kColY, v);
+      float dy[16];
 #pragma unroll
-    for (int nt = 0; nt < 8; ++nt)
+      for (int o = 0; o < 16; ++o) {
+        const float e = o < 7 ? v[o] + sm.bias[128 + o] - tv[o] : 0.f;
+        dy[o] = 2.f * wo[o & 7] * ws * e * inv_batch;
+        loss += ws * wo[o & 7] * e * e * inv_batch;
+      }
 #pragma unroll
-      for (int j = 0; j < 4; ++j) d1[nt][j] = h1[nt][j] > 0.f ? d1[nt][j] : 0.f;
-    // stage transposed tiles for the weight gradients
-#pragma unroll
-    for (int nt = 0; nt < 8; ++nt) {
-      store_t(st.h1T, h1[nt], nt * 8, g, tig);
-      store_t(st.h2T, h2[nt], nt * 8, g, tig);
-      store_t(st.d1T, d1[nt], nt * 8, g, tig);
-      store_t(st.d2T, d2[nt], nt * 8, g, tig);
+      for (int o = 0; o < 16; o += 2) {
+        st_pair(sm.dy, km_off(r, o, 16), dy[o], dy[o + 1]);
+        sm.dyT[km_off(o, r, 128)] = __float2bfloat16_rn(dy[o]);
+        sm.dyT[km_off(o + 1, r, 128)] = __float2bfloat16_rn(dy[o + 1]);
+      }
     }
-    store_t(st.dyT, dy, 0, g, tig);
-    for (int i = lane; i < 8 * 16; i += 32) {
-      (&st.xT[8][0])[i] = __float2bfloat16_rn(0.f);
-      (&st.dyT[8][0])[i] = __float2bfloat16_rn(0.f);
-    }
-    __syncwarp();
-    // dW3[o][i] = sum_s dy[s][o] h2[s][i]; dW2 = d2^T h1; dW1 = d1^T x
-    wgrad<16, kHid>(st.dyT, st.h2T, sm.grad, kW3, kHid, kOut, g, tig);
-    wgrad<kHid, kHid>(st.d2T, st.h1T, sm.grad, kW2, kHid, kHid, g, tig);
-    wgrad<kHid, 8>(st.d1T, st.xT, sm.grad, kW1, 16, kHid, g, tig);
-    bias_grad(dy, sm.grad, kB3, 0, g, tig, kOut);
+    // dH2 = dY W3 and dW3 += dy^T [h2 | 1]
+    const bool acc_w = ntile > 0;
+    ok = tc_run(&sm.mbar, phase, [&] {
+      tc_gemm(tm + kColD2, sm.dy, sm.w3t, 16, 64, false);
+      tc_gemm(tm + kColW3, sm.dyT, sm.h2T, 128, 80, acc_w);
+    });
+    if (!ok) break;
 #pragma unroll
-    for (int nt = 0; nt < 8; ++nt) {
-      bias_grad(d2[nt], sm.grad, kB2, nt * 8, g, tig, kHid);
-      bias_grad(d1[nt], sm.grad, kB1, nt * 8, g, tig, kHid);
+    for (int c = 0; c < 4; ++c) {
+      float v[16];
+      tmem_ld16(tm + lane + kColD2 + 16 * c, v);
+#pragma unroll
+      for (int j = 0; j < 16; j += 2) {
+        const int o = 16 * c + j;
+        const float a = (m2[o >> 5] >> (o & 31)) & 1u ? v[j] : 0.f;
+        const float b = (m2[(o + 1) >> 5] >> ((o + 1) & 31)) & 1u ? v[j + 1] : 0.f;
+        st_pair(sm.d2, km_off(r, o, 64), a, b);
+        sm.dT[km_off(o, r, 128)] = __float2bfloat16_rn(a);
+        sm.dT[km_off(o + 1, r, 128)] = __float2bfloat16_rn(b);
+      }
     }
-    __syncwarp();
+    // dH1 = d2 W2
+    ok = tc_run(&sm.mbar, phase, [&] { tc_gemm(tm + kColD1, sm.d2, sm.w2t, 64, 64, false); });
+    if (!ok) break;
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      float v[16];
+      tmem_ld16(tm + lane + kColD1 + 16 * c, v);
+#pragma unroll
+      for (int j = 0; j < 16; ++j) {
+        const int o = 16 * c + j;
+        sm.dT[km_off(64 + o, r, 128)] = __float2bfloat16_rn((m1[o >> 5] >> (o & 31)) & 1u ? v[j] : 0.f);
+      }
+    }
+    // [dW2; dW1] += [d2^T; d1^T] [h1 | x | 1]
+    ok = tc_run(&sm.mbar, phase, [&] { tc_gemm(tm + kColW21, sm.dT, sm.hxT, 128, 96, acc_w); });
   }
+  if (ok && ntile > 0) {
+    // gradient accumulators out of TMEM, one global add per entry and CTA
+#pragma unroll 1
+    for (int c = 0; c < 6; ++c) {
+      float v[16];
+      tmem_ld16(tm + lane + kColW21 + 16 * c, v);
+#pragma unroll
+      for (int j = 0; j < 16; ++j) {
+        const int n = 16 * c + j;
+        if (r < 64) {  // layer 2, output r
+          if (n < 64) atomicAdd(&grad_out[kW2 + r * 64 + n], v[j]);
+          else if (n == 80) atomicAdd(&grad_out[kB2 + r], v[j]);
+        } else {  // layer 1, output r - 64
+          if (n >= 64 && n < 72) atomicAdd(&grad_out[kW1 + (r - 64) * 16 + (n - 64)], v[j]);
+          else if (n == 80) atomicAdd(&grad_out[kB1 + (r - 64)], v[j]);
+        }
+      }
+    }
+#pragma unroll 1
+    for (int c = 0; c < 5; ++c) {
+      float v[16];
+      tmem_ld16(tm + lane + kColW3 + 16 * c, v);
+      if (r < kOut) {
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+          const int n = 16 * c + j;
+          if (n < 64) atomicAdd(&grad_out[kW3 + r * 64 + n], v[j]);
+          else if (n == 64) atomicAdd(&grad_out[kB3 + r], v[j]);
+        }
+      }
+    }
+  }
+  if (!ok) {
+    // a completion wait gave up: one more bounded wait for the MMA group in flight, then leave
+    tc_wait(&sm.mbar, phase);
+    if (r == 0) atomicOr(err, 1u);
+  }
+  for (int o = 16; o; o >>= 1) loss += __shfl_xor_sync(0xffffffffu, loss, o);
+  if ((r & 31) == 0 && loss != 0.f) atomicAdd(loss_out, loss);
+  tc_fence_before();
   __syncthreads();
-  for (int i = threadIdx.x; i < kParams; i += blockDim.x) {
-    const float v = sm.grad[i];
-    if (v != 0.f) atomicAdd(&grad_out[i], v);
+  if (warp == 0) {
+    tc_fence_after();
+    tc_dealloc(tm, kTmemCols);
   }
-  if (threadIdx.x < kTrainWarps && sm.loss[threadIdx.x] != 0.f) atomicAdd(loss_out, sm.loss[threadIdx.x]);
 }
 
 // AdamW on the FP32 master parameters, then the BF16 copies (padding entries stay zero).
@@ -393,6 +469,7 @@ struct SampleSpec {
   float strain_lo, strain_hi;  // log-uniform magnitude of the principal trial log strains
   float T_lo, T_hi, ep_hi;
   unsigned long long seed;
+  float dt_lo, dt_hi;          // log-uniform substep (rate-dependent laws)
 };
 
 // Trial Hencky strain of F (Voigt, shear components scaled by sqrt 2) from D = F - I.
@@ -527,16 +604,22 @@ __global__ void __launch_bounds__(256) k_forward(const WeightsBf16* wg, const fl
 }
 
 // ---------------------------------------------------------------------------------------------
-// Gated return map over particles. Each thread owns one particle; the warp's 32 particles go
-// through the MLP as two 16-row tiles staged in shared memory.
+// Gated return map over particles, 128 per tile: thread r owns particle r of the tile and TMEM lane
+// r; when a tile holds a plastic particle the network runs as three tcgen05 GEMMs (M = 128) with
+// the epilogues of k_train_tc's forward pass.
+constexpr int kGateThreads = 128;
+constexpr int kGateTmemCols = 256;  // H1 columns 0..63, H2 64..127, Y 128..143
 
-constexpr int kGateThreads = 256;
-
-struct GateSmem {
-  WeightsBf16 w;
-  float bias[kParams];
-  float x[kGateThreads][8];
-  float y[kGateThreads][8];
+struct __align__(1024) GateSmem {
+  __nv_bfloat16 w1[64 * 16];
+  __nv_bfloat16 w2[64 * 64];
+  __nv_bfloat16 w3[16 * 64];
+  __nv_bfloat16 x[128 * 16];
+  __nv_bfloat16 h1[128 * 64];
+  __nv_bfloat16 h2[128 * 64];
+  float bias[64 + 64 + 16];
+  unsigned long long mbar;
+  unsigned tmem_base;
 };
 
 struct GateOut {
@@ -546,22 +629,36 @@ struct GateOut {
 // D = F - I (n x 9 float, formed by the caller in higher precision), ep, T in; D, dep and tau
 // (n x 6: xx yy zz xy xz yz) out; path: 0 elastic, 1 learned, 2 exact fallback. use_mlp = 0 runs
 // the exact map for every particle through the same kernel, so both timings share loads and stores.
+// err: set when a tensor-core completion wait gave up (the tile's predictions are then rejected).
 __global__ void __launch_bounds__(kGateThreads) k_gated(const WeightsBf16* wg, const float* params, mpm::MaterialDev mt,
                                                         Scales sc, float gate_tol, int use_mlp, long long n,
                                                         const float* Din, const float* epin, const float* Tin, float* Dout,
-                                                        float* dep, float* tau, signed char* path, GateOut* counts) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+                                                        float* dep, float* tau, signed char* path, GateOut* counts,
+                                                        unsigned* err) {
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
   GateSmem& sm = *reinterpret_cast<GateSmem*>(smem_raw);
+  const int r = threadIdx.x, warp = r >> 5;
+  uint32_t tm = 0, phase = 0;
+  bool tc_ok = true;
   if (use_mlp) {
-    load_weights(sm.w, wg);
-    for (int i = threadIdx.x; i < kParams; i += blockDim.x) sm.bias[i] = params[i];
+    for (int i = r; i < 64 * 16; i += kGateThreads) sm.w1[km_off(i / 16, i % 16, 16)] = wg->w1f[i];
+    for (int i = r; i < 64 * 64; i += kGateThreads) sm.w2[km_off(i / 64, i % 64, 64)] = wg->w2f[i];
+    for (int i = r; i < 16 * 64; i += kGateThreads)
+      sm.w3[km_off(i / 64, i % 64, 64)] = i / 64 < 8 ? wg->w3f[i] : __float2bfloat16_rn(0.f);
+    for (int i = r; i < 144; i += kGateThreads)
+      sm.bias[i] = i < 64 ? params[kB1 + i] : i < 128 ? params[kB2 + i - 64] : (i - 128 < 8 ? params[kB3 + i - 128] : 0.f);
+    if (r == 0) mbar_init1(&sm.mbar);
+    if (warp == 0) tc_alloc(&sm.tmem_base, kGateTmemCols);
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    tm = sm.tmem_base;
   }
-  __syncthreads();
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, tig = lane & 3;
+  const uint32_t lane = static_cast<uint32_t>(warp * 32) << 16;
   unsigned c_el = 0, c_ml = 0, c_fb = 0;
   const float r2 = 1.41421356237f, ir2 = 0.70710678118f, s15 = 1.224744871391589f;
   for (long long base = (long long)blockIdx.x * kGateThreads; base < n; base += (long long)gridDim.x * kGateThreads) {
-    const long long i = base + threadIdx.x;
+    const long long i = base + r;
     const bool live = i < n;
     float D[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, ep = 0.f, T = 0.f, L6[6] = {0, 0, 0, 0, 0, 0};
     if (live) {
@@ -575,29 +672,50 @@ __global__ void __launch_bounds__(kGateThreads) k_gated(const WeightsBf16* wg, c
     const bool plastic = live && tr.q > tr.yield;
     bool accepted = false;
     float tau6[6], dp = 0.f;
-    if (use_mlp && __any_sync(0xffffffffu, plastic)) {
+    if (use_mlp && tc_ok && __syncthreads_or(plastic)) {
       float x[8];
       features(sc, tr, T, ep, x);
-      for (int k = 0; k < 8; ++k) sm.x[threadIdx.x][k] = x[k];
-      __syncwarp();
 #pragma unroll
-      for (int half = 0; half < 2; ++half) {
-        const int row0 = warp * 32 + half * 16;
-        const float2 x0 = *reinterpret_cast<const float2*>(&sm.x[row0 + g][tig * 2]);
-        const float2 x1 = *reinterpret_cast<const float2*>(&sm.x[row0 + g + 8][tig * 2]);
-        const uint32_t xa[4] = {pack_bf16(x0.x, x0.y), pack_bf16(x1.x, x1.y), 0u, 0u};
-        float h1[8][4], h2[8][4], y[4];
-        forward(sm.w, sm.bias, xa, h1, h2, y, g, tig);
-        *reinterpret_cast<float2*>(&sm.y[row0 + g][tig * 2]) = make_float2(y[0], y[1]);
-        *reinterpret_cast<float2*>(&sm.y[row0 + g + 8][tig * 2]) = make_float2(y[2], y[3]);
+      for (int k = 0; k < 16; k += 2) st_pair(sm.x, km_off(r, k, 16), k < 8 ? x[k] : 0.f, k < 8 ? x[k + 1] : 0.f);
+      float y[16];
+      tc_ok = tc_run(&sm.mbar, phase, [&] { tc_gemm(tm + 0, sm.x, sm.w1, 16, 64, false); });
+      if (tc_ok) {
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+          float v[16];
+          tmem_ld16(tm + lane + 16 * c, v);
+#pragma unroll
+          for (int j = 0; j < 16; j += 2)
+            st_pair(sm.h1, km_off(r, 16 * c + j, 64), fmaxf(v[j] + sm.bias[16 * c + j], 0.f),
+                    fmaxf(v[j + 1] + sm.bias[16 * c + j + 1], 0.f));
+        }
+        tc_ok = tc_run(&sm.mbar, phase, [&] { tc_gemm(tm + 64, sm.h1, sm.w2, 64, 64, false); });
       }
-      __syncwarp();
-      if (plastic) {
+      if (tc_ok) {
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+          float v[16];
+          tmem_ld16(tm + lane + 64 + 16 * c, v);
+#pragma unroll
+          for (int j = 0; j < 16; j += 2)
+            st_pair(sm.h2, km_off(r, 16 * c + j, 64), fmaxf(v[j] + sm.bias[64 + 16 * c + j], 0.f),
+                    fmaxf(v[j + 1] + sm.bias[64 + 16 * c + j + 1], 0.f));
+        }
+        tc_ok = tc_run(&sm.mbar, phase, [&] { tc_gemm(tm + 128, sm.h2, sm.w3, 64, 16, false); });
+      }
+      if (tc_ok) {
+        tmem_ld16(tm + lane + 128, y);
+#pragma unroll
+        for (int k = 0; k < 7; ++k) y[k] += sm.bias[128 + k];
+      } else if (r == 0) {
+        atomicOr(err, 1u);
+      }
+      if (plastic && tc_ok) {
         float t6[6];
         trial_stress(mt, L6, t6);
         const float smag = 2.f * mt.mu * s15 * tr.dep_est;
-        for (int k = 0; k < 6; ++k) tau6[k] = t6[k] + smag * sm.y[threadIdx.x][k];
-        dp = tr.dep_est * sm.y[threadIdx.x][6];
+        for (int k = 0; k < 6; ++k) tau6[k] = t6[k] + smag * y[k];
+        dp = tr.dep_est * y[6];
         // residuals of the prediction against the return's two defining equations
         const float y0 = fmaxf(mt.yield_stress * tr.soft, 1e-30f);
         const float p3 = (tau6[0] + tau6[1] + tau6[2]) * (1.f / 3.f);
@@ -663,7 +781,108 @@ __global__ void __launch_bounds__(kGateThreads) k_gated(const WeightsBf16* wg, c
       c_ml += __shfl_xor_sync(0xffffffffu, c_ml, o);
       c_fb += __shfl_xor_sync(0xffffffffu, c_fb, o);
     }
-    if (lane == 0) {
+    if ((r & 31) == 0) {
+      atomicAdd(&counts->elastic, c_el);
+      atomicAdd(&counts->learned, c_ml);
+      atomicAdd(&counts->fallback, c_fb);
+    }
+  }
+  if (use_mlp) {
+    if (!tc_ok) tc_wait(&sm.mbar, phase);  // one more bounded wait for a group still in flight
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) {
+      tc_fence_after();
+      tc_dealloc(tm, kGateTmemCols);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Johnson-Cook (models 6, 7): the network maps the dimensionless trial state (mpm::jc_features) to
+// the consistency root u = dep / s of src/three/metal-plasticity.js:28-34 (output 0); the in-step
+// use refines it by Newton steps and gates it (mpm::jc_refine).
+
+// One random Johnson-Cook trial state: tr e uniform in [-0.01, 0.01], ep and T uniform, the substep
+// log-uniform; even draws take |dev e| log-uniform, odd draws a trial stress just above the
+// initial flow stress, q = flow(ep, 0, T) (1 + d) with d log-uniform in [1e-4, 1] (the states of
+// a loading step, whose increment is small).
+struct JcState {
+  float q, J, ep, T, dt;
+};
+
+__device__ JcState jc_random_state(const mpm::MaterialDev& mt, const SampleSpec& sp, long long i) {
+  JcState st;
+  const float trv = 0.02f * urand(sp.seed, i, 1) - 0.01f;
+  st.J = expf(trv);
+  st.ep = sp.ep_hi * urand(sp.seed, i, 2);
+  st.T = sp.T_lo + (sp.T_hi - sp.T_lo) * urand(sp.seed, i, 3);
+  st.dt = expf(logf(sp.dt_lo) + urand(sp.seed, i, 4) * (logf(sp.dt_hi) - logf(sp.dt_lo)));
+  if (i & 1) {
+    const float d = expf(-9.210340372f * (1.f - urand(sp.seed, i, 0)));
+    st.q = mpm::jc_flow(mt, st.ep, 0.f, st.T) * (1.f + d);
+  } else {
+    const float mag = expf(logf(sp.strain_lo) + urand(sp.seed, i, 0) * (logf(sp.strain_hi) - logf(sp.strain_lo)));
+    st.q = 2.449489742783178f * mt.mu * mag / st.J;
+  }
+  return st;
+}
+
+// Training rows for Johnson-Cook: X the eight inputs, Y[0] the exact root u from the bisection,
+// Y[7] the sample weight (1 for plastic states; elastic states have no return and weight 0).
+__global__ void k_samples_jc(mpm::MaterialDev mt, SampleSpec sp, long long n, float* X, float* Y) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const JcState st = jc_random_state(mt, sp, i);
+    const bool plastic = st.q > mpm::jc_flow(mt, st.ep, 0.f, st.T);
+    float x[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    float u = 0.f;
+    if (plastic) {
+      mpm::jc_features(mt, st.q, st.J, st.ep, st.T, st.dt, x);
+      const float s = st.q * st.J / (3.f * mt.mu);
+      u = mpm::jc_bisect(mt, st.q, st.J, st.ep, st.T, st.dt) / s;
+    }
+    for (int k = 0; k < 8; ++k) X[i * 8 + k] = x[k];
+    Y[i * 8 + 0] = u;
+    for (int k = 1; k < 7; ++k) Y[i * 8 + k] = 0.f;
+    Y[i * 8 + 7] = plastic ? 1.f : 0.f;
+  }
+}
+
+// The plastic increment of random Johnson-Cook trial states: exact bisection for every state
+// (use_mlp 0), or the network (warp-wide tensor-core tiles) + Newton refinement + gate with the
+// bisection for rejected states. dep out (keeps the work); counts: elastic, accepted, rejected.
+__global__ void __launch_bounds__(256) k_gated_jc(const WeightsBf16* wg, const float* params, mpm::MaterialDev mt,
+                                                  SampleSpec sp, float gate_tol, int newton, int use_mlp, long long n,
+                                                  float* dep_out, GateOut* counts) {
+  unsigned c_el = 0, c_ml = 0, c_fb = 0;
+  for (long long base = (long long)blockIdx.x * blockDim.x; base < n; base += (long long)gridDim.x * blockDim.x) {
+    const long long i = base + threadIdx.x;
+    const bool live = i < n;
+    const JcState st = jc_random_state(mt, sp, live ? i : 0);
+    const bool plastic = live && st.q > mpm::jc_flow(mt, st.ep, 0.f, st.T);
+    float dep = 0.f;
+    bool accepted = false;
+    if (use_mlp) {
+      float x[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+      if (plastic) mpm::jc_features(mt, st.q, st.J, st.ep, st.T, st.dt, x);
+      const float u = warp_predict_first(wg, params, x, plastic);
+      if (plastic) accepted = mpm::jc_refine(mt, st.q, st.J, st.ep, st.T, st.dt, u, gate_tol, newton, dep);
+    }
+    if (plastic && !accepted) dep = mpm::jc_bisect(mt, st.q, st.J, st.ep, st.T, st.dt);
+    if (live) {
+      dep_out[i] = dep;
+      if (!plastic) ++c_el;
+      else if (accepted) ++c_ml;
+      else ++c_fb;
+    }
+  }
+  if (counts) {
+    for (int o = 16; o; o >>= 1) {
+      c_el += __shfl_xor_sync(0xffffffffu, c_el, o);
+      c_ml += __shfl_xor_sync(0xffffffffu, c_ml, o);
+      c_fb += __shfl_xor_sync(0xffffffffu, c_fb, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
       atomicAdd(&counts->elastic, c_el);
       atomicAdd(&counts->learned, c_ml);
       atomicAdd(&counts->fallback, c_fb);
@@ -671,20 +890,7 @@ __global__ void __launch_bounds__(kGateThreads) k_gated(const WeightsBf16* wg, c
   }
 }
 
-mpm::MaterialDev to_dev(const mpm_material& m) {
-  mpm::MaterialDev d{};
-  d.model = m.model;
-  d.mu = (float)m.mu;
-  d.lam = (float)m.lambda;
-  d.yield_stress = (float)m.yield_stress;
-  d.hardening = (float)m.hardening;
-  d.T_ref = (float)m.T_ref;
-  d.inv_T_span = m.T_hot > m.T_ref ? (float)(1.0 / (m.T_hot - m.T_ref)) : 0.f;
-  d.hot_ratio = (float)m.hot_ratio;
-  d.heat_per_work = m.specific_heat > 0 ? (float)(m.heat_fraction / m.specific_heat) : 0.f;
-  d.wave_modulus = (float)(m.lambda + 2 * m.mu);
-  return d;
-}
+mpm::MaterialDev to_dev(const mpm_material& m) { return mpm::material_to_device(m); }
 
 }  // namespace surr
 
@@ -700,6 +906,7 @@ struct mpm_surrogate {
   float* adam_v = nullptr;
   float* loss = nullptr;
   surr::WeightsBf16* wbf = nullptr;
+  unsigned* tc_err = nullptr;  // set by a tensor-core kernel when a completion wait gave up
   int num_sms = 148;
   int adam_t = 0;
   std::string err;
@@ -719,6 +926,41 @@ int sfail(mpm_surrogate* s, int rc, const std::string& why) {
                                         std::string(#call) + ": " + cudaGetErrorString(e_));       \
   } while (0)
 
+surr::SampleSpec spec_of(const mpm_surrogate_config* cfg) {
+  surr::SampleSpec sp{(float)cfg->strain_min, (float)cfg->strain_max, (float)cfg->T_min, (float)cfg->T_max,
+                      (float)cfg->ep_max, cfg->seed, 1e-7f, 1e-5f};
+  if (cfg->dt_min > 0 && cfg->dt_max >= cfg->dt_min) {
+    sp.dt_lo = (float)cfg->dt_min;
+    sp.dt_hi = (float)cfg->dt_max;
+  }
+  return sp;
+}
+
+bool is_jc(const mpm_surrogate* s) { return mpm::learned_model(s->mat.model); }
+
+// One forward/backward pass over `batch` rows (row r of the call is (first + r stride) mod n_data)
+// adding the gradient to s->grad and the loss to *loss: tiles of 128 rows, one CTA per SM.
+void launch_train(mpm_surrogate* s, const float* X, const float* Y, long long n_data, long long first, long long stride,
+                  int batch, const float* wout, float* loss) {
+  const int tiles = (batch + surr::kTcRows - 1) / surr::kTcRows;
+  const int blocks = std::min(s->num_sms, tiles);
+  surr::k_train_tc<<<blocks, surr::kTcThreads, sizeof(surr::TcSmem), s->stream>>>(
+      s->wbf, s->params, X, Y, n_data, first, stride, batch, 1.f / batch, wout, s->grad, loss, s->tc_err);
+}
+
+// The tensor-core kernels' completion-wait flag (and its clearing).
+int check_tc(mpm_surrogate* s) {
+  unsigned e = 0;
+  if (cudaMemcpyAsync(&e, s->tc_err, sizeof e, cudaMemcpyDeviceToHost, s->stream) != cudaSuccess ||
+      cudaStreamSynchronize(s->stream) != cudaSuccess)
+    return sfail(s, MPM_ERR_CUDA, "reading the tensor-core kernels' status failed");
+  if (e) {
+    cudaMemsetAsync(s->tc_err, 0, sizeof(unsigned), s->stream);
+    return sfail(s, MPM_ERR_TIMEOUT, "a tensor-core completion wait gave up (the network's work was not used)");
+  }
+  return MPM_OK;
+}
+
 int sync_bf16(mpm_surrogate* s) {
   surr::k_pad_zero<<<2, 256, 0, s->stream>>>(s->params);
   surr::k_to_bf16<<<16, 256, 0, s->stream>>>(s->params, s->wbf);
@@ -733,7 +975,8 @@ extern "C" {
 int mpm_surrogate_create(const mpm_material* material, uint64_t seed, mpm_surrogate** out) {
   if (!material || !out) return MPM_ERR_INVALID_ARG;
   *out = nullptr;
-  if (material->model != 4 && material->model != 5 && material->model != 10) return MPM_ERR_UNSUPPORTED;
+  if (material->model != 4 && material->model != 5 && material->model != 10 && !mpm::learned_model(material->model))
+    return MPM_ERR_UNSUPPORTED;
   if (!(material->mu > 0) || !(material->yield_stress > 0)) return MPM_ERR_INVALID_ARG;
   mpm_surrogate* s = new mpm_surrogate();
   s->mat = *material;
@@ -749,12 +992,15 @@ int mpm_surrogate_create(const mpm_material* material, uint64_t seed, mpm_surrog
   const size_t pb = surr::kParams * sizeof(float);
   if (cudaMalloc(&s->params, pb) != cudaSuccess || cudaMalloc(&s->grad, pb) != cudaSuccess ||
       cudaMalloc(&s->adam_m, pb) != cudaSuccess || cudaMalloc(&s->adam_v, pb) != cudaSuccess ||
-      cudaMalloc(&s->loss, 16) != cudaSuccess || cudaMalloc(&s->wbf, sizeof(surr::WeightsBf16)) != cudaSuccess)
+      cudaMalloc(&s->loss, 16) != cudaSuccess || cudaMalloc(&s->wbf, sizeof(surr::WeightsBf16)) != cudaSuccess ||
+      cudaMalloc(&s->tc_err, sizeof(unsigned)) != cudaSuccess)
     return bail(MPM_ERR_OUT_OF_MEMORY);
-  if (cudaFuncSetAttribute(surr::k_train, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(surr::TrainSmem)) !=
-          cudaSuccess ||
-      cudaFuncSetAttribute(surr::k_gated, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(surr::GateSmem)) !=
+  if (cudaMemset(s->tc_err, 0, sizeof(unsigned)) != cudaSuccess ||
+      cudaFuncSetAttribute(surr::k_train_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(surr::TcSmem)) !=
           cudaSuccess)
+    return bail(MPM_ERR_CUDA);
+  if (cudaFuncSetAttribute(surr::k_gated, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(surr::GateSmem)) !=
+      cudaSuccess)
     return bail(MPM_ERR_CUDA);
   // He initialisation from a seeded host generator (fan-in 8, 64, 64), zero biases
   std::vector<float> p(surr::kParams, 0.f);
@@ -788,7 +1034,7 @@ int mpm_surrogate_create(const mpm_material* material, uint64_t seed, mpm_surrog
 int mpm_surrogate_destroy(mpm_surrogate* s) {
   if (!s) return MPM_ERR_INVALID_ARG;
   if (s->stream) cudaStreamSynchronize(s->stream);
-  void* bufs[] = {s->params, s->grad, s->adam_m, s->adam_v, s->loss, s->wbf};
+  void* bufs[] = {s->params, s->grad, s->adam_m, s->adam_v, s->loss, s->wbf, s->tc_err};
   for (void* b : bufs)
     if (b) cudaFree(b);
   if (s->stream) cudaStreamDestroy(s->stream);
@@ -817,8 +1063,8 @@ int mpm_surrogate_set_weights(mpm_surrogate* s, const float* params) {
 int mpm_surrogate_samples(mpm_surrogate* s, const mpm_surrogate_config* cfg, int64_t n, float* X, float* Y, double* F,
                           double* ep, double* T) {
   if (!s || !cfg || n <= 0 || !X || !Y) return MPM_ERR_INVALID_ARG;
-  surr::SampleSpec sp{(float)cfg->strain_min, (float)cfg->strain_max, (float)cfg->T_min, (float)cfg->T_max,
-                      (float)cfg->ep_max, cfg->seed};
+  if (F && is_jc(s)) return sfail(s, MPM_ERR_UNSUPPORTED, "Johnson-Cook rows carry no trial F");
+  const surr::SampleSpec sp = spec_of(cfg);
   float *dX = nullptr, *dY = nullptr, *dD = nullptr, *dep = nullptr, *dT = nullptr;
   SCUDA(s, cudaMalloc(&dX, n * 8 * sizeof(float)));
   SCUDA(s, cudaMalloc(&dY, n * 8 * sizeof(float)));
@@ -827,7 +1073,10 @@ int mpm_surrogate_samples(mpm_surrogate* s, const mpm_surrogate_config* cfg, int
     SCUDA(s, cudaMalloc(&dep, n * sizeof(float)));
     SCUDA(s, cudaMalloc(&dT, n * sizeof(float)));
   }
-  surr::k_samples<<<s->num_sms * 8, 256, 0, s->stream>>>(s->mt, s->sc, sp, n, dX, dY, dD, dep, dT);
+  if (is_jc(s))
+    surr::k_samples_jc<<<s->num_sms * 8, 256, 0, s->stream>>>(s->mt, sp, n, dX, dY);
+  else
+    surr::k_samples<<<s->num_sms * 8, 256, 0, s->stream>>>(s->mt, s->sc, sp, n, dX, dY, dD, dep, dT);
   cudaError_t e = cudaGetLastError();
   if (e == cudaSuccess) e = cudaMemcpyAsync(X, dX, n * 8 * sizeof(float), cudaMemcpyDeviceToHost, s->stream);
   if (e == cudaSuccess) e = cudaMemcpyAsync(Y, dY, n * 8 * sizeof(float), cudaMemcpyDeviceToHost, s->stream);
@@ -866,13 +1115,18 @@ int mpm_surrogate_train(mpm_surrogate* s, const mpm_surrogate_config* cfg, float
   SCUDA(s, cudaMalloc(&X, n * 8 * sizeof(float)));
   SCUDA(s, cudaMalloc(&Y, n * 8 * sizeof(float)));
   SCUDA(s, cudaMalloc(&wout, 8 * sizeof(float)));
-  const float w[8] = {1, 1, 1, 1, 1, 1, (float)(cfg->dep_weight > 0 ? cfg->dep_weight : 1.0), 0};
-  surr::SampleSpec sp{(float)cfg->strain_min, (float)cfg->strain_max, (float)cfg->T_min, (float)cfg->T_max,
-                      (float)cfg->ep_max, cfg->seed};
+  // J2 / thermal J2: the stress correction (6) and dep (weighted); Johnson-Cook: the root u alone
+  const float w_j2[8] = {1, 1, 1, 1, 1, 1, (float)(cfg->dep_weight > 0 ? cfg->dep_weight : 1.0), 0};
+  const float w_jc[8] = {1, 0, 0, 0, 0, 0, 0, 0};
+  const float* w = is_jc(s) ? w_jc : w_j2;
+  const surr::SampleSpec sp = spec_of(cfg);
   int rc = MPM_OK;
-  cudaError_t e = cudaMemcpyAsync(wout, w, sizeof w, cudaMemcpyHostToDevice, s->stream);
+  cudaError_t e = cudaMemcpyAsync(wout, w, 8 * sizeof(float), cudaMemcpyHostToDevice, s->stream);
   if (e == cudaSuccess) {
-    surr::k_samples<<<s->num_sms * 8, 256, 0, s->stream>>>(s->mt, s->sc, sp, n, X, Y, nullptr, nullptr, nullptr);
+    if (is_jc(s))
+      surr::k_samples_jc<<<s->num_sms * 8, 256, 0, s->stream>>>(s->mt, sp, n, X, Y);
+    else
+      surr::k_samples<<<s->num_sms * 8, 256, 0, s->stream>>>(s->mt, s->sc, sp, n, X, Y, nullptr, nullptr, nullptr);
     e = cudaGetLastError();
   }
   // stride coprime with n walks every sample once per epoch in a scattered order
@@ -896,10 +1150,7 @@ int mpm_surrogate_train(mpm_surrogate* s, const mpm_surrogate_config* cfg, float
     const float lr_scale = cfg->cosine ? 0.5f * (1.f + cosf(3.14159265f * t / cfg->steps)) : 1.f;
     mpm_surrogate_config c = *cfg;
     c.lr = cfg->lr * lr_scale;
-    const int tiles = cfg->batch / 16;
-    const int blocks = std::min(s->num_sms, (tiles + surr::kTrainWarps - 1) / surr::kTrainWarps);
-    surr::k_train<<<blocks, surr::kTrainThreads, sizeof(surr::TrainSmem), s->stream>>>(
-        s->wbf, s->params, X, Y, n, first, stride, cfg->batch, 1.f / cfg->batch, wout, s->grad, dloss + t);
+    launch_train(s, X, Y, n, first, stride, cfg->batch, wout, dloss + t);
     ++s->adam_t;
     surr::k_adamw<<<(surr::kParams + 255) / 256, 256, 0, s->stream>>>(s->params, s->grad, s->adam_m, s->adam_v,
                                                                        s->adam_t, (float)c.lr, 0.9f, 0.999f, 1e-8f,
@@ -918,7 +1169,7 @@ int mpm_surrogate_train(mpm_surrogate* s, const mpm_surrogate_config* cfg, float
   if (rc != MPM_OK) return rc;
   if (e != cudaSuccess) return sfail(s, MPM_ERR_CUDA, cudaGetErrorString(e));
   if (loss_history) std::memcpy(loss_history, hist.data(), cfg->steps * sizeof(float));
-  return MPM_OK;
+  return check_tc(s);
 }
 
 int mpm_surrogate_grad(mpm_surrogate* s, int64_t n, const float* X, const float* Y, const float* out_weight,
@@ -936,10 +1187,7 @@ int mpm_surrogate_grad(mpm_surrogate* s, int64_t n, const float* X, const float*
   if (e == cudaSuccess) e = cudaMemsetAsync(dl, 0, sizeof(float), s->stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(s->grad, 0, surr::kParams * sizeof(float), s->stream);
   if (e == cudaSuccess) {
-    const int tiles = (int)(n / 16);
-    const int blocks = std::min(s->num_sms, (tiles + surr::kTrainWarps - 1) / surr::kTrainWarps);
-    surr::k_train<<<blocks, surr::kTrainThreads, sizeof(surr::TrainSmem), s->stream>>>(
-        s->wbf, s->params, dX, dY, n, 0, 1, (int)n, 1.f / n, dw, s->grad, dl);
+    launch_train(s, dX, dY, n, 0, 1, (int)n, dw, dl);
     e = cudaGetLastError();
   }
   float lh = 0;
@@ -953,7 +1201,7 @@ int mpm_surrogate_grad(mpm_surrogate* s, int64_t n, const float* X, const float*
   cudaFree(dl);
   if (e != cudaSuccess) return sfail(s, MPM_ERR_CUDA, cudaGetErrorString(e));
   if (loss) *loss = lh;
-  return MPM_OK;
+  return check_tc(s);
 }
 
 int mpm_surrogate_forward(mpm_surrogate* s, int64_t n, const float* X, float* Y) {
@@ -981,6 +1229,9 @@ int mpm_return_map_learned(mpm_surrogate* s, int64_t n, const double* F_in, cons
                            double gate_tol, int32_t use_mlp, double* F_out, double* dep, double* tau, int8_t* path,
                            mpm_gate_counts* counts) {
   if (!s || n < 0 || (n > 0 && (!F_in || !F_out || !dep || !tau))) return MPM_ERR_INVALID_ARG;
+  if (is_jc(s))
+    return sfail(s, MPM_ERR_UNSUPPORTED, "Johnson-Cook networks run inside the step (mpm_set_return_mode) or in "
+                                         "mpm_surrogate_time: their return depends on the substep");
   if (n == 0) return MPM_OK;
   // D = F - I in double before rounding: at small strains F - I in FP32 would lose digits
   std::vector<float> hF(n * 9), he(n, 0.f), hT(n, 0.f);
@@ -1005,9 +1256,9 @@ int mpm_return_map_learned(mpm_surrogate* s, int64_t n, const double* F_in, cons
   if (e == cudaSuccess) e = cudaMemcpyAsync(dT, hT.data(), n * sizeof(float), cudaMemcpyHostToDevice, s->stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(dc, 0, sizeof(surr::GateOut), s->stream);
   if (e == cudaSuccess) {
-    const int blocks = (int)std::min<long long>(s->num_sms * 4, (n + surr::kGateThreads - 1) / surr::kGateThreads);
+    const int blocks = (int)std::min<long long>(s->num_sms * 2, (n + surr::kGateThreads - 1) / surr::kGateThreads);
     surr::k_gated<<<blocks, surr::kGateThreads, sizeof(surr::GateSmem), s->stream>>>(
-        s->wbf, s->params, s->mt, s->sc, (float)gate_tol, use_mlp, n, dF, de, dT, dFo, ddep, dtau, dpath, dc);
+        s->wbf, s->params, s->mt, s->sc, (float)gate_tol, use_mlp, n, dF, de, dT, dFo, ddep, dtau, dpath, dc, s->tc_err);
     e = cudaGetLastError();
   }
   std::vector<float> oF(n * 9), od(n), ot(n * 6);
@@ -1034,15 +1285,60 @@ int mpm_return_map_learned(mpm_surrogate* s, int64_t n, const double* F_in, cons
     counts->learned = hc.learned;
     counts->fallback = hc.fallback;
   }
-  return MPM_OK;
+  return check_tc(s);
 }
 
 // Timing of the gated map against the exact map on n device-resident random trial states.
+static int time_jc(mpm_surrogate* s, const mpm_surrogate_config* cfg, int64_t n, int32_t iters, double gate_tol,
+                   double* ms_exact, double* ms_learned, mpm_gate_counts* counts) {
+  const surr::SampleSpec sp = spec_of(cfg);
+  const int newton = cfg->newton > 0 ? cfg->newton : 4;
+  float* dep = nullptr;
+  surr::GateOut* dc = nullptr;
+  SCUDA(s, cudaMalloc(&dep, n * sizeof(float)));
+  SCUDA(s, cudaMalloc(&dc, sizeof(surr::GateOut)));
+  const int blocks = (int)std::min<long long>(s->num_sms * 8, (n + 255) / 256);
+  cudaEvent_t ev[4];
+  for (auto& x : ev) cudaEventCreate(&x);
+  cudaError_t e = cudaMemsetAsync(dc, 0, sizeof(surr::GateOut), s->stream);
+  for (int mode = 0; mode < 2 && e == cudaSuccess; ++mode) {
+    for (int w = 0; w < 2; ++w)
+      surr::k_gated_jc<<<blocks, 256, 0, s->stream>>>(s->wbf, s->params, s->mt, sp, (float)gate_tol, newton, mode, n,
+                                                      dep, nullptr);
+    cudaEventRecord(ev[2 * mode], s->stream);
+    for (int it = 0; it < iters; ++it)
+      surr::k_gated_jc<<<blocks, 256, 0, s->stream>>>(s->wbf, s->params, s->mt, sp, (float)gate_tol, newton, mode, n,
+                                                      dep, (mode == 1 && it == 0) ? dc : nullptr);
+    cudaEventRecord(ev[2 * mode + 1], s->stream);
+    e = cudaGetLastError();
+  }
+  surr::GateOut hc{};
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&hc, dc, sizeof hc, cudaMemcpyDeviceToHost, s->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+  float t0 = 0, t1 = 0;
+  if (e == cudaSuccess) {
+    cudaEventElapsedTime(&t0, ev[0], ev[1]);
+    cudaEventElapsedTime(&t1, ev[2], ev[3]);
+  }
+  for (auto& x : ev) cudaEventDestroy(x);
+  cudaFree(dep);
+  cudaFree(dc);
+  if (e != cudaSuccess) return sfail(s, MPM_ERR_CUDA, cudaGetErrorString(e));
+  *ms_exact = t0 / iters;
+  *ms_learned = t1 / iters;
+  if (counts) {
+    counts->elastic = hc.elastic;
+    counts->learned = hc.learned;
+    counts->fallback = hc.fallback;
+  }
+  return MPM_OK;
+}
+
 int mpm_surrogate_time(mpm_surrogate* s, const mpm_surrogate_config* cfg, int64_t n, int32_t iters, double gate_tol,
                        double* ms_exact, double* ms_learned, mpm_gate_counts* counts) {
   if (!s || !cfg || n <= 0 || iters <= 0 || !ms_exact || !ms_learned) return MPM_ERR_INVALID_ARG;
-  surr::SampleSpec sp{(float)cfg->strain_min, (float)cfg->strain_max, (float)cfg->T_min, (float)cfg->T_max,
-                      (float)cfg->ep_max, cfg->seed};
+  if (is_jc(s)) return time_jc(s, cfg, n, iters, gate_tol, ms_exact, ms_learned, counts);
+  const surr::SampleSpec sp = spec_of(cfg);
   float *X = nullptr, *Y = nullptr, *dD = nullptr, *de = nullptr, *dT = nullptr, *dFo = nullptr, *ddep = nullptr,
         *dtau = nullptr;
   surr::GateOut* dc = nullptr;
@@ -1057,19 +1353,20 @@ int mpm_surrogate_time(mpm_surrogate* s, const mpm_surrogate_config* cfg, int64_
   SCUDA(s, cudaMalloc(&dc, sizeof(surr::GateOut)));
   surr::k_samples<<<s->num_sms * 8, 256, 0, s->stream>>>(s->mt, s->sc, sp, n, X, Y, dD, de, dT);
   cudaError_t e = cudaGetLastError();
-  const int blocks = (int)std::min<long long>(s->num_sms * 4, (n + surr::kGateThreads - 1) / surr::kGateThreads);
+  const int blocks = (int)std::min<long long>(s->num_sms * 2, (n + surr::kGateThreads - 1) / surr::kGateThreads);
   cudaEvent_t ev[4];
   for (auto& x : ev) cudaEventCreate(&x);
   for (int mode = 0; mode < 2 && e == cudaSuccess; ++mode) {
     for (int w = 0; w < 2; ++w)
       surr::k_gated<<<blocks, surr::kGateThreads, sizeof(surr::GateSmem), s->stream>>>(
-          s->wbf, s->params, s->mt, s->sc, (float)gate_tol, mode, n, dD, de, dT, dFo, ddep, dtau, nullptr, nullptr);
+          s->wbf, s->params, s->mt, s->sc, (float)gate_tol, mode, n, dD, de, dT, dFo, ddep, dtau, nullptr, nullptr,
+          s->tc_err);
     cudaMemsetAsync(dc, 0, sizeof(surr::GateOut), s->stream);
     cudaEventRecord(ev[2 * mode], s->stream);
     for (int it = 0; it < iters; ++it)
       surr::k_gated<<<blocks, surr::kGateThreads, sizeof(surr::GateSmem), s->stream>>>(
           s->wbf, s->params, s->mt, s->sc, (float)gate_tol, mode, n, dD, de, dT, dFo, ddep, dtau, nullptr,
-          it == 0 ? dc : nullptr);
+          it == 0 ? dc : nullptr, s->tc_err);
     cudaEventRecord(ev[2 * mode + 1], s->stream);
     e = cudaGetLastError();
   }
@@ -1092,7 +1389,25 @@ int mpm_surrogate_time(mpm_surrogate* s, const mpm_surrogate_config* cfg, int64_
     counts->learned = hc.learned;
     counts->fallback = hc.fallback;
   }
-  return MPM_OK;
+  return check_tc(s);
 }
 
 }  // extern "C"
+
+namespace surr {
+
+int surrogate_model(const mpm_surrogate* s) { return s ? s->mat.model : -1; }
+
+size_t weights_bytes() { return sizeof(WeightsBf16); }
+
+int export_weights(mpm_surrogate* s, void* dst_w, float* dst_params, cudaStream_t st) {
+  if (!s || !dst_w || !dst_params) return MPM_ERR_INVALID_ARG;
+  // the surrogate's own stream finishes its pending updates first
+  if (cudaStreamSynchronize(s->stream) != cudaSuccess) return MPM_ERR_CUDA;
+  if (cudaMemcpyAsync(dst_w, s->wbf, sizeof(WeightsBf16), cudaMemcpyDeviceToDevice, st) != cudaSuccess ||
+      cudaMemcpyAsync(dst_params, s->params, kParams * sizeof(float), cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+    return MPM_ERR_CUDA;
+  return MPM_OK;
+}
+
+}  // namespace surr

@@ -79,8 +79,9 @@ class MpmTuning(ctypes.Structure):
 
 class MpmSurrogateConfig(ctypes.Structure):
     _fields_ = [("samples", _I64), ("batch", _I32), ("steps", _I32), ("lr", _D), ("weight_decay", _D),
-                ("dep_weight", _D), ("cosine", _I32), ("reserved", _I32), ("seed", ctypes.c_uint64),
-                ("strain_min", _D), ("strain_max", _D), ("T_min", _D), ("T_max", _D), ("ep_max", _D)]
+                ("dep_weight", _D), ("cosine", _I32), ("newton", _I32), ("seed", ctypes.c_uint64),
+                ("strain_min", _D), ("strain_max", _D), ("T_min", _D), ("T_max", _D), ("ep_max", _D),
+                ("dt_min", _D), ("dt_max", _D)]
 
 
 class MpmGateCounts(ctypes.Structure):
@@ -89,6 +90,7 @@ class MpmGateCounts(ctypes.Structure):
 
 
 SURROGATE_PARAMS = 5768
+RETURN_EXACT, RETURN_LEARNED_GATED = 0, 1
 
 
 class MpmFrameInfo(ctypes.Structure):
@@ -186,6 +188,8 @@ SIGNATURES = {
                                                ctypes.POINTER(MpmGateCounts)]),
     "mpm_surrogate_time": (ctypes.c_int, [_P, ctypes.POINTER(MpmSurrogateConfig), _I64, _I32, _D, ctypes.POINTER(_D),
                                            ctypes.POINTER(_D), ctypes.POINTER(MpmGateCounts)]),
+    "mpm_set_return_mode": (ctypes.c_int, [_P, _I32, _P, _D, _I32]),
+    "mpm_gate_counts_read": (ctypes.c_int, [_P, ctypes.POINTER(MpmGateCounts), _I32]),
     "smpm_create": (ctypes.c_int, [_I64, ctypes.POINTER(_P)]),
     "smpm_destroy": (ctypes.c_int, [_P]),
     "smpm_last_error": (ctypes.c_char_p, [_P]),

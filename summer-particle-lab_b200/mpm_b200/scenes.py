@@ -11,7 +11,8 @@ sizes and value distributions (no external dataset is involved):
   elastic_cube         13,824-particle fixed-corotated block on a 32^3 grid
   j2_drop              J2 linear-hardening block (64x32x64 or 64x64x64 cells, 8 ppc) on 128^3
   thermal_j2           thermal-softening J2 block (80^3 cells, 4,096,000 particles) on 160^3
-  ensemble             256 independent J2 scenes of uneven particle and grid counts
+  ensemble             256 independent J2 scenes of uneven particle and grid counts (or Johnson-Cook)
+  jc_impact            Johnson-Cook block (64^3 cells, 8 ppc, 2,097,152 particles) hitting the floor at 60 m/s
   coupled_collision    two thermal J2 blocks colliding at +-20 m/s on 256^3 (16.8M particles)
 """
 from dataclasses import dataclass, field
@@ -20,7 +21,7 @@ import math
 import numpy as np
 
 from .params import Domain, Material, FIXED_ONE, MODEL_FIXED_COROTATED, MODEL_J2, \
-    MODEL_J2_HARDENING, MODEL_THERMAL_J2
+    MODEL_J2_HARDENING, MODEL_JOHNSON_COOK_SIMPLE, MODEL_THERMAL_J2
 
 _M32 = np.uint64(0xFFFFFFFF)
 
@@ -140,6 +141,29 @@ def j2_drop(shape=(64, 64, 64), seed=2, grid=128, plastic=False):
                   meta=dict(dt=2e-6, steps=1000, workload=f"{name}_{n}_{sx}x{sy}x{sz}_grid{grid}"))
 
 
+def johnson_cook_metal(model=MODEL_JOHNSON_COOK_SIMPLE, E=70e9, nu=0.33, yield_stress=250e6, density=2700.0, **kw):
+    """Johnson-Cook metal: A = yield_stress, B = A, n = 0.35, C = 0.025, rate0 = 1/s (the reference's
+    ratios, src/three/metal-plasticity.js:3), temperatures in K for model 6 (T_ref 293, T_melt 933)."""
+    kw.setdefault("hardening", yield_stress)
+    return Material.from_young(model, E, nu, density=density, yield_stress=yield_stress, jc_n=0.35, jc_C=0.025,
+                               jc_rate0=1.0, T_ref=293.0, T_melt=933.0, jc_m=1.0, **kw)
+
+
+def jc_impact(shape=(64, 64, 64), seed=4, grid=128, model=MODEL_JOHNSON_COOK_SIMPLE, v0=-60.0):
+    """Johnson-Cook block of 8 ppc on a 128^3 grid resting on the floor, moving down at 60 m/s: a
+    plastic impact whose returns run the reference's 24-halving bisection (the law the learned
+    return map is built for). Requested dt 2e-6 s sub-stepped to CFL 0.4."""
+    d = Domain(lower=(0, 0, 0), upper=(1, 1, 1), H=1 / grid, gravity=(0, -9.8, 0), sticky_floor=True)
+    sx, sy, sz = shape
+    x0 = (grid - sx) // 2
+    z0 = (grid - sz) // 2
+    x = block_particles(d, (x0, 1, z0), (x0 + sx, 1 + sy, z0 + sz), seed)
+    n = x.shape[0]
+    T = np.full(n, 293.0) if model == 6 else None
+    return _scene("jc_impact", d, [johnson_cook_metal(model)], x, (0, v0, 0), T=T,
+                  meta=dict(dt=2e-6, steps=1000, workload=f"jc_impact_{n}_{sx}x{sy}x{sz}_grid{grid}"))
+
+
 def thermal_j2(seed=3, grid=160, block=80, v0=-20.0):
     """Thermal-softening J2: dsigma_y/dT = -0.3 MPa/K from T_ref = 293 K restated as model 10 with
     hot_ratio 0.001 (T_hot = T_ref + 0.999 * 250e6 / 0.3e6), T0 ~ U[293, 600] K from the hash,
@@ -189,7 +213,7 @@ def coupled_collision(scale=1, seed=5):
     return s
 
 
-def ensemble(count=256, seed0=1000, steps=500):
+def ensemble(count=256, seed0=1000, steps=500, model=MODEL_J2):
     """Independent J2 scenes: N_p log-uniform in [5e3, 2e5], grid side U{32..96} cells over a unit
     cube, E log-uniform [1e4, 1e11] Pa, nu U[0.2, 0.45], yield log-uniform [1e3, 5e8] Pa, rho=1000,
     ideal J2. The block is a centred cube of N_p/8 cells (clamped to 3/4 of the grid side) whose
@@ -208,7 +232,10 @@ def ensemble(count=256, seed0=1000, steps=500):
         side = max(4, min(int(round((n_p / 8) ** (1 / 3))), (3 * grid) // 4))
         d = Domain(lower=(0, 0, 0), upper=(1, 1, 1), H=1 / grid, gravity=(0, -9.8, 0),
                    sticky_floor=True)
-        mat = Material.from_young(MODEL_J2, E, nu, density=1000.0, yield_stress=sy)
+        if model == MODEL_JOHNSON_COOK_SIMPLE:  # the same draws as a Johnson-Cook law (B = A)
+            mat = johnson_cook_metal(model, E, nu, yield_stress=sy, density=1000.0)
+        else:
+            mat = Material.from_young(model, E, nu, density=1000.0, yield_stress=sy)
         c0 = (grid - side) // 2
         y0 = max(1, min(grid // 4, grid - side - 2))
         x = block_particles(d, (c0, y0, c0), (c0 + side, y0 + side, c0 + side), seed)
@@ -239,6 +266,7 @@ def translation_block(phase=0.0, velocity=(2.0, 0.0, 0.0)):
 
 WORKLOADS = {
     "elastic_cube": elastic_cube,
+    "jc_impact": jc_impact,
     "j2_drop": j2_drop,
     "thermal_j2": thermal_j2,
     "coupled_collision": coupled_collision,

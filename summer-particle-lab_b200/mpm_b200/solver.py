@@ -258,6 +258,21 @@ class Solver:
         """One regularisation pass now (regularizeSolids(s, dt) after a step)."""
         self._check(_lib.lib().mpm_regularize(self.h, float(dt)))
 
+    def set_return_mode(self, surrogate=None, gate_tol=1e-5, newton=4):
+        """Learned return map inside the step (mpm_set_return_mode) with a Johnson-Cook network, or
+        the exact map again with surrogate None."""
+        if surrogate is None:
+            self._check(_lib.lib().mpm_set_return_mode(self.h, _lib.RETURN_EXACT, None, 0.0, 0))
+        else:
+            self._check(_lib.lib().mpm_set_return_mode(self.h, _lib.RETURN_LEARNED_GATED, surrogate.h, float(gate_tol),
+                                                       int(newton)))
+
+    def gate_counts(self, reset=False):
+        """(returns served by the network, returns sent to the exact map) since the last reset."""
+        c = _lib.MpmGateCounts()
+        self._check(_lib.lib().mpm_gate_counts_read(self.h, ctypes.byref(c), 1 if reset else 0))
+        return c.learned, c.fallback
+
     def autotune(self, trial_substeps=8):
         t = MpmTuning()
         self._check(_lib.lib().mpm_batch_autotune(self.h, int(trial_substeps), ctypes.byref(t)))

@@ -3,7 +3,9 @@
 The network and its training run on the device through the C ABI; this module only moves numpy
 arrays across it. Defaults follow the thermo-elastoplastic configuration the map is built for:
 trial principal log strains log-uniform in [1e-5, 5e-2] with random principal directions,
-temperature uniform in [293, 600] K and plastic strain uniform in [0, 0.2].
+temperature uniform in [293, 600] K and plastic strain uniform in [0, 0.2]. Networks for the
+Johnson-Cook laws (models 6, 7) train on jc_config() draws and serve the fused step through
+Solver.set_return_mode (mpm_set_return_mode).
 """
 import ctypes
 
@@ -17,10 +19,23 @@ _P = ctypes.c_void_p
 
 
 def config(samples=10_000_000, batch=16384, steps=30000, lr=2e-3, weight_decay=0.0, dep_weight=4.0, cosine=True, seed=31,
-           strain_min=1e-5, strain_max=5e-2, T_min=293.0, T_max=600.0, ep_max=0.2):
+           strain_min=1e-5, strain_max=5e-2, T_min=293.0, T_max=600.0, ep_max=0.2, dt_min=0.0, dt_max=0.0, newton=0):
     return MpmSurrogateConfig(samples=samples, batch=batch, steps=steps, lr=lr, weight_decay=weight_decay,
                               dep_weight=dep_weight, cosine=1 if cosine else 0, seed=seed, strain_min=strain_min,
-                              strain_max=strain_max, T_min=T_min, T_max=T_max, ep_max=ep_max)
+                              strain_max=strain_max, T_min=T_min, T_max=T_max, ep_max=ep_max, dt_min=dt_min,
+                              dt_max=dt_max, newton=newton)
+
+
+def jc_config(samples=4_000_000, batch=16384, steps=8000, lr=2e-3, seed=37, strain_min=1e-4, strain_max=5e-2,
+              T_min=293.0, T_max=700.0, ep_max=0.5, dt_min=1e-8, dt_max=1e-5, newton=4):
+    """Training and timing draws for a Johnson-Cook network: deviatoric trial log strains log-uniform
+    in [strain_min, strain_max] (every other draw a trial stress just above the initial flow stress),
+    plastic strain uniform in [0, ep_max], temperature uniform in [T_min, T_max] (model 6 softening),
+    substeps log-uniform in [dt_min, dt_max]; the target is the consistency root of the reference's
+    bisection (only plastic states weigh in the loss)."""
+    return config(samples=samples, batch=batch, steps=steps, lr=lr, seed=seed, strain_min=strain_min,
+                  strain_max=strain_max, T_min=T_min, T_max=T_max, ep_max=ep_max, dt_min=dt_min, dt_max=dt_max,
+                  newton=newton)
 
 
 def _f32(a, shape):

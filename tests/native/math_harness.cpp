@@ -112,3 +112,34 @@ extern "C" void harness_eig(int n, const double* S6, double* lam, double* U) {
     for (int k = 0; k < 9; ++k) U[i * 9 + k] = u[k];
   }
 }
+
+// The learned Johnson-Cook return's refinement and gate (mpm::jc_refine), the exact bisection
+// (mpm::jc_bisect) and the network inputs (mpm::jc_features) on trial states (q, J, ep, T, dt):
+// prm as harness_constitutive_full. ok[i] = 1 when the gate accepts the refined prediction u_pred[i].
+extern "C" void harness_jc_refine(int model, const double* prm, int n, const double* q, const double* J,
+                                  const double* ep, const double* T, const double* dt, const double* u_pred,
+                                  double tol, int newton, int* ok, double* dep_learned, double* dep_exact,
+                                  double* features) {
+  mpm::MaterialDev m{};
+  m.model = model;
+  m.mu = (float)prm[0];
+  m.lam = (float)prm[1];
+  m.yield_stress = (float)prm[2];
+  m.hardening = (float)prm[3];
+  m.T_ref = (float)prm[4];
+  m.jc_n = (float)prm[7];
+  m.jc_C = (float)prm[8];
+  m.jc_inv_rate0 = prm[9] > 0 ? (float)(1.0 / prm[9]) : 0.f;
+  m.jc_inv_T_span = prm[10] > prm[4] ? (float)(1.0 / (prm[10] - prm[4])) : 0.f;
+  m.jc_m = (float)prm[11];
+  for (int i = 0; i < n; ++i) {
+    float d = 0.f;
+    ok[i] = mpm::jc_refine(m, (float)q[i], (float)J[i], (float)ep[i], (float)T[i], (float)dt[i], (float)u_pred[i],
+                           (float)tol, newton, d) ? 1 : 0;
+    dep_learned[i] = d;
+    dep_exact[i] = mpm::plastic_increment(m, (float)q[i], (float)J[i], (float)ep[i], (float)T[i], (float)dt[i]);
+    float x[8];
+    mpm::jc_features(m, (float)q[i], (float)J[i], (float)ep[i], (float)T[i], (float)dt[i], x);
+    for (int k = 0; k < 8; ++k) features[i * 8 + k] = x[k];
+  }
+}

@@ -221,3 +221,55 @@ def test_norton_creep_matches_oracle(harness):
     _, dep, _ = _full(harness, lin, .01, [F], 0.0, 20.0)
     Fo_ref, inc_ref, _ = orc.project(F, orc.material_from(lin), ep=0.0, dt=.01, T=20.0)
     assert abs(dep[0] - inc_ref) <= 1e-6 + 1e-4 * inc_ref
+
+
+def jc_prm(mat):
+    return np.array([mat.mu, mat.lam, mat.yield_stress, mat.hardening, mat.T_ref, mat.T_hot, mat.hot_ratio, mat.jc_n,
+                     mat.jc_C, mat.jc_rate0, mat.T_melt, mat.jc_m, 0, 0, 1, 1, 0], dtype=np.float64)
+
+
+@pytest.mark.parametrize("model", [6, 7])
+def test_learned_johnson_cook_gate_against_the_oracle(harness, model):
+    """The learned Johnson-Cook return's refinement and gate (the device math on the host): from a
+    guess within 20% of the root, at most four Newton steps reach the gate (consistency residual
+    <= 1e-5 of the trial stress), including roots just past the rate term's kink, and every
+    accepted increment satisfies the FP64 oracle's consistency condition
+    (src/three/metal-plasticity.js:28-34) to that bound plus FP32 rounding,
+    |q - 3 mu / J dep - flow(ep + dep, dep / dt, T)| <= 2e-5 q, and agrees with the exact bisection.
+    A guess the gate cannot vouch for (no Newton steps from a wrong root) is rejected."""
+    from mpm_b200 import scenes
+    mat = scenes.johnson_cook_metal(model)
+    om = orc.material_from(mat)
+    rng = np.random.default_rng(12)
+    n = 400
+    J = np.exp(rng.uniform(-0.01, 0.01, n))
+    ep = rng.uniform(0, 0.4, n)
+    T = rng.uniform(293, 700, n)
+    dt = np.exp(rng.uniform(np.log(1e-8), np.log(1e-5), n))
+    flow0 = np.array([orc.flow_stress(model, e, 0.0, t, om) for e, t in zip(ep, T)])
+    q = flow0 * (1 + np.exp(rng.uniform(np.log(1e-3), np.log(3.0), n)))
+    L = harness
+    L.harness_jc_refine.argtypes = [ctypes.c_int, P, ctypes.c_int, P, P, P, P, P, P, ctypes.c_double, ctypes.c_int,
+                                    P, P, P, P]
+    c = lambda a: a.ctypes.data_as(P)
+    prm = jc_prm(mat)
+
+    def refine(u, newton):
+        ok = np.zeros(n, np.int32)
+        dl, de, feat = np.zeros(n), np.zeros(n), np.zeros((n, 8))
+        L.harness_jc_refine(model, c(prm), n, c(q), c(J), c(ep), c(T), c(dt), c(np.ascontiguousarray(u)), 1e-5, newton,
+                            c(ok), c(dl), c(de), c(feat))
+        return ok.astype(bool), dl, de, feat
+
+    s = q * J / (3 * mat.mu)
+    _, _, dep_exact, feat = refine(np.full(n, 0.5), 0)
+    u_exact = dep_exact / s
+    assert np.all((feat[:, 0] > 0) & (feat[:, 0] <= 1))  # A soft / q of a plastic state
+    ok, dl, _, _ = refine(u_exact * rng.uniform(0.8, 1.2, n), 4)
+    assert ok.mean() >= 0.98, ok.mean()
+    for i in np.flatnonzero(ok):
+        r = q[i] - 3 * mat.mu / J[i] * dl[i] - orc.flow_stress(model, ep[i] + dl[i], dl[i] / dt[i], T[i], om)
+        assert abs(r) <= 2e-5 * q[i], (i, r / q[i])
+        assert abs(dl[i] - dep_exact[i]) <= 2e-5 * s[i] + 1e-4 * dep_exact[i], i
+    bad, _, _, _ = refine(np.clip(u_exact * 3 + 0.3, 0, 1), 0)
+    assert bad.mean() <= 0.05
