@@ -2178,6 +2178,7 @@ int mpm_batch_create(const mpm_scene_desc* scenes, int32_t nscenes, mpm_handle**
   }
   h->scenes = list;
   h->batch = true;
+  h->ctx.scene_material = 1;  // each particle takes its scene's material
   h->dom = scenes[0].domain;
   rc = alloc_grid(h);
   if (rc == MPM_OK && cudaStreamSynchronize(h->stream) != cudaSuccess) rc = MPM_ERR_CUDA;

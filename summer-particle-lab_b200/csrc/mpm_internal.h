@@ -153,6 +153,7 @@ struct Ctx {
   int total_node_tiles;
   int has_pinned;
   int single_material;
+  int scene_material;   // every particle has its scene's material (batch handles): one row per tile
   int has_thermal;      // temperature array is read and written
   int has_plastic;      // plastic strain array is read and written
   int has_aux;          // aux array is read and written (a snow, sand or pressure material is set)

@@ -1306,7 +1306,7 @@ __device__ __forceinline__ void prefetch_tile_state(const Ctx& c, uint4 it) {
   if (c.has_plastic) pf(c.p.ep, 4);
   if (c.has_thermal) pf(c.p.T, 4);
   if (AUX) pf(c.p.aux, 4);
-  if (!c.single_material) pf(c.p.mat, 2);
+  if (!c.single_material && !c.scene_material) pf(c.p.mat, 2);
   if (c.has_pinned) pf(c.p.pinned, 1);
 }
 
@@ -1412,9 +1412,10 @@ __global__ void __launch_bounds__(kBlock, 2) k_particles(const __grid_constant__
       tl.mat = sc.mat_base;
       sm.tc = tl;
     }
-    // the material row of a single-material scene, copied word by word by the whole block, and
-    // only when it changes (every tile of a one-scene handle shares it)
-    if (c.single_material && sc.mat_base != mt_row) {
+    // the material row of a single-material handle or of the tile's scene in a batch, copied word
+    // by word by the whole block, and only when it changes (every tile of a one-scene handle shares
+    // it; a batch's tiles come scene by scene)
+    if ((c.single_material || c.scene_material) && sc.mat_base != mt_row) {
       static_assert(sizeof(MaterialDev) % 4 == 0, "word copy");
       const unsigned* src = reinterpret_cast<const unsigned*>(c.mats + sc.mat_base);
       unsigned* dst = reinterpret_cast<unsigned*>(&sm.mt);
@@ -1434,7 +1435,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_particles(const __grid_constant__
     }
     const TileCtx& tc = sm.tc;
     const float dt = GATHER ? c.dt_scene[scene] : 0.f;
-    const bool single = c.single_material != 0;
+    const bool single = c.single_material != 0 || c.scene_material != 0;
     float wave_acc = 0.f, grad_acc = 0.f;
     unsigned flags_acc = 0;
     for (unsigned r0 = 0; r0 < it.z; r0 += kCap) {
@@ -1650,7 +1651,7 @@ __global__ void __launch_bounds__(kWsThreads, 1) k_particles_ws(const __grid_con
     int s = 0, cb = 0;
     unsigned uses[2] = {0u, 0u}, pe[2] = {0u, 0u}, tph[2] = {0u, 0u};
     bool in_flight[2] = {tid == 0 && use_tma && sm.item[0].x != 0xffffffffu, false};  // thread 0's TMA copies
-    const bool single = c.single_material != 0;
+    const bool single = c.single_material != 0 || c.scene_material != 0;
     bool stop = false;
     while (!stop) {
       group_sync(1);

@@ -7,7 +7,8 @@ x within 1e-6 m, F within 2e-6, plastic strain within 2e-6 + 1e-4 max ep after t
 gate accepts a refined prediction only when its consistency residual is at most gate_tol (1e-5) of
 the trial stress, so the learned step carries the same stated stress error as the exact one.
 What the trained network gains over the method without it: the share of plastic returns it serves
-(the rest run the bisection), against an untrained network of the same shape.
+(the rest run the bisection), against an untrained network of the same shape (about 98% against
+about half in the impact).
 """
 import numpy as np
 import pytest
@@ -68,13 +69,14 @@ def test_learned_step_matches_oracle_and_serves_most_returns(trained):
     out, (learned, fallback) = run(sc, trained)
     check_parity(out, st)
     assert learned + fallback > 500
-    assert learned >= 0.6 * (learned + fallback), (learned, fallback)
+    assert learned >= 0.8 * (learned + fallback), (learned, fallback)
 
 
-def test_untrained_network_gains_nothing_and_stays_exact():
+def test_untrained_network_serves_fewer_returns_and_stays_exact(trained):
     """The same gate with an untrained network: the step is still within the oracle bounds (the gate
-    sends what it cannot vouch for to the bisection), and the network serves far fewer returns than
-    the trained one."""
+    sends what it cannot vouch for to the bisection). The Newton refinement alone carries about half
+    the returns through the gate from an untrained guess; the trained network raises that share to
+    nearly all of them (what the network gains over the method without it)."""
     s = Surrogate(scenes.johnson_cook_metal(7), seed=3)
     sc = impact_scene()
     st = oracle_run(sc)
@@ -82,7 +84,9 @@ def test_untrained_network_gains_nothing_and_stays_exact():
     s.close()
     check_parity(out, st)
     assert learned + fallback > 500
-    assert learned <= 0.3 * (learned + fallback), (learned, fallback)
+    _, (lt, ft) = run(sc, trained)
+    share_untrained, share_trained = learned / (learned + fallback), lt / (lt + ft)
+    assert share_trained >= share_untrained + 0.25, (share_untrained, share_trained)
 
 
 def test_exact_mode_restores_the_reference_map(trained):
@@ -142,4 +146,4 @@ def test_kernel_level_timing_reports_counts(trained):
     assert r["ms_exact"] > 0 and r["ms_learned"] > 0
     plastic = r["learned"] + r["fallback"]
     assert plastic > 100_000
-    assert r["learned"] >= 0.7 * plastic, r
+    assert r["learned"] >= 0.8 * plastic, r
