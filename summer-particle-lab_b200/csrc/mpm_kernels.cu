@@ -888,10 +888,19 @@ __device__ __forceinline__ float gather_w27(Ld ld, const float w[3][3]) {
   return sz;
 }
 
-// Gather straight from global memory (a particle whose stencil is outside the staged window).
-__device__ __noinline__ void gather_global(const float4* base, int sy, long long sz, const float t[3], const float w[3][3],
-                                           float out[12]) {
-  gather27([&](int kz, int ky, int kx) { return base[kz * sz + ky * sy + kx]; }, t, w, out);
+// Gather straight from global memory (a particle whose stencil is outside the staged window). The
+// fractions come by value and the result returns by value, so the caller's arrays keep no address.
+struct Gather12 {
+  float v[12];
+};
+__device__ __noinline__ Gather12 gather_global(const float4* base, int sy, long long sz, float t0, float t1, float t2) {
+  const float t[3] = {t0, t1, t2};
+  float w[3][3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) bspline_weights(t[a], w[a]);
+  Gather12 g;
+  gather27([&](int kz, int ky, int kx) { return base[kz * sz + ky * sy + kx]; }, t, w, g.v);
+  return g;
 }
 
 // Phase A of one particle (home slot `home`, payload row j): G2P from the staged window, F update,
@@ -913,7 +922,7 @@ __device__ __forceinline__ unsigned particle_phase_a(const Ctx& c, const SceneDe
 #pragma unroll
   for (int e = 0; e < 9; ++e) D[e] = c.p.Dc[e][home];
   const float m = c.p.m[home], V = c.p.V[home];
-  const MaterialDev mt = single ? mt_single : c.mats[c.p.mat[home]];
+  const MaterialDev& mt = single ? mt_single : c.mats[c.p.mat[home]];
   const MaterialExt* xp = AUX ? &c.mats_ext[single ? tc.mat : c.p.mat[home]] : nullptr;
   const bool pinned = c.has_pinned && c.p.pinned[home];
   float ep = c.has_plastic ? c.p.ep[home] : 0.f;
@@ -941,8 +950,10 @@ __device__ __forceinline__ unsigned particle_phase_a(const Ctx& c, const SceneDe
       const float4* win = &vwin[(l2 * kWinG + l1) * kWinG + l0];
       gather27([&](int kz, int ky, int kx) { return win[(kz * kWinG + ky) * kWinG + kx]; }, t, w, acc12);
     } else {
-      gather_global(c.g.vel + tc.node_base + ((long long)b[2] * tc.gdim[1] + b[1]) * tc.gdim[0] + b[0], tc.gdim[0],
-                    (long long)tc.gdim[0] * tc.gdim[1], t, w, acc12);
+      const Gather12 g = gather_global(c.g.vel + tc.node_base + ((long long)b[2] * tc.gdim[1] + b[1]) * tc.gdim[0] + b[0],
+                                       tc.gdim[0], (long long)tc.gdim[0] * tc.gdim[1], t[0], t[1], t[2]);
+#pragma unroll
+      for (int e = 0; e < 12; ++e) acc12[e] = g.v[e];
     }
     // grid heat conduction: the node temperature increments, interpolated like the velocity, and
     // relaxation of the particle's offset from the interpolated node temperature at the rate of the
@@ -1110,7 +1121,7 @@ __device__ __forceinline__ unsigned particle_phase_a_learned(const Ctx& c, const
 #pragma unroll
   for (int e = 0; e < 9; ++e) D[e] = c.p.Dc[e][home];
   const float m = c.p.m[home], V = c.p.V[home];
-  const MaterialDev mt = single ? mt_single : c.mats[c.p.mat[home]];
+  const MaterialDev& mt = single ? mt_single : c.mats[c.p.mat[home]];
   const bool pinned = c.has_pinned && c.p.pinned[home];
   float ep = c.has_plastic ? c.p.ep[home] : 0.f;
   float T = c.has_thermal ? c.p.T[home] : 0.f;
@@ -1136,8 +1147,10 @@ __device__ __forceinline__ unsigned particle_phase_a_learned(const Ctx& c, const
       const float4* win = &vwin[(l2 * kWinG + l1) * kWinG + l0];
       gather27([&](int kz, int ky, int kx) { return win[(kz * kWinG + ky) * kWinG + kx]; }, t, w, acc12);
     } else {
-      gather_global(c.g.vel + tc.node_base + ((long long)b[2] * tc.gdim[1] + b[1]) * tc.gdim[0] + b[0], tc.gdim[0],
-                    (long long)tc.gdim[0] * tc.gdim[1], t, w, acc12);
+      const Gather12 g = gather_global(c.g.vel + tc.node_base + ((long long)b[2] * tc.gdim[1] + b[1]) * tc.gdim[0] + b[0],
+                                       tc.gdim[0], (long long)tc.gdim[0] * tc.gdim[1], t[0], t[1], t[2]);
+#pragma unroll
+      for (int e = 0; e < 12; ++e) acc12[e] = g.v[e];
     }
     const float s4 = 4.f * tc.invH;
     v[0] = acc12[0]; v[1] = acc12[1]; v[2] = acc12[2];

@@ -431,7 +431,7 @@ MPM_HD float hencky_strain(float beta) {
 
 // Large-strain path (|B| > 0.15): Jacobi eigen-decomposition of B. Out of line so its registers do
 // not count against the series path that almost every particle takes.
-MPM_NOINLINE ConstitutiveOut constitutive_eigen(const MaterialDev& mt, const Sym3& B, float D[9], float ep,
+MPM_NOINLINE ConstitutiveOut constitutive_eigen(const MaterialDev& mt, Sym3 B, float D[9], float ep,
                                                 float T, float inv_rho0, bool do_return, float dt) {
   ConstitutiveOut out;
   out.dep = 0.f;
@@ -502,7 +502,7 @@ MPM_NOINLINE ConstitutiveOut constitutive_eigen(const MaterialDev& mt, const Sym
 // Always on the eigen-decomposition: the snow clamp acts per principal stretch, and these laws
 // are not on the benchmark path whose registers the series path keeps small. Without the law's
 // constants (xp null) only the stress of the stored state is available (no return).
-MPM_NOINLINE ConstitutiveOut constitutive_pressure(const MaterialDev& mt, const MaterialExt* xp, const Sym3& B,
+MPM_NOINLINE ConstitutiveOut constitutive_pressure(const MaterialDev& mt, const MaterialExt* xp, Sym3 B,
                                                    float D[9], float ep, float& aux, bool do_return) {
   if (!xp) do_return = false;
   const MaterialExt none{};
