@@ -608,7 +608,7 @@ __global__ void __launch_bounds__(256) k_forward(const WeightsBf16* wg, const fl
 // r; when a tile holds a plastic particle the network runs as three tcgen05 GEMMs (M = 128) with
 // the epilogues of k_train_tc's forward pass.
 constexpr int kGateThreads = 128;
-constexpr int kGateTmemCols = 256;  // H1 columns 0..63, H2 64..127, Y 128..143
+constexpr int kGateTmemCols = 128;  // H1 and then H2 in columns 0..63 (H1 is read before H2 lands), Y 64..79
 
 struct __align__(1024) GateSmem {
   __nv_bfloat16 w1[64 * 16];
@@ -689,22 +689,22 @@ __global__ void __launch_bounds__(kGateThreads) k_gated(const WeightsBf16* wg, c
             st_pair(sm.h1, km_off(r, 16 * c + j, 64), fmaxf(v[j] + sm.bias[16 * c + j], 0.f),
                     fmaxf(v[j + 1] + sm.bias[16 * c + j + 1], 0.f));
         }
-        tc_ok = tc_run(&sm.mbar, phase, [&] { tc_gemm(tm + 64, sm.h1, sm.w2, 64, 64, false); });
+        tc_ok = tc_run(&sm.mbar, phase, [&] { tc_gemm(tm + 0, sm.h1, sm.w2, 64, 64, false); });
       }
       if (tc_ok) {
 #pragma unroll
         for (int c = 0; c < 4; ++c) {
           float v[16];
-          tmem_ld16(tm + lane + 64 + 16 * c, v);
+          tmem_ld16(tm + lane + 16 * c, v);
 #pragma unroll
           for (int j = 0; j < 16; j += 2)
             st_pair(sm.h2, km_off(r, 16 * c + j, 64), fmaxf(v[j] + sm.bias[64 + 16 * c + j], 0.f),
                     fmaxf(v[j + 1] + sm.bias[64 + 16 * c + j + 1], 0.f));
         }
-        tc_ok = tc_run(&sm.mbar, phase, [&] { tc_gemm(tm + 128, sm.h2, sm.w3, 64, 16, false); });
+        tc_ok = tc_run(&sm.mbar, phase, [&] { tc_gemm(tm + 64, sm.h2, sm.w3, 64, 16, false); });
       }
       if (tc_ok) {
-        tmem_ld16(tm + lane + 128, y);
+        tmem_ld16(tm + lane + 64, y);
 #pragma unroll
         for (int k = 0; k < 7; ++k) y[k] += sm.bias[128 + k];
       } else if (r == 0) {
@@ -1256,7 +1256,7 @@ int mpm_return_map_learned(mpm_surrogate* s, int64_t n, const double* F_in, cons
   if (e == cudaSuccess) e = cudaMemcpyAsync(dT, hT.data(), n * sizeof(float), cudaMemcpyHostToDevice, s->stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(dc, 0, sizeof(surr::GateOut), s->stream);
   if (e == cudaSuccess) {
-    const int blocks = (int)std::min<long long>(s->num_sms * 2, (n + surr::kGateThreads - 1) / surr::kGateThreads);
+    const int blocks = (int)std::min<long long>(s->num_sms * 4, (n + surr::kGateThreads - 1) / surr::kGateThreads);
     surr::k_gated<<<blocks, surr::kGateThreads, sizeof(surr::GateSmem), s->stream>>>(
         s->wbf, s->params, s->mt, s->sc, (float)gate_tol, use_mlp, n, dF, de, dT, dFo, ddep, dtau, dpath, dc, s->tc_err);
     e = cudaGetLastError();
@@ -1353,7 +1353,7 @@ int mpm_surrogate_time(mpm_surrogate* s, const mpm_surrogate_config* cfg, int64_
   SCUDA(s, cudaMalloc(&dc, sizeof(surr::GateOut)));
   surr::k_samples<<<s->num_sms * 8, 256, 0, s->stream>>>(s->mt, s->sc, sp, n, X, Y, dD, de, dT);
   cudaError_t e = cudaGetLastError();
-  const int blocks = (int)std::min<long long>(s->num_sms * 2, (n + surr::kGateThreads - 1) / surr::kGateThreads);
+  const int blocks = (int)std::min<long long>(s->num_sms * 4, (n + surr::kGateThreads - 1) / surr::kGateThreads);
   cudaEvent_t ev[4];
   for (auto& x : ev) cudaEventCreate(&x);
   for (int mode = 0; mode < 2 && e == cudaSuccess; ++mode) {
