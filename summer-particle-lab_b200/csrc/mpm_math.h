@@ -728,19 +728,7 @@ MPM_HD ConstitutiveOut constitutive_update_t(const MaterialDev& mt, float D[9], 
   out.dep = 0.f;
   out.dT = 0.f;
   const Sym3 B = cauchy_green_minus_identity(D);
-  if (AUX && aux_model(mt.model)) {
-    // the out-of-line return works on copies scoped to this branch, so the caller's D and aux keep
-    // no address (they would otherwise be written to local memory on every particle's path)
-    float Dt[9];
-#pragma unroll
-    for (int e = 0; e < 9; ++e) Dt[e] = D[e];
-    float at = aux;
-    const ConstitutiveOut o = constitutive_pressure(mt, xp, B, Dt, ep, at, do_return);
-#pragma unroll
-    for (int e = 0; e < 9; ++e) D[e] = Dt[e];
-    aux = at;
-    return o;
-  }
+  if (AUX && aux_model(mt.model)) return constitutive_pressure(mt, xp, B, D, ep, aux, do_return);
   if (mt.model == 1) {  // Neo-Hookean: mu (F F^T - I) + lambda log J I
     const float Jm1 = det_minus_one(D);
     const float J = 1.f + Jm1;
@@ -779,14 +767,7 @@ MPM_HD ConstitutiveOut constitutive_update_t(const MaterialDev& mt, float D[9], 
     const float dep = do_return ? plastic_increment(mt, tr.q, tr.J, ep, T, dt) : 0.f;
     return j2_finish(mt, tr, D, dep, inv_rho0);
   }
-  // large strain: out of line, on a copy of D scoped to this branch (see above)
-  float Dt[9];
-#pragma unroll
-  for (int e = 0; e < 9; ++e) Dt[e] = D[e];
-  const ConstitutiveOut o = constitutive_eigen(mt, B, Dt, ep, T, inv_rho0, do_return, dt);
-#pragma unroll
-  for (int e = 0; e < 9; ++e) D[e] = Dt[e];
-  return o;
+  return constitutive_eigen(mt, B, D, ep, T, inv_rho0, do_return, dt);
 }
 
 MPM_HD ConstitutiveOut constitutive_update_aux(const MaterialDev& mt, const MaterialExt* xp, float D[9], float ep,

@@ -938,6 +938,18 @@ surr::SampleSpec spec_of(const mpm_surrogate_config* cfg) {
 
 bool is_jc(const mpm_surrogate* s) { return mpm::learned_model(s->mat.model); }
 
+// Launch shape of k_gated: with the network, 4 CTAs per SM (128 TMEM columns and 49 KB of shared
+// memory each); the exact map alone needs neither, so it runs 16 CTAs per SM for latency hiding.
+struct GateLaunch {
+  int blocks;
+  size_t smem;
+};
+GateLaunch gate_launch(const mpm_surrogate* s, int use_mlp, long long n) {
+  const long long tiles = (n + surr::kGateThreads - 1) / surr::kGateThreads;
+  if (use_mlp) return {(int)std::min<long long>(s->num_sms * 4, tiles), sizeof(surr::GateSmem)};
+  return {(int)std::min<long long>(s->num_sms * 16, tiles), 0};
+}
+
 // One forward/backward pass over `batch` rows (row r of the call is (first + r stride) mod n_data)
 // adding the gradient to s->grad and the loss to *loss: tiles of 128 rows, one CTA per SM.
 void launch_train(mpm_surrogate* s, const float* X, const float* Y, long long n_data, long long first, long long stride,
@@ -1256,8 +1268,8 @@ int mpm_return_map_learned(mpm_surrogate* s, int64_t n, const double* F_in, cons
   if (e == cudaSuccess) e = cudaMemcpyAsync(dT, hT.data(), n * sizeof(float), cudaMemcpyHostToDevice, s->stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(dc, 0, sizeof(surr::GateOut), s->stream);
   if (e == cudaSuccess) {
-    const int blocks = (int)std::min<long long>(s->num_sms * 4, (n + surr::kGateThreads - 1) / surr::kGateThreads);
-    surr::k_gated<<<blocks, surr::kGateThreads, sizeof(surr::GateSmem), s->stream>>>(
+    const GateLaunch gl = gate_launch(s, use_mlp, n);
+    surr::k_gated<<<gl.blocks, surr::kGateThreads, gl.smem, s->stream>>>(
         s->wbf, s->params, s->mt, s->sc, (float)gate_tol, use_mlp, n, dF, de, dT, dFo, ddep, dtau, dpath, dc, s->tc_err);
     e = cudaGetLastError();
   }
@@ -1353,18 +1365,17 @@ int mpm_surrogate_time(mpm_surrogate* s, const mpm_surrogate_config* cfg, int64_
   SCUDA(s, cudaMalloc(&dc, sizeof(surr::GateOut)));
   surr::k_samples<<<s->num_sms * 8, 256, 0, s->stream>>>(s->mt, s->sc, sp, n, X, Y, dD, de, dT);
   cudaError_t e = cudaGetLastError();
-  const int blocks = (int)std::min<long long>(s->num_sms * 4, (n + surr::kGateThreads - 1) / surr::kGateThreads);
   cudaEvent_t ev[4];
   for (auto& x : ev) cudaEventCreate(&x);
   for (int mode = 0; mode < 2 && e == cudaSuccess; ++mode) {
     for (int w = 0; w < 2; ++w)
-      surr::k_gated<<<blocks, surr::kGateThreads, sizeof(surr::GateSmem), s->stream>>>(
+      surr::k_gated<<<gate_launch(s, mode, n).blocks, surr::kGateThreads, gate_launch(s, mode, n).smem, s->stream>>>(
           s->wbf, s->params, s->mt, s->sc, (float)gate_tol, mode, n, dD, de, dT, dFo, ddep, dtau, nullptr, nullptr,
           s->tc_err);
     cudaMemsetAsync(dc, 0, sizeof(surr::GateOut), s->stream);
     cudaEventRecord(ev[2 * mode], s->stream);
     for (int it = 0; it < iters; ++it)
-      surr::k_gated<<<blocks, surr::kGateThreads, sizeof(surr::GateSmem), s->stream>>>(
+      surr::k_gated<<<gate_launch(s, mode, n).blocks, surr::kGateThreads, gate_launch(s, mode, n).smem, s->stream>>>(
           s->wbf, s->params, s->mt, s->sc, (float)gate_tol, mode, n, dD, de, dT, dFo, ddep, dtau, nullptr,
           it == 0 ? dc : nullptr, s->tc_err);
     cudaEventRecord(ev[2 * mode + 1], s->stream);
