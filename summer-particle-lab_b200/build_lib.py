@@ -16,7 +16,7 @@ CSRC = os.path.join(PKG, "csrc")
 LIB_DIR = os.path.join(PKG, "lib")
 LIB = os.path.join(LIB_DIR, "libmpm_b200.so")
 SOURCES = ["mpm_kernels.cu", "mpm_api.cu", "mpm_noalloc.cu", "solid2d.cu", "surrogate.cu", "pairs.cu"]
-HEADERS = ["mpm_internal.h", "mpm_math.h", "pairs.h"]
+HEADERS = ["mpm_internal.h", "mpm_math.h", "pairs.h", "surrogate_net.h"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

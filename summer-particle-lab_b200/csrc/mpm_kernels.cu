@@ -1096,6 +1096,28 @@ __device__ __forceinline__ unsigned particle_phase_a(const Ctx& c, const SceneDe
   return key;
 }
 
+// The learned Johnson-Cook return of one warp's particles. Every lane of the warp calls it; lanes
+// with need set hold a trial stress above the initial flow stress. The network's guess (warp-wide
+// tensor-core tiles), the refinement and gate, and the exact bisection for what the gate rejects,
+// all in one out-of-line call, so the caller's live particle state is saved once around the whole
+// return and only in warps with such a lane. gate: 0 no return, 1 accepted, 2 bisection.
+struct LearnedDep {
+  float dep;
+  int gate;
+};
+static __device__ __noinline__ LearnedDep learned_jc_return(const void* mlp_w, const float* mlp_params,
+                                                           const MaterialDev& mt, float q, float J, float ep, float T,
+                                                           float dt, bool need, float tol, int newton) {
+  float x[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+  if (need) jc_features(mt, q, J, ep, T, dt, x);
+  const float u = surr::warp_predict_core(static_cast<const surr::WeightsBf16*>(mlp_w), mlp_params, x[0], x[1], x[2],
+                                          x[3], x[4], x[5], x[6], x[7]);
+  if (!need) return {0.f, 0};
+  const JcRefined r = jc_refine(mt, q, J, ep, T, dt, u, tol, newton);
+  if (r.ok) return {r.dep, 1};
+  return {jc_bisect(mt, q, J, ep, T, dt), 2};
+}
+
 // Phase A of the learned return mode (fused or gather-only pass; scenes without conduction and
 // without the history laws). The same particle update as particle_phase_a, with the plastic
 // increment of Johnson-Cook trial states (src/three/metal-plasticity.js:28-34) taken from the
@@ -1193,22 +1215,19 @@ __device__ __forceinline__ unsigned particle_phase_a_learned(const Ctx& c, const
 #pragma unroll
     for (int e = 0; e < 9; ++e) C[e] = c.p.Cc[e][home];
   }
-  // the warp's network evaluation (every lane arrives here)
+  // the warp's learned return (every lane arrives here)
   const bool need = live && series && learned_model(mt.model) && tr.q > jc_flow(mt, ep, 0.f, T);
-  float x[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-  if (need) jc_features(mt, tr.q, tr.J, ep, T, dt, x);
-  const float u = surr::warp_predict_first(static_cast<const surr::WeightsBf16*>(c.mlp_w), c.mlp_params, x, need);
+  LearnedDep ld{0.f, 0};
+  if (__any_sync(0xffffffffu, need))
+    ld = learned_jc_return(c.mlp_w, c.mlp_params, mt, tr.q, tr.J, ep, T, dt, need, c.gate_tol, c.learned_newton);
+  n_learned += ld.gate == 1;
+  n_exact += ld.gate == 2;
   ConstitutiveOut co;
   if (moving) {
     if (series) {
       float dep = 0.f;
       if (need) {  // a Johnson-Cook trial stress above the initial flow stress
-        if (jc_refine(mt, tr.q, tr.J, ep, T, dt, u, c.gate_tol, c.learned_newton, dep)) {
-          ++n_learned;
-        } else {
-          dep = jc_bisect(mt, tr.q, tr.J, ep, T, dt);
-          ++n_exact;
-        }
+        dep = ld.dep;
       } else if (!learned_model(mt.model)) {  // the other J2-type laws (a Johnson-Cook state below yield: 0)
         dep = plastic_increment(mt, tr.q, tr.J, ep, T, dt);
       }

@@ -312,15 +312,52 @@ MPM_HD float plastic_increment(const MaterialDev& mt, float q, float J, float ep
 // (the stress residual |q - slope dep - flow| is then at most tol q); otherwise the caller runs the
 // exact bisection.
 
-// Flow stress and its derivative with respect to dep at dep = d (d > 0).
+// Hardware approximations for the learned return's refinement and network inputs (device), the
+// libm functions on the host. Relative errors are a few 1e-7 over the arguments used here, far
+// below the gate's tolerance (1e-5 of the trial stress), and the gate is evaluated with the same
+// functions, so an accepted increment's true residual is within the tolerance plus that error.
+MPM_HD float fast_logf(float x) {
+#if defined(__CUDA_ARCH__)
+  return __logf(x);
+#else
+  return logf(x);
+#endif
+}
+
+MPM_HD float fast_expf(float x) {
+#if defined(__CUDA_ARCH__)
+  return __expf(x);
+#else
+  return expf(x);
+#endif
+}
+
+// x^y for x > 0
+MPM_HD float fast_powf(float x, float y) {
+#if defined(__CUDA_ARCH__)
+  return __powf(x, y);
+#else
+  return powf(x, y);
+#endif
+}
+
+MPM_HD float fast_divf(float a, float b) {
+#if defined(__CUDA_ARCH__)
+  return __fdividef(a, b);
+#else
+  return a / b;
+#endif
+}
+
+// Flow stress and its derivative with respect to dep at dep = d >= 0 (fast functions).
 MPM_HD float jc_flow_d(const MaterialDev& mt, float ep, float d, float inv_dt, float soft, float& dflow) {
   const float e = fmaxf(ep + d, 1e-30f);
-  const float pw = powf(e, mt.jc_n);
+  const float pw = fast_powf(e, mt.jc_n);
   const float hard = mt.yield_stress + mt.hardening * pw;
   const float r = d * inv_dt * mt.jc_inv_rate0;
   const bool rate_on = r > 1.f;
-  const float rf = 1.f + (rate_on ? mt.jc_C * logf(r) : 0.f);
-  dflow = soft * (mt.hardening * mt.jc_n * pw / e * rf + (rate_on ? hard * mt.jc_C / d : 0.f));
+  const float rf = 1.f + mt.jc_C * fast_logf(fmaxf(r, 1.f));
+  dflow = soft * (mt.hardening * mt.jc_n * fast_divf(pw, e) * rf + (rate_on ? fast_divf(hard * mt.jc_C, d) : 0.f));
   return soft * hard * rf;
 }
 
@@ -334,21 +371,23 @@ MPM_HD float jc_soft(const MaterialDev& mt, float T) {
 // The eight network inputs of a plastic Johnson-Cook trial state (q > flow(ep, 0, T)); all are
 // dimensionless, so one network serves every material with the same B / A, n and C:
 //   a = A soft / q, the hardening at ep and at ep + s relative to q, C ln max(1, s / (dt rate0)),
-//   log10 of the bracket s, ep, 1 - a - h0 and the network's bias input.
+//   log10 of the bracket s, ep, 1 - a - h0 and the network's bias input. Fast functions: the
+//   inputs only steer the guess, which the refinement and the gate check.
 MPM_NOINLINE void jc_features(const MaterialDev& mt, float q, float J, float ep, float T, float dt, float x[8]) {
   const float slope = 3.f * mt.mu / J;
   const float s = q / slope;
   const float soft = jc_soft(mt, T);
   const float iq = 1.f / q;
+  const float e0 = fmaxf(ep, 0.f);
   const float a = mt.yield_stress * soft * iq;
-  const float h0 = mt.hardening * soft * powf(fmaxf(ep, 0.f), mt.jc_n) * iq;
-  const float h1 = mt.hardening * soft * powf(fmaxf(ep, 0.f) + s, mt.jc_n) * iq;
-  const float L = logf(fmaxf(1.f, s / fmaxf(dt, 1e-30f) * mt.jc_inv_rate0));
+  const float h0 = mt.hardening * soft * fast_powf(fmaxf(e0, 1e-30f), mt.jc_n) * iq;
+  const float h1 = mt.hardening * soft * fast_powf(e0 + s, mt.jc_n) * iq;
+  const float L = fast_logf(fmaxf(1.f, s * fast_divf(mt.jc_inv_rate0, fmaxf(dt, 1e-30f))));
   x[0] = a;
   x[1] = h0;
   x[2] = h1 - h0;
   x[3] = mt.jc_C * L;
-  x[4] = 0.25f * log10f(fmaxf(s, 1e-12f)) + 1.5f;
+  x[4] = 0.10857362f * fast_logf(fmaxf(s, 1e-12f)) + 1.5f;  // 0.25 log10(s) + 1.5
   x[5] = ep;
   x[6] = 1.f - a - h0;
   x[7] = 1.f;
@@ -357,51 +396,43 @@ MPM_NOINLINE void jc_features(const MaterialDev& mt, float q, float J, float ep,
 // Newton refinement of a predicted root u and the gate. The rate factor max(1, rate / rate0) has a
 // kink at u_k = dt rate0 / s, where the slope of g jumps; g is smooth on either side, so when the
 // kink lies inside the bracket the refinement first finds the side of the root (the sign of g(u_k)).
-// Left of the kink Newton runs on u; right of it on w = ln(u / u_k), in which the logarithmic rate
-// term is linear (the curvature that slows Newton on u just past the kink). At most `newton` steps,
-// stopping as soon as |g| <= tol; a step that would leave the side is replaced by the midpoint toward
-// its end. Returns true with dep = u s when the final |g(u)| <= tol.
-MPM_NOINLINE bool jc_refine(const MaterialDev& mt, float q, float J, float ep, float T, float dt, float u_pred, float tol,
-                            int newton, float& dep) {
+// Left of the kink Newton runs on v = u; right of it on v = ln(u / u_k), in which the logarithmic
+// rate term is linear (the curvature that slows Newton on u just past the kink). Both sides share
+// one loop (the side only selects the map from v to u), so the lanes of a warp do not split by
+// side. At most `newton` steps, stopping as soon as |g| <= tol; a step that would leave the side's
+// interval is replaced by the midpoint toward its end. Returns dep = u s, and ok when the final
+// |g(u)| <= tol (returned by value: a reference output would give the caller's variable an address).
+struct JcRefined {
+  float dep;
+  bool ok;
+};
+MPM_NOINLINE JcRefined jc_refine(const MaterialDev& mt, float q, float J, float ep, float T, float dt, float u_pred,
+                                 float tol, int newton) {
   const float slope = 3.f * mt.mu / J;
   const float s = q / slope;
   const float soft = jc_soft(mt, T);
   const float inv_dt = 1.f / fmaxf(dt, 1e-12f);
   const float iq = 1.f / q;
+  const float sq = s * iq;
   float df;
   const float uk = mt.jc_C > 0.f ? 1.f / (s * inv_dt * mt.jc_inv_rate0) : 2.f;
   bool right = false;  // the root lies past the kink (the rate term is on)
   if (uk > 0.f && uk < 1.f) right = 1.f - uk - jc_flow_d(mt, ep, uk * s, inv_dt, soft, df) * iq > 0.f;
+  const float vhi = right ? -fast_logf(uk) : fminf(1.f, uk);
+  float v = right ? fast_logf(fast_divf(fmaxf(u_pred, uk), uk)) : u_pred;
+  v = fminf(vhi, fmaxf(0.f, v));
   float u, g;
-  if (right) {
-    const float whi = -logf(uk);
-    float w = fminf(whi, fmaxf(0.f, logf(fmaxf(u_pred, uk) / uk)));
-    u = uk * expf(w);
+  for (int k = 0;; ++k) {
+    u = right ? uk * fast_expf(v) : v;
     g = 1.f - u - jc_flow_d(mt, ep, u * s, inv_dt, soft, df) * iq;
-    for (int k = 0; k < newton && !(fabsf(g) <= tol); ++k) {
-      const float dgw = (-1.f - df * s * iq) * u;  // dg / dw
-      float wn = w - g / dgw;
-      if (!(wn > 0.f)) wn = 0.5f * w;
-      if (!(wn < whi)) wn = 0.5f * (w + whi);
-      w = wn;
-      u = uk * expf(w);
-      g = 1.f - u - jc_flow_d(mt, ep, u * s, inv_dt, soft, df) * iq;
-    }
-  } else {
-    const float hi = fminf(1.f, uk);
-    u = fminf(hi, fmaxf(0.f, u_pred));
-    g = 1.f - u - jc_flow_d(mt, ep, u * s, inv_dt, soft, df) * iq;
-    for (int k = 0; k < newton && !(fabsf(g) <= tol); ++k) {
-      const float dg = -1.f - df * s * iq;
-      float un = u - g / dg;
-      if (!(un > 0.f)) un = 0.5f * u;
-      if (!(un < hi)) un = 0.5f * (u + hi);
-      u = un;
-      g = 1.f - u - jc_flow_d(mt, ep, u * s, inv_dt, soft, df) * iq;
-    }
+    if (k >= newton || fabsf(g) <= tol) break;
+    const float dgu = -1.f - df * sq;  // dg / du
+    float vn = v - fast_divf(g, right ? dgu * u : dgu);
+    if (!(vn > 0.f)) vn = 0.5f * v;
+    if (!(vn < vhi)) vn = 0.5f * (v + vhi);
+    v = vn;
   }
-  dep = u * s;
-  return fabsf(g) <= tol;
+  return {u * s, fabsf(g) <= tol};
 }
 
 struct ConstitutiveOut {

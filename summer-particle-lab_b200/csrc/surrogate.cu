@@ -866,7 +866,11 @@ __global__ void __launch_bounds__(256) k_gated_jc(const WeightsBf16* wg, const f
       float x[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
       if (plastic) mpm::jc_features(mt, st.q, st.J, st.ep, st.T, st.dt, x);
       const float u = warp_predict_first(wg, params, x, plastic);
-      if (plastic) accepted = mpm::jc_refine(mt, st.q, st.J, st.ep, st.T, st.dt, u, gate_tol, newton, dep);
+      if (plastic) {
+        const mpm::JcRefined r = mpm::jc_refine(mt, st.q, st.J, st.ep, st.T, st.dt, u, gate_tol, newton);
+        dep = r.dep;
+        accepted = r.ok;
+      }
     }
     if (plastic && !accepted) dep = mpm::jc_bisect(mt, st.q, st.J, st.ep, st.T, st.dt);
     if (live) {

@@ -133,10 +133,10 @@ extern "C" void harness_jc_refine(int model, const double* prm, int n, const dou
   m.jc_inv_T_span = prm[10] > prm[4] ? (float)(1.0 / (prm[10] - prm[4])) : 0.f;
   m.jc_m = (float)prm[11];
   for (int i = 0; i < n; ++i) {
-    float d = 0.f;
-    ok[i] = mpm::jc_refine(m, (float)q[i], (float)J[i], (float)ep[i], (float)T[i], (float)dt[i], (float)u_pred[i],
-                           (float)tol, newton, d) ? 1 : 0;
-    dep_learned[i] = d;
+    const mpm::JcRefined r = mpm::jc_refine(m, (float)q[i], (float)J[i], (float)ep[i], (float)T[i], (float)dt[i],
+                                            (float)u_pred[i], (float)tol, newton);
+    ok[i] = r.ok ? 1 : 0;
+    dep_learned[i] = r.dep;
     dep_exact[i] = mpm::plastic_increment(m, (float)q[i], (float)J[i], (float)ep[i], (float)T[i], (float)dt[i]);
     float x[8];
     mpm::jc_features(m, (float)q[i], (float)J[i], (float)ep[i], (float)T[i], (float)dt[i], x);
