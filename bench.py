@@ -56,7 +56,7 @@ def parse():
     ap.add_argument("--no-ensemble", action="store_true")
     ap.add_argument("--no-surrogate", action="store_true")
     ap.add_argument("--surrogate-only", action="store_true")
-    ap.add_argument("--learned-newton", type=int, default=4, help="most Newton steps after the network's prediction")
+    ap.add_argument("--learned-newton", type=int, default=8, help="most Newton steps after the network's prediction")
     ap.add_argument("--learned-gate", type=float, default=1e-5, help="gate: consistency residual / trial stress")
     ap.add_argument("--surrogate-steps", type=int, default=0, help="training steps (0: the default schedule)")
     ap.add_argument("--ensemble-only", action="store_true")

@@ -464,7 +464,7 @@ typedef struct mpm_surrogate_config {
   double lr, weight_decay;
   double dep_weight;     /* loss weight of the dep output (others 1) */
   int32_t cosine;        /* 1: cosine learning-rate decay */
-  int32_t newton;        /* Johnson-Cook: most Newton steps after the prediction (0: 4) */
+  int32_t newton;        /* Johnson-Cook: most Newton steps after the prediction (0: 8) */
   uint64_t seed;
   double strain_min, strain_max; /* log-uniform magnitude of the principal trial log strains */
   double T_min, T_max, ep_max;   /* uniform temperature and plastic strain */

@@ -572,6 +572,7 @@ struct __align__(128) PartSmem {
   uint4 item[2];
   int abort_flag;
   unsigned red[3 * (kBlock / 32)];
+  unsigned gate[2];  // learned mode: returns the gate accepted / sent to the bisection
   double work[kBlock / 32];
   TileCtx tc;
   MaterialDev mt;
@@ -1100,22 +1101,24 @@ __device__ __forceinline__ unsigned particle_phase_a(const Ctx& c, const SceneDe
 // with need set hold a trial stress above the initial flow stress. The network's guess (warp-wide
 // tensor-core tiles), the refinement and gate, and the exact bisection for what the gate rejects,
 // all in one out-of-line call, so the caller's live particle state is saved once around the whole
-// return and only in warps with such a lane. gate: 0 no return, 1 accepted, 2 bisection.
-struct LearnedDep {
-  float dep;
-  int gate;
-};
-static __device__ __noinline__ LearnedDep learned_jc_return(const void* mlp_w, const float* mlp_params,
-                                                           const MaterialDev& mt, float q, float J, float ep, float T,
-                                                           float dt, bool need, float tol, int newton) {
+// return and only in warps with such a lane. gate[0] / gate[1] (shared memory) count the returns
+// the gate accepted / sent to the bisection.
+static __device__ __noinline__ float learned_jc_return(const void* mlp_w, const float* mlp_params,
+                                                      const MaterialDev& mt, float q, float J, float ep, float T,
+                                                      float dt, bool need, float tol, int newton, unsigned* gate) {
   float x[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
   if (need) jc_features(mt, q, J, ep, T, dt, x);
   const float u = surr::warp_predict_core(static_cast<const surr::WeightsBf16*>(mlp_w), mlp_params, x[0], x[1], x[2],
                                           x[3], x[4], x[5], x[6], x[7]);
-  if (!need) return {0.f, 0};
-  const JcRefined r = jc_refine(mt, q, J, ep, T, dt, u, tol, newton);
-  if (r.ok) return {r.dep, 1};
-  return {jc_bisect(mt, q, J, ep, T, dt), 2};
+  JcRefined r{0.f, false};
+  if (need) r = jc_refine(mt, q, J, ep, T, dt, u, tol, newton);
+  const unsigned acc = __ballot_sync(0xffffffffu, need && r.ok), rej = __ballot_sync(0xffffffffu, need && !r.ok);
+  if ((threadIdx.x & 31) == 0) {
+    if (acc) atomicAdd(&gate[0], __popc(acc));
+    if (rej) atomicAdd(&gate[1], __popc(rej));
+  }
+  if (need && !r.ok) r.dep = jc_bisect(mt, q, J, ep, T, dt);
+  return r.dep;
 }
 
 // Phase A of the learned return mode (fused or gather-only pass; scenes without conduction and
@@ -1133,8 +1136,7 @@ __device__ __forceinline__ unsigned particle_phase_a_learned(const Ctx& c, const
                                                              const float4* vwin, bool live, unsigned home, unsigned j,
                                                              float dt, int nxt, float2* pay, unsigned* meta, int* hist,
                                                              float& wave_acc, float& grad_acc, unsigned& flags_acc,
-                                                             double& work_acc, bool store_vc, unsigned& n_learned,
-                                                             unsigned& n_exact) {
+                                                             double& work_acc, bool store_vc, unsigned* gate) {
   constexpr bool SCATTER = PASS != kPassG2P;
   static_assert(PASS != kPassP2G, "the learned mode changes only returns");
   unsigned key = 0xffffffffu;
@@ -1217,17 +1219,16 @@ __device__ __forceinline__ unsigned particle_phase_a_learned(const Ctx& c, const
   }
   // the warp's learned return (every lane arrives here)
   const bool need = live && series && learned_model(mt.model) && tr.q > jc_flow(mt, ep, 0.f, T);
-  LearnedDep ld{0.f, 0};
+  float dep_learned = 0.f;
   if (__any_sync(0xffffffffu, need))
-    ld = learned_jc_return(c.mlp_w, c.mlp_params, mt, tr.q, tr.J, ep, T, dt, need, c.gate_tol, c.learned_newton);
-  n_learned += ld.gate == 1;
-  n_exact += ld.gate == 2;
+    dep_learned = learned_jc_return(c.mlp_w, c.mlp_params, mt, tr.q, tr.J, ep, T, dt, need, c.gate_tol,
+                                    c.learned_newton, gate);
   ConstitutiveOut co;
   if (moving) {
     if (series) {
       float dep = 0.f;
       if (need) {  // a Johnson-Cook trial stress above the initial flow stress
-        dep = ld.dep;
+        dep = dep_learned;
       } else if (!learned_model(mt.model)) {  // the other J2-type laws (a Johnson-Cook state below yield: 0)
         dep = plastic_increment(mt, tr.q, tr.J, ep, T, dt);
       }
@@ -1371,6 +1372,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_particles(const __grid_constant__
     mbar_init(&sm.mbar[1], 1);
     fence_barrier_init();
     sm.abort_flag = 0;
+    sm.gate[0] = sm.gate[1] = 0u;
     const unsigned idx = atomicAdd(&ct->work_next, 1u);
     sm.item[0] = idx < ct->work_count[lst] ? c.s.work[lst][idx] : make_uint4(0xffffffffu, 0, 0, 0);
     if (use_tma && sm.item[0].x != 0xffffffffu) {
@@ -1384,7 +1386,6 @@ __global__ void __launch_bounds__(kBlock, 2) k_particles(const __grid_constant__
   }
   unsigned phase0 = 0, phase1 = 0;
   double work_acc = 0.0;
-  unsigned n_learned = 0, n_exact = 0;  // learned mode: returns the gate accepted / sent to the exact map
   int cb = 0;
   int mt_row = -1;  // material row held in sm.mt
   // perm entries of the next tile's first round (j = tid, tid + kBlock), loaded one tile ahead
@@ -1487,7 +1488,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_particles(const __grid_constant__
                                                                                  : c.p.perm[it.y + r0 + j];
           key = particle_phase_a_learned<PASS>(c, sc, tc, sm.mt, single, sm.vwin[cb], live, home, j, dt, nxt, sm.pay,
                                                sm.meta, sm.hist, wave_acc, grad_acc, flags_acc, work_acc, store_vc,
-                                               n_learned, n_exact);
+                                               sm.gate);
         } else if (j < nround) {
           const unsigned home = (r0 == 0 && pf_ok && jj < kPf * kBlock) ? pf[jj / kBlock] : c.p.perm[it.y + r0 + j];
           key = particle_phase_a<PASS, HEAT, AUX>(c, sc, tc, sm.mt, single, sm.vwin[cb], home, j, dt, nxt, sm.pay, sm.meta,
@@ -1532,12 +1533,9 @@ __global__ void __launch_bounds__(kBlock, 2) k_particles(const __grid_constant__
     if (SCATTER) flush_window(c, sc, sm, nxt, tc.tile);
     cb ^= 1;
   }
-  if (LEARNED) {  // gate counts: one atomic per warp
-    const unsigned nl = __reduce_add_sync(0xffffffffu, n_learned), ne = __reduce_add_sync(0xffffffffu, n_exact);
-    if ((threadIdx.x & 31) == 0 && (nl | ne)) {
-      atomicAdd(&c.gate_counts[0], nl);
-      atomicAdd(&c.gate_counts[1], ne);
-    }
+  if (LEARNED && threadIdx.x == 0) {  // gate counts: one atomic each per CTA (the loop ended at a barrier)
+    if (sm.gate[0]) atomicAdd(&c.gate_counts[0], sm.gate[0]);
+    if (sm.gate[1]) atomicAdd(&c.gate_counts[1], sm.gate[1]);
   }
   // heat from plastic work: one FP64 atomic per CTA
   if (GATHER) {

@@ -734,14 +734,7 @@ __global__ void __launch_bounds__(kGateThreads) k_gated(const WeightsBf16* wg, c
       }
     }
     if (live) {
-      if (!plastic) {
-        const mpm::ConstitutiveOut co = mpm::constitutive_update(mt, D, ep, T, 0.f, false);
-        tau6[0] = co.tau.xx; tau6[1] = co.tau.yy; tau6[2] = co.tau.zz;
-        tau6[3] = co.tau.xy * r2; tau6[4] = co.tau.xz * r2; tau6[5] = co.tau.yz * r2;
-        dp = 0.f;
-        ++c_el;
-        if (path) path[i] = 0;
-      } else if (accepted) {
+      if (accepted) {
         // the predicted increment returns F: F' = exp((scale - 1) dev L) F
         const float scale = fmaxf(0.f, 1.f - s15 * dp / fmaxf(tr.len, 1e-20f));
         const float gs = scale - 1.f;
@@ -761,12 +754,14 @@ __global__ void __launch_bounds__(kGateThreads) k_gated(const WeightsBf16* wg, c
         ++c_ml;
         if (path) path[i] = 1;
       } else {
-        const mpm::ConstitutiveOut co = mpm::constitutive_update(mt, D, ep, T, 0.f, true);
+        // elastic states and the exact fallback share one call (the return only where plastic),
+        // so a warp holding both runs the constitutive update once
+        const mpm::ConstitutiveOut co = mpm::constitutive_update(mt, D, ep, T, 0.f, plastic);
         tau6[0] = co.tau.xx; tau6[1] = co.tau.yy; tau6[2] = co.tau.zz;
         tau6[3] = co.tau.xy * r2; tau6[4] = co.tau.xz * r2; tau6[5] = co.tau.yz * r2;
-        dp = co.dep;
-        ++c_fb;
-        if (path) path[i] = 2;
+        dp = plastic ? co.dep : 0.f;
+        if (plastic) ++c_fb; else ++c_el;
+        if (path) path[i] = plastic ? 2 : 0;
       }
       for (int k = 0; k < 9; ++k) Dout[i * 9 + k] = D[k];
       dep[i] = dp;
@@ -1308,7 +1303,7 @@ int mpm_return_map_learned(mpm_surrogate* s, int64_t n, const double* F_in, cons
 static int time_jc(mpm_surrogate* s, const mpm_surrogate_config* cfg, int64_t n, int32_t iters, double gate_tol,
                    double* ms_exact, double* ms_learned, mpm_gate_counts* counts) {
   const surr::SampleSpec sp = spec_of(cfg);
-  const int newton = cfg->newton > 0 ? cfg->newton : 4;
+  const int newton = cfg->newton > 0 ? cfg->newton : 8;
   float* dep = nullptr;
   surr::GateOut* dc = nullptr;
   SCUDA(s, cudaMalloc(&dep, n * sizeof(float)));

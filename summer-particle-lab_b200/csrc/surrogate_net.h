@@ -104,54 +104,6 @@ __device__ __forceinline__ void forward(const WeightsBf16& w, const float* bias,
   }
 }
 
-// The same forward pass with few registers live, for kernels that hold a particle's state around
-// it: the hidden activations are packed to BF16 A fragments as soon as they are formed, and the
-// second layer is produced two column tiles at a time, each pair feeding the output layer at once.
-__device__ __forceinline__ void forward_lean(const WeightsBf16& w, const float* bias, const uint32_t xa[4], float y[4],
-                                             int g, int tig) {
-  uint32_t a1[4][4];  // layer-1 activations as the layer-2 A fragments (K chunks of 16)
-#pragma unroll
-  for (int kc = 0; kc < 4; ++kc) {
-    float h[2][4];
-#pragma unroll
-    for (int u = 0; u < 2; ++u) {
-      const int nt = 2 * kc + u;
-      const float b0 = bias[kB1 + nt * 8 + tig * 2], b1 = bias[kB1 + nt * 8 + tig * 2 + 1];
-      h[u][0] = b0; h[u][1] = b1; h[u][2] = b0; h[u][3] = b1;
-      const __nv_bfloat16* wr = w.w1f + (nt * 8 + g) * 16 + tig * 2;
-      mma(h[u], xa, ld32(wr), ld32(wr + 8));
-#pragma unroll
-      for (int j = 0; j < 4; ++j) h[u][j] = fmaxf(h[u][j], 0.f);
-    }
-    chain(h, 0, a1[kc]);
-  }
-  {
-    const float b0 = bias[kB3 + tig * 2], b1 = bias[kB3 + tig * 2 + 1];
-    y[0] = b0; y[1] = b1; y[2] = b0; y[3] = b1;
-  }
-#pragma unroll
-  for (int oc = 0; oc < 4; ++oc) {  // layer-2 column tiles 2 oc, 2 oc + 1 = layer-3 K chunk oc
-    float h[2][4];
-#pragma unroll
-    for (int u = 0; u < 2; ++u) {
-      const int nt = 2 * oc + u;
-      const float b0 = bias[kB2 + nt * 8 + tig * 2], b1 = bias[kB2 + nt * 8 + tig * 2 + 1];
-      h[u][0] = b0; h[u][1] = b1; h[u][2] = b0; h[u][3] = b1;
-#pragma unroll
-      for (int kc = 0; kc < 4; ++kc) {
-        const __nv_bfloat16* wr = w.w2f + (nt * 8 + g) * kHid + kc * 16 + tig * 2;
-        mma(h[u], a1[kc], ld32(wr), ld32(wr + 8));
-      }
-#pragma unroll
-      for (int j = 0; j < 4; ++j) h[u][j] = fmaxf(h[u][j], 0.f);
-    }
-    uint32_t a[4];
-    chain(h, 0, a);
-    const __nv_bfloat16* wr = w.w3f + g * kHid + oc * 16 + tig * 2;
-    mma(y, a, ld32(wr), ld32(wr + 8));
-  }
-}
-
 static __device__ __noinline__ float warp_predict_core(const WeightsBf16* w, const float* params, float x0, float x1,
                                                        float x2, float x3, float x4, float x5, float x6, float x7);
 
@@ -167,12 +119,81 @@ __device__ __forceinline__ float warp_predict_first(const WeightsBf16* w, const 
   return warp_predict_core(w, params, x[0], x[1], x[2], x[3], x[4], x[5], x[6], x[7]);
 }
 
+// The forward pass of a warp's two 16-row tiles with few registers live, for kernels that hold a
+// particle's state around it: the hidden activations are packed to BF16 A fragments as soon as they
+// are formed, the second layer is produced two column tiles at a time, each pair feeding the output
+// layer at once, and each B fragment (weights) is loaded once for both tiles, whose MMA chains
+// interleave.
+__device__ __forceinline__ void forward_lean(const WeightsBf16& w, const float* bias, const uint32_t xa[2][4],
+                                              float y[2][4], int g, int tig) {
+  uint32_t a1[2][4][4];  // per tile: layer-1 activations as the layer-2 A fragments
+#pragma unroll
+  for (int kc = 0; kc < 4; ++kc) {
+    float h[2][2][4];
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+      const int nt = 2 * kc + u;
+      const float b0 = bias[kB1 + nt * 8 + tig * 2], b1 = bias[kB1 + nt * 8 + tig * 2 + 1];
+      const __nv_bfloat16* wr = w.w1f + (nt * 8 + g) * 16 + tig * 2;
+      const uint32_t w0 = ld32(wr), w1 = ld32(wr + 8);
+#pragma unroll
+      for (int t = 0; t < 2; ++t) {
+        h[t][u][0] = b0; h[t][u][1] = b1; h[t][u][2] = b0; h[t][u][3] = b1;
+        mma(h[t][u], xa[t], w0, w1);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) h[t][u][j] = fmaxf(h[t][u][j], 0.f);
+      }
+    }
+#pragma unroll
+    for (int t = 0; t < 2; ++t) chain(h[t], 0, a1[t][kc]);
+  }
+  {
+    const float b0 = bias[kB3 + tig * 2], b1 = bias[kB3 + tig * 2 + 1];
+#pragma unroll
+    for (int t = 0; t < 2; ++t) {
+      y[t][0] = b0; y[t][1] = b1; y[t][2] = b0; y[t][3] = b1;
+    }
+  }
+#pragma unroll
+  for (int oc = 0; oc < 4; ++oc) {  // layer-2 column tiles 2 oc, 2 oc + 1 = layer-3 K chunk oc
+    float h[2][2][4];
+#pragma unroll
+    for (int u = 0; u < 2; ++u) {
+      const int nt = 2 * oc + u;
+      const float b0 = bias[kB2 + nt * 8 + tig * 2], b1 = bias[kB2 + nt * 8 + tig * 2 + 1];
+#pragma unroll
+      for (int t = 0; t < 2; ++t) {
+        h[t][u][0] = b0; h[t][u][1] = b1; h[t][u][2] = b0; h[t][u][3] = b1;
+      }
+#pragma unroll
+      for (int kc = 0; kc < 4; ++kc) {
+        const __nv_bfloat16* wr = w.w2f + (nt * 8 + g) * kHid + kc * 16 + tig * 2;
+        const uint32_t w0 = ld32(wr), w1 = ld32(wr + 8);
+#pragma unroll
+        for (int t = 0; t < 2; ++t) mma(h[t][u], a1[t][kc], w0, w1);
+      }
+#pragma unroll
+      for (int t = 0; t < 2; ++t)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) h[t][u][j] = fmaxf(h[t][u][j], 0.f);
+    }
+    const __nv_bfloat16* wr = w.w3f + g * kHid + oc * 16 + tig * 2;
+    const uint32_t w0 = ld32(wr), w1 = ld32(wr + 8);
+#pragma unroll
+    for (int t = 0; t < 2; ++t) {
+      uint32_t a[4];
+      chain(h[t], 0, a);
+      mma(y[t], a, w0, w1);
+    }
+  }
+}
+
 static __device__ __noinline__ float warp_predict_core(const WeightsBf16* w, const float* params, float x0, float x1,
                                                        float x2, float x3, float x4, float x5, float x6, float x7) {
   const float x[8] = {x0, x1, x2, x3, x4, x5, x6, x7};
   __syncwarp();
   const int lane = threadIdx.x & 31, g = lane >> 2, tig = lane & 3;
-  float out = 0.f;
+  uint32_t xa[2][4];
 #pragma unroll
   for (int half = 0; half < 2; ++half) {
     const int r0 = half * 16 + g, r1 = r0 + 8;
@@ -186,14 +207,20 @@ static __device__ __noinline__ float warp_predict_core(const WeightsBf16* w, con
         a00 = p0; a01 = p1; a10 = q0; a11 = q1;
       }
     }
-    const uint32_t xa[4] = {pack_bf16(a00, a01), pack_bf16(a10, a11), 0u, 0u};
-    float y[4];
-    forward_lean(*w, params, xa, y, g, tig);
-    // output column 0 of row r sits in lane 4 (r % 8): y[0] for r < 8, y[2] for r >= 8
-    const int r = lane - half * 16;
-    const int src = 4 * (r & 7);
-    const float lo = __shfl_sync(0xffffffffu, y[0], src), hi = __shfl_sync(0xffffffffu, y[2], src);
-    if (r >= 0 && r < 16) out = r < 8 ? lo : hi;
+    xa[half][0] = pack_bf16(a00, a01);
+    xa[half][1] = pack_bf16(a10, a11);
+    xa[half][2] = 0u;
+    xa[half][3] = 0u;
+  }
+  float y[2][4];
+  forward_lean(*w, params, xa, y, g, tig);
+  // output column 0 of row r of a tile sits in lane 4 (r % 8): y[0] for r < 8, y[2] for r >= 8
+  const int r = lane & 15, src = 4 * (r & 7);
+  float out = 0.f;
+#pragma unroll
+  for (int half = 0; half < 2; ++half) {
+    const float lo = __shfl_sync(0xffffffffu, y[half][0], src), hi = __shfl_sync(0xffffffffu, y[half][2], src);
+    if ((lane >> 4) == half) out = r < 8 ? lo : hi;
   }
   return out;
 }

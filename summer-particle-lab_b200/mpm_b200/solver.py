@@ -258,7 +258,7 @@ class Solver:
         """One regularisation pass now (regularizeSolids(s, dt) after a step)."""
         self._check(_lib.lib().mpm_regularize(self.h, float(dt)))
 
-    def set_return_mode(self, surrogate=None, gate_tol=1e-5, newton=4):
+    def set_return_mode(self, surrogate=None, gate_tol=1e-5, newton=8):
         """Learned return map inside the step (mpm_set_return_mode) with a Johnson-Cook network, or
         the exact map again with surrogate None."""
         if surrogate is None:

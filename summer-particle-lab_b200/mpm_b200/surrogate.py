@@ -27,7 +27,7 @@ def config(samples=10_000_000, batch=16384, steps=30000, lr=2e-3, weight_decay=0
 
 
 def jc_config(samples=4_000_000, batch=16384, steps=8000, lr=2e-3, seed=37, strain_min=1e-4, strain_max=5e-2,
-              T_min=293.0, T_max=700.0, ep_max=0.5, dt_min=1e-8, dt_max=1e-5, newton=4):
+              T_min=293.0, T_max=700.0, ep_max=0.5, dt_min=1e-8, dt_max=1e-5, newton=8):
     """Training and timing draws for a Johnson-Cook network: deviatoric trial log strains log-uniform
     in [strain_min, strain_max] (every other draw a trial stress just above the initial flow stress),
     plastic strain uniform in [0, ep_max], temperature uniform in [T_min, T_max] (model 6 softening),
