@@ -104,8 +104,8 @@ __device__ __forceinline__ void forward(const WeightsBf16& w, const float* bias,
   }
 }
 
-static __device__ __noinline__ float warp_predict_core(const WeightsBf16* w, const float* params, float x0, float x1,
-                                                       float x2, float x3, float x4, float x5, float x6, float x7);
+static __device__ __forceinline__ float warp_predict_core(const WeightsBf16* w, const float* params, float x0, float x1,
+                                                          float x2, float x3, float x4, float x5, float x6, float x7);
 
 // Warp-collective prediction inside a per-particle kernel: every lane of the warp calls it (the
 // tensor-core tiles are warp-wide). Lanes with need set get the network's first output for their
@@ -115,7 +115,6 @@ static __device__ __noinline__ float warp_predict_core(const WeightsBf16* w, con
 __device__ __forceinline__ float warp_predict_first(const WeightsBf16* w, const float* params, const float x[8],
                                                     bool need) {
   if (!__any_sync(0xffffffffu, need)) return 0.f;
-  // out of line: the caller's live state is saved around the call only when some lane needs it
   return warp_predict_core(w, params, x[0], x[1], x[2], x[3], x[4], x[5], x[6], x[7]);
 }
 
@@ -188,8 +187,8 @@ __device__ __forceinline__ void forward_lean(const WeightsBf16& w, const float* 
   }
 }
 
-static __device__ __noinline__ float warp_predict_core(const WeightsBf16* w, const float* params, float x0, float x1,
-                                                       float x2, float x3, float x4, float x5, float x6, float x7) {
+static __device__ __forceinline__ float warp_predict_core(const WeightsBf16* w, const float* params, float x0, float x1,
+                                                          float x2, float x3, float x4, float x5, float x6, float x7) {
   const float x[8] = {x0, x1, x2, x3, x4, x5, x6, x7};
   __syncwarp();
   const int lane = threadIdx.x & 31, g = lane >> 2, tig = lane & 3;
