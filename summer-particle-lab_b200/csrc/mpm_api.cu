@@ -423,17 +423,11 @@ static int alloc_grid(mpm_handle* h) {
   return MPM_OK;
 }
 
-// The Johnson-Cook instances of the particle pass serve scenes without grid conduction and without
-// the history laws (snow, sand, pressure): in exact mode whenever a Johnson-Cook material is set (the
-// fused pass then runs its bisections in full warps), in learned mode with the network. Anything
-// else runs the plain instances and the exact return map.
+// The learned instances of the particle pass serve scenes without grid conduction and without the
+// history laws (snow, sand, pressure); anything else runs the exact return map.
 static void apply_return_mode(mpm_handle* h) {
-  const bool eligible = !h->ctx.has_aux && !h->ctx.conduct;
-  bool jc = false;
-  for (size_t i = 0; i < h->mats_host.size(); ++i)
-    if (h->mat_set[i] && mpm::learned_model(h->mats_host[i].model)) jc = true;
-  h->ctx.jc_dense = eligible && jc ? 1 : 0;
-  h->ctx.learned = h->return_mode == MPM_RETURN_LEARNED_GATED && h->mlp_block && eligible ? 1 : 0;
+  h->ctx.learned = h->return_mode == MPM_RETURN_LEARNED_GATED && h->mlp_block && !h->ctx.has_aux && !h->ctx.conduct
+                       ? 1 : 0;
 }
 
 static void refresh_flags(mpm_handle* h) {
@@ -821,7 +815,6 @@ int mpm_set_material(mpm_handle* h, int32_t index, const mpm_material* material)
   MPM_CUDA(h, cudaMemcpyAsync(const_cast<mpm::MaterialExt*>(h->ctx.mats_ext) + index, &h->mats_ext[index],
                               sizeof(mpm::MaterialExt), cudaMemcpyHostToDevice, h->stream));
   refresh_flags(h);
-  drop_graph(h);          // the kernel instances and the flags a captured graph holds may change
   h->grid_valid = false;  // stresses change
   h->last_estimate = 0;
   return MPM_OK;

@@ -166,9 +166,6 @@ struct Ctx {
   // and the counts of returns the gate accepted and sent to the exact map (2 unsigned)
   int learned;
   int learned_newton;
-  // a Johnson-Cook material is set (and no conduction, no history law): the fused pass runs the
-  // Johnson-Cook instance, whose returns go to a per-round return phase in full warps
-  int jc_dense;
   float gate_tol;
   const void* mlp_w;
   const float* mlp_params;

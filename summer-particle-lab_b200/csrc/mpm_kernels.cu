@@ -573,7 +573,6 @@ struct __align__(128) PartSmem {
   int abort_flag;
   unsigned red[3 * (kBlock / 32)];
   unsigned gate[2];  // learned mode: returns the gate accepted / sent to the bisection
-  int nlist;         // Johnson-Cook instance: rows of the round whose return phase A deferred
   double work[kBlock / 32];
   TileCtx tc;
   MaterialDev mt;
@@ -905,40 +904,17 @@ __device__ __noinline__ Gather12 gather_global(const float4* base, int sy, long 
   return g;
 }
 
-// Whether the scatter stencil of a particle at fixed-point position q lies inside the tile's shared
-// scatter window (the test of the payload path in particle_phase_a).
-__device__ __forceinline__ bool payload_in_window(const unsigned q[3], const TileCtx& tc) {
-  bool in = true;
-#pragma unroll
-  for (int a = 0; a < 3; ++a) {
-    int nb;
-    float t;
-    stencil_axis(q[a], tc.dims[a], nb, t);
-    const int l = nb - (tc.tile[a] * kTile - 1);
-    in = in && l >= 0 && l <= kWinS - 3;
-  }
-  return in;
-}
-
 // Phase A of one particle (home slot `home`, payload row j): G2P from the staged window, F update,
 // fixed-point advection and the constitutive update / return map (src/three/mpm.js:107-131), or,
 // for the P2G pass and pinned particles, the stress of the stored state; then the scatter payload
 // bucketed by its new stencil base in the shared window (pay, meta, hist), and the CFL terms.
 // Writes the particle's new state and returns its next sort key (all ones when not needed).
-// DEFER (the Johnson-Cook instance of the fused pass): a Johnson-Cook trial stress above the
-// initial flow stress whose payload lands in the shared window leaves its return to the round's
-// return phase (jc_return_round): the particle stores its trial F, a payload without stress and its
-// speed in the payload's free word, and appends its row to jlist; its wave speed waits for the
-// returned F. A plastic one outside the window returns here by the bisection.
-template <int PASS, bool HEAT, bool AUX, bool DEFER = false>
+template <int PASS, bool HEAT, bool AUX>
 __device__ __forceinline__ unsigned particle_phase_a(const Ctx& c, const SceneDev& sc, const TileCtx& tc,
                                                      const MaterialDev& mt_single, bool single, const float4* vwin,
                                                      unsigned home, unsigned j, float dt, int nxt, float2* pay,
                                                      unsigned* meta, int* hist, float& wave_acc, float& grad_acc,
-                                                     unsigned& flags_acc, double& work_acc, bool store_vc,
-                                                     unsigned short* jlist = nullptr, int* nlist = nullptr,
-                                                     unsigned* gate = nullptr) {
-  static_assert(!DEFER || (PASS == kPassG2P2G && !HEAT && !AUX), "deferred returns: the fused pass, J2-type laws");
+                                                     unsigned& flags_acc, double& work_acc, bool store_vc) {
   constexpr bool SCATTER = PASS != kPassG2P;
   constexpr bool GATHER = PASS != kPassP2G;
   unsigned key = 0xffffffffu;
@@ -956,7 +932,6 @@ __device__ __forceinline__ unsigned particle_phase_a(const Ctx& c, const SceneDe
   float v[3], C[9];
   ConstitutiveOut co;
   unsigned flags = 0;
-  bool deferred = false;
   if (GATHER && !pinned) {
     int b[3];
     float t[3], w[3][3];
@@ -1037,41 +1012,7 @@ __device__ __forceinline__ unsigned particle_phase_a(const Ctx& c, const SceneDe
       q[a] = static_cast<unsigned>(qn);
     }
     // return map / stress for the next P2G (src/three/mpm.js:126-131)
-    if constexpr (DEFER) {
-      int nt = 0;
-      Sym3 B{};
-      if (learned_model(mt.model)) {
-        B = cauchy_green_minus_identity(D);
-        nt = series_terms_sq(sym_norm2(B));
-      }
-      if (nt > 0) {  // the series path of constitutive_update_t, with the return deferred or inline
-        const J2Trial tr = j2_trial_series(mt, B, nt);
-        const bool plastic = tr.q > jc_flow(mt, ep, 0.f, T);
-        deferred = plastic && payload_in_window(q, tc);
-        float dep = 0.f;
-        if (plastic && !deferred) {
-          dep = jc_bisect(mt, tr.q, tr.J, ep, T, dt);
-          if (c.learned) atomicAdd(&gate[1], 1u);
-        }
-        if (deferred) {
-          co.tau = Sym3{0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-          co.dep = co.dT = co.Jm1 = 0.f;
-          // one shared atomic per group of converged lanes
-          const unsigned act = __activemask();
-          const int lane = threadIdx.x & 31, leader = __ffs(act) - 1;
-          int base = 0;
-          if (lane == leader) base = atomicAdd(nlist, __popc(act));
-          base = __shfl_sync(act, base, leader);
-          jlist[base + __popc(act & ((1u << lane) - 1u))] = static_cast<unsigned short>(j);
-        } else {
-          co = j2_finish(mt, tr, D, dep, V / m);
-        }
-      } else {
-        co = constitutive_update_t<AUX>(mt, D, ep, aux, T, V / m, true, dt, xp);
-      }
-    } else {
-      co = constitutive_update_t<AUX>(mt, D, ep, aux, T, V / m, true, dt, xp);
-    }
+    co = constitutive_update_t<AUX>(mt, D, ep, aux, T, V / m, true, dt, xp);
     ep += co.dep;
     T += co.dT;
     c.p.qx[home] = q[0]; c.p.qy[home] = q[1]; c.p.qz[home] = q[2];
@@ -1140,8 +1081,7 @@ __device__ __forceinline__ unsigned particle_phase_a(const Ctx& c, const SceneDe
       P[8 * kPayStride] = make_float2(mC[7], s6[3]);
       P[9 * kPayStride] = make_float2(mC[0], mC[3]);
       P[10 * kPayStride] = make_float2(mC[6], s6[0]);
-      // the free word: a deferred particle's speed for the return phase's wave-speed term
-      P[11 * kPayStride] = make_float2(s6[1], DEFER && deferred ? sqrtf(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]) : 0.f);
+      P[11 * kPayStride] = make_float2(s6[1], 0.f);
     } else {
       meta[j] = kMetaInvalid;
       if (!in_w) flags |= 0x10u;
@@ -1152,7 +1092,7 @@ __device__ __forceinline__ unsigned particle_phase_a(const Ctx& c, const SceneDe
   cfl_terms<AUX>(mt, D, v, C, m, V, co.Jm1, aux, wave, grad);
   flags |= state_flags(v, D, co.tau, co.Jm1);
   flags_acc |= flags;
-  if (!(DEFER && deferred)) wave_acc = fmaxf(wave_acc, wave);
+  wave_acc = fmaxf(wave_acc, wave);
   grad_acc = fmaxf(grad_acc, grad);
   return key;
 }
@@ -1180,72 +1120,6 @@ static __device__ __forceinline__ float learned_jc_return(const void* mlp_w, con
   }
   if (need && !r.ok) r.dep = jc_bisect(mt, q, J, ep, T, dt);
   return r.dep;
-}
-
-// Return phase of a scatter round in the Johnson-Cook instance of the fused pass: the n particles
-// phase A deferred (rows jlist[0..n) of the round starting at perm offset `first`) take their
-// Johnson-Cook return in full warps, instead of in the warps of phase A where a few plastic lanes
-// hold up a mostly elastic warp: the network with the refinement and gate in learned mode, the
-// reference's bisection otherwise. Each reloads its trial F (stored by phase A), recomputes the
-// trial invariants (the same float operations on the same F, so the same trial state), finishes
-// the return (F, stress, plastic strain, heat), stores the state, writes the stress into its
-// payload and adds its wave speed with the returned F. Called by every thread of the CTA between
-// phase A and the bucket scan.
-__device__ __forceinline__ void jc_return_round(const Ctx& c, const TileCtx& tc, const MaterialDev& mt_single,
-                                                bool single, unsigned first, int n, float dt,
-                                                const unsigned short* jlist, float2* pay, unsigned* gate,
-                                                float& wave_acc, unsigned& flags_acc, double& work_acc) {
-  for (int base = 0; base < n; base += kBlock) {
-    if (base + static_cast<int>(threadIdx.x & ~31u) >= n) break;  // no entry left for this warp
-    const int k = base + static_cast<int>(threadIdx.x);
-    const bool has = k < n;
-    // lanes past the end repeat the round's first entry for the warp's network and write nothing
-    const unsigned j = jlist[has ? k : 0];
-    const unsigned home = c.p.perm[first + j];
-    const MaterialDev& mt = single ? mt_single : c.mats[c.p.mat[home]];
-    float D[9];
-#pragma unroll
-    for (int e = 0; e < 9; ++e) D[e] = c.p.Dc[e][home];
-    const float m = c.p.m[home], V = c.p.V[home];
-    float ep = c.has_plastic ? c.p.ep[home] : 0.f;
-    float T = c.has_thermal ? c.p.T[home] : 0.f;
-    const Sym3 B = cauchy_green_minus_identity(D);
-    const J2Trial tr = j2_trial_series(mt, B, series_terms_sq(sym_norm2(B)));
-    float dep = 0.f;
-    if (c.learned) {
-      dep = learned_jc_return(c.mlp_w, c.mlp_params, mt, tr.q, tr.J, ep, T, dt, has, c.gate_tol, c.learned_newton,
-                              gate);
-    } else if (has) {
-      dep = jc_bisect(mt, tr.q, tr.J, ep, T, dt);
-    }
-    if (!has) continue;
-    const ConstitutiveOut co = j2_finish(mt, tr, D, dep, V / m);
-    ep += co.dep;
-    T += co.dT;
-#pragma unroll
-    for (int e = 0; e < 9; ++e) c.p.Dc[e][home] = D[e];
-    if (c.has_plastic) c.p.ep[home] = ep;
-    if (c.has_thermal) c.p.T[home] = T;
-    if (co.dep > 0.f && mt.heat_per_work > 0.f) work_acc += static_cast<double>(co.dT) * m / mt.heat_per_work;
-    float2* P = pay + pay_slot(j);
-    const float sv = -4.f * V * tc.invH;
-    float* P5 = reinterpret_cast<float*>(P + 5 * kPayStride);
-    float* P8 = reinterpret_cast<float*>(P + 8 * kPayStride);
-    float* P10 = reinterpret_cast<float*>(P + 10 * kPayStride);
-    float* P11 = reinterpret_cast<float*>(P + 11 * kPayStride);
-    P5[1] = sv * co.tau.xz;
-    P[6 * kPayStride] = make_float2(sv * co.tau.yz, sv * co.tau.zz);
-    P8[1] = sv * co.tau.xy;
-    P10[1] = sv * co.tau.xx;
-    const float speed = P11[1];
-    P11[0] = sv * co.tau.yy;
-    const float v[3] = {speed, 0.f, 0.f};
-    const float Cz[9] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-    float wave, grad;
-    cfl_terms<false>(mt, D, v, Cz, m, V, co.Jm1, 0.f, wave, grad);
-    wave_acc = fmaxf(wave_acc, wave);
-    flags_acc |= state_flags(v, D, co.tau, co.Jm1);
-  }
 }
 
 // Phase A of the learned return mode (fused or gather-only pass; scenes without conduction and
@@ -1470,13 +1344,9 @@ __device__ __forceinline__ void prefetch_tile_state(const Ctx& c, uint4 it) {
   if (c.has_pinned) pf(c.p.pinned, 1);
 }
 
-// JC: the Johnson-Cook instance (scenes without conduction and without the history laws). The fused
-// pass defers Johnson-Cook returns to a return phase per scatter round that runs them in full warps
-// (network + gate in learned mode, the bisection otherwise); the gather-only pass serves the
-// learned mode with the network in the warps of phase A.
-template <int PASS, bool HEAT, bool AUX, bool JC = false>
+template <int PASS, bool HEAT, bool AUX, bool LEARNED = false>
 __global__ void __launch_bounds__(kBlock, 2) k_particles(const __grid_constant__ Ctx c) {
-  static_assert(!JC || (!HEAT && !AUX && PASS != kPassP2G), "Johnson-Cook instances: no conduction, no history laws");
+  static_assert(!LEARNED || (!HEAT && !AUX && PASS != kPassP2G), "learned instances: no conduction, no history laws");
   extern __shared__ __align__(128) unsigned char smem_raw[];
   PartSmem& sm = *reinterpret_cast<PartSmem*>(smem_raw);
   constexpr bool SCATTER = PASS != kPassG2P;
@@ -1504,7 +1374,6 @@ __global__ void __launch_bounds__(kBlock, 2) k_particles(const __grid_constant__
     fence_barrier_init();
     sm.abort_flag = 0;
     sm.gate[0] = sm.gate[1] = 0u;
-    sm.nlist = 0;
     const unsigned idx = atomicAdd(&ct->work_next, 1u);
     sm.item[0] = idx < ct->work_count[lst] ? c.s.work[lst][idx] : make_uint4(0xffffffffu, 0, 0, 0);
     if (use_tma && sm.item[0].x != 0xffffffffu) {
@@ -1610,7 +1479,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_particles(const __grid_constant__
       for (unsigned jj = 0; jj < nround; jj += kBlock) {
         const unsigned j = jj + threadIdx.x;
         unsigned key = 0xffffffffu;
-        if constexpr (JC && PASS == kPassG2P) {
+        if constexpr (LEARNED) {
           // every lane of a warp with a live particle takes part in its network evaluation (warps
           // past the end of the round skip as a whole)
           if (jj + (threadIdx.x & ~31u) >= nround) continue;
@@ -1623,23 +1492,16 @@ __global__ void __launch_bounds__(kBlock, 2) k_particles(const __grid_constant__
                                                sm.gate);
         } else if (j < nround) {
           const unsigned home = (r0 == 0 && pf_ok && jj < kPf * kBlock) ? pf[jj / kBlock] : c.p.perm[it.y + r0 + j];
-          // the deferred rows go to sidx, which is free until the bucket scan
-          key = particle_phase_a<PASS, HEAT, AUX, JC>(c, sc, tc, sm.mt, single, sm.vwin[cb], home, j, dt, nxt, sm.pay,
-                                                      sm.meta, sm.hist, wave_acc, grad_acc, flags_acc, work_acc, store_vc,
-                                                      sm.sidx, &sm.nlist, sm.gate);
+          key = particle_phase_a<PASS, HEAT, AUX>(c, sc, tc, sm.mt, single, sm.vwin[cb], home, j, dt, nxt, sm.pay, sm.meta,
+                                       sm.hist, wave_acc, grad_acc, flags_acc, work_acc, store_vc);
         }
         if (PASS == kPassG2P2G) count_key(c, key);
       }
       if (!SCATTER && r0 == 0 && threadIdx.x == 0) prefetch_next();
       if (SCATTER) {
         __syncthreads();
-        if constexpr (JC) {
-          jc_return_round(c, tc, sm.mt, single, it.y + r0, sm.nlist, dt, sm.sidx, sm.pay, sm.gate, wave_acc, flags_acc,
-                          work_acc);
-        }
         scan_buckets(sm);
         __syncthreads();
-        if (JC && threadIdx.x == 0) sm.nlist = 0;  // read by every thread before the scan's barriers
         for (unsigned j = threadIdx.x; j < nround; j += kBlock) {
           const unsigned mm = sm.meta[j];
           if (!(mm & kMetaInvalid)) sm.sidx[sm.bstart[mm & 0xffu] + (mm >> 8)] = static_cast<unsigned short>(j);
@@ -1672,7 +1534,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_particles(const __grid_constant__
     if (SCATTER) flush_window(c, sc, sm, nxt, tc.tile);
     cb ^= 1;
   }
-  if (JC && threadIdx.x == 0) {  // gate counts: one atomic each per CTA (the loop ended at a barrier)
+  if (LEARNED && threadIdx.x == 0) {  // gate counts: one atomic each per CTA (the loop ended at a barrier)
     if (sm.gate[0]) atomicAdd(&c.gate_counts[0], sm.gate[0]);
     if (sm.gate[1]) atomicAdd(&c.gate_counts[1], sm.gate[1]);
   }
@@ -2002,7 +1864,7 @@ __global__ void __launch_bounds__(kWsThreads, 1) k_particles_ws(const __grid_con
 template <int PASS, bool HEAT, bool AUX>
 static void launch_pass_t(const Ctx& c, cudaStream_t st, int grid_blocks) {
   if constexpr (PASS != kPassP2G && !HEAT && !AUX) {
-    if (c.learned || (c.jc_dense && PASS == kPassG2P2G)) {
+    if (c.learned) {
       k_particles<PASS, false, false, true><<<grid_blocks, kBlock, sizeof(PartSmem), st>>>(c);
       return;
     }
