@@ -815,6 +815,7 @@ int mpm_set_material(mpm_handle* h, int32_t index, const mpm_material* material)
   MPM_CUDA(h, cudaMemcpyAsync(const_cast<mpm::MaterialExt*>(h->ctx.mats_ext) + index, &h->mats_ext[index],
                               sizeof(mpm::MaterialExt), cudaMemcpyHostToDevice, h->stream));
   refresh_flags(h);
+  drop_graph(h);          // the kernel instances and the flags a captured graph holds may change
   h->grid_valid = false;  // stresses change
   h->last_estimate = 0;
   return MPM_OK;

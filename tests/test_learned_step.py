@@ -89,6 +89,18 @@ def test_untrained_network_serves_fewer_returns_and_stays_exact(trained):
     assert share_trained >= share_untrained + 0.25, (share_untrained, share_trained)
 
 
+def test_learned_step_on_dense_tiles_matches_oracle(trained):
+    """27 particles per cell (three scatter rounds per tile, each with its own return phase) in
+    learned mode: the oracle bounds after ten substeps and most returns served."""
+    from test_gpu_parity import dense_j2_scene
+    sc = dense_j2_scene(material=scenes.johnson_cook_metal(7))
+    st = oracle_run(sc)
+    out, (learned, fallback) = run(sc, trained)
+    check_parity(out, st)
+    assert learned + fallback > 1000
+    assert learned >= 0.8 * (learned + fallback), (learned, fallback)
+
+
 def test_exact_mode_restores_the_reference_map(trained):
     sc = impact_scene()
     sol = Solver(sc.domain, sc.n)
