@@ -528,7 +528,7 @@ void launch_sort_scatter(const Ctx& c, cudaStream_t st, bool initial) {
 // fraction of a cell leaves a third of its tiles a few particles over 512 (up to ~530); at
 // kCap = 512 those took a second round (every phase and barrier again for a handful of particles).
 constexpr int kCap = 768;
-constexpr int kPf = 2;         // perm entries of the next tile's first round held in registers per thread
+constexpr int kPf = 2;         // perm entries of the next tile's first round held per thread (shared memory)
 // Payload of one particle: 12 float pairs, laid out for the paired FMAs of phase B:
 //   0 (tx, ty)   1 (tz, m)    2 (mv0, mv1)  3 (mv2, m T)  [m T only with conduction, else 0]
 //   4 (c02, c12) 5 (c22, s02) 6 (s12, s22)  7 (c01, c11)  8 (c21, s01)  9 (c00, c10)  10 (c20, s00)
@@ -573,7 +573,15 @@ struct __align__(128) PartSmem {
   int abort_flag;
   unsigned red[3 * (kBlock / 32)];
   unsigned gate[2];  // learned mode: returns the gate accepted / sent to the bisection
-  double work[kBlock / 32];
+  // State the CTA carries from tile to tile sits here rather than in registers: at 128 registers a
+  // thread, every register held across the tiles is one fewer for phase A, and moving these (with
+  // the heat sum, which was a per-thread double) cut the pass by 7%.
+  unsigned tma_phase[2];       // mbarrier phases of the two window buffers (thread 0)
+  double work_sum;             // heat from plastic work of the CTA's particles
+  int mt_row;                  // material row held in mt
+  int pf_ok;                   // pfs holds the next tile's first-round perm entries
+  unsigned pfs[kPf * kBlock];  // perm entries j of the next tile's first round, j < kPf x kBlock
+
   TileCtx tc;
   MaterialDev mt;
 };
@@ -1029,7 +1037,7 @@ __device__ __forceinline__ unsigned particle_phase_a(const Ctx& c, const SceneDe
     if (c.has_plastic) c.p.ep[home] = ep;
     if (c.has_thermal) c.p.T[home] = T;
     if (AUX) c.p.aux[home] = aux;
-    if (co.dep > 0.f && mt.heat_per_work > 0.f) work_acc += static_cast<double>(co.dT) * m / mt.heat_per_work;
+    if (co.dep > 0.f && mt.heat_per_work > 0.f) atomicAdd(&work_acc, static_cast<double>(co.dT) * m / mt.heat_per_work);
   } else {
     // P2G of the stored state, and pinned particles (not moved, src/three/mpm.js:108)
     v[0] = c.p.vx[home]; v[1] = c.p.vy[home]; v[2] = c.p.vz[home];
@@ -1085,7 +1093,21 @@ __device__ __forceinline__ unsigned particle_phase_a(const Ctx& c, const SceneDe
     } else {
       meta[j] = kMetaInvalid;
       if (!in_w) flags |= 0x10u;
-      scatter_global(c, sc, tc, nxt, nb, t, m, mv, mC, s6, pinned, m * T);
+      // copies scoped to this rare branch: the arrays passed to the out-of-line scatter would
+      // otherwise live in local memory on every particle's path (3% of the fused pass)
+      int nb_g[3];
+      float t_g[3], mv_g[3], mC_g[9], s6_g[6];
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        nb_g[a] = nb[a];
+        t_g[a] = t[a];
+        mv_g[a] = mv[a];
+      }
+#pragma unroll
+      for (int e = 0; e < 9; ++e) mC_g[e] = mC[e];
+#pragma unroll
+      for (int e = 0; e < 6; ++e) s6_g[e] = s6[e];
+      scatter_global(c, sc, tc, nxt, nb_g, t_g, m, mv_g, mC_g, s6_g, pinned, m * T);
     }
   }
   float wave, grad;
@@ -1250,7 +1272,7 @@ __device__ __forceinline__ unsigned particle_phase_a_learned(const Ctx& c, const
       }
       if (c.has_plastic) c.p.ep[home] = ep;
       if (c.has_thermal) c.p.T[home] = T;
-      if (co.dep > 0.f && mt.heat_per_work > 0.f) work_acc += static_cast<double>(co.dT) * m / mt.heat_per_work;
+      if (co.dep > 0.f && mt.heat_per_work > 0.f) atomicAdd(&work_acc, static_cast<double>(co.dT) * m / mt.heat_per_work);
     }
   } else {
     float Dc[9];
@@ -1301,7 +1323,21 @@ __device__ __forceinline__ unsigned particle_phase_a_learned(const Ctx& c, const
     } else {
       meta[j] = kMetaInvalid;
       if (!in_w) flags |= 0x10u;
-      scatter_global(c, sc, tc, nxt, nb, t, m, mv, mC, s6, pinned, 0.f);
+      // copies scoped to this rare branch: the arrays passed to the out-of-line scatter would
+      // otherwise live in local memory on every particle's path
+      int nb_g[3];
+      float t_g[3], mv_g[3], mC_g[9], s6_g[6];
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        nb_g[a] = nb[a];
+        t_g[a] = t[a];
+        mv_g[a] = mv[a];
+      }
+#pragma unroll
+      for (int e = 0; e < 9; ++e) mC_g[e] = mC[e];
+#pragma unroll
+      for (int e = 0; e < 6; ++e) s6_g[e] = s6[e];
+      scatter_global(c, sc, tc, nxt, nb_g, t_g, m, mv_g, mC_g, s6_g, pinned, 0.f);
     }
   }
   float wave, grad;
@@ -1374,6 +1410,10 @@ __global__ void __launch_bounds__(kBlock, 2) k_particles(const __grid_constant__
     fence_barrier_init();
     sm.abort_flag = 0;
     sm.gate[0] = sm.gate[1] = 0u;
+    sm.tma_phase[0] = sm.tma_phase[1] = 0u;
+    sm.work_sum = 0.0;
+    sm.mt_row = -1;
+    sm.pf_ok = 0;
     const unsigned idx = atomicAdd(&ct->work_next, 1u);
     sm.item[0] = idx < ct->work_count[lst] ? c.s.work[lst][idx] : make_uint4(0xffffffffu, 0, 0, 0);
     if (use_tma && sm.item[0].x != 0xffffffffu) {
@@ -1385,26 +1425,20 @@ __global__ void __launch_bounds__(kBlock, 2) k_particles(const __grid_constant__
                   ((lt / sc.tiles[0]) % sc.tiles[1]) * kTile, (lt / (sc.tiles[0] * sc.tiles[1])) * kTile, &sm.mbar[0]);
     }
   }
-  unsigned phase0 = 0, phase1 = 0;
-  double work_acc = 0.0;
   int cb = 0;
-  int mt_row = -1;  // material row held in sm.mt
-  // perm entries of the next tile's first round (j = tid, tid + kBlock), loaded one tile ahead
-  unsigned pf[kPf] = {};
-  bool pf_ok = false;
   while (true) {
     __syncthreads();
     const uint4 it = sm.item[cb];
     if (it.x == 0xffffffffu) break;
     if (threadIdx.x == 0) {
       if (use_tma) {
-        const unsigned ph = cb ? phase1 : phase0;
+        const unsigned ph = sm.tma_phase[cb];
         if (!mbar_wait_bounded(&sm.mbar[cb], ph)) {
           atomicOr(&ct->status, 0x8u);
           mbar_wait_bounded(&sm.mbar[cb], ph);  // a second bounded chance for the copy in flight
           sm.abort_flag = 1;
         }
-        if (cb) phase1 ^= 1u; else phase0 ^= 1u;
+        sm.tma_phase[cb] ^= 1u;
       }
     }
     // The next work item is claimed, and its velocity window requested, by thread 0 after phase A
@@ -1449,12 +1483,14 @@ __global__ void __launch_bounds__(kBlock, 2) k_particles(const __grid_constant__
     // the material row of a single-material handle or of the tile's scene in a batch, copied word
     // by word by the whole block, and only when it changes (every tile of a one-scene handle shares
     // it; a batch's tiles come scene by scene)
+    const int mt_row = sm.mt_row;
     if ((c.single_material || c.scene_material) && sc.mat_base != mt_row) {
       static_assert(sizeof(MaterialDev) % 4 == 0, "word copy");
       const unsigned* src = reinterpret_cast<const unsigned*>(c.mats + sc.mat_base);
       unsigned* dst = reinterpret_cast<unsigned*>(&sm.mt);
       for (int i = threadIdx.x; i < static_cast<int>(sizeof(MaterialDev) / 4); i += kBlock) dst[i] = src[i];
-      mt_row = sc.mat_base;
+      __syncthreads();
+      if (threadIdx.x == 0) sm.mt_row = sc.mat_base;
     }
     __syncthreads();
     if (sm.abort_flag) return;
@@ -1472,8 +1508,8 @@ __global__ void __launch_bounds__(kBlock, 2) k_particles(const __grid_constant__
     const bool single = c.single_material != 0 || c.scene_material != 0;
     float wave_acc = 0.f, grad_acc = 0.f;
     unsigned flags_acc = 0;
-    for (unsigned r0 = 0; r0 < it.z; r0 += kCap) {
-      const unsigned nround = min(static_cast<unsigned>(kCap), it.z - r0);
+    for (unsigned r0 = 0; r0 < sm.item[cb].z; r0 += kCap) {
+      const unsigned nround = min(static_cast<unsigned>(kCap), sm.item[cb].z - r0);
       // ---- phase A: one thread per particle (the bucket histogram is zero: cleared at the start
       // and by each round's scan) ----
       for (unsigned jj = 0; jj < nround; jj += kBlock) {
@@ -1485,15 +1521,15 @@ __global__ void __launch_bounds__(kBlock, 2) k_particles(const __grid_constant__
           if (jj + (threadIdx.x & ~31u) >= nround) continue;
           const bool live = j < nround;
           const unsigned home = !live ? c.p.perm[it.y + r0]
-                                      : (r0 == 0 && pf_ok && jj < kPf * kBlock) ? pf[jj / kBlock]
+                                      : (r0 == 0 && sm.pf_ok && jj < kPf * kBlock) ? sm.pfs[jj + threadIdx.x]
                                                                                  : c.p.perm[it.y + r0 + j];
           key = particle_phase_a_learned<PASS>(c, sc, tc, sm.mt, single, sm.vwin[cb], live, home, j, dt, nxt, sm.pay,
-                                               sm.meta, sm.hist, wave_acc, grad_acc, flags_acc, work_acc, store_vc,
+                                               sm.meta, sm.hist, wave_acc, grad_acc, flags_acc, sm.work_sum, store_vc,
                                                sm.gate);
         } else if (j < nround) {
-          const unsigned home = (r0 == 0 && pf_ok && jj < kPf * kBlock) ? pf[jj / kBlock] : c.p.perm[it.y + r0 + j];
+          const unsigned home = (r0 == 0 && sm.pf_ok && jj < kPf * kBlock) ? sm.pfs[jj + threadIdx.x] : c.p.perm[sm.item[cb].y + r0 + j];
           key = particle_phase_a<PASS, HEAT, AUX>(c, sc, tc, sm.mt, single, sm.vwin[cb], home, j, dt, nxt, sm.pay, sm.meta,
-                                       sm.hist, wave_acc, grad_acc, flags_acc, work_acc, store_vc);
+                                       sm.hist, wave_acc, grad_acc, flags_acc, sm.work_sum, store_vc);
         }
         if (PASS == kPassG2P2G) count_key(c, key);
       }
@@ -1518,12 +1554,13 @@ __global__ void __launch_bounds__(kBlock, 2) k_particles(const __grid_constant__
         __syncthreads();
         if (r0 == 0) {  // perm of the next tile's first round, consumed there
           const uint4 nx = sm.item[cb ^ 1];
-          pf_ok = nx.x != 0xffffffffu;
-          if (pf_ok) {
+          const bool ok = nx.x != 0xffffffffu;
+          if (threadIdx.x == 0) sm.pf_ok = ok;
+          if (ok) {
 #pragma unroll
             for (int k = 0; k < kPf; ++k) {
               const unsigned j = k * kBlock + threadIdx.x;
-              pf[k] = j < nx.z ? c.p.perm[nx.y + j] : 0u;
+              sm.pfs[j] = j < nx.z ? c.p.perm[nx.y + j] : 0u;
             }
           }
         }
@@ -1538,18 +1575,8 @@ __global__ void __launch_bounds__(kBlock, 2) k_particles(const __grid_constant__
     if (sm.gate[0]) atomicAdd(&c.gate_counts[0], sm.gate[0]);
     if (sm.gate[1]) atomicAdd(&c.gate_counts[1], sm.gate[1]);
   }
-  // heat from plastic work: one FP64 atomic per CTA
-  if (GATHER) {
-    double wsum = warp_sum_d(work_acc);
-    __syncthreads();
-    if ((threadIdx.x & 31) == 0) sm.work[threadIdx.x >> 5] = wsum;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      double tsum = 0.0;
-      for (int w = 0; w < kBlock / 32; ++w) tsum += sm.work[w];
-      if (tsum != 0.0) atomicAdd(&ct->plastic_work, tsum);
-    }
-  }
+  // heat from plastic work: one FP64 atomic per CTA (the loop ended at a barrier)
+  if (GATHER && threadIdx.x == 0 && sm.work_sum != 0.0) atomicAdd(&ct->plastic_work, sm.work_sum);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -1593,7 +1620,7 @@ struct __align__(128) WsSmem {
   int abort_flag;                         // producer gave up (its TMA wait timed out)
   int consumer_exit;                      // consumer gave up waiting for a stage
   unsigned red[3 * (kWsGroup / 32)];
-  double work[kWsGroup / 32];
+  double work_sum;  // heat from plastic work of the CTA's particles
   TileCtx tc;
   MaterialDev mt;
 };
@@ -1670,12 +1697,12 @@ __global__ void __launch_bounds__(kWsThreads, 1) k_particles_ws(const __grid_con
     fence_barrier_init();
     sm.abort_flag = 0;
     sm.consumer_exit = 0;
+    sm.work_sum = 0.0;
     const unsigned idx = atomicAdd(&ct->work_next, 1u);
     sm.item[0] = idx < ct->work_count[lst] ? c.s.work[lst][idx] : make_uint4(0xffffffffu, 0, 0, 0);
     if (use_tma && sm.item[0].x != 0xffffffffu) issue_window(0, sm.item[0]);
   }
   __syncthreads();
-  double work_acc = 0.0;
   if (threadIdx.x < kWsGroup) {
     // ================= producer =================
     const int tid = threadIdx.x;
@@ -1767,7 +1794,7 @@ __global__ void __launch_bounds__(kWsThreads, 1) k_particles_ws(const __grid_con
           if (j < nround) {
             const unsigned home = c.p.perm[it.y + r0 + j];
             key = particle_phase_a<PASS, HEAT, AUX>(c, sc, tc, sm.mt, single, sm.vwin[cb], home, j, dt, nxt, sm.pay[s],
-                                         sm.meta[s], sm.hist[s], wave_acc, grad_acc, flags_acc, work_acc, store_vc);
+                                         sm.meta[s], sm.hist[s], wave_acc, grad_acc, flags_acc, sm.work_sum, store_vc);
           }
           if (PASS == kPassG2P2G) count_key(c, key);
         }
@@ -1847,18 +1874,9 @@ __global__ void __launch_bounds__(kWsThreads, 1) k_particles_ws(const __grid_con
       s ^= 1;
     }
   }
-  // heat from plastic work: one FP64 atomic per CTA (producer threads hold it)
+  // heat from plastic work: one FP64 atomic per CTA
   __syncthreads();
-  if (GATHER) {
-    const double wsum = warp_sum_d(work_acc);
-    if ((threadIdx.x & 31) == 0 && threadIdx.x < kWsGroup) sm.work[threadIdx.x >> 5] = wsum;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      double tsum = 0.0;
-      for (int w = 0; w < kWsGroup / 32; ++w) tsum += sm.work[w];
-      if (tsum != 0.0) atomicAdd(&ct->plastic_work, tsum);
-    }
-  }
+  if (GATHER && threadIdx.x == 0 && sm.work_sum != 0.0) atomicAdd(&ct->plastic_work, sm.work_sum);
 }
 
 template <int PASS, bool HEAT, bool AUX>

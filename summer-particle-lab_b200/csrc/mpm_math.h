@@ -759,7 +759,20 @@ MPM_HD ConstitutiveOut constitutive_update_t(const MaterialDev& mt, float D[9], 
   out.dep = 0.f;
   out.dT = 0.f;
   const Sym3 B = cauchy_green_minus_identity(D);
-  if (AUX && aux_model(mt.model)) return constitutive_pressure(mt, xp, B, D, ep, aux, do_return);
+  // The out-of-line returns work on copies scoped to their branch, so the caller's D (and aux)
+  // keep no address: passed directly, they live in local memory on every particle's path (2% of
+  // the fused pass).
+  if (AUX && aux_model(mt.model)) {
+    float Dt[9];
+#pragma unroll
+    for (int e = 0; e < 9; ++e) Dt[e] = D[e];
+    float at = aux;
+    const ConstitutiveOut o = constitutive_pressure(mt, xp, B, Dt, ep, at, do_return);
+#pragma unroll
+    for (int e = 0; e < 9; ++e) D[e] = Dt[e];
+    aux = at;
+    return o;
+  }
   if (mt.model == 1) {  // Neo-Hookean: mu (F F^T - I) + lambda log J I
     const float Jm1 = det_minus_one(D);
     const float J = 1.f + Jm1;
@@ -798,7 +811,13 @@ MPM_HD ConstitutiveOut constitutive_update_t(const MaterialDev& mt, float D[9], 
     const float dep = do_return ? plastic_increment(mt, tr.q, tr.J, ep, T, dt) : 0.f;
     return j2_finish(mt, tr, D, dep, inv_rho0);
   }
-  return constitutive_eigen(mt, B, D, ep, T, inv_rho0, do_return, dt);
+  float Dt[9];
+#pragma unroll
+  for (int e = 0; e < 9; ++e) Dt[e] = D[e];
+  const ConstitutiveOut o = constitutive_eigen(mt, B, Dt, ep, T, inv_rho0, do_return, dt);
+#pragma unroll
+  for (int e = 0; e < 9; ++e) D[e] = Dt[e];
+  return o;
 }
 
 MPM_HD ConstitutiveOut constitutive_update_aux(const MaterialDev& mt, const MaterialExt* xp, float D[9], float ep,
