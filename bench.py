@@ -263,8 +263,8 @@ class Clocks:
 # DRAM bytes per particle of one fused G2P2G launch (dram__bytes_read.sum + dram__bytes_write.sum of
 # one ncu --set full capture of k_particles<1,0,0> on the 2M-particle J2 drop, divided by the particle
 # count), set by hand from that capture; bench.py scales it to the timed workload's particle count.
-TRAFFIC_PER_PARTICLE = 162.3
-TRAFFIC_SOURCE = "ncu --set full capture of k_particles<1,0,0,0>, j2_drop 2,097,152 particles (340.4 MB per launch)"
+TRAFFIC_PER_PARTICLE = 153.9
+TRAFFIC_SOURCE = "ncu --set full capture of k_particles<1,0,0,0>, j2_drop 2,097,152 particles (322.8 MB per launch)"
 
 
 def peaks():
