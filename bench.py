@@ -62,6 +62,9 @@ def parse():
     ap.add_argument("--ensemble-only", action="store_true")
     ap.add_argument("--ensemble-scenes", type=int, default=256)
     ap.add_argument("--ensemble-steps", type=int, default=64)
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="ensemble: keep the default schedule (2 CTAs/SM, TMA, re-sort every 32 substeps) "
+                         "instead of timing the candidates first (for profiling a known launch sequence)")
     ap.add_argument("--slabs", action="store_true",
                     help="N > 1: split the one scene into N slabs along z with an overlap exchange per substep "
                          "(strong scaling) instead of N replicas")
@@ -342,7 +345,7 @@ def ensemble_leg(args, rank, world, dist):
     n_mine = sum(sc.n for sc in mine)
     b = Batch(mine)
     b.upload()
-    tune = b.autotune(6)
+    tune = b.autotune(6) if not args.no_autotune else {"skipped": "default schedule (--no-autotune)"}
     b.run(K, graph=True)  # warm-up, captures the graph
     torch.cuda.synchronize()
     if dist is not None:
