@@ -1131,8 +1131,8 @@ static __device__ __forceinline__ float learned_jc_return(const void* mlp_w, con
                                                       float dt, bool need, float tol, int newton, unsigned* gate) {
   float x[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
   if (need) jc_features(mt, q, J, ep, T, dt, x);
-  const float u = surr::warp_predict_core(static_cast<const surr::WeightsBf16*>(mlp_w), mlp_params, x[0], x[1], x[2],
-                                          x[3], x[4], x[5], x[6], x[7]);
+  const float u = surr::warp_predict_seq(static_cast<const surr::WeightsBf16*>(mlp_w), mlp_params, x[0], x[1], x[2],
+                                         x[3], x[4], x[5], x[6], x[7]);
   JcRefined r{0.f, false};
   if (need) r = jc_refine(mt, q, J, ep, T, dt, u, tol, newton);
   const unsigned acc = __ballot_sync(0xffffffffu, need && r.ok), rej = __ballot_sync(0xffffffffu, need && !r.ok);
