@@ -363,12 +363,11 @@ def test_tiles_over_one_scatter_round_match_oracle():
     sol.close()
 
 
-def test_johnson_cook_return_phase_on_dense_tiles_matches_oracle():
-    """Johnson-Cook (model 7) impact with 27 particles per cell: the fused pass defers the plastic
-    returns of each of a tile's three scatter rounds to the round's return phase (full warps, the
-    bisection). Ten CFL substeps against the oracle's CFL stepping (the wave speed of a deferred
-    particle comes from its returned F): time advanced within 1e-5, x within 1e-6 m, F within
-    2e-6, ep within 2e-6 + 1e-4 max ep."""
+def test_johnson_cook_on_dense_tiles_matches_oracle():
+    """Johnson-Cook (model 7) impact with 27 particles per cell, so each tile runs three scatter
+    rounds with bisection returns in each. Ten CFL substeps against the oracle's CFL stepping (the
+    wave-speed term uses each particle's returned F): time advanced within 1e-5, x within 1e-6 m, F
+    within 2e-6, ep within 2e-6 + 1e-4 max ep."""
     sc = dense_j2_scene(material=scenes.johnson_cook_metal(7))
     sol = Solver(sc.domain, sc.n)
     sol.upload(sc)

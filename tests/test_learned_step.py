@@ -90,8 +90,8 @@ def test_untrained_network_serves_fewer_returns_and_stays_exact(trained):
 
 
 def test_learned_step_on_dense_tiles_matches_oracle(trained):
-    """27 particles per cell (three scatter rounds per tile, each with its own return phase) in
-    learned mode: the oracle bounds after ten substeps and most returns served."""
+    """27 particles per cell (three scatter rounds per tile) in learned mode: the oracle bounds
+    after ten substeps and most returns served."""
     from test_gpu_parity import dense_j2_scene
     sc = dense_j2_scene(material=scenes.johnson_cook_metal(7))
     st = oracle_run(sc)
