@@ -158,12 +158,6 @@ __device__ __forceinline__ double warp_sum_d(double x) {
 
 __device__ __forceinline__ unsigned fbits(float x) { return __float_as_uint(fmaxf(x, 0.f)); }
 
-struct StepOut {
-  float wave, grad;
-  unsigned key;
-  unsigned flags;
-};
-
 // CFL terms of src/three/mpm.js:43-54 for one particle (F = I + D)
 template <bool AUX>
 __device__ __forceinline__ void cfl_terms(const MaterialDev& mt, const float D[9], const float v[3],
