@@ -626,6 +626,73 @@ struct GateOut {
   unsigned elastic, learned, fallback;
 };
 
+// Stages the BF16 weights in the canonical layouts and the biases, initialises the completion
+// barrier and allocates the tile's TMEM columns; returns their base. Every thread of the CTA calls it.
+__device__ __forceinline__ uint32_t gate_setup(GateSmem& sm, const WeightsBf16* wg, const float* params) {
+  const int r = threadIdx.x, warp = r >> 5;
+  for (int i = r; i < 64 * 16; i += kGateThreads) sm.w1[km_off(i / 16, i % 16, 16)] = wg->w1f[i];
+  for (int i = r; i < 64 * 64; i += kGateThreads) sm.w2[km_off(i / 64, i % 64, 64)] = wg->w2f[i];
+  for (int i = r; i < 16 * 64; i += kGateThreads)
+    sm.w3[km_off(i / 64, i % 64, 64)] = i / 64 < 8 ? wg->w3f[i] : __float2bfloat16_rn(0.f);
+  for (int i = r; i < 144; i += kGateThreads)
+    sm.bias[i] = i < 64 ? params[kB1 + i] : i < 128 ? params[kB2 + i - 64] : (i - 128 < 8 ? params[kB3 + i - 128] : 0.f);
+  if (r == 0) mbar_init1(&sm.mbar);
+  if (warp == 0) tc_alloc(&sm.tmem_base, kGateTmemCols);
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  return sm.tmem_base;
+}
+
+// The network on the tile's 128 input rows (thread r writes row r, x[8]): three tcgen05 GEMM groups
+// (M = 128) with the ReLU epilogues of k_train_tc's forward pass; y[0..6] are thread r's outputs
+// before the output bias (y[7..15] are zero). Returns false when a completion wait gave up (the
+// tile's outputs are then not to be used). Every thread of the CTA calls it.
+__device__ __forceinline__ bool gate_network(GateSmem& sm, uint32_t tm, uint32_t& phase, const float x[8], float y[16]) {
+  const int r = threadIdx.x;
+  const uint32_t lane = static_cast<uint32_t>((r >> 5) * 32) << 16;
+#pragma unroll
+  for (int k = 0; k < 16; k += 2) st_pair(sm.x, km_off(r, k, 16), k < 8 ? x[k] : 0.f, k < 8 ? x[k + 1] : 0.f);
+  bool ok = tc_run(&sm.mbar, phase, [&] { tc_gemm(tm + 0, sm.x, sm.w1, 16, 64, false); });
+  if (ok) {
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      float v[16];
+      tmem_ld16(tm + lane + 16 * c, v);
+#pragma unroll
+      for (int j = 0; j < 16; j += 2)
+        st_pair(sm.h1, km_off(r, 16 * c + j, 64), fmaxf(v[j] + sm.bias[16 * c + j], 0.f),
+                fmaxf(v[j + 1] + sm.bias[16 * c + j + 1], 0.f));
+    }
+    ok = tc_run(&sm.mbar, phase, [&] { tc_gemm(tm + 0, sm.h1, sm.w2, 64, 64, false); });
+  }
+  if (ok) {
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      float v[16];
+      tmem_ld16(tm + lane + 16 * c, v);
+#pragma unroll
+      for (int j = 0; j < 16; j += 2)
+        st_pair(sm.h2, km_off(r, 16 * c + j, 64), fmaxf(v[j] + sm.bias[64 + 16 * c + j], 0.f),
+                fmaxf(v[j + 1] + sm.bias[64 + 16 * c + j + 1], 0.f));
+    }
+    ok = tc_run(&sm.mbar, phase, [&] { tc_gemm(tm + 64, sm.h2, sm.w3, 64, 16, false); });
+  }
+  if (ok) tmem_ld16(tm + lane + 64, y);
+  return ok;
+}
+
+// Releases the TMEM columns (after one more bounded wait when a group may still be in flight).
+__device__ __forceinline__ void gate_teardown(GateSmem& sm, uint32_t tm, uint32_t phase, bool tc_ok) {
+  if (!tc_ok) tc_wait(&sm.mbar, phase);
+  tc_fence_before();
+  __syncthreads();
+  if ((threadIdx.x >> 5) == 0) {
+    tc_fence_after();
+    tc_dealloc(tm, kGateTmemCols);
+  }
+}
+
 // D = F - I (n x 9 float, formed by the caller in higher precision), ep, T in; D, dep and tau
 // (n x 6: xx yy zz xy xz yz) out; path: 0 elastic, 1 learned, 2 exact fallback. use_mlp = 0 runs
 // the exact map for every particle through the same kernel, so both timings share loads and stores.
@@ -637,24 +704,10 @@ __global__ void __launch_bounds__(kGateThreads) k_gated(const WeightsBf16* wg, c
                                                         unsigned* err) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   GateSmem& sm = *reinterpret_cast<GateSmem*>(smem_raw);
-  const int r = threadIdx.x, warp = r >> 5;
+  const int r = threadIdx.x;
   uint32_t tm = 0, phase = 0;
   bool tc_ok = true;
-  if (use_mlp) {
-    for (int i = r; i < 64 * 16; i += kGateThreads) sm.w1[km_off(i / 16, i % 16, 16)] = wg->w1f[i];
-    for (int i = r; i < 64 * 64; i += kGateThreads) sm.w2[km_off(i / 64, i % 64, 64)] = wg->w2f[i];
-    for (int i = r; i < 16 * 64; i += kGateThreads)
-      sm.w3[km_off(i / 64, i % 64, 64)] = i / 64 < 8 ? wg->w3f[i] : __float2bfloat16_rn(0.f);
-    for (int i = r; i < 144; i += kGateThreads)
-      sm.bias[i] = i < 64 ? params[kB1 + i] : i < 128 ? params[kB2 + i - 64] : (i - 128 < 8 ? params[kB3 + i - 128] : 0.f);
-    if (r == 0) mbar_init1(&sm.mbar);
-    if (warp == 0) tc_alloc(&sm.tmem_base, kGateTmemCols);
-    tc_fence_before();
-    __syncthreads();
-    tc_fence_after();
-    tm = sm.tmem_base;
-  }
-  const uint32_t lane = static_cast<uint32_t>(warp * 32) << 16;
+  if (use_mlp) tm = gate_setup(sm, wg, params);
   unsigned c_el = 0, c_ml = 0, c_fb = 0;
   const float r2 = 1.41421356237f, ir2 = 0.70710678118f, s15 = 1.224744871391589f;
   for (long long base = (long long)blockIdx.x * kGateThreads; base < n; base += (long long)gridDim.x * kGateThreads) {
@@ -675,36 +728,9 @@ __global__ void __launch_bounds__(kGateThreads) k_gated(const WeightsBf16* wg, c
     if (use_mlp && tc_ok && __syncthreads_or(plastic)) {
       float x[8];
       features(sc, tr, T, ep, x);
-#pragma unroll
-      for (int k = 0; k < 16; k += 2) st_pair(sm.x, km_off(r, k, 16), k < 8 ? x[k] : 0.f, k < 8 ? x[k + 1] : 0.f);
       float y[16];
-      tc_ok = tc_run(&sm.mbar, phase, [&] { tc_gemm(tm + 0, sm.x, sm.w1, 16, 64, false); });
+      tc_ok = gate_network(sm, tm, phase, x, y);
       if (tc_ok) {
-#pragma unroll
-        for (int c = 0; c < 4; ++c) {
-          float v[16];
-          tmem_ld16(tm + lane + 16 * c, v);
-#pragma unroll
-          for (int j = 0; j < 16; j += 2)
-            st_pair(sm.h1, km_off(r, 16 * c + j, 64), fmaxf(v[j] + sm.bias[16 * c + j], 0.f),
-                    fmaxf(v[j + 1] + sm.bias[16 * c + j + 1], 0.f));
-        }
-        tc_ok = tc_run(&sm.mbar, phase, [&] { tc_gemm(tm + 0, sm.h1, sm.w2, 64, 64, false); });
-      }
-      if (tc_ok) {
-#pragma unroll
-        for (int c = 0; c < 4; ++c) {
-          float v[16];
-          tmem_ld16(tm + lane + 16 * c, v);
-#pragma unroll
-          for (int j = 0; j < 16; j += 2)
-            st_pair(sm.h2, km_off(r, 16 * c + j, 64), fmaxf(v[j] + sm.bias[64 + 16 * c + j], 0.f),
-                    fmaxf(v[j + 1] + sm.bias[64 + 16 * c + j + 1], 0.f));
-        }
-        tc_ok = tc_run(&sm.mbar, phase, [&] { tc_gemm(tm + 64, sm.h2, sm.w3, 64, 16, false); });
-      }
-      if (tc_ok) {
-        tmem_ld16(tm + lane + 64, y);
 #pragma unroll
         for (int k = 0; k < 7; ++k) y[k] += sm.bias[128 + k];
       } else if (r == 0) {
@@ -782,15 +808,7 @@ __global__ void __launch_bounds__(kGateThreads) k_gated(const WeightsBf16* wg, c
       atomicAdd(&counts->fallback, c_fb);
     }
   }
-  if (use_mlp) {
-    if (!tc_ok) tc_wait(&sm.mbar, phase);  // one more bounded wait for a group still in flight
-    tc_fence_before();
-    __syncthreads();
-    if (warp == 0) {
-      tc_fence_after();
-      tc_dealloc(tm, kGateTmemCols);
-    }
-  }
+  if (use_mlp) gate_teardown(sm, tm, phase, tc_ok);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -1312,14 +1330,19 @@ static int time_jc(mpm_surrogate* s, const mpm_surrogate_config* cfg, int64_t n,
   cudaEvent_t ev[4];
   for (auto& x : ev) cudaEventCreate(&x);
   cudaError_t e = cudaMemsetAsync(dc, 0, sizeof(surr::GateOut), s->stream);
+  // the exact map: the reference's bisection for every plastic state; the learned map: the network
+  // as warp-wide tensor-core tiles (the fused pass's code), the refinement, the gate and the
+  // bisection for what it rejects. (A tcgen05 form with 128 states per tile measured 0.466 ms against
+  // 0.417 ms on 4,096,000 states: the CTA-wide barriers around its MMA groups cost more than the
+  // 10 kFLOP network saves.)
+  auto launch = [&](int mode, surr::GateOut* cnt) {
+    surr::k_gated_jc<<<blocks, 256, 0, s->stream>>>(s->wbf, s->params, s->mt, sp, (float)gate_tol, newton, mode, n, dep,
+                                                    cnt);
+  };
   for (int mode = 0; mode < 2 && e == cudaSuccess; ++mode) {
-    for (int w = 0; w < 2; ++w)
-      surr::k_gated_jc<<<blocks, 256, 0, s->stream>>>(s->wbf, s->params, s->mt, sp, (float)gate_tol, newton, mode, n,
-                                                      dep, nullptr);
+    for (int w = 0; w < 2; ++w) launch(mode, nullptr);
     cudaEventRecord(ev[2 * mode], s->stream);
-    for (int it = 0; it < iters; ++it)
-      surr::k_gated_jc<<<blocks, 256, 0, s->stream>>>(s->wbf, s->params, s->mt, sp, (float)gate_tol, newton, mode, n,
-                                                      dep, (mode == 1 && it == 0) ? dc : nullptr);
+    for (int it = 0; it < iters; ++it) launch(mode, (mode == 1 && it == 0) ? dc : nullptr);
     cudaEventRecord(ev[2 * mode + 1], s->stream);
     e = cudaGetLastError();
   }
