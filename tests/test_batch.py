@@ -99,6 +99,35 @@ def test_batch_graph_replay_matches_eager_launches():
 
 
 @pytest.mark.gpu
+def test_material_change_after_a_captured_graph_takes_effect():
+    """A material set after the batch captured a graph acts from the next run: the handle-wide
+    flags and kernel instances a graph holds (here: no plastic material, so no plastic strain is read
+    or written) are rebuilt. Three elastic scenes, one turned into a soft J2 material after a
+    captured run; the graph-replayed batch matches the same sequence run eagerly, and the changed
+    scene yields."""
+    from mpm_b200.solver import Batch
+    scenes = small_scenes()
+    for sc in scenes:
+        sc.materials = [Material.from_young(MODEL_FIXED_COROTATED, 1e5, .25, density=1000.)]
+    soft = Material.from_young(MODEL_J2, 1e5, .25, density=1000., yield_stress=5.0)
+    outs = []
+    for graph in (True, False):
+        b = Batch(scenes)
+        b.upload()
+        b.run(64, graph=graph)
+        b.set_material(0, soft)
+        b.run(64, graph=graph)
+        outs.append(b.split(b.download(("x", "v", "F", "ep"))))
+        assert b.status() == 0
+        b.close()
+    (og, oe) = outs
+    assert np.max(oe[0]["ep"]) > 0 and np.max(og[0]["ep"]) > 0
+    for k in range(len(scenes)):
+        for f in ("x", "v", "F", "ep"):
+            assert rel(og[k][f], oe[k][f]) <= 1e-5, (k, f, rel(og[k][f], oe[k][f]))
+
+
+@pytest.mark.gpu
 def test_batch_scene_one_substep_matches_oracle():
     from mpm_b200.solver import Batch
     from oracle import oracle as orc
