@@ -102,14 +102,16 @@ def test_batch_graph_replay_matches_eager_launches():
 def test_material_change_after_a_captured_graph_takes_effect():
     """A material set after the batch captured a graph acts from the next run: the handle-wide
     flags and kernel instances a graph holds (here: no plastic material, so no plastic strain is read
-    or written) are rebuilt. Three elastic scenes, one turned into a soft J2 material after a
-    captured run; the graph-replayed batch matches the same sequence run eagerly, and the changed
-    scene yields."""
+    or written) are rebuilt. Three elastic scenes, one turned into a J2 material after a captured
+    run; the graph-replayed batch matches the same sequence run eagerly, and the changed scene
+    yields."""
     from mpm_b200.solver import Batch
     scenes = small_scenes()
-    for sc in scenes:
-        sc.materials = [Material.from_young(MODEL_FIXED_COROTATED, 1e5, .25, density=1000.)]
-    soft = Material.from_young(MODEL_J2, 1e5, .25, density=1000., yield_stress=5.0)
+    # the J2 scenes start elastic (fixed-corotated, same moduli); scene 0 turns J2 after a run
+    scenes[0].materials = [Material.from_young(MODEL_FIXED_COROTATED, 1e5, .3, density=1000.)]
+    scenes[2].materials = [Material.from_young(MODEL_FIXED_COROTATED, 7e10, .33, density=2700.)]
+    # soft enough that its CFL substeps reach the floor within the runs, and it then yields
+    soft = Material.from_young(MODEL_J2, 1e5, .3, density=1000., yield_stress=5.0)
     outs = []
     for graph in (True, False):
         b = Batch(scenes)
