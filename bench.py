@@ -481,7 +481,9 @@ def learned_step_leg(args):
         exact and learned,
     both at one stated stress error: the gate accepts a prediction only when its consistency
     residual is at most gate_tol x the trial stress (the bisection's own FP32 residual is below it);
-    the end states of the two modes are compared."""
+    the end states of the modes are compared. Beside them the same refinement and gate without the
+    network (newton_gated: Newton from the initial flow stress's guess), what the network is
+    measured against."""
     import torch
     from mpm_b200 import scenes
     from mpm_b200.solver import Batch, Solver
@@ -500,11 +502,13 @@ def learned_step_leg(args):
     dt_req = scene.meta["dt"]
     K = args.steps
 
-    def timed(learned):
+    def timed(mode):
         sol = Solver(scene.domain, scene.n)
         sol.upload(scene)
-        if learned:
+        if mode == "learned":
             sol.set_return_mode(s, gate_tol=gate_tol, newton=newton)
+        elif mode == "newton":
+            sol.set_return_mode(mode="newton", gate_tol=gate_tol, newton=newton)
         ext = torch.cuda.ExternalStream(sol.stream())
         sol.run(dt_req, max(1, args.warmup))
         sol.gate_counts(reset=True)
@@ -522,12 +526,17 @@ def learned_step_leg(args):
         return {"value": scene.n * sub / (ms / 1e3), "ms_per_step": ms / K, "substeps": sub, "status": st,
                 "gate_learned": counts[0], "gate_fallback": counts[1]}, out
 
-    ex, ox = timed(False)
-    le, ol = timed(True)
+    ex, ox = timed(None)
+    le, ol = timed("learned")
+    ne, on = timed("newton")
     served = le["gate_learned"] / max(1, le["gate_learned"] + le["gate_fallback"])
     step = {"workload": scene.meta["workload"], "particles": scene.n, "requested_steps": K, "dt_requested": dt_req,
             "exact": ex, "learned": le, "speedup_learned_vs_exact": le["value"] / ex["value"],
             "learned_share_of_returns": served,
+            "newton_gated": ne, "speedup_newton_vs_exact": ne["value"] / ex["value"],
+            "newton_share_of_returns": ne["gate_learned"] / max(1, ne["gate_learned"] + ne["gate_fallback"]),
+            "newton_end_state_difference": {"x_m": float(np.max(np.abs(ox["x"] - on["x"]))),
+                                            "ep": float(np.max(np.abs(ox["ep"] - on["ep"])))},
             "end_state_difference": {"x_m": float(np.max(np.abs(ox["x"] - ol["x"]))),
                                      "ep": float(np.max(np.abs(ox["ep"] - ol["ep"]))),
                                      "F": float(np.max(np.abs(ox["F"] - ol["F"]))),
@@ -537,11 +546,13 @@ def learned_step_leg(args):
     Ke = args.ensemble_steps
     n_all = sum(sc.n for sc in ens)
 
-    def batch_run(learned):
+    def batch_run(mode):
         b = Batch(ens)
         b.upload()
-        if learned:
+        if mode == "learned":
             b.set_return_mode(s, gate_tol=gate_tol, newton=newton)
+        elif mode == "newton":
+            b.set_return_mode(mode="newton", gate_tol=gate_tol, newton=newton)
         b.run(Ke, graph=True)  # warm-up, captures the graph
         b.gate_counts(reset=True)
         torch.cuda.synchronize()
@@ -558,8 +569,9 @@ def learned_step_leg(args):
         return {"value": n_all * Ke / (ms / 1e3), "ms_per_substep": ms / Ke, "status": st,
                 "gate_learned": counts[0], "gate_fallback": counts[1]}
 
-    bex = batch_run(False)
-    ble = batch_run(True)
+    bex = batch_run(None)
+    ble = batch_run("learned")
+    bne = batch_run("newton")
     s.close()
     mlp_flop = 2 * (8 * 64 + 64 * 64 + 64 * 7)
     return {"law": "Johnson-Cook model 7 (A = B = yield, n 0.35, C 0.025, rate0 1/s; src/three/metal-plasticity.js:28-34, "
@@ -579,8 +591,9 @@ def learned_step_leg(args):
                                           "plastic": plastic_k},
             "step": step,
             "ensemble": {"workload": f"vv_ensemble_jc_{len(ens)}_seeds_1000", "particles": n_all, "substeps": Ke,
-                         "exact_batched": bex, "learned_batched": ble,
-                         "speedup_learned_vs_exact": ble["value"] / bex["value"]}}
+                         "exact_batched": bex, "learned_batched": ble, "newton_gated_batched": bne,
+                         "speedup_learned_vs_exact": ble["value"] / bex["value"],
+                         "speedup_newton_vs_exact": bne["value"] / bex["value"]}}
 
 
 def slab_leg(args, rank, world, dist):

@@ -517,6 +517,9 @@ int mpm_return_map_learned(mpm_surrogate* s, int64_t n, const double* F_in, cons
  * handle). Batch handles take it for all their scenes. */
 #define MPM_RETURN_EXACT 0
 #define MPM_RETURN_LEARNED_GATED 1
+/* The same refinement and gate without a network (s may be NULL): the Newton steps start from the
+ * root of the rate- and hardening-free condition, u0 = 1 - flow(ep, 0, T) / q. */
+#define MPM_RETURN_NEWTON_GATED 2
 int mpm_set_return_mode(mpm_handle* h, int32_t mode, mpm_surrogate* s, double gate_tol, int32_t newton);
 /* Returns served by the network (learned) and sent to the exact map (fallback) since the mode was
  * set or the counts were last reset (reset != 0 clears them after the read); elastic is 0. */

@@ -423,11 +423,14 @@ static int alloc_grid(mpm_handle* h) {
   return MPM_OK;
 }
 
-// The learned instances of the particle pass serve scenes without grid conduction and without the
-// history laws (snow, sand, pressure); anything else runs the exact return map.
+// The gated instances of the particle pass (learned: the network's guess; newton: a guess from the
+// initial flow stress) serve scenes without grid conduction and without the history laws (snow,
+// sand, pressure); anything else runs the exact return map.
 static void apply_return_mode(mpm_handle* h) {
-  h->ctx.learned = h->return_mode == MPM_RETURN_LEARNED_GATED && h->mlp_block && !h->ctx.has_aux && !h->ctx.conduct
-                       ? 1 : 0;
+  const bool eligible = h->mlp_block && !h->ctx.has_aux && !h->ctx.conduct;
+  h->ctx.learned = eligible && h->return_mode == MPM_RETURN_LEARNED_GATED   ? 1
+                   : eligible && h->return_mode == MPM_RETURN_NEWTON_GATED ? 2
+                                                                             : 0;
 }
 
 static void refresh_flags(mpm_handle* h) {
@@ -1950,14 +1953,17 @@ int mpm_set_return_mode(mpm_handle* h, int32_t mode, mpm_surrogate* s, double ga
     drop_graph(h);
     return MPM_OK;
   }
-  if (mode != MPM_RETURN_LEARNED_GATED || !s) return fail(h, MPM_ERR_INVALID_ARG, "mode must be exact or learned_gated with a network");
-  if (!mpm::learned_model(surr::surrogate_model(s)))
+  const bool net = mode == MPM_RETURN_LEARNED_GATED;
+  if (!(net && s) && mode != MPM_RETURN_NEWTON_GATED)
+    return fail(h, MPM_ERR_INVALID_ARG, "mode must be exact, learned_gated with a network, or newton_gated");
+  if (net && !mpm::learned_model(surr::surrogate_model(s)))
     return fail(h, MPM_ERR_UNSUPPORTED, "the learned return mode serves networks trained for Johnson-Cook (models 6, 7)");
   if (!(gate_tol > 0) || !(gate_tol < 1)) return fail(h, MPM_ERR_INVALID_ARG, "gate_tol must lie in (0, 1)");
   if (newton < 0 || newton > 8) return fail(h, MPM_ERR_INVALID_ARG, "newton must lie in [0, 8]");
   if (h->ctx.has_aux || h->ctx.conduct)
-    return fail(h, MPM_ERR_UNSUPPORTED, "the learned return mode serves scenes without conduction and without snow, sand "
+    return fail(h, MPM_ERR_UNSUPPORTED, "the gated return modes serve scenes without conduction and without snow, sand "
                                         "or pressure materials");
+  // one device block: the network's BF16 weights and FP32 parameters (learned mode), then the counts
   const size_t wbytes = surr::weights_bytes();
   if (!h->mlp_block) {
     MPM_CUDA(h, cudaMalloc(&h->mlp_block, wbytes + surr::kParams * sizeof(float) + 16));
@@ -1965,8 +1971,10 @@ int mpm_set_return_mode(mpm_handle* h, int32_t mode, mpm_surrogate* s, double ga
   char* base = static_cast<char*>(h->mlp_block);
   float* params = reinterpret_cast<float*>(base + wbytes);
   unsigned* counts = reinterpret_cast<unsigned*>(params + surr::kParams);
-  const int rc = surr::export_weights(s, base, params, h->stream);
-  if (rc != MPM_OK) return fail(h, rc, "copying the network's weights failed");
+  if (net) {
+    const int rc = surr::export_weights(s, base, params, h->stream);
+    if (rc != MPM_OK) return fail(h, rc, "copying the network's weights failed");
+  }
   MPM_CUDA(h, cudaMemsetAsync(counts, 0, 16, h->stream));
   MPM_CUDA(h, cudaStreamSynchronize(h->stream));
   h->ctx.mlp_w = base;
@@ -1974,7 +1982,7 @@ int mpm_set_return_mode(mpm_handle* h, int32_t mode, mpm_surrogate* s, double ga
   h->ctx.gate_counts = counts;
   h->ctx.gate_tol = static_cast<float>(gate_tol);
   h->ctx.learned_newton = newton;
-  h->return_mode = MPM_RETURN_LEARNED_GATED;
+  h->return_mode = mode;
   apply_return_mode(h);
   drop_graph(h);
   return MPM_OK;

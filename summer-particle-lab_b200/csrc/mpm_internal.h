@@ -164,7 +164,7 @@ struct Ctx {
   // learned return mode (Johnson-Cook laws): the network's BF16 weights and FP32 parameters (the
   // handle's own copy), the gate's residual tolerance, the most Newton steps after the prediction,
   // and the counts of returns the gate accepted and sent to the exact map (2 unsigned)
-  int learned;
+  int learned;         // 0 exact, 1 the network's guess, 2 the guess from the initial flow stress
   int learned_newton;
   float gate_tol;
   const void* mlp_w;

@@ -1138,6 +1138,26 @@ static __device__ __forceinline__ float learned_jc_return(const void* mlp_w, con
   return r.dep;
 }
 
+// The Newton-gated Johnson-Cook return without a network: the same refinement, gate and counts as
+// learned_jc_return, from the root of the rate- and hardening-free consistency condition,
+// u0 = 1 - flow(ep, 0, T) / q (the elastic predictor's excess over the initial flow stress).
+// Every lane of the warp calls it (the counts are warp ballots).
+static __device__ __forceinline__ float newton_jc_return(const MaterialDev& mt, float q, float J, float ep, float T,
+                                                        float dt, bool need, float tol, int newton, unsigned* gate) {
+  JcRefined r{0.f, false};
+  if (need) {
+    const float u0 = fminf(1.f, fmaxf(0.f, 1.f - jc_flow(mt, ep, 0.f, T) / q));
+    r = jc_refine(mt, q, J, ep, T, dt, u0, tol, newton);
+  }
+  const unsigned acc = __ballot_sync(0xffffffffu, need && r.ok), rej = __ballot_sync(0xffffffffu, need && !r.ok);
+  if ((threadIdx.x & 31) == 0) {
+    if (acc) atomicAdd(&gate[0], __popc(acc));
+    if (rej) atomicAdd(&gate[1], __popc(rej));
+  }
+  if (need && !r.ok) r.dep = jc_bisect(mt, q, J, ep, T, dt);
+  return r.dep;
+}
+
 // Phase A of the learned return mode (fused or gather-only pass; scenes without conduction and
 // without the history laws). The same particle update as particle_phase_a, with the plastic
 // increment of Johnson-Cook trial states (src/three/metal-plasticity.js:28-34) taken from the
@@ -1146,8 +1166,9 @@ static __device__ __forceinline__ float learned_jc_return(const void* mlp_w, con
 // consistency residual passes the gate (|g| <= gate_tol, i.e. the stress residual is at most
 // gate_tol x the trial stress), and every other lane runs the exact bisection. Every lane of the
 // warp calls it: lanes past the end of the round (live false) read the round's first particle,
-// take part in the network evaluation and write nothing.
-template <int PASS>
+// take part in the network evaluation and write nothing. MODE 1: the network's guess; MODE 2: the
+// guess from the initial flow stress (newton_jc_return), no network.
+template <int PASS, int MODE>
 __device__ __forceinline__ unsigned particle_phase_a_learned(const Ctx& c, const SceneDev& sc, const TileCtx& tc,
                                                              const MaterialDev& mt_single, bool single,
                                                              const float4* vwin, bool live, unsigned home, unsigned j,
@@ -1237,9 +1258,13 @@ __device__ __forceinline__ unsigned particle_phase_a_learned(const Ctx& c, const
   // the warp's learned return (every lane arrives here)
   const bool need = live && series && learned_model(mt.model) && tr.q > jc_flow(mt, ep, 0.f, T);
   float dep_learned = 0.f;
-  if (__any_sync(0xffffffffu, need))
-    dep_learned = learned_jc_return(c.mlp_w, c.mlp_params, mt, tr.q, tr.J, ep, T, dt, need, c.gate_tol,
-                                    c.learned_newton, gate);
+  if (__any_sync(0xffffffffu, need)) {
+    if constexpr (MODE == 1)
+      dep_learned = learned_jc_return(c.mlp_w, c.mlp_params, mt, tr.q, tr.J, ep, T, dt, need, c.gate_tol,
+                                      c.learned_newton, gate);
+    else
+      dep_learned = newton_jc_return(mt, tr.q, tr.J, ep, T, dt, need, c.gate_tol, c.learned_newton, gate);
+  }
   ConstitutiveOut co;
   if (moving) {
     if (series) {
@@ -1374,9 +1399,11 @@ __device__ __forceinline__ void prefetch_tile_state(const Ctx& c, uint4 it) {
   if (c.has_pinned) pf(c.p.pinned, 1);
 }
 
-template <int PASS, bool HEAT, bool AUX, bool LEARNED = false>
+// JC: 0 the exact return map; 1 and 2 the gated Johnson-Cook returns (1 from the network's guess,
+// 2 from the initial flow stress), scenes without conduction and without the history laws.
+template <int PASS, bool HEAT, bool AUX, int JC = 0>
 __global__ void __launch_bounds__(kBlock, 2) k_particles(const __grid_constant__ Ctx c) {
-  static_assert(!LEARNED || (!HEAT && !AUX && PASS != kPassP2G), "learned instances: no conduction, no history laws");
+  static_assert(JC == 0 || (!HEAT && !AUX && PASS != kPassP2G), "gated instances: no conduction, no history laws");
   extern __shared__ __align__(128) unsigned char smem_raw[];
   PartSmem& sm = *reinterpret_cast<PartSmem*>(smem_raw);
   constexpr bool SCATTER = PASS != kPassG2P;
@@ -1509,7 +1536,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_particles(const __grid_constant__
       for (unsigned jj = 0; jj < nround; jj += kBlock) {
         const unsigned j = jj + threadIdx.x;
         unsigned key = 0xffffffffu;
-        if constexpr (LEARNED) {
+        if constexpr (JC != 0) {
           // every lane of a warp with a live particle takes part in its network evaluation (warps
           // past the end of the round skip as a whole)
           if (jj + (threadIdx.x & ~31u) >= nround) continue;
@@ -1517,7 +1544,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_particles(const __grid_constant__
           const unsigned home = !live ? c.p.perm[it.y + r0]
                                       : (r0 == 0 && sm.pf_ok && jj < kPf * kBlock) ? sm.pfs[jj + threadIdx.x]
                                                                                  : c.p.perm[it.y + r0 + j];
-          key = particle_phase_a_learned<PASS>(c, sc, tc, sm.mt, single, sm.vwin[cb], live, home, j, dt, nxt, sm.pay,
+          key = particle_phase_a_learned<PASS, JC>(c, sc, tc, sm.mt, single, sm.vwin[cb], live, home, j, dt, nxt, sm.pay,
                                                sm.meta, sm.hist, wave_acc, grad_acc, flags_acc, sm.work_sum, store_vc,
                                                sm.gate);
         } else if (j < nround) {
@@ -1565,7 +1592,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_particles(const __grid_constant__
     if (SCATTER) flush_window(c, sc, sm, nxt, tc.tile);
     cb ^= 1;
   }
-  if (LEARNED && threadIdx.x == 0) {  // gate counts: one atomic each per CTA (the loop ended at a barrier)
+  if (JC != 0 && threadIdx.x == 0) {  // gate counts: one atomic each per CTA (the loop ended at a barrier)
     if (sm.gate[0]) atomicAdd(&c.gate_counts[0], sm.gate[0]);
     if (sm.gate[1]) atomicAdd(&c.gate_counts[1], sm.gate[1]);
   }
@@ -1876,8 +1903,12 @@ __global__ void __launch_bounds__(kWsThreads, 1) k_particles_ws(const __grid_con
 template <int PASS, bool HEAT, bool AUX>
 static void launch_pass_t(const Ctx& c, cudaStream_t st, int grid_blocks) {
   if constexpr (PASS != kPassP2G && !HEAT && !AUX) {
-    if (c.learned) {
-      k_particles<PASS, false, false, true><<<grid_blocks, kBlock, sizeof(PartSmem), st>>>(c);
+    if (c.learned == 1) {
+      k_particles<PASS, false, false, 1><<<grid_blocks, kBlock, sizeof(PartSmem), st>>>(c);
+      return;
+    }
+    if (c.learned == 2) {
+      k_particles<PASS, false, false, 2><<<grid_blocks, kBlock, sizeof(PartSmem), st>>>(c);
       return;
     }
   }
@@ -1917,8 +1948,10 @@ static int blocks_per_sm() {
   cudaFuncSetAttribute(k_particles<PASS, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
   cudaFuncSetAttribute(k_particles<PASS, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
   cudaFuncSetAttribute(k_particles<PASS, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-  if constexpr (PASS != kPassP2G)
-    cudaFuncSetAttribute(k_particles<PASS, false, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  if constexpr (PASS != kPassP2G) {
+    cudaFuncSetAttribute(k_particles<PASS, false, false, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    cudaFuncSetAttribute(k_particles<PASS, false, false, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+  }
   int n = 0;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_particles<PASS, false, false>, kBlock, sizeof(PartSmem));
   return n > 0 ? n : 1;

@@ -90,7 +90,7 @@ class MpmGateCounts(ctypes.Structure):
 
 
 SURROGATE_PARAMS = 5768
-RETURN_EXACT, RETURN_LEARNED_GATED = 0, 1
+RETURN_EXACT, RETURN_LEARNED_GATED, RETURN_NEWTON_GATED = 0, 1, 2
 
 
 class MpmFrameInfo(ctypes.Structure):

@@ -258,10 +258,16 @@ class Solver:
         """One regularisation pass now (regularizeSolids(s, dt) after a step)."""
         self._check(_lib.lib().mpm_regularize(self.h, float(dt)))
 
-    def set_return_mode(self, surrogate=None, gate_tol=1e-5, newton=8):
+    def set_return_mode(self, surrogate=None, gate_tol=1e-5, newton=8, mode=None):
         """Learned return map inside the step (mpm_set_return_mode) with a Johnson-Cook network, or
-        the exact map again with surrogate None."""
-        if surrogate is None:
+        the exact map again with surrogate None. mode="newton": the same refinement and gate from
+        the initial flow stress's guess, without a network."""
+        if mode == "newton":
+            self._check(_lib.lib().mpm_set_return_mode(self.h, _lib.RETURN_NEWTON_GATED, None, float(gate_tol),
+                                                       int(newton)))
+        elif mode is not None:
+            raise ValueError("mode must be None or 'newton'")
+        elif surrogate is None:
             self._check(_lib.lib().mpm_set_return_mode(self.h, _lib.RETURN_EXACT, None, 0.0, 0))
         else:
             self._check(_lib.lib().mpm_set_return_mode(self.h, _lib.RETURN_LEARNED_GATED, surrogate.h, float(gate_tol),

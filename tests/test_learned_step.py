@@ -101,6 +101,25 @@ def test_learned_step_on_dense_tiles_matches_oracle(trained):
     assert learned >= 0.8 * (learned + fallback), (learned, fallback)
 
 
+def test_newton_gated_step_without_a_network_matches_oracle():
+    """The same refinement and gate started from the initial flow stress's guess, u0 = 1 - flow(ep,
+    0, T) / q, with no network (mpm_set_return_mode with MPM_RETURN_NEWTON_GATED): within the oracle
+    bounds after ten substeps, and with eight Newton steps it serves nearly every return."""
+    sc = impact_scene()
+    st = oracle_run(sc)
+    sol = Solver(sc.domain, sc.n)
+    sol.upload(sc)
+    sol.set_return_mode(mode="newton", gate_tol=GATE_TOL, newton=8)
+    sol.step_fixed(1e-6, 10)
+    out = sol.download()
+    served, fallback = sol.gate_counts()
+    assert sol.status() == 0
+    sol.close()
+    check_parity(out, st)
+    assert served + fallback > 500
+    assert served >= 0.95 * (served + fallback), (served, fallback)
+
+
 def test_exact_mode_restores_the_reference_map(trained):
     sc = impact_scene()
     sol = Solver(sc.domain, sc.n)
