@@ -497,6 +497,7 @@ def learned_step_leg(args):
     hist = s.train(cfg)
     train_s = time.perf_counter() - t0
     kern = s.time(4_096_000, iters=10, gate_tol=gate_tol, cfg=cfg)
+    kern_nw = s.time_newton(4_096_000, iters=10, gate_tol=gate_tol, cfg=cfg)
     plastic_k = kern["learned"] + kern["fallback"]
     scene = scenes.jc_impact()
     dt_req = scene.meta["dt"]
@@ -588,7 +589,11 @@ def learned_step_leg(args):
             "return_map_4096000_states": {"ms_exact": kern["ms_exact"], "ms_learned": kern["ms_learned"],
                                           "speedup": kern["ms_exact"] / kern["ms_learned"],
                                           "learned_share_of_plastic": kern["learned"] / max(1, plastic_k),
-                                          "plastic": plastic_k},
+                                          "plastic": plastic_k,
+                                          "ms_newton_gated": kern_nw["ms"],
+                                          "speedup_newton_vs_exact": kern["ms_exact"] / kern_nw["ms"],
+                                          "newton_share_of_plastic": kern_nw["accepted"] / max(
+                                              1, kern_nw["accepted"] + kern_nw["fallback"])},
             "step": step,
             "ensemble": {"workload": f"vv_ensemble_jc_{len(ens)}_seeds_1000", "particles": n_all, "substeps": Ke,
                          "exact_batched": bex, "learned_batched": ble, "newton_gated_batched": bne,

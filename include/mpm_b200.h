@@ -529,6 +529,11 @@ int mpm_gate_counts_read(mpm_handle* h, mpm_gate_counts* out, int32_t reset);
  * states drawn like cfg's training set (iters calls each, CUDA events). */
 int mpm_surrogate_time(mpm_surrogate* s, const mpm_surrogate_config* cfg, int64_t n, int32_t iters, double gate_tol,
                        double* ms_exact, double* ms_learned, mpm_gate_counts* counts);
+/* The same random Johnson-Cook states through the Newton-gated map without the network (the
+ * refinement and gate of the learned map from u0 = 1 - flow(ep, 0, T) / q, the bisection for what the
+ * gate rejects): device time per call; counts as above (learned = accepted). */
+int mpm_surrogate_time_newton(mpm_surrogate* s, const mpm_surrogate_config* cfg, int64_t n, int32_t iters,
+                              double gate_tol, double* ms, mpm_gate_counts* counts);
 
 /* ======================================================================================
  * 2D elastic solid: drop-in for the reference's SolidMPM (src/solid-mpm.js:20-116).

@@ -862,8 +862,9 @@ __global__ void k_samples_jc(mpm::MaterialDev mt, SampleSpec sp, long long n, fl
 }
 
 // The plastic increment of random Johnson-Cook trial states: exact bisection for every state
-// (use_mlp 0), or the network (warp-wide tensor-core tiles) + Newton refinement + gate with the
-// bisection for rejected states. dep out (keeps the work); counts: elastic, accepted, rejected.
+// (use_mlp 0), or the network (warp-wide tensor-core tiles, use_mlp 1) or the initial flow stress's
+// guess (use_mlp 2) + Newton refinement + gate with the bisection for rejected states. dep out
+// (keeps the work); counts: elastic, accepted, rejected.
 __global__ void __launch_bounds__(256) k_gated_jc(const WeightsBf16* wg, const float* params, mpm::MaterialDev mt,
                                                   SampleSpec sp, float gate_tol, int newton, int use_mlp, long long n,
                                                   float* dep_out, GateOut* counts) {
@@ -875,7 +876,7 @@ __global__ void __launch_bounds__(256) k_gated_jc(const WeightsBf16* wg, const f
     const bool plastic = live && st.q > mpm::jc_flow(mt, st.ep, 0.f, st.T);
     float dep = 0.f;
     bool accepted = false;
-    if (use_mlp) {
+    if (use_mlp == 1) {
       float x[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
       if (plastic) mpm::jc_features(mt, st.q, st.J, st.ep, st.T, st.dt, x);
       const float u = warp_predict_first(wg, params, x, plastic);
@@ -884,6 +885,11 @@ __global__ void __launch_bounds__(256) k_gated_jc(const WeightsBf16* wg, const f
         dep = r.dep;
         accepted = r.ok;
       }
+    } else if (use_mlp == 2 && plastic) {  // the same refinement from the initial flow stress's guess
+      const float u0 = fminf(1.f, fmaxf(0.f, 1.f - mpm::jc_flow(mt, st.ep, 0.f, st.T) / st.q));
+      const mpm::JcRefined r = mpm::jc_refine(mt, st.q, st.J, st.ep, st.T, st.dt, u0, gate_tol, newton);
+      dep = r.dep;
+      accepted = r.ok;
     }
     if (plastic && !accepted) dep = mpm::jc_bisect(mt, st.q, st.J, st.ep, st.T, st.dt);
     if (live) {
@@ -1423,6 +1429,47 @@ int mpm_surrogate_time(mpm_surrogate* s, const mpm_surrogate_config* cfg, int64_
     counts->fallback = hc.fallback;
   }
   return check_tc(s);
+}
+
+int mpm_surrogate_time_newton(mpm_surrogate* s, const mpm_surrogate_config* cfg, int64_t n, int32_t iters,
+                              double gate_tol, double* ms, mpm_gate_counts* counts) {
+  if (!s || !cfg || !ms || n <= 0 || iters <= 0 || !(gate_tol > 0)) return MPM_ERR_INVALID_ARG;
+  if (!is_jc(s)) return sfail(s, MPM_ERR_UNSUPPORTED, "the Newton-gated map serves the Johnson-Cook laws (models 6, 7)");
+  const surr::SampleSpec sp = spec_of(cfg);
+  const int newton = cfg->newton > 0 ? cfg->newton : 8;
+  float* dep = nullptr;
+  surr::GateOut* dc = nullptr;
+  SCUDA(s, cudaMalloc(&dep, n * sizeof(float)));
+  SCUDA(s, cudaMalloc(&dc, sizeof(surr::GateOut)));
+  const int blocks = (int)std::min<long long>(s->num_sms * 8, (n + 255) / 256);
+  cudaEvent_t ev[2];
+  for (auto& x : ev) cudaEventCreate(&x);
+  cudaError_t e = cudaMemsetAsync(dc, 0, sizeof(surr::GateOut), s->stream);
+  for (int w = 0; w < 2 && e == cudaSuccess; ++w)
+    surr::k_gated_jc<<<blocks, 256, 0, s->stream>>>(s->wbf, s->params, s->mt, sp, (float)gate_tol, newton, 2, n, dep,
+                                                    nullptr);
+  cudaEventRecord(ev[0], s->stream);
+  for (int it = 0; it < iters && e == cudaSuccess; ++it)
+    surr::k_gated_jc<<<blocks, 256, 0, s->stream>>>(s->wbf, s->params, s->mt, sp, (float)gate_tol, newton, 2, n, dep,
+                                                    it == 0 ? dc : nullptr);
+  cudaEventRecord(ev[1], s->stream);
+  if (e == cudaSuccess) e = cudaGetLastError();
+  surr::GateOut hc{};
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&hc, dc, sizeof hc, cudaMemcpyDeviceToHost, s->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+  float t = 0;
+  if (e == cudaSuccess) cudaEventElapsedTime(&t, ev[0], ev[1]);
+  for (auto& x : ev) cudaEventDestroy(x);
+  cudaFree(dep);
+  cudaFree(dc);
+  if (e != cudaSuccess) return sfail(s, MPM_ERR_CUDA, cudaGetErrorString(e));
+  *ms = t / iters;
+  if (counts) {
+    counts->elastic = hc.elastic;
+    counts->learned = hc.learned;
+    counts->fallback = hc.fallback;
+  }
+  return MPM_OK;
 }
 
 }  // extern "C"

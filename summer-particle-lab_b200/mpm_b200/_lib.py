@@ -188,6 +188,8 @@ SIGNATURES = {
                                                ctypes.POINTER(MpmGateCounts)]),
     "mpm_surrogate_time": (ctypes.c_int, [_P, ctypes.POINTER(MpmSurrogateConfig), _I64, _I32, _D, ctypes.POINTER(_D),
                                            ctypes.POINTER(_D), ctypes.POINTER(MpmGateCounts)]),
+    "mpm_surrogate_time_newton": (ctypes.c_int, [_P, ctypes.POINTER(MpmSurrogateConfig), _I64, _I32, _D,
+                                                  ctypes.POINTER(_D), ctypes.POINTER(MpmGateCounts)]),
     "mpm_set_return_mode": (ctypes.c_int, [_P, _I32, _P, _D, _I32]),
     "mpm_gate_counts_read": (ctypes.c_int, [_P, ctypes.POINTER(MpmGateCounts), _I32]),
     "smpm_create": (ctypes.c_int, [_I64, ctypes.POINTER(_P)]),

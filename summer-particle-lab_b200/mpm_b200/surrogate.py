@@ -132,3 +132,13 @@ class Surrogate:
                                                   ctypes.byref(ml), ctypes.byref(c)))
         return dict(ms_exact=me.value, ms_learned=ml.value, elastic=c.elastic, learned=c.learned,
                     fallback=c.fallback)
+
+    def time_newton(self, n, iters=10, gate_tol=1e-5, cfg=None):
+        """The same Johnson-Cook states through the Newton-gated map without the network
+        (mpm_surrogate_time_newton): device ms per call and the gate's counts."""
+        cfg = cfg or jc_config()
+        ms = ctypes.c_double()
+        c = MpmGateCounts()
+        self._check(_lib.lib().mpm_surrogate_time_newton(self.h, ctypes.byref(cfg), n, iters, gate_tol, ctypes.byref(ms),
+                                                         ctypes.byref(c)))
+        return dict(ms=ms.value, elastic=c.elastic, accepted=c.learned, fallback=c.fallback)

@@ -178,3 +178,13 @@ def test_kernel_level_timing_reports_counts(trained):
     plastic = r["learned"] + r["fallback"]
     assert plastic > 100_000
     assert r["learned"] >= 0.8 * plastic, r
+
+
+def test_newton_gated_standalone_map_reports_counts(trained):
+    """mpm_surrogate_time_newton on the same random Johnson-Cook states: the network-free map runs
+    and its gate accepts nearly every plastic state within eight Newton steps."""
+    r = trained.time_newton(1_000_000, iters=2, gate_tol=GATE_TOL, cfg=jc_config())
+    assert r["ms"] > 0
+    plastic = r["accepted"] + r["fallback"]
+    assert plastic > 100_000
+    assert r["accepted"] >= 0.95 * plastic, r
