@@ -911,12 +911,17 @@ __device__ __noinline__ Gather12 gather_global(const float4* base, int sy, long 
 // for the P2G pass and pinned particles, the stress of the stored state; then the scatter payload
 // bucketed by its new stencil base in the shared window (pay, meta, hist), and the CFL terms.
 // Writes the particle's new state and returns its next sort key (all ones when not needed).
-template <int PASS, bool HEAT, bool AUX>
+// NEWTON (the Newton-gated return mode): a Johnson-Cook trial stress above the initial flow stress
+// takes the gated refinement from u0 = 1 - flow(ep, 0, T) / q instead of the bisection, which stays
+// the fallback; gate[0] / gate[1] count the returns accepted / sent to the bisection.
+template <int PASS, bool HEAT, bool AUX, bool NEWTON = false>
 __device__ __forceinline__ unsigned particle_phase_a(const Ctx& c, const SceneDev& sc, const TileCtx& tc,
                                                      const MaterialDev& mt_single, bool single, const float4* vwin,
                                                      unsigned home, unsigned j, float dt, int nxt, float2* pay,
                                                      unsigned* meta, int* hist, float& wave_acc, float& grad_acc,
-                                                     unsigned& flags_acc, double& work_acc, bool store_vc) {
+                                                     unsigned& flags_acc, double& work_acc, bool store_vc,
+                                                     unsigned* gate = nullptr) {
+  static_assert(!NEWTON || (!HEAT && !AUX && PASS != kPassP2G), "Newton-gated returns: J2-type laws, gather passes");
   constexpr bool SCATTER = PASS != kPassG2P;
   constexpr bool GATHER = PASS != kPassP2G;
   unsigned key = 0xffffffffu;
@@ -1014,7 +1019,31 @@ __device__ __forceinline__ unsigned particle_phase_a(const Ctx& c, const SceneDe
       q[a] = static_cast<unsigned>(qn);
     }
     // return map / stress for the next P2G (src/three/mpm.js:126-131)
-    co = constitutive_update_t<AUX>(mt, D, ep, aux, T, V / m, true, dt, xp);
+    if constexpr (NEWTON) {
+      const Sym3 B = cauchy_green_minus_identity(D);
+      const int nt = learned_model(mt.model) ? series_terms_sq(sym_norm2(B)) : 0;
+      if (nt > 0) {  // the series path of constitutive_update_t with the gated Johnson-Cook return
+        const J2Trial tr = j2_trial_series(mt, B, nt);
+        float dep = 0.f;
+        const float f0 = jc_flow(mt, ep, 0.f, T);
+        if (tr.q > f0) {
+          const float u0 = fminf(1.f, fmaxf(0.f, 1.f - f0 / tr.q));
+          const JcRefined r = jc_refine(mt, tr.q, tr.J, ep, T, dt, u0, c.gate_tol, c.learned_newton);
+          dep = r.ok ? r.dep : jc_bisect(mt, tr.q, tr.J, ep, T, dt);
+          // one shared atomic per group of converged lanes
+          const unsigned act = __activemask(), acc = __ballot_sync(act, r.ok);
+          if ((threadIdx.x & 31) == __ffs(act) - 1) {
+            if (acc) atomicAdd(&gate[0], __popc(acc));
+            if (act & ~acc) atomicAdd(&gate[1], __popc(act & ~acc));
+          }
+        }
+        co = j2_finish(mt, tr, D, dep, V / m);
+      } else {
+        co = constitutive_update_t<AUX>(mt, D, ep, aux, T, V / m, true, dt, xp);
+      }
+    } else {
+      co = constitutive_update_t<AUX>(mt, D, ep, aux, T, V / m, true, dt, xp);
+    }
     ep += co.dep;
     T += co.dT;
     c.p.qx[home] = q[0]; c.p.qy[home] = q[1]; c.p.qz[home] = q[2];
@@ -1138,26 +1167,6 @@ static __device__ __forceinline__ float learned_jc_return(const void* mlp_w, con
   return r.dep;
 }
 
-// The Newton-gated Johnson-Cook return without a network: the same refinement, gate and counts as
-// learned_jc_return, from the root of the rate- and hardening-free consistency condition,
-// u0 = 1 - flow(ep, 0, T) / q (the elastic predictor's excess over the initial flow stress).
-// Every lane of the warp calls it (the counts are warp ballots).
-static __device__ __forceinline__ float newton_jc_return(const MaterialDev& mt, float q, float J, float ep, float T,
-                                                        float dt, bool need, float tol, int newton, unsigned* gate) {
-  JcRefined r{0.f, false};
-  if (need) {
-    const float u0 = fminf(1.f, fmaxf(0.f, 1.f - jc_flow(mt, ep, 0.f, T) / q));
-    r = jc_refine(mt, q, J, ep, T, dt, u0, tol, newton);
-  }
-  const unsigned acc = __ballot_sync(0xffffffffu, need && r.ok), rej = __ballot_sync(0xffffffffu, need && !r.ok);
-  if ((threadIdx.x & 31) == 0) {
-    if (acc) atomicAdd(&gate[0], __popc(acc));
-    if (rej) atomicAdd(&gate[1], __popc(rej));
-  }
-  if (need && !r.ok) r.dep = jc_bisect(mt, q, J, ep, T, dt);
-  return r.dep;
-}
-
 // Phase A of the learned return mode (fused or gather-only pass; scenes without conduction and
 // without the history laws). The same particle update as particle_phase_a, with the plastic
 // increment of Johnson-Cook trial states (src/three/metal-plasticity.js:28-34) taken from the
@@ -1166,9 +1175,8 @@ static __device__ __forceinline__ float newton_jc_return(const MaterialDev& mt, 
 // consistency residual passes the gate (|g| <= gate_tol, i.e. the stress residual is at most
 // gate_tol x the trial stress), and every other lane runs the exact bisection. Every lane of the
 // warp calls it: lanes past the end of the round (live false) read the round's first particle,
-// take part in the network evaluation and write nothing. MODE 1: the network's guess; MODE 2: the
-// guess from the initial flow stress (newton_jc_return), no network.
-template <int PASS, int MODE>
+// take part in the network evaluation and write nothing.
+template <int PASS>
 __device__ __forceinline__ unsigned particle_phase_a_learned(const Ctx& c, const SceneDev& sc, const TileCtx& tc,
                                                              const MaterialDev& mt_single, bool single,
                                                              const float4* vwin, bool live, unsigned home, unsigned j,
@@ -1258,13 +1266,9 @@ __device__ __forceinline__ unsigned particle_phase_a_learned(const Ctx& c, const
   // the warp's learned return (every lane arrives here)
   const bool need = live && series && learned_model(mt.model) && tr.q > jc_flow(mt, ep, 0.f, T);
   float dep_learned = 0.f;
-  if (__any_sync(0xffffffffu, need)) {
-    if constexpr (MODE == 1)
-      dep_learned = learned_jc_return(c.mlp_w, c.mlp_params, mt, tr.q, tr.J, ep, T, dt, need, c.gate_tol,
-                                      c.learned_newton, gate);
-    else
-      dep_learned = newton_jc_return(mt, tr.q, tr.J, ep, T, dt, need, c.gate_tol, c.learned_newton, gate);
-  }
+  if (__any_sync(0xffffffffu, need))
+    dep_learned = learned_jc_return(c.mlp_w, c.mlp_params, mt, tr.q, tr.J, ep, T, dt, need, c.gate_tol,
+                                    c.learned_newton, gate);
   ConstitutiveOut co;
   if (moving) {
     if (series) {
@@ -1400,7 +1404,8 @@ __device__ __forceinline__ void prefetch_tile_state(const Ctx& c, uint4 it) {
 }
 
 // JC: 0 the exact return map; 1 and 2 the gated Johnson-Cook returns (1 from the network's guess,
-// 2 from the initial flow stress), scenes without conduction and without the history laws.
+// warp-collective phase A; 2 from the initial flow stress, the plain phase A with the gated
+// return), scenes without conduction and without the history laws.
 template <int PASS, bool HEAT, bool AUX, int JC = 0>
 __global__ void __launch_bounds__(kBlock, 2) k_particles(const __grid_constant__ Ctx c) {
   static_assert(JC == 0 || (!HEAT && !AUX && PASS != kPassP2G), "gated instances: no conduction, no history laws");
@@ -1536,7 +1541,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_particles(const __grid_constant__
       for (unsigned jj = 0; jj < nround; jj += kBlock) {
         const unsigned j = jj + threadIdx.x;
         unsigned key = 0xffffffffu;
-        if constexpr (JC != 0) {
+        if constexpr (JC == 1) {
           // every lane of a warp with a live particle takes part in its network evaluation (warps
           // past the end of the round skip as a whole)
           if (jj + (threadIdx.x & ~31u) >= nround) continue;
@@ -1544,13 +1549,14 @@ __global__ void __launch_bounds__(kBlock, 2) k_particles(const __grid_constant__
           const unsigned home = !live ? c.p.perm[it.y + r0]
                                       : (r0 == 0 && sm.pf_ok && jj < kPf * kBlock) ? sm.pfs[jj + threadIdx.x]
                                                                                  : c.p.perm[it.y + r0 + j];
-          key = particle_phase_a_learned<PASS, JC>(c, sc, tc, sm.mt, single, sm.vwin[cb], live, home, j, dt, nxt, sm.pay,
+          key = particle_phase_a_learned<PASS>(c, sc, tc, sm.mt, single, sm.vwin[cb], live, home, j, dt, nxt, sm.pay,
                                                sm.meta, sm.hist, wave_acc, grad_acc, flags_acc, sm.work_sum, store_vc,
                                                sm.gate);
         } else if (j < nround) {
           const unsigned home = (r0 == 0 && sm.pf_ok && jj < kPf * kBlock) ? sm.pfs[jj + threadIdx.x] : c.p.perm[sm.item[cb].y + r0 + j];
-          key = particle_phase_a<PASS, HEAT, AUX>(c, sc, tc, sm.mt, single, sm.vwin[cb], home, j, dt, nxt, sm.pay, sm.meta,
-                                       sm.hist, wave_acc, grad_acc, flags_acc, sm.work_sum, store_vc);
+          key = particle_phase_a<PASS, HEAT, AUX, JC == 2>(c, sc, tc, sm.mt, single, sm.vwin[cb], home, j, dt, nxt,
+                                                           sm.pay, sm.meta, sm.hist, wave_acc, grad_acc, flags_acc,
+                                                           sm.work_sum, store_vc, sm.gate);
         }
         if (PASS == kPassG2P2G) count_key(c, key);
       }
