@@ -8,7 +8,8 @@ gate accepts a refined prediction only when its consistency residual is at most 
 the trial stress, so the learned step carries the same stated stress error as the exact one.
 What the trained network gains over the method without it: the share of plastic returns it serves
 (the rest run the bisection), against an untrained network of the same shape (about 98% against
-about half in the impact).
+about half in the impact). The Newton-gated mode runs the same refinement and gate from a guess
+taken from the initial flow stress, with no network, under the same bounds.
 """
 import numpy as np
 import pytest
