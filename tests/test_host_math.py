@@ -236,7 +236,9 @@ def test_learned_johnson_cook_gate_against_the_oracle(harness, model):
     accepted increment satisfies the FP64 oracle's consistency condition
     (src/three/metal-plasticity.js:28-34) to that bound plus FP32 rounding,
     |q - 3 mu / J dep - flow(ep + dep, dep / dt, T)| <= 2e-5 q, and agrees with the exact bisection.
-    A guess the gate cannot vouch for (no Newton steps from a wrong root) is rejected."""
+    A guess the gate cannot vouch for (no Newton steps from a wrong root) is rejected. The
+    Newton-gated mode's guess from the initial flow stress passes within eight steps, to the same
+    bounds."""
     from mpm_b200 import scenes
     mat = scenes.johnson_cook_metal(model)
     om = orc.material_from(mat)
@@ -273,3 +275,13 @@ def test_learned_johnson_cook_gate_against_the_oracle(harness, model):
         assert abs(dl[i] - dep_exact[i]) <= 2e-5 * s[i] + 1e-4 * dep_exact[i], i
     bad, _, _, _ = refine(np.clip(u_exact * 3 + 0.3, 0, 1), 0)
     assert bad.mean() <= 0.05
+    # the Newton-gated mode's guess, the root of the rate- and hardening-free condition: within eight
+    # Newton steps the gate passes for all but a few states, every accepted increment satisfies the
+    # oracle's consistency condition to the gate's bound, and it agrees with the bisection
+    u0 = np.clip(1 - flow0 / q, 0, 1)
+    ok8, dl8, _, _ = refine(u0, 8)
+    assert ok8.mean() >= 0.99, ok8.mean()
+    for i in np.flatnonzero(ok8):
+        r = q[i] - 3 * mat.mu / J[i] * dl8[i] - orc.flow_stress(model, ep[i] + dl8[i], dl8[i] / dt[i], T[i], om)
+        assert abs(r) <= 2e-5 * q[i], (i, r / q[i])
+        assert abs(dl8[i] - dep_exact[i]) <= 2e-5 * s[i] + 1e-4 * dep_exact[i], i
